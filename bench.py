@@ -1,0 +1,356 @@
+"""Benchmark of the CCTag detection hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config NAME]
+
+One step = one 1920x1080 synthetic frame (12 markers, noise, motion blur,
+illumination gradient; seeded) through ``cctagb_detect``.  N > 1 runs one
+independent replica per GPU (frames are independent units: no collective on
+the data path); the reported value is frames/s over all ranks, timed as the
+max over ranks.
+
+``value``: frames/s with the frame already in device memory
+(``cctagb_detect_device``).  ``e2e``: frames/s through ``cctagb_detect`` with
+the frame in pinned host memory (host->device copy and the result download
+inside the timed region).  Between timed steps the L2 is flushed by writing a
+256 MiB buffer (untimed); each step is bracketed by CUDA events on the
+library's stream.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "1080p frames/s + per-stage HBM GB/s; batched/adjoint vs plain at <=0.05 px"
+UNIT = "frames/s"
+N_FRAMES = 4  # distinct seeded frames cycled through the steps
+
+
+# ------------------------------------------------------------------ helpers --
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([c.strip() for c in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_frames(config, n=N_FRAMES):
+    from cctag_b200.synth import config_frame
+
+    return [config_frame(config, seed=100 + i).image for i in range(n)]
+
+
+# -------------------------------------------------------- algorithmic bytes --
+def stage_bytes(levels, E, S, V):
+    """Algorithmic bytes per stage for one frame (n = level pixels, E = edge
+    points, S = seeds, V = votes cast)."""
+    n = [w * h for (w, h) in levels]
+    nt = sum(n)
+    Et, St, Vt = sum(E), sum(S), sum(V)
+    return {
+        "pyramid": n[0] + sum(n[1:]),                 # read level 0, write levels 1..3
+        "deriv_nms": 6 * nt,                          # 1 B in, dx+dy 4 B + class map 1 B out
+        "hyst_merge": 1 * nt,                         # class map in (parents are its output)
+        "hyst_compress": 1 * nt,                      # class map in
+        "final_thin": 1 * nt + nt // 8,               # hysteresis result in, edge bitmap out
+        "row_scan": 8 * sum(h for (_, h) in levels),
+        "emit": nt // 8 + 8 * Et + 4 * Et + 4 * Et,   # bitmap in, dx/dy gathers, points + index map out
+        "walk": 8 * Et + 8 * Et + nt // 8,            # points + gradients in, links out, bitmap once
+        "vote": 8 * Et + 8 * Et,                      # links in, chosen + length out
+        "voter_scan": 4 * Et + 4 * Et,
+        "voter_fill": 4 * Et + 4 * Vt,
+        "voter_sort": 8 * Vt + 4 * Et + 8 * St,
+    }
+
+
+# ------------------------------------------------------------ the b200 arm --
+def run_b200(args, rank, world, local):
+    import torch
+
+    import cctag_b200
+    from cctag_b200 import capi
+
+    torch.cuda.set_device(local)
+    frames = make_frames(args.config)
+    H, W = frames[0].shape
+    det = cctag_b200.Detector(max_w=W, max_h=H)
+    stream = torch.cuda.ExternalStream(det.stream)
+    d_frames = [torch.from_numpy(f).to(f"cuda:{local}") for f in frames]
+    h_frames = [torch.from_numpy(f).pin_memory() for f in frames]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step_device(i):
+        t = d_frames[i % len(d_frames)]
+        return det.detect_device(t.data_ptr(), W, H, W, frame_id=i)
+
+    def step_host(i):
+        t = h_frames[i % len(h_frames)]
+        out = (capi.Marker * 256)()
+        n = C.c_int()
+        st = capi.Stats()
+        det._check(det._lib.cctagb_detect(det._h, C.c_void_p(t.data_ptr()), W, H, W, i, out, 256, C.byref(n),
+                                          C.byref(st)), "detect")
+        return [out[k] for k in range(n.value)], st
+
+    def timed(step_fn, steps):
+        total = 0.0
+        last = None
+        for i in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            last = step_fn(i)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total, last
+
+    for i in range(args.warmup):
+        step_device(i)
+        step_host(i)
+    torch.cuda.synchronize()
+    barrier(world)
+    with ClockSampler(local) as clk:
+        ms_dev, (markers, stats) = timed(step_device, args.steps)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms_e2e, (_, stats_h) = timed(step_host, args.steps)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_dev = max_over_ranks(ms_dev, world)
+    ms_e2e = max_over_ranks(ms_e2e, world)
+
+    # Per-stage device times (events captured between the stages), separate pass.
+    det.set_stage_timing(True)
+    acc = {}
+    for i in range(max(3, args.steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        step_device(i)
+        for k, v in det.stage_times().items():
+            acc.setdefault(k, []).append(v)
+    det.set_stage_timing(False)
+    stage_ms = {k: statistics.median(v) for k, v in acc.items()}
+
+    levels = [det.level_size(l) for l in range(4)]
+    E = [stats.edge_points[l] for l in range(4)]
+    S = [stats.seeds[l] for l in range(4)]
+    V = [int(len(det.votes(l)["vlist"])) for l in range(4)]
+    sb = stage_bytes(levels, E, S, V)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    stages = {k: {"ms": round(stage_ms[k], 5), "bytes": sb[k],
+                  "GB_s": round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) if stage_ms[k] > 0 else None}
+              for k in sb}
+    top = max(stage_ms, key=lambda k: stage_ms[k])
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(top)
+    ach = sb[top] / (stage_ms[top] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": peak_src}
+
+    fps_dev = world * args.steps / (ms_dev * 1e-3)
+    fps_e2e = world * args.steps / (ms_e2e * 1e-3)
+    kernels_per_step = 15
+    line = {
+        "metric": METRIC, "value": round(fps_dev, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_dev / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16/f32", "data": "synthetic",
+        "config": {"workload": f"{args.config}: detection step = image stage (pyramid..seeds)",
+                   "frame": f"{W}x{H}", "levels": levels, "edge_points": E, "seeds": S,
+                   "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": round(fps_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": W * H,
+                "d2h_bytes_per_step": 32 * 4},
+        "stages": stages,
+        "roofline": roofline,
+        "gpu_launches": kernels_per_step * args.steps * 2,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(frames[:1], budget_s=args.cpu_budget, threads=1)
+    det.close()
+    return line
+
+
+# ------------------------------------------------------ CPU (oracle) legs --
+def oracle_frame(img):
+    """Reference CPU image stage + vote (C++ restatement), one frame."""
+    import oracle
+
+    for src in oracle.pyramid(img, 4):
+        dx, dy, e = oracle.level(src)
+        oracle.vote(e, dx, dy)
+
+
+def cpu_baseline(frames, budget_s=15.0, threads=1):
+    import oracle
+
+    oracle.load()
+    oracle_frame(frames[0])  # warm
+    t0 = time.perf_counter()
+    n = 0
+    if threads == 1:
+        while time.perf_counter() - t0 < budget_s or n < 1:
+            oracle_frame(frames[n % len(frames)])
+            n += 1
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(threads) as ex:
+            while time.perf_counter() - t0 < budget_s or n < threads:
+                list(ex.map(oracle_frame, [frames[(n + k) % len(frames)] for k in range(threads)]))
+                n += threads
+    dt = time.perf_counter() - t0
+    return {"value": round(n / dt, 3), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} frames of the same workload in {dt:.1f} s (image stage + vote, C++ restatement)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    frames = make_frames(args.config)
+    threads = os.cpu_count() or 1
+    import oracle
+
+    oracle.load()
+    for i in range(args.warmup):
+        oracle_frame(frames[i % len(frames)])
+    from concurrent.futures import ThreadPoolExecutor
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        for s in range(args.steps):
+            list(ex.map(oracle_frame, [frames[(s + k) % len(frames)] for k in range(threads)]))
+    dt = time.perf_counter() - t0
+    fps = args.steps * threads / dt
+    H, W = frames[0].shape
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16/f32",
+        "data": "synthetic",
+        "config": {"workload": f"{args.config}: detection step = image stage (pyramid..seeds)", "frame": f"{W}x{H}"},
+        "cpu_baseline": {"value": round(fps, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{threads} frames per step, one per host thread (C++ restatement of the "
+                                   "reference CPU path; the reference cannot be built here)"},
+        "e2e": {"value": round(fps, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="c2_1080p")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line))
+        return
+    rank, world, local = dist_setup(args.gpus)
+    line = run_b200(args, rank, world, local)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+"""B200-native CCTag detection hot path.
+
+Python view of the C ABI (``include/cctag_b200.h``) for tests, benchmarks and
+scripting.  C++ callers use the header-only shim ``include/cctag_b200/ICCTag.hpp``
+which mirrors the reference's ``ICCTag.hpp`` API.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import CCTagError, Params, default_params
+
+__all__ = ["Detector", "CCTagError", "Params", "default_params", "capi"]
+
+
+class Detector:
+    """One handle (device arena, stream, captured graphs).  Not thread-safe."""
+
+    def __init__(self, params: Params | None = None, max_w: int = 1920, max_h: int = 1080, max_batch: int = 1):
+        self._lib = capi.load()
+        self.params = params if params is not None else default_params(3)
+        h = C.c_void_p()
+        st = self._lib.cctagb_create(C.byref(self.params), int(max_w), int(max_h), int(max_batch), C.byref(h))
+        if st != capi.OK:
+            raise CCTagError(st, f"cctagb_create failed: {self._lib.cctagb_status_string(st).decode()}")
+        self._h = h
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cctagb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st != capi.OK:
+            msg = self._lib.cctagb_last_error_string(self._h).decode()
+            raise CCTagError(st, f"{what}: {msg}")
+
+    # -- configuration -----------------------------------------------------
+    def set_bank(self, ratios):
+        a = np.ascontiguousarray(np.asarray(ratios, dtype=np.float32))
+        if a.ndim != 2:
+            raise ValueError("bank must be a 2-D array (ids x ratios)")
+        self._check(self._lib.cctagb_set_bank(self._h, capi.ptr(a), a.shape[0], a.shape[1]), "set_bank")
+
+    # -- image stage ---------------------------------------------------------
+    def image_stage(self, gray: np.ndarray):
+        g = np.ascontiguousarray(gray, dtype=np.uint8)
+        H, W = g.shape
+        self._check(self._lib.cctagb_image_stage(self._h, capi.ptr(g), W, H, W, 0), "image_stage")
+
+    def image_stage_device(self, dptr: int, w: int, h: int, pitch: int):
+        self._check(self._lib.cctagb_image_stage(self._h, C.c_void_p(dptr), w, h, pitch, 1), "image_stage")
+
+    def level_size(self, level: int):
+        w, h = C.c_int(), C.c_int()
+        self._check(self._lib.cctagb_level_size(self._h, level, C.byref(w), C.byref(h)), "level_size")
+        return w.value, h.value
+
+    def level_planes(self, level: int):
+        w, h = self.level_size(level)
+        src = np.empty((h, w), np.uint8)
+        dx = np.empty((h, w), np.int16)
+        dy = np.empty((h, w), np.int16)
+        edges = np.empty((h, w), np.uint8)
+        self._check(self._lib.cctagb_level_planes(self._h, level, capi.ptr(src), capi.ptr(dx), capi.ptr(dy),
+                                                  capi.ptr(edges)), "level_planes")
+        return src, dx, dy, edges
+
+    def edge_points(self, level: int):
+        w, h = self.level_size(level)
+        cap = w * h
+        n = C.c_int()
+        x = np.empty(cap, np.int32)
+        y = np.empty(cap, np.int32)
+        self._check(self._lib.cctagb_level_edge_points(self._h, level, cap, C.byref(n), capi.ptr(x), capi.ptr(y)),
+                    "edge_points")
+        return x[:n.value].copy(), y[:n.value].copy()
+
+    def links(self, level: int):
+        x, _ = self.edge_points(level)
+        n = len(x)
+        b = np.empty(max(n, 1), np.int32)
+        a = np.empty(max(n, 1), np.int32)
+        self._check(self._lib.cctagb_level_links(self._h, level, max(n, 1), capi.ptr(b), capi.ptr(a)), "links")
+        return b[:n].copy(), a[:n].copy()
+
+    def votes(self, level: int):
+        x, _ = self.edge_points(level)
+        n = len(x)
+        cap = max(n, 1)
+        chosen = np.empty(cap, np.int32)
+        nvotes = np.empty(cap, np.int32)
+        flow = np.empty(cap, np.float32)
+        voff = np.empty(cap + 1, np.int32)
+        vlist = np.empty(cap, np.int32)
+        nv = np.zeros(1, np.int32)
+        self._check(self._lib.cctagb_level_votes(self._h, level, cap, capi.ptr(chosen), capi.ptr(nvotes),
+                                                 capi.ptr(flow), capi.ptr(voff), capi.ptr(vlist), cap,
+                                                 capi.ptr(nv)), "votes")
+        return dict(chosen=chosen[:n].copy(), nvotes=nvotes[:n].copy(), flow=flow[:n].copy(),
+                    voff=voff[:n + 1].copy(), vlist=vlist[:nv[0]].copy())
+
+    def seeds(self, level: int):
+        x, _ = self.edge_points(level)
+        cap = max(len(x), 1)
+        s = np.empty(cap, np.int32)
+        n = C.c_int()
+        self._check(self._lib.cctagb_level_seeds(self._h, level, cap, capi.ptr(s), C.byref(n)), "seeds")
+        return s[:n.value].copy()
+
+    def canny_from_derivatives(self, dx: np.ndarray, dy: np.ndarray) -> np.ndarray:
+        dx = np.ascontiguousarray(dx, dtype=np.int16)
+        dy = np.ascontiguousarray(dy, dtype=np.int16)
+        H, W = dx.shape
+        out = np.empty((H, W), np.uint8)
+        self._check(self._lib.cctagb_canny_from_derivatives(self._h, capi.ptr(dx), capi.ptr(dy), W, H,
+                                                            capi.ptr(out)), "canny_from_derivatives")
+        return out
+
+    # -- timing --------------------------------------------------------------
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(self._lib.cctagb_get_stream(self._h, C.byref(s)), "get_stream")
+        return s.value or 0
+
+    def set_stage_timing(self, on: bool = True):
+        self._check(self._lib.cctagb_set_stage_timing(self._h, int(bool(on))), "set_stage_timing")
+
+    def stage_times(self) -> dict:
+        ms = np.zeros(64, np.float32)
+        n = C.c_int()
+        self._check(self._lib.cctagb_stage_times(self._h, 64, capi.ptr(ms), C.byref(n)), "stage_times")
+        return {self._lib.cctagb_stage_name(k).decode(): float(ms[k]) for k in range(n.value)}
+
+    # -- detection -----------------------------------------------------------
+    def detect_device(self, dptr: int, w: int, h: int, pitch: int, frame_id: int = 0, cap: int = 256):
+        out = (capi.Marker * cap)()
+        n = C.c_int()
+        stats = capi.Stats()
+        self._check(self._lib.cctagb_detect_device(self._h, C.c_void_p(dptr), w, h, pitch, frame_id, out, cap,
+                                                   C.byref(n), C.byref(stats)), "detect_device")
+        return [out[i] for i in range(n.value)], stats
+
+    def detect(self, gray: np.ndarray, frame_id: int = 0, cap: int = 256):
+        g = np.ascontiguousarray(gray, dtype=np.uint8)
+        H, W = g.shape
+        out = (capi.Marker * cap)()
+        n = C.c_int()
+        stats = capi.Stats()
+        self._check(self._lib.cctagb_detect(self._h, capi.ptr(g), W, H, W, frame_id, out, cap, C.byref(n),
+                                            C.byref(stats)), "detect")
+        return [out[i] for i in range(n.value)], stats

@@ -1,0 +1,270 @@
+// C ABI of the library (include/cctag_b200.h).  Converts exceptions into
+// status codes; nothing crosses the ABI as a C++ exception.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "cctag_b200.h"
+#include "detector.hpp"
+#include "pipeline.hpp"
+
+struct cctagb_handle {
+    std::unique_ptr<cctagb::Detector> det;
+    std::string last_error;
+};
+
+namespace {
+
+template <class F>
+cctagb_status guarded(cctagb_handle* h, F&& f)
+{
+    try {
+        f();
+        if (h) h->last_error.clear();
+        return CCTAGB_OK;
+    } catch (const cctagb::Error& e) {
+        if (h) h->last_error = e.msg;
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        if (h) h->last_error = "host allocation failed";
+        return CCTAGB_INTERNAL;
+    } catch (const std::exception& e) {
+        if (h) h->last_error = e.what();
+        return CCTAGB_INTERNAL;
+    } catch (...) {
+        if (h) h->last_error = "unknown error";
+        return CCTAGB_INTERNAL;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void cctagb_params_default(cctagb_params* p, int nCrowns)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->cannyThrLow = 0.01f;
+    p->cannyThrHigh = 0.04f;
+    p->distSearch = 30;
+    p->thrGradientMagInVote = 2500;
+    p->angleVoting = 0.f;
+    p->ratioVoting = 4.f;
+    p->averageVoteMin = 0.f;
+    p->thrMedianDistanceEllipse = 3.f;
+    p->maximumNbSeeds = 500;
+    p->maximumNbCandidatesLoopTwo = 40;
+    p->nCrowns = nCrowns;
+    p->nCircles = 2 * nCrowns;
+    p->minPointsSegmentCandidate = 10;
+    p->minVotesToSelectCandidate = 3;
+    p->threshRobustEstimationOfOuterEllipse = 30.f;
+    p->ellipseGrowingEllipticHullWidth = 2.3f;
+    p->windowSizeOnInnerEllipticSegment = 20;
+    p->numberOfMultiresLayers = 4;
+    p->numberOfProcessedMultiresLayers = 4;
+    p->nSamplesOuterEllipse = 150;
+    p->numCutsInIdentStep = 22;
+    p->numSamplesOuterEdgePointsRefinement = 20;
+    p->cutsSelectionTrials = 500;
+    p->sampleCutLength = 100;
+    p->imagedCenterNGridSample = 5;
+    p->imagedCenterNeighbourSize = 0.20f;
+    p->minIdentProba = 1e-6f;
+    p->useLMDif = 1;
+    p->searchForAnotherSegment = 1;
+    p->writeOutput = 0;
+    p->doIdentification = 1;
+    p->maxEdges = 20000;
+    p->refineMode = CCTAGB_REFINE_GRID;
+    p->gnIterations = 6;
+    p->edgeCapacityDivisor = 4;
+}
+
+const char* cctagb_status_string(cctagb_status s)
+{
+    switch (s) {
+    case CCTAGB_OK: return "ok";
+    case CCTAGB_BAD_ARG: return "bad argument";
+    case CCTAGB_CUDA_ERROR: return "CUDA error";
+    case CCTAGB_NO_DEVICE: return "no sm_100 CUDA device";
+    case CCTAGB_OVERFLOW_EDGES: return "edge-point capacity exceeded";
+    case CCTAGB_OVERFLOW_SEEDS: return "seed capacity exceeded";
+    case CCTAGB_OVERFLOW_VOTERS: return "voter capacity exceeded";
+    case CCTAGB_HYST_NO_CONVERGE: return "hysteresis did not converge";
+    case CCTAGB_TOO_LARGE: return "frame larger than the handle";
+    case CCTAGB_BANK_ERROR: return "bad marker bank";
+    case CCTAGB_INTERNAL: return "internal error";
+    }
+    return "unknown status";
+}
+
+cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int max_batch, cctagb_handle** out)
+{
+    if (!out) return CCTAGB_BAD_ARG;
+    *out = nullptr;
+    cctagb_params def;
+    if (!p) {
+        cctagb_params_default(&def, 3);
+        p = &def;
+    }
+    std::unique_ptr<cctagb_handle> h(new (std::nothrow) cctagb_handle);
+    if (!h) return CCTAGB_INTERNAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return CCTAGB_NO_DEVICE;
+    }
+    const cctagb_status s = guarded(h.get(), [&] { h->det.reset(new cctagb::Detector(*p, max_w, max_h, max_batch)); });
+    if (s != CCTAGB_OK) return s;
+    *out = h.release();
+    return CCTAGB_OK;
+}
+
+cctagb_status cctagb_destroy(cctagb_handle* h)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    delete h;
+    return CCTAGB_OK;
+}
+
+const char* cctagb_last_error_string(const cctagb_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+cctagb_status cctagb_set_bank(cctagb_handle* h, const float* ratios, int n_ids, int n_ratios)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->set_bank(ratios, n_ids, n_ratios); });
+}
+
+cctagb_status cctagb_image_stage(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int is_device)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->pipeline().image_stage(gray, w, hgt, pitch, is_device != 0); });
+}
+
+cctagb_status cctagb_level_size(cctagb_handle* h, int level, int* w, int* hgt)
+{
+    if (!h || !w || !hgt) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->pipeline().level_size(level, w, hgt); });
+}
+
+cctagb_status cctagb_level_planes(cctagb_handle* h, int level, uint8_t* src, int16_t* dx, int16_t* dy, uint8_t* edges)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->pipeline().copy_planes(level, src, dx, dy, edges); });
+}
+
+cctagb_status cctagb_level_edge_points(cctagb_handle* h, int level, int cap, int* n, int32_t* x, int32_t* y)
+{
+    if (!h || !n) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        cctagb::HostLevel hl;
+        h->det->pipeline().download_level(level, hl);
+        *n = hl.E;
+        if (hl.E > cap) throw cctagb::Error{CCTAGB_BAD_ARG, "output capacity too small"};
+        for (int i = 0; i < hl.E; ++i) {
+            if (x) x[i] = hl.exy[i] & 0xffff;
+            if (y) y[i] = hl.exy[i] >> 16;
+        }
+    });
+}
+
+cctagb_status cctagb_level_links(cctagb_handle* h, int level, int cap, int32_t* before, int32_t* after)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        cctagb::HostLevel hl;
+        h->det->pipeline().download_level(level, hl);
+        if (hl.E > cap) throw cctagb::Error{CCTAGB_BAD_ARG, "output capacity too small"};
+        if (before) std::copy(hl.before.begin(), hl.before.end(), before);
+        if (after) std::copy(hl.after.begin(), hl.after.end(), after);
+    });
+}
+
+cctagb_status cctagb_level_votes(cctagb_handle* h, int level, int cap, int32_t* chosen, int32_t* nvotes,
+                                 float* flow_length, int32_t* voter_off, int32_t* voter_list, int voter_cap,
+                                 int32_t* n_voters)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        cctagb::HostLevel hl;
+        h->det->pipeline().download_level(level, hl);
+        if (hl.E > cap || hl.V > voter_cap) throw cctagb::Error{CCTAGB_BAD_ARG, "output capacity too small"};
+        if (n_voters) *n_voters = hl.V;
+        if (chosen) {
+            std::fill(chosen, chosen + hl.E, -1);
+            for (int c = 0; c < hl.E; ++c)
+                for (int k = hl.voff[c]; k < hl.voff[c + 1]; ++k) chosen[hl.vlist[k]] = c;
+        }
+        for (int c = 0; c < hl.E; ++c) {
+            if (nvotes) nvotes[c] = hl.voff[c + 1] - hl.voff[c];
+            if (flow_length) flow_length[c] = hl.flow[c];
+        }
+        if (voter_off) std::copy(hl.voff.begin(), hl.voff.end(), voter_off);
+        if (voter_list) std::copy(hl.vlist.begin(), hl.vlist.end(), voter_list);
+    });
+}
+
+cctagb_status cctagb_level_seeds(cctagb_handle* h, int level, int cap, int32_t* seeds, int* n)
+{
+    if (!h || !n) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        cctagb::HostLevel hl;
+        h->det->pipeline().download_level(level, hl);
+        *n = int(hl.seeds.size());
+        if (*n > cap) throw cctagb::Error{CCTAGB_BAD_ARG, "output capacity too small"};
+        if (seeds) std::copy(hl.seeds.begin(), hl.seeds.end(), seeds);
+    });
+}
+
+cctagb_status cctagb_get_stream(cctagb_handle* h, void** stream)
+{
+    if (!h || !stream) return CCTAGB_BAD_ARG;
+    *stream = reinterpret_cast<void*>(h->det->pipeline().stream());
+    return CCTAGB_OK;
+}
+
+cctagb_status cctagb_set_stage_timing(cctagb_handle* h, int enable)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->pipeline().set_stage_timing(enable != 0); });
+}
+
+cctagb_status cctagb_stage_times(cctagb_handle* h, int cap, float* ms, int* n)
+{
+    if (!h || !n) return CCTAGB_BAD_ARG;
+    *n = cctagb::kStageCount;
+    if (cap < cctagb::kStageCount || !ms) return CCTAGB_BAD_ARG;
+    const float* src = h->det->pipeline().stage_ms();
+    std::copy(src, src + cctagb::kStageCount, ms);
+    return CCTAGB_OK;
+}
+
+const char* cctagb_stage_name(int stage) { return cctagb::stage_name(stage); }
+
+cctagb_status cctagb_canny_from_derivatives(cctagb_handle* h, const int16_t* dx, const int16_t* dy, int w, int hgt,
+                                            uint8_t* edges)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->pipeline().canny_only(dx, dy, w, hgt, edges); });
+}
+
+cctagb_status cctagb_detect(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int frame_id,
+                            cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->detect(gray, w, hgt, pitch, false, frame_id, out, cap, n_out, stats); });
+}
+
+cctagb_status cctagb_detect_device(cctagb_handle* h, const uint8_t* d_gray, int w, int hgt, size_t pitch,
+                                   int frame_id, cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->detect(d_gray, w, hgt, pitch, true, frame_id, out, cap, n_out, stats); });
+}
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+// Shared definitions of the B200 CCTag library (host and device).
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "cctag_b200.h"
+
+namespace cctagb {
+
+constexpr int kMaxLevels = 4;
+
+// One pyramid level as the kernels see it.  All pointers are device memory.
+struct LevelView {
+    int W, H, WW;            // size; WW = 32-pixel words per bitmap row
+    uint8_t* src;            // W*H gray
+    int16_t* dx;             // W*H
+    int16_t* dy;             // W*H
+    uint8_t* map;            // W*H: 0 no edge, 1 weak candidate, 2 strong candidate
+    int32_t* label;          // W*H union-find parents (valid at candidates)
+    uint8_t* sroot;          // W*H strong-component flags (valid at roots)
+    uint32_t* bitmap;        // WW*H final thinned edges, bit x&31 of word x>>5
+    int32_t* idxmap;         // W*H edge index (valid where the bitmap is set)
+    int32_t* row_count;      // H
+    int32_t* row_off;        // H+1
+    int cap;                 // edge-point capacity
+    int32_t* exy;            // cap: x | y << 16
+    int32_t* grad;           // cap: (uint16)dx | dy << 16
+    int32_t* before;         // cap
+    int32_t* after;          // cap
+    int32_t* chosen;         // cap
+    float* total;            // cap: field-line length of a successful vote
+    int32_t* nvotes;         // cap: votes received
+    int32_t* fill;           // cap: fill cursors of the voter lists
+    int32_t* voff;           // cap+1: voter list offsets (CSR)
+    int32_t* vlist;          // cap: voter lists, ascending voter index
+    float* flow;             // cap: running-mean flow length (Vote.cpp:232)
+    int seedcap;
+    int32_t* seed_idx;       // seedcap
+    int32_t* seed_key;       // seedcap: index of the voter that made it a seed
+    int32_t* bigq;           // cap: points whose voter list needs a block sort
+    // launch geometry of the tiled kernels
+    int nms_tx, nms_tiles;   // 30x30 output tiles
+    int thin_tx, thin_tiles; // 32x16 output tiles
+    int pix_blocks;          // 256-pixel blocks
+};
+
+struct LevelCounters {
+    int32_t E;       // edge points
+    int32_t V;       // votes cast (= voters)
+    int32_t S;       // seeds
+    int32_t err;     // error bits (kErr*)
+    int32_t bigq;    // long voter lists queued for the block sort
+    int32_t pad[3];
+};
+
+constexpr int kErrEdgeOverflow = 1;
+constexpr int kErrSeedOverflow = 2;
+constexpr int kErrUnionFind = 4;
+
+struct Levels {
+    int n;
+    LevelView l[kMaxLevels];
+    LevelCounters* cnt;  // device, n entries
+};
+
+struct VoteParamsDev {
+    int distSearch;
+    int thrGradient;
+    float angleVoting;
+    float ratioVoting;
+    int nCrowns;
+    int minVotes;
+    int low, high;  // Canny thresholds after cvFloor
+};
+
+// Error type carried by host code; converted to cctagb_status at the ABI.
+struct Error {
+    cctagb_status status;
+    std::string msg;
+};
+
+#define CCTAGB_CUDA(call)                                                                   \
+    do {                                                                                    \
+        cudaError_t e__ = (call);                                                           \
+        if (e__ != cudaSuccess)                                                             \
+            throw ::cctagb::Error{CCTAGB_CUDA_ERROR, std::string(#call) + ": " +             \
+                                                         cudaGetErrorString(e__)};          \
+    } while (0)
+
+// Optional per-stage timing: when `ev` is non-null the launcher records
+// ev[k] after stage k (ev[0] before the first stage), kStageCount+1 events.
+enum Stage {
+    kStPyramid = 0, kStDerivNms, kStHystMerge, kStHystCompress, kStFinalThin, kStRowScan, kStEmit,
+    kStWalk, kStVote, kStVoterScan, kStVoterFill, kStVoterSort, kStageCount
+};
+const char* stage_name(int k);
+
+// Host launchers (image_stage.cu).
+void upload_constants(const float* bank, int n_ids, int n_ratios);
+void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, bool fused_pyramid,
+                        cudaEvent_t* ev = nullptr);
+void launch_canny_only(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s);
+
+}  // namespace cctagb

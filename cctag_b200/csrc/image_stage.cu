@@ -1,0 +1,925 @@
+// Image stage of the CCTag hot path on sm_100a: pyramid, 9x9 DoG derivatives,
+// Canny NMS + hysteresis, thinning, raster-order edge compaction, Bresenham
+// gradient walk, vote, voter lists and seeds.  Every launch covers all pyramid
+// levels at once (the block index is split into level and tile), no launch
+// needs a host synchronisation, so a frame is one capturable launch sequence.
+//
+// Bit-exactness with the reference CPU path (file:line in the CCTag project):
+//  * derivatives: same 72-tap FMA chain as cv::filter2D, cvRecode.cpp:74-92
+//  * magnitude / NMS / hysteresis: cvRecode.cpp:174-409 (final edge set is the
+//    8-connected components of NMS candidates that hold a strong pixel)
+//  * thinning: thinning.cpp:12-51 (Lam-Lee-Suen tables, temp border = 0)
+//  * edge order: raster order, Canny.cpp:15-31
+//  * walk: Bresenham.cpp:18-209, vote: Vote.cpp:58-247 (no FMA contraction,
+//    IEEE division and square root, same accumulation order)
+#include <cstdint>
+
+#include "common.hpp"
+
+namespace cctagb {
+
+__constant__ float cK[9][9];         // kerneldX of cvRecode.cpp:74-83
+__constant__ uint32_t cThin[2][16];  // thinning tables as bitsets
+
+// ------------------------------------------------------------------ utils --
+__device__ __forceinline__ int level_of_block(const Levels& lv, int b, int LevelView::*tiles, int& local)
+{
+    int l = 0;
+    while (l < lv.n - 1 && b >= lv.l[l].*tiles) {
+        b -= lv.l[l].*tiles;
+        ++l;
+    }
+    local = b;
+    return l;
+}
+
+__device__ __forceinline__ int16_t sat_round16(float s)
+{
+    float r = rintf(s);
+    r = fminf(32767.f, fmaxf(-32768.f, r));
+    return int16_t(r);
+}
+
+__device__ __forceinline__ bool edge_bit(const LevelView& L, int x, int y)
+{
+    return (L.bitmap[size_t(y) * L.WW + (x >> 5)] >> (x & 31)) & 1u;
+}
+
+// ---------------------------------------------------------------- pyramid --
+// ImagePyramid.cpp:23-52, Level.cpp:57-81.  Exact 2x reductions (every level
+// of a frame whose sides are multiples of 8) are the rounded 2x2 mean, as
+// cv::resize's area fast path; one thread builds an 8x8 block of level 0 into
+// levels 1..3.
+__global__ void k_pyramid3(Levels lv)
+{
+    const LevelView& L0 = lv.l[0];
+    const int W3 = L0.W >> 3, H3 = L0.H >> 3;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W3 || y >= H3) return;
+    uint32_t p[8][8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const uint2 v = *reinterpret_cast<const uint2*>(L0.src + size_t(8 * y + r) * L0.W + 8 * x);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            p[r][c] = (v.x >> (8 * c)) & 0xff;
+            p[r][c + 4] = (v.y >> (8 * c)) & 0xff;
+        }
+    }
+    uint32_t q1[4][4], q2[2][2];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            q1[r][c] = (p[2 * r][2 * c] + p[2 * r][2 * c + 1] + p[2 * r + 1][2 * c] + p[2 * r + 1][2 * c + 1] + 2) >> 2;
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            q2[r][c] = (q1[2 * r][2 * c] + q1[2 * r][2 * c + 1] + q1[2 * r + 1][2 * c] + q1[2 * r + 1][2 * c + 1] + 2) >> 2;
+    const uint32_t q3 = (q2[0][0] + q2[0][1] + q2[1][0] + q2[1][1] + 2) >> 2;
+    const LevelView& L1 = lv.l[1];
+    const LevelView& L2 = lv.l[2];
+    const LevelView& L3 = lv.l[3];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+        *reinterpret_cast<uint32_t*>(L1.src + size_t(4 * y + r) * L1.W + 4 * x) =
+            q1[r][0] | (q1[r][1] << 8) | (q1[r][2] << 16) | (q1[r][3] << 24);
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+        *reinterpret_cast<uint16_t*>(L2.src + size_t(2 * y + r) * L2.W + 2 * x) = uint16_t(q2[r][0] | (q2[r][1] << 8));
+    L3.src[size_t(y) * L3.W + x] = uint8_t(q3);
+}
+
+// One level from the previous one, any size: exact 2x -> 2x2 rounded mean,
+// otherwise cv::resize INTER_LINEAR fixed point (11-bit coefficients and the
+// vectorised vertical pass of OpenCV: 16-bit high products, rounding shift 2).
+__device__ __forceinline__ void resize_coef(int d, int dn, int sn, int& s, int& c0)
+{
+    const double scale = double(sn) / dn;
+    float f = float((d + 0.5) * scale - 0.5);
+    s = int(floorf(f));
+    f -= float(s);
+    if (s < 0) { f = 0.f; s = 0; }
+    if (s >= sn - 1) { f = 0.f; s = sn - 1; }
+    c0 = int(rintf(__fmul_rn(1.f - f, 2048.f)));
+}
+
+__global__ void k_resize_level(const uint8_t* __restrict__ src, int sw, int sh, uint8_t* __restrict__ dst, int dw, int dh)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= dw || y >= dh) return;
+    if (sw == 2 * dw && sh == 2 * dh) {
+        const uint8_t* p = src + size_t(2 * y) * sw + 2 * x;
+        dst[size_t(y) * dw + x] = uint8_t((p[0] + p[1] + p[sw] + p[sw + 1] + 2) >> 2);
+        return;
+    }
+    int sx, cx0, sy, cy0;
+    resize_coef(x, dw, sw, sx, cx0);
+    resize_coef(y, dh, sh, sy, cy0);
+    const int cx1 = 2048 - cx0, cy1 = 2048 - cy0;
+    const int sx1 = min(sx + 1, sw - 1), sy1 = min(sy + 1, sh - 1);
+    const int r0 = src[size_t(sy) * sw + sx] * cx0 + src[size_t(sy) * sw + sx1] * cx1;
+    const int r1 = src[size_t(sy1) * sw + sx] * cx0 + src[size_t(sy1) * sw + sx1] * cx1;
+    int v = ((((r0 >> 4) * cy0) >> 16) + (((r1 >> 4) * cy1) >> 16) + 2) >> 2;
+    dst[size_t(y) * dw + x] = uint8_t(min(255, max(0, v)));
+}
+
+// --------------------------------------------- derivatives + magnitude + NMS --
+// Output tile 30x30.  Derivatives are computed on the 32x32 region around it
+// (NMS needs the magnitude of the 8 neighbours) from a 40x40 source region.
+// Thread t owns derivative column t&31 and the 8-row strip t>>5: it walks the
+// 16 source rows of its strip once and feeds each loaded row to every output
+// row whose 9x9 window covers it, which keeps each pixel's taps in the
+// reference's row-major order.
+constexpr int kNmsT = 30;      // output tile side
+constexpr int kNmsD = 32;      // derivative region side
+constexpr int kNmsS = 40;      // source region side
+
+__global__ void __launch_bounds__(128) k_deriv_nms(Levels lv, VoteParamsDev vp, int write_derivs)
+{
+    __shared__ float s_src[kNmsS][kNmsS];
+    __shared__ int16_t s_dx[kNmsD][kNmsD];
+    __shared__ int16_t s_dy[kNmsD][kNmsD];
+    __shared__ int s_mag[kNmsD][kNmsD + 1];
+
+    int tile;
+    const int l = level_of_block(lv, blockIdx.x, &LevelView::nms_tiles, tile);
+    const LevelView& L = lv.l[l];
+    const int W = L.W, H = L.H;
+    const int x0 = (tile % L.nms_tx) * kNmsT;
+    const int y0 = (tile / L.nms_tx) * kNmsT;
+    const int t = threadIdx.x;
+
+    if (write_derivs) {
+        for (int i = t; i < kNmsS * kNmsS; i += 128) {
+            const int sr = i / kNmsS, sc = i % kNmsS;
+            const int yy = min(H - 1, max(0, y0 - 5 + sr));
+            const int xx = min(W - 1, max(0, x0 - 5 + sc));
+            s_src[sr][sc] = float(L.src[size_t(yy) * W + xx]);
+        }
+        __syncthreads();
+        const int c = t & 31;
+        const int r0 = (t >> 5) * 8;
+        float ax[8], ay[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) { ax[r] = 0.f; ay[r] = 0.f; }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            float v[9];
+#pragma unroll
+            for (int j = 0; j < 9; ++j) v[j] = s_src[r0 + q][c + j];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const int i = q - r;
+                if (i < 0 || i > 8) continue;
+#pragma unroll
+                for (int j = 0; j < 9; ++j) {
+                    if (j != 4) ax[r] = __fmaf_rn(cK[i][j], v[j], ax[r]);
+                    if (i != 4) ay[r] = __fmaf_rn(cK[j][i], v[j], ay[r]);
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            s_dx[r0 + r][c] = sat_round16(ax[r]);
+            s_dy[r0 + r][c] = sat_round16(ay[r]);
+        }
+    } else {
+        // Derivatives supplied by the caller: load them with the same halo.
+        for (int i = t; i < kNmsD * kNmsD; i += 128) {
+            const int r = i / kNmsD, c = i % kNmsD;
+            const int yy = y0 - 1 + r, xx = x0 - 1 + c;
+            int16_t gx = 0, gy = 0;
+            if (xx >= 0 && xx < W && yy >= 0 && yy < H) {
+                gx = L.dx[size_t(yy) * W + xx];
+                gy = L.dy[size_t(yy) * W + xx];
+            }
+            s_dx[r][c] = gx;
+            s_dy[r][c] = gy;
+        }
+    }
+    __syncthreads();
+    // Magnitude, rintf(sqrtf(dx^2 + dy^2)) as cvRecode.cpp:200-211; 0 outside the image.
+    for (int i = t; i < kNmsD * kNmsD; i += 128) {
+        const int r = i / kNmsD, c = i % kNmsD;
+        const int yy = y0 - 1 + r, xx = x0 - 1 + c;
+        int m = 0;
+        if (xx >= 0 && xx < W && yy >= 0 && yy < H) {
+            const float fx = float(s_dx[r][c]), fy = float(s_dy[r][c]);
+            m = int(rintf(__fsqrt_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)))));
+        }
+        s_mag[r][c] = m;
+    }
+    __syncthreads();
+    // NMS, cvRecode.cpp:258-323.
+    const int TG22 = int(0.4142135623730950488016887242097 * (1 << 15) + 0.5);
+    for (int i = t; i < kNmsT * kNmsT; i += 128) {
+        const int oy = i / kNmsT, ox = i % kNmsT;
+        const int x = x0 + ox, y = y0 + oy;
+        if (x >= W || y >= H) continue;
+        const int r = oy + 1, c = ox + 1;
+        int gx = s_dx[r][c], gy = s_dy[r][c];
+        const int s = gx ^ gy;
+        const int m = s_mag[r][c];
+        gx = abs(gx);
+        gy = abs(gy);
+        bool is_max = false;
+        if (m > vp.low) {
+            const int tg22x = gx * TG22;
+            const int tg67x = tg22x + ((gx + gx) << 15);
+            const int gy15 = gy << 15;
+            if (gy15 < tg22x) {
+                is_max = m > s_mag[r][c - 1] && m >= s_mag[r][c + 1];
+            } else if (gy15 > tg67x) {
+                is_max = m > s_mag[r - 1][c] && m >= s_mag[r + 1][c];
+            } else {
+                const int sg = s < 0 ? -1 : 1;
+                is_max = m > s_mag[r - 1][c - sg] && m > s_mag[r + 1][c + sg];
+            }
+        }
+        const size_t p = size_t(y) * W + x;
+        const uint8_t cls = is_max ? (m > vp.high ? 2 : 1) : 0;
+        L.map[p] = cls;
+        if (cls) {
+            L.label[p] = int32_t(p);
+            L.sroot[p] = 0;
+        }
+        if (write_derivs) {
+            L.dx[p] = s_dx[r][c];
+            L.dy[p] = s_dy[r][c];
+        }
+    }
+}
+
+// ------------------------------------------------------------- hysteresis --
+// The reference's stack hysteresis (cvRecode.cpp:362-394) keeps exactly the
+// 8-connected components of NMS candidates that contain a strong pixel.  Here
+// the components come from a lock-free union-find (parent <= self invariant,
+// roots linked by atomicMin), which gives the same set in any schedule.
+constexpr int kUfCap = 1 << 22;
+
+__device__ __forceinline__ int uf_find(const int32_t* L, int p)
+{
+    int q = *(volatile const int32_t*)&L[p];
+    int guard = 0;
+    while (q != p && guard++ < kUfCap) {
+        p = q;
+        q = *(volatile const int32_t*)&L[p];
+    }
+    return p;
+}
+
+__device__ __forceinline__ void uf_union(int32_t* L, int a, int b, int32_t* err)
+{
+    for (int it = 0; it < kUfCap; ++it) {
+        a = uf_find(L, a);
+        b = uf_find(L, b);
+        if (a == b) return;
+        if (a > b) { const int tmp = a; a = b; b = tmp; }
+        const int old = atomicMin(&L[b], a);
+        if (old == b) return;
+        b = old;
+    }
+    atomicOr(err, kErrUnionFind);
+}
+
+__global__ void k_hyst_merge(Levels lv)
+{
+    int blk;
+    const int l = level_of_block(lv, blockIdx.x, &LevelView::pix_blocks, blk);
+    const LevelView& L = lv.l[l];
+    const int p = blk * blockDim.x + threadIdx.x;
+    if (p >= L.W * L.H) return;
+    if (!L.map[p]) return;
+    const int x = p % L.W, y = p / L.W;
+    if (x > 0 && L.map[p - 1]) uf_union(L.label, p, p - 1, &lv.cnt[l].err);
+    if (y > 0) {
+        const int u = p - L.W;
+        if (x > 0 && L.map[u - 1]) uf_union(L.label, p, u - 1, &lv.cnt[l].err);
+        if (L.map[u]) uf_union(L.label, p, u, &lv.cnt[l].err);
+        if (x + 1 < L.W && L.map[u + 1]) uf_union(L.label, p, u + 1, &lv.cnt[l].err);
+    }
+}
+
+__global__ void k_hyst_compress_mark(Levels lv)
+{
+    int blk;
+    const int l = level_of_block(lv, blockIdx.x, &LevelView::pix_blocks, blk);
+    const LevelView& L = lv.l[l];
+    const int p = blk * blockDim.x + threadIdx.x;
+    if (p >= L.W * L.H) return;
+    const uint8_t cls = L.map[p];
+    if (!cls) return;
+    const int r = uf_find(L.label, p);
+    L.label[p] = r;
+    if (cls == 2) L.sroot[r] = 1;
+}
+
+// ------------------------------------------------ final edges + thinning --
+// Output tile 32 x 16 (one warp per row, so a ballot is one bitmap word).
+constexpr int kThX = 32, kThY = 16;
+
+__global__ void __launch_bounds__(kThX * kThY) k_final_thin(Levels lv)
+{
+    __shared__ uint8_t s_e[kThY + 4][kThX + 4];
+    __shared__ uint8_t s_t[kThY + 2][kThX + 2];
+    __shared__ uint32_t s_lut[2][16];
+    int tile;
+    const int l = level_of_block(lv, blockIdx.x, &LevelView::thin_tiles, tile);
+    const LevelView& L = lv.l[l];
+    const int W = L.W, H = L.H;
+    const int x0 = (tile % L.thin_tx) * kThX;
+    const int y0 = (tile / L.thin_tx) * kThY;
+    const int t = threadIdx.y * kThX + threadIdx.x;
+    if (t < 32) s_lut[t >> 4][t & 15] = cThin[t >> 4][t & 15];
+    for (int i = t; i < (kThY + 4) * (kThX + 4); i += kThX * kThY) {
+        const int r = i / (kThX + 4), c = i % (kThX + 4);
+        const int x = x0 - 2 + c, y = y0 - 2 + r;
+        uint8_t e = 0;
+        if (x >= 0 && x < W && y >= 0 && y < H) {
+            const size_t p = size_t(y) * W + x;
+            if (L.map[p]) e = L.sroot[L.label[p]];
+        }
+        s_e[r][c] = e;
+    }
+    __syncthreads();
+    auto lut = [&](int k, int idx) -> uint8_t { return (s_lut[k][idx >> 5] >> (idx & 31)) & 1u; };
+    for (int i = t; i < (kThY + 2) * (kThX + 2); i += kThX * kThY) {
+        const int r = i / (kThX + 2), c = i % (kThX + 2);
+        const int x = x0 - 1 + c, y = y0 - 1 + r;
+        uint8_t v = 0;
+        if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1 && s_e[r + 1][c + 1]) {
+            const int rr = r + 1, cc = c + 1;
+            const int idx = s_e[rr - 1][cc - 1] * 1 + s_e[rr][cc - 1] * 2 + s_e[rr + 1][cc - 1] * 4 +
+                            s_e[rr - 1][cc] * 8 + 16 + s_e[rr + 1][cc] * 32 +
+                            s_e[rr - 1][cc + 1] * 64 + s_e[rr][cc + 1] * 128 + s_e[rr + 1][cc + 1] * 256;
+            v = lut(0, idx);
+        }
+        s_t[r][c] = v;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    bool on = false;
+    if (x < W && y < H) {
+        if (x == 0 || y == 0 || x == W - 1 || y == H - 1) {
+            on = s_e[threadIdx.y + 2][threadIdx.x + 2];
+        } else {
+            const int rr = threadIdx.y + 1, cc = threadIdx.x + 1;
+            if (s_t[rr][cc]) {
+                const int idx = s_t[rr - 1][cc - 1] * 1 + s_t[rr][cc - 1] * 2 + s_t[rr + 1][cc - 1] * 4 +
+                                s_t[rr - 1][cc] * 8 + 16 + s_t[rr + 1][cc] * 32 +
+                                s_t[rr - 1][cc + 1] * 64 + s_t[rr][cc + 1] * 128 + s_t[rr + 1][cc + 1] * 256;
+                on = lut(1, idx);
+            }
+        }
+    }
+    const uint32_t mask = __ballot_sync(0xffffffffu, on);
+    if (threadIdx.x == 0 && y < H) {
+        L.bitmap[size_t(y) * L.WW + (x0 >> 5)] = mask;
+        if (mask) atomicAdd(&L.row_count[y], __popc(mask));
+    }
+}
+
+// ------------------------------------------------------------------ scans --
+__device__ __forceinline__ int warp_incl_scan(int v)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) >= o) v += n;
+    }
+    return v;
+}
+
+// Exclusive block scan (blockDim.x multiple of 32, <= 1024); returns the block total in *total.
+__device__ __forceinline__ int block_excl_scan(int v, int* s_warp, int* total)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int inc = warp_incl_scan(v);
+    if (lane == 31) s_warp[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        const int w = lane < nw ? s_warp[lane] : 0;
+        const int wi = warp_incl_scan(w);
+        if (lane < nw) s_warp[lane] = wi - w;
+        if (lane == nw - 1) s_warp[32] = wi;
+    }
+    __syncthreads();
+    const int res = inc - v + s_warp[wid];
+    *total = s_warp[32];
+    __syncthreads();
+    return res;
+}
+
+// One block per level: row_off = exclusive scan of row_count; E clamped to the
+// capacity (overflow flagged); row_count is cleared for the next frame.
+__global__ void __launch_bounds__(1024) k_row_scan(Levels lv)
+{
+    __shared__ int s_warp[33];
+    const int l = blockIdx.x;
+    const LevelView& L = lv.l[l];
+    int carry = 0;
+    for (int base = 0; base < L.H; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = i < L.H ? L.row_count[i] : 0;
+        int total;
+        const int ex = block_excl_scan(v, s_warp, &total);
+        if (i < L.H) {
+            L.row_off[i] = carry + ex;
+            L.row_count[i] = 0;
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        L.row_off[L.H] = carry;
+        int E = carry;
+        if (E > L.cap) {
+            atomicOr(&lv.cnt[l].err, kErrEdgeOverflow);
+            E = L.cap;
+        }
+        lv.cnt[l].E = E;
+    }
+}
+
+// One block (4 warps) per image row: raster-order edge list, index map,
+// per-point state reset.  EdgePointCollection::add_point, Types.cpp:40-61.
+__global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
+{
+    __shared__ int s_warp[4];
+    int y = blockIdx.x, l = 0;
+    while (l < lv.n - 1 && y >= lv.l[l].H) { y -= lv.l[l].H; ++l; }
+    const LevelView& L = lv.l[l];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int per = (L.WW + 3) / 4;
+    const int w0 = wid * per, w1 = min(L.WW, w0 + per);
+    const uint32_t* row = L.bitmap + size_t(y) * L.WW;
+    int cnt = 0;
+    for (int w = w0 + lane; w < w1; w += 32) cnt += __popc(row[w]);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0) s_warp[wid] = cnt;
+    __syncthreads();
+    int base = L.row_off[y];
+    for (int k = 0; k < wid; ++k) base += s_warp[k];
+    for (int w = w0; w < w1; ++w) {
+        const uint32_t m = row[w];
+        if (!m) continue;
+        if ((m >> lane) & 1u) {
+            const int idx = base + __popc(m & ((1u << lane) - 1u));
+            if (idx < L.cap) {
+                const int x = (w << 5) + lane;
+                const size_t p = size_t(y) * L.W + x;
+                L.exy[idx] = x | (y << 16);
+                L.grad[idx] = int32_t(uint16_t(L.dx[p])) | (int32_t(L.dy[p]) << 16);
+                L.idxmap[p] = idx;
+                L.nvotes[idx] = 0;
+                L.fill[idx] = 0;
+            }
+        }
+        base += __popc(m);
+    }
+}
+
+// ------------------------------------------------------ gradient walk --
+// Bresenham.cpp:18-209.  Returns the index of the first edge point met, or -1.
+__device__ __forceinline__ int sgn_i(int v) { return (v > 0) - (v < 0); }
+
+__device__ int gradient_walk(const LevelView& L, int px, int py, int gdx, int gdy, int dir, int nmax, int thr)
+{
+    float e = 0.f;
+    float dx = float(dir * gdx), dy = float(dir * gdy);
+    const float dxRef = dx, dyRef = dy;
+    const bool y_major = fabsf(dy) > fabsf(dx);
+    int x = px, y = py, stpX = 0, stpY = 0, n = 0;
+    const int W = L.W, H = L.H;
+    auto step = [&]() {
+        const float dmaj = y_major ? dy : dx, dmin = y_major ? dx : dy;
+        const float a = fabsf(__fdiv_rn(dmin, dmaj));
+        const int smaj = sgn_i(int(dmaj)), smin = sgn_i(int(dmin));
+        e = __fadd_rn(e, a);
+        if (y_major) { stpY = smaj; stpX = smin; y += smaj; } else { stpX = smaj; stpY = smin; x += smaj; }
+        if (e >= 0.5f) {
+            if (y_major) x += smin; else y += smin;
+            e = __fadd_rn(e, -1.f);
+        }
+        ++n;
+    };
+    step();
+    if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > float(thr)) {
+        const float v = __fadd_rn(__fmul_rn(float(gdx), dxRef), __fmul_rn(float(gdy), dyRef));
+        const int d = (v > 0.f) - (v < 0.f);
+        dx = float(d * gdx);
+        dy = float(d * gdy);
+    }
+    step();
+    if (x < 0 || x >= W || y < 0 || y >= H) return -1;
+    if (edge_bit(L, x, y)) return L.idxmap[size_t(y) * W + x];
+    while (n <= nmax) {
+        step();
+        if (x < 0 || x >= W || y < 0 || y >= H) return -1;
+        if (edge_bit(L, x, y)) return L.idxmap[size_t(y) * W + x];
+        const int bx = y_major ? x : x - stpX;
+        const int by = y_major ? y - stpY : y;
+        if (bx < 0 || bx >= W || by < 0 || by >= H) return -1;
+        if (edge_bit(L, bx, by)) return L.idxmap[size_t(by) * W + bx];
+    }
+    return -1;
+}
+
+__global__ void k_walk(Levels lv, VoteParamsDev vp)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int l = 0; l < lv.n; ++l) {
+        const LevelView& L = lv.l[l];
+        const int E = lv.cnt[l].E;
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * E; t += stride) {
+            const int p = t >> 1;
+            const int dir = (t & 1) ? 1 : -1;
+            const int xy = L.exy[p], g = L.grad[p];
+            const int px = xy & 0xffff, py = xy >> 16;
+            const int gdx = int16_t(g & 0xffff), gdy = g >> 16;
+            const int hit = gradient_walk(L, px, py, gdx, gdy, dir, vp.distSearch, vp.thrGradient);
+            if (dir < 0) L.before[p] = hit; else L.after[p] = hit;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ vote --
+// Vote.cpp:101-243: follow before/after links across the 2*nCrowns-1 ring
+// edges with the gradient-angle and distance-ratio tests.
+__device__ __forceinline__ float pt_dist(int xya, int xyb)
+{
+    const int ddx = (xyb & 0xffff) - (xya & 0xffff), ddy = (xyb >> 16) - (xya >> 16);
+    return __fsqrt_rn(__fadd_rn(float(ddx * ddx), float(ddy * ddy)));
+}
+
+__device__ __forceinline__ float neg_dot(int ga, int gb)
+{
+    const int d = int(int16_t(ga & 0xffff)) * int(int16_t(gb & 0xffff)) + (ga >> 16) * (gb >> 16);
+    return -float(d);
+}
+
+__global__ void k_vote(Levels lv, VoteParamsDev vp)
+{
+    const int stride = gridDim.x * blockDim.x;
+    constexpr int kMaxSeg = 16;
+    for (int l = 0; l < lv.n; ++l) {
+        const LevelView& L = lv.l[l];
+        const int E = lv.cnt[l].E;
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += stride) {
+            float vd[kMaxSeg];
+            int nd = 0;
+            float total = 0.f;
+            int chosen = -1;
+            int current = L.before[p];
+            const int gp = L.grad[p];
+            const int xyp = L.exy[p];
+            auto ratio_ok = [&]() {
+                bool ok = true;
+                for (int i = 0; i < nd; ++i)
+                    for (int j = i + 1; j < nd; ++j)
+                        ok = ok && (vd[i] <= __fmul_rn(vd[j], vp.ratioVoting)) && (vd[j] <= __fmul_rn(vd[i], vp.ratioVoting));
+                return ok;
+            };
+            if (current >= 0 && neg_dot(gp, L.grad[current]) >= vp.angleVoting && 2 * vp.nCrowns - 1 <= kMaxSeg) {
+                float d = pt_dist(xyp, L.exy[current]);
+                vd[nd++] = d;
+                total = __fadd_rn(total, d);
+                for (int i = 1; i < vp.nCrowns; ++i) {
+                    chosen = -1;
+                    int target = L.after[current];
+                    if (target < 0) break;
+                    if (!(neg_dot(L.grad[target], L.grad[current]) >= vp.angleVoting)) break;
+                    d = pt_dist(L.exy[target], L.exy[current]);
+                    vd[nd++] = d;
+                    total = __fadd_rn(total, d);
+                    if (nd > 1 && !ratio_ok()) break;
+                    current = target;
+                    target = L.before[current];
+                    if (target < 0) break;
+                    if (!(neg_dot(L.grad[target], L.grad[current]) >= vp.angleVoting)) break;
+                    d = pt_dist(L.exy[target], L.exy[current]);
+                    vd[nd++] = d;
+                    total = __fadd_rn(total, d);
+                    if (!ratio_ok()) break;
+                    current = target;
+                    chosen = current;
+                }
+            }
+            L.chosen[p] = chosen;
+            L.total[p] = chosen >= 0 ? total : 0.f;
+            if (chosen >= 0) atomicAdd(&L.nvotes[chosen], 1);
+        }
+    }
+}
+
+// ----------------------------------------------------- voter lists (CSR) --
+// Chunked exclusive scan of nvotes[0, E) into voff, all levels, fixed grid.
+constexpr int kScanBlocks = 148;
+constexpr int kScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads) k_vscan_partial(Levels lv, int32_t* partial)
+{
+    __shared__ int s_red[32];
+    for (int l = 0; l < lv.n; ++l) {
+        const LevelView& L = lv.l[l];
+        const int E = lv.cnt[l].E;
+        const int chunk = (E + kScanBlocks - 1) / kScanBlocks;
+        const int b0 = blockIdx.x * chunk, b1 = min(E, b0 + chunk);
+        int s = 0;
+        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) s += L.nvotes[i];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            int v = s_red[threadIdx.x];
+#pragma unroll
+            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (threadIdx.x == 0) partial[l * kScanBlocks + blockIdx.x] = v;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_vscan_final(Levels lv, const int32_t* partial)
+{
+    __shared__ int s_warp[33];
+    __shared__ int s_base;
+    for (int l = 0; l < lv.n; ++l) {
+        const LevelView& L = lv.l[l];
+        const int E = lv.cnt[l].E;
+        const int chunk = (E + kScanBlocks - 1) / kScanBlocks;
+        const int b0 = blockIdx.x * chunk, b1 = min(E, b0 + chunk);
+        if (threadIdx.x == 0) {
+            int b = 0;
+            for (int k = 0; k < int(blockIdx.x); ++k) b += partial[l * kScanBlocks + k];
+            s_base = b;
+        }
+        __syncthreads();
+        int carry = s_base;
+        for (int base = b0; base < b1; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            const int v = i < b1 ? L.nvotes[i] : 0;
+            int total;
+            const int ex = block_excl_scan(v, s_warp, &total);
+            if (i < b1) L.voff[i] = carry + ex;
+            carry += total;
+        }
+        if (blockIdx.x == kScanBlocks - 1 && threadIdx.x == 0) {
+            int V = 0;
+            for (int k = 0; k < kScanBlocks; ++k) V += partial[l * kScanBlocks + k];
+            L.voff[E] = V;
+            lv.cnt[l].V = V;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_vfill(Levels lv)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int l = 0; l < lv.n; ++l) {
+        const LevelView& L = lv.l[l];
+        const int E = lv.cnt[l].E;
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < E; p += stride) {
+            const int c = L.chosen[p];
+            if (c < 0) continue;
+            const int slot = atomicAdd(&L.fill[c], 1);
+            L.vlist[L.voff[c] + slot] = p;
+        }
+    }
+}
+
+// Running mean of the field-line lengths in ascending voter order
+// (Vote.cpp:232) and seed registration (Vote.cpp:236-241).
+__device__ __forceinline__ void finish_point(const LevelView& L, LevelCounters& cnt, const VoteParamsDev& vp, int c,
+                                             const int32_t* list, int n)
+{
+    float fl = 0.f;
+    for (int k = 0; k < n; ++k) {
+        const float nk = float(k + 1);
+        fl = __fdiv_rn(__fadd_rn(__fmul_rn(fl, float(k)), L.total[list[k]]), nk);
+    }
+    L.flow[c] = fl;
+    if (n >= vp.minVotes) {
+        const int s = atomicAdd(&cnt.S, 1);
+        if (s < L.seedcap) {
+            L.seed_idx[s] = c;
+            L.seed_key[s] = list[vp.minVotes - 1];
+        } else {
+            atomicOr(&cnt.err, kErrSeedOverflow);
+        }
+    }
+}
+
+constexpr int kSmallList = 32;
+
+__global__ void k_vlists_small(Levels lv, VoteParamsDev vp)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int l = 0; l < lv.n; ++l) {
+        const LevelView& L = lv.l[l];
+        const int E = lv.cnt[l].E;
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < E; c += stride) {
+            const int n = L.voff[c + 1] - L.voff[c];
+            if (n == 0) {
+                L.flow[c] = 0.f;
+                continue;
+            }
+            if (n > kSmallList) {
+                const int q = atomicAdd(&lv.cnt[l].bigq, 1);
+                L.bigq[q] = c;
+                continue;
+            }
+            int32_t* list = L.vlist + L.voff[c];
+            int v[kSmallList];
+            for (int k = 0; k < n; ++k) v[k] = list[k];
+            for (int k = 1; k < n; ++k) {
+                const int key = v[k];
+                int j = k - 1;
+                while (j >= 0 && v[j] > key) { v[j + 1] = v[j]; --j; }
+                v[j + 1] = key;
+            }
+            for (int k = 0; k < n; ++k) list[k] = v[k];
+            finish_point(L, lv.cnt[l], vp, c, list, n);
+        }
+    }
+}
+
+// Long voter lists: one block per list, rank sort (voter indices are distinct).
+constexpr int kBigSmem = 4096;
+
+__global__ void __launch_bounds__(256) k_vlists_big(Levels lv, VoteParamsDev vp)
+{
+    __shared__ int32_t s_in[kBigSmem];
+    __shared__ int32_t s_out[kBigSmem];
+    for (int l = 0; l < lv.n; ++l) {
+        const LevelView& L = lv.l[l];
+        const int nq = lv.cnt[l].bigq;
+        for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+            const int c = L.bigq[qi];
+            int32_t* list = L.vlist + L.voff[c];
+            const int n = L.voff[c + 1] - L.voff[c];
+            if (n <= kBigSmem) {
+                for (int k = threadIdx.x; k < n; k += blockDim.x) s_in[k] = list[k];
+                __syncthreads();
+                for (int k = threadIdx.x; k < n; k += blockDim.x) {
+                    const int v = s_in[k];
+                    int rank = 0;
+                    for (int j = 0; j < n; ++j) rank += s_in[j] < v;
+                    s_out[rank] = v;
+                }
+                __syncthreads();
+                for (int k = threadIdx.x; k < n; k += blockDim.x) list[k] = s_out[k];
+            } else {
+                // Very long list: rank from global memory into the upper half of
+                // the chosen list's own slots is impossible in place, so stage
+                // the ranks through the fill array (free after k_vfill).
+                for (int k = threadIdx.x; k < n; k += blockDim.x) {
+                    const int v = list[k];
+                    int rank = 0;
+                    for (int j = 0; j < n; ++j) rank += list[j] < v;
+                    L.fill[L.voff[c] + rank] = v;
+                }
+                __syncthreads();
+                for (int k = threadIdx.x; k < n; k += blockDim.x) list[k] = L.fill[L.voff[c] + k];
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) finish_point(L, lv.cnt[l], vp, c, list, n);
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------- launchers --
+static int total_of(const Levels& lv, int LevelView::*f)
+{
+    int s = 0;
+    for (int l = 0; l < lv.n; ++l) s += lv.l[l].*f;
+    return s;
+}
+
+void upload_constants(const float*, int, int)
+{
+    static const float K[9][9] = {
+        {-0.000000143284235f, -0.000003558691641f, -0.000028902492951f, -0.000064765993382f, 0.f, 0.000064765993382f, 0.000028902492951f, 0.000003558691641f, 0.000000143284235f},
+        {-0.000004744922188f, -0.000117847682078f, -0.000957119116802f, -0.002144755142391f, 0.f, 0.002144755142391f, 0.000957119116802f, 0.000117847682078f, 0.000004744922188f},
+        {-0.000057804985902f, -0.001435678675203f, -0.011660097860113f, -0.026128466569370f, 0.f, 0.026128466569370f, 0.011660097860113f, 0.001435678675203f, 0.000057804985902f},
+        {-0.000259063973527f, -0.006434265427174f, -0.052256933138740f, -0.117099663048638f, 0.f, 0.117099663048638f, 0.052256933138740f, 0.006434265427174f, 0.000259063973527f},
+        {-0.000427124283626f, -0.010608310271112f, -0.086157117207395f, -0.193064705260108f, 0.f, 0.193064705260108f, 0.086157117207395f, 0.010608310271112f, 0.000427124283626f},
+        {-0.000259063973527f, -0.006434265427174f, -0.052256933138740f, -0.117099663048638f, 0.f, 0.117099663048638f, 0.052256933138740f, 0.006434265427174f, 0.000259063973527f},
+        {-0.000057804985902f, -0.001435678675203f, -0.011660097860113f, -0.026128466569370f, 0.f, 0.026128466569370f, 0.011660097860113f, 0.001435678675203f, 0.000057804985902f},
+        {-0.000004744922188f, -0.000117847682078f, -0.000957119116802f, -0.002144755142391f, 0.f, 0.002144755142391f, 0.000957119116802f, 0.000117847682078f, 0.000004744922188f},
+        {-0.000000143284235f, -0.000003558691641f, -0.000028902492951f, -0.000064765993382f, 0.f, 0.000064765993382f, 0.000028902492951f, 0.000003558691641f, 0.000000143284235f}};
+    CCTAGB_CUDA(cudaMemcpyToSymbol(cK, K, sizeof(K)));
+    // Lam-Lee-Suen sub-iteration tables (see thin_lut in the host code).
+    uint32_t bits[2][16] = {};
+    for (int pass = 1; pass <= 2; ++pass)
+        for (int idx = 0; idx < 512; ++idx) {
+            auto bit = [&](int w) { return (idx & w) ? 1 : 0; };
+            if (!bit(16)) continue;
+            const int x[10] = {0, bit(128), bit(64), bit(8), bit(1), bit(2), bit(4), bit(32), bit(256), bit(128)};
+            int xh = 0, n1 = 0, n2 = 0;
+            for (int i = 1; i <= 4; ++i) {
+                xh += (x[2 * i - 1] == 0 && (x[2 * i] == 1 || x[2 * i + 1] == 1)) ? 1 : 0;
+                n1 += x[2 * i - 1] | x[2 * i];
+                n2 += x[2 * i] | x[2 * i + 1];
+            }
+            const int mn = n1 < n2 ? n1 : n2;
+            const bool g1 = xh == 1, g2 = mn >= 2 && mn <= 3;
+            const bool g3 = pass == 1 ? (((x[2] | x[3] | (1 - x[8])) & x[1]) == 0)
+                                      : (((x[6] | x[7] | (1 - x[4])) & x[5]) == 0);
+            if (!(g1 && g2 && g3)) bits[pass - 1][idx >> 5] |= 1u << (idx & 31);
+        }
+    CCTAGB_CUDA(cudaMemcpyToSymbol(cThin, bits, sizeof(bits)));
+}
+
+static void launch_pyramid(const Levels& lv, cudaStream_t s, bool fused)
+{
+    if (lv.n < 2) return;
+    if (fused && lv.n == 4) {
+        const dim3 blk(32, 8);
+        const dim3 grd((lv.l[0].W / 8 + 31) / 32, (lv.l[0].H / 8 + 7) / 8);
+        k_pyramid3<<<grd, blk, 0, s>>>(lv);
+        return;
+    }
+    for (int l = 1; l < lv.n; ++l) {
+        const dim3 blk(32, 8);
+        const dim3 grd((lv.l[l].W + 31) / 32, (lv.l[l].H + 7) / 8);
+        k_resize_level<<<grd, blk, 0, s>>>(lv.l[l - 1].src, lv.l[l - 1].W, lv.l[l - 1].H, lv.l[l].src, lv.l[l].W,
+                                           lv.l[l].H);
+    }
+}
+
+const char* stage_name(int k)
+{
+    static const char* names[kStageCount] = {"pyramid", "deriv_nms", "hyst_merge", "hyst_compress", "final_thin",
+                                             "row_scan", "emit", "walk", "vote", "voter_scan", "voter_fill",
+                                             "voter_sort"};
+    return (k >= 0 && k < kStageCount) ? names[k] : "?";
+}
+
+static void mark(cudaEvent_t* ev, int k, cudaStream_t s)
+{
+    if (ev) CCTAGB_CUDA(cudaEventRecord(ev[k], s));
+}
+
+static void launch_edges(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, int write_derivs,
+                         cudaEvent_t* ev)
+{
+    k_deriv_nms<<<total_of(lv, &LevelView::nms_tiles), 128, 0, s>>>(lv, vp, write_derivs);
+    mark(ev, kStDerivNms + 1, s);
+    const int pb = total_of(lv, &LevelView::pix_blocks);
+    k_hyst_merge<<<pb, 256, 0, s>>>(lv);
+    mark(ev, kStHystMerge + 1, s);
+    k_hyst_compress_mark<<<pb, 256, 0, s>>>(lv);
+    mark(ev, kStHystCompress + 1, s);
+    k_final_thin<<<total_of(lv, &LevelView::thin_tiles), dim3(kThX, kThY), 0, s>>>(lv);
+    mark(ev, kStFinalThin + 1, s);
+    k_row_scan<<<lv.n, 1024, 0, s>>>(lv);
+    mark(ev, kStRowScan + 1, s);
+    int rows = 0;
+    for (int l = 0; l < lv.n; ++l) rows += lv.l[l].H;
+    k_emit<<<rows, 128, 0, s>>>(lv, rows);
+    mark(ev, kStEmit + 1, s);
+}
+
+// The partial sums of the voter-count scan live in the counters allocation
+// (see Pipeline): cnt + 8 ints per level, then kMaxLevels*kScanBlocks ints.
+void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, bool fused_pyramid,
+                        cudaEvent_t* ev)
+{
+    CCTAGB_CUDA(cudaMemsetAsync(lv.cnt, 0, sizeof(LevelCounters) * kMaxLevels, s));
+    mark(ev, 0, s);
+    launch_pyramid(lv, s, fused_pyramid);
+    mark(ev, kStPyramid + 1, s);
+    launch_edges(lv, vp, s, 1, ev);
+    const int G = 148 * 8;
+    k_walk<<<G, 256, 0, s>>>(lv, vp);
+    mark(ev, kStWalk + 1, s);
+    k_vote<<<G, 256, 0, s>>>(lv, vp);
+    mark(ev, kStVote + 1, s);
+    int32_t* partial = reinterpret_cast<int32_t*>(lv.cnt + kMaxLevels);
+    k_vscan_partial<<<kScanBlocks, kScanThreads, 0, s>>>(lv, partial);
+    k_vscan_final<<<kScanBlocks, kScanThreads, 0, s>>>(lv, partial);
+    mark(ev, kStVoterScan + 1, s);
+    k_vfill<<<G, 256, 0, s>>>(lv);
+    mark(ev, kStVoterFill + 1, s);
+    k_vlists_small<<<G, 256, 0, s>>>(lv, vp);
+    k_vlists_big<<<148, 256, 0, s>>>(lv, vp);
+    mark(ev, kStVoterSort + 1, s);
+    CCTAGB_CUDA(cudaGetLastError());
+}
+
+void launch_canny_only(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s)
+{
+    CCTAGB_CUDA(cudaMemsetAsync(lv.cnt, 0, sizeof(LevelCounters) * kMaxLevels, s));
+    launch_edges(lv, vp, s, 0, nullptr);
+    CCTAGB_CUDA(cudaGetLastError());
+}
+
+}  // namespace cctagb

@@ -1,0 +1,296 @@
+// Host orchestration: device arena, per-resolution CUDA graph of the image
+// stage, downloads of the per-level edge-point collections.
+#include "pipeline.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace cctagb {
+
+namespace {
+
+template <class T>
+T* dev_alloc(std::vector<void*>& list, size_t n)
+{
+    void* p = nullptr;
+    CCTAGB_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    list.push_back(p);
+    return static_cast<T*>(p);
+}
+
+}  // namespace
+
+Pipeline::Pipeline(const cctagb_params& p, int max_w, int max_h, int max_batch) : params_(p)
+{
+    (void)max_batch;
+    int dev = 0;
+    CCTAGB_CUDA(cudaGetDevice(&dev));
+    cudaDeviceProp prop{};
+    CCTAGB_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major < 10) throw Error{CCTAGB_NO_DEVICE, "device is not sm_100 (compute capability " +
+                                                           std::to_string(prop.major) + "." +
+                                                           std::to_string(prop.minor) + ")"};
+    if (p.numberOfProcessedMultiresLayers < 1 || p.numberOfProcessedMultiresLayers > kMaxLevels)
+        throw Error{CCTAGB_BAD_ARG, "numberOfProcessedMultiresLayers must be in [1, 4]"};
+    if (p.nCrowns < 1 || 2 * p.nCrowns - 1 > 16) throw Error{CCTAGB_BAD_ARG, "nCrowns out of range"};
+    if (p.edgeCapacityDivisor < 1) throw Error{CCTAGB_BAD_ARG, "edgeCapacityDivisor must be >= 1"};
+    vp_.distSearch = p.distSearch;
+    vp_.thrGradient = p.thrGradientMagInVote;
+    vp_.angleVoting = p.angleVoting;
+    vp_.ratioVoting = p.ratioVoting;
+    vp_.nCrowns = p.nCrowns;
+    vp_.minVotes = p.minVotesToSelectCandidate;
+    float lo = p.cannyThrLow * 256.f, hi = p.cannyThrHigh * 256.f;
+    if (lo > hi) std::swap(lo, hi);
+    vp_.low = int(std::floor(lo));
+    vp_.high = int(std::floor(hi));
+    CCTAGB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CCTAGB_CUDA(cudaEventCreate(&ev0_));
+    CCTAGB_CUDA(cudaEventCreate(&ev1_));
+    upload_constants(nullptr, 0, 0);
+    alloc(max_w, max_h);
+}
+
+Pipeline::~Pipeline()
+{
+    if (graph_) cudaGraphExecDestroy(graph_);
+    for (cudaEvent_t e : st_ev_)
+        if (e) cudaEventDestroy(e);
+    for (void* p : allocs_) cudaFree(p);
+    if (h_cnt_) cudaFreeHost(h_cnt_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Pipeline::alloc(int max_w, int max_h)
+{
+    if (max_w < 1 || max_h < 1 || max_w > 16384 || max_h > 16384)
+        throw Error{CCTAGB_BAD_ARG, "max frame size must be in [1, 16384]"};
+    max_w_ = max_w;
+    max_h_ = max_h;
+    int w = max_w, h = max_h;
+    const int nl = params_.numberOfProcessedMultiresLayers;
+    for (int l = 0; l < nl; ++l) {
+        LevelAlloc& a = la_[l];
+        // Level buffers are sized for the largest frame; +8 rows/cols of slack
+        // lets a smaller frame use its own width as the row stride.
+        const size_t px = size_t(w) * h;
+        a.px = px;
+        a.cap = int(std::max<size_t>(px / params_.edgeCapacityDivisor, 1024));
+        a.seedcap = a.cap;
+        LevelView& v = a.v;
+        v.src = dev_alloc<uint8_t>(allocs_, px + 16);
+        v.dx = dev_alloc<int16_t>(allocs_, px);
+        v.dy = dev_alloc<int16_t>(allocs_, px);
+        v.map = dev_alloc<uint8_t>(allocs_, px);
+        v.label = dev_alloc<int32_t>(allocs_, px);
+        v.sroot = dev_alloc<uint8_t>(allocs_, px);
+        v.bitmap = dev_alloc<uint32_t>(allocs_, size_t((w + 31) / 32) * h);
+        v.idxmap = dev_alloc<int32_t>(allocs_, px);
+        v.row_count = dev_alloc<int32_t>(allocs_, h);
+        v.row_off = dev_alloc<int32_t>(allocs_, h + 1);
+        CCTAGB_CUDA(cudaMemset(v.row_count, 0, sizeof(int32_t) * h));
+        v.cap = a.cap;
+        v.exy = dev_alloc<int32_t>(allocs_, a.cap);
+        v.grad = dev_alloc<int32_t>(allocs_, a.cap);
+        v.before = dev_alloc<int32_t>(allocs_, a.cap);
+        v.after = dev_alloc<int32_t>(allocs_, a.cap);
+        v.chosen = dev_alloc<int32_t>(allocs_, a.cap);
+        v.total = dev_alloc<float>(allocs_, a.cap);
+        v.nvotes = dev_alloc<int32_t>(allocs_, a.cap);
+        v.fill = dev_alloc<int32_t>(allocs_, a.cap);
+        v.voff = dev_alloc<int32_t>(allocs_, a.cap + 1);
+        v.vlist = dev_alloc<int32_t>(allocs_, a.cap);
+        v.flow = dev_alloc<float>(allocs_, a.cap);
+        v.seedcap = a.seedcap;
+        v.seed_idx = dev_alloc<int32_t>(allocs_, a.seedcap);
+        v.seed_key = dev_alloc<int32_t>(allocs_, a.seedcap);
+        v.bigq = dev_alloc<int32_t>(allocs_, a.cap);
+        w /= 2;
+        h /= 2;
+        if (w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "frame too small for the number of pyramid levels"};
+    }
+    // Counters followed by the partial sums of the voter-count scan.
+    const size_t cnt_bytes = sizeof(LevelCounters) * kMaxLevels + sizeof(int32_t) * kMaxLevels * 148;
+    d_cnt_ = reinterpret_cast<LevelCounters*>(dev_alloc<uint8_t>(allocs_, cnt_bytes));
+    CCTAGB_CUDA(cudaMemset(d_cnt_, 0, cnt_bytes));
+    CCTAGB_CUDA(cudaMallocHost(&h_cnt_, sizeof(LevelCounters) * kMaxLevels));
+    std::memset(h_cnt_, 0, sizeof(LevelCounters) * kMaxLevels);
+}
+
+void Pipeline::set_views(int w, int h)
+{
+    if (w > max_w_ || h > max_h_) throw Error{CCTAGB_TOO_LARGE, "frame larger than the handle's maximum"};
+    const int nl = params_.numberOfProcessedMultiresLayers;
+    lv_.n = nl;
+    lv_.cnt = d_cnt_;
+    for (int l = 0; l < nl; ++l) {
+        if (w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "frame too small for the number of pyramid levels"};
+        LevelView v = la_[l].v;
+        v.W = w;
+        v.H = h;
+        v.WW = (w + 31) / 32;
+        v.nms_tx = (w + 29) / 30;
+        v.nms_tiles = v.nms_tx * ((h + 29) / 30);
+        v.thin_tx = (w + 31) / 32;
+        v.thin_tiles = v.thin_tx * ((h + 15) / 16);
+        v.pix_blocks = int((size_t(w) * h + 255) / 256);
+        lv_.l[l] = v;
+        w /= 2;
+        h /= 2;
+    }
+}
+
+void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool is_device)
+{
+    if (!gray || w < 1 || h < 1 || pitch < size_t(w)) throw Error{CCTAGB_BAD_ARG, "bad frame arguments"};
+    set_views(w, h);
+    CCTAGB_CUDA(cudaMemcpy2DAsync(lv_.l[0].src, w, gray, pitch, w, h,
+                                  is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    if (!graph_ || graph_w_ != w || graph_h_ != h) {
+        if (graph_) {
+            cudaGraphExecDestroy(graph_);
+            graph_ = nullptr;
+        }
+        const bool fused = (w % 8 == 0) && (h % 8 == 0) && lv_.n == 4;
+        cudaGraph_t g = nullptr;
+        CCTAGB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        try {
+            launch_image_stage(lv_, vp_, stream_, fused, timing_ ? st_ev_ : nullptr);
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        CCTAGB_CUDA(cudaStreamEndCapture(stream_, &g));
+        const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+        cudaGraphDestroy(g);
+        CCTAGB_CUDA(e);
+        graph_w_ = w;
+        graph_h_ = h;
+    }
+    CCTAGB_CUDA(cudaEventRecord(ev0_, stream_));
+    CCTAGB_CUDA(cudaGraphLaunch(graph_, stream_));
+    CCTAGB_CUDA(cudaEventRecord(ev1_, stream_));
+    sync_counters();
+    CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
+    if (timing_)
+        for (int k = 0; k < kStageCount; ++k) CCTAGB_CUDA(cudaEventElapsedTime(&stage_ms_[k], st_ev_[k], st_ev_[k + 1]));
+}
+
+void Pipeline::set_stage_timing(bool on)
+{
+    if (on == timing_) return;
+    if (on && !st_ev_[0])
+        for (cudaEvent_t& e : st_ev_) CCTAGB_CUDA(cudaEventCreate(&e));
+    timing_ = on;
+    graph_w_ = graph_h_ = -1;  // recapture with or without the event nodes
+    std::fill(stage_ms_, stage_ms_ + kStageCount, 0.f);
+}
+
+void Pipeline::sync_counters()
+{
+    CCTAGB_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(LevelCounters) * kMaxLevels, cudaMemcpyDeviceToHost, stream_));
+    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    for (int l = 0; l < lv_.n; ++l) {
+        const int err = h_cnt_[l].err;
+        if (err & kErrUnionFind) throw Error{CCTAGB_HYST_NO_CONVERGE, "hysteresis union-find exceeded its cap"};
+        if (err & kErrEdgeOverflow)
+            throw Error{CCTAGB_OVERFLOW_EDGES, "level " + std::to_string(l) + ": edge points exceed capacity " +
+                                                   std::to_string(lv_.l[l].cap)};
+        if (err & kErrSeedOverflow) throw Error{CCTAGB_OVERFLOW_SEEDS, "seed capacity exceeded"};
+    }
+}
+
+void Pipeline::canny_only(const int16_t* dx, const int16_t* dy, int w, int h, uint8_t* edges_out)
+{
+    if (!dx || !dy || !edges_out || w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "bad arguments"};
+    set_views(w, h);
+    lv_.n = 1;
+    const size_t px = size_t(w) * h;
+    CCTAGB_CUDA(cudaMemcpyAsync(lv_.l[0].dx, dx, px * 2, cudaMemcpyHostToDevice, stream_));
+    CCTAGB_CUDA(cudaMemcpyAsync(lv_.l[0].dy, dy, px * 2, cudaMemcpyHostToDevice, stream_));
+    launch_canny_only(lv_, vp_, stream_);
+    sync_counters();
+    copy_planes(0, nullptr, nullptr, nullptr, edges_out);
+    graph_w_ = graph_h_ = -1;  // views were narrowed; force a fresh capture next frame
+}
+
+void Pipeline::level_size(int l, int* w, int* h) const
+{
+    if (l < 0 || l >= lv_.n) throw Error{CCTAGB_BAD_ARG, "level out of range"};
+    *w = lv_.l[l].W;
+    *h = lv_.l[l].H;
+}
+
+void Pipeline::copy_planes(int l, uint8_t* src, int16_t* dx, int16_t* dy, uint8_t* edges)
+{
+    if (l < 0 || l >= lv_.n) throw Error{CCTAGB_BAD_ARG, "level out of range"};
+    const LevelView& v = lv_.l[l];
+    const size_t px = size_t(v.W) * v.H;
+    if (src) CCTAGB_CUDA(cudaMemcpyAsync(src, v.src, px, cudaMemcpyDeviceToHost, stream_));
+    if (dx) CCTAGB_CUDA(cudaMemcpyAsync(dx, v.dx, px * 2, cudaMemcpyDeviceToHost, stream_));
+    if (dy) CCTAGB_CUDA(cudaMemcpyAsync(dy, v.dy, px * 2, cudaMemcpyDeviceToHost, stream_));
+    std::vector<uint32_t> bits;
+    if (edges) {
+        bits.resize(size_t(v.WW) * v.H);
+        CCTAGB_CUDA(cudaMemcpyAsync(bits.data(), v.bitmap, bits.size() * 4, cudaMemcpyDeviceToHost, stream_));
+    }
+    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    if (edges) {
+        for (int y = 0; y < v.H; ++y)
+            for (int x = 0; x < v.W; ++x)
+                edges[size_t(y) * v.W + x] = ((bits[size_t(y) * v.WW + (x >> 5)] >> (x & 31)) & 1u) ? 255 : 0;
+    }
+}
+
+void Pipeline::download_level(int l, HostLevel& out)
+{
+    if (l < 0 || l >= lv_.n) throw Error{CCTAGB_BAD_ARG, "level out of range"};
+    const LevelView& v = lv_.l[l];
+    const LevelCounters& c = h_cnt_[l];
+    out.W = v.W;
+    out.H = v.H;
+    out.E = c.E;
+    out.V = c.V;
+    const int E = c.E;
+    out.exy.resize(E);
+    out.grad.resize(E);
+    out.before.resize(E);
+    out.after.resize(E);
+    out.voff.resize(E + 1);
+    out.vlist.resize(c.V);
+    out.flow.resize(E);
+    const int S = std::min(c.S, v.seedcap);
+    std::vector<int32_t> sidx(S), skey(S);
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) CCTAGB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_));
+    };
+    d2h(out.exy.data(), v.exy, size_t(E) * 4);
+    d2h(out.grad.data(), v.grad, size_t(E) * 4);
+    d2h(out.before.data(), v.before, size_t(E) * 4);
+    d2h(out.after.data(), v.after, size_t(E) * 4);
+    d2h(out.voff.data(), v.voff, size_t(E + 1) * 4);
+    d2h(out.vlist.data(), v.vlist, size_t(c.V) * 4);
+    d2h(out.flow.data(), v.flow, size_t(E) * 4);
+    d2h(sidx.data(), v.seed_idx, size_t(S) * 4);
+    d2h(skey.data(), v.seed_key, size_t(S) * 4);
+    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    // Seeds in the order vote() appends them (the voter that brings a point to
+    // minVotes, Vote.cpp:236-241), then std::sort by votes received, as
+    // Multiresolution.cpp:239-242 does (same comparator, same libstdc++ sort).
+    std::vector<std::pair<int32_t, int32_t>> ks(S);
+    for (int i = 0; i < S; ++i) ks[i] = {skey[i], sidx[i]};
+    std::sort(ks.begin(), ks.end());
+    out.seeds.resize(S);
+    for (int i = 0; i < S; ++i) out.seeds[i] = ks[i].second;
+    const int32_t* voff = out.voff.data();
+    if (S > 1)
+        std::sort(out.seeds.begin(), out.seeds.end(), [voff](int32_t a, int32_t b) {
+            return (voff[a + 1] - voff[a]) > (voff[b + 1] - voff[b]);
+        });
+}
+
+}  // namespace cctagb

@@ -1,0 +1,77 @@
+// Host orchestration of one detection pipeline (one handle).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+
+namespace cctagb {
+
+// Host copy of one level's edge-point collection, the interchange format of
+// the reference (EdgePointCollection, Types.hpp:19-158): raster-ordered edge
+// points with gradients, before/after links, CSR voter lists, vote-derived
+// per-point state and the seeds in processing order.
+struct HostLevel {
+    int W = 0, H = 0;
+    int E = 0, V = 0;
+    std::vector<int32_t> exy, grad, before, after, voff, vlist;
+    std::vector<float> flow;
+    std::vector<int32_t> seeds;  // processing order (Multiresolution.cpp:239-242)
+};
+
+class Pipeline {
+public:
+    Pipeline(const cctagb_params& p, int max_w, int max_h, int max_batch);
+    ~Pipeline();
+    Pipeline(const Pipeline&) = delete;
+    Pipeline& operator=(const Pipeline&) = delete;
+
+    const cctagb_params& params() const { return params_; }
+    cudaStream_t stream() const { return stream_; }
+
+    // Pyramid .. seeds for one frame; results stay on the device.
+    void image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool is_device);
+    // Canny + thinning from caller derivatives (level 0 buffers).
+    void canny_only(const int16_t* dx, const int16_t* dy, int w, int h, uint8_t* edges_out);
+
+    int levels() const { return lv_.n; }
+    void level_size(int l, int* w, int* h) const;
+    void copy_planes(int l, uint8_t* src, int16_t* dx, int16_t* dy, uint8_t* edges);
+    const LevelCounters& counters(int l) const { return h_cnt_[l]; }
+    // Downloads one level's edge-point collection (after image_stage).
+    void download_level(int l, HostLevel& out);
+    float last_image_stage_ms() const { return last_ms_; }
+    // Per-stage device times of the last frame (events captured into the graph).
+    void set_stage_timing(bool on);
+    const float* stage_ms() const { return stage_ms_; }
+
+private:
+    void alloc(int max_w, int max_h);
+    void set_views(int w, int h);
+    void sync_counters();
+
+    cctagb_params params_;
+    VoteParamsDev vp_{};
+    int max_w_ = 0, max_h_ = 0;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    std::vector<void*> allocs_;
+    struct LevelAlloc {
+        size_t px = 0;  // pixel capacity
+        int cap = 0, seedcap = 0;
+        LevelView v{};
+    } la_[kMaxLevels];
+    Levels lv_{};
+    LevelCounters* d_cnt_ = nullptr;  // + scan partials
+    LevelCounters* h_cnt_ = nullptr;  // pinned
+    cudaGraphExec_t graph_ = nullptr;
+    int graph_w_ = -1, graph_h_ = -1;
+    float last_ms_ = 0.f;
+    bool timing_ = false;
+    cudaEvent_t st_ev_[kStageCount + 1] = {};
+    float stage_ms_[kStageCount] = {};
+};
+
+}  // namespace cctagb

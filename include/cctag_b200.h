@@ -1,0 +1,196 @@
+/*
+ * cctag_b200 -- C ABI of the B200 CCTag detection hot path.
+ *
+ * Every entry point returns a cctagb_status, never exits and never throws
+ * across the ABI.  Device memory, streams and captured CUDA graphs are owned by
+ * the handle.  A handle is not thread-safe: use one handle per host thread.
+ *
+ * Reference interfaces replaced (paths inside the CCTag project):
+ *   cctagb_detect          <- cctag::cctagDetection(ptr_list<ICCTag>&, pipeId, frame,
+ *                             const cv::Mat&, const Parameters&, logtime::Mgmt*,
+ *                             const CCTagMarkersBank*)           src/cctag/ICCTag.hpp:125-131
+ *                             (file-path overload                 src/cctag/ICCTag.hpp:103-110)
+ *   cctagb_params          <- cctag::Parameters                   src/cctag/Params.hpp:108-255
+ *   cctagb_params_default  <- Parameters::Parameters(nCrowns)     src/cctag/Params.cpp:38-82
+ *   cctagb_set_bank        <- CCTagMarkersBank(nCrowns / file)    src/cctag/CCTagMarkersBank.cpp:22-78
+ *   cctagb_marker          <- ICCTag / CCTag accessors            src/cctag/ICCTag.hpp:28-82, CCTag.hpp
+ *   status codes           <- cctag::status                       src/cctag/CCTag.hpp:416-426
+ *   cctagb_create          <- initCuda / TagPipe::initialize      src/cctag/Detection.cpp:732-760,
+ *                                                                  src/cctag/cuda/tag.cu:76-127
+ *   cctagb_level_*         <- ImagePyramid::getLevel(i)->getSrc/getDx/getDy/getEdges
+ *                                                                  src/cctag/Level.hpp:38-42
+ *   cctagb_level_edge_points / _links / _votes
+ *                          <- EdgePointCollection + vote()        src/cctag/Types.hpp:19-158,
+ *                                                                  src/cctag/Vote.cpp:58-247
+ *   cctagb_canny_from_derivatives
+ *                          <- cvRecodedCanny after filter2D        src/cctag/filter/cvRecode.cpp:94-421
+ *                             followed by thin()                  src/cctag/filter/thinning.cpp:15-19
+ *   cctagb_identify        <- identify_step_2 / refineConicFamilyGlob + orazioDistanceRobust
+ *                                                                  src/cctag/Identification.cpp:813-965,1318-1480
+ *   cctagb_cut_cost / cctagb_cut_cost_adjoint / cctagb_refine_gn
+ *                          <- costFunctionGlob (forward only in the reference)
+ *                                                                  src/cctag/Identification.cpp:1122-1158
+ */
+#ifndef CCTAG_B200_H
+#define CCTAG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cctagb_status {
+    CCTAGB_OK = 0,
+    CCTAGB_BAD_ARG = 1,            /* null pointer, bad size, bad parameter value      */
+    CCTAGB_CUDA_ERROR = 2,         /* a CUDA runtime call failed (see last_error)       */
+    CCTAGB_NO_DEVICE = 3,          /* no CUDA device, or not an sm_100 device           */
+    CCTAGB_OVERFLOW_EDGES = 4,     /* more edge points than the handle's capacity       */
+    CCTAGB_OVERFLOW_SEEDS = 5,     /* more seeds than the handle's capacity             */
+    CCTAGB_OVERFLOW_VOTERS = 6,    /* reserved: voter list larger than capacity         */
+    CCTAGB_HYST_NO_CONVERGE = 7,   /* hysteresis union-find exceeded its iteration cap  */
+    CCTAGB_TOO_LARGE = 8,          /* frame larger than the handle was created for      */
+    CCTAGB_BANK_ERROR = 9,         /* marker bank missing, empty or malformed           */
+    CCTAGB_INTERNAL = 10
+} cctagb_status;
+
+/* Marker status values, as cctag::status (CCTag.hpp:416-426). */
+#define CCTAGB_ID_RELIABLE 1
+#define CCTAGB_TOO_FEW_OUTER_POINTS (-1)
+#define CCTAGB_NO_COLLECTED_CUTS (-1)
+#define CCTAGB_NO_SELECTED_CUTS (-2)
+#define CCTAGB_OPTI_HAS_DIVERGED (-3)
+#define CCTAGB_ID_NOT_RELIABLE (-4)
+#define CCTAGB_DEGENERATE (-5)
+
+/* Center refinement used by identification. */
+#define CCTAGB_REFINE_GRID 0          /* the reference's 5x5 shrinking grid search       */
+#define CCTAGB_REFINE_GAUSS_NEWTON 1  /* adjoint-driven Gauss-Newton, FP64 normal solve  */
+
+/* Field names and defaults follow cctag::Parameters (Params.hpp:27-66). */
+typedef struct cctagb_params {
+    float cannyThrLow;                          /* 0.01  */
+    float cannyThrHigh;                         /* 0.04  */
+    int distSearch;                             /* 30    */
+    int thrGradientMagInVote;                   /* 2500  */
+    float angleVoting;                          /* 0     */
+    float ratioVoting;                          /* 4     */
+    float averageVoteMin;                       /* 0     */
+    float thrMedianDistanceEllipse;             /* 3     */
+    int maximumNbSeeds;                         /* 500   */
+    int maximumNbCandidatesLoopTwo;             /* 40    */
+    int nCrowns;                                /* 3     */
+    int nCircles;                               /* 2*nCrowns */
+    int minPointsSegmentCandidate;              /* 10    */
+    int minVotesToSelectCandidate;              /* 3     */
+    float threshRobustEstimationOfOuterEllipse; /* 30    */
+    float ellipseGrowingEllipticHullWidth;      /* 2.3   */
+    int windowSizeOnInnerEllipticSegment;       /* 20    */
+    int numberOfMultiresLayers;                 /* 4     */
+    int numberOfProcessedMultiresLayers;        /* 4     */
+    int nSamplesOuterEllipse;                   /* 150   */
+    int numCutsInIdentStep;                     /* 22    */
+    int numSamplesOuterEdgePointsRefinement;    /* 20    */
+    int cutsSelectionTrials;                    /* 500   */
+    int sampleCutLength;                        /* 100   */
+    int imagedCenterNGridSample;                /* 5     */
+    float imagedCenterNeighbourSize;            /* 0.2   */
+    float minIdentProba;                        /* 1e-6  */
+    int useLMDif;                               /* 1 (unused by the reference path) */
+    int searchForAnotherSegment;                /* 1     */
+    int writeOutput;                            /* 0     */
+    int doIdentification;                       /* 1     */
+    uint32_t maxEdges;                          /* 20000 (unused by the reference path) */
+    /* B200-specific */
+    int refineMode;                             /* CCTAGB_REFINE_GRID */
+    int gnIterations;                           /* 6: Gauss-Newton steps in REFINE_GAUSS_NEWTON */
+    int edgeCapacityDivisor;                    /* 4: edge capacity per level = W*H/divisor */
+} cctagb_params;
+
+typedef struct cctagb_ellipse {
+    float cx, cy, a, b, angle; /* parameters (Ellipse.hpp)            */
+    float m[9];                /* row-major conic matrix               */
+} cctagb_ellipse;
+
+typedef struct cctagb_marker {
+    int id;                    /* 0-based bank row, -1 if none         */
+    int status;                /* CCTAGB_ID_RELIABLE or a failure code */
+    float x, y;                /* refined imaged center (centerImg)    */
+    cctagb_ellipse outer;      /* rescaledOuterEllipse (level-0 frame) */
+    float homography[9];       /* row-major, marker plane -> image     */
+    float quality;             /* 1 / normalised residual              */
+    int pyramidLevel;
+    float scale;
+} cctagb_marker;
+
+typedef struct cctagb_stats {
+    int edge_points[8];        /* per level                            */
+    int seeds[8];              /* per level                            */
+    int candidates;            /* markers before identification        */
+    int markers;               /* markers returned                     */
+    float ms_image_stage;      /* device time: pyramid .. seeds        */
+    float ms_host_candidates;  /* host wall time of the candidate stage */
+    float ms_identify;         /* device time of identification        */
+    float ms_total;            /* host wall time of the whole call     */
+} cctagb_stats;
+
+typedef struct cctagb_handle cctagb_handle;
+
+void cctagb_params_default(cctagb_params* p, int nCrowns);
+const char* cctagb_status_string(cctagb_status s);
+
+cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int max_batch, cctagb_handle** out);
+cctagb_status cctagb_destroy(cctagb_handle* h);
+const char* cctagb_last_error_string(const cctagb_handle* h);
+
+/* Replace the marker bank: n_ids rows of n_ratios radius ratios (outer/ring). */
+cctagb_status cctagb_set_bank(cctagb_handle* h, const float* ratios, int n_ids, int n_ratios);
+
+/* Full detection of one 8-bit gray frame held in host memory. */
+cctagb_status cctagb_detect(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int frame_id,
+                            cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats);
+
+/* Same, with the frame already in device memory (pitch in bytes). */
+cctagb_status cctagb_detect_device(cctagb_handle* h, const uint8_t* d_gray, int w, int hgt, size_t pitch,
+                                   int frame_id, cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats);
+
+/* Image stage only (pyramid, derivatives, Canny, thinning, edge points, vote,
+ * seeds) on the handle's stream; results stay on the device and are read with
+ * the cctagb_level_* calls.  d_gray may be a device or a host pointer
+ * (is_device says which). */
+cctagb_status cctagb_image_stage(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int is_device);
+
+/* Per-level results of the last image stage (host copies). */
+cctagb_status cctagb_level_size(cctagb_handle* h, int level, int* w, int* hgt);
+cctagb_status cctagb_level_planes(cctagb_handle* h, int level, uint8_t* src, int16_t* dx, int16_t* dy,
+                                  uint8_t* edges);
+cctagb_status cctagb_level_edge_points(cctagb_handle* h, int level, int cap, int* n, int32_t* x, int32_t* y);
+cctagb_status cctagb_level_links(cctagb_handle* h, int level, int cap, int32_t* before, int32_t* after);
+cctagb_status cctagb_level_votes(cctagb_handle* h, int level, int cap, int32_t* chosen, int32_t* nvotes,
+                                 float* flow_length, int32_t* voter_off, int32_t* voter_list, int voter_cap,
+                                 int32_t* n_voters);
+/* Seeds in the reference's processing order (push order, then std::sort by votes). */
+cctagb_status cctagb_level_seeds(cctagb_handle* h, int level, int cap, int32_t* seeds, int* n);
+
+/* The CUDA stream (cudaStream_t) on which the handle launches its work, so a
+ * caller can order its own work or CUDA events against it. */
+cctagb_status cctagb_get_stream(cctagb_handle* h, void** stream);
+
+/* Per-stage device timing of the image stage: when enabled, CUDA events are
+ * captured between the stages and cctagb_stage_times returns the last frame's
+ * milliseconds per stage (names from cctagb_stage_name). */
+cctagb_status cctagb_set_stage_timing(cctagb_handle* h, int enable);
+cctagb_status cctagb_stage_times(cctagb_handle* h, int cap, float* ms, int* n);
+const char* cctagb_stage_name(int stage);
+
+/* Canny NMS + hysteresis + thinning from caller-given derivatives (host
+ * arrays, w*hgt int16 each); edges out as 0/255 bytes. */
+cctagb_status cctagb_canny_from_derivatives(cctagb_handle* h, const int16_t* dx, const int16_t* dy, int w, int hgt,
+                                            uint8_t* edges);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCTAG_B200_H */

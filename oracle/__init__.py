@@ -1,0 +1,142 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes binding of the CPU oracle (liboracle.so).
+
+Imported by the test-suite, ``__graft_entry__.smoke()`` and the CPU-baseline leg
+of ``bench.py`` only, as the checker / the timed CPU restatement of the
+reference path.  The product library never loads it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .build import LIB, build_oracle
+
+_P = C.c_void_p
+_I = C.c_int
+_F = C.c_float
+
+
+class VoteParams(C.Structure):
+    _fields_ = [("distSearch", _I), ("thrGradientMagInVote", _I), ("angleVoting", _F), ("ratioVoting", _F),
+                ("nCrowns", _I), ("minVotesToSelectCandidate", _I)]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build_oracle()
+        lib = C.CDLL(str(LIB))
+        lib.orc_pyramid_down.argtypes = [_P, _I, _I, _P, _I, _I]
+        lib.orc_derivatives.argtypes = [_P, _I, _I, _P, _P]
+        lib.orc_canny.argtypes = [_P, _P, _I, _I, _F, _F, _P, _P]
+        lib.orc_thin_lut.argtypes = [_I, _P]
+        lib.orc_thin.argtypes = [_P, _I, _I]
+        lib.orc_vote.argtypes = [_P, _P, _P, _I, _I, C.POINTER(VoteParams), _I] + [_P] * 14
+        lib.orc_vote.restype = _I
+        lib.orc_level.argtypes = [_P, _I, _I, _F, _F, _P, _P, _P]
+        _extra_signatures(lib)
+        _lib = lib
+    return _lib
+
+
+def _extra_signatures(lib):
+    """Signatures of the identification / candidate entry points (oracle_ident.cpp)."""
+    for name, (res, args) in IDENT_SIGNATURES.items():
+        if hasattr(lib, name):
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+
+
+IDENT_SIGNATURES: dict = {}
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def pyramid(gray: np.ndarray, levels: int = 4):
+    lib = load()
+    out = [np.ascontiguousarray(gray, dtype=np.uint8)]
+    for _ in range(1, levels):
+        h, w = out[-1].shape
+        d = np.empty((h // 2, w // 2), np.uint8)
+        lib.orc_pyramid_down(_p(out[-1]), w, h, _p(d), w // 2, h // 2)
+        out.append(d)
+    return out
+
+
+def derivatives(img: np.ndarray):
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape
+    dx = np.empty((h, w), np.int16)
+    dy = np.empty((h, w), np.int16)
+    load().orc_derivatives(_p(img), w, h, _p(dx), _p(dy))
+    return dx, dy
+
+
+def canny(dx: np.ndarray, dy: np.ndarray, thr_low=0.01 * 256, thr_high=0.04 * 256, with_map=False):
+    dx = np.ascontiguousarray(dx, dtype=np.int16)
+    dy = np.ascontiguousarray(dy, dtype=np.int16)
+    h, w = dx.shape
+    e = np.empty((h, w), np.uint8)
+    m = np.empty((h, w), np.uint8) if with_map else None
+    load().orc_canny(_p(dx), _p(dy), w, h, np.float32(thr_low), np.float32(thr_high), _p(e), _p(m))
+    return (e, m) if with_map else e
+
+
+def thin_lut(pass_no: int) -> np.ndarray:
+    lut = np.empty(512, np.uint8)
+    load().orc_thin_lut(pass_no, _p(lut))
+    return lut
+
+
+def thin(edges: np.ndarray) -> np.ndarray:
+    e = np.ascontiguousarray(edges, dtype=np.uint8).copy()
+    h, w = e.shape
+    load().orc_thin(_p(e), w, h)
+    return e
+
+
+def level(img: np.ndarray, thr_low=np.float32(0.01) * np.float32(256), thr_high=np.float32(0.04) * np.float32(256)):
+    """Derivatives -> Canny -> thinning of one pyramid level."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w = img.shape
+    dx = np.empty((h, w), np.int16)
+    dy = np.empty((h, w), np.int16)
+    e = np.empty((h, w), np.uint8)
+    load().orc_level(_p(img), w, h, np.float32(thr_low), np.float32(thr_high), _p(dx), _p(dy), _p(e))
+    return dx, dy, e
+
+
+def vote(edges, dx, dy, distSearch=30, thrGradient=2500, angleVoting=0.0, ratioVoting=4.0, nCrowns=3, minVotes=3):
+    edges = np.ascontiguousarray(edges, dtype=np.uint8)
+    dx = np.ascontiguousarray(dx, dtype=np.int16)
+    dy = np.ascontiguousarray(dy, dtype=np.int16)
+    h, w = edges.shape
+    cap = int((edges == 255).sum()) + 1
+    i32 = lambda n=cap: np.empty(n, np.int32)  # noqa: E731
+    ex, ey, before, after, chosen = i32(), i32(), i32(), i32(), i32()
+    total = np.empty(cap, np.float32)
+    nvotes, is_max = i32(), i32()
+    flow = np.empty(cap, np.float32)
+    voff, vlist = i32(cap + 1), i32()
+    spush, ssorted = i32(), i32()
+    ns = np.zeros(1, np.int32)
+    vp = VoteParams(distSearch, thrGradient, angleVoting, ratioVoting, nCrowns, minVotes)
+    E = load().orc_vote(_p(edges), _p(dx), _p(dy), w, h, C.byref(vp), cap, _p(ex), _p(ey), _p(before), _p(after),
+                        _p(chosen), _p(total), _p(nvotes), _p(is_max), _p(flow), _p(voff), _p(vlist), _p(spush),
+                        _p(ssorted), _p(ns))
+    if E < 0:
+        raise RuntimeError("oracle vote: capacity exceeded")
+    S = int(ns[0])
+    return dict(x=ex[:E].copy(), y=ey[:E].copy(), before=before[:E].copy(), after=after[:E].copy(),
+                chosen=chosen[:E].copy(), total=total[:E].copy(), nvotes=nvotes[:E].copy(),
+                is_max=is_max[:E].copy(), flow=flow[:E].copy(), voff=voff[:E + 1].copy(),
+                vlist=vlist[:voff[E]].copy(), seeds_push=spush[:S].copy(), seeds=ssorted[:S].copy())

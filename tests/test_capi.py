@@ -1,0 +1,53 @@
+"""CPU tests of the C ABI: the library loads, exports every declared symbol,
+and the calls that need no GPU behave."""
+import ctypes as C
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").rglob("*.h"):
+        text = h.read_text()
+        names |= set(re.findall(r"^\s*(?:[\w\*\s]+?)\b(cctagb_\w+)\s*\(", text, flags=re.M))
+    return names
+
+
+def test_library_exports_every_declared_symbol(built_library):
+    lib = C.CDLL(str(built_library))
+    names = declared_symbols()
+    assert len(names) >= 15
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_every_declared_symbol(built_library):
+    from cctag_b200 import capi
+
+    assert declared_symbols() <= set(capi.SIGNATURES)
+
+
+def test_default_params_match_reference_defaults(built_library):
+    from cctag_b200 import capi
+
+    p = capi.default_params(3)
+    # Params.hpp:27-66
+    assert (p.distSearch, p.thrGradientMagInVote, p.nCrowns, p.nCircles) == (30, 2500, 3, 6)
+    assert abs(p.cannyThrLow - 0.01) < 1e-9 and abs(p.cannyThrHigh - 0.04) < 1e-9
+    assert (p.maximumNbSeeds, p.maximumNbCandidatesLoopTwo, p.minVotesToSelectCandidate) == (500, 40, 3)
+    assert (p.nSamplesOuterEllipse, p.numCutsInIdentStep, p.sampleCutLength) == (150, 22, 100)
+    assert p.imagedCenterNGridSample == 5 and abs(p.imagedCenterNeighbourSize - 0.2) < 1e-7
+    assert abs(p.ellipseGrowingEllipticHullWidth - 2.3) < 1e-6
+
+
+def test_status_strings_and_null_handles(built_library):
+    from cctag_b200 import capi
+
+    lib = capi.load()
+    assert lib.cctagb_status_string(capi.OK) == b"ok"
+    assert lib.cctagb_destroy(None) == capi.BAD_ARG
+    n = C.c_int()
+    assert lib.cctagb_detect(None, None, 1, 1, 1, 0, None, 0, C.byref(n), None) == capi.BAD_ARG
+    assert lib.cctagb_create(None, 64, 64, 1, None) == capi.BAD_ARG
