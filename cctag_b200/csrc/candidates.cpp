@@ -1,0 +1,779 @@
+// Host candidate stage (see candidates.hpp).  The reference runs its three
+// candidate loops with TBB and shared per-point flags, so its output depends
+// on the thread schedule; here the loops run in index order (the order of the
+// reference's single-threaded CCTAG_SERIALIZE build) and the PCG32 stream is
+// reset for every frame, which makes the result deterministic.
+#include "candidates.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <deque>
+#include <limits>
+#include <stdexcept>
+#include <unordered_set>
+
+namespace cctagb {
+
+using geo::Ellipse;
+using geo::Pt;
+
+void EdgeSet::reset_state()
+{
+    processed_in.assign(E, 0);
+    processed_aux.assign(E, 0);
+    processed.assign(E, 0);
+    n_segment_out.assign(E, -1);
+}
+
+namespace {
+
+constexpr int kEdgeNotFound = -1;
+constexpr int kConvexityLost = -2;
+constexpr float kPi = 3.14159265358979323846f;
+
+inline uint32_t packxy(int x, int y) { return (uint32_t(x) << 16) | (uint32_t(y) & 0xFFFF); }
+
+// Vote.cpp:272-394 edgeLinkingDir: follow the edge contour from p while the
+// gradient direction keeps turning one way (convexity).
+void edge_linking_dir(EdgeSet& es, std::unordered_set<uint32_t>& processed, int p, int dir, std::deque<int>& seg,
+                      size_t window, float averageVoteMin)
+{
+    std::deque<float> phi;
+    size_t i = 0;
+    bool found = true;
+    int stop = 0;
+    const size_t maxLength = 100;
+    float averageVote = float(es.voters(p));
+    static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+    while (i < maxLength && found && averageVote >= averageVoteMin) {
+        const float angle = std::fmod(std::atan2(es.dy(p), es.dx(p)) + 2.0f * kPi, 2.0f * kPi);
+        phi.push_back(angle);
+        if (phi.size() > window) phi.pop_front();
+        const int shifting = int(std::round(((angle + kPi / 4.0f) / (2.0f * kPi)) * 8.0f)) - 1;
+        const int yoff[8] = {0, -dir, -dir, -dir, 0, dir, dir, dir};
+        int j = 0;
+        stop = 0;
+        while (!stop) {
+            if (j >= 8) {
+                stop = kEdgeNotFound;
+            } else {
+                const int k = dir == 1 ? (8 - shifting + j) % 8 : (shifting + j) % 8;
+                const int sx = es.x(p) + xoff[k];
+                const int sy = es.y(p) + yoff[k];
+                if (sx >= 0 && sx < es.W && sy >= 0 && sy < es.H && es.at(sx, sy) >= 0 &&
+                    !processed.count(packxy(sx, sy))) {
+                    const float d = phi.back() - phi.front();
+                    if (phi.size() == window) {
+                        if (float(dir) * std::sin(d) < 0.0f) stop = kConvexityLost;
+                    } else {
+                        const float s = float(dir) * std::sin(d);
+                        const float c = std::cos(d);
+                        if ((s < -0.707f && c > 0.f) || (s < 0.f && c < 0.f)) stop = kConvexityLost;
+                    }
+                    if (stop == 0) {
+                        processed.insert(packxy(es.x(p), es.y(p)));
+                        p = es.at(sx, sy);
+                        if (dir > 0) seg.push_back(p);
+                        else seg.push_front(p);
+                        averageVote = (averageVote * float(seg.size()) + float(es.voters(p))) / (float(seg.size()) + 1.f);
+                        stop = 1;
+                    }
+                    processed.insert(packxy(es.x(p), es.y(p)));
+                }
+            }
+            ++j;
+        }
+        found = stop == 1;
+        ++i;
+    }
+    if (i == maxLength || stop == kConvexityLost) {
+        if (seg.size() > window) {
+            size_t n = 0;
+            for (int q : seg) {
+                if (n == seg.size() - window) break;
+                es.processed_in[q] = 1;
+                ++n;
+            }
+        }
+    } else if (stop == kEdgeNotFound) {
+        for (int q : seg) es.processed_in[q] = 1;
+    }
+}
+
+// Vote.cpp:255-270
+void edge_linking(EdgeSet& es, std::deque<int>& seg, int pmax, size_t window, float averageVoteMin)
+{
+    std::unordered_set<uint32_t> processed;
+    seg.push_back(pmax);
+    es.processed_in[pmax] = 1;
+    processed.insert(packxy(es.x(pmax), es.y(pmax)));
+    edge_linking_dir(es, processed, pmax, 1, seg, window, averageVoteMin);
+    edge_linking_dir(es, processed, pmax, -1, seg, window, averageVoteMin);
+}
+
+// Vote.cpp:396-412: voters of the segment's points that received at least
+// voteMax/14 votes.
+void children_of(const EdgeSet& es, const std::deque<int>& seg, std::vector<int>& children)
+{
+    size_t voteMax = 1;
+    for (int e : seg) voteMax = std::max(voteMax, size_t(es.voters(e)));
+    for (int e : seg) {
+        const int n = es.voters(e);
+        if (n > 0 && size_t(n) >= voteMax / 14)
+            for (int k = es.voff[e]; k < es.voff[e + 1]; ++k) children.push_back(es.vlist[k]);
+    }
+}
+
+enum Weight { kNoWeight = 0, kInvGradWeight = 1 };
+
+// 5x5 linear solve with partial pivoting (FP64); false if singular.
+bool solve5(double A[5][5], double b[5], double x[5])
+{
+    int perm[5] = {0, 1, 2, 3, 4};
+    for (int c = 0; c < 5; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 5; ++r)
+            if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+        if (A[piv][c] == 0.0) return false;
+        if (piv != c) {
+            for (int k = 0; k < 5; ++k) std::swap(A[piv][k], A[c][k]);
+            std::swap(b[piv], b[c]);
+            std::swap(perm[piv], perm[c]);
+        }
+        for (int r = c + 1; r < 5; ++r) {
+            const double f = A[r][c] / A[c][c];
+            for (int k = c; k < 5; ++k) A[r][k] -= f * A[c][k];
+            b[r] -= f * b[c];
+        }
+    }
+    for (int r = 4; r >= 0; --r) {
+        double s = b[r];
+        for (int k = r + 1; k < 5; ++k) s -= A[r][k] * x[k];
+        x[r] = s / A[r][r];
+    }
+    return true;
+}
+
+// Vote.cpp:414-576 outlierRemoval: LMedS ellipse from random 5-point subsets
+// of (a regular subsample of) the points; keeps the points whose (weighted)
+// distance is below threshold * median.  The reference retries forever when
+// the conic of a draw is not a real ellipse; here the number of draws is
+// capped (an outlier-free run needs < 100 draws, the cap is 100x that).
+void outlier_removal(const EdgeSet& es, const std::vector<int>& children, std::vector<int>& filtered, float& SmFinal,
+                     float threshold, int weightedType, size_t maxSize, geo::Pcg32& rng)
+{
+    filtered.reserve(children.size());
+    const size_t nSub = std::min(children.size(), maxSize);
+    if (nSub < 5) return;
+    const float step = float(children.size()) / float(nSub);
+    std::vector<Pt> pts;
+    std::vector<float> weights;
+    pts.reserve(children.size());
+    size_t k = 0;
+    for (size_t i = 0; i < children.size(); ++i) {
+        if (i == size_t(float(k) * step)) {
+            ++k;
+            const int e = children[i];
+            pts.push_back({float(es.x(e)), float(es.y(e))});
+            if (weightedType == kInvGradWeight) weights.push_back(255.f / es.norm(e));
+        }
+    }
+    Ellipse qm;
+    float Sm = 10000000.0f;
+    size_t counter = 0, draws = 0;
+    int perm[5];
+    std::vector<float> dist(pts.size());
+    while (counter < 70 && draws < 7000) {
+        ++draws;
+        rng.rand5(perm, pts.size());
+        double A[5][5], b[5], t[5];
+        for (int i = 0; i < 5; ++i) {
+            const double x = pts[perm[i]].x, y = pts[perm[i]].y;
+            A[i][0] = x * x;
+            A[i][1] = 2.0 * x * y;
+            A[i][2] = y * y;
+            A[i][3] = 2.0 * x;
+            A[i][4] = 2.0 * y;
+            b[i] = -1.0;
+        }
+        if (!solve5(A, b, t)) {
+            ++counter;
+            continue;
+        }
+        if (!(float(t[0]) * float(t[2]) - float(t[1]) * float(t[1]) > 0)) {
+            ++counter;
+            continue;
+        }
+        geo::Mat3 Q;
+        Q.m[0][0] = float(t[0]);
+        Q.m[0][1] = Q.m[1][0] = float(t[1]);
+        Q.m[0][2] = Q.m[2][0] = float(t[3]);
+        Q.m[1][1] = float(t[2]);
+        Q.m[1][2] = Q.m[2][1] = float(t[4]);
+        Q.m[2][2] = 1.f;
+        try {
+            const Ellipse q = Ellipse::from_matrix(Q);
+            const float ratio = q.a / q.b;
+            if (ratio < 0.04f || ratio > 25) {
+                ++counter;
+                continue;
+            }
+            for (size_t i = 0; i < pts.size(); ++i) dist[i] = geo::dist_point_ellipse(q.Q, pts[i].x, pts[i].y);
+            if (weightedType != kNoWeight)
+                for (size_t i = 0; i < dist.size(); ++i) dist[i] *= weights[i];
+            std::vector<float> tmp = dist;
+            const float S = geo::median_ref(tmp);
+            if (S < Sm) {
+                counter = 0;
+                qm = q;
+                Sm = S;
+            } else {
+                ++counter;
+            }
+        } catch (...) {
+        }
+    }
+    std::vector<float> vd;
+    vd.reserve(children.size());
+    for (int e : children) {
+        float d = geo::dist_point_ellipse(qm.Q, float(es.x(e)), float(es.y(e)));
+        if (weightedType == kInvGradWeight) d = d * 255 / es.norm(e);
+        if (d < threshold * Sm) {
+            filtered.push_back(e);
+            vd.push_back(d);
+        }
+    }
+    if (vd.empty()) return;
+    SmFinal = geo::median_ref(vd);
+}
+
+// Fitting.cpp:213-292 innerProdMin (only its return value is used).
+float inner_prod_min(const EdgeSet& es, const std::vector<int>& fc, float thr)
+{
+    if (fc.empty()) return 1.1f;
+    const int p0 = fc.front();
+    float ng = std::sqrt(es.dx(p0) * es.dx(p0) + es.dy(p0) * es.dy(p0));
+    const float gx0 = es.dx(p0) / ng, gy0 = es.dy(p0) / ng;
+    float mn = 1.1f;
+    int pA = -1;
+    for (size_t i = 1; i < fc.size(); ++i) {
+        const int q = fc[i];
+        ng = std::sqrt(es.dx(q) * es.dx(q) + es.dy(q) * es.dy(q));
+        const float ip = gx0 * (es.dx(q) / ng) + gy0 * (es.dy(q) / ng);
+        if (ip <= thr) return ip;
+        if (ip < mn) {
+            mn = ip;
+            pA = q;
+        }
+    }
+    if (pA < 0) return mn;
+    ng = std::sqrt(es.dx(pA) * es.dx(pA) + es.dy(pA) * es.dy(pA));
+    const float gxm = es.dx(pA) / ng, gym = es.dy(pA) / ng;
+    mn = 1.f;
+    for (int q : fc) {
+        ng = std::sqrt(es.dx(q) * es.dx(q) + es.dy(q) * es.dy(q));
+        const float ip = gxm * (es.dx(q) / ng) + gym * (es.dy(q) / ng);
+        if (ip <= thr) return ip;
+        if (ip < mn) mn = ip;
+    }
+    return mn;
+}
+
+Ellipse fit_points(const EdgeSet& es, const std::vector<int>& idx)
+{
+    std::vector<Pt> p(idx.size());
+    for (size_t i = 0; i < idx.size(); ++i) p[i] = {float(es.x(idx[i])), float(es.y(idx[i]))};
+    return geo::fit_ellipse(p.data(), p.size());
+}
+
+Ellipse fit_circle_points(const EdgeSet& es, const std::vector<int>& idx)
+{
+    std::vector<Pt> p(idx.size());
+    for (size_t i = 0; i < idx.size(); ++i) p[i] = {float(es.x(idx[i])), float(es.y(idx[i]))};
+    return geo::fit_circle(p.data(), p.size());
+}
+
+// EllipseGrowing.cpp:345-357 (isGoodEGPoints) + :359-376 (ellipseGrowingInit)
+bool ellipse_growing_init(const EdgeSet& es, const std::vector<int>& fc, Ellipse& e)
+{
+    if (inner_prod_min(es, fc, 0.25f) <= 0.25f) {
+        e = fit_points(es, fc);
+        return true;
+    }
+    e = fit_circle_points(es, fc);
+    return false;
+}
+
+// EllipseGrowing.cpp:378-422 connectedPoint: depth-first growth through
+// 8-neighbours inside the hull whose gradient points away from the center.
+// Iterative form of the reference's recursion (same visiting order).
+void connected_point(std::vector<int>& pts, uint64_t mask, EdgeSet& es, const Ellipse& qIn, const Ellipse& qOut,
+                     int x, int y)
+{
+    static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+    static const int yoff[8] = {0, -1, -1, -1, 0, 1, 1, 1};
+    struct Frame {
+        int x, y, k;
+    };
+    std::vector<Frame> st;
+    es.processed[es.at(x, y)] |= mask;
+    st.push_back({x, y, 0});
+    while (!st.empty()) {
+        Frame& f = st.back();
+        if (f.k >= 8) {
+            st.pop_back();
+            continue;
+        }
+        const int k = f.k++;
+        const int sx = f.x + xoff[k], sy = f.y + yoff[k];
+        if (sx < 0 || sx >= es.W || sy < 0 || sy >= es.H) continue;
+        const int e = es.at(sx, sy);
+        if (e < 0) continue;
+        if (!geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e))) || (es.processed[e] & mask)) continue;
+        const float ox = qIn.cx - float(es.x(e)), oy = qIn.cy - float(es.y(e));
+        if (es.dx(e) * ox + es.dy(e) * oy < 0) {
+            pts.push_back(e);
+            es.processed[e] |= mask;
+            st.push_back({sx, sy, 0});
+        }
+    }
+}
+
+// EllipseGrowing.cpp:443-457
+void ellipse_hull(EdgeSet& es, std::vector<int>& pts, const Ellipse& e, float delta, uint64_t mask)
+{
+    Ellipse qIn, qOut;
+    geo::compute_hull(e, delta, qIn, qOut);
+    const size_t init = pts.size();
+    for (size_t i = 0; i < init; ++i) {
+        const int p = pts[i];
+        connected_point(pts, mask, es, qIn, qOut, es.x(p), es.y(p));
+    }
+}
+
+size_t count_in_hull(const EdgeSet& es, const std::vector<int>& pts, const Ellipse& e, float width)
+{
+    Ellipse qIn, qOut;
+    geo::compute_hull(e, width, qIn, qOut);
+    size_t n = 0;
+    for (int p : pts)
+        if (geo::is_in_hull(qIn, qOut, float(es.x(p)), float(es.y(p)))) ++n;
+    return n;
+}
+
+// EllipseGrowing.cpp:459-551 ellipseGrowing2
+void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>& outer, Ellipse& ellipse, float width,
+                      size_t runId, bool goodInit)
+{
+    const uint64_t mask = uint64_t(1) << (runId & 63);
+    outer = fc;
+    for (int c : fc) es.processed[c] |= mask;
+    if (!goodInit) {
+        int newSize = int(outer.size());
+        int maxNb = newSize, nIterMax = 0, lastSize = 0, nIter = 0;
+        std::vector<std::vector<int>> sets{outer};
+        std::vector<Ellipse> ells{ellipse};
+        ++nIter;
+        while (newSize - lastSize > 0) {
+            lastSize = int(count_in_hull(es, outer, ellipse, width));
+            ellipse_hull(es, outer, ellipse, width, mask);
+            sets.push_back(outer);
+            ells.push_back(ellipse);
+            ellipse = fit_circle_points(es, outer);
+            newSize = int(count_in_hull(es, outer, ellipse, width));
+            if (newSize > maxNb) {
+                maxNb = newSize;
+                nIterMax = nIter;
+            }
+            ++nIter;
+        }
+        outer = sets[nIterMax];
+        ellipse = ells[nIterMax];
+        for (auto& s : sets)
+            for (int p : s) es.processed[p] &= ~mask;
+        for (int p : outer) es.processed[p] |= mask;
+    }
+    ellipse = fit_points(es, outer);
+    size_t lastSize = 0;
+    while (outer.size() > lastSize) {
+        lastSize = outer.size();
+        ellipse_hull(es, outer, ellipse, width, mask);
+        ellipse = fit_points(es, outer);
+    }
+}
+
+struct Candidate {
+    int seed = -1;
+    std::deque<int> segment;
+    std::vector<int> outer;
+    Ellipse outerEllipse;
+    std::vector<int> filtered;
+    int score = 0;
+    size_t nLabel = 0;
+    float averageReceivedVote = 0.f;
+};
+
+float quality_of(size_t npts, const Ellipse& e) { return float(npts) / float(geo::rasterize_perimeter(e)); }
+
+// Detection.cpp:115-267 completeFlowComponent
+void complete_flow_component(Candidate& c, EdgeSet& es, std::vector<Candidate>& loop2, size_t& nSegmentOut,
+                             size_t runId, const cctagb_params& p, geo::Pcg32& rng)
+{
+    try {
+        std::vector<int> children;
+        children_of(es, c.segment, children);
+        if (children.size() < size_t(p.minPointsSegmentCandidate)) return;
+        c.score = int(children.size());
+        float SmFinal = 1e+10f;
+        outlier_removal(es, children, c.filtered, SmFinal, p.threshRobustEstimationOfOuterEllipse, kInvGradWeight, 60,
+                        rng);
+        if (c.filtered.size() < 5) return;
+        size_t nLabel;
+        {
+            long common = -1;
+            for (int q : c.filtered)
+                if (es.n_segment_out[q] != -1) {
+                    common = es.n_segment_out[q];
+                    break;
+                }
+            nLabel = common == -1 ? nSegmentOut++ : size_t(common);
+            for (int q : c.filtered) es.n_segment_out[q] = int32_t(nLabel);
+        }
+        const bool goodInit = ellipse_growing_init(es, c.filtered, c.outerEllipse);
+        ellipse_growing2(es, c.filtered, c.outer, c.outerEllipse, p.ellipseGrowingEllipticHullWidth, runId, goodInit);
+        c.nLabel = nLabel;
+        std::vector<float> vd;
+        vd.reserve(c.outer.size());
+        for (int q : c.outer) vd.push_back(geo::dist_point_ellipse(c.outerEllipse.Q, float(es.x(q)), float(es.y(q))));
+        if (vd.empty()) return;
+        SmFinal = geo::median_ref(vd);
+        if (SmFinal > p.thrMedianDistanceEllipse) return;
+        if (quality_of(c.outer.size(), c.outerEllipse) > 1.1f) return;
+        const float ratio = c.outerEllipse.a / c.outerEllipse.b;
+        if (ratio < 0.05f || ratio > 20) return;
+        loop2.push_back(c);
+    } catch (...) {
+    }
+}
+
+bool same_side(float x1, float y1, float x2, float y2, const float line[3])
+{
+    const float s1 = x1 * line[0] + y1 * line[1] + line[2];
+    const float s2 = x2 * line[0] + y2 * line[1] + line[2];
+    return s1 * s2 > 0;
+}
+
+// EllipseGrowing.hpp:24-33 isInEllipse: p^T Q p and p^T Q c have the same sign.
+bool in_ellipse(const Ellipse& e, float x, float y)
+{
+    const geo::Mat3& Q = e.Q;
+    const float s1 = geo::qform(Q, x, y);
+    const float qc0 = Q.m[0][0] * e.cx + Q.m[0][1] * e.cy + Q.m[0][2];
+    const float qc1 = Q.m[1][0] * e.cx + Q.m[1][1] * e.cy + Q.m[1][2];
+    const float qc2 = Q.m[2][0] * e.cx + Q.m[2][1] * e.cy + Q.m[2][2];
+    const float s2 = x * qc0 + y * qc1 + qc2;
+    return s1 * s2 > 0;
+}
+
+// EllipseGrowing.cpp:63-178 addCandidateFlowtoCCTag
+bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vector<int>& outer, const Ellipse& oe,
+                        std::vector<std::vector<DirPoint>>& pts, size_t numCircles)
+{
+    pts.resize(numCircles);
+    for (int e : outer) pts.back().push_back({float(es.x(e)), float(es.y(e)), es.dx(e), es.dy(e)});
+    std::vector<int> touched;
+    size_t nGradientOut = 0, nAdded = 0;
+    auto undo = [&]() {
+        for (int q : touched) es.processed_aux[q] = 0;
+    };
+    for (int p0 : fc) {
+        int dir = -1;
+        int p = p0;
+        const float ox = float(es.x(p0)), oy = float(es.y(p0));
+        const float a = ox - oe.cx, b = oy - oe.cy;
+        const float line[3] = {a, b, -a * oe.cx - b * oe.cy};
+        for (size_t j = 1; j < numCircles; ++j) {
+            p = dir == -1 ? es.before[p] : es.after[p];
+            if (p < 0) {
+                undo();
+                throw std::out_of_range("EdgePointCollection: missing link");
+            }
+            if (!es.processed_aux[p]) {
+                es.processed_aux[p] = 1;
+                touched.push_back(p);
+                const float ng = std::sqrt(es.dx(p) * es.dx(p) + es.dy(p) * es.dy(p));
+                const float gx = es.dx(p) / ng, gy = es.dy(p) / ng;
+                float tx = oe.cx - float(es.x(p)), ty = oe.cy - float(es.y(p));
+                const float dc = std::sqrt(tx * tx + ty * ty);
+                tx /= dc;
+                ty /= dc;
+                const DirPoint q{float(es.x(p)), float(es.y(p)), es.dx(p), es.dy(p)};
+                if (in_ellipse(oe, q.x, q.y) && same_side(ox, oy, q.x, q.y, line)) {
+                    if (float(-dir) * (gx * tx + gy * ty) < -0.5f && j >= numCircles - 2) ++nGradientOut;
+                    pts[numCircles - j - 1].push_back(q);
+                    if (j >= numCircles - 2) ++nAdded;
+                } else {
+                    pts.clear();
+                    undo();
+                    return false;
+                }
+            }
+            dir = -dir;
+        }
+    }
+    undo();
+    if (float(nGradientOut) / float(nAdded) > 0.5f) {
+        pts.clear();
+        return false;
+    }
+    return true;
+}
+
+// Vote.cpp:578-742 isAnotherSegment
+bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& outer, const Candidate& another,
+                        std::vector<std::vector<DirPoint>>& pts, size_t numCircles, float thrMedian, geo::Pcg32& rng)
+{
+    const std::vector<int>& aout = another.outer;
+    if (outer.size() < 5 || aout.size() < 5) return false;
+    std::vector<Pt> P(outer.size()), AP(aout.size());
+    for (size_t i = 0; i < outer.size(); ++i) P[i] = {float(es.x(outer[i])), float(es.y(outer[i]))};
+    for (size_t i = 0; i < aout.size(); ++i) AP[i] = {float(es.x(aout[i])), float(es.y(aout[i]))};
+    std::vector<float> d;
+    d.reserve(std::max(P.size(), AP.size()));
+    for (const Pt& q : P) d.push_back(geo::dist_point_ellipse(outerEllipse.Q, q.x, q.y));
+    const float SRef = geo::median_ref(d);
+    Ellipse qm;
+    float Sm = std::numeric_limits<float>::max();
+    size_t cnt = 0;
+    int perm[5];
+    while (cnt < 100) {
+        Pt pp[8];
+        rng.rand5(perm, outer.size());
+        for (int i = 0; i < 4; ++i) pp[i] = P[perm[i]];
+        rng.rand5(perm, aout.size());
+        for (int i = 0; i < 4; ++i) pp[4 + i] = AP[perm[i]];
+        try {
+            const Ellipse q = Ellipse::from_matrix(geo::fit_ellipse(pp, 8).Q);
+            const float ratio = q.a / q.b;
+            if (ratio < 0.12f || ratio > 8) {
+                ++cnt;
+                continue;
+            }
+            d.clear();
+            for (const Pt& r : P) d.push_back(geo::dist_point_ellipse(q.Q, r.x, r.y));
+            const float S1 = geo::median_ref(d);
+            d.clear();
+            for (const Pt& r : AP) d.push_back(geo::dist_point_ellipse(q.Q, r.x, r.y));
+            const float S2 = geo::median_ref(d);
+            const float S = S1 + S2;
+            if (S < Sm) {
+                cnt = 0;
+                qm = q;
+                Sm = S;
+            } else {
+                ++cnt;
+            }
+        } catch (...) {
+            ++cnt;
+        }
+    }
+    if (!(Sm < 6.f * SRef)) return false;
+    std::vector<int> merged = outer;
+    merged.insert(merged.end(), aout.begin(), aout.end());
+    const Ellipse fitted = fit_points(es, merged);
+    if (!(quality_of(merged.size(), fitted) < 1.1f)) return false;
+    d.clear();
+    for (int q : merged) d.push_back(geo::dist_point_ellipse(fitted.Q, float(es.x(q)), float(es.y(q))));
+    const float SmFinal = geo::median_ref(d);
+    if (!(SmFinal < thrMedian)) return false;
+    if (!add_candidate_flow(es, another.filtered, aout, fitted, pts, numCircles)) return false;
+    outer = merged;
+    outerEllipse = fitted;
+    return true;
+}
+
+// Detection.cpp:278-377 flowComponentAssembling
+void flow_component_assembling(EdgeSet& es, float& quality, size_t ci, const std::vector<Candidate>& loop2,
+                               Ellipse& outerEllipse, std::vector<int>& outer,
+                               std::vector<std::vector<DirPoint>>& pts, const cctagb_params& p, geo::Pcg32& rng)
+{
+    const Candidate& c = loop2[ci];
+    int score = -1;
+    size_t iMax = 0;
+    const float r = es.flow[c.seed] * 2.5f;
+    const Ellipse area = Ellipse::from_params(float(es.x(c.seed)), float(es.y(c.seed)), r, r, 0.f);
+    for (size_t i = 0; i < loop2.size(); ++i) {
+        if (i == ci) continue;
+        const Candidate& o = loop2[i];
+        if (c.nLabel == o.nLabel) continue;
+        const float ratio = es.flow[o.seed] / es.flow[c.seed];
+        if (!(ratio > 0.666f && ratio < 1.5f)) continue;
+        if (in_ellipse(area, float(es.x(o.seed)), float(es.y(o.seed)))) {
+            if (o.score > score) {
+                score = o.score;
+                iMax = i;
+            }
+        }
+    }
+    if (score > 0) {
+        if (is_another_segment(es, outerEllipse, outer, loop2[iMax], pts, size_t(p.nCrowns) * 2,
+                               p.thrMedianDistanceEllipse, rng))
+            quality = quality_of(outer.size(), outerEllipse);
+    }
+}
+
+// Detection.cpp:379-566 cctagDetectionFromEdgesLoopTwoIteration
+void loop_two_iteration(EdgeSet& es, const std::vector<Candidate>& loop2, size_t ci, int level, float scale,
+                        const cctagb_params& p, geo::Pcg32& rng, std::vector<MarkerCand>& markers)
+{
+    const Candidate& c = loop2[ci];
+    std::vector<int> outer = c.outer;
+    Ellipse oe = c.outerEllipse;
+    std::vector<std::vector<DirPoint>> pts;
+    try {
+        float quality = quality_of(outer.size(), oe);
+        if (p.searchForAnotherSegment && quality > 0.25f && quality < 0.7f)
+            flow_component_assembling(es, quality, ci, loop2, oe, outer, pts, p, rng);
+        if (!add_candidate_flow(es, c.filtered, c.outer, oe, pts, size_t(p.nCrowns) * 2)) return;
+        const Ellipse rescale = Ellipse::from_params(oe.cx, oe.cy, oe.a * scale, oe.b * scale, oe.angle);
+        const float realSize = quality * float(geo::rasterize_perimeter(rescale));
+        if ((quality <= 0.35f && realSize >= 300.0f) ||
+            (quality <= 0.45f && realSize >= 200.0f && realSize < 300.0f) ||
+            (quality <= 0.5f && realSize >= 100.0f && realSize < 200.0f) ||
+            (quality <= 0.5f && realSize >= 70.0f && realSize < 100.0f) ||
+            (quality <= 0.96f && realSize >= 50.0f && realSize < 70.0f) || (realSize < 50.0f))
+            return;
+        const float ratio = oe.a / oe.b;
+        if (ratio > 8.0f || ratio < 0.125f) return;
+        Ellipse qIn, qOut;
+        geo::compute_hull(oe, 3.6f, qIn, qOut);
+        for (int q : outer)
+            if (!geo::is_in_hull(qIn, qOut, float(es.x(q)), float(es.y(q)))) return;
+        float quality2 = 0;
+        for (int q : outer) quality2 += es.norm(q);
+        quality2 *= scale;
+        // CCTag constructor (CCTag.hpp:67-92): centerImg = ellipse center,
+        // stored ellipse shifted by +0.5, rescaled copy in level-0 pixels.
+        MarkerCand m;
+        m.cx_img = oe.cx;
+        m.cy_img = oe.cy;
+        m.outer = Ellipse::from_params(oe.cx + 0.5f, oe.cy + 0.5f, oe.a, oe.b, oe.angle);
+        m.rescaled = Ellipse::from_params(m.outer.cx * scale, m.outer.cy * scale, m.outer.a * scale,
+                                          m.outer.b * scale, m.outer.angle);
+        m.points = std::move(pts);
+        m.level = level;
+        m.scale = scale;
+        m.quality = quality2;
+        markers.push_back(std::move(m));
+    } catch (...) {
+    }
+}
+
+}  // namespace
+
+void detect_from_edges(EdgeSet& es, const std::vector<int32_t>& seeds, int level, float scale,
+                       const cctagb_params& p, geo::Pcg32& rng, std::vector<MarkerCand>& out)
+{
+    if (seeds.empty()) return;
+    const size_t nMax = size_t(std::max(es.H / 2, p.maximumNbSeeds));
+    const size_t nProc = std::min(seeds.size(), nMax);
+    // Loop 1 (Detection.cpp:69-113, 609-627): convex segments from the seeds,
+    // ranked by averageReceivedVote (stable insertion before equal keys).
+    std::vector<Candidate> loop1;
+    for (size_t s = 0; s < nProc; ++s) {
+        const int seed = seeds[s];
+        if (es.processed_in[seed]) continue;
+        Candidate c;
+        c.seed = seed;
+        edge_linking(es, c.segment, seed, size_t(p.windowSizeOnInnerEllipticSegment), p.averageVoteMin);
+        int nReceived = 0, nVoted = 0;
+        for (int q : c.segment) {
+            const int v = es.voters(q);
+            nReceived += v;
+            if (v > 0) ++nVoted;
+        }
+        c.averageReceivedVote = float(nReceived * nReceived) / float(nVoted);
+        auto it = std::lower_bound(loop1.begin(), loop1.end(), c, [](const Candidate& a, const Candidate& b) {
+            return a.averageReceivedVote > b.averageReceivedVote;
+        });
+        loop1.insert(it, std::move(c));
+    }
+    // Loop 2 (Detection.cpp:629-655)
+    const size_t n2 = std::min(loop1.size(), size_t(p.maximumNbCandidatesLoopTwo));
+    std::vector<Candidate> loop2;
+    size_t nSegmentOut = 0;
+    for (size_t i = 0; i < n2; ++i) complete_flow_component(loop1[i], es, loop2, nSegmentOut, i, p, rng);
+    // Loop 3 (Detection.cpp:677-688)
+    for (size_t i = 0; i < loop2.size(); ++i) loop_two_iteration(es, loop2, i, level, scale, p, rng, out);
+}
+
+namespace {
+
+// Multiresolution.cpp:43-142 intersectLineToTwoEllipses
+bool intersect_line_two(int y, const Ellipse& qIn, const Ellipse& qOut, const EdgeSet& es, std::vector<int>& hull)
+{
+    float io[2], ii[2];
+    const int no = geo::intersect_line(qOut, float(y), true, io);
+    const int ni = geo::intersect_line(qIn, float(y), true, ii);
+    auto take = [&](int x) {
+        const int e = es.at(x, y);
+        if (e < 0) return;
+        const float cx = qIn.cx - float(es.x(e)), cy = qIn.cy - float(es.y(e));
+        if (es.dx(e) * cx + es.dy(e) * cy < 0) hull.push_back(e);
+    };
+    if (no == 2 && ni == 2) {
+        const int b1 = std::max(0, int(io[0])), e1 = std::min(es.W - 1, int(ii[0]));
+        const int b2 = std::max(0, int(ii[1])), e2 = std::min(es.W - 1, int(io[1]));
+        for (int x = b1; x <= e1; ++x) take(x);
+        for (int x = b2; x <= e2; ++x) take(x);
+    } else if (no == 2 && ni <= 1) {
+        const int b = std::max(0, int(io[0])), e = std::min(es.W - 1, int(io[1]));
+        for (int x = b; x <= e; ++x) take(x);
+    } else if (no == 1 && ni == 0) {
+        if (io[0] >= 0 && io[0] < float(es.W)) take(int(io[0]));
+    } else {
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, geo::Pcg32& rng)
+{
+    for (MarkerCand& m : markers) {
+        if (m.level > 0) {
+            const float scale = m.scale;
+            Ellipse qIn, qOut;
+            geo::compute_hull(m.rescaled, scale, qIn, qOut);
+            std::vector<int> hull;
+            const float yc = m.rescaled.cy;
+            const int maxY = std::max(int(yc), 0);
+            const int minY = std::min(int(yc), es0.H - 1);
+            for (int y = maxY; y < es0.H; ++y)
+                if (!intersect_line_two(y, qIn, qOut, es0, hull)) break;
+            for (int y = minY; y >= 0; --y)
+                if (!intersect_line_two(y, qIn, qOut, es0, hull)) break;
+            if (hull.size() < 5) continue;
+            std::vector<int> filtered;
+            float SmFinal = 1e+10f;
+            outlier_removal(es0, hull, filtered, SmFinal, 20.0f, kNoWeight, 60, rng);
+            if (filtered.size() < 5) continue;
+            try {
+                const Ellipse fitted = fit_points(es0, filtered);
+                std::vector<DirPoint> dp;
+                dp.reserve(filtered.size());
+                for (int e : filtered) dp.push_back({float(es0.x(e)), float(es0.y(e)), es0.dx(e), es0.dy(e)});
+                m.cx_img *= scale;
+                m.cy_img *= scale;
+                m.rescaled = fitted;
+                m.rescaled_points = std::move(dp);
+            } catch (...) {
+            }
+        } else {
+            m.rescaled_points = m.points.empty() ? std::vector<DirPoint>() : m.points.back();
+        }
+    }
+}
+
+}  // namespace cctagb

@@ -1,0 +1,68 @@
+// Host candidate stage: seeds -> flow components -> outer ellipses -> marker
+// candidates, and the level-0 re-fit of markers found on coarse levels
+// (Detection.cpp:69-693, Vote.cpp:249-742, EllipseGrowing.cpp,
+// Multiresolution.cpp:43-193,319-401 of the reference).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "cctag_b200.h"
+#include "geometry.hpp"
+
+namespace cctagb {
+
+// Host view of one level's edge-point collection (EdgePointCollection,
+// Types.hpp:19-158) with the per-point state the candidate stage mutates.
+struct EdgeSet {
+    int W = 0, H = 0, E = 0;
+    const int32_t* exy = nullptr;
+    const int32_t* grad = nullptr;
+    const int32_t* before = nullptr;
+    const int32_t* after = nullptr;
+    const int32_t* voff = nullptr;
+    const int32_t* vlist = nullptr;
+    const float* flow = nullptr;
+    int32_t* idxmap = nullptr;  // W*H, -1 where no edge point (owned by the caller)
+
+    std::vector<uint8_t> processed_in, processed_aux;
+    std::vector<uint64_t> processed;  // per-candidate bit masks (ellipse growing)
+    std::vector<int32_t> n_segment_out;
+
+    int x(int i) const { return exy[i] & 0xffff; }
+    int y(int i) const { return exy[i] >> 16; }
+    float dx(int i) const { return float(int16_t(grad[i] & 0xffff)); }
+    float dy(int i) const { return float(int16_t(grad[i] >> 16)); }
+    float norm(int i) const { return std::sqrt(dx(i) * dx(i) + dy(i) * dy(i)); }
+    int voters(int i) const { return voff[i + 1] - voff[i]; }
+    int at(int px, int py) const { return idxmap[size_t(py) * W + px]; }
+    void reset_state();
+};
+
+struct DirPoint {
+    float x, y, dx, dy;
+};
+
+// A marker before identification (CCTag.hpp fields used downstream).
+struct MarkerCand {
+    float cx_img = 0, cy_img = 0;          // centerImg
+    geo::Ellipse outer;                     // outer ellipse at its level (+0.5 shift)
+    geo::Ellipse rescaled;                  // outer ellipse in level-0 pixels
+    std::vector<std::vector<DirPoint>> points;
+    std::vector<DirPoint> rescaled_points;  // outer points in level-0 pixels
+    int level = 0;
+    float scale = 1.f;
+    float quality = 0.f;
+    int status = 0;
+    int id = -1;
+    geo::Mat3 H = geo::Mat3::zero();
+};
+
+// Candidate markers of one level (cctagDetectionFromEdges, Detection.cpp:568-693).
+void detect_from_edges(EdgeSet& es, const std::vector<int32_t>& seeds, int level, float scale,
+                       const cctagb_params& p, geo::Pcg32& rng, std::vector<MarkerCand>& out);
+
+// Level-0 re-fit of markers detected on coarser levels (Multiresolution.cpp:319-401).
+void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, geo::Pcg32& rng);
+
+}  // namespace cctagb

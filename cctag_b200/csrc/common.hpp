@@ -104,5 +104,6 @@ void upload_constants(const float* bank, int n_ids, int n_ratios);
 void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, bool fused_pyramid,
                         cudaEvent_t* ev = nullptr);
 void launch_canny_only(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s);
+void launch_gate(cudaStream_t s, int us);
 
 }  // namespace cctagb

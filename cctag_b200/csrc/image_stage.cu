@@ -868,6 +868,16 @@ static void mark(cudaEvent_t* ev, int k, cudaStream_t s)
     if (ev) CCTAGB_CUDA(cudaEventRecord(ev[k], s));
 }
 
+// Holds the stream for about `us` microseconds (bounded loop) so that the
+// host can queue every stage behind it; used only by the per-stage timing
+// mode, which launches without a graph.
+__global__ void k_gate(int us)
+{
+    for (int i = 0; i < us; ++i) __nanosleep(1000);
+}
+
+void launch_gate(cudaStream_t s, int us) { k_gate<<<1, 1, 0, s>>>(us); }
+
 static void launch_edges(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, int write_derivs,
                          cudaEvent_t* ev)
 {

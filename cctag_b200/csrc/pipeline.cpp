@@ -120,10 +120,9 @@ void Pipeline::alloc(int max_w, int max_h)
     std::memset(h_cnt_, 0, sizeof(LevelCounters) * kMaxLevels);
 }
 
-void Pipeline::set_views(int w, int h)
+void Pipeline::set_views(int w, int h, int nl)
 {
     if (w > max_w_ || h > max_h_) throw Error{CCTAGB_TOO_LARGE, "frame larger than the handle's maximum"};
-    const int nl = params_.numberOfProcessedMultiresLayers;
     lv_.n = nl;
     lv_.cnt = d_cnt_;
     for (int l = 0; l < nl; ++l) {
@@ -146,19 +145,31 @@ void Pipeline::set_views(int w, int h)
 void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool is_device)
 {
     if (!gray || w < 1 || h < 1 || pitch < size_t(w)) throw Error{CCTAGB_BAD_ARG, "bad frame arguments"};
-    set_views(w, h);
+    set_views(w, h, params_.numberOfProcessedMultiresLayers);
     CCTAGB_CUDA(cudaMemcpy2DAsync(lv_.l[0].src, w, gray, pitch, w, h,
                                   is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    const bool fused = (w % 8 == 0) && (h % 8 == 0) && lv_.n == 4;
+    if (timing_) {
+        // Per-stage timing: eager launches queued behind a ~2 ms gate so the
+        // GPU never waits for the host between two stage events.
+        launch_gate(stream_, 2000);
+        CCTAGB_CUDA(cudaEventRecord(ev0_, stream_));
+        launch_image_stage(lv_, vp_, stream_, fused, st_ev_);
+        CCTAGB_CUDA(cudaEventRecord(ev1_, stream_));
+        sync_counters();
+        CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
+        for (int k = 0; k < kStageCount; ++k) CCTAGB_CUDA(cudaEventElapsedTime(&stage_ms_[k], st_ev_[k], st_ev_[k + 1]));
+        return;
+    }
     if (!graph_ || graph_w_ != w || graph_h_ != h) {
         if (graph_) {
             cudaGraphExecDestroy(graph_);
             graph_ = nullptr;
         }
-        const bool fused = (w % 8 == 0) && (h % 8 == 0) && lv_.n == 4;
         cudaGraph_t g = nullptr;
         CCTAGB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         try {
-            launch_image_stage(lv_, vp_, stream_, fused, timing_ ? st_ev_ : nullptr);
+            launch_image_stage(lv_, vp_, stream_, fused, nullptr);
         } catch (...) {
             cudaStreamEndCapture(stream_, &g);
             if (g) cudaGraphDestroy(g);
@@ -176,8 +187,6 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
     CCTAGB_CUDA(cudaEventRecord(ev1_, stream_));
     sync_counters();
     CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
-    if (timing_)
-        for (int k = 0; k < kStageCount; ++k) CCTAGB_CUDA(cudaEventElapsedTime(&stage_ms_[k], st_ev_[k], st_ev_[k + 1]));
 }
 
 void Pipeline::set_stage_timing(bool on)
@@ -186,7 +195,6 @@ void Pipeline::set_stage_timing(bool on)
     if (on && !st_ev_[0])
         for (cudaEvent_t& e : st_ev_) CCTAGB_CUDA(cudaEventCreate(&e));
     timing_ = on;
-    graph_w_ = graph_h_ = -1;  // recapture with or without the event nodes
     std::fill(stage_ms_, stage_ms_ + kStageCount, 0.f);
 }
 
@@ -207,8 +215,7 @@ void Pipeline::sync_counters()
 void Pipeline::canny_only(const int16_t* dx, const int16_t* dy, int w, int h, uint8_t* edges_out)
 {
     if (!dx || !dy || !edges_out || w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "bad arguments"};
-    set_views(w, h);
-    lv_.n = 1;
+    set_views(w, h, 1);
     const size_t px = size_t(w) * h;
     CCTAGB_CUDA(cudaMemcpyAsync(lv_.l[0].dx, dx, px * 2, cudaMemcpyHostToDevice, stream_));
     CCTAGB_CUDA(cudaMemcpyAsync(lv_.l[0].dy, dy, px * 2, cudaMemcpyHostToDevice, stream_));

@@ -49,7 +49,7 @@ public:
 
 private:
     void alloc(int max_w, int max_h);
-    void set_views(int w, int h);
+    void set_views(int w, int h, int nlevels);
     void sync_counters();
 
     cctagb_params params_;

@@ -114,3 +114,18 @@ def test_errors_are_status_codes(built_library):
         assert ei.value.status == cctag_b200.capi.OVERFLOW_EDGES
         # the handle stays usable after an error
         d.image_stage(np.full((120, 160), 5, np.uint8))
+
+
+def test_stage_timing_mode_gives_same_results(detector, orc):
+    img = config_frame("small", seed=5).image
+    detector.set_stage_timing(True)
+    try:
+        detector.image_stage(img)
+        times = detector.stage_times()
+    finally:
+        detector.set_stage_timing(False)
+    assert set(times) >= {"pyramid", "deriv_nms", "vote", "voter_sort"}
+    assert all(v >= 0 for v in times.values()) and sum(times.values()) > 0
+    ref = oracle_frame(orc, img)
+    for lvl in range(4):
+        check_level(detector, lvl, ref[lvl])
