@@ -1,9 +1,14 @@
-// Detection driver: image stage on the GPU, candidate stage on the host,
-// identification on the GPU (Detection.cpp:773-999 of the reference).
+// Detection driver (cctagDetection, Detection.cpp:773-999): image stage on
+// the GPU, candidate stage on the host (one thread per pyramid level), level-0
+// re-fit, cut selection on the host, identification on the GPU, duplicate
+// removal and sort.
 #include "detector.hpp"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <future>
+#include <list>
 
 #include "bank_data.hpp"
 
@@ -14,7 +19,47 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch)
 {
     if (p.nCrowns == 3) {
         for (const auto& row : kThreeCrownsBank) bank_.emplace_back(row, row + 5);
+        upload_bank(bank_);
     }
+    int w = max_w, h = max_h;
+    for (int l = 0; l < p.numberOfProcessedMultiresLayers; ++l) {
+        idxmaps_.emplace_back(size_t(w) * h, -1);
+        w /= 2;
+        h /= 2;
+    }
+    CCTAGB_CUDA(cudaEventCreate(&ev_id0_));
+    CCTAGB_CUDA(cudaEventCreate(&ev_id1_));
+    ensure_ident_capacity(256);
+}
+
+Detector::~Detector()
+{
+    if (d_tasks_) cudaFree(d_tasks_);
+    if (d_res_) cudaFree(d_res_);
+    if (h_tasks_) cudaFreeHost(h_tasks_);
+    if (h_res_) cudaFreeHost(h_res_);
+    if (ev_id0_) cudaEventDestroy(ev_id0_);
+    if (ev_id1_) cudaEventDestroy(ev_id1_);
+}
+
+void Detector::ensure_ident_capacity(int n)
+{
+    if (n <= ident_cap_) return;
+    const int cap = std::max(n, 2 * ident_cap_);
+    if (d_tasks_) cudaFree(d_tasks_);
+    if (d_res_) cudaFree(d_res_);
+    if (h_tasks_) cudaFreeHost(h_tasks_);
+    if (h_res_) cudaFreeHost(h_res_);
+    d_tasks_ = nullptr;
+    d_res_ = nullptr;
+    h_tasks_ = nullptr;
+    h_res_ = nullptr;
+    ident_cap_ = 0;
+    CCTAGB_CUDA(cudaMalloc(&d_tasks_, sizeof(IdentTask) * cap));
+    CCTAGB_CUDA(cudaMalloc(&d_res_, sizeof(IdentResult) * cap));
+    CCTAGB_CUDA(cudaMallocHost(&h_tasks_, sizeof(IdentTask) * cap));
+    CCTAGB_CUDA(cudaMallocHost(&h_res_, sizeof(IdentResult) * cap));
+    ident_cap_ = cap;
 }
 
 void Detector::set_bank(const float* ratios, int n_ids, int n_ratios)
@@ -22,14 +67,92 @@ void Detector::set_bank(const float* ratios, int n_ids, int n_ratios)
     if (!ratios || n_ids < 1 || n_ratios < 1) throw Error{CCTAGB_BANK_ERROR, "empty marker bank"};
     if (n_ratios != 2 * params_.nCrowns - 1)
         throw Error{CCTAGB_BANK_ERROR, "bank rows must hold 2*nCrowns-1 radius ratios"};
+    if (n_ids > kMaxBankIds || n_ratios > kMaxBankRatios) throw Error{CCTAGB_BANK_ERROR, "bank too large"};
     std::vector<std::vector<float>> b(n_ids);
     for (int i = 0; i < n_ids; ++i) {
         b[i].assign(ratios + size_t(i) * n_ratios, ratios + size_t(i + 1) * n_ratios);
         for (float r : b[i])
             if (!(r > 1.f)) throw Error{CCTAGB_BANK_ERROR, "radius ratios must be > 1"};
     }
+    upload_bank(b);
     bank_ = std::move(b);
 }
+
+void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
+{
+    if (n <= 0) return;
+    if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
+    ensure_ident_capacity(n);
+    int W, H;
+    pipe_.level_size(0, &W, &H);
+    std::memcpy(h_tasks_, tasks, sizeof(IdentTask) * n);
+    IdentParams ip{};
+    ip.nSamples = std::min(params_.sampleCutLength, kMaxSamples);
+    ip.beginSig = begin_signal(params_.nCrowns);
+    ip.neighbourSize = params_.imagedCenterNeighbourSize;
+    ip.gridN = params_.imagedCenterNGridSample;
+    ip.minIdentProba = params_.minIdentProba;
+    ip.nIds = int(bank_.size());
+    ip.nRatios = int(bank_[0].size());
+    ip.refineMode = params_.refineMode;
+    ip.gnIterations = params_.gnIterations;
+    cudaStream_t s = pipe_.stream();
+    CCTAGB_CUDA(cudaMemcpyAsync(d_tasks_, h_tasks_, sizeof(IdentTask) * n, cudaMemcpyHostToDevice, s));
+    CCTAGB_CUDA(cudaEventRecord(ev_id0_, s));
+    launch_identify(pipe_.level0_src(), W, H, d_tasks_, d_res_, n, ip, s);
+    CCTAGB_CUDA(cudaEventRecord(ev_id1_, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(h_res_, d_res_, sizeof(IdentResult) * n, cudaMemcpyDeviceToHost, s));
+    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(out, h_res_, sizeof(IdentResult) * n);
+}
+
+namespace {
+
+void fill_ellipse(const geo::Ellipse& e, cctagb_ellipse& o)
+{
+    o.cx = e.cx;
+    o.cy = e.cy;
+    o.a = e.a;
+    o.b = e.b;
+    o.angle = e.angle;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) o.m[r * 3 + c] = e.Q.m[r][c];
+}
+
+// CCTag::isEqual (CCTag.cpp:42-57): circles of radius b/2 around each
+// center; equal when either contains the other's center.
+bool markers_overlap(const MarkerCand& A, const MarkerCand& B)
+{
+    auto small = [](const geo::Ellipse& e) {
+        return geo::Ellipse::from_params(e.cx, e.cy, e.b * 0.5f, e.b * 0.5f, e.angle);
+    };
+    const geo::Ellipse a = small(A.rescaled), b = small(B.rescaled);
+    auto inside = [](const geo::Ellipse& e, float x, float y) {
+        const geo::Mat3& Q = e.Q;
+        const float s1 = geo::qform(Q, x, y);
+        const float q0 = Q.m[0][0] * e.cx + Q.m[0][1] * e.cy + Q.m[0][2];
+        const float q1 = Q.m[1][0] * e.cx + Q.m[1][1] * e.cy + Q.m[1][2];
+        const float q2 = Q.m[2][0] * e.cx + Q.m[2][1] * e.cy + Q.m[2][2];
+        return s1 * (x * q0 + y * q1 + q2) > 0;
+    };
+    return inside(a, b.cx, b.cy) || inside(b, a.cx, a.cy);
+}
+
+// Multiresolution.cpp:172-193 update(): keep the better of two overlapping
+// identified markers.
+void update(std::vector<MarkerCand>& list, const MarkerCand& m)
+{
+    bool flag = false;
+    for (MarkerCand& cur : list) {
+        if (cur.status > 0 && m.status > 0 && markers_overlap(cur, m)) {
+            if (m.quality > cur.quality) cur = m;
+            flag = true;
+        }
+    }
+    if (!flag) list.push_back(m);
+}
+
+}  // namespace
 
 void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_device, int frame_id,
                       cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats)
@@ -37,17 +160,146 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     (void)frame_id;
     if (!n_out || (cap > 0 && !out)) throw Error{CCTAGB_BAD_ARG, "bad output arguments"};
     if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
-    const auto t0 = std::chrono::steady_clock::now();
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     pipe_.image_stage(gray, w, h, pitch, is_device);
-    *n_out = 0;
+    const int nl = pipe_.levels();
+
+    // Candidate stage, one host thread per level (levels are independent until
+    // the level-0 re-fit; each level has its own PCG32 stream, seed 271828).
+    const auto t1 = clk::now();
+    std::vector<HostLevel> hl(nl);
+    std::vector<EdgeSet> es(nl);
+    for (int l = 0; l < nl; ++l) pipe_.download_level(l, hl[l]);
+    std::vector<std::vector<MarkerCand>> per_level(nl);
+    auto run_level = [&](int l) {
+        EdgeSet& e = es[l];
+        const HostLevel& L = hl[l];
+        e.W = L.W;
+        e.H = L.H;
+        e.E = L.E;
+        e.exy = L.exy.data();
+        e.grad = L.grad.data();
+        e.before = L.before.data();
+        e.after = L.after.data();
+        e.voff = L.voff.data();
+        e.vlist = L.vlist.data();
+        e.flow = L.flow.data();
+        e.idxmap = idxmaps_[l].data();
+        for (int i = 0; i < L.E; ++i) e.idxmap[size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = i;
+        e.reset_state();
+        geo::Pcg32 rng(271828);
+        detect_from_edges(e, L.seeds, l, float(1 << l), params_, rng, per_level[l]);
+    };
+    {
+        std::vector<std::future<void>> fut;
+        for (int l = 1; l < nl; ++l) fut.push_back(std::async(std::launch::async, run_level, l));
+        run_level(0);
+        for (auto& f : fut) f.get();
+    }
+    // Coarse levels first, as the reference's loop from the top level down.
+    std::vector<MarkerCand> markers;
+    for (int l = nl - 1; l >= 0; --l)
+        for (auto& m : per_level[l]) markers.push_back(std::move(m));
+    geo::Pcg32 rng0(271828);
+    refit_on_level0(es[0], markers, rng0);
+    for (int l = 0; l < nl; ++l) {
+        const HostLevel& L = hl[l];
+        for (int i = 0; i < L.E; ++i) idxmaps_[l][size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = -1;
+    }
+    const auto t2 = clk::now();
+
+    // Identification.
+    float ms_ident = 0.f;
+    if (params_.doIdentification && !markers.empty()) {
+        const uint8_t* img = gray;
+        size_t stride = pitch;
+        if (is_device) {
+            frame_host_.resize(size_t(w) * h);
+            CCTAGB_CUDA(cudaMemcpy(frame_host_.data(), pipe_.level0_src(), frame_host_.size(), cudaMemcpyDeviceToHost));
+            img = frame_host_.data();
+            stride = size_t(w);
+        } else if (pitch != size_t(w)) {
+            frame_host_.resize(size_t(w) * h);
+            for (int y = 0; y < h; ++y) std::memcpy(&frame_host_[size_t(y) * w], gray + y * pitch, size_t(w));
+            img = frame_host_.data();
+            stride = size_t(w);
+        }
+        (void)stride;
+        std::vector<IdentTask> tasks;
+        std::vector<int> task_of(markers.size(), -1);
+        for (size_t i = 0; i < markers.size(); ++i) {
+            IdentTask t{};
+            const int st = identify_step1(markers[i], img, w, h, params_, t);
+            markers[i].status = st;
+            if (st == CCTAGB_ID_RELIABLE) {
+                task_of[i] = int(tasks.size());
+                tasks.push_back(t);
+            }
+        }
+        std::vector<IdentResult> res(tasks.size());
+        if (!tasks.empty()) {
+            identify(tasks.data(), int(tasks.size()), res.data());
+            CCTAGB_CUDA(cudaEventElapsedTime(&ms_ident, ev_id0_, ev_id1_));
+        }
+        for (size_t i = 0; i < markers.size(); ++i) {
+            if (task_of[i] < 0) continue;
+            const IdentResult& r = res[task_of[i]];
+            MarkerCand& m = markers[i];
+            m.status = r.status;
+            m.cx_img = r.x;
+            m.cy_img = r.y;
+            m.quality = 1.f / r.residual;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) m.H.m[a][b] = r.H[a * 3 + b];
+            if (r.status != CCTAGB_OPTI_HAS_DIVERGED) m.id = r.id;
+            // Ring ellipses from the homography (Identification.cpp:1438-1459):
+            // a singular H makes the marker degenerate.
+            if (r.status != CCTAGB_OPTI_HAS_DIVERGED) {
+                try {
+                    (void)geo::inverse(m.H);
+                } catch (...) {
+                    m.status = CCTAGB_DEGENERATE;
+                }
+            }
+        }
+    }
+    // Duplicate removal twice, then sort by id (Detection.cpp:975-989).
+    std::vector<MarkerCand> prelim, fin;
+    for (const auto& m : markers) update(prelim, m);
+    for (const auto& m : prelim) update(fin, m);
+    std::stable_sort(fin.begin(), fin.end(), [](const MarkerCand& a, const MarkerCand& b) { return a.id < b.id; });
+
+    const int n = int(fin.size());
+    *n_out = n;
+    if (n > cap) throw Error{CCTAGB_BAD_ARG, "marker output capacity too small (" + std::to_string(n) + " markers)"};
+    for (int i = 0; i < n; ++i) {
+        const MarkerCand& m = fin[i];
+        cctagb_marker& o = out[i];
+        std::memset(&o, 0, sizeof(o));
+        o.id = m.id;
+        o.status = m.status;
+        o.x = m.cx_img;
+        o.y = m.cy_img;
+        fill_ellipse(m.rescaled, o.outer);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) o.homography[a * 3 + b] = m.H.m[a][b];
+        o.quality = m.quality;
+        o.pyramidLevel = m.level;
+        o.scale = m.scale;
+    }
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
-        for (int l = 0; l < pipe_.levels(); ++l) {
+        for (int l = 0; l < nl; ++l) {
             stats->edge_points[l] = pipe_.counters(l).E;
             stats->seeds[l] = pipe_.counters(l).S;
         }
+        stats->candidates = int(markers.size());
+        stats->markers = n;
         stats->ms_image_stage = pipe_.last_image_stage_ms();
-        stats->ms_total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        stats->ms_host_candidates = std::chrono::duration<float, std::milli>(t2 - t1).count();
+        stats->ms_identify = ms_ident;
+        stats->ms_total = std::chrono::duration<float, std::milli>(clk::now() - t0).count();
     }
 }
 

@@ -5,6 +5,8 @@
 
 #include <vector>
 
+#include "candidates.hpp"
+#include "ident_host.hpp"
 #include "pipeline.hpp"
 
 namespace cctagb {
@@ -12,6 +14,9 @@ namespace cctagb {
 class Detector {
 public:
     Detector(const cctagb_params& p, int max_w, int max_h, int max_batch);
+    ~Detector();
+    Detector(const Detector&) = delete;
+    Detector& operator=(const Detector&) = delete;
 
     Pipeline& pipeline() { return pipe_; }
     void set_bank(const float* ratios, int n_ids, int n_ratios);
@@ -20,10 +25,24 @@ public:
     void detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_device, int frame_id, cctagb_marker* out,
                 int cap, int* n_out, cctagb_stats* stats);
 
+    // Identification of caller-given markers (ellipse + initial center + cuts)
+    // on the frame last passed to the image stage.
+    void identify(const IdentTask* tasks, int n, IdentResult* out);
+
 private:
+    void ensure_ident_capacity(int n);
+
     cctagb_params params_;
     Pipeline pipe_;
     std::vector<std::vector<float>> bank_;
+    std::vector<std::vector<int32_t>> idxmaps_;  // per level, -1 where no edge point
+    std::vector<uint8_t> frame_host_;
+    IdentTask* d_tasks_ = nullptr;
+    IdentResult* d_res_ = nullptr;
+    IdentTask* h_tasks_ = nullptr;
+    IdentResult* h_res_ = nullptr;
+    int ident_cap_ = 0;
+    cudaEvent_t ev_id0_ = nullptr, ev_id1_ = nullptr;
 };
 
 }  // namespace cctagb

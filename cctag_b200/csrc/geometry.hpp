@@ -238,6 +238,7 @@ inline float dist_point_ellipse(const Mat3& Q, float x, float y)
 // (horizontal) or x = const (vertical).
 inline int intersect_line(const Ellipse& e, float y, bool horizontal, float out[2])
 {
+    out[0] = out[1] = 0.f;
     const Mat3& C = e.Q;
     float a, b, c;
     if (horizontal) {
@@ -358,6 +359,7 @@ struct Pcg32 {
     // Five distinct indices in [0, n) (Statistic.cpp:16-29).
     void rand5(int perm[5], size_t n)
     {
+        for (int i = 0; i < 5; ++i) perm[i] = -1;
         for (int i = 0; i < 5; ++i) {
             int r;
             do {

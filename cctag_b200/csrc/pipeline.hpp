@@ -37,6 +37,7 @@ public:
     void canny_only(const int16_t* dx, const int16_t* dy, int w, int h, uint8_t* edges_out);
 
     int levels() const { return lv_.n; }
+    const uint8_t* level0_src() const { return lv_.l[0].src; }
     void level_size(int l, int* w, int* h) const;
     void copy_planes(int l, uint8_t* src, int16_t* dx, int16_t* dy, uint8_t* edges);
     const LevelCounters& counters(int l) const { return h_cnt_[l]; }
