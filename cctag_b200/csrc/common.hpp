@@ -46,6 +46,7 @@ struct LevelView {
     int nms_tx, nms_tiles;   // 30x30 output tiles
     int thin_tx, thin_tiles; // 32x16 output tiles
     int pix_blocks;          // 256-pixel blocks
+    int uf_tx, uf_tiles;     // 32x32 union-find tiles
 };
 
 struct LevelCounters {

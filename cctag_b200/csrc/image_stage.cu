@@ -243,10 +243,6 @@ __global__ void __launch_bounds__(128) k_deriv_nms(Levels lv, VoteParamsDev vp, 
         const size_t p = size_t(y) * W + x;
         const uint8_t cls = is_max ? (m > vp.high ? 2 : 1) : 0;
         L.map[p] = cls;
-        if (cls) {
-            L.label[p] = int32_t(p);
-            L.sroot[p] = 0;
-        }
         if (write_derivs) {
             L.dx[p] = s_dx[r][c];
             L.dy[p] = s_dy[r][c];
@@ -286,21 +282,98 @@ __device__ __forceinline__ void uf_union(int32_t* L, int a, int b, int32_t* err)
     atomicOr(err, kErrUnionFind);
 }
 
-__global__ void k_hyst_merge(Levels lv)
+// Components inside one 32x32 tile, with a shared-memory union-find over
+// tile-local indices.  Tile-local row-major order is the global order
+// restricted to the tile, so the parent <= self invariant carries over when
+// the local roots are written back as global indices.
+constexpr int kUfT = 32;
+
+__device__ __forceinline__ int uf_find_s(const int* L, int p)
 {
-    int blk;
-    const int l = level_of_block(lv, blockIdx.x, &LevelView::pix_blocks, blk);
+    int q = *(volatile const int*)&L[p];
+    int guard = 0;
+    while (q != p && guard++ < kUfT * kUfT) {
+        p = q;
+        q = *(volatile const int*)&L[p];
+    }
+    return p;
+}
+
+__device__ __forceinline__ void uf_union_s(int* L, int a, int b)
+{
+    for (int it = 0; it < kUfT * kUfT; ++it) {
+        a = uf_find_s(L, a);
+        b = uf_find_s(L, b);
+        if (a == b) return;
+        if (a > b) { const int tmp = a; a = b; b = tmp; }
+        const int old = atomicMin(&L[b], a);
+        if (old == b) return;
+        b = old;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_hyst_local(Levels lv)
+{
+    __shared__ int s_lab[kUfT * kUfT];
+    __shared__ uint8_t s_cls[kUfT * kUfT];
+    int tile;
+    const int l = level_of_block(lv, blockIdx.x, &LevelView::uf_tiles, tile);
     const LevelView& L = lv.l[l];
-    const int p = blk * blockDim.x + threadIdx.x;
-    if (p >= L.W * L.H) return;
+    const int x0 = (tile % L.uf_tx) * kUfT, y0 = (tile / L.uf_tx) * kUfT;
+    for (int i = threadIdx.x; i < kUfT * kUfT; i += 256) {
+        const int lx = i % kUfT, ly = i / kUfT, x = x0 + lx, y = y0 + ly;
+        const uint8_t c = (x < L.W && y < L.H) ? L.map[size_t(y) * L.W + x] : 0;
+        s_cls[i] = c;
+        s_lab[i] = c ? i : -1;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kUfT * kUfT; i += 256) {
+        if (!s_cls[i]) continue;
+        const int lx = i % kUfT, ly = i / kUfT;
+        if (lx > 0 && s_cls[i - 1]) uf_union_s(s_lab, i, i - 1);
+        if (ly > 0) {
+            const int u = i - kUfT;
+            if (lx > 0 && s_cls[u - 1]) uf_union_s(s_lab, i, u - 1);
+            if (s_cls[u]) uf_union_s(s_lab, i, u);
+            if (lx + 1 < kUfT && s_cls[u + 1]) uf_union_s(s_lab, i, u + 1);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kUfT * kUfT; i += 256) {
+        if (!s_cls[i]) continue;
+        const int r = uf_find_s(s_lab, i);
+        const int x = x0 + i % kUfT, y = y0 + i / kUfT;
+        const size_t p = size_t(y) * L.W + x;
+        L.label[p] = (y0 + r / kUfT) * L.W + (x0 + r % kUfT);
+        L.sroot[p] = 0;
+    }
+}
+
+// 8-connections that cross a tile border: the first row and column of a tile
+// look up/left, the last column looks up-right.  96 threads per tile.
+__global__ void __launch_bounds__(96) k_hyst_border(Levels lv)
+{
+    int tile;
+    const int l = level_of_block(lv, blockIdx.x, &LevelView::uf_tiles, tile);
+    const LevelView& L = lv.l[l];
+    const int x0 = (tile % L.uf_tx) * kUfT, y0 = (tile / L.uf_tx) * kUfT;
+    const int t = threadIdx.x;
+    int x, y;
+    if (t < 32) { x = x0 + t; y = y0; }                 // first row
+    else if (t < 64) { x = x0; y = y0 + (t - 32); }     // first column
+    else { x = x0 + kUfT - 1; y = y0 + (t - 64); }      // last column
+    if (x >= L.W || y >= L.H) return;
+    const int W = L.W;
+    const int p = y * W + x;
     if (!L.map[p]) return;
-    const int x = p % L.W, y = p / L.W;
-    if (x > 0 && L.map[p - 1]) uf_union(L.label, p, p - 1, &lv.cnt[l].err);
+    int32_t* err = &lv.cnt[l].err;
+    const bool firstRow = (y == y0), firstCol = (x == x0), lastCol = (x == x0 + kUfT - 1);
+    if (firstCol && x > 0 && L.map[p - 1]) uf_union(L.label, p, p - 1, err);
     if (y > 0) {
-        const int u = p - L.W;
-        if (x > 0 && L.map[u - 1]) uf_union(L.label, p, u - 1, &lv.cnt[l].err);
-        if (L.map[u]) uf_union(L.label, p, u, &lv.cnt[l].err);
-        if (x + 1 < L.W && L.map[u + 1]) uf_union(L.label, p, u + 1, &lv.cnt[l].err);
+        const int u = p - W;
+        if (x > 0 && (firstRow || firstCol) && L.map[u - 1]) uf_union(L.label, p, u - 1, err);
+        if (firstRow && L.map[u]) uf_union(L.label, p, u, err);
+        if (x + 1 < W && (firstRow || lastCol) && L.map[u + 1]) uf_union(L.label, p, u + 1, err);
     }
 }
 
@@ -884,7 +957,8 @@ static void launch_edges(const Levels& lv, const VoteParamsDev& vp, cudaStream_t
     k_deriv_nms<<<total_of(lv, &LevelView::nms_tiles), 128, 0, s>>>(lv, vp, write_derivs);
     mark(ev, kStDerivNms + 1, s);
     const int pb = total_of(lv, &LevelView::pix_blocks);
-    k_hyst_merge<<<pb, 256, 0, s>>>(lv);
+    k_hyst_local<<<total_of(lv, &LevelView::uf_tiles), 256, 0, s>>>(lv);
+    k_hyst_border<<<total_of(lv, &LevelView::uf_tiles), 96, 0, s>>>(lv);
     mark(ev, kStHystMerge + 1, s);
     k_hyst_compress_mark<<<pb, 256, 0, s>>>(lv);
     mark(ev, kStHystCompress + 1, s);

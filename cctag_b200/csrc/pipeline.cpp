@@ -136,6 +136,8 @@ void Pipeline::set_views(int w, int h, int nl)
         v.thin_tx = (w + 31) / 32;
         v.thin_tiles = v.thin_tx * ((h + 15) / 16);
         v.pix_blocks = int((size_t(w) * h + 255) / 256);
+        v.uf_tx = (w + 31) / 32;
+        v.uf_tiles = v.uf_tx * ((h + 31) / 32);
         lv_.l[l] = v;
         w /= 2;
         h /= 2;

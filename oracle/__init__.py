@@ -140,3 +140,23 @@ def vote(edges, dx, dy, distSearch=30, thrGradient=2500, angleVoting=0.0, ratioV
                 chosen=chosen[:E].copy(), total=total[:E].copy(), nvotes=nvotes[:E].copy(),
                 is_max=is_max[:E].copy(), flow=flow[:E].copy(), voff=voff[:E + 1].copy(),
                 vlist=vlist[:voff[E]].copy(), seeds_push=spush[:S].copy(), seeds=ssorted[:S].copy())
+
+
+class Marker(C.Structure):
+    _fields_ = [("id", _I), ("status", _I), ("x", _F), ("y", _F), ("cx", _F), ("cy", _F), ("a", _F), ("b", _F),
+                ("angle", _F), ("quality", _F), ("level", _I)]
+
+
+def detect(gray: np.ndarray, params=None, fp64: bool = False, cap: int = 512):
+    """Whole CPU detection (oracle image stage + candidate stage + oracle
+    identification); returns a list of Marker records."""
+    from cctag_b200 import capi
+
+    lib = load()
+    lib.orc_detect.argtypes = [_P, _I, _I, C.POINTER(capi.Params), _I, _P, _I]
+    lib.orc_detect.restype = _I
+    p = params if params is not None else capi.default_params(3)
+    g = np.ascontiguousarray(gray, dtype=np.uint8)
+    out = (Marker * cap)()
+    n = lib.orc_detect(_p(g), g.shape[1], g.shape[0], C.byref(p), int(bool(fp64)), C.cast(out, C.c_void_p), cap)
+    return [out[i] for i in range(min(n, cap))]

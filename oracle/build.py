@@ -17,8 +17,12 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
-SOURCES = sorted(HERE.glob("*.cpp"))
-HEADERS = sorted(HERE.glob("*.h"))
+# The host candidate stage is shared with the product library (it is host
+# code in both); its sources are compiled in from the package.
+PKG_CSRC = HERE.parent / "cctag_b200" / "csrc"
+SOURCES = sorted(HERE.glob("*.cpp")) + [PKG_CSRC / "candidates.cpp", PKG_CSRC / "geometry.cpp"]
+HEADERS = sorted(HERE.glob("*.h")) + sorted(HERE.glob("*.hpp")) + sorted(PKG_CSRC.glob("*.hpp"))
+INCLUDE = HERE.parent / "include"
 FLAGS = ["-O3", "-std=c++17", "-fPIC", "-shared", "-mavx2", "-mfma", "-ffp-contract=off", "-Wall", "-pthread"]
 
 
@@ -27,7 +31,7 @@ def build_oracle(force: bool = False, verbose: bool = False) -> Path:
     if LIB.exists() and not force and LIB.stat().st_mtime >= newest:
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = ["g++", *FLAGS, "-o", str(tmp), *map(str, SOURCES)]
+    cmd = ["g++", *FLAGS, "-I", str(INCLUDE), "-I", "/usr/local/cuda/include", "-o", str(tmp), *map(str, SOURCES)]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -4,6 +4,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "cctag_b200.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -29,6 +31,18 @@ int orc_vote(const uint8_t* edges, const int16_t* dx, const int16_t* dy, int W, 
              int32_t* seeds_push, int32_t* seeds_sorted, int32_t* n_seeds);
 void orc_level(const uint8_t* src, int W, int H, float thrLow, float thrHigh, int16_t* dx, int16_t* dy,
                uint8_t* edges);
+
+typedef struct {
+    int id, status;
+    float x, y;                  /* imaged center */
+    float cx, cy, a, b, angle;   /* outer ellipse, level-0 pixels */
+    float quality;
+    int level;
+} orc_marker;
+
+/* Whole detection on the CPU; fp64 != 0 runs the center refinement in FP64.
+ * Returns the number of markers (all written when <= cap). */
+int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params* p, int fp64, orc_marker* out, int cap);
 
 #ifdef __cplusplus
 }

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "oracle.h"
+#include "oracle_internal.hpp"
 
 namespace orc {
 
@@ -353,15 +354,6 @@ int gradient_walk(const int32_t* idxmap, int W, int H, int px, int py, int gdx, 
     }
     return -1;
 }
-
-struct VoteParams {
-    int distSearch;
-    int thrGradientMagInVote;
-    float angleVoting;
-    float ratioVoting;
-    int nCrowns;
-    int minVotesToSelectCandidate;
-};
 
 // Vote.cpp:58-247.  `seeds_push` receives the seeds in the order the reference
 // appends them (the voter that brings a point to minVotes); `seeds_sorted`

@@ -51,3 +51,20 @@ def test_status_strings_and_null_handles(built_library):
     n = C.c_int()
     assert lib.cctagb_detect(None, None, 1, 1, 1, 0, None, 0, C.byref(n), None) == capi.BAD_ARG
     assert lib.cctagb_create(None, 64, 64, 1, None) == capi.BAD_ARG
+
+
+def build_shim_example(built_library, tmp_path):
+    import subprocess
+
+    exe = tmp_path / "shim_example"
+    cmd = ["g++", "-std=c++17", "-O2", "-I", str(ROOT / "include"), str(ROOT / "tests" / "cpp" / "shim_example.cpp"),
+           "-o", str(exe), str(built_library), f"-Wl,-rpath,{built_library.parent}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_cpp_shim_compiles_and_links(built_library, tmp_path):
+    """The header-only ICCTag.hpp shim compiles against the C ABI with no
+    OpenCV/Boost/Eigen, using cv::Mat / ptr_list look-alike types."""
+    assert build_shim_example(built_library, tmp_path).exists()
