@@ -2,18 +2,19 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config NAME]
 
-One step = one 1920x1080 synthetic frame (12 markers, noise, motion blur,
-illumination gradient; seeded) through ``cctagb_detect``.  N > 1 runs one
-independent replica per GPU (frames are independent units: no collective on
-the data path); the reported value is frames/s over all ranks, timed as the
+One step = one synthetic 1920x1080 frame (12 markers, noise, motion blur,
+illumination gradient; seeded) through the whole detection: pyramid,
+derivatives, Canny, thinning, edge points, vote and seeds on the GPU, the
+candidate stage on the host, cut selection on the host, identification on the
+GPU.  N > 1 runs one independent replica per GPU on its own frames (no
+collective on the data path); `value` is frames/s over all ranks, timed as the
 max over ranks.
 
-``value``: frames/s with the frame already in device memory
-(``cctagb_detect_device``).  ``e2e``: frames/s through ``cctagb_detect`` with
-the frame in pinned host memory (host->device copy and the result download
-inside the timed region).  Between timed steps the L2 is flushed by writing a
-256 MiB buffer (untimed); each step is bracketed by CUDA events on the
-library's stream.
+`value`: frames/s with the frame already in device memory (cctagb_detect_device).
+`e2e`: frames/s through cctagb_detect with the frame in pinned host memory
+(host->device copy and every device->host download inside the timed region).
+Between timed steps the L2 is flushed by writing a 256 MiB buffer (untimed);
+each step is bracketed by CUDA events on the library's stream.
 """
 from __future__ import annotations
 
@@ -39,7 +40,7 @@ N_FRAMES = 4  # distinct seeded frames cycled through the steps
 
 
 # ------------------------------------------------------------------ helpers --
-def dist_setup(n_gpus):
+def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -108,8 +109,15 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in self.rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in self.rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
@@ -124,25 +132,32 @@ def make_frames(config, n=N_FRAMES):
 
 # -------------------------------------------------------- algorithmic bytes --
 def stage_bytes(levels, E, S, V):
-    """Algorithmic bytes per stage for one frame (n = level pixels, E = edge
-    points, S = seeds, V = votes cast)."""
+    """Algorithmic bytes per image-stage kernel group for one frame (n = level
+    pixels, E = edge points, S = seeds, V = votes cast)."""
     n = [w * h for (w, h) in levels]
     nt = sum(n)
     Et, St, Vt = sum(E), sum(S), sum(V)
     return {
         "pyramid": n[0] + sum(n[1:]),                 # read level 0, write levels 1..3
         "deriv_nms": 6 * nt,                          # 1 B in, dx+dy 4 B + class map 1 B out
-        "hyst_merge": 1 * nt,                         # class map in (parents are its output)
+        "hyst_merge": 1 * nt,                         # class map in (labels are its own output)
         "hyst_compress": 1 * nt,                      # class map in
         "final_thin": 1 * nt + nt // 8,               # hysteresis result in, edge bitmap out
         "row_scan": 8 * sum(h for (_, h) in levels),
-        "emit": nt // 8 + 8 * Et + 4 * Et + 4 * Et,   # bitmap in, dx/dy gathers, points + index map out
+        "emit": nt // 8 + 4 * Et + 4 * Et + 4 * Et,   # bitmap in, dx/dy gathers, points + index map out
         "walk": 8 * Et + 8 * Et + nt // 8,            # points + gradients in, links out, bitmap once
         "vote": 8 * Et + 8 * Et,                      # links in, chosen + length out
         "voter_scan": 4 * Et + 4 * Et,
         "voter_fill": 4 * Et + 4 * Vt,
         "voter_sort": 8 * Vt + 4 * Et + 8 * St,
     }
+
+
+def ident_flops(n_markers, rounds=10, trials=25, cuts=22, samples=100):
+    """FP32 operations of the grid refinement (per candidate and round: 25
+    trials x 22 cuts x 100 samples of homography + bilinear ~ 30 flop, plus the
+    cost accumulation ~ 3 flop per sample)."""
+    return n_markers * rounds * trials * cuts * samples * 33
 
 
 # ------------------------------------------------------------ the b200 arm --
@@ -160,6 +175,7 @@ def run_b200(args, rank, world, local):
     d_frames = [torch.from_numpy(f).to(f"cuda:{local}") for f in frames]
     h_frames = [torch.from_numpy(f).pin_memory() for f in frames]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    out = (capi.Marker * 512)()
 
     def step_device(i):
         t = d_frames[i % len(d_frames)]
@@ -167,16 +183,16 @@ def run_b200(args, rank, world, local):
 
     def step_host(i):
         t = h_frames[i % len(h_frames)]
-        out = (capi.Marker * 256)()
         n = C.c_int()
         st = capi.Stats()
-        det._check(det._lib.cctagb_detect(det._h, C.c_void_p(t.data_ptr()), W, H, W, i, out, 256, C.byref(n),
+        det._check(det._lib.cctagb_detect(det._h, C.c_void_p(t.data_ptr()), W, H, W, i, out, 512, C.byref(n),
                                           C.byref(st)), "detect")
         return [out[k] for k in range(n.value)], st
 
     def timed(step_fn, steps):
         total = 0.0
         last = None
+        per = []
         for i in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -186,8 +202,10 @@ def run_b200(args, rank, world, local):
             last = step_fn(i)
             e1.record(stream)
             e1.synchronize()
-            total += e0.elapsed_time(e1)
-        return total, last
+            ms = e0.elapsed_time(e1)
+            per.append(ms)
+            total += ms
+        return total, last, per
 
     for i in range(args.warmup):
         step_device(i)
@@ -195,24 +213,28 @@ def run_b200(args, rank, world, local):
     torch.cuda.synchronize()
     barrier(world)
     with ClockSampler(local) as clk:
-        ms_dev, (markers, stats) = timed(step_device, args.steps)
+        ms_dev, (markers, stats), per_dev = timed(step_device, args.steps)
         torch.cuda.synchronize()
         barrier(world)
-        ms_e2e, (_, stats_h) = timed(step_host, args.steps)
+        ms_e2e, (_, stats_h), _ = timed(step_host, args.steps)
     torch.cuda.synchronize()
     barrier(world)
     ms_dev = max_over_ranks(ms_dev, world)
     ms_e2e = max_over_ranks(ms_e2e, world)
 
-    # Per-stage device times (events captured between the stages), separate pass.
+    # Per-stage device times (events between the image-stage kernels) and the
+    # identification kernel, separate pass (not part of the timed region).
     det.set_stage_timing(True)
     acc = {}
-    for i in range(max(3, args.steps)):
+    id_ms, host_ms = [], []
+    for i in range(max(3, min(args.steps, 20))):
         flush.zero_()
         torch.cuda.synchronize()
-        step_device(i)
+        _, st = step_device(i)
         for k, v in det.stage_times().items():
             acc.setdefault(k, []).append(v)
+        id_ms.append(st.ms_identify)
+        host_ms.append(st.ms_host_candidates)
     det.set_stage_timing(False)
     stage_ms = {k: statistics.median(v) for k, v in acc.items()}
 
@@ -225,8 +247,16 @@ def run_b200(args, rank, world, local):
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     stages = {k: {"ms": round(stage_ms[k], 5), "bytes": sb[k],
-                  "GB_s": round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) if stage_ms[k] > 0 else None}
+                  "GB_s": round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) if stage_ms[k] > 0 else None,
+                  "frac_of_measured_hbm": round(sb[k] / (stage_ms[k] * 1e-3) / 1e9 / peak, 4) if stage_ms[k] > 0
+                  else None}
               for k in sb}
+    n_ident = sum(1 for m in markers if m.status in (1, -4))
+    idm = statistics.median(id_ms)
+    stages["identify"] = {"ms": round(idm, 5), "markers": n_ident, "bound": "fp32 SIMT + L2 gathers",
+                          "GFLOP_s": round(ident_flops(n_ident) / (idm * 1e-3) / 1e9, 1) if idm > 0 else None}
+    stages["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++)"}
+    # Roofline object for the dominant HBM-class kernel group of the image stage.
     top = max(stage_ms, key=lambda k: stage_ms[k])
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
@@ -234,39 +264,41 @@ def run_b200(args, rank, world, local):
         traffic = json.loads(tf.read_text()).get(top)
     ach = sb[top] / (stage_ms[top] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": peak_src}
+                "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": peak_src,
+                "note": "achieved = algorithmic bytes / CUDA-event time of the kernel group, frac of measured"}
 
     fps_dev = world * args.steps / (ms_dev * 1e-3)
     fps_e2e = world * args.steps / (ms_e2e * 1e-3)
-    kernels_per_step = 15
+    found = sorted(m.id for m in markers if m.status == 1)
     line = {
         "metric": METRIC, "value": round(fps_dev, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_dev / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16/f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: detection step = image stage (pyramid..seeds)",
+        "config": {"workload": f"{args.config}: full detection per frame (pyramid .. identification, 3 crowns)",
                    "frame": f"{W}x{H}", "levels": levels, "edge_points": E, "seeds": S,
-                   "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}"},
-        "e2e": {"value": round(fps_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": W * H,
-                "d2h_bytes_per_step": 32 * 4},
+                   "markers_reliable": len(found), "candidates": stats.candidates,
+                   "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}",
+                   "p50_ms": round(statistics.median(per_dev), 3),
+                   "p99_ms": round(float(np.percentile(per_dev, 99)), 3)},
+        "e2e": {"value": round(fps_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(stats_h.h2d_bytes),
+                "d2h_bytes_per_step": int(stats_h.d2h_bytes)},
         "stages": stages,
         "roofline": roofline,
-        "gpu_launches": kernels_per_step * args.steps * 2,
+        "gpu_launches": int(stats.kernel_launches + stats_h.kernel_launches) * args.steps,
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(frames[:1], budget_s=args.cpu_budget, threads=1)
+        line["cpu_baseline"] = cpu_baseline(frames[:2], budget_s=args.cpu_budget, threads=1)
     det.close()
     return line
 
 
 # ------------------------------------------------------ CPU (oracle) legs --
 def oracle_frame(img):
-    """Reference CPU image stage + vote (C++ restatement), one frame."""
+    """The reference CPU path (C++ restatement): whole detection of one frame."""
     import oracle
 
-    for src in oracle.pyramid(img, 4):
-        dx, dy, e = oracle.level(src)
-        oracle.vote(e, dx, dy)
+    return oracle.detect(img)
 
 
 def cpu_baseline(frames, budget_s=15.0, threads=1):
@@ -276,20 +308,13 @@ def cpu_baseline(frames, budget_s=15.0, threads=1):
     oracle_frame(frames[0])  # warm
     t0 = time.perf_counter()
     n = 0
-    if threads == 1:
-        while time.perf_counter() - t0 < budget_s or n < 1:
-            oracle_frame(frames[n % len(frames)])
-            n += 1
-    else:
-        from concurrent.futures import ThreadPoolExecutor
-
-        with ThreadPoolExecutor(threads) as ex:
-            while time.perf_counter() - t0 < budget_s or n < threads:
-                list(ex.map(oracle_frame, [frames[(n + k) % len(frames)] for k in range(threads)]))
-                n += threads
+    while time.perf_counter() - t0 < budget_s or n < 1:
+        oracle_frame(frames[n % len(frames)])
+        n += 1
     dt = time.perf_counter() - t0
     return {"value": round(n / dt, 3), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} frames of the same workload in {dt:.1f} s (image stage + vote, C++ restatement)"}
+            "sample": f"{n} frames of the same workload in {dt:.1f} s on 1 core (whole detection: C++ "
+                      f"restatement of the reference CPU path)"}
 
 
 def run_reference(args, rank, world):
@@ -300,15 +325,15 @@ def run_reference(args, rank, world):
     import oracle
 
     oracle.load()
-    for i in range(args.warmup):
-        oracle_frame(frames[i % len(frames)])
     from concurrent.futures import ThreadPoolExecutor
 
-    t0 = time.perf_counter()
     with ThreadPoolExecutor(threads) as ex:
+        for i in range(args.warmup):
+            list(ex.map(oracle_frame, [frames[(i + k) % len(frames)] for k in range(threads)]))
+        t0 = time.perf_counter()
         for s in range(args.steps):
             list(ex.map(oracle_frame, [frames[(s + k) % len(frames)] for k in range(threads)]))
-    dt = time.perf_counter() - t0
+        dt = time.perf_counter() - t0
     fps = args.steps * threads / dt
     H, W = frames[0].shape
     return {
@@ -316,10 +341,11 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16/f32",
         "data": "synthetic",
-        "config": {"workload": f"{args.config}: detection step = image stage (pyramid..seeds)", "frame": f"{W}x{H}"},
+        "config": {"workload": f"{args.config}: full detection per frame (pyramid .. identification, 3 crowns)",
+                   "frame": f"{W}x{H}"},
         "cpu_baseline": {"value": round(fps, 3), "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{threads} frames per step, one per host thread (C++ restatement of the "
-                                   "reference CPU path; the reference cannot be built here)"},
+                                   "reference CPU path; the reference itself cannot be built here)"},
         "e2e": {"value": round(fps, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -342,7 +368,7 @@ def main():
         if line is not None:
             print(json.dumps(line))
         return
-    rank, world, local = dist_setup(args.gpus)
+    rank, world, local = dist_setup()
     line = run_b200(args, rank, world, local)
     if rank == 0:
         print(json.dumps(line))

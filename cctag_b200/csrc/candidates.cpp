@@ -10,7 +10,6 @@
 #include <deque>
 #include <limits>
 #include <stdexcept>
-#include <unordered_set>
 
 namespace cctagb {
 
@@ -23,6 +22,8 @@ void EdgeSet::reset_state()
     processed_aux.assign(E, 0);
     processed.assign(E, 0);
     n_segment_out.assign(E, -1);
+    link_stamp.assign(E, 0);
+    link_token = 0;
 }
 
 namespace {
@@ -31,12 +32,12 @@ constexpr int kEdgeNotFound = -1;
 constexpr int kConvexityLost = -2;
 constexpr float kPi = 3.14159265358979323846f;
 
-inline uint32_t packxy(int x, int y) { return (uint32_t(x) << 16) | (uint32_t(y) & 0xFFFF); }
-
 // Vote.cpp:272-394 edgeLinkingDir: follow the edge contour from p while the
 // gradient direction keeps turning one way (convexity).
-void edge_linking_dir(EdgeSet& es, std::unordered_set<uint32_t>& processed, int p, int dir, std::deque<int>& seg,
-                      size_t window, float averageVoteMin)
+// The reference keeps the visited positions of one edgeLinking call in a set
+// of packed (x, y); every such position is an edge point, so a per-point stamp
+// equal to the call's token is the same set.
+void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t window, float averageVoteMin)
 {
     std::deque<float> phi;
     size_t i = 0;
@@ -61,7 +62,7 @@ void edge_linking_dir(EdgeSet& es, std::unordered_set<uint32_t>& processed, int 
                 const int sx = es.x(p) + xoff[k];
                 const int sy = es.y(p) + yoff[k];
                 if (sx >= 0 && sx < es.W && sy >= 0 && sy < es.H && es.at(sx, sy) >= 0 &&
-                    !processed.count(packxy(sx, sy))) {
+                    es.link_stamp[es.at(sx, sy)] != es.link_token) {
                     const float d = phi.back() - phi.front();
                     if (phi.size() == window) {
                         if (float(dir) * std::sin(d) < 0.0f) stop = kConvexityLost;
@@ -71,14 +72,14 @@ void edge_linking_dir(EdgeSet& es, std::unordered_set<uint32_t>& processed, int 
                         if ((s < -0.707f && c > 0.f) || (s < 0.f && c < 0.f)) stop = kConvexityLost;
                     }
                     if (stop == 0) {
-                        processed.insert(packxy(es.x(p), es.y(p)));
+                        es.link_stamp[p] = es.link_token;
                         p = es.at(sx, sy);
                         if (dir > 0) seg.push_back(p);
                         else seg.push_front(p);
                         averageVote = (averageVote * float(seg.size()) + float(es.voters(p))) / (float(seg.size()) + 1.f);
                         stop = 1;
                     }
-                    processed.insert(packxy(es.x(p), es.y(p)));
+                    es.link_stamp[p] = es.link_token;
                 }
             }
             ++j;
@@ -103,12 +104,15 @@ void edge_linking_dir(EdgeSet& es, std::unordered_set<uint32_t>& processed, int 
 // Vote.cpp:255-270
 void edge_linking(EdgeSet& es, std::deque<int>& seg, int pmax, size_t window, float averageVoteMin)
 {
-    std::unordered_set<uint32_t> processed;
+    if (++es.link_token == 0) {  // wrapped: clear the stamps
+        std::fill(es.link_stamp.begin(), es.link_stamp.end(), 0u);
+        es.link_token = 1;
+    }
     seg.push_back(pmax);
     es.processed_in[pmax] = 1;
-    processed.insert(packxy(es.x(pmax), es.y(pmax)));
-    edge_linking_dir(es, processed, pmax, 1, seg, window, averageVoteMin);
-    edge_linking_dir(es, processed, pmax, -1, seg, window, averageVoteMin);
+    es.link_stamp[pmax] = es.link_token;
+    edge_linking_dir(es, pmax, 1, seg, window, averageVoteMin);
+    edge_linking_dir(es, pmax, -1, seg, window, averageVoteMin);
 }
 
 // Vote.cpp:396-412: voters of the segment's points that received at least

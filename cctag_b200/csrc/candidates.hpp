@@ -28,6 +28,8 @@ struct EdgeSet {
     std::vector<uint8_t> processed_in, processed_aux;
     std::vector<uint64_t> processed;  // per-candidate bit masks (ellipse growing)
     std::vector<int32_t> n_segment_out;
+    std::vector<uint32_t> link_stamp;  // edge linking: point visited in call `link_token`
+    uint32_t link_token = 0;
 
     int x(int i) const { return exy[i] & 0xffff; }
     int y(int i) const { return exy[i] >> 16; }

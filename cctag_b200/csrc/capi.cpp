@@ -180,8 +180,8 @@ cctagb_status cctagb_level_links(cctagb_handle* h, int level, int cap, int32_t* 
         cctagb::HostLevel hl;
         h->det->pipeline().download_level(level, hl);
         if (hl.E > cap) throw cctagb::Error{CCTAGB_BAD_ARG, "output capacity too small"};
-        if (before) std::copy(hl.before.begin(), hl.before.end(), before);
-        if (after) std::copy(hl.after.begin(), hl.after.end(), after);
+        if (before) std::copy(hl.before, hl.before + hl.E, before);
+        if (after) std::copy(hl.after, hl.after + hl.E, after);
     });
 }
 
@@ -204,8 +204,8 @@ cctagb_status cctagb_level_votes(cctagb_handle* h, int level, int cap, int32_t* 
             if (nvotes) nvotes[c] = hl.voff[c + 1] - hl.voff[c];
             if (flow_length) flow_length[c] = hl.flow[c];
         }
-        if (voter_off) std::copy(hl.voff.begin(), hl.voff.end(), voter_off);
-        if (voter_list) std::copy(hl.vlist.begin(), hl.vlist.end(), voter_list);
+        if (voter_off) std::copy(hl.voff, hl.voff + hl.E + 1, voter_off);
+        if (voter_list) std::copy(hl.vlist, hl.vlist + hl.V, voter_list);
     });
 }
 

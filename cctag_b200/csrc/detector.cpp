@@ -30,6 +30,10 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch)
     CCTAGB_CUDA(cudaEventCreate(&ev_id0_));
     CCTAGB_CUDA(cudaEventCreate(&ev_id1_));
     ensure_ident_capacity(256);
+    hl_.resize(idxmaps_.size());
+    es_.resize(idxmaps_.size());
+    const unsigned hc = std::thread::hardware_concurrency();
+    pool_.reset(new ThreadPool(int(std::min(7u, hc > 1 ? hc - 1 : 0u))));
 }
 
 Detector::~Detector()
@@ -104,6 +108,7 @@ void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
     CCTAGB_CUDA(cudaMemcpyAsync(h_res_, d_res_, sizeof(IdentResult) * n, cudaMemcpyDeviceToHost, s));
     CCTAGB_CUDA(cudaStreamSynchronize(s));
     std::memcpy(out, h_res_, sizeof(IdentResult) * n);
+    pipe_.add_io((long long)sizeof(IdentTask) * n, (long long)sizeof(IdentResult) * n, 1);
 }
 
 namespace {
@@ -168,9 +173,9 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     // Candidate stage, one host thread per level (levels are independent until
     // the level-0 re-fit; each level has its own PCG32 stream, seed 271828).
     const auto t1 = clk::now();
-    std::vector<HostLevel> hl(nl);
-    std::vector<EdgeSet> es(nl);
-    for (int l = 0; l < nl; ++l) pipe_.download_level(l, hl[l]);
+    std::vector<HostLevel>& hl = hl_;
+    std::vector<EdgeSet>& es = es_;
+    pipe_.download_levels(hl);
     std::vector<std::vector<MarkerCand>> per_level(nl);
     auto run_level = [&](int l) {
         EdgeSet& e = es[l];
@@ -178,25 +183,20 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         e.W = L.W;
         e.H = L.H;
         e.E = L.E;
-        e.exy = L.exy.data();
-        e.grad = L.grad.data();
-        e.before = L.before.data();
-        e.after = L.after.data();
-        e.voff = L.voff.data();
-        e.vlist = L.vlist.data();
-        e.flow = L.flow.data();
+        e.exy = L.exy;
+        e.grad = L.grad;
+        e.before = L.before;
+        e.after = L.after;
+        e.voff = L.voff;
+        e.vlist = L.vlist;
+        e.flow = L.flow;
         e.idxmap = idxmaps_[l].data();
         for (int i = 0; i < L.E; ++i) e.idxmap[size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = i;
         e.reset_state();
         geo::Pcg32 rng(271828);
         detect_from_edges(e, L.seeds, l, float(1 << l), params_, rng, per_level[l]);
     };
-    {
-        std::vector<std::future<void>> fut;
-        for (int l = 1; l < nl; ++l) fut.push_back(std::async(std::launch::async, run_level, l));
-        run_level(0);
-        for (auto& f : fut) f.get();
-    }
+    pool_->parallel_for(nl, run_level);
     // Coarse levels first, as the reference's loop from the top level down.
     std::vector<MarkerCand> markers;
     for (int l = nl - 1; l >= 0; --l)
@@ -217,6 +217,7 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         if (is_device) {
             frame_host_.resize(size_t(w) * h);
             CCTAGB_CUDA(cudaMemcpy(frame_host_.data(), pipe_.level0_src(), frame_host_.size(), cudaMemcpyDeviceToHost));
+            pipe_.add_io(0, (long long)frame_host_.size(), 0);
             img = frame_host_.data();
             stride = size_t(w);
         } else if (pitch != size_t(w)) {
@@ -226,15 +227,17 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
             stride = size_t(w);
         }
         (void)stride;
+        std::vector<IdentTask> all(markers.size());
+        pool_->parallel_for(int(markers.size()), [&](int i) {
+            all[i] = IdentTask{};
+            markers[i].status = identify_step1(markers[i], img, w, h, params_, all[i]);
+        });
         std::vector<IdentTask> tasks;
         std::vector<int> task_of(markers.size(), -1);
         for (size_t i = 0; i < markers.size(); ++i) {
-            IdentTask t{};
-            const int st = identify_step1(markers[i], img, w, h, params_, t);
-            markers[i].status = st;
-            if (st == CCTAGB_ID_RELIABLE) {
+            if (markers[i].status == CCTAGB_ID_RELIABLE) {
                 task_of[i] = int(tasks.size());
-                tasks.push_back(t);
+                tasks.push_back(all[i]);
             }
         }
         std::vector<IdentResult> res(tasks.size());
@@ -300,6 +303,9 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         stats->ms_host_candidates = std::chrono::duration<float, std::milli>(t2 - t1).count();
         stats->ms_identify = ms_ident;
         stats->ms_total = std::chrono::duration<float, std::milli>(clk::now() - t0).count();
+        stats->h2d_bytes = pipe_.h2d_bytes();
+        stats->d2h_bytes = pipe_.d2h_bytes();
+        stats->kernel_launches = pipe_.kernel_launches();
     }
 }
 

@@ -3,9 +3,11 @@
 // Detection.cpp:773-999).
 #pragma once
 
+#include <memory>
 #include <vector>
 
 #include "candidates.hpp"
+#include "thread_pool.hpp"
 #include "ident_host.hpp"
 #include "pipeline.hpp"
 
@@ -36,6 +38,9 @@ private:
     Pipeline pipe_;
     std::vector<std::vector<float>> bank_;
     std::vector<std::vector<int32_t>> idxmaps_;  // per level, -1 where no edge point
+    std::vector<HostLevel> hl_;                  // per level, pinned downloads
+    std::vector<EdgeSet> es_;                    // per level, candidate-stage state
+    std::unique_ptr<ThreadPool> pool_;
     std::vector<uint8_t> frame_host_;
     IdentTask* d_tasks_ = nullptr;
     IdentResult* d_res_ = nullptr;

@@ -58,6 +58,7 @@ Pipeline::~Pipeline()
     for (cudaEvent_t e : st_ev_)
         if (e) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
+    for (void* p : host_allocs_) cudaFreeHost(p);
     if (h_cnt_) cudaFreeHost(h_cnt_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
@@ -108,6 +109,21 @@ void Pipeline::alloc(int max_w, int max_h)
         v.seed_idx = dev_alloc<int32_t>(allocs_, a.seedcap);
         v.seed_key = dev_alloc<int32_t>(allocs_, a.seedcap);
         v.bigq = dev_alloc<int32_t>(allocs_, a.cap);
+        auto pinned = [&](size_t n) {
+            void* q = nullptr;
+            CCTAGB_CUDA(cudaMallocHost(&q, std::max<size_t>(n, 1) * 4));
+            host_allocs_.push_back(q);
+            return q;
+        };
+        a.h_exy = static_cast<int32_t*>(pinned(a.cap));
+        a.h_grad = static_cast<int32_t*>(pinned(a.cap));
+        a.h_before = static_cast<int32_t*>(pinned(a.cap));
+        a.h_after = static_cast<int32_t*>(pinned(a.cap));
+        a.h_voff = static_cast<int32_t*>(pinned(size_t(a.cap) + 1));
+        a.h_vlist = static_cast<int32_t*>(pinned(a.cap));
+        a.h_flow = static_cast<float*>(pinned(a.cap));
+        a.h_sidx = static_cast<int32_t*>(pinned(a.seedcap));
+        a.h_skey = static_cast<int32_t*>(pinned(a.seedcap));
         w /= 2;
         h /= 2;
         if (w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "frame too small for the number of pyramid levels"};
@@ -151,6 +167,10 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
     CCTAGB_CUDA(cudaMemcpy2DAsync(lv_.l[0].src, w, gray, pitch, w, h,
                                   is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
     const bool fused = (w % 8 == 0) && (h % 8 == 0) && lv_.n == 4;
+    h2d_bytes_ = is_device ? 0 : (long long)w * h;
+    d2h_bytes_ = 0;
+    // kernels of one image stage: pyramid (1 fused or one per level), 14 others
+    launches_ = (fused ? 1 : lv_.n - 1) + 14;
     if (timing_) {
         // Per-stage timing: eager launches queued behind a ~2 ms gate so the
         // GPU never waits for the host between two stage events.
@@ -203,6 +223,7 @@ void Pipeline::set_stage_timing(bool on)
 void Pipeline::sync_counters()
 {
     CCTAGB_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(LevelCounters) * kMaxLevels, cudaMemcpyDeviceToHost, stream_));
+    d2h_bytes_ += sizeof(LevelCounters) * kMaxLevels;
     CCTAGB_CUDA(cudaStreamSynchronize(stream_));
     for (int l = 0; l < lv_.n; ++l) {
         const int err = h_cnt_[l].err;
@@ -255,51 +276,74 @@ void Pipeline::copy_planes(int l, uint8_t* src, int16_t* dx, int16_t* dy, uint8_
     }
 }
 
-void Pipeline::download_level(int l, HostLevel& out)
+void Pipeline::issue_level_download(int l)
 {
-    if (l < 0 || l >= lv_.n) throw Error{CCTAGB_BAD_ARG, "level out of range"};
     const LevelView& v = lv_.l[l];
     const LevelCounters& c = h_cnt_[l];
+    LevelAlloc& a = la_[l];
+    const int E = c.E;
+    const int S = std::min(c.S, v.seedcap);
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes) CCTAGB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_));
+    };
+    d2h(a.h_exy, v.exy, size_t(E) * 4);
+    d2h(a.h_grad, v.grad, size_t(E) * 4);
+    d2h(a.h_before, v.before, size_t(E) * 4);
+    d2h(a.h_after, v.after, size_t(E) * 4);
+    d2h(a.h_voff, v.voff, size_t(E + 1) * 4);
+    d2h(a.h_vlist, v.vlist, size_t(c.V) * 4);
+    d2h(a.h_flow, v.flow, size_t(E) * 4);
+    d2h(a.h_sidx, v.seed_idx, size_t(S) * 4);
+    d2h(a.h_skey, v.seed_key, size_t(S) * 4);
+    d2h_bytes_ += (long long)E * 24 + 4 + (long long)c.V * 4 + (long long)S * 8;
+}
+
+void Pipeline::finish_level_download(int l, HostLevel& out)
+{
+    const LevelView& v = lv_.l[l];
+    const LevelCounters& c = h_cnt_[l];
+    const LevelAlloc& a = la_[l];
     out.W = v.W;
     out.H = v.H;
     out.E = c.E;
     out.V = c.V;
-    const int E = c.E;
-    out.exy.resize(E);
-    out.grad.resize(E);
-    out.before.resize(E);
-    out.after.resize(E);
-    out.voff.resize(E + 1);
-    out.vlist.resize(c.V);
-    out.flow.resize(E);
+    out.exy = a.h_exy;
+    out.grad = a.h_grad;
+    out.before = a.h_before;
+    out.after = a.h_after;
+    out.voff = a.h_voff;
+    out.vlist = a.h_vlist;
+    out.flow = a.h_flow;
     const int S = std::min(c.S, v.seedcap);
-    std::vector<int32_t> sidx(S), skey(S);
-    auto d2h = [&](void* dst, const void* src, size_t bytes) {
-        if (bytes) CCTAGB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream_));
-    };
-    d2h(out.exy.data(), v.exy, size_t(E) * 4);
-    d2h(out.grad.data(), v.grad, size_t(E) * 4);
-    d2h(out.before.data(), v.before, size_t(E) * 4);
-    d2h(out.after.data(), v.after, size_t(E) * 4);
-    d2h(out.voff.data(), v.voff, size_t(E + 1) * 4);
-    d2h(out.vlist.data(), v.vlist, size_t(c.V) * 4);
-    d2h(out.flow.data(), v.flow, size_t(E) * 4);
-    d2h(sidx.data(), v.seed_idx, size_t(S) * 4);
-    d2h(skey.data(), v.seed_key, size_t(S) * 4);
-    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
     // Seeds in the order vote() appends them (the voter that brings a point to
     // minVotes, Vote.cpp:236-241), then std::sort by votes received, as
     // Multiresolution.cpp:239-242 does (same comparator, same libstdc++ sort).
     std::vector<std::pair<int32_t, int32_t>> ks(S);
-    for (int i = 0; i < S; ++i) ks[i] = {skey[i], sidx[i]};
+    for (int i = 0; i < S; ++i) ks[i] = {a.h_skey[i], a.h_sidx[i]};
     std::sort(ks.begin(), ks.end());
     out.seeds.resize(S);
     for (int i = 0; i < S; ++i) out.seeds[i] = ks[i].second;
-    const int32_t* voff = out.voff.data();
+    const int32_t* voff = a.h_voff;
     if (S > 1)
-        std::sort(out.seeds.begin(), out.seeds.end(), [voff](int32_t a, int32_t b) {
-            return (voff[a + 1] - voff[a]) > (voff[b + 1] - voff[b]);
+        std::sort(out.seeds.begin(), out.seeds.end(), [voff](int32_t x, int32_t y) {
+            return (voff[x + 1] - voff[x]) > (voff[y + 1] - voff[y]);
         });
+}
+
+void Pipeline::download_level(int l, HostLevel& out)
+{
+    if (l < 0 || l >= lv_.n) throw Error{CCTAGB_BAD_ARG, "level out of range"};
+    issue_level_download(l);
+    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    finish_level_download(l, out);
+}
+
+void Pipeline::download_levels(std::vector<HostLevel>& out)
+{
+    out.resize(lv_.n);
+    for (int l = 0; l < lv_.n; ++l) issue_level_download(l);
+    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    for (int l = 0; l < lv_.n; ++l) finish_level_download(l, out[l]);
 }
 
 }  // namespace cctagb

@@ -13,11 +13,18 @@ namespace cctagb {
 // the reference (EdgePointCollection, Types.hpp:19-158): raster-ordered edge
 // points with gradients, before/after links, CSR voter lists, vote-derived
 // per-point state and the seeds in processing order.
+// The arrays live in pinned host memory owned by the Pipeline and stay valid
+// until the next download of the same level.
 struct HostLevel {
     int W = 0, H = 0;
     int E = 0, V = 0;
-    std::vector<int32_t> exy, grad, before, after, voff, vlist;
-    std::vector<float> flow;
+    const int32_t* exy = nullptr;
+    const int32_t* grad = nullptr;
+    const int32_t* before = nullptr;
+    const int32_t* after = nullptr;
+    const int32_t* voff = nullptr;   // E + 1
+    const int32_t* vlist = nullptr;  // V
+    const float* flow = nullptr;
     std::vector<int32_t> seeds;  // processing order (Multiresolution.cpp:239-242)
 };
 
@@ -43,7 +50,19 @@ public:
     const LevelCounters& counters(int l) const { return h_cnt_[l]; }
     // Downloads one level's edge-point collection (after image_stage).
     void download_level(int l, HostLevel& out);
+    // Downloads every level with one synchronisation.
+    void download_levels(std::vector<HostLevel>& out);
     float last_image_stage_ms() const { return last_ms_; }
+    // Transfers and kernel launches since the last image_stage() began.
+    long long h2d_bytes() const { return h2d_bytes_; }
+    long long d2h_bytes() const { return d2h_bytes_; }
+    int kernel_launches() const { return launches_; }
+    void add_io(long long h2d, long long d2h, int launches)
+    {
+        h2d_bytes_ += h2d;
+        d2h_bytes_ += d2h;
+        launches_ += launches;
+    }
     // Per-stage device times of the last frame (events captured into the graph).
     void set_stage_timing(bool on);
     const float* stage_ms() const { return stage_ms_; }
@@ -63,13 +82,28 @@ private:
         size_t px = 0;  // pixel capacity
         int cap = 0, seedcap = 0;
         LevelView v{};
+        // pinned staging of the downloads
+        int32_t* h_exy = nullptr;
+        int32_t* h_grad = nullptr;
+        int32_t* h_before = nullptr;
+        int32_t* h_after = nullptr;
+        int32_t* h_voff = nullptr;
+        int32_t* h_vlist = nullptr;
+        float* h_flow = nullptr;
+        int32_t* h_sidx = nullptr;
+        int32_t* h_skey = nullptr;
     } la_[kMaxLevels];
+    std::vector<void*> host_allocs_;
+    void issue_level_download(int l);
+    void finish_level_download(int l, HostLevel& out);
     Levels lv_{};
     LevelCounters* d_cnt_ = nullptr;  // + scan partials
     LevelCounters* h_cnt_ = nullptr;  // pinned
     cudaGraphExec_t graph_ = nullptr;
     int graph_w_ = -1, graph_h_ = -1;
     float last_ms_ = 0.f;
+    long long h2d_bytes_ = 0, d2h_bytes_ = 0;
+    int launches_ = 0;
     bool timing_ = false;
     cudaEvent_t st_ev_[kStageCount + 1] = {};
     float stage_ms_[kStageCount] = {};

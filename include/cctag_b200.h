@@ -133,6 +133,9 @@ typedef struct cctagb_stats {
     float ms_host_candidates;  /* host wall time of the candidate stage */
     float ms_identify;         /* device time of identification        */
     float ms_total;            /* host wall time of the whole call     */
+    long long h2d_bytes;       /* host->device bytes copied by the call */
+    long long d2h_bytes;       /* device->host bytes copied by the call */
+    int kernel_launches;       /* kernels launched by the call         */
 } cctagb_stats;
 
 typedef struct cctagb_handle cctagb_handle;

@@ -150,12 +150,16 @@ class Marker(C.Structure):
 def detect(gray: np.ndarray, params=None, fp64: bool = False, cap: int = 512):
     """Whole CPU detection (oracle image stage + candidate stage + oracle
     identification); returns a list of Marker records."""
-    from cctag_b200 import capi
+    from cctag_b200.capi import Params  # the ctypes layout of cctagb_params only
 
     lib = load()
-    lib.orc_detect.argtypes = [_P, _I, _I, C.POINTER(capi.Params), _I, _P, _I]
+    lib.orc_detect.argtypes = [_P, _I, _I, C.POINTER(Params), _I, _P, _I]
     lib.orc_detect.restype = _I
-    p = params if params is not None else capi.default_params(3)
+    lib.orc_params_default.argtypes = [C.POINTER(Params), _I]
+    if params is None:
+        params = Params()
+        lib.orc_params_default(C.byref(params), 3)
+    p = params
     g = np.ascontiguousarray(gray, dtype=np.uint8)
     out = (Marker * cap)()
     n = lib.orc_detect(_p(g), g.shape[1], g.shape[0], C.byref(p), int(bool(fp64)), C.cast(out, C.c_void_p), cap)

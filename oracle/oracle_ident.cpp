@@ -693,3 +693,40 @@ extern "C" int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params
     }
     return int(fin.size());
 }
+
+// Parameters::Parameters(nCrowns) defaults (Params.hpp:27-66, Params.cpp:38-75).
+extern "C" void orc_params_default(cctagb_params* p, int nCrowns)
+{
+    std::memset(p, 0, sizeof(*p));
+    p->cannyThrLow = 0.01f;
+    p->cannyThrHigh = 0.04f;
+    p->distSearch = 30;
+    p->thrGradientMagInVote = 2500;
+    p->angleVoting = 0.f;
+    p->ratioVoting = 4.f;
+    p->averageVoteMin = 0.f;
+    p->thrMedianDistanceEllipse = 3.f;
+    p->maximumNbSeeds = 500;
+    p->maximumNbCandidatesLoopTwo = 40;
+    p->nCrowns = nCrowns;
+    p->nCircles = 2 * nCrowns;
+    p->minPointsSegmentCandidate = 10;
+    p->minVotesToSelectCandidate = 3;
+    p->threshRobustEstimationOfOuterEllipse = 30.f;
+    p->ellipseGrowingEllipticHullWidth = 2.3f;
+    p->windowSizeOnInnerEllipticSegment = 20;
+    p->numberOfMultiresLayers = 4;
+    p->numberOfProcessedMultiresLayers = 4;
+    p->nSamplesOuterEllipse = 150;
+    p->numCutsInIdentStep = 22;
+    p->numSamplesOuterEdgePointsRefinement = 20;
+    p->cutsSelectionTrials = 500;
+    p->sampleCutLength = 100;
+    p->imagedCenterNGridSample = 5;
+    p->imagedCenterNeighbourSize = 0.20f;
+    p->minIdentProba = 1e-6f;
+    p->useLMDif = 1;
+    p->searchForAnotherSegment = 1;
+    p->doIdentification = 1;
+    p->maxEdges = 20000;
+}

@@ -54,3 +54,38 @@ def test_detect_is_deterministic(detector):
     a, _ = detector.detect(fr.image)
     b, _ = detector.detect(fr.image)
     assert [(m.id, m.status, m.x, m.y) for m in a] == [(m.id, m.status, m.x, m.y) for m in b]
+
+
+@pytest.mark.parametrize("name,seed", [("c1_720p", 1), ("c1_720p", 3), ("c2_1080p", 2)])
+def test_detect_matches_oracle(detector, orc, name, seed):
+    """Same markers as the CPU oracle (same image-stage inputs, same candidate
+    stage): IDs and statuses exact; centres within 0.05 px of the oracle's FP64
+    refinement."""
+    fr = config_frame(name, seed=seed)
+    got, _ = detector.detect(fr.image)
+    want = orc.detect(fr.image, fp64=True)
+    assert [(m.id, m.status, m.pyramidLevel) for m in got] == [(m.id, m.status, m.level) for m in want]
+    for g, w in zip(got, want):
+        assert abs(g.outer.cx - w.cx) < 1e-3 and abs(g.outer.a - w.a) < 1e-3
+        if g.status == 1:
+            assert np.hypot(g.x - w.x, g.y - w.y) <= 0.05, (g.x, g.y, w.x, w.y)
+
+
+def test_cpp_shim_example_runs(built_library, tmp_path):
+    """The C++ drop-in example (reference-style cctagDetection) finds the
+    markers of a rendered frame."""
+    import subprocess
+    import sys
+
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).parent))
+    from test_capi import build_shim_example
+
+    fr = config_frame("c1_720p", seed=2)
+    raw = tmp_path / "frame.raw"
+    raw.write_bytes(np.array(fr.image.shape[::-1], np.int32).tobytes() + fr.image.tobytes())
+    exe = build_shim_example(built_library, tmp_path)
+    r = subprocess.run([str(exe), str(raw)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    rows = [l.split() for l in r.stdout.strip().splitlines()]
+    ids = sorted(int(x[0]) for x in rows if int(x[1]) == 1)
+    assert ids == sorted(g.id for g in fr.markers)
