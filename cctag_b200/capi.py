@@ -81,6 +81,7 @@ SIGNATURES = {
     "cctagb_set_stage_timing": (_I, [_P, _I]),
     "cctagb_stage_times": (_I, [_P, _I, _P, C.POINTER(_I)]),
     "cctagb_stage_name": (C.c_char_p, [_I]),
+    "cctagb_edges_noalloc": (_I, [_P, _I, _I, _SZ, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

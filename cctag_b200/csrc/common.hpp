@@ -106,5 +106,7 @@ void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t 
                         cudaEvent_t* ev = nullptr);
 void launch_canny_only(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s);
 void launch_gate(cudaStream_t s, int us);
+void launch_edge_level(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, uint8_t* edges_out,
+                       int32_t* status_out);
 
 }  // namespace cctagb

@@ -1006,4 +1006,36 @@ void launch_canny_only(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s
     CCTAGB_CUDA(cudaGetLastError());
 }
 
+// Edge stage of one level from its gray image (derivatives, NMS, hysteresis,
+// thinning, edge bitmap) without the compaction.  The caller clears
+// lv.cnt[0] and lv.l[0].row_count beforehand.
+__global__ void k_bitmap_to_bytes(Levels lv, uint8_t* out)
+{
+    const LevelView& L = lv.l[0];
+    const size_t n = size_t(L.W) * L.H;
+    for (size_t p = size_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n; p += size_t(gridDim.x) * blockDim.x) {
+        const int x = int(p % L.W), y = int(p / L.W);
+        out[p] = edge_bit(L, x, y) ? 255 : 0;
+    }
+}
+
+__global__ void k_copy_status(const LevelCounters* cnt, int32_t* status)
+{
+    *status = cnt->err;
+}
+
+void launch_edge_level(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, uint8_t* edges_out,
+                       int32_t* status_out)
+{
+    const LevelView& L = lv.l[0];
+    k_deriv_nms<<<L.nms_tiles, 128, 0, s>>>(lv, vp, 1);
+    k_hyst_local<<<L.uf_tiles, 256, 0, s>>>(lv);
+    k_hyst_border<<<L.uf_tiles, 96, 0, s>>>(lv);
+    k_hyst_compress_mark<<<L.pix_blocks, 256, 0, s>>>(lv);
+    k_final_thin<<<L.thin_tiles, dim3(kThX, kThY), 0, s>>>(lv);
+    k_bitmap_to_bytes<<<148 * 4, 256, 0, s>>>(lv, edges_out);
+    if (status_out) k_copy_status<<<1, 1, 0, s>>>(lv.cnt, status_out);
+    CCTAGB_CUDA(cudaGetLastError());
+}
+
 }  // namespace cctagb

@@ -1,0 +1,154 @@
+// Allocation-free edge stage: cctagb_edges_noalloc.
+//
+// Some callers cannot allocate device memory at the time they want edges: an
+// application that hands every byte of the GPU to its own memory pool at start
+// up, a real-time loop whose rules forbid cudaMalloc/cudaFree after
+// initialisation (they can block and synchronise the device), or a caller that
+// has no handle and only owns the frame and output buffers.  This entry point
+// runs the edge stage of one frame (9x9 derivatives, Canny NMS, hysteresis,
+// thinning) with the caller's input and output buffers and keeps its own
+// scratch (class map, union-find labels, strong-component flags, edge bitmap,
+// row counts, counters) in the file-scope device array below.  It calls no
+// cudaMalloc, cudaFree or allocating library routine.
+//
+// Limits and rules:
+//  * at most kNoAllocMaxPixels pixels and kNoAllocMaxSide per side, frame rows
+//    contiguous (pitch == width); larger frames are rejected with
+//    CCTAGB_TOO_LARGE;
+//  * the array (about 6.4 MB) is held by every GPU that loads the library,
+//    until the process exits;
+//  * the first call on a device resolves the array's device address
+//    (cudaGetSymbolAddress) and uploads the filter constants, with that device
+//    current; make that first call before any stream capture;
+//  * all calls share the one array and it keeps the last call's contents:
+//    calls whose GPU work overlaps (different streams, or host threads) race
+//    and give wrong results; serialise them on one stream.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <mutex>
+
+#include "common.hpp"
+
+namespace cctagb {
+
+namespace {
+
+constexpr int kNoAllocMaxPixels = 1 << 20;
+constexpr int kNoAllocMaxSide = 4096;
+constexpr size_t kAlign = 256;
+
+constexpr size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// Layout of the scratch array.
+constexpr size_t kOffCounters = 0;
+constexpr size_t kOffRowCount = align_up(kOffCounters + sizeof(LevelCounters));
+constexpr size_t kOffMap = align_up(kOffRowCount + sizeof(int32_t) * kNoAllocMaxSide);
+constexpr size_t kOffLabel = align_up(kOffMap + size_t(kNoAllocMaxPixels));
+constexpr size_t kOffSroot = align_up(kOffLabel + sizeof(int32_t) * size_t(kNoAllocMaxPixels));
+constexpr size_t kOffBitmap = align_up(kOffSroot + size_t(kNoAllocMaxPixels));
+constexpr size_t kBitmapWords = size_t(kNoAllocMaxPixels) / 32 + kNoAllocMaxSide;
+constexpr size_t kScratchBytes = align_up(kOffBitmap + sizeof(uint32_t) * kBitmapWords);
+
+constexpr int kMaxDevices = 64;
+
+struct DeviceSlot {
+    bool ready = false;
+    uint8_t* base = nullptr;
+};
+
+std::mutex g_mu;
+DeviceSlot g_slots[kMaxDevices];
+
+}  // namespace
+
+static __device__ __align__(256) uint8_t g_edge_scratch[kScratchBytes];
+
+// Resolves the device address of the scratch array on the current device
+// (once per device) and uploads the filter constants there.
+static uint8_t* scratch_for_current_device(cctagb_status& st)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        st = CCTAGB_NO_DEVICE;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    DeviceSlot& s = g_slots[dev];
+    if (!s.ready) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_edge_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            st = CCTAGB_CUDA_ERROR;
+            return nullptr;
+        }
+        try {
+            upload_constants(nullptr, 0, 0);
+        } catch (const Error& err) {
+            st = err.status;
+            return nullptr;
+        }
+        s.base = static_cast<uint8_t*>(p);
+        s.ready = true;
+    }
+    st = CCTAGB_OK;
+    return s.base;
+}
+
+}  // namespace cctagb
+
+extern "C" cctagb_status cctagb_edges_noalloc(const uint8_t* d_gray, int w, int h, size_t pitch, float cannyThrLow,
+                                              float cannyThrHigh, int16_t* d_dx, int16_t* d_dy, uint8_t* d_edges,
+                                              int32_t* d_status, void* stream)
+{
+    using namespace cctagb;
+    if (!d_gray || !d_dx || !d_dy || !d_edges || w < 1 || h < 1 || pitch != size_t(w)) return CCTAGB_BAD_ARG;
+    if (size_t(w) * size_t(h) > size_t(kNoAllocMaxPixels) || w > kNoAllocMaxSide || h > kNoAllocMaxSide)
+        return CCTAGB_TOO_LARGE;
+    cctagb_status st;
+    uint8_t* base = scratch_for_current_device(st);
+    if (!base) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // What must start at zero: the counters (error bits) and the per-row edge
+    // counts the thinning kernel accumulates into.
+    if (cudaMemsetAsync(base + kOffCounters, 0, sizeof(LevelCounters), s) != cudaSuccess ||
+        cudaMemsetAsync(base + kOffRowCount, 0, sizeof(int32_t) * size_t(h), s) != cudaSuccess) {
+        cudaGetLastError();
+        return CCTAGB_CUDA_ERROR;
+    }
+    Levels lv{};
+    lv.n = 1;
+    lv.cnt = reinterpret_cast<LevelCounters*>(base + kOffCounters);
+    LevelView& L = lv.l[0];
+    L.W = w;
+    L.H = h;
+    L.WW = (w + 31) / 32;
+    L.src = const_cast<uint8_t*>(d_gray);
+    L.dx = d_dx;
+    L.dy = d_dy;
+    L.map = base + kOffMap;
+    L.label = reinterpret_cast<int32_t*>(base + kOffLabel);
+    L.sroot = base + kOffSroot;
+    L.bitmap = reinterpret_cast<uint32_t*>(base + kOffBitmap);
+    L.row_count = reinterpret_cast<int32_t*>(base + kOffRowCount);
+    L.nms_tx = (w + 29) / 30;
+    L.nms_tiles = L.nms_tx * ((h + 29) / 30);
+    L.thin_tx = (w + 31) / 32;
+    L.thin_tiles = L.thin_tx * ((h + 15) / 16);
+    L.pix_blocks = int((size_t(w) * h + 255) / 256);
+    L.uf_tx = (w + 31) / 32;
+    L.uf_tiles = L.uf_tx * ((h + 31) / 32);
+    VoteParamsDev vp{};
+    float lo = cannyThrLow * 256.f, hi = cannyThrHigh * 256.f;
+    if (lo > hi) std::swap(lo, hi);
+    vp.low = int(std::floor(lo));
+    vp.high = int(std::floor(hi));
+    try {
+        launch_edge_level(lv, vp, s, d_edges, d_status);
+    } catch (const Error& err) {
+        return err.status;
+    }
+    return CCTAGB_OK;
+}

@@ -192,6 +192,24 @@ const char* cctagb_stage_name(int stage);
 cctagb_status cctagb_canny_from_derivatives(cctagb_handle* h, const int16_t* dx, const int16_t* dy, int w, int hgt,
                                             uint8_t* edges);
 
+/* Edge stage of one frame without any device allocation.  No counterpart in
+ * the reference: it is for callers that cannot allocate device memory when
+ * they need edges (all memory handed to their own pool, or a real-time loop
+ * that forbids cudaMalloc/cudaFree after start-up), and it needs no handle.
+ * d_gray (w*hgt bytes, pitch == w), d_dx, d_dy (w*hgt int16 each) and d_edges
+ * (w*hgt bytes, 0/255) are device buffers owned by the caller; d_status (one
+ * int, may be null) receives 0 or an internal error bit.  Runs asynchronously
+ * on `stream` (a cudaStream_t; null = legacy default stream).  Its scratch is a
+ * fixed device array inside the library (about 6.4 MB on every GPU that loads
+ * it): frames are limited to 1,048,576 pixels and 4096 per side
+ * (CCTAGB_TOO_LARGE beyond).  The first call on a device sets the array up
+ * (resolves its address, uploads filter constants) with that device current:
+ * make it before any stream capture.  Calls share the array: calls whose GPU
+ * work overlaps race; serialise them on one stream. */
+cctagb_status cctagb_edges_noalloc(const uint8_t* d_gray, int w, int hgt, size_t pitch, float cannyThrLow,
+                                   float cannyThrHigh, int16_t* d_dx, int16_t* d_dy, uint8_t* d_edges,
+                                   int32_t* d_status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
