@@ -1,8 +1,12 @@
 // Host candidate stage (see candidates.hpp).  The reference runs its three
 // candidate loops with TBB and shared per-point flags, so its output depends
-// on the thread schedule; here the loops run in index order (the order of the
-// reference's single-threaded CCTAG_SERIALIZE build) and the PCG32 stream is
-// reset for every frame, which makes the result deterministic.
+// on the thread schedule.  Here loop 1 runs per level in seed order (the order
+// of the reference's single-threaded CCTAG_SERIALIZE build); loops 2 and 3 run
+// per candidate on any number of threads, each candidate with its own PCG32
+// stream (seed 271828, stream from level, candidate index and loop), and the
+// only state they share (the segment labels of loop 2) is assigned in
+// candidate order between the two loops.  The result is therefore the same
+// for every thread count and schedule.
 #include "candidates.hpp"
 
 #include <algorithm>
@@ -10,6 +14,7 @@
 #include <deque>
 #include <limits>
 #include <stdexcept>
+#include <unordered_set>
 
 namespace cctagb {
 
@@ -31,6 +36,16 @@ namespace {
 constexpr int kEdgeNotFound = -1;
 constexpr int kConvexityLost = -2;
 constexpr float kPi = 3.14159265358979323846f;
+
+// Per-point candidate masks of the ellipse growing (EdgePoint::_processed, one
+// bit per candidate of the second loop): candidates grow concurrently, each on
+// its own bit, so the word updates are atomic.
+inline void bit_set(EdgeSet& es, int i, uint64_t m) { __atomic_fetch_or(&es.processed[i], m, __ATOMIC_RELAXED); }
+inline void bit_clear(EdgeSet& es, int i, uint64_t m) { __atomic_fetch_and(&es.processed[i], ~m, __ATOMIC_RELAXED); }
+inline bool bit_test(const EdgeSet& es, int i, uint64_t m)
+{
+    return (__atomic_load_n(&es.processed[i], __ATOMIC_RELAXED) & m) != 0;
+}
 
 // Vote.cpp:272-394 edgeLinkingDir: follow the edge contour from p while the
 // gradient direction keeps turning one way (convexity).
@@ -316,11 +331,10 @@ void connected_point(std::vector<int>& pts, uint64_t mask, EdgeSet& es, const El
 {
     static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
     static const int yoff[8] = {0, -1, -1, -1, 0, 1, 1, 1};
-    struct Frame {
-        int x, y, k;
-    };
-    std::vector<Frame> st;
-    es.processed[es.at(x, y)] |= mask;
+    using Frame = EdgeSet::DfsFrame;
+    thread_local std::vector<Frame> st;  // reused across calls of this thread
+    st.clear();
+    bit_set(es, es.at(x, y), mask);
     st.push_back({x, y, 0});
     while (!st.empty()) {
         Frame& f = st.back();
@@ -333,11 +347,11 @@ void connected_point(std::vector<int>& pts, uint64_t mask, EdgeSet& es, const El
         if (sx < 0 || sx >= es.W || sy < 0 || sy >= es.H) continue;
         const int e = es.at(sx, sy);
         if (e < 0) continue;
-        if (!geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e))) || (es.processed[e] & mask)) continue;
+        if (!geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e))) || bit_test(es, e, mask)) continue;
         const float ox = qIn.cx - float(es.x(e)), oy = qIn.cy - float(es.y(e));
         if (es.dx(e) * ox + es.dy(e) * oy < 0) {
             pts.push_back(e);
-            es.processed[e] |= mask;
+            bit_set(es, e, mask);
             st.push_back({sx, sy, 0});
         }
     }
@@ -371,7 +385,7 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
 {
     const uint64_t mask = uint64_t(1) << (runId & 63);
     outer = fc;
-    for (int c : fc) es.processed[c] |= mask;
+    for (int c : fc) bit_set(es, c, mask);
     if (!goodInit) {
         int newSize = int(outer.size());
         int maxNb = newSize, nIterMax = 0, lastSize = 0, nIter = 0;
@@ -394,8 +408,8 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
         outer = sets[nIterMax];
         ellipse = ells[nIterMax];
         for (auto& s : sets)
-            for (int p : s) es.processed[p] &= ~mask;
-        for (int p : outer) es.processed[p] |= mask;
+            for (int p : s) bit_clear(es, p, mask);
+        for (int p : outer) bit_set(es, p, mask);
     }
     ellipse = fit_points(es, outer);
     size_t lastSize = 0;
@@ -419,44 +433,59 @@ struct Candidate {
 
 float quality_of(size_t npts, const Ellipse& e) { return float(npts) / float(geo::rasterize_perimeter(e)); }
 
-// Detection.cpp:115-267 completeFlowComponent
-void complete_flow_component(Candidate& c, EdgeSet& es, std::vector<Candidate>& loop2, size_t& nSegmentOut,
-                             size_t runId, const cctagb_params& p, geo::Pcg32& rng)
+// Detection.cpp:115-267 completeFlowComponent, in three phases so that the
+// per-candidate work can run in parallel: (B) children and LMedS outlier
+// removal, (C) segment labels -- sequential, in candidate order, as the
+// reference assigns them -- and (D) ellipse growing and the final checks.
+// Phase B: returns whether the candidate continues (>= 5 filtered children).
+bool flow_component_filter(Candidate& c, EdgeSet& es, const cctagb_params& p, geo::Pcg32& rng)
 {
     try {
         std::vector<int> children;
         children_of(es, c.segment, children);
-        if (children.size() < size_t(p.minPointsSegmentCandidate)) return;
+        if (children.size() < size_t(p.minPointsSegmentCandidate)) return false;
         c.score = int(children.size());
         float SmFinal = 1e+10f;
         outlier_removal(es, children, c.filtered, SmFinal, p.threshRobustEstimationOfOuterEllipse, kInvGradWeight, 60,
                         rng);
-        if (c.filtered.size() < 5) return;
-        size_t nLabel;
-        {
-            long common = -1;
-            for (int q : c.filtered)
-                if (es.n_segment_out[q] != -1) {
-                    common = es.n_segment_out[q];
-                    break;
-                }
-            nLabel = common == -1 ? nSegmentOut++ : size_t(common);
-            for (int q : c.filtered) es.n_segment_out[q] = int32_t(nLabel);
+        return c.filtered.size() >= 5;
+    } catch (...) {
+        return false;
+    }
+}
+
+// Phase C (Detection.cpp:157-189)
+void flow_component_label(Candidate& c, EdgeSet& es, size_t& nSegmentOut)
+{
+    long common = -1;
+    for (int q : c.filtered)
+        if (es.n_segment_out[q] != -1) {
+            common = es.n_segment_out[q];
+            break;
         }
+    const size_t nLabel = common == -1 ? nSegmentOut++ : size_t(common);
+    for (int q : c.filtered) es.n_segment_out[q] = int32_t(nLabel);
+    c.nLabel = nLabel;
+}
+
+// Phase D: returns whether the candidate enters the second list.
+bool flow_component_grow(Candidate& c, EdgeSet& es, size_t runId, const cctagb_params& p)
+{
+    try {
         const bool goodInit = ellipse_growing_init(es, c.filtered, c.outerEllipse);
         ellipse_growing2(es, c.filtered, c.outer, c.outerEllipse, p.ellipseGrowingEllipticHullWidth, runId, goodInit);
-        c.nLabel = nLabel;
         std::vector<float> vd;
         vd.reserve(c.outer.size());
         for (int q : c.outer) vd.push_back(geo::dist_point_ellipse(c.outerEllipse.Q, float(es.x(q)), float(es.y(q))));
-        if (vd.empty()) return;
-        SmFinal = geo::median_ref(vd);
-        if (SmFinal > p.thrMedianDistanceEllipse) return;
-        if (quality_of(c.outer.size(), c.outerEllipse) > 1.1f) return;
+        if (vd.empty()) return false;
+        const float SmFinal = geo::median_ref(vd);
+        if (SmFinal > p.thrMedianDistanceEllipse) return false;
+        if (quality_of(c.outer.size(), c.outerEllipse) > 1.1f) return false;
         const float ratio = c.outerEllipse.a / c.outerEllipse.b;
-        if (ratio < 0.05f || ratio > 20) return;
-        loop2.push_back(c);
+        if (ratio < 0.05f || ratio > 20) return false;
+        return true;
     } catch (...) {
+        return false;
     }
 }
 
@@ -485,11 +514,12 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
 {
     pts.resize(numCircles);
     for (int e : outer) pts.back().push_back({float(es.x(e)), float(es.y(e)), es.dx(e), es.dy(e)});
-    std::vector<int> touched;
+    // The reference marks visited points in a shared per-point flag and clears
+    // it on return; a per-call set gives the same visits and lets candidates
+    // run concurrently.
+    std::unordered_set<int> visited;
     size_t nGradientOut = 0, nAdded = 0;
-    auto undo = [&]() {
-        for (int q : touched) es.processed_aux[q] = 0;
-    };
+    auto undo = [&]() { visited.clear(); };
     for (int p0 : fc) {
         int dir = -1;
         int p = p0;
@@ -502,9 +532,7 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
                 undo();
                 throw std::out_of_range("EdgePointCollection: missing link");
             }
-            if (!es.processed_aux[p]) {
-                es.processed_aux[p] = 1;
-                touched.push_back(p);
+            if (visited.insert(p).second) {
                 const float ng = std::sqrt(es.dx(p) * es.dx(p) + es.dy(p) * es.dy(p));
                 const float gx = es.dx(p) / ng, gy = es.dy(p) / ng;
                 float tx = oe.cx - float(es.x(p)), ty = oe.cy - float(es.y(p));
@@ -675,15 +703,20 @@ void loop_two_iteration(EdgeSet& es, const std::vector<Candidate>& loop2, size_t
 
 }  // namespace
 
-void detect_from_edges(EdgeSet& es, const std::vector<int32_t>& seeds, int level, float scale,
-                       const cctagb_params& p, geo::Pcg32& rng, std::vector<MarkerCand>& out)
+namespace {
+
+// Loop 1 (Detection.cpp:69-113, 609-627) of one level: convex segments from
+// the seeds in order, ranked by averageReceivedVote.  The reference inserts
+// each candidate before the first one with a key <= its own (std::lower_bound
+// with '>'), i.e. key descending and, for equal keys, newest first.
+void link_level(EdgeSet& es, const std::vector<int32_t>& seeds, const cctagb_params& p, std::vector<Candidate>& loop1)
 {
+    loop1.clear();
     if (seeds.empty()) return;
     const size_t nMax = size_t(std::max(es.H / 2, p.maximumNbSeeds));
     const size_t nProc = std::min(seeds.size(), nMax);
-    // Loop 1 (Detection.cpp:69-113, 609-627): convex segments from the seeds,
-    // ranked by averageReceivedVote (stable insertion before equal keys).
-    std::vector<Candidate> loop1;
+    std::vector<Candidate> made;
+    made.reserve(nProc);
     for (size_t s = 0; s < nProc; ++s) {
         const int seed = seeds[s];
         if (es.processed_in[seed]) continue;
@@ -697,18 +730,93 @@ void detect_from_edges(EdgeSet& es, const std::vector<int32_t>& seeds, int level
             if (v > 0) ++nVoted;
         }
         c.averageReceivedVote = float(nReceived * nReceived) / float(nVoted);
-        auto it = std::lower_bound(loop1.begin(), loop1.end(), c, [](const Candidate& a, const Candidate& b) {
-            return a.averageReceivedVote > b.averageReceivedVote;
-        });
-        loop1.insert(it, std::move(c));
+        made.push_back(std::move(c));
     }
-    // Loop 2 (Detection.cpp:629-655)
-    const size_t n2 = std::min(loop1.size(), size_t(p.maximumNbCandidatesLoopTwo));
-    std::vector<Candidate> loop2;
-    size_t nSegmentOut = 0;
-    for (size_t i = 0; i < n2; ++i) complete_flow_component(loop1[i], es, loop2, nSegmentOut, i, p, rng);
-    // Loop 3 (Detection.cpp:677-688)
-    for (size_t i = 0; i < loop2.size(); ++i) loop_two_iteration(es, loop2, i, level, scale, p, rng, out);
+    std::vector<int> order(made.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = int(i);
+    std::sort(order.begin(), order.end(), [&](int x, int y) {
+        const float kx = made[x].averageReceivedVote, ky = made[y].averageReceivedVote;
+        if (kx > ky) return true;
+        if (ky > kx) return false;
+        return x > y;
+    });
+    loop1.reserve(made.size());
+    for (int i : order) loop1.push_back(std::move(made[i]));
+}
+
+// PCG32 stream of one candidate in one phase: results do not depend on how
+// candidates are spread over threads.
+geo::Pcg32 candidate_rng(int level, size_t index, int phase)
+{
+    return geo::Pcg32(271828, (uint64_t(level) << 32) | (uint64_t(index) << 1) | uint64_t(phase));
+}
+
+}  // namespace
+
+void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf)
+{
+    const int nl = int(jobs.size());
+    struct State {
+        std::vector<Candidate> loop1, loop2;
+        std::vector<uint8_t> keep;
+        std::vector<std::vector<MarkerCand>> out3;
+    };
+    std::vector<State> st(static_cast<size_t>(nl));
+    // Phase A: loop 1, one task per level.
+    pf(nl, [&](int l) { link_level(*jobs[l].es, *jobs[l].seeds, p, st[l].loop1); });
+    // Flat task list over (level, candidate) of loop 2.
+    std::vector<std::pair<int, int>> tasks;
+    for (int l = 0; l < nl; ++l) {
+        const size_t n2 = std::min(st[l].loop1.size(), size_t(p.maximumNbCandidatesLoopTwo));
+        st[l].keep.assign(n2, 0);
+        for (size_t i = 0; i < n2; ++i) tasks.emplace_back(l, int(i));
+    }
+    // Phase B: children and outlier removal.
+    pf(int(tasks.size()), [&](int t) {
+        const int l = tasks[t].first, i = tasks[t].second;
+        geo::Pcg32 rng = candidate_rng(jobs[l].level, size_t(i), 0);
+        st[l].keep[i] = flow_component_filter(st[l].loop1[i], *jobs[l].es, p, rng) ? 1 : 0;
+    });
+    // Phase C: segment labels in candidate order.
+    for (int l = 0; l < nl; ++l) {
+        size_t nSegmentOut = 0;
+        for (size_t i = 0; i < st[l].keep.size(); ++i)
+            if (st[l].keep[i]) flow_component_label(st[l].loop1[i], *jobs[l].es, nSegmentOut);
+    }
+    // Phase D: ellipse growing (runId = index in loop 1, as the reference).
+    // A run only tests its own bit of the per-point masks, so candidates grow
+    // in groups of 64 indices with the masks cleared between groups.
+    size_t n2max = 0;
+    for (int l = 0; l < nl; ++l) n2max = std::max(n2max, st[l].keep.size());
+    for (size_t g0 = 0; g0 < n2max; g0 += 64) {
+        std::vector<std::pair<int, int>> group;
+        for (const auto& t : tasks)
+            if (size_t(t.second) >= g0 && size_t(t.second) < g0 + 64) group.push_back(t);
+        if (g0 > 0)
+            for (int l = 0; l < nl; ++l) std::fill(jobs[l].es->processed.begin(), jobs[l].es->processed.end(), 0);
+        pf(int(group.size()), [&](int t) {
+            const int l = group[t].first, i = group[t].second;
+            if (st[l].keep[i] && !flow_component_grow(st[l].loop1[i], *jobs[l].es, size_t(i), p)) st[l].keep[i] = 0;
+        });
+    }
+    tasks.clear();
+    for (int l = 0; l < nl; ++l) {
+        for (size_t i = 0; i < st[l].keep.size(); ++i)
+            if (st[l].keep[i]) st[l].loop2.push_back(std::move(st[l].loop1[i]));
+        st[l].out3.assign(st[l].loop2.size(), {});
+        for (size_t i = 0; i < st[l].loop2.size(); ++i) tasks.emplace_back(l, int(i));
+    }
+    // Phase E: loop 3 (Detection.cpp:677-688), markers kept in candidate order.
+    pf(int(tasks.size()), [&](int t) {
+        const int l = tasks[t].first, i = tasks[t].second;
+        geo::Pcg32 rng = candidate_rng(jobs[l].level, size_t(i), 1);
+        loop_two_iteration(*jobs[l].es, st[l].loop2, size_t(i), jobs[l].level, jobs[l].scale, p, rng, st[l].out3[i]);
+    });
+    for (int l = 0; l < nl; ++l) {
+        jobs[l].out.clear();
+        for (auto& v : st[l].out3)
+            for (auto& m : v) jobs[l].out.push_back(std::move(m));
+    }
 }
 
 namespace {

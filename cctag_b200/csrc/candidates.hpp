@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 #include "cctag_b200.h"
@@ -30,6 +31,10 @@ struct EdgeSet {
     std::vector<int32_t> n_segment_out;
     std::vector<uint32_t> link_stamp;  // edge linking: point visited in call `link_token`
     uint32_t link_token = 0;
+    struct DfsFrame {
+        int x, y, k;
+    };
+    std::vector<DfsFrame> dfs_stack;  // ellipse-growing DFS scratch
 
     int x(int i) const { return exy[i] & 0xffff; }
     int y(int i) const { return exy[i] >> 16; }
@@ -60,9 +65,25 @@ struct MarkerCand {
     geo::Mat3 H = geo::Mat3::zero();
 };
 
-// Candidate markers of one level (cctagDetectionFromEdges, Detection.cpp:568-693).
-void detect_from_edges(EdgeSet& es, const std::vector<int32_t>& seeds, int level, float scale,
-                       const cctagb_params& p, geo::Pcg32& rng, std::vector<MarkerCand>& out);
+// One pyramid level's input to the candidate stage and its markers.
+struct LevelJob {
+    EdgeSet* es = nullptr;
+    const std::vector<int32_t>* seeds = nullptr;  // processing order
+    int level = 0;
+    float scale = 1.f;
+    std::vector<MarkerCand> out;
+};
+
+// Runs fn(i) for every i in [0, n), possibly concurrently; returns when all
+// have finished.
+using ParallelFor = std::function<void(int, const std::function<void(int)>&)>;
+
+// Candidate markers of every level (cctagDetectionFromEdges, Detection.cpp:
+// 568-693).  Loop 1 runs per level in seed order; loops 2 and 3 run per
+// candidate (each with its own PCG32 stream, seed 271828), with the segment
+// labels of loop 2 assigned in candidate order between them, so the result is
+// the same for any ParallelFor.
+void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf);
 
 // Level-0 re-fit of markers detected on coarser levels (Multiresolution.cpp:319-401).
 void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, geo::Pcg32& rng);

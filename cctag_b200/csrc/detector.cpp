@@ -170,14 +170,14 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     pipe_.image_stage(gray, w, h, pitch, is_device);
     const int nl = pipe_.levels();
 
-    // Candidate stage, one host thread per level (levels are independent until
-    // the level-0 re-fit; each level has its own PCG32 stream, seed 271828).
+    // Candidate stage on the host worker pool: the per-level edge sets are
+    // filled in parallel, then the phases of detect_from_edges spread their
+    // seeds and candidates over the pool (deterministic for any pool size).
     const auto t1 = clk::now();
     std::vector<HostLevel>& hl = hl_;
     std::vector<EdgeSet>& es = es_;
     pipe_.download_levels(hl);
-    std::vector<std::vector<MarkerCand>> per_level(nl);
-    auto run_level = [&](int l) {
+    auto fill_level = [&](int l) {
         EdgeSet& e = es[l];
         const HostLevel& L = hl[l];
         e.W = L.W;
@@ -193,14 +193,21 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         e.idxmap = idxmaps_[l].data();
         for (int i = 0; i < L.E; ++i) e.idxmap[size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = i;
         e.reset_state();
-        geo::Pcg32 rng(271828);
-        detect_from_edges(e, L.seeds, l, float(1 << l), params_, rng, per_level[l]);
     };
-    pool_->parallel_for(nl, run_level);
+    pool_->parallel_for(nl, fill_level);
+    std::vector<LevelJob> jobs(nl);
+    for (int l = 0; l < nl; ++l) {
+        jobs[l].es = &es[l];
+        jobs[l].seeds = &hl[l].seeds;
+        jobs[l].level = l;
+        jobs[l].scale = float(1 << l);
+    }
+    detect_from_edges(jobs, params_,
+                      [this](int n, const std::function<void(int)>& f) { pool_->parallel_for(n, f); });
     // Coarse levels first, as the reference's loop from the top level down.
     std::vector<MarkerCand> markers;
     for (int l = nl - 1; l >= 0; --l)
-        for (auto& m : per_level[l]) markers.push_back(std::move(m));
+        for (auto& m : jobs[l].out) markers.push_back(std::move(m));
     geo::Pcg32 rng0(271828);
     refit_on_level0(es[0], markers, rng0);
     for (int l = 0; l < nl; ++l) {

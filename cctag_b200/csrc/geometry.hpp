@@ -338,12 +338,25 @@ struct Pcg32 {
     uint64_t state = 0;
     static constexpr uint64_t kMul = 6364136223846793005ULL;
     static constexpr uint64_t kInc = 1442695040888963407ULL;
+    uint64_t inc = kInc;
     explicit Pcg32(uint64_t seed = 271828) { reseed(seed); }
-    void reseed(uint64_t seed) { state = (seed + kInc) * kMul + kInc; }
+    // Stream `stream` of the generator (PCG's selectable increment).
+    Pcg32(uint64_t seed, uint64_t stream) : inc((stream << 1) | 1u)
+    {
+        state = 0;
+        state = state * kMul + inc;
+        state += seed;
+        state = state * kMul + inc;
+    }
+    void reseed(uint64_t seed)
+    {
+        inc = kInc;
+        state = (seed + kInc) * kMul + kInc;
+    }
     uint32_t next()
     {
         const uint64_t old = state;
-        state = old * kMul + kInc;
+        state = old * kMul + inc;
         const uint32_t xs = uint32_t(((old >> 18) ^ old) >> 27);
         const uint32_t rot = uint32_t(old >> 59);
         return (xs >> rot) | (xs << ((32u - rot) & 31u));
@@ -370,10 +383,12 @@ struct Pcg32 {
     }
 };
 
-// Statistic.hpp:112-117 (medianRef): upper median after a full sort.
+// Statistic.hpp:112-117 (medianRef): the element at index size/2 of the
+// sorted values; nth_element yields the same element without a full sort.
+// The vector is reordered.
 inline float median_ref(std::vector<float>& v)
 {
-    std::sort(v.begin(), v.end());
+    std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
     return v[v.size() / 2];
 }
 

@@ -581,7 +581,6 @@ extern "C" int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params
     std::vector<LevelData> ld(nl);
     std::vector<cctagb::EdgeSet> es(nl);
     std::vector<MarkerCand> markers;
-    std::vector<std::vector<MarkerCand>> per(nl);
     const float lo = p.cannyThrLow * 256.f, hi = p.cannyThrHigh * 256.f;
     for (int l = 0; l < nl; ++l) {
         const int w = lw[l], h = lh[l];
@@ -630,11 +629,19 @@ extern "C" int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params
         S.flow = L.flow.data();
         S.idxmap = L.idxmap.data();
         S.reset_state();
-        geo::Pcg32 rng(271828);
-        cctagb::detect_from_edges(S, L.seeds, l, float(1 << l), p, rng, per[l]);
     }
+    std::vector<cctagb::LevelJob> jobs(nl);
+    for (int l = 0; l < nl; ++l) {
+        jobs[l].es = &es[l];
+        jobs[l].seeds = &ld[l].seeds;
+        jobs[l].level = l;
+        jobs[l].scale = float(1 << l);
+    }
+    cctagb::detect_from_edges(jobs, p, [](int n, const std::function<void(int)>& f) {
+        for (int i = 0; i < n; ++i) f(i);
+    });
     for (int l = nl - 1; l >= 0; --l)
-        for (auto& m : per[l]) markers.push_back(m);
+        for (auto& m : jobs[l].out) markers.push_back(m);
     geo::Pcg32 rng0(271828);
     cctagb::refit_on_level0(es[0], markers, rng0);
     if (p.doIdentification) {
