@@ -2,19 +2,25 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config NAME]
 
-One step = one synthetic 1920x1080 frame (12 markers, noise, motion blur,
-illumination gradient; seeded) through the whole detection: pyramid,
-derivatives, Canny, thinning, edge points, vote and seeds on the GPU, the
-candidate stage on the host, cut selection on the host, identification on the
-GPU.  N > 1 runs one independent replica per GPU on its own frames (no
-collective on the data path); `value` is frames/s over all ranks, timed as the
-max over ranks.
+One step = a batch of 16 synthetic 1920x1080 frames (12 markers each, noise,
+motion blur, illumination gradient; seeded) through the whole detection:
+pyramid, derivatives, Canny, thinning, edge points, vote and seeds on the GPU,
+the candidate stage on the host, cut selection on the host, identification on
+the GPU.  The batch goes through cctagb_detect_batch, whose slots overlap one
+frame's host stage with other frames' GPU stages.  N > 1 runs one independent
+replica per GPU on its own frames (no collective on the data path); `value` is
+frames/s over all ranks, timed as the max over ranks.
 
-`value`: frames/s with the frame already in device memory (cctagb_detect_device).
-`e2e`: frames/s through cctagb_detect with the frame in pinned host memory
-(host->device copy and every device->host download inside the timed region).
+`value`: frames/s with the frames already in device memory.
+`e2e`: frames/s with the frames in pinned host memory (host->device copies and
+every device->host download inside the timed region).
+`plain`: the same frames one at a time through cctagb_detect_device /
+cctagb_detect (single-frame latency path).
+`c4_cameras`: 16 cameras per step at mixed resolutions (640x480 .. 3840x2160,
+0-20 markers each) through cctagb_detect_batch, with per-frame p50/p99.
 Between timed steps the L2 is flushed by writing a 256 MiB buffer (untimed);
-each step is bracketed by CUDA events on the library's stream.
+each step is bracketed by CUDA events on the library's stream (every call is
+synchronous, so the closing event follows all of the step's work).
 """
 from __future__ import annotations
 
@@ -36,7 +42,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "1080p frames/s + per-stage HBM GB/s; batched/adjoint vs plain at <=0.05 px"
 UNIT = "frames/s"
-N_FRAMES = 4  # distinct seeded frames cycled through the steps
+BATCH = 16  # frames per step (distinct seeded frames)
+N_FRAMES = BATCH
 
 
 # ------------------------------------------------------------------ helpers --
@@ -160,6 +167,23 @@ def ident_flops(n_markers, rounds=10, trials=25, cuts=22, samples=100):
     return n_markers * rounds * trials * cuts * samples * 33
 
 
+def profiled_traffic(config):
+    """DRAM bytes per launch of each image-stage kernel group, from the ncu
+    summary of this workload under profiles/ (cold-cache capture; the
+    `stage: bytes` lines of its last code block)."""
+    name = {"c2_1080p": "dram_image_stage_c2_1080p.md"}.get(config)
+    f = ROOT / "profiles" / name if name else None
+    if not f or not f.exists():
+        return {}
+    blocks = f.read_text().split("```")
+    out = {}
+    for line in blocks[-2].splitlines() if len(blocks) >= 3 else []:
+        k, _, v = line.partition(":")
+        if v.strip().isdigit():
+            out[k.strip()] = int(v)
+    return out
+
+
 # ------------------------------------------------------------ the b200 arm --
 def run_b200(args, rank, world, local):
     import torch
@@ -168,14 +192,37 @@ def run_b200(args, rank, world, local):
     from cctag_b200 import capi
 
     torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
     frames = make_frames(args.config)
     H, W = frames[0].shape
-    det = cctag_b200.Detector(max_w=W, max_h=H)
+    det = cctag_b200.Detector(max_w=W, max_h=H, max_batch=BATCH)
     stream = torch.cuda.ExternalStream(det.stream)
-    d_frames = [torch.from_numpy(f).to(f"cuda:{local}") for f in frames]
+    d_frames = [torch.from_numpy(f).to(dev) for f in frames]
     h_frames = [torch.from_numpy(f).pin_memory() for f in frames]
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-    out = (capi.Marker * 512)()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    cap = 512
+    outs = [(capi.Marker * cap)() for _ in range(BATCH)]
+
+    def batch_struct(tensors, is_device):
+        fr = (capi.Frame * len(tensors))()
+        for i, t in enumerate(tensors):
+            h, w = t.shape
+            fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch = t.data_ptr(), w, h, w
+            fr[i].is_device, fr[i].frame_id = int(is_device), i
+            fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
+            fr[i].cap = cap
+        return fr
+
+    fr_dev = batch_struct(d_frames, True)
+    fr_host = batch_struct(h_frames, False)
+
+    def step_batch(fr):
+        def run(i):
+            det._check(det._lib.cctagb_detect_batch(det._h, fr, len(fr)), "detect_batch")
+            return fr
+        return run
+
+    out1 = (capi.Marker * cap)()
 
     def step_device(i):
         t = d_frames[i % len(d_frames)]
@@ -185,9 +232,9 @@ def run_b200(args, rank, world, local):
         t = h_frames[i % len(h_frames)]
         n = C.c_int()
         st = capi.Stats()
-        det._check(det._lib.cctagb_detect(det._h, C.c_void_p(t.data_ptr()), W, H, W, i, out, 512, C.byref(n),
+        det._check(det._lib.cctagb_detect(det._h, C.c_void_p(t.data_ptr()), W, H, W, i, out1, cap, C.byref(n),
                                           C.byref(st)), "detect")
-        return [out[k] for k in range(n.value)], st
+        return [out1[k] for k in range(n.value)], st
 
     def timed(step_fn, steps):
         total = 0.0
@@ -208,19 +255,38 @@ def run_b200(args, rank, world, local):
         return total, last, per
 
     for i in range(args.warmup):
+        step_batch(fr_dev)(i)
+        step_batch(fr_host)(i)
         step_device(i)
         step_host(i)
     torch.cuda.synchronize()
     barrier(world)
+    n_plain = max(args.steps, BATCH)
     with ClockSampler(local) as clk:
-        ms_dev, (markers, stats), per_dev = timed(step_device, args.steps)
+        ms_dev, fr_last, _ = timed(step_batch(fr_dev), args.steps)
         torch.cuda.synchronize()
         barrier(world)
-        ms_e2e, (_, stats_h), _ = timed(step_host, args.steps)
+        ms_e2e, fr_last_h, _ = timed(step_batch(fr_host), args.steps)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms_plain, (markers, stats), per_plain = timed(step_device, n_plain)
+        ms_plain_h, (_, stats_h), _ = timed(step_host, n_plain)
     torch.cuda.synchronize()
     barrier(world)
     ms_dev = max_over_ranks(ms_dev, world)
     ms_e2e = max_over_ranks(ms_e2e, world)
+    ms_plain = max_over_ranks(ms_plain, world)
+    ms_plain_h = max_over_ranks(ms_plain_h, world)
+    batch_frame_ms = [fr_last[i].stats.ms_total for i in range(BATCH)]
+    launches_batch = sum(fr_last[i].stats.kernel_launches for i in range(BATCH))
+    launches_batch_h = sum(fr_last_h[i].stats.kernel_launches for i in range(BATCH))
+    h2d = sum(fr_last_h[i].stats.h2d_bytes for i in range(BATCH))
+    d2h = sum(fr_last_h[i].stats.d2h_bytes for i in range(BATCH))
+    # Batched and single-frame paths return the same markers for a frame.
+    same = all(
+        [(m.id, m.status, m.x, m.y) for m in det.detect(frames[i])[0]]
+        == [(outs[i][k].id, outs[i][k].status, outs[i][k].x, outs[i][k].y) for k in range(fr_last_h[i].n_out)]
+        for i in range(min(4, BATCH)))
 
     # Per-stage device times (events between the image-stage kernels) and the
     # identification kernel, separate pass (not part of the timed region).
@@ -258,39 +324,93 @@ def run_b200(args, rank, world, local):
     stages["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++)"}
     # Roofline object for the dominant HBM-class kernel group of the image stage.
     top = max(stage_ms, key=lambda k: stage_ms[k])
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get(top)
+    traffic = profiled_traffic(args.config).get(top)
     ach = sb[top] / (stage_ms[top] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": peak_src,
                 "note": "achieved = algorithmic bytes / CUDA-event time of the kernel group, frac of measured"}
 
-    fps_dev = world * args.steps / (ms_dev * 1e-3)
-    fps_e2e = world * args.steps / (ms_e2e * 1e-3)
+    c4 = run_c4(args, det, stream, flush, torch) if rank == 0 and not args.no_c4 else None
+
+    fps_dev = world * args.steps * BATCH / (ms_dev * 1e-3)
+    fps_e2e = world * args.steps * BATCH / (ms_e2e * 1e-3)
     found = sorted(m.id for m in markers if m.status == 1)
     line = {
         "metric": METRIC, "value": round(fps_dev, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_dev / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16/f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: full detection per frame (pyramid .. identification, 3 crowns)",
-                   "frame": f"{W}x{H}", "levels": levels, "edge_points": E, "seeds": S,
-                   "markers_reliable": len(found), "candidates": stats.candidates,
+        "config": {"workload": f"{args.config}: full detection (pyramid .. identification, 3 crowns) of a batch "
+                               f"of {BATCH} frames per step through cctagb_detect_batch",
+                   "frame": f"{W}x{H}", "frames_per_step": BATCH, "levels": levels, "edge_points": E,
+                   "seeds": S, "markers_reliable": len(found), "candidates": stats.candidates,
                    "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}",
-                   "p50_ms": round(statistics.median(per_dev), 3),
-                   "p99_ms": round(float(np.percentile(per_dev, 99)), 3)},
-        "e2e": {"value": round(fps_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(stats_h.h2d_bytes),
-                "d2h_bytes_per_step": int(stats_h.d2h_bytes)},
+                   "batch_frame_p50_ms": round(statistics.median(batch_frame_ms), 3),
+                   "batch_frame_p99_ms": round(float(np.percentile(batch_frame_ms, 99)), 3),
+                   "batched_equals_single": bool(same)},
+        "e2e": {"value": round(fps_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "plain": {"value": round(world * n_plain / (ms_plain * 1e-3), 2),
+                  "e2e": round(world * n_plain / (ms_plain_h * 1e-3), 2), "unit": UNIT,
+                  "p50_ms": round(statistics.median(per_plain), 3),
+                  "p99_ms": round(float(np.percentile(per_plain, 99)), 3),
+                  "note": "one frame per call (cctagb_detect_device / cctagb_detect)"},
         "stages": stages,
         "roofline": roofline,
-        "gpu_launches": int(stats.kernel_launches + stats_h.kernel_launches) * args.steps,
+        "gpu_launches": int(launches_batch + launches_batch_h) * args.steps
+                        + int(stats.kernel_launches + stats_h.kernel_launches) * n_plain,
         "clocks": clk.summary(),
     }
+    if c4 is not None:
+        line["c4_cameras"] = c4
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(frames[:2], budget_s=args.cpu_budget, threads=1)
     det.close()
     return line
+
+
+def run_c4(args, det_c2, stream_c2, flush, torch):
+    """Multi-camera step: 16 frames of mixed resolution per call."""
+    import cctag_b200
+    from cctag_b200 import capi
+    from cctag_b200.synth import camera_batch
+
+    cams = [f.image for f in camera_batch(seed=0, n=BATCH)]
+    det = cctag_b200.Detector(max_w=3840, max_h=2160, max_batch=BATCH)
+    stream = torch.cuda.ExternalStream(det.stream)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = [torch.from_numpy(c).to(dev) for c in cams]
+    cap = 512
+    outs = [(capi.Marker * cap)() for _ in cams]
+    fr = (capi.Frame * len(cams))()
+    for i, t in enumerate(d):
+        h, w = t.shape
+        fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch, fr[i].is_device, fr[i].frame_id = t.data_ptr(), w, h, w, 1, i
+        fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
+        fr[i].cap = cap
+    for _ in range(args.warmup):
+        det._check(det._lib.cctagb_detect_batch(det._h, fr, len(cams)), "detect_batch")
+    steps = max(3, min(args.steps, 10))
+    total, per_frame = 0.0, []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        det._check(det._lib.cctagb_detect_batch(det._h, fr, len(cams)), "detect_batch")
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+        per_frame += [fr[i].stats.ms_total for i in range(len(cams))]
+    det.close()
+    sizes = sorted({f"{c.shape[1]}x{c.shape[0]}" for c in cams})
+    return {"value": round(steps * len(cams) / (total * 1e-3), 2), "unit": UNIT, "steps": steps,
+            "frames_per_step": len(cams), "resolutions": sizes,
+            "markers": int(sum(fr[i].n_out for i in range(len(cams)))),
+            "frame_p50_ms": round(statistics.median(per_frame), 3),
+            "frame_p99_ms": round(float(np.percentile(per_frame, 99)), 3),
+            "note": "cctagb_detect_batch, frames in device memory; per-frame latency = host wall time of the "
+                    "frame's detection inside the batch"}
 
 
 # ------------------------------------------------------ CPU (oracle) legs --
@@ -329,23 +449,24 @@ def run_reference(args, rank, world):
 
     with ThreadPoolExecutor(threads) as ex:
         for i in range(args.warmup):
-            list(ex.map(oracle_frame, [frames[(i + k) % len(frames)] for k in range(threads)]))
+            list(ex.map(oracle_frame, frames[:BATCH]))
         t0 = time.perf_counter()
         for s in range(args.steps):
-            list(ex.map(oracle_frame, [frames[(s + k) % len(frames)] for k in range(threads)]))
+            list(ex.map(oracle_frame, frames[:BATCH]))
         dt = time.perf_counter() - t0
-    fps = args.steps * threads / dt
+    fps = args.steps * BATCH / dt
     H, W = frames[0].shape
     return {
         "impl": "reference", "metric": METRIC, "value": round(fps, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16/f32",
         "data": "synthetic",
-        "config": {"workload": f"{args.config}: full detection per frame (pyramid .. identification, 3 crowns)",
-                   "frame": f"{W}x{H}"},
+        "config": {"workload": f"{args.config}: full detection (pyramid .. identification, 3 crowns) of a batch "
+                               f"of {BATCH} frames per step", "frame": f"{W}x{H}", "frames_per_step": BATCH},
         "cpu_baseline": {"value": round(fps, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{threads} frames per step, one per host thread (C++ restatement of the "
-                                   "reference CPU path; the reference itself cannot be built here)"},
+                         "sample": f"{BATCH} frames per step spread over {threads} host threads, one frame per "
+                                   "thread at a time (C++ restatement of the reference CPU path; the reference "
+                                   "itself cannot be built here)"},
         "e2e": {"value": round(fps, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -359,6 +480,7 @@ def main():
     ap.add_argument("--config", default="c2_1080p")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the multi-camera (mixed resolution) leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
