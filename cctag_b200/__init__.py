@@ -158,6 +158,31 @@ class Detector:
                                                    C.byref(n), C.byref(stats)), "detect_device")
         return [out[i] for i in range(n.value)], stats
 
+    def detect_batch(self, frames, cap: int = 256):
+        """Detection of several independent frames (cctagb_detect_batch).
+
+        `frames` holds uint8 numpy arrays (host) or ``(device_ptr, w, h, pitch)``
+        tuples (device memory).  Returns one ``(markers, stats)`` pair per frame.
+        """
+        n = len(frames)
+        fr = (capi.Frame * n)()
+        outs = [(capi.Marker * cap)() for _ in range(n)]
+        keep = []
+        for i, f in enumerate(frames):
+            if isinstance(f, np.ndarray):
+                g = np.ascontiguousarray(f, dtype=np.uint8)
+                keep.append(g)
+                fr[i].gray, fr[i].h, fr[i].w = g.ctypes.data, g.shape[0], g.shape[1]
+                fr[i].pitch, fr[i].is_device = g.shape[1], 0
+            else:
+                fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch = f
+                fr[i].is_device = 1
+            fr[i].frame_id = i
+            fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
+            fr[i].cap = cap
+        self._check(self._lib.cctagb_detect_batch(self._h, fr, n), "detect_batch")
+        return [([outs[i][k] for k in range(fr[i].n_out)], fr[i].stats) for i in range(n)]
+
     def detect(self, gray: np.ndarray, frame_id: int = 0, cap: int = 256):
         g = np.ascontiguousarray(gray, dtype=np.uint8)
         H, W = g.shape

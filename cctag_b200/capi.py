@@ -56,6 +56,12 @@ class Stats(C.Structure):
                 ("d2h_bytes", C.c_longlong), ("kernel_launches", C.c_int)]
 
 
+class Frame(C.Structure):
+    _fields_ = [("gray", C.c_void_p), ("w", C.c_int), ("h", C.c_int), ("pitch", C.c_size_t),
+                ("frame_id", C.c_int), ("is_device", C.c_int), ("out", C.POINTER(Marker)), ("cap", C.c_int),
+                ("n_out", C.c_int), ("status", C.c_int), ("stats", Stats)]
+
+
 # Every symbol declared in include/cctag_b200.h, with its signature.
 _P = C.c_void_p
 _I = C.c_int
@@ -69,6 +75,7 @@ SIGNATURES = {
     "cctagb_set_bank": (_I, [_P, _P, _I, _I]),
     "cctagb_detect": (_I, [_P, _P, _I, _I, _SZ, _I, _P, _I, C.POINTER(_I), _P]),
     "cctagb_detect_device": (_I, [_P, _P, _I, _I, _SZ, _I, _P, _I, C.POINTER(_I), _P]),
+    "cctagb_detect_batch": (_I, [_P, _P, _I]),
     "cctagb_image_stage": (_I, [_P, _P, _I, _I, _SZ, _I]),
     "cctagb_level_size": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_I)]),
     "cctagb_level_planes": (_I, [_P, _I, _P, _P, _P, _P]),

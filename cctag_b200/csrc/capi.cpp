@@ -1,10 +1,12 @@
 // C ABI of the library (include/cctag_b200.h).  Converts exceptions into
 // status codes; nothing crosses the ABI as a C++ exception.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "cctag_b200.h"
@@ -12,8 +14,36 @@
 #include "pipeline.hpp"
 
 struct cctagb_handle {
-    std::unique_ptr<cctagb::Detector> det;
+    std::unique_ptr<cctagb::Detector> det;        // slot 0: every single-frame call
+    std::vector<std::unique_ptr<cctagb::Detector>> extra;  // slots 1..: cctagb_detect_batch
+    cctagb_params params{};
+    int max_w = 0, max_h = 0, max_batch = 1, device = 0;
     std::string last_error;
+
+    int slots() const { return std::max(1, std::min(max_batch, 8)); }
+    // Detection slots for a batch: own device buffers, stream and host pool,
+    // the host threads shared out between the slots.
+    static int workers_per_slot(int n)
+    {
+        const int hc = int(std::max(1u, std::thread::hardware_concurrency()));
+        return std::max(0, std::min(7, hc / n - 1));
+    }
+    void ensure_slots(int n)
+    {
+        while (int(extra.size()) + 1 < n) {
+            extra.emplace_back(new cctagb::Detector(params, max_w, max_h, 1, workers_per_slot(n)));
+            copy_bank(*extra.back());
+        }
+    }
+    void copy_bank(cctagb::Detector& d) const
+    {
+        const auto& b = det->bank();
+        if (b.empty()) return;
+        std::vector<float> flat;
+        for (const auto& row : b) flat.insert(flat.end(), row.begin(), row.end());
+        d.set_bank(flat.data(), int(b.size()), int(b[0].size()));
+    }
+    cctagb::Detector& slot(int i) { return i == 0 ? *det : *extra[size_t(i - 1)]; }
 };
 
 namespace {
@@ -119,6 +149,11 @@ cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int ma
         cudaGetLastError();
         return CCTAGB_NO_DEVICE;
     }
+    h->params = *p;
+    h->max_w = max_w;
+    h->max_h = max_h;
+    h->max_batch = max_batch;
+    cudaGetDevice(&h->device);
     const cctagb_status s = guarded(h.get(), [&] { h->det.reset(new cctagb::Detector(*p, max_w, max_h, max_batch)); });
     if (s != CCTAGB_OK) return s;
     *out = h.release();
@@ -137,7 +172,10 @@ const char* cctagb_last_error_string(const cctagb_handle* h) { return h ? h->las
 cctagb_status cctagb_set_bank(cctagb_handle* h, const float* ratios, int n_ids, int n_ratios)
 {
     if (!h) return CCTAGB_BAD_ARG;
-    return guarded(h, [&] { h->det->set_bank(ratios, n_ids, n_ratios); });
+    return guarded(h, [&] {
+        h->det->set_bank(ratios, n_ids, n_ratios);
+        for (auto& d : h->extra) d->set_bank(ratios, n_ids, n_ratios);
+    });
 }
 
 cctagb_status cctagb_image_stage(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int is_device)
@@ -265,6 +303,55 @@ cctagb_status cctagb_detect_device(cctagb_handle* h, const uint8_t* d_gray, int 
 {
     if (!h) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->detect(d_gray, w, hgt, pitch, true, frame_id, out, cap, n_out, stats); });
+}
+
+cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)
+{
+    if (!h || n < 0 || (n > 0 && !frames)) return CCTAGB_BAD_ARG;
+    if (n == 0) return CCTAGB_OK;
+    return guarded(h, [&] {
+        const int S = std::min(n, h->slots());
+        h->ensure_slots(S);
+        const int workers = cctagb_handle::workers_per_slot(S);
+        for (int s = 0; s < S; ++s) h->slot(s).set_host_workers(workers);
+        for (int i = 0; i < n; ++i) {
+            frames[i].n_out = 0;
+            frames[i].status = CCTAGB_INTERNAL;
+        }
+        std::vector<std::string> msg(static_cast<size_t>(n));
+        std::atomic<int> next{0};
+        // Each slot takes the next frame until none is left; a frame's result
+        // does not depend on the slot that ran it.
+        auto run = [&](int s) {
+            cudaSetDevice(h->device);
+            cctagb::Detector& d = h->slot(s);
+            for (int i; (i = next.fetch_add(1)) < n;) {
+                cctagb_frame& f = frames[i];
+                try {
+                    d.detect(f.gray, f.w, f.h, f.pitch, f.is_device != 0, f.frame_id, f.out, f.cap, &f.n_out,
+                             &f.stats);
+                    f.status = CCTAGB_OK;
+                } catch (const cctagb::Error& e) {
+                    f.status = e.status;
+                    msg[size_t(i)] = e.msg;
+                } catch (const std::exception& e) {
+                    f.status = CCTAGB_INTERNAL;
+                    msg[size_t(i)] = e.what();
+                } catch (...) {
+                    f.status = CCTAGB_INTERNAL;
+                    msg[size_t(i)] = "unknown error";
+                }
+            }
+        };
+        std::vector<std::thread> threads;
+        for (int s = 1; s < S; ++s) threads.emplace_back(run, s);
+        run(0);
+        for (auto& t : threads) t.join();
+        h->det->set_host_workers(h->det->host_workers_max());
+        for (int i = 0; i < n; ++i)
+            if (frames[i].status != CCTAGB_OK)
+                throw cctagb::Error{frames[i].status, "frame " + std::to_string(i) + ": " + msg[size_t(i)]};
+    });
 }
 
 }  // extern "C"

@@ -1,7 +1,7 @@
 // Detection driver (cctagDetection, Detection.cpp:773-999): image stage on
-// the GPU, candidate stage on the host (one thread per pyramid level), level-0
-// re-fit, cut selection on the host, identification on the GPU, duplicate
-// removal and sort.
+// the GPU, candidate stage on the host worker pool, level-0 re-fit, cut
+// selection on the host, identification on the GPU, duplicate removal and
+// sort.
 #include "detector.hpp"
 
 #include <algorithm>
@@ -14,12 +14,13 @@
 
 namespace cctagb {
 
-Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch)
+Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, int host_workers)
     : params_(p), pipe_(p, max_w, max_h, max_batch)
 {
+    CCTAGB_CUDA(cudaMalloc(&d_bank_inv_, sizeof(float) * kMaxBankIds * kMaxBankRatios));
     if (p.nCrowns == 3) {
         for (const auto& row : kThreeCrownsBank) bank_.emplace_back(row, row + 5);
-        upload_bank(bank_);
+        upload_bank(bank_, d_bank_inv_);
     }
     int w = max_w, h = max_h;
     for (int l = 0; l < p.numberOfProcessedMultiresLayers; ++l) {
@@ -32,12 +33,16 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch)
     ensure_ident_capacity(256);
     hl_.resize(idxmaps_.size());
     es_.resize(idxmaps_.size());
-    const unsigned hc = std::thread::hardware_concurrency();
-    pool_.reset(new ThreadPool(int(std::min(7u, hc > 1 ? hc - 1 : 0u))));
+    if (host_workers < 0) {
+        const unsigned hc = std::thread::hardware_concurrency();
+        host_workers = int(std::min(7u, hc > 1 ? hc - 1 : 0u));
+    }
+    pool_.reset(new ThreadPool(host_workers));
 }
 
 Detector::~Detector()
 {
+    if (d_bank_inv_) cudaFree(d_bank_inv_);
     if (d_tasks_) cudaFree(d_tasks_);
     if (d_res_) cudaFree(d_res_);
     if (h_tasks_) cudaFreeHost(h_tasks_);
@@ -78,7 +83,7 @@ void Detector::set_bank(const float* ratios, int n_ids, int n_ratios)
         for (float r : b[i])
             if (!(r > 1.f)) throw Error{CCTAGB_BANK_ERROR, "radius ratios must be > 1"};
     }
-    upload_bank(b);
+    upload_bank(b, d_bank_inv_);
     bank_ = std::move(b);
 }
 
@@ -103,7 +108,7 @@ void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
     cudaStream_t s = pipe_.stream();
     CCTAGB_CUDA(cudaMemcpyAsync(d_tasks_, h_tasks_, sizeof(IdentTask) * n, cudaMemcpyHostToDevice, s));
     CCTAGB_CUDA(cudaEventRecord(ev_id0_, s));
-    launch_identify(pipe_.level0_src(), W, H, d_tasks_, d_res_, n, ip, s);
+    launch_identify(pipe_.level0_src(), W, H, d_tasks_, d_res_, n, d_bank_inv_, ip, s);
     CCTAGB_CUDA(cudaEventRecord(ev_id1_, s));
     CCTAGB_CUDA(cudaMemcpyAsync(h_res_, d_res_, sizeof(IdentResult) * n, cudaMemcpyDeviceToHost, s));
     CCTAGB_CUDA(cudaStreamSynchronize(s));

@@ -15,12 +15,18 @@ namespace cctagb {
 
 class Detector {
 public:
-    Detector(const cctagb_params& p, int max_w, int max_h, int max_batch);
+    // host_workers: threads of the host candidate stage besides the caller
+    // (-1: min(7, cores - 1)).
+    Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, int host_workers = -1);
     ~Detector();
     Detector(const Detector&) = delete;
     Detector& operator=(const Detector&) = delete;
 
     Pipeline& pipeline() { return pipe_; }
+    // Host threads of the candidate stage besides the caller (at most the
+    // number the detector was created with).
+    void set_host_workers(int n) { pool_->set_active(n); }
+    int host_workers_max() const { return pool_->size(); }
     void set_bank(const float* ratios, int n_ids, int n_ratios);
     const std::vector<std::vector<float>>& bank() const { return bank_; }
 
@@ -42,6 +48,7 @@ private:
     std::vector<EdgeSet> es_;                    // per level, candidate-stage state
     std::unique_ptr<ThreadPool> pool_;
     std::vector<uint8_t> frame_host_;
+    float* d_bank_inv_ = nullptr;                // kMaxBankIds x kMaxBankRatios
     IdentTask* d_tasks_ = nullptr;
     IdentResult* d_res_ = nullptr;
     IdentTask* h_tasks_ = nullptr;

@@ -54,9 +54,10 @@ int identify_step1(const MarkerCand& m, const uint8_t* img, int W, int H, const 
 // Signal start along the cut as a fraction of the unit radius.
 float begin_signal(int nCrowns);
 
-// Device launcher (identify.cu).
-void upload_bank(const std::vector<std::vector<float>>& bank);
+// Device side (identify.cu).  The bank lives in a device buffer of
+// kMaxBankIds x kMaxBankRatios floats (1 / ratio) owned by the caller.
+void upload_bank(const std::vector<std::vector<float>>& bank, float* d_bank_inv);
 void launch_identify(const uint8_t* d_img, int W, int H, const IdentTask* d_tasks, IdentResult* d_res, int n,
-                     const IdentParams& ip, cudaStream_t s);
+                     const float* d_bank_inv, const IdentParams& ip, cudaStream_t s);
 
 }  // namespace cctagb

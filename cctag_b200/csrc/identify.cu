@@ -18,21 +18,27 @@
 //
 // Cost: the reference's mean over cut pairs of sum_k (s_i[k] - s_j[k])^2, here
 // in the equivalent form n * sum_i (s_i[k] - mean_k)^2 summed over k, divided
-// by the n(n-1)/2 pairs (FP64 accumulation).
+// by the n(n-1)/2 pairs (shifted FP32 sums per sample, FP64 over samples).
+// The sample loop avoids the XU pipe (conversions, divisions), which bounds
+// a straightforward version of it.
 #include <cfloat>
 #include <cstdint>
+
+#include <cooperative_groups.h>
 
 #include "common.hpp"
 #include "ident_host.hpp"
 
 namespace cctagb {
 
-__constant__ float cBankInv[kMaxBankIds][kMaxBankRatios];  // 1 / ratio
-
 namespace {
 
 constexpr int kMaxTrials = 25;
 constexpr int kThreads = 32 * kMaxTrials;
+// Thread blocks per marker (one cluster): each evaluates every trial on its
+// quarter of the samples along the cuts, so a marker's trials run on four
+// SMs; the partial costs meet through distributed shared memory.
+constexpr int kCluster = 4;
 
 __device__ __forceinline__ void mat_mul(const float* a, const float* b, float* r)
 {
@@ -173,6 +179,7 @@ struct Shared {
     uint32_t trialOob[kMaxTrials];
     uint32_t valid[kMaxTrials];
     float cost[kMaxTrials];
+    double part[2][kMaxTrials];    // this block's share of each trial's cost (by round parity)
     float sig[kMaxCuts][kMaxSamples];
     float barcode[kMaxSamples];
     int winner[kMaxCuts];
@@ -215,33 +222,102 @@ __device__ void setup_trial(Shared& S, const IdentTask& T, int t, float px, floa
     if (lane == 0) S.trialOob[t] = m & ((T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u));
 }
 
-// Cost of one trial over its valid cuts (one warp).
-__device__ float trial_cost(const Shared& S, const uint8_t* img, int W, int t, uint32_t valid, int nS, int lane)
+// Byte -> float without a conversion instruction (exponent 2^23 trick).
+__device__ __forceinline__ float byte_to_float(uint32_t b) { return __uint_as_float(0x4B000000u | b) - 8388608.f; }
+
+// floor(x) for 0 <= x < 2^22 without a conversion instruction: adding 2^23
+// with round-toward-zero leaves floor(x) in the mantissa.  Returns the
+// integer and stores its float value in fl.
+__device__ __forceinline__ int floor_small(float x, float& fl)
+{
+    const float t = __fadd_rz(x, 8388608.f);
+    fl = t - 8388608.f;
+    return __float_as_int(t) - 0x4B000000;
+}
+
+// Identification.hpp:197-219 for a sample known to lie inside the image
+// (the integer corner is clamped so that rounding at the border never reads
+// outside the frame).
+__device__ __forceinline__ float bilinear_in(const uint8_t* __restrict__ img, int W, int H, float x, float y)
+{
+    float fpx, fpy;
+    int px = floor_small(fmaxf(x, 0.f), fpx);
+    int py = floor_small(fmaxf(y, 0.f), fpy);
+    const float fx = x - fpx, fy = y - fpy;
+    px = min(px, W - 2);
+    py = min(py, H - 2);
+    const uint8_t* p0 = img + px + size_t(py) * W;
+    const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
+    const float p1 = byte_to_float(__ldg(p0)), p2 = byte_to_float(__ldg(p0 + 1));
+    const float p3 = byte_to_float(__ldg(p0 + W)), p4 = byte_to_float(__ldg(p0 + W + 1));
+    return (p1 * (fx1 * fy1) + p2 * (fx * fy1) + p3 * (fx1 * fy) + p4 * (fx * fy)) * 0.5f;
+}
+
+// One sample of cut c of trial t (marker plane -> image, bilinear read).
+__device__ __forceinline__ float cut_sample(const Shared& S, const uint8_t* __restrict__ img, int W, int H, int t,
+                                            int c, float kf, const float* Hm)
+{
+    const float* cp = S.cutp[t][c];
+    const float x = cp[0] + kf * cp[2], y = cp[1] + kf * cp[3];
+    const float u = Hm[0] * x + Hm[1] * y + Hm[2];
+    const float v = Hm[3] * x + Hm[4] * y + Hm[5];
+    const float w = Hm[6] * x + Hm[7] * y + Hm[8];
+    const float r = __frcp_rn(w);
+    return bilinear_in(img, W, H, u * r, v * r);
+}
+
+// This block's share of the cost of trial t (one warp): the samples
+// k0 <= k < k1 (at most 32, one per lane) over the valid cuts, taken four
+// cuts at a time so that their reads overlap.  Per sample the cut values are
+// shifted by the first valid cut's value before the FP32 sums (the cost term
+// n * sum(d^2) - (sum d)^2 does not change under a common shift, and the
+// shifted sums stay small); the per-sample terms are summed in FP64.
+__device__ double trial_partial(const Shared& S, const uint8_t* __restrict__ img, int W, int H, int t,
+                               uint32_t valid, int k0, int k1, int lane)
 {
     const int n = __popc(valid);
-    if (n < 2) return FLT_MAX;
-    const float* Hm = S.trialH[t];
+    const int k = k0 + lane;
     double acc = 0.0;
-    for (int k = lane; k < nS; k += 32) {
-        double s1 = 0.0, s2 = 0.0;
+    if (n >= 2 && k < k1) {
+        float Hm[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Hm[i] = S.trialH[t][i];
+        const float kf = float(k);
+        float v0 = 0.f, s1 = 0.f, s2 = 0.f;
+        bool first = true;
         uint32_t m = valid;
         while (m) {
-            const int c = __ffs(m) - 1;
-            m &= m - 1;
-            const float* cp = S.cutp[t][c];
-            const float x = cp[0] + float(k) * cp[2], y = cp[1] + float(k) * cp[3];
-            float xr, yr, w;
-            apply_h(Hm, x, y, xr, yr, w);
-            const double v = bilinear(img, W, xr, yr);
-            s1 += v;
-            s2 += v * v;
+            int c[4];
+            int cnt = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                c[q] = m ? __ffs(m) - 1 : c[q > 0 ? q - 1 : 0];
+                if (m) {
+                    m &= m - 1;
+                    ++cnt;
+                }
+            }
+            float val[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) val[q] = cut_sample(S, img, W, H, t, c[q], kf, Hm);
+            if (first) {
+                v0 = val[0];
+                first = false;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (q < cnt) {
+                    const float d = val[q] - v0;
+                    s1 += d;
+                    s2 = fmaf(d, d, s2);
+                }
+            }
         }
-        acc += double(n) * s2 - s1 * s1;
+        acc = double(float(n) * s2 - s1 * s1);
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    const double pairs = 0.5 * double(n) * double(n - 1);
-    return float(acc / pairs);
+    return acc;
 }
 
 // Identification.hpp:373-384
@@ -257,14 +333,21 @@ __device__ __forceinline__ float dis(float sig, float val, float mub, float muw,
 
 }  // namespace
 
-__global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict__ img, int W, int H,
-                                                       const IdentTask* __restrict__ tasks, IdentResult* res,
-                                                       IdentParams ip)
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
+    k_identify(const uint8_t* __restrict__ img, int W, int H, const IdentTask* __restrict__ tasks, IdentResult* res,
+               const float* __restrict__ bankInv, IdentParams ip)
 {
+    namespace cg = cooperative_groups;
     __shared__ Shared S;
-    const IdentTask& T = tasks[blockIdx.x];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = int(cluster.block_rank());
+    const int marker = blockIdx.x / kCluster;
+    const IdentTask& T = tasks[marker];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nS = ip.nSamples;
+    // this block's samples along every cut (at most 32: one per lane)
+    const int chunk = (nS + kCluster - 1) / kCluster;
+    const int k0 = min(nS, crank * chunk), k1 = min(nS, k0 + chunk);
     const int gridN = ip.gridN;
     const int nTrials = gridN * gridN;
     const uint32_t cutMask = (T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u);
@@ -330,9 +413,20 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
             S.oob = m;
         }
         __syncthreads();
+        const int par = round & 1;
         if (warp < nTrials) {
-            const float c = trial_cost(S, img, W, warp, S.valid[warp], nS, lane);
-            if (lane == 0) S.cost[warp] = c;
+            const double c = trial_partial(S, img, W, H, warp, S.valid[warp], k0, k1, lane);
+            if (lane == 0) S.part[par][warp] = c;
+        }
+        // All blocks of the marker have their shares; a block reuses this
+        // parity's array two rounds later, after the next cluster barrier,
+        // when every block has finished reading it.
+        cluster.sync();
+        if (warp == 0 && lane < nTrials) {
+            double acc = 0.0;
+            for (int r = 0; r < kCluster; ++r) acc += cluster.map_shared_rank(&S.part[par][0], r)[lane];
+            const int n = __popc(S.valid[lane]);
+            S.cost[lane] = n >= 2 ? float(acc / (0.5 * double(n) * double(n - 1))) : FLT_MAX;
         }
         __syncthreads();
         if (tid == 0) {
@@ -360,7 +454,11 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
         if (S.fail) break;
         ns /= float((gridN - 1) / 2);
     }
-    IdentResult& R = res[blockIdx.x];
+    // No block leaves while another may still read its shared memory; the
+    // rest of the identification runs in the first block of the cluster.
+    cluster.sync();
+    if (crank != 0) return;
+    IdentResult& R = res[marker];
     if (S.fail || S.rounds == 0) {
         if (tid == 0) {
             R.status = CCTAGB_OPTI_HAS_DIVERGED;
@@ -375,11 +473,12 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
         return;
     }
     // Final signals with the optimal homography (getSignals, Identification.cpp:901).
-    if (warp < T.ncuts) {
+    constexpr int kWarps = kThreads / 32;
+    for (int c = warp; c < T.ncuts; c += kWarps) {
         float Hi[9];
         mat_inv(S.Hopt, Hi);
         float bx, by, w;
-        apply_h(Hi, T.stop[warp][0], T.stop[warp][1], bx, by, w);
+        apply_h(Hi, T.stop[c][0], T.stop[c][1], bx, by, w);
         const float xs = bx * ip.beginSig, ys = by * ip.beginSig;
         const float sx = (bx - xs) / (float(nS) - 1.f), sy = (by - ys) / (float(nS) - 1.f);
         bool bad = false;
@@ -387,11 +486,11 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
             const float x = xs + float(k) * sx, y = ys + float(k) * sy;
             float xr, yr;
             apply_h(S.Hopt, x, y, xr, yr, w);
-            if (inside(xr, yr, W, H)) S.sig[warp][k] = bilinear(img, W, xr, yr);
+            if (inside(xr, yr, W, H)) S.sig[c][k] = bilinear(img, W, xr, yr);
             else bad = true;
         }
         const uint32_t any = __ballot_sync(0xffffffffu, bad);
-        if (lane == 0 && any) atomicOr(&S.oob, 1u << warp);
+        if (lane == 0 && any) atomicOr(&S.oob, 1u << c);
     }
     __syncthreads();
     const uint32_t valid = ~S.oob & cutMask;
@@ -418,8 +517,9 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
     }
     __syncthreads();
     // Orazio distance per valid cut: lane = bank id (Identification.cpp:77-190).
-    if (warp < T.ncuts && ((valid >> warp) & 1u)) {
-        const float* sg = S.sig[warp];
+    for (int c = warp; c < T.ncuts; c += kWarps) {
+        if (!((valid >> c) & 1u)) continue;
+        const float* sg = S.sig[c];
         // statistics over samples [30, n): Boost immediate mean / variance
         float mean = 0.f, var = 0.f;
         {
@@ -461,10 +561,16 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
             const int idc = base + lane;
             unsigned long long key = 0ull;
             if (idc < ip.nIds) {
+                // this lane's bank row (1 / ratio), padded with +inf
+                float inv[kMaxBankRatios];
+#pragma unroll
+                for (int r = 0; r < kMaxBankRatios; ++r)
+                    inv[r] = r < ip.nRatios ? __ldg(&bankInv[idc * kMaxBankRatios + r]) : FLT_MAX;
                 float x = ip.beginSig, dist = 0.f;
                 for (int k = 0; k < nS; ++k) {
                     int ldum = 0;
-                    for (int r = 0; r < ip.nRatios; ++r) ldum += (cBankInv[idc][r] <= x) ? 1 : 0;
+#pragma unroll
+                    for (int r = 0; r < kMaxBankRatios; ++r) ldum += (inv[r] <= x) ? 1 : 0;
                     dist += dis(sg[k], float(-(ldum % 2) * 2 + 1), mub, muw, var);
                     x += stepX;
                 }
@@ -481,8 +587,8 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
         const int bestId = int(best & 0xffffffffull);
         const float bestV = __uint_as_float(unsigned(best >> 32));
         if (lane == 0) {
-            S.winner[warp] = bestId;
-            S.vwin[warp] = bestV;
+            S.winner[c] = bestId;
+            S.vwin[c] = bestV;
         }
     }
     __syncthreads();
@@ -526,24 +632,24 @@ __global__ void __launch_bounds__(kThreads) k_identify(const uint8_t* __restrict
     }
 }
 
-void upload_bank(const std::vector<std::vector<float>>& bank)
+void upload_bank(const std::vector<std::vector<float>>& bank, float* d_bank_inv)
 {
-    static float inv[kMaxBankIds][kMaxBankRatios];
+    std::vector<float> inv(size_t(kMaxBankIds) * kMaxBankRatios, 0.f);
     if (bank.empty() || bank.size() > size_t(kMaxBankIds) || bank[0].size() > size_t(kMaxBankRatios))
         throw Error{CCTAGB_BANK_ERROR, "bank larger than the identification kernel supports"};
     for (size_t i = 0; i < bank.size(); ++i)
-        for (size_t r = 0; r < bank[i].size(); ++r) inv[i][r] = 1.f / bank[i][r];
-    CCTAGB_CUDA(cudaMemcpyToSymbol(cBankInv, inv, sizeof(inv)));
+        for (size_t r = 0; r < bank[i].size(); ++r) inv[i * kMaxBankRatios + r] = 1.f / bank[i][r];
+    CCTAGB_CUDA(cudaMemcpy(d_bank_inv, inv.data(), inv.size() * sizeof(float), cudaMemcpyHostToDevice));
 }
 
 void launch_identify(const uint8_t* d_img, int W, int H, const IdentTask* d_tasks, IdentResult* d_res, int n,
-                     const IdentParams& ip, cudaStream_t s)
+                     const float* d_bank_inv, const IdentParams& ip, cudaStream_t s)
 {
     if (n <= 0) return;
     if (ip.gridN * ip.gridN > kMaxTrials || ip.gridN < 3 || (ip.gridN & 1) == 0)
         throw Error{CCTAGB_BAD_ARG, "imagedCenterNGridSample must be 3 or 5"};
     if (ip.nSamples > kMaxSamples || ip.nSamples < 32) throw Error{CCTAGB_BAD_ARG, "sampleCutLength out of range"};
-    k_identify<<<n, kThreads, 0, s>>>(d_img, W, H, d_tasks, d_res, ip);
+    k_identify<<<n * kCluster, kThreads, 0, s>>>(d_img, W, H, d_tasks, d_res, d_bank_inv, ip);
     CCTAGB_CUDA(cudaGetLastError());
 }
 

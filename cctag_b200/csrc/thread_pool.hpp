@@ -1,6 +1,7 @@
 // Small persistent worker pool for the host stages (one per handle).
 #pragma once
 
+#include <algorithm>
 #include <condition_variable>
 #include <exception>
 #include <functional>
@@ -12,9 +13,9 @@ namespace cctagb {
 
 class ThreadPool {
 public:
-    explicit ThreadPool(int n)
+    explicit ThreadPool(int n) : active_(n)
     {
-        for (int i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+        for (int i = 0; i < n; ++i) workers_.emplace_back([this, i] { loop(i); });
     }
     ~ThreadPool()
     {
@@ -26,13 +27,20 @@ public:
         for (auto& t : workers_) t.join();
     }
     int size() const { return int(workers_.size()); }
+    // Only the first n workers take part in later parallel_for calls (the
+    // others stay idle); n is clamped to [0, size()].
+    void set_active(int n)
+    {
+        std::lock_guard<std::mutex> l(mu_);
+        active_ = std::max(0, std::min(n, size()));
+    }
 
     // Runs fn(i) for i in [0, n) on the workers and the calling thread; the
     // first exception thrown by a task is rethrown here.
     void parallel_for(int n, const std::function<void(int)>& fn)
     {
         if (n <= 0) return;
-        if (n == 1 || workers_.empty()) {
+        if (n == 1 || workers_.empty() || active_ == 0) {
             for (int i = 0; i < n; ++i) fn(i);
             return;
         }
@@ -77,17 +85,19 @@ private:
             }
         }
     }
-    void loop()
+    void loop(int index)
     {
         unsigned seen = 0;
         for (;;) {
+            bool take_part;
             {
                 std::unique_lock<std::mutex> l(mu_);
                 cv_.wait(l, [&] { return stop_ || gen_ != seen; });
                 if (stop_) return;
                 seen = gen_;
+                take_part = index < active_;
             }
-            work();
+            if (take_part) work();
         }
     }
 
@@ -96,6 +106,7 @@ private:
     std::condition_variable cv_, done_cv_;
     const std::function<void(int)>* fn_ = nullptr;
     int next_ = 0, total_ = 0, done_ = 0;
+    int active_ = 0;
     unsigned gen_ = 0;
     bool stop_ = false;
     std::exception_ptr err_;

@@ -256,3 +256,20 @@ def config_frame(name: str, seed: int = 0) -> Frame:
     if name == "small":
         return render_frame(320, 240, 1, (40, 60), 30, seed=seed, noise_sigma=3.0, blur_sigma=1.0)
     raise ValueError(f"unknown configuration {name!r}")
+
+
+CAMERA_SIZES = ((640, 480), (1280, 720), (1920, 1080), (3840, 2160))
+
+
+def camera_batch(seed: int = 0, n: int = 16) -> list:
+    """Multi-camera step: n frames, each of a resolution drawn uniformly from
+    CAMERA_SIZES, with 0-20 markers (outer radius up to a quarter of the
+    shorter side), tilt <= 60 deg, noise sigma 4-8."""
+    rng = np.random.default_rng(seed + 7000)
+    out = []
+    for i in range(n):
+        w, h = CAMERA_SIZES[int(rng.integers(len(CAMERA_SIZES)))]
+        rmax = min(200.0, min(w, h) / 4.0)
+        out.append(render_frame(w, h, int(rng.integers(0, 21)), (15.0, rmax), 60, seed=seed * 1000 + i,
+                                noise_sigma=float(rng.uniform(4.0, 8.0)), blur_sigma=1.0))
+    return out

@@ -158,6 +158,32 @@ cctagb_status cctagb_detect(cctagb_handle* h, const uint8_t* gray, int w, int hg
 cctagb_status cctagb_detect_device(cctagb_handle* h, const uint8_t* d_gray, int w, int hgt, size_t pitch,
                                    int frame_id, cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats);
 
+/* One frame of a batch: input view, caller-owned output array, and what the
+ * call wrote back for this frame. */
+typedef struct cctagb_frame {
+    const uint8_t* gray;       /* host or device pointer (is_device)   */
+    int w, h;
+    size_t pitch;              /* bytes between rows                   */
+    int frame_id;
+    int is_device;
+    cctagb_marker* out;        /* cap entries                          */
+    int cap;
+    int n_out;                 /* written: markers returned            */
+    cctagb_status status;      /* written: this frame's status         */
+    cctagb_stats stats;        /* written: this frame's statistics     */
+} cctagb_frame;
+
+/* Detection of n independent frames (cameras), of any sizes up to the
+ * handle's max_w x max_h.  The handle runs min(max_batch, 8) detection slots,
+ * each with its own device buffers and stream, so one frame's host candidate
+ * stage overlaps other frames' GPU stages; every frame's result equals that
+ * of cctagb_detect on the same frame.  Returns CCTAGB_OK when every frame
+ * succeeded, else the status of the first failing frame (last_error_string
+ * names it); per-frame statuses are in frames[i].status.  The reference runs
+ * one frame per cctagDetection call (ICCTag.hpp:125-131); this is the
+ * multi-camera form of that call. */
+cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n);
+
 /* Image stage only (pyramid, derivatives, Canny, thinning, edge points, vote,
  * seeds) on the handle's stream; results stay on the device and are read with
  * the cctagb_level_* calls.  d_gray may be a device or a host pointer

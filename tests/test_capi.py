@@ -68,3 +68,39 @@ def test_cpp_shim_compiles_and_links(built_library, tmp_path):
     """The header-only ICCTag.hpp shim compiles against the C ABI with no
     OpenCV/Boost/Eigen, using cv::Mat / ptr_list look-alike types."""
     assert build_shim_example(built_library, tmp_path).exists()
+
+
+def test_binding_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of the ABI structs have the C compiler's sizes and
+    field offsets."""
+    import shutil
+    import subprocess
+
+    from cctag_b200 import capi
+
+    if not shutil.which("gcc"):
+        import pytest
+        pytest.skip("gcc not available")
+    root = Path(__file__).resolve().parents[1]
+    checks = {
+        "cctagb_params": (capi.Params, []),
+        "cctagb_marker": (capi.Marker, ["outer", "homography", "quality", "scale"]),
+        "cctagb_stats": (capi.Stats, ["ms_image_stage", "h2d_bytes", "kernel_launches"]),
+        "cctagb_frame": (capi.Frame, ["pitch", "out", "n_out", "status", "stats"]),
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cctag_b200.h"', "int main(void) {"]
+    for cname, (_, fields) in checks.items():
+        lines.append(f'printf("%zu\\n", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'printf("%zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(root / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = []
+    for _, (ct, fields) in checks.items():
+        want.append(C.sizeof(ct))
+        want += [getattr(ct, f).offset for f in fields]
+    assert got == want

@@ -89,3 +89,37 @@ def test_cpp_shim_example_runs(built_library, tmp_path):
     rows = [l.split() for l in r.stdout.strip().splitlines()]
     ids = sorted(int(x[0]) for x in rows if int(x[1]) == 1)
     assert ids == sorted(g.id for g in fr.markers)
+
+
+def _key(markers):
+    return [(m.id, m.status, m.x, m.y, m.outer.a, m.outer.b) for m in markers]
+
+
+def test_detect_batch_matches_single_frames(built_library, detector):
+    """Every frame of a mixed-resolution batch gives exactly what a single
+    detect of that frame gives, whatever slot ran it."""
+    from cctag_b200.synth import CAMERA_SIZES, render_frame
+    frames = []
+    for i, (w, h) in enumerate(CAMERA_SIZES[:3] * 2):
+        frames.append(render_frame(w, h, 3 + i, (15.0, min(w, h) / 5.0), 50, seed=300 + i, noise_sigma=5.0).image)
+    with cctag_b200.Detector(max_w=1920, max_h=1080, max_batch=4) as bd:
+        got = bd.detect_batch(frames)
+        again = bd.detect_batch(frames[::-1])[::-1]
+    for f, (m, st), (m2, _) in zip(frames, got, again):
+        want, _ = detector.detect(f)
+        assert _key(m) == _key(want)
+        assert _key(m2) == _key(want)
+        assert st.markers == len(m)
+
+
+def test_detect_batch_reports_the_failing_frame(built_library):
+    """A frame larger than the handle fails alone; the others are detected."""
+    small = config_frame("small", seed=4).image
+    big = np.zeros((1080, 1920), np.uint8)
+    with cctag_b200.Detector(max_w=1280, max_h=720, max_batch=2) as bd:
+        with pytest.raises(cctag_b200.CCTagError) as e:
+            bd.detect_batch([small, big, small])
+        assert e.value.status == cctag_b200.capi.TOO_LARGE
+        assert "frame 1" in str(e.value)
+        ok = bd.detect_batch([small, small])
+    assert len(ok) == 2 and _key(ok[0][0]) == _key(ok[1][0])
