@@ -331,6 +331,7 @@ def run_b200(args, rank, world, local):
                 "note": "achieved = algorithmic bytes / CUDA-event time of the kernel group, frac of measured"}
 
     c4 = run_c4(args, det, stream, flush, torch) if rank == 0 and not args.no_c4 else None
+    c5 = run_c5(args, torch) if rank == 0 and not args.no_c5 else None
 
     fps_dev = world * args.steps * BATCH / (ms_dev * 1e-3)
     fps_e2e = world * args.steps * BATCH / (ms_e2e * 1e-3)
@@ -362,10 +363,91 @@ def run_b200(args, rank, world, local):
     }
     if c4 is not None:
         line["c4_cameras"] = c4
+    if c5 is not None:
+        line["c5_refine"] = c5
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(frames[:2], budget_s=args.cpu_budget, threads=1)
     det.close()
     return line
+
+
+def run_c5(args, torch):
+    """Candidate refinement: 4096 candidates (256 distinct crops, r 8-150 px,
+    tilt <= 70 deg, noise 2-12) in one atlas, identified per call with the
+    reference's grid and with Gauss-Newton, and the cost adjoint."""
+    import cctag_b200
+    from cctag_b200 import capi
+    from cctag_b200.synth import cut_task_from_marker, refine_atlas
+
+    atlas, crops = refine_atlas(seed=0, n_crops=256)
+    base = [cut_task_from_marker(m, roi, offset=roi[:2]) for m, roi in crops]
+    n_total = 4096
+    tasks = [base[i % len(base)] for i in range(n_total)]
+    H, W = atlas.shape
+    det = cctag_b200.Detector(max_w=640, max_h=480)
+    stream = torch.cuda.ExternalStream(det.stream)
+    d = torch.from_numpy(atlas).to(torch.device("cuda", torch.cuda.current_device()))
+    arr = (capi.CutTask * n_total)(*tasks)
+    out = (capi.IdentResult * n_total)()
+    centers = np.array([[t.x0, t.y0] for t in tasks], np.float32)
+    cost = np.zeros(n_total, np.float32)
+    dcen = np.zeros((n_total, 2), np.float32)
+    dh = np.zeros((n_total, 9), np.float32)
+
+    def ident(mode):
+        det._check(det._lib.cctagb_identify_tasks(det._h, C.c_void_p(d.data_ptr()), W, H, W, arr, n_total, mode, out),
+                   "identify_tasks")
+        return [(r.status, r.id, r.x, r.y, r.iterations) for r in out]
+
+    def adjoint():
+        det._check(det._lib.cctagb_cut_cost(det._h, C.c_void_p(d.data_ptr()), W, H, W, arr, n_total,
+                                            capi.ptr(centers), capi.ptr(cost), capi.ptr(dcen), capi.ptr(dh)),
+                   "cut_cost")
+
+    def timed(fn, steps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps, r
+
+    steps = max(3, min(args.steps, 10))
+    ms_grid, res_grid = timed(lambda: ident(capi.REFINE_GRID), steps)
+    ms_gn, res_gn = timed(lambda: ident(capi.REFINE_GAUSS_NEWTON), steps)
+    ms_adj, _ = timed(adjoint, steps)
+    det.close()
+    # agreement of the two refinements on the distinct candidates (the FP64
+    # reference comparison is in the test-suite)
+    egn = [float(np.hypot(a[2] - b[2], a[3] - b[3])) for a, b in zip(res_grid[:len(base)], res_gn[:len(base)])
+           if a[0] == 1 and b[0] == 1]
+
+    def stats(v):
+        return {"median_px": round(float(np.median(v)), 4), "p95_px": round(float(np.percentile(v, 95)), 4),
+                "max_px": round(float(np.max(v)), 4)} if v else None
+
+    ok_grid = sum(1 for r in res_grid[:len(base)] if r[0] == 1)
+    ok_gn = sum(1 for r in res_gn[:len(base)] if r[0] == 1)
+    same_id = sum(1 for a, b in zip(res_grid[:len(base)], res_gn[:len(base)]) if a[0] == 1 and b[0] == 1
+                  and a[1] == b[1])
+    return {
+        "candidates_per_call": n_total, "distinct": len(base), "atlas": f"{W}x{H}",
+        "grid": {"candidates_per_s": round(n_total / (ms_grid * 1e-3), 1), "ms_per_call": round(ms_grid, 3),
+                 "identified": ok_grid},
+        "gauss_newton": {"candidates_per_s": round(n_total / (ms_gn * 1e-3), 1), "ms_per_call": round(ms_gn, 3),
+                         "identified": ok_gn, "vs_grid": stats(egn),
+                         "same_id_as_grid": same_id,
+                         "mean_iterations": round(float(np.mean([r[4] for r in res_gn[:len(base)]])), 2)},
+        "adjoint": {"candidates_per_s": round(n_total / (ms_adj * 1e-3), 1), "ms_per_call": round(ms_adj, 3),
+                    "note": "cctagb_cut_cost: cost + d/dcenter + d/dH per candidate"},
+        "speedup_gn_vs_grid": round(ms_grid / ms_gn, 2),
+        "note": "cctagb_identify_tasks on one device atlas; tasks from the rendered outer ellipses (22 cuts)",
+    }
 
 
 def run_c4(args, det_c2, stream_c2, flush, torch):
@@ -481,6 +563,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the multi-camera (mixed resolution) leg")
+    ap.add_argument("--no-c5", action="store_true", help="skip the candidate-refinement leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -183,6 +183,36 @@ class Detector:
         self._check(self._lib.cctagb_detect_batch(self._h, fr, n), "detect_batch")
         return [([outs[i][k] for k in range(fr[i].n_out)], fr[i].stats) for i in range(n)]
 
+    # -- identification of caller-given candidates ---------------------------
+    def last_tasks(self):
+        """Identification tasks of the last detect call (ctypes CutTask array)."""
+        n = C.c_int()
+        cap = 1024
+        out = (capi.CutTask * cap)()
+        self._check(self._lib.cctagb_last_tasks(self._h, out, cap, C.byref(n)), "last_tasks")
+        return out[:n.value]
+
+    def identify_tasks(self, dptr: int, w: int, h: int, pitch: int, tasks, refine_mode: int = capi.REFINE_GRID):
+        """cctagb_identify_tasks on a device image; returns IdentResult list."""
+        n = len(tasks)
+        arr = (capi.CutTask * n)(*tasks)
+        out = (capi.IdentResult * n)()
+        self._check(self._lib.cctagb_identify_tasks(self._h, C.c_void_p(dptr), w, h, pitch, arr, n, refine_mode,
+                                                    out), "identify_tasks")
+        return list(out)
+
+    def cut_cost(self, dptr: int, w: int, h: int, pitch: int, tasks, centers: np.ndarray):
+        """cctagb_cut_cost: (cost[n], d_center[n,2], d_h[n,9])."""
+        n = len(tasks)
+        arr = (capi.CutTask * n)(*tasks)
+        c = np.ascontiguousarray(centers, dtype=np.float32).reshape(n, 2)
+        cost = np.zeros(n, np.float32)
+        dc = np.zeros((n, 2), np.float32)
+        dh = np.zeros((n, 9), np.float32)
+        self._check(self._lib.cctagb_cut_cost(self._h, C.c_void_p(dptr), w, h, pitch, arr, n, capi.ptr(c),
+                                              capi.ptr(cost), capi.ptr(dc), capi.ptr(dh)), "cut_cost")
+        return cost, dc, dh
+
     def detect(self, gray: np.ndarray, frame_id: int = 0, cap: int = 256):
         g = np.ascontiguousarray(gray, dtype=np.uint8)
         H, W = g.shape

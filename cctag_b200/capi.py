@@ -34,7 +34,7 @@ class Params(C.Structure):
         ("imagedCenterNeighbourSize", C.c_float), ("minIdentProba", C.c_float), ("useLMDif", C.c_int),
         ("searchForAnotherSegment", C.c_int), ("writeOutput", C.c_int), ("doIdentification", C.c_int),
         ("maxEdges", C.c_uint32), ("refineMode", C.c_int), ("gnIterations", C.c_int),
-        ("edgeCapacityDivisor", C.c_int),
+        ("gnCoarseRounds", C.c_int), ("edgeCapacityDivisor", C.c_int),
     ]
 
 
@@ -62,6 +62,20 @@ class Frame(C.Structure):
                 ("n_out", C.c_int), ("status", C.c_int), ("stats", Stats)]
 
 
+MAX_CUTS = 32
+
+
+class CutTask(C.Structure):
+    _fields_ = [("Q", C.c_float * 9), ("cx", C.c_float), ("cy", C.c_float), ("a", C.c_float), ("b", C.c_float),
+                ("angle", C.c_float), ("x0", C.c_float), ("y0", C.c_float), ("ncuts", C.c_int),
+                ("stop", (C.c_float * 2) * MAX_CUTS), ("roi", C.c_int * 4)]
+
+
+class IdentResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("id", C.c_int), ("x", C.c_float), ("y", C.c_float), ("H", C.c_float * 9),
+                ("residual", C.c_float), ("score", C.c_float), ("nvalid", C.c_int), ("iterations", C.c_int)]
+
+
 # Every symbol declared in include/cctag_b200.h, with its signature.
 _P = C.c_void_p
 _I = C.c_int
@@ -76,6 +90,9 @@ SIGNATURES = {
     "cctagb_detect": (_I, [_P, _P, _I, _I, _SZ, _I, _P, _I, C.POINTER(_I), _P]),
     "cctagb_detect_device": (_I, [_P, _P, _I, _I, _SZ, _I, _P, _I, C.POINTER(_I), _P]),
     "cctagb_detect_batch": (_I, [_P, _P, _I]),
+    "cctagb_last_tasks": (_I, [_P, _P, _I, C.POINTER(_I)]),
+    "cctagb_identify_tasks": (_I, [_P, _P, _I, _I, _SZ, _P, _I, _I, _P]),
+    "cctagb_cut_cost": (_I, [_P, _P, _I, _I, _SZ, _P, _I, _P, _P, _P, _P]),
     "cctagb_image_stage": (_I, [_P, _P, _I, _I, _SZ, _I]),
     "cctagb_level_size": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_I)]),
     "cctagb_level_planes": (_I, [_P, _I, _P, _P, _P, _P]),

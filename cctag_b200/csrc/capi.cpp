@@ -111,7 +111,8 @@ void cctagb_params_default(cctagb_params* p, int nCrowns)
     p->doIdentification = 1;
     p->maxEdges = 20000;
     p->refineMode = CCTAGB_REFINE_GRID;
-    p->gnIterations = 6;
+    p->gnIterations = 10;
+    p->gnCoarseRounds = 2;
     p->edgeCapacityDivisor = 4;
 }
 
@@ -303,6 +304,32 @@ cctagb_status cctagb_detect_device(cctagb_handle* h, const uint8_t* d_gray, int 
 {
     if (!h) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->detect(d_gray, w, hgt, pitch, true, frame_id, out, cap, n_out, stats); });
+}
+
+cctagb_status cctagb_last_tasks(cctagb_handle* h, cctagb_cut_task* out, int cap, int* n)
+{
+    if (!h || !n || (cap > 0 && !out)) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        const auto& t = h->det->last_tasks();
+        *n = int(t.size());
+        if (*n > cap) throw cctagb::Error{CCTAGB_BAD_ARG, "output capacity too small"};
+        std::copy(t.begin(), t.end(), out);
+    });
+}
+
+cctagb_status cctagb_identify_tasks(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
+                                    const cctagb_cut_task* tasks, int n, int refine_mode, cctagb_ident_result* out)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->identify_tasks(d_img, w, hgt, pitch, tasks, n, refine_mode, out); });
+}
+
+cctagb_status cctagb_cut_cost(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
+                              const cctagb_cut_task* tasks, int n, const float* centers, float* cost,
+                              float* d_center, float* d_h)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->cut_cost(d_img, w, hgt, pitch, tasks, n, centers, cost, d_center, d_h); });
 }
 
 cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)

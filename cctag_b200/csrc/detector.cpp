@@ -6,7 +6,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstring>
+#include <string>
 #include <future>
 #include <list>
 
@@ -43,6 +45,9 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, 
 Detector::~Detector()
 {
     if (d_bank_inv_) cudaFree(d_bank_inv_);
+    if (d_centers_) cudaFree(d_centers_);
+    if (d_cost_) cudaFree(d_cost_);
+    if (h_cost_) cudaFreeHost(h_cost_);
     if (d_tasks_) cudaFree(d_tasks_);
     if (d_res_) cudaFree(d_res_);
     if (h_tasks_) cudaFreeHost(h_tasks_);
@@ -87,33 +92,117 @@ void Detector::set_bank(const float* ratios, int n_ids, int n_ratios)
     bank_ = std::move(b);
 }
 
-void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
+IdentParams Detector::ident_params(int refine_mode) const
 {
-    if (n <= 0) return;
-    if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
-    ensure_ident_capacity(n);
-    int W, H;
-    pipe_.level_size(0, &W, &H);
-    std::memcpy(h_tasks_, tasks, sizeof(IdentTask) * n);
     IdentParams ip{};
     ip.nSamples = std::min(params_.sampleCutLength, kMaxSamples);
     ip.beginSig = begin_signal(params_.nCrowns);
     ip.neighbourSize = params_.imagedCenterNeighbourSize;
     ip.gridN = params_.imagedCenterNGridSample;
     ip.minIdentProba = params_.minIdentProba;
-    ip.nIds = int(bank_.size());
-    ip.nRatios = int(bank_[0].size());
-    ip.refineMode = params_.refineMode;
+    ip.nIds = bank_.empty() ? 0 : int(bank_.size());
+    ip.nRatios = bank_.empty() ? 0 : int(bank_[0].size());
+    ip.refineMode = refine_mode;
     ip.gnIterations = params_.gnIterations;
+    ip.coarseRounds = params_.gnCoarseRounds;
+    return ip;
+}
+
+void Detector::identify_on(const uint8_t* d_img, size_t pitch, const IdentTask* tasks, int n, const IdentParams& ip,
+                           IdentResult* out)
+{
+    if (n <= 0) return;
+    if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
+    ensure_ident_capacity(n);
+    std::memcpy(h_tasks_, tasks, sizeof(IdentTask) * n);
     cudaStream_t s = pipe_.stream();
     CCTAGB_CUDA(cudaMemcpyAsync(d_tasks_, h_tasks_, sizeof(IdentTask) * n, cudaMemcpyHostToDevice, s));
     CCTAGB_CUDA(cudaEventRecord(ev_id0_, s));
-    launch_identify(pipe_.level0_src(), W, H, d_tasks_, d_res_, n, d_bank_inv_, ip, s);
+    launch_identify(d_img, pitch, d_tasks_, d_res_, n, d_bank_inv_, ip, s);
     CCTAGB_CUDA(cudaEventRecord(ev_id1_, s));
     CCTAGB_CUDA(cudaMemcpyAsync(h_res_, d_res_, sizeof(IdentResult) * n, cudaMemcpyDeviceToHost, s));
     CCTAGB_CUDA(cudaStreamSynchronize(s));
     std::memcpy(out, h_res_, sizeof(IdentResult) * n);
     pipe_.add_io((long long)sizeof(IdentTask) * n, (long long)sizeof(IdentResult) * n, 1);
+}
+
+void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
+{
+    int W, H;
+    pipe_.level_size(0, &W, &H);
+    identify_on(pipe_.level0_src(), size_t(W), tasks, n, ident_params(params_.refineMode), out);
+}
+
+namespace {
+
+// Caller-given tasks must stay inside the image and within the kernel's limits.
+void check_tasks(const IdentTask* tasks, int n, int w, int h, size_t pitch)
+{
+    if (n < 0 || (n > 0 && !tasks)) throw Error{CCTAGB_BAD_ARG, "bad task array"};
+    if (w < 2 || h < 2 || pitch < size_t(w)) throw Error{CCTAGB_BAD_ARG, "bad image size or pitch"};
+    for (int i = 0; i < n; ++i) {
+        const IdentTask& t = tasks[i];
+        const int* r = t.roi;
+        if (r[0] < 0 || r[1] < 0 || r[2] < 2 || r[3] < 2 || r[0] + r[2] > w || r[1] + r[3] > h)
+            throw Error{CCTAGB_BAD_ARG, "task " + std::to_string(i) + ": rectangle outside the image"};
+        if (t.ncuts < 0 || t.ncuts > kMaxCuts)
+            throw Error{CCTAGB_BAD_ARG, "task " + std::to_string(i) + ": ncuts out of range"};
+        bool finite = std::isfinite(t.x0) && std::isfinite(t.y0) && std::isfinite(t.a) && std::isfinite(t.b);
+        for (float q : t.Q) finite = finite && std::isfinite(q);
+        for (int c = 0; c < t.ncuts; ++c) finite = finite && std::isfinite(t.stop[c][0]) && std::isfinite(t.stop[c][1]);
+        if (!finite) throw Error{CCTAGB_BAD_ARG, "task " + std::to_string(i) + ": non-finite value"};
+    }
+}
+
+}  // namespace
+
+void Detector::identify_tasks(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
+                              int refine_mode, IdentResult* out)
+{
+    if (!d_img || (n > 0 && !out)) throw Error{CCTAGB_BAD_ARG, "bad image or output pointer"};
+    check_tasks(tasks, n, w, h, pitch);
+    identify_on(d_img, pitch, tasks, n, ident_params(refine_mode), out);
+}
+
+void Detector::cut_cost(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
+                        const float* centers, float* cost, float* d_center, float* d_h)
+{
+    if (!d_img || (n > 0 && !centers)) throw Error{CCTAGB_BAD_ARG, "bad image or center pointer"};
+    check_tasks(tasks, n, w, h, pitch);
+    if (n == 0) return;
+    ensure_ident_capacity(n);
+    if (n > cost_cap_) {
+        if (d_centers_) cudaFree(d_centers_);
+        if (d_cost_) cudaFree(d_cost_);
+        if (h_cost_) cudaFreeHost(h_cost_);
+        d_centers_ = nullptr;
+        d_cost_ = nullptr;
+        h_cost_ = nullptr;
+        cost_cap_ = 0;
+        CCTAGB_CUDA(cudaMalloc(&d_centers_, sizeof(float) * 2 * size_t(n)));
+        CCTAGB_CUDA(cudaMalloc(&d_cost_, sizeof(float) * 12 * size_t(n)));
+        CCTAGB_CUDA(cudaMallocHost(&h_cost_, sizeof(float) * 12 * size_t(n)));
+        cost_cap_ = n;
+    }
+    std::memcpy(h_tasks_, tasks, sizeof(IdentTask) * n);
+    std::memcpy(h_cost_, centers, sizeof(float) * 2 * size_t(n));
+    cudaStream_t s = pipe_.stream();
+    CCTAGB_CUDA(cudaMemcpyAsync(d_tasks_, h_tasks_, sizeof(IdentTask) * n, cudaMemcpyHostToDevice, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(d_centers_, h_cost_, sizeof(float) * 2 * size_t(n), cudaMemcpyHostToDevice, s));
+    launch_cut_cost(d_img, pitch, d_tasks_, d_centers_, d_cost_, n, ident_params(params_.refineMode), s);
+    CCTAGB_CUDA(cudaMemcpyAsync(h_cost_, d_cost_, sizeof(float) * 12 * size_t(n), cudaMemcpyDeviceToHost, s));
+    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; ++i) {
+        const float* o = h_cost_ + 12 * size_t(i);
+        if (cost) cost[i] = o[0];
+        if (d_center) {
+            d_center[2 * i] = o[1];
+            d_center[2 * i + 1] = o[2];
+        }
+        if (d_h)
+            for (int j = 0; j < 9; ++j) d_h[9 * size_t(i) + j] = o[3 + j];
+    }
+    pipe_.add_io((long long)(sizeof(IdentTask) + 8) * n, 48LL * n, 1);
 }
 
 namespace {
@@ -172,6 +261,7 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
     using clk = std::chrono::steady_clock;
     const auto t0 = clk::now();
+    last_tasks_.clear();
     pipe_.image_stage(gray, w, h, pitch, is_device);
     const int nl = pipe_.levels();
 
@@ -252,6 +342,7 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
                 tasks.push_back(all[i]);
             }
         }
+        last_tasks_ = tasks;
         std::vector<IdentResult> res(tasks.size());
         if (!tasks.empty()) {
             identify(tasks.data(), int(tasks.size()), res.data());

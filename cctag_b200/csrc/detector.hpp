@@ -36,9 +36,20 @@ public:
     // Identification of caller-given markers (ellipse + initial center + cuts)
     // on the frame last passed to the image stage.
     void identify(const IdentTask* tasks, int n, IdentResult* out);
+    // Batched identification / cost and adjoints on a caller's device image
+    // (cctagb_identify_tasks, cctagb_cut_cost).
+    void identify_tasks(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
+                        int refine_mode, IdentResult* out);
+    void cut_cost(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
+                  const float* centers, float* cost, float* d_center, float* d_h);
+    // Tasks handed to the identification kernel by the last detect().
+    const std::vector<IdentTask>& last_tasks() const { return last_tasks_; }
 
 private:
     void ensure_ident_capacity(int n);
+    IdentParams ident_params(int refine_mode) const;
+    void identify_on(const uint8_t* d_img, size_t pitch, const IdentTask* tasks, int n, const IdentParams& ip,
+                     IdentResult* out);
 
     cctagb_params params_;
     Pipeline pipe_;
@@ -54,6 +65,11 @@ private:
     IdentTask* h_tasks_ = nullptr;
     IdentResult* h_res_ = nullptr;
     int ident_cap_ = 0;
+    float* d_centers_ = nullptr;
+    float* d_cost_ = nullptr;
+    float* h_cost_ = nullptr;
+    int cost_cap_ = 0;
+    std::vector<IdentTask> last_tasks_;
     cudaEvent_t ev_id0_ = nullptr, ev_id1_ = nullptr;
 };
 

@@ -202,6 +202,10 @@ int identify_step1(const MarkerCand& m, const uint8_t* img, int W, int H, const 
     task.angle = e.angle;
     task.x0 = m.cx_img;
     task.y0 = m.cy_img;
+    task.roi[0] = 0;
+    task.roi[1] = 0;
+    task.roi[2] = W;
+    task.roi[3] = H;
     return CCTAGB_ID_RELIABLE;
 }
 

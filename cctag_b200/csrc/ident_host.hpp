@@ -11,30 +11,15 @@
 
 namespace cctagb {
 
-constexpr int kMaxCuts = 32;
+constexpr int kMaxCuts = CCTAGB_MAX_CUTS;
 constexpr int kMaxSamples = 128;
 constexpr int kMaxBankIds = 128;
 constexpr int kMaxBankRatios = 8;
 
-// One marker to identify on the GPU.
-struct IdentTask {
-    float Q[9];                // outer ellipse conic, row-major (level-0 pixels)
-    float cx, cy, a, b, angle; // its parameters
-    float x0, y0;              // initial imaged center (centerImg)
-    int ncuts;
-    float stop[kMaxCuts][2];   // selected cut end points (refined outer edge)
-};
-
-struct IdentResult {
-    int status;        // CCTAGB_ID_RELIABLE, CCTAGB_OPTI_HAS_DIVERGED, CCTAGB_ID_NOT_RELIABLE
-    int id;
-    float x, y;        // refined imaged center
-    float H[9];        // marker plane -> image, row-major
-    float residual;    // normalised residual (sqrt(cost) / barcode range)
-    float score;       // mean identification probability of the winning id
-    int nvalid;        // cuts inside the image at the end
-    int pad;
-};
+// One marker to identify on the GPU (the ABI's cctagb_cut_task) and its
+// result (cctagb_ident_result).
+using IdentTask = cctagb_cut_task;
+using IdentResult = cctagb_ident_result;
 
 struct IdentParams {
     int nSamples;           // sampleCutLength (<= kMaxSamples)
@@ -44,7 +29,8 @@ struct IdentParams {
     float minIdentProba;
     int nIds, nRatios;      // bank shape
     int refineMode;         // CCTAGB_REFINE_GRID / CCTAGB_REFINE_GAUSS_NEWTON
-    int gnIterations;
+    int gnIterations;       // Gauss-Newton cost evaluations at most
+    int coarseRounds;       // grid rounds before Gauss-Newton
 };
 
 // Cut selection of one marker (identify_step_1).  Returns the marker status
@@ -57,7 +43,12 @@ float begin_signal(int nCrowns);
 // Device side (identify.cu).  The bank lives in a device buffer of
 // kMaxBankIds x kMaxBankRatios floats (1 / ratio) owned by the caller.
 void upload_bank(const std::vector<std::vector<float>>& bank, float* d_bank_inv);
-void launch_identify(const uint8_t* d_img, int W, int H, const IdentTask* d_tasks, IdentResult* d_res, int n,
+// Tasks carry their image rectangle; d_img rows are pitch bytes apart.
+void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_tasks, IdentResult* d_res, int n,
                      const float* d_bank_inv, const IdentParams& ip, cudaStream_t s);
+// Cost and adjoints at given centers (cctagb_cut_cost): out is 12 floats per
+// task (cost, d/dcenter x2, d/dH x9).
+void launch_cut_cost(const uint8_t* d_img, size_t pitch, const IdentTask* d_tasks, const float* d_centers,
+                     float* d_out, int n, const IdentParams& ip, cudaStream_t s);
 
 }  // namespace cctagb

@@ -77,20 +77,36 @@ __device__ __forceinline__ void apply_h(const float* H, float x, float y, float&
     oy = v / w;
 }
 
+// The image a candidate is read from: a device image with its row pitch and
+// the candidate's rectangle [x0, x1) x [y0, y1) (the whole frame in a
+// detection; one crop of an atlas in the batched form).
+struct Roi {
+    const uint8_t* img;
+    size_t pitch;
+    int x0, y0, x1, y1;
+};
+
+__device__ __forceinline__ Roi make_roi(const uint8_t* img, size_t pitch, const IdentTask& T)
+{
+    return Roi{img, pitch, T.roi[0], T.roi[1], T.roi[0] + T.roi[2], T.roi[1] + T.roi[3]};
+}
+
 // Identification.hpp:197-219
-__device__ __forceinline__ float bilinear(const uint8_t* __restrict__ img, int W, float x, float y)
+__device__ __forceinline__ float bilinear(const Roi& R, float x, float y)
 {
     const int px = int(x), py = int(y);
-    const uint8_t* p0 = img + px + size_t(py) * W;
+    const uint8_t* p0 = R.img + px + size_t(py) * R.pitch;
     const float fx = x - float(px), fy = y - float(py);
     const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
-    const float p1 = __ldg(p0), p2 = __ldg(p0 + 1), p3 = __ldg(p0 + W), p4 = __ldg(p0 + W + 1);
+    const float p1 = __ldg(p0), p2 = __ldg(p0 + 1), p3 = __ldg(p0 + R.pitch), p4 = __ldg(p0 + R.pitch + 1);
     return (p1 * (fx1 * fy1) + p2 * (fx * fy1) + p3 * (fx1 * fy) + p4 * (fx * fy)) / 2;
 }
 
-__device__ __forceinline__ bool inside(float x, float y, int W, int H)
+// The reference's test "x >= 0 && x < cols - 1 && y >= 0 && y < rows - 1",
+// on the candidate's rectangle.
+__device__ __forceinline__ bool inside(const Roi& R, float x, float y)
 {
-    return x >= 0.f && x < float(W - 1) && y >= 0.f && y < float(H - 1);
+    return x >= float(R.x0) && x < float(R.x1 - 1) && y >= float(R.y0) && y < float(R.y1 - 1);
 }
 
 // Ellipse.cpp:103-159 semi axes of a conic (for the conditioned ellipse).
@@ -175,7 +191,22 @@ struct Shared {
     int fail;
     float trialH[kMaxTrials][9];
     float trialPt[kMaxTrials][2];
-    float cutp[kMaxTrials][kMaxCuts][4];  // xStart, yStart, stepX, stepY (marker plane)
+    union {
+        float cutp[kMaxTrials][kMaxCuts][4];  // grid: xStart, yStart, stepX, stepY (marker plane)
+        struct {                              // Gauss-Newton: this block's samples
+            float s[kMaxCuts][32];            // value
+            float dx[kMaxCuts][32];           // d value / d center x
+            float dy[kMaxCuts][32];           // d value / d center y
+        } gn;
+    } u;
+    // Gauss-Newton state
+    float gH[9], gHi[9], gdH[2][9], gdHi[2][9];  // homography at the trial center, inverse, center derivatives
+    float gTry[2];                               // trial center
+    uint32_t gOob;                               // cuts whose end samples leave the rectangle at the trial
+    double gPart[2][6];                          // this block's sums (cost, J^T r, J^T J) by parity
+    double gSum[6];
+    double gA[3], gG[2], gBest, gLambda;         // normal equations at the best center, its cost, damping
+    int gHave, gStop, iterations;
     uint32_t trialOob[kMaxTrials];
     uint32_t valid[kMaxTrials];
     float cost[kMaxTrials];
@@ -188,8 +219,8 @@ struct Shared {
 
 // Per trial (one warp): homography, cut parameters in the marker plane and
 // the cuts whose end samples leave the image.
-__device__ void setup_trial(Shared& S, const IdentTask& T, int t, float px, float py, const IdentParams& ip, int W,
-                            int H, int lane)
+__device__ void setup_trial(Shared& S, const IdentTask& T, int t, float px, float py, const IdentParams& ip,
+                            const Roi& R, int lane)
 {
     float Hm[9], Hi[9];
     homography_from_center(S.C, S.Tp, S.Td, px, py, Hm);
@@ -207,16 +238,16 @@ __device__ void setup_trial(Shared& S, const IdentTask& T, int t, float px, floa
         else bx = by = NAN;
         const float xs = bx * ip.beginSig, ys = by * ip.beginSig;
         const float sx = (bx - xs) / (float(ip.nSamples) - 1.f), sy = (by - ys) / (float(ip.nSamples) - 1.f);
-        S.cutp[t][lane][0] = xs;
-        S.cutp[t][lane][1] = ys;
-        S.cutp[t][lane][2] = sx;
-        S.cutp[t][lane][3] = sy;
+        S.u.cutp[t][lane][0] = xs;
+        S.u.cutp[t][lane][1] = ys;
+        S.u.cutp[t][lane][2] = sx;
+        S.u.cutp[t][lane][3] = sy;
         float x0, y0, w0, x1, y1, w1;
         apply_h(Hm, xs, ys, x0, y0, w0);
         const float kl = float(ip.nSamples - 1);
         apply_h(Hm, xs + kl * sx, ys + kl * sy, x1, y1, w1);
         bad = !(w0 > 0.f && w1 > 0.f) && !(w0 < 0.f && w1 < 0.f);
-        bad = bad || !inside(x0, y0, W, H) || !inside(x1, y1, W, H);
+        bad = bad || !inside(R, x0, y0) || !inside(R, x1, y1);
     }
     const uint32_t m = __ballot_sync(0xffffffffu, bad);
     if (lane == 0) S.trialOob[t] = m & ((T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u));
@@ -235,35 +266,56 @@ __device__ __forceinline__ int floor_small(float x, float& fl)
     return __float_as_int(t) - 0x4B000000;
 }
 
-// Identification.hpp:197-219 for a sample known to lie inside the image
-// (the integer corner is clamped so that rounding at the border never reads
-// outside the frame).
-__device__ __forceinline__ float bilinear_in(const uint8_t* __restrict__ img, int W, int H, float x, float y)
+// The four pixels around a sample known to lie inside the rectangle (the
+// integer corner is clamped so that rounding at the border never reads
+// outside it), and the fractional offsets.
+__device__ __forceinline__ void bilinear_taps(const Roi& R, float x, float y, float p[4], float& fx, float& fy)
 {
     float fpx, fpy;
     int px = floor_small(fmaxf(x, 0.f), fpx);
     int py = floor_small(fmaxf(y, 0.f), fpy);
-    const float fx = x - fpx, fy = y - fpy;
-    px = min(px, W - 2);
-    py = min(py, H - 2);
-    const uint8_t* p0 = img + px + size_t(py) * W;
+    fx = x - fpx;
+    fy = y - fpy;
+    px = min(max(px, R.x0), R.x1 - 2);
+    py = min(max(py, R.y0), R.y1 - 2);
+    const uint8_t* p0 = R.img + px + size_t(py) * R.pitch;
+    p[0] = byte_to_float(__ldg(p0));
+    p[1] = byte_to_float(__ldg(p0 + 1));
+    p[2] = byte_to_float(__ldg(p0 + R.pitch));
+    p[3] = byte_to_float(__ldg(p0 + R.pitch + 1));
+}
+
+// Identification.hpp:197-219 for a sample inside the rectangle.
+__device__ __forceinline__ float bilinear_in(const Roi& R, float x, float y)
+{
+    float p[4], fx, fy;
+    bilinear_taps(R, x, y, p, fx, fy);
     const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
-    const float p1 = byte_to_float(__ldg(p0)), p2 = byte_to_float(__ldg(p0 + 1));
-    const float p3 = byte_to_float(__ldg(p0 + W)), p4 = byte_to_float(__ldg(p0 + W + 1));
-    return (p1 * (fx1 * fy1) + p2 * (fx * fy1) + p3 * (fx1 * fy) + p4 * (fx * fy)) * 0.5f;
+    return (p[0] * (fx1 * fy1) + p[1] * (fx * fy1) + p[2] * (fx1 * fy) + p[3] * (fx * fy)) * 0.5f;
+}
+
+// Same value and its gradient in x and y (the derivative of the bilinear
+// patch the sample falls in).
+__device__ __forceinline__ float bilinear_grad(const Roi& R, float x, float y, float& gx, float& gy)
+{
+    float p[4], fx, fy;
+    bilinear_taps(R, x, y, p, fx, fy);
+    const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
+    gx = ((p[1] - p[0]) * fy1 + (p[3] - p[2]) * fy) * 0.5f;
+    gy = ((p[2] - p[0]) * fx1 + (p[3] - p[1]) * fx) * 0.5f;
+    return (p[0] * (fx1 * fy1) + p[1] * (fx * fy1) + p[2] * (fx1 * fy) + p[3] * (fx * fy)) * 0.5f;
 }
 
 // One sample of cut c of trial t (marker plane -> image, bilinear read).
-__device__ __forceinline__ float cut_sample(const Shared& S, const uint8_t* __restrict__ img, int W, int H, int t,
-                                            int c, float kf, const float* Hm)
+__device__ __forceinline__ float cut_sample(const Shared& S, const Roi& R, int t, int c, float kf, const float* Hm)
 {
-    const float* cp = S.cutp[t][c];
+    const float* cp = S.u.cutp[t][c];
     const float x = cp[0] + kf * cp[2], y = cp[1] + kf * cp[3];
     const float u = Hm[0] * x + Hm[1] * y + Hm[2];
     const float v = Hm[3] * x + Hm[4] * y + Hm[5];
     const float w = Hm[6] * x + Hm[7] * y + Hm[8];
     const float r = __frcp_rn(w);
-    return bilinear_in(img, W, H, u * r, v * r);
+    return bilinear_in(R, u * r, v * r);
 }
 
 // This block's share of the cost of trial t (one warp): the samples
@@ -272,8 +324,7 @@ __device__ __forceinline__ float cut_sample(const Shared& S, const uint8_t* __re
 // shifted by the first valid cut's value before the FP32 sums (the cost term
 // n * sum(d^2) - (sum d)^2 does not change under a common shift, and the
 // shifted sums stay small); the per-sample terms are summed in FP64.
-__device__ double trial_partial(const Shared& S, const uint8_t* __restrict__ img, int W, int H, int t,
-                               uint32_t valid, int k0, int k1, int lane)
+__device__ double trial_partial(const Shared& S, const Roi& R, int t, uint32_t valid, int k0, int k1, int lane)
 {
     const int n = __popc(valid);
     const int k = k0 + lane;
@@ -299,7 +350,7 @@ __device__ double trial_partial(const Shared& S, const uint8_t* __restrict__ img
             }
             float val[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) val[q] = cut_sample(S, img, W, H, t, c[q], kf, Hm);
+            for (int q = 0; q < 4; ++q) val[q] = cut_sample(S, R, t, c[q], kf, Hm);
             if (first) {
                 v0 = val[0];
                 first = false;
@@ -331,10 +382,286 @@ __device__ __forceinline__ float dis(float sig, float val, float mub, float muw,
     return d * d / (2.0f * var);
 }
 
+
+// ------------------------------------------------------- center derivatives --
+// A value with its derivatives along the two imaged-center coordinates
+// (forward mode), for the homography of a trial center.
+struct D2 {
+    float v, a, b;
+};
+__device__ __forceinline__ D2 d2c(float v) { return D2{v, 0.f, 0.f}; }
+__device__ __forceinline__ D2 operator+(D2 p, D2 q) { return D2{p.v + q.v, p.a + q.a, p.b + q.b}; }
+__device__ __forceinline__ D2 operator*(D2 p, float s) { return D2{p.v * s, p.a * s, p.b * s}; }
+__device__ __forceinline__ D2 operator+(D2 p, float s) { return D2{p.v + s, p.a, p.b}; }
+__device__ __forceinline__ D2 operator*(D2 p, D2 q) { return D2{p.v * q.v, p.a * q.v + p.v * q.a, p.b * q.v + p.v * q.b}; }
+__device__ __forceinline__ D2 operator/(D2 p, D2 q)
+{
+    const float r = p.v / q.v;
+    return D2{r, (p.a - r * q.a) / q.v, (p.b - r * q.b) / q.v};
+}
+__device__ __forceinline__ D2 dsqrt(D2 p)
+{
+    const float r = sqrtf(p.v);
+    const float h = 0.5f / r;
+    return D2{r, p.a * h, p.b * h};
+}
+
+// homography_from_center and its derivatives with respect to (x, y).
+__device__ void homography_center_derivs(const float* C, const float* Tp, const float* Td, float x, float y,
+                                         float* H, float* dHx, float* dHy)
+{
+    const D2 X{x, 1.f, 0.f}, Y{y, 0.f, 1.f};
+    const D2 u = X * Tp[0] + Y * Tp[1] + Tp[2];
+    const D2 v = X * Tp[3] + Y * Tp[4] + Tp[5];
+    const D2 w = X * Tp[6] + Y * Tp[7] + Tp[8];
+    const D2 xc = u / w, yc = v / w;
+    const float Q11 = C[0], Q22 = C[4], Q33 = C[8];
+    D2 h[9];
+    h[0] = d2c(Q33);        h[1] = xc * yc * Q22;          h[2] = xc * (-Q33);
+    h[3] = d2c(0.f);        h[4] = xc * xc * (-Q11) + (-Q33); h[5] = yc * (-Q33);
+    h[6] = xc * (-Q11);     h[7] = yc * Q22;               h[8] = d2c(-Q33);
+    const D2 e0 = dsqrt((xc * xc * Q11 + yc * yc * Q22 + Q33) * (Q22 * Q33 / Q11));
+    const D2 e2 = dsqrt((xc * xc * Q11 + Q33) * (-Q22));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        h[i * 3 + 0] = h[i * 3 + 0] * e0;
+        h[i * 3 + 1] = h[i * 3 + 1] * Q33;
+        h[i * 3 + 2] = h[i * 3 + 2] * e2;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const D2 r = h[j] * Td[i * 3] + h[3 + j] * Td[i * 3 + 1] + h[6 + j] * Td[i * 3 + 2];
+            H[i * 3 + j] = r.v;
+            dHx[i * 3 + j] = r.a;
+            dHy[i * 3 + j] = r.b;
+        }
+}
+
+// Back-projected end of a cut (stop point through Hi, normalised) and its
+// derivatives along the center, given dHi for both center coordinates.
+__device__ __forceinline__ void back_project(const float* Hi, const float* dHi0, const float* dHi1, float px, float py,
+                                             float& bx, float& by, float db[2][2])
+{
+    const float z0 = Hi[0] * px + Hi[1] * py + Hi[2];
+    const float z1 = Hi[3] * px + Hi[4] * py + Hi[5];
+    const float z2 = Hi[6] * px + Hi[7] * py + Hi[8];
+    bx = z0 / z2;
+    by = z1 / z2;
+    const float* d[2] = {dHi0, dHi1};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const float e0 = d[q][0] * px + d[q][1] * py + d[q][2];
+        const float e1 = d[q][3] * px + d[q][4] * py + d[q][5];
+        const float e2 = d[q][6] * px + d[q][7] * py + d[q][8];
+        db[q][0] = (e0 - bx * e2) / z2;
+        db[q][1] = (e1 - by * e2) / z2;
+    }
+}
+
+// dHi = -Hi dH Hi
+__device__ __forceinline__ void inverse_derivative(const float* Hi, const float* dH, float* dHi)
+{
+    float t[9];
+    mat_mul(dH, Hi, t);
+    mat_mul(Hi, t, dHi);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) dHi[k] = -dHi[k];
+}
+
+// Levenberg-Marquardt on the cut-consistency cost (CCTAGB_REFINE_GAUSS_NEWTON):
+// residuals r_ik = s_ik - mean_k over the valid cuts i and samples k, whose
+// sum of squares is the reference's pair cost up to the factor n / pairs;
+// Jacobian d r_ik / d center from the forward derivatives of the trial
+// homography, its inverse (which moves the back-projected cut ends) and the
+// bilinear patch.  Each block of the cluster sums its samples; the sums meet
+// through distributed shared memory and every block takes the same step.
+// Starts from the grid's center; a step that raises the cost is rejected and
+// the damping raised.  Stops when a step is below 1e-3 px, or after
+// gnIterations cost evaluations.
+template <class Cluster>
+__device__ void gn_refine(Shared& S, const IdentTask& T, const Roi& roi, const IdentParams& ip, uint32_t cutMask,
+                          int k0, int k1, Cluster& cluster)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = kThreads / 32;
+    const int nS = ip.nSamples;
+    const float bs = ip.beginSig;
+    const float den = float(nS) - 1.f;
+    if (tid == 0) {
+        S.gTry[0] = S.cx;
+        S.gTry[1] = S.cy;
+        S.gHave = 0;
+        S.gStop = 0;
+        S.gLambda = 1e-3;
+    }
+    __syncthreads();
+    for (int it = 0; it < ip.gnIterations; ++it) {
+        if (tid == 0) {
+            homography_center_derivs(S.C, S.Tp, S.Td, S.gTry[0], S.gTry[1], S.gH, S.gdH[0], S.gdH[1]);
+            if (!mat_inv(S.gH, S.gHi)) {
+                S.gStop = 1;
+            } else {
+                inverse_derivative(S.gHi, S.gdH[0], S.gdHi[0]);
+                inverse_derivative(S.gHi, S.gdH[1], S.gdHi[1]);
+            }
+        }
+        __syncthreads();
+        if (S.gStop) break;
+        // cuts whose end samples leave the rectangle at this center
+        if (warp == 0) {
+            bool bad = false;
+            if (lane < T.ncuts) {
+                float bx, by, w;
+                apply_h(S.gHi, T.stop[lane][0], T.stop[lane][1], bx, by, w);
+                const float xs = bx * bs, ys = by * bs;
+                const float sx = (bx - xs) / den, sy = (by - ys) / den;
+                float x0, y0, w0, x1, y1, w1;
+                apply_h(S.gH, xs, ys, x0, y0, w0);
+                apply_h(S.gH, xs + den * sx, ys + den * sy, x1, y1, w1);
+                bad = !(w0 > 0.f && w1 > 0.f) && !(w0 < 0.f && w1 < 0.f);
+                bad = bad || !inside(roi, x0, y0) || !inside(roi, x1, y1);
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, bad);
+            if (lane == 0) S.gOob = m & cutMask;
+        }
+        __syncthreads();
+        const uint32_t valid = ~(S.oob | S.gOob) & cutMask;
+        // this block's samples: value and its derivatives along the center
+        const int k = k0 + lane;
+        for (int c = warp; c < T.ncuts; c += kWarps) {
+            if (!((valid >> c) & 1u) || k >= k1) continue;
+            float bx, by, db[2][2];
+            back_project(S.gHi, S.gdHi[0], S.gdHi[1], T.stop[c][0], T.stop[c][1], bx, by, db);
+            const float xs = bx * bs, ys = by * bs;
+            const float sx = (bx - xs) / den, sy = (by - ys) / den;
+            const float kf = float(k);
+            const float x = xs + kf * sx, y = ys + kf * sy;
+            const float t = bs + kf * (1.f - bs) / den;
+            const float* Hm = S.gH;
+            const float u = Hm[0] * x + Hm[1] * y + Hm[2];
+            const float v = Hm[3] * x + Hm[4] * y + Hm[5];
+            const float w = Hm[6] * x + Hm[7] * y + Hm[8];
+            const float r = __frcp_rn(w);
+            const float qx = u * r, qy = v * r;
+            float gx, gy;
+            const float val = bilinear_grad(roi, qx, qy, gx, gy);
+            float ds[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const float* dH = S.gdH[q];
+                const float dxq = t * db[q][0], dyq = t * db[q][1];
+                const float du = dH[0] * x + dH[1] * y + dH[2] + Hm[0] * dxq + Hm[1] * dyq;
+                const float dv = dH[3] * x + dH[4] * y + dH[5] + Hm[3] * dxq + Hm[4] * dyq;
+                const float dw = dH[6] * x + dH[7] * y + dH[8] + Hm[6] * dxq + Hm[7] * dyq;
+                ds[q] = gx * (du - qx * dw) * r + gy * (dv - qy * dw) * r;
+            }
+            S.u.gn.s[c][lane] = val;
+            S.u.gn.dx[c][lane] = ds[0];
+            S.u.gn.dy[c][lane] = ds[1];
+        }
+        __syncthreads();
+        const int par = it & 1;
+        if (warp == 0) {
+            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            const int n = __popc(valid);
+            if (k < k1 && n >= 2) {
+                float v0 = 0.f, s1 = 0.f, s2 = 0.f, a1 = 0.f, b1 = 0.f, aa = 0.f, ab = 0.f, bb = 0.f, ad = 0.f,
+                      bd = 0.f;
+                bool first = true;
+                uint32_t m = valid;
+                while (m) {
+                    const int c = __ffs(m) - 1;
+                    m &= m - 1;
+                    const float v = S.u.gn.s[c][lane], a = S.u.gn.dx[c][lane], b = S.u.gn.dy[c][lane];
+                    if (first) {
+                        v0 = v;
+                        first = false;
+                    }
+                    const float d = v - v0;
+                    s1 += d;
+                    s2 = fmaf(d, d, s2);
+                    a1 += a;
+                    b1 += b;
+                    aa = fmaf(a, a, aa);
+                    ab = fmaf(a, b, ab);
+                    bb = fmaf(b, b, bb);
+                    ad = fmaf(a, d, ad);
+                    bd = fmaf(b, d, bd);
+                }
+                const float fn = float(n);
+                acc[0] = double(fn * s2 - s1 * s1);
+                acc[1] = double(ad - a1 * s1 / fn);
+                acc[2] = double(bd - b1 * s1 / fn);
+                acc[3] = double(aa - a1 * a1 / fn);
+                acc[4] = double(ab - a1 * b1 / fn);
+                acc[5] = double(bb - b1 * b1 / fn);
+            }
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+#pragma unroll
+                for (int o = 16; o; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+            }
+            if (lane == 0)
+#pragma unroll
+                for (int j = 0; j < 6; ++j) S.gPart[par][j] = acc[j];
+        }
+        // every block's sums are in; a parity's array is rewritten two
+        // evaluations later, past the next cluster barrier
+        cluster.sync();
+        if (warp == 0 && lane < 6) {
+            double a = 0.0;
+            for (int q = 0; q < kCluster; ++q) a += cluster.map_shared_rank(&S.gPart[par][0], q)[lane];
+            S.gSum[lane] = a;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const int n = __popc(valid);
+            const double cost = n >= 2 ? S.gSum[0] / (0.5 * double(n) * double(n - 1)) : DBL_MAX;
+            ++S.iterations;
+            if (n >= 2 && (!S.gHave || cost < S.gBest)) {
+                S.gHave = 1;
+                S.gBest = cost;
+                S.cx = S.gTry[0];
+                S.cy = S.gTry[1];
+                S.oob |= S.gOob;
+                for (int q = 0; q < 9; ++q) S.Hopt[q] = S.gH[q];
+                S.minRes = float(cost);
+                S.gG[0] = S.gSum[1];
+                S.gG[1] = S.gSum[2];
+                S.gA[0] = S.gSum[3];
+                S.gA[1] = S.gSum[4];
+                S.gA[2] = S.gSum[5];
+                S.gLambda = fmax(S.gLambda * 0.1, 1e-7);
+            } else {
+                S.gLambda *= 10.0;
+            }
+            if (!S.gHave) {
+                S.gStop = 1;
+            } else {
+                const double a = S.gA[0] * (1.0 + S.gLambda), b = S.gA[1], c = S.gA[2] * (1.0 + S.gLambda);
+                const double det = a * c - b * b;
+                if (!(det > 0.0)) {
+                    S.gStop = 1;
+                } else {
+                    const double dx = -(c * S.gG[0] - b * S.gG[1]) / det;
+                    const double dy = -(a * S.gG[1] - b * S.gG[0]) / det;
+                    if (dx * dx + dy * dy < 1e-6) S.gStop = 1;
+                    S.gTry[0] = float(double(S.cx) + dx);
+                    S.gTry[1] = float(double(S.cy) + dy);
+                }
+            }
+        }
+        __syncthreads();
+        if (S.gStop) break;
+    }
+}
+
 }  // namespace
 
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
-    k_identify(const uint8_t* __restrict__ img, int W, int H, const IdentTask* __restrict__ tasks, IdentResult* res,
+    k_identify(const uint8_t* __restrict__ img, size_t pitch, const IdentTask* __restrict__ tasks, IdentResult* res,
                const float* __restrict__ bankInv, IdentParams ip)
 {
     namespace cg = cooperative_groups;
@@ -343,6 +670,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
     const int crank = int(cluster.block_rank());
     const int marker = blockIdx.x / kCluster;
     const IdentTask& T = tasks[marker];
+    const Roi roi = make_roi(img, pitch, T);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nS = ip.nSamples;
     // this block's samples along every cut (at most 32: one per lane)
@@ -386,7 +714,9 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
             ++r;
             ns /= float((gridN - 1) / 2);
         }
+        if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON) r = min(r, ip.coarseRounds);
         S.rounds = r;
+        S.iterations = r;
     }
     __syncthreads();
     float ns = ip.neighbourSize;
@@ -401,7 +731,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
             const float qx = ccx - half + float(i) * step, qy = ccy - half + float(j) * step;
             float px, py, w;
             apply_h(S.mTi, qx, qy, px, py, w);
-            setup_trial(S, T, warp, px, py, ip, W, H, lane);
+            setup_trial(S, T, warp, px, py, ip, roi, lane);
         }
         __syncthreads();
         if (tid == 0) {
@@ -415,7 +745,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
         __syncthreads();
         const int par = round & 1;
         if (warp < nTrials) {
-            const double c = trial_partial(S, img, W, H, warp, S.valid[warp], k0, k1, lane);
+            const double c = trial_partial(S, roi, warp, S.valid[warp], k0, k1, lane);
             if (lane == 0) S.part[par][warp] = c;
         }
         // All blocks of the marker have their shares; a block reuses this
@@ -454,6 +784,8 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
         if (S.fail) break;
         ns /= float((gridN - 1) / 2);
     }
+    if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON && !S.fail && S.rounds > 0)
+        gn_refine(S, T, roi, ip, cutMask, k0, k1, cluster);
     // No block leaves while another may still read its shared memory; the
     // rest of the identification runs in the first block of the cluster.
     cluster.sync();
@@ -469,6 +801,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
             R.residual = FLT_MAX;
             R.score = 0.f;
             R.nvalid = 0;
+            R.iterations = S.iterations;
         }
         return;
     }
@@ -486,7 +819,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
             const float x = xs + float(k) * sx, y = ys + float(k) * sy;
             float xr, yr;
             apply_h(S.Hopt, x, y, xr, yr, w);
-            if (inside(xr, yr, W, H)) S.sig[c][k] = bilinear(img, W, xr, yr);
+            if (inside(roi, xr, yr)) S.sig[c][k] = bilinear(roi, xr, yr);
             else bad = true;
         }
         const uint32_t any = __ballot_sync(0xffffffffu, bad);
@@ -620,6 +953,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
         for (int k = 0; k < 9; ++k) R.H[k] = S.Hopt[k];
         R.residual = residual;
         R.nvalid = nValid;
+        R.iterations = S.iterations;
         if (residual > 2.7f || !(residual == residual)) {
             R.status = CCTAGB_OPTI_HAS_DIVERGED;
             R.id = -1;
@@ -629,6 +963,205 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
             R.score = score;
             R.status = score > ip.minIdentProba ? CCTAGB_ID_RELIABLE : CCTAGB_ID_NOT_RELIABLE;
         }
+    }
+}
+
+
+namespace {
+
+struct CostShared {
+    float C[9], Tp[9], Td[9];
+    float H[9], Hi[9], dH[2][9];
+    float sig[kMaxCuts][kMaxSamples];
+    float mean[kMaxSamples];
+    float dz[kMaxCuts][3];        // d cost / d (Hi p) of each cut's back-projected end
+    double red[kThreads / 32][10];
+    uint32_t oob;
+    int bad;
+};
+
+__device__ void write_cost(float* o, float cost)
+{
+    o[0] = cost;
+    for (int j = 1; j < 12; ++j) o[j] = 0.f;
+}
+
+}  // namespace
+
+// Cut-consistency cost of one task at a given center and its adjoints (one
+// block per task).  Pass 1 reads every sample (a sample outside the
+// rectangle drops its cut, as extractSignalUsingHomography does); pass 2
+// sends d cost / d s_ik = 2 n / pairs (s_ik - mean_k) back through the
+// bilinear patch to the image position, from there to H directly and to the
+// sample's marker-plane position, whose cut end is H^-1 applied to the stop
+// point; the inverse's adjoint is -H^-T G H^-T.  The center gradient is the
+// H gradient contracted with dH/dcenter (forward derivatives).
+__global__ void __launch_bounds__(kThreads) k_cut_cost(const uint8_t* __restrict__ img, size_t pitch,
+                                                       const IdentTask* __restrict__ tasks,
+                                                       const float* __restrict__ centers, float* out, IdentParams ip)
+{
+    __shared__ CostShared S;
+    const IdentTask& T = tasks[blockIdx.x];
+    const Roi roi = make_roi(img, pitch, T);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = kThreads / 32;
+    const int nS = ip.nSamples;
+    const float bs = ip.beginSig;
+    const float den = float(nS) - 1.f;
+    float* o = out + 12 * size_t(blockIdx.x);
+    const uint32_t cutMask = (T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u);
+    if (tid == 0) {
+        canonic_form(T.Q, S.C, S.Tp, S.Td);
+        homography_center_derivs(S.C, S.Tp, S.Td, centers[2 * blockIdx.x], centers[2 * blockIdx.x + 1], S.H,
+                                 S.dH[0], S.dH[1]);
+        S.bad = mat_inv(S.H, S.Hi) ? 0 : 1;
+        S.oob = 0u;
+    }
+    if (tid < kMaxCuts * 3) S.dz[tid / 3][tid % 3] = 0.f;
+    __syncthreads();
+    if (S.bad) {
+        if (tid == 0) write_cost(o, FLT_MAX);
+        return;
+    }
+    for (int c = warp; c < T.ncuts; c += kWarps) {
+        float bx, by, w;
+        apply_h(S.Hi, T.stop[c][0], T.stop[c][1], bx, by, w);
+        const float xs = bx * bs, ys = by * bs;
+        const float sx = (bx - xs) / den, sy = (by - ys) / den;
+        bool bad = false;
+        for (int k = lane; k < nS; k += 32) {
+            const float x = xs + float(k) * sx, y = ys + float(k) * sy;
+            float xr, yr;
+            apply_h(S.H, x, y, xr, yr, w);
+            if (inside(roi, xr, yr)) S.sig[c][k] = bilinear(roi, xr, yr);
+            else bad = true;
+        }
+        if (__ballot_sync(0xffffffffu, bad) && lane == 0) atomicOr(&S.oob, 1u << c);
+    }
+    __syncthreads();
+    const uint32_t valid = ~S.oob & cutMask;
+    const int n = __popc(valid);
+    if (n < 2) {
+        if (tid == 0) write_cost(o, FLT_MAX);
+        return;
+    }
+    const double pairs = 0.5 * double(n) * double(n - 1);
+    double costPart = 0.0;
+    for (int k = tid; k < nS; k += kThreads) {
+        double s1 = 0.0, s2 = 0.0;
+        uint32_t m = valid;
+        while (m) {
+            const int c = __ffs(m) - 1;
+            m &= m - 1;
+            const double v = S.sig[c][k];
+            s1 += v;
+            s2 += v * v;
+        }
+        S.mean[k] = float(s1 / double(n));
+        costPart += double(n) * s2 - s1 * s1;
+    }
+    __syncthreads();
+    float gH[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) gH[j] = 0.f;
+    const float coef = float(2.0 * double(n) / pairs);
+    const float* Hm = S.H;
+    for (int c = warp; c < T.ncuts; c += kWarps) {
+        if (!((valid >> c) & 1u)) continue;
+        const float px = T.stop[c][0], py = T.stop[c][1];
+        const float z0 = S.Hi[0] * px + S.Hi[1] * py + S.Hi[2];
+        const float z1 = S.Hi[3] * px + S.Hi[4] * py + S.Hi[5];
+        const float z2 = S.Hi[6] * px + S.Hi[7] * py + S.Hi[8];
+        const float bx = z0 / z2, by = z1 / z2;
+        const float xs = bx * bs, ys = by * bs;
+        const float sx = (bx - xs) / den, sy = (by - ys) / den;
+        float gbx = 0.f, gby = 0.f;
+        for (int k = lane; k < nS; k += 32) {
+            const float x = xs + float(k) * sx, y = ys + float(k) * sy;
+            const float u = Hm[0] * x + Hm[1] * y + Hm[2];
+            const float v = Hm[3] * x + Hm[4] * y + Hm[5];
+            const float w = Hm[6] * x + Hm[7] * y + Hm[8];
+            const float rw = 1.f / w;
+            const float qx = u / w, qy = v / w;
+            float gx, gy;
+            (void)bilinear_grad(roi, qx, qy, gx, gy);
+            const float lam = coef * (S.sig[c][k] - S.mean[k]);
+            const float fx = lam * gx, fy = lam * gy;
+            const float fw = -(fx * qx + fy * qy);
+            const float y3[3] = {x, y, 1.f};
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                gH[j] = fmaf(fx * rw, y3[j], gH[j]);
+                gH[3 + j] = fmaf(fy * rw, y3[j], gH[3 + j]);
+                gH[6 + j] = fmaf(fw * rw, y3[j], gH[6 + j]);
+            }
+            const float fX = (fx * (Hm[0] - qx * Hm[6]) + fy * (Hm[3] - qy * Hm[6])) * rw;
+            const float fY = (fx * (Hm[1] - qx * Hm[7]) + fy * (Hm[4] - qy * Hm[7])) * rw;
+            const float t = bs + float(k) * (1.f - bs) / den;
+            gbx = fmaf(t, fX, gbx);
+            gby = fmaf(t, fY, gby);
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            gbx += __shfl_xor_sync(0xffffffffu, gbx, off);
+            gby += __shfl_xor_sync(0xffffffffu, gby, off);
+        }
+        if (lane == 0) {
+            S.dz[c][0] = gbx / z2;
+            S.dz[c][1] = gby / z2;
+            S.dz[c][2] = -(gbx * bx + gby * by) / z2;
+        }
+    }
+    double red[10];
+    red[0] = costPart;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) red[1 + j] = double(gH[j]);
+#pragma unroll
+    for (int j = 0; j < 10; ++j) {
+#pragma unroll
+        for (int off = 16; off; off >>= 1) red[j] += __shfl_xor_sync(0xffffffffu, red[j], off);
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < 10; ++j) S.red[warp][j] = red[j];
+    __syncthreads();
+    if (tid == 0) {
+        double cost = 0.0, G[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int w = 0; w < kWarps; ++w) {
+            cost += S.red[w][0];
+            for (int j = 0; j < 9; ++j) G[j] += S.red[w][1 + j];
+        }
+        cost /= pairs;
+        // adjoint of Hi from the cut ends, then -Hi^T GHi Hi^T into G
+        double GHi[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int c = 0; c < T.ncuts; ++c) {
+            const double p3[3] = {T.stop[c][0], T.stop[c][1], 1.0};
+            for (int r = 0; r < 3; ++r)
+                for (int q = 0; q < 3; ++q) GHi[r * 3 + q] += double(S.dz[c][r]) * p3[q];
+        }
+        double M[9], Mt[9];
+        for (int i = 0; i < 3; ++i)      // M = GHi Hi^T
+            for (int j = 0; j < 3; ++j) {
+                double a = 0.0;
+                for (int q = 0; q < 3; ++q) a += GHi[i * 3 + q] * double(S.Hi[j * 3 + q]);
+                M[i * 3 + j] = a;
+            }
+        for (int i = 0; i < 3; ++i)      // Mt = Hi^T M
+            for (int j = 0; j < 3; ++j) {
+                double a = 0.0;
+                for (int q = 0; q < 3; ++q) a += double(S.Hi[q * 3 + i]) * M[q * 3 + j];
+                Mt[i * 3 + j] = a;
+            }
+        double dc[2] = {0.0, 0.0};
+        for (int j = 0; j < 9; ++j) {
+            G[j] -= Mt[j];
+            dc[0] += G[j] * double(S.dH[0][j]);
+            dc[1] += G[j] * double(S.dH[1][j]);
+        }
+        o[0] = float(cost);
+        o[1] = float(dc[0]);
+        o[2] = float(dc[1]);
+        for (int j = 0; j < 9; ++j) o[3 + j] = float(G[j]);
     }
 }
 
@@ -642,14 +1175,29 @@ void upload_bank(const std::vector<std::vector<float>>& bank, float* d_bank_inv)
     CCTAGB_CUDA(cudaMemcpy(d_bank_inv, inv.data(), inv.size() * sizeof(float), cudaMemcpyHostToDevice));
 }
 
-void launch_identify(const uint8_t* d_img, int W, int H, const IdentTask* d_tasks, IdentResult* d_res, int n,
+void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_tasks, IdentResult* d_res, int n,
                      const float* d_bank_inv, const IdentParams& ip, cudaStream_t s)
 {
     if (n <= 0) return;
     if (ip.gridN * ip.gridN > kMaxTrials || ip.gridN < 3 || (ip.gridN & 1) == 0)
         throw Error{CCTAGB_BAD_ARG, "imagedCenterNGridSample must be 3 or 5"};
     if (ip.nSamples > kMaxSamples || ip.nSamples < 32) throw Error{CCTAGB_BAD_ARG, "sampleCutLength out of range"};
-    k_identify<<<n * kCluster, kThreads, 0, s>>>(d_img, W, H, d_tasks, d_res, d_bank_inv, ip);
+    if (ip.refineMode != CCTAGB_REFINE_GRID && ip.refineMode != CCTAGB_REFINE_GAUSS_NEWTON)
+        throw Error{CCTAGB_BAD_ARG, "unknown refineMode"};
+    if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON && (ip.gnIterations < 1 || ip.gnIterations > 100))
+        throw Error{CCTAGB_BAD_ARG, "gnIterations must be in [1, 100]"};
+    if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON && (ip.coarseRounds < 1 || ip.coarseRounds > 64))
+        throw Error{CCTAGB_BAD_ARG, "gnCoarseRounds must be in [1, 64]"};
+    k_identify<<<n * kCluster, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_res, d_bank_inv, ip);
+    CCTAGB_CUDA(cudaGetLastError());
+}
+
+void launch_cut_cost(const uint8_t* d_img, size_t pitch, const IdentTask* d_tasks, const float* d_centers,
+                     float* d_out, int n, const IdentParams& ip, cudaStream_t s)
+{
+    if (n <= 0) return;
+    if (ip.nSamples > kMaxSamples || ip.nSamples < 32) throw Error{CCTAGB_BAD_ARG, "sampleCutLength out of range"};
+    k_cut_cost<<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_centers, d_out, ip);
     CCTAGB_CUDA(cudaGetLastError());
 }
 

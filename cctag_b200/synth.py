@@ -273,3 +273,77 @@ def camera_batch(seed: int = 0, n: int = 16) -> list:
         out.append(render_frame(w, h, int(rng.integers(0, 21)), (15.0, rmax), 60, seed=seed * 1000 + i,
                                 noise_sigma=float(rng.uniform(4.0, 8.0)), blur_sigma=1.0))
     return out
+
+
+def ellipse_of_conic(Q: np.ndarray):
+    """(cx, cy, a, b, angle) of an ellipse conic x^T Q x = 0 (a along angle)."""
+    Q = np.asarray(Q, np.float64)
+    A, bvec = Q[:2, :2], Q[:2, 2]
+    c = -np.linalg.solve(A, bvec)
+    k = Q[2, 2] + bvec @ c
+    w, V = np.linalg.eigh(A / -k)
+    a, b = 1.0 / np.sqrt(w[0]), 1.0 / np.sqrt(w[1])
+    ang = float(np.arctan2(V[1, 0], V[0, 0]))
+    return float(c[0]), float(c[1]), float(a), float(b), ang
+
+
+def cut_task_from_marker(m: Marker, roi, n_cuts: int = 22, offset=(0.0, 0.0), start=None):
+    """A cctagb_cut_task for a rendered marker: its true outer ellipse, cut
+    stops spread evenly on it, the ellipse center as the initial imaged center
+    (as detection starts), all shifted by `offset` (an atlas placement);
+    `roi` = (x, y, w, h) in the shifted image."""
+    from .capi import CutTask
+
+    ox, oy = offset
+    T = np.array([[1, 0, -ox], [0, 1, -oy], [0, 0, 1.0]])
+    Q = T.T @ m.outer_conic @ T          # conic in shifted coordinates
+    Q = Q / np.abs(Q).max()
+    cx, cy, a, b, ang = ellipse_of_conic(Q)
+    t = CutTask()
+    for k in range(9):
+        t.Q[k] = float(Q.flat[k])
+    t.cx, t.cy, t.a, t.b, t.angle = cx, cy, a, b, ang
+    t.x0, t.y0 = (cx, cy) if start is None else start
+    t.ncuts = n_cuts
+    ca, sa = np.cos(ang), np.sin(ang)
+    for i in range(n_cuts):
+        th = 2 * np.pi * i / n_cuts
+        t.stop[i][0] = cx + a * np.cos(th) * ca - b * np.sin(th) * sa
+        t.stop[i][1] = cy + a * np.cos(th) * sa + b * np.sin(th) * ca
+    for k in range(4):
+        t.roi[k] = int(roi[k])
+    return t
+
+
+def refine_atlas(seed: int = 0, n_crops: int = 256, width: int = 4096):
+    """Candidate-refinement workload: n_crops single-marker crops (outer radius
+    8-150 px, tilt <= 70 deg, noise sigma 2-12) packed row by row into one
+    atlas image.  Returns (atlas, [(marker in atlas coordinates, roi)]), roi =
+    (x, y, w, h) of the crop in the atlas."""
+    rng = np.random.default_rng(seed + 9000)
+    crops = []
+    for i in range(n_crops):
+        r = float(rng.uniform(8.0, 150.0))
+        s = int(np.ceil(4.2 * r + 12))
+        f = render_frame(s, s, 1, (r, r), 70, seed=seed * 100000 + i, noise_sigma=float(rng.uniform(2.0, 12.0)),
+                         blur_sigma=1.0)
+        if f.markers:
+            crops.append(f)
+    # shelf packing
+    x = y = shelf = 0
+    places = []
+    for f in crops:
+        h, w = f.image.shape
+        if x + w > width:
+            x, y, shelf = 0, y + shelf, 0
+        places.append((x, y))
+        x += w
+        shelf = max(shelf, h)
+    atlas = np.full((y + shelf, width), 128, np.uint8)
+    out = []
+    for f, (ox, oy) in zip(crops, places):
+        h, w = f.image.shape
+        atlas[oy:oy + h, ox:ox + w] = f.image
+        m = f.markers[0]
+        out.append((m, (ox, oy, w, h)))
+    return atlas, out

@@ -25,11 +25,13 @@
  *   cctagb_canny_from_derivatives
  *                          <- cvRecodedCanny after filter2D        src/cctag/filter/cvRecode.cpp:94-421
  *                             followed by thin()                  src/cctag/filter/thinning.cpp:15-19
- *   cctagb_identify        <- identify_step_2 / refineConicFamilyGlob + orazioDistanceRobust
+ *   cctagb_detect_batch    <- one cctagDetection call per camera  src/cctag/ICCTag.hpp:125-131
+ *   cctagb_identify_tasks  <- identify_step_2 / refineConicFamilyGlob + orazioDistanceRobust
  *                                                                  src/cctag/Identification.cpp:813-965,1318-1480
- *   cctagb_cut_cost / cctagb_cut_cost_adjoint / cctagb_refine_gn
- *                          <- costFunctionGlob (forward only in the reference)
- *                                                                  src/cctag/Identification.cpp:1122-1158
+ *   cctagb_last_tasks      <- the cuts identify_step_1 selects     src/cctag/Identification.cpp:1172-1301
+ *   cctagb_cut_cost        <- costFunctionGlob (forward only in the reference; here with its
+ *                             gradient in the center and in H)   src/cctag/Identification.cpp:1122-1158
+ *   cctagb_edges_noalloc   <- cvRecodedCanny + thin on caller buffers (no allocation)
  */
 #ifndef CCTAG_B200_H
 #define CCTAG_B200_H
@@ -104,7 +106,8 @@ typedef struct cctagb_params {
     uint32_t maxEdges;                          /* 20000 (unused by the reference path) */
     /* B200-specific */
     int refineMode;                             /* CCTAGB_REFINE_GRID */
-    int gnIterations;                           /* 6: Gauss-Newton steps in REFINE_GAUSS_NEWTON */
+    int gnIterations;                           /* 10: cost evaluations at most in REFINE_GAUSS_NEWTON */
+    int gnCoarseRounds;                         /* 2: grid rounds before Gauss-Newton */
     int edgeCapacityDivisor;                    /* 4: edge capacity per level = W*H/divisor */
 } cctagb_params;
 
@@ -235,6 +238,66 @@ cctagb_status cctagb_canny_from_derivatives(cctagb_handle* h, const int16_t* dx,
 cctagb_status cctagb_edges_noalloc(const uint8_t* d_gray, int w, int hgt, size_t pitch, float cannyThrLow,
                                    float cannyThrHigh, int16_t* d_dx, int16_t* d_dy, uint8_t* d_edges,
                                    int32_t* d_status, void* stream);
+
+/* ---- Identification of candidate markers (batched form) -----------------
+ * The reference identifies each candidate inside cctagDetection
+ * (Identification.cpp:1172-1480 identify: cut collection and selection, then
+ * refineConicFamilyGlob :813-965 and the ID vote).  These calls expose the
+ * second half on caller-given candidates, many per call, on one device image
+ * (one frame, or an atlas of crops with one rectangle per candidate). */
+
+#define CCTAGB_MAX_CUTS 32
+
+/* One candidate: what identify_step_1 (cut selection) hands to the
+ * refinement.  Coordinates are image pixels of the whole device image. */
+typedef struct cctagb_cut_task {
+    float Q[9];                     /* outer ellipse conic, row-major              */
+    float cx, cy, a, b, angle;      /* its parameters                              */
+    float x0, y0;                   /* initial imaged center (centerImg)           */
+    int ncuts;                      /* selected cuts, <= CCTAGB_MAX_CUTS           */
+    float stop[CCTAGB_MAX_CUTS][2]; /* cut end points on the outer edge            */
+    int roi[4];                     /* x, y, w, h: the candidate's image rectangle;
+                                       a sample outside it drops its cut, as the
+                                       image border does in the reference        */
+} cctagb_cut_task;
+
+typedef struct cctagb_ident_result {
+    int status;                     /* CCTAGB_ID_RELIABLE, _ID_NOT_RELIABLE, _OPTI_HAS_DIVERGED */
+    int id;                         /* bank row, -1 if none                        */
+    float x, y;                     /* refined imaged center                       */
+    float H[9];                     /* marker plane -> image at (x, y), row-major  */
+    float residual;                 /* sqrt(cost) / barcode range                  */
+    float score;                    /* mean probability of the winning id          */
+    int nvalid;                     /* cuts inside the rectangle at the end        */
+    int iterations;                 /* grid rounds + Gauss-Newton evaluations      */
+} cctagb_ident_result;
+
+/* The identification tasks of the last cctagb_detect / cctagb_detect_device
+ * call on this handle (the candidates whose cut selection succeeded, in the
+ * order they were identified); *n receives their number. */
+cctagb_status cctagb_last_tasks(cctagb_handle* h, cctagb_cut_task* out, int cap, int* n);
+
+/* Center refinement and ID reading of n candidates on the device image d_img
+ * (w x hgt, pitch bytes per row).  refine_mode CCTAGB_REFINE_GRID is the
+ * reference's shrinking 5x5 grid; CCTAGB_REFINE_GAUSS_NEWTON runs the first
+ * params.gnCoarseRounds grid rounds, then Levenberg-Marquardt steps on the cut-consistency
+ * cost with the center Jacobian from forward derivatives of the homography
+ * (params.gnIterations evaluations at most).  tasks and out are host arrays. */
+cctagb_status cctagb_identify_tasks(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
+                                    const cctagb_cut_task* tasks, int n, int refine_mode,
+                                    cctagb_ident_result* out);
+
+/* The cut-consistency cost (costFunctionGlob, Identification.cpp:1122-1158)
+ * of each task at the imaged center centers[2i], centers[2i+1], with its
+ * gradient with respect to the center (d_center, 2 per task) and to the nine
+ * entries of the homography H (d_h, 9 per task, row-major; the cut end points
+ * are back-projected through H, so both uses of H are differentiated).  Any
+ * of cost, d_center, d_h may be null.  A cut with a sample outside its task's
+ * rectangle is left out; with fewer than two cuts the cost is FLT_MAX and the
+ * gradients are zero.  All arrays are host arrays. */
+cctagb_status cctagb_cut_cost(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
+                              const cctagb_cut_task* tasks, int n, const float* centers, float* cost,
+                              float* d_center, float* d_h);
 
 #ifdef __cplusplus
 }

@@ -164,3 +164,55 @@ def detect(gray: np.ndarray, params=None, fp64: bool = False, cap: int = 512):
     out = (Marker * cap)()
     n = lib.orc_detect(_p(g), g.shape[1], g.shape[0], C.byref(p), int(bool(fp64)), C.cast(out, C.c_void_p), cap)
     return [out[i] for i in range(min(n, cap))]
+
+
+# ------------------------------------------------ batched identification --
+def _refine_sigs(lib):
+    D = C.c_double
+    lib.orc_cut_cost_h.argtypes = [_P, C.c_size_t, _P, _P, _I, D, _P, _P]
+    lib.orc_cut_cost_h.restype = _I
+    lib.orc_cut_cost.argtypes = [_P, C.c_size_t, _P, D, D, _I, D, _P, _P]
+    lib.orc_cut_cost.restype = _I
+    lib.orc_refine_grid.argtypes = [_P, C.c_size_t, _P, _I, D, _I, D, D, _P]
+    lib.orc_refine_grid.restype = _I
+
+
+def _begin_sig(n_crowns=3):
+    return float(np.float32(1.0) - np.float32(2 * n_crowns - 1) * np.float32(0.15))
+
+
+def cut_cost(img: np.ndarray, task, cx: float, cy: float, n_samples: int = 100, n_crowns: int = 3):
+    """FP64 cost of a cctagb_cut_task at an imaged center: (cost, d_center[2],
+    d_h[9], H[9]); cost is None when fewer than two cuts stay inside."""
+    lib = load()
+    _refine_sigs(lib)
+    g = np.ascontiguousarray(img, dtype=np.uint8)
+    out = np.zeros(12)
+    H = np.zeros(9)
+    ok = lib.orc_cut_cost(_p(g), g.shape[1], C.byref(task), cx, cy, n_samples, _begin_sig(n_crowns), _p(out), _p(H))
+    return (out[0] if ok else None), out[1:3].copy(), out[3:12].copy(), H
+
+
+def cut_cost_h(img: np.ndarray, task, H, n_samples: int = 100, n_crowns: int = 3):
+    """FP64 cost of a task at a given homography and d cost / d H."""
+    lib = load()
+    _refine_sigs(lib)
+    g = np.ascontiguousarray(img, dtype=np.uint8)
+    Hd = np.ascontiguousarray(H, dtype=np.float64).reshape(9)
+    cost = C.c_double()
+    grad = np.zeros(9)
+    ok = lib.orc_cut_cost_h(_p(g), g.shape[1], C.byref(task), _p(Hd), n_samples, _begin_sig(n_crowns), C.byref(cost),
+                            _p(grad))
+    return (cost.value if ok else None), grad
+
+
+def refine_grid(img: np.ndarray, task, stop_width: float = 0.02, n_samples: int = 100, n_crowns: int = 3,
+                grid_n: int = 5, neighbour_size: float = 0.2):
+    """FP64 grid refinement of a task continued to `stop_width`: (x, y, cost) or None."""
+    lib = load()
+    _refine_sigs(lib)
+    g = np.ascontiguousarray(img, dtype=np.uint8)
+    out = np.zeros(3)
+    ok = lib.orc_refine_grid(_p(g), g.shape[1], C.byref(task), n_samples, _begin_sig(n_crowns), grid_n,
+                             neighbour_size, stop_width, _p(out))
+    return (float(out[0]), float(out[1]), float(out[2])) if ok else None

@@ -87,6 +87,8 @@ def test_binding_struct_layouts_match_the_header(tmp_path):
         "cctagb_marker": (capi.Marker, ["outer", "homography", "quality", "scale"]),
         "cctagb_stats": (capi.Stats, ["ms_image_stage", "h2d_bytes", "kernel_launches"]),
         "cctagb_frame": (capi.Frame, ["pitch", "out", "n_out", "status", "stats"]),
+        "cctagb_cut_task": (capi.CutTask, ["x0", "ncuts", "stop", "roi"]),
+        "cctagb_ident_result": (capi.IdentResult, ["H", "residual", "nvalid", "iterations"]),
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cctag_b200.h"', "int main(void) {"]
     for cname, (_, fields) in checks.items():
