@@ -330,7 +330,7 @@ def run_b200(args, rank, world, local):
                 "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": peak_src,
                 "note": "achieved = algorithmic bytes / CUDA-event time of the kernel group, frac of measured"}
 
-    c4 = run_c4(args, det, stream, flush, torch) if rank == 0 and not args.no_c4 else None
+    c4 = run_c4(args, flush, torch) if rank == 0 and not args.no_c4 else None
     c5 = run_c5(args, torch) if rank == 0 and not args.no_c5 else None
 
     fps_dev = world * args.steps * BATCH / (ms_dev * 1e-3)
@@ -450,7 +450,7 @@ def run_c5(args, torch):
     }
 
 
-def run_c4(args, det_c2, stream_c2, flush, torch):
+def run_c4(args, flush, torch):
     """Multi-camera step: 16 frames of mixed resolution per call."""
     import cctag_b200
     from cctag_b200 import capi
@@ -564,6 +564,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the multi-camera (mixed resolution) leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the candidate-refinement leg")
+    ap.add_argument("--leg", default="all", choices=["all", "c4", "c5"],
+                    help="run one secondary leg alone and print its object (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -574,6 +576,16 @@ def main():
             print(json.dumps(line))
         return
     rank, world, local = dist_setup()
+    if args.leg != "all":
+        import torch
+
+        torch.cuda.set_device(local)
+        if args.leg == "c5":
+            print(json.dumps({"c5_refine": run_c5(args, torch)}))
+        else:
+            flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+            print(json.dumps({"c4_cameras": run_c4(args, flush, torch)}))
+        return
     line = run_b200(args, rank, world, local)
     if rank == 0:
         print(json.dumps(line))

@@ -35,10 +35,16 @@ namespace {
 
 constexpr int kMaxTrials = 25;
 constexpr int kThreads = 32 * kMaxTrials;
-// Thread blocks per marker (one cluster): each evaluates every trial on its
-// quarter of the samples along the cuts, so a marker's trials run on four
-// SMs; the partial costs meet through distributed shared memory.
-constexpr int kCluster = 4;
+constexpr int kWarps = kThreads / 32;
+// The samples along a cut come in chunks of 32 (one per lane).  A marker is
+// either one thread block doing every chunk, or a cluster of kCluster blocks,
+// block r doing chunk r, whose per-chunk sums meet through distributed shared
+// memory: few markers per launch spread over four SMs each, many markers
+// keep one SM each.  Per-chunk sums are formed the same way in both, and
+// added in chunk order, so both give the same bits.
+constexpr int kChunk = 32;
+constexpr int kMaxChunks = kMaxSamples / kChunk;
+constexpr int kCluster = kMaxChunks;
 
 __device__ __forceinline__ void mat_mul(const float* a, const float* b, float* r)
 {
@@ -192,33 +198,33 @@ struct Shared {
     float trialH[kMaxTrials][9];
     float trialPt[kMaxTrials][2];
     union {
-        float cutp[kMaxTrials][kMaxCuts][4];  // grid: xStart, yStart, stepX, stepY (marker plane)
-        struct {                              // Gauss-Newton: this block's samples
-            float s[kMaxCuts][32];            // value
-            float dx[kMaxCuts][32];           // d value / d center x
-            float dy[kMaxCuts][32];           // d value / d center y
+        float cutp[kMaxTrials][kMaxCuts][6];  // grid: image line of the cut's samples, U0 dU V0 dV W0 dW
+        struct {                              // Gauss-Newton: one chunk of samples
+            float s[kMaxCuts][kChunk];        // value
+            float dx[kMaxCuts][kChunk];       // d value / d center x
+            float dy[kMaxCuts][kChunk];       // d value / d center y
         } gn;
     } u;
     // Gauss-Newton state
     float gH[9], gHi[9], gdH[2][9], gdHi[2][9];  // homography at the trial center, inverse, center derivatives
     float gTry[2];                               // trial center
     uint32_t gOob;                               // cuts whose end samples leave the rectangle at the trial
-    double gPart[2][6];                          // this block's sums (cost, J^T r, J^T J) by parity
+    double gPart[2][kMaxChunks][6];              // per-chunk sums (cost, J^T r, J^T J) by parity
     double gSum[6];
     double gA[3], gG[2], gBest, gLambda;         // normal equations at the best center, its cost, damping
     int gHave, gStop, iterations;
     uint32_t trialOob[kMaxTrials];
     uint32_t valid[kMaxTrials];
     float cost[kMaxTrials];
-    double part[2][kMaxTrials];    // this block's share of each trial's cost (by round parity)
+    double part[2][kMaxChunks][kMaxTrials];  // per-chunk shares of each trial's cost (by round parity)
     float sig[kMaxCuts][kMaxSamples];
     float barcode[kMaxSamples];
     int winner[kMaxCuts];
     float vwin[kMaxCuts];
 };
 
-// Per trial (one warp): homography, cut parameters in the marker plane and
-// the cuts whose end samples leave the image.
+// Per trial (one warp): homography, the image line of each cut's samples and
+// the cuts whose end samples leave the rectangle.
 __device__ void setup_trial(Shared& S, const IdentTask& T, int t, float px, float py, const IdentParams& ip,
                             const Roi& R, int lane)
 {
@@ -238,14 +244,20 @@ __device__ void setup_trial(Shared& S, const IdentTask& T, int t, float px, floa
         else bx = by = NAN;
         const float xs = bx * ip.beginSig, ys = by * ip.beginSig;
         const float sx = (bx - xs) / (float(ip.nSamples) - 1.f), sy = (by - ys) / (float(ip.nSamples) - 1.f);
-        S.u.cutp[t][lane][0] = xs;
-        S.u.cutp[t][lane][1] = ys;
-        S.u.cutp[t][lane][2] = sx;
-        S.u.cutp[t][lane][3] = sy;
-        float x0, y0, w0, x1, y1, w1;
-        apply_h(Hm, xs, ys, x0, y0, w0);
+        // sample k is (xs + k sx, ys + k sy) in the marker plane; its image in
+        // homogeneous coordinates is linear in k: H (xs, ys, 1) + k H (sx, sy, 0)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            S.u.cutp[t][lane][2 * i] = __fmaf_rn(Hm[3 * i], xs, __fmaf_rn(Hm[3 * i + 1], ys, Hm[3 * i + 2]));
+            S.u.cutp[t][lane][2 * i + 1] = __fmaf_rn(Hm[3 * i], sx, __fmul_rn(Hm[3 * i + 1], sy));
+        }
+        // end samples, with the sample loop's own arithmetic
+        const float* cp = S.u.cutp[t][lane];
         const float kl = float(ip.nSamples - 1);
-        apply_h(Hm, xs + kl * sx, ys + kl * sy, x1, y1, w1);
+        const float w0 = cp[4], w1 = __fmaf_rn(kl, cp[5], cp[4]);
+        const float r0 = __fdividef(1.0f, w0), r1 = __fdividef(1.0f, w1);
+        const float x0 = __fmul_rn(cp[0], r0), y0 = __fmul_rn(cp[2], r0);
+        const float x1 = __fmul_rn(__fmaf_rn(kl, cp[1], cp[0]), r1), y1 = __fmul_rn(__fmaf_rn(kl, cp[3], cp[2]), r1);
         bad = !(w0 > 0.f && w1 > 0.f) && !(w0 < 0.f && w1 < 0.f);
         bad = bad || !inside(R, x0, y0) || !inside(R, x1, y1);
     }
@@ -285,13 +297,23 @@ __device__ __forceinline__ void bilinear_taps(const Roi& R, float x, float y, fl
     p[3] = byte_to_float(__ldg(p0 + R.pitch + 1));
 }
 
-// Identification.hpp:197-219 for a sample inside the rectangle.
+// Identification.hpp:197-219 for a sample inside the rectangle (explicit
+// roundings, so that every caller gets the same bits).
+__device__ __forceinline__ float bilinear_value(const float p[4], float fx, float fy)
+{
+    const float fx1 = __fsub_rn(1.0f, fx), fy1 = __fsub_rn(1.0f, fy);
+    float a = __fmul_rn(p[0], __fmul_rn(fx1, fy1));
+    a = __fmaf_rn(p[1], __fmul_rn(fx, fy1), a);
+    a = __fmaf_rn(p[2], __fmul_rn(fx1, fy), a);
+    a = __fmaf_rn(p[3], __fmul_rn(fx, fy), a);
+    return __fmul_rn(a, 0.5f);
+}
+
 __device__ __forceinline__ float bilinear_in(const Roi& R, float x, float y)
 {
     float p[4], fx, fy;
     bilinear_taps(R, x, y, p, fx, fy);
-    const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
-    return (p[0] * (fx1 * fy1) + p[1] * (fx * fy1) + p[2] * (fx1 * fy) + p[3] * (fx * fy)) * 0.5f;
+    return bilinear_value(p, fx, fy);
 }
 
 // Same value and its gradient in x and y (the derivative of the bilinear
@@ -303,72 +325,99 @@ __device__ __forceinline__ float bilinear_grad(const Roi& R, float x, float y, f
     const float fx1 = 1.0f - fx, fy1 = 1.0f - fy;
     gx = ((p[1] - p[0]) * fy1 + (p[3] - p[2]) * fy) * 0.5f;
     gy = ((p[2] - p[0]) * fx1 + (p[3] - p[1]) * fx) * 0.5f;
-    return (p[0] * (fx1 * fy1) + p[1] * (fx * fy1) + p[2] * (fx1 * fy) + p[3] * (fx * fy)) * 0.5f;
+    return bilinear_value(p, fx, fy);
 }
 
-// One sample of cut c of trial t (marker plane -> image, bilinear read).
-__device__ __forceinline__ float cut_sample(const Shared& S, const Roi& R, int t, int c, float kf, const float* Hm)
+// Row i of H applied to (x, y, 1), explicit roundings.
+__device__ __forceinline__ float hrow(const float* Hm, int i, float x, float y)
+{
+    return __fmaf_rn(Hm[3 * i], x, __fmaf_rn(Hm[3 * i + 1], y, Hm[3 * i + 2]));
+}
+
+// One sample of cut c of trial t: its point on the cut's image line, then a
+// bilinear read (fast reciprocal: one MUFU op, no IEEE fix-up).
+__device__ __forceinline__ float cut_sample(const Shared& S, const Roi& R, int t, int c, float kf)
 {
     const float* cp = S.u.cutp[t][c];
-    const float x = cp[0] + kf * cp[2], y = cp[1] + kf * cp[3];
-    const float u = Hm[0] * x + Hm[1] * y + Hm[2];
-    const float v = Hm[3] * x + Hm[4] * y + Hm[5];
-    const float w = Hm[6] * x + Hm[7] * y + Hm[8];
-    const float r = __frcp_rn(w);
-    return bilinear_in(R, u * r, v * r);
+    const float u = __fmaf_rn(kf, cp[1], cp[0]);
+    const float v = __fmaf_rn(kf, cp[3], cp[2]);
+    const float w = __fmaf_rn(kf, cp[5], cp[4]);
+    const float r = __fdividef(1.0f, w);
+    return bilinear_in(R, __fmul_rn(u, r), __fmul_rn(v, r));
 }
 
-// This block's share of the cost of trial t (one warp): the samples
-// k0 <= k < k1 (at most 32, one per lane) over the valid cuts, taken four
-// cuts at a time so that their reads overlap.  Per sample the cut values are
-// shifted by the first valid cut's value before the FP32 sums (the cost term
-// n * sum(d^2) - (sum d)^2 does not change under a common shift, and the
-// shifted sums stay small); the per-sample terms are summed in FP64.
-__device__ double trial_partial(const Shared& S, const Roi& R, int t, uint32_t valid, int k0, int k1, int lane)
+// Sum over the 32 lanes (the same butterfly, so the same bits, everywhere).
+__device__ __forceinline__ double lane_sum(double v)
 {
-    const int n = __popc(valid);
-    const int k = k0 + lane;
-    double acc = 0.0;
-    if (n >= 2 && k < k1) {
-        float Hm[9];
 #pragma unroll
-        for (int i = 0; i < 9; ++i) Hm[i] = S.trialH[t][i];
-        const float kf = float(k);
-        float v0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per-chunk shares of the cost of trial t (one warp): chunks j0 .. j0+NCH-1
+// (those below nch), lane = sample within the chunk, over the valid cuts in
+// order, a few cuts at a time so that their reads overlap.  Per sample the
+// cut values are shifted by the first valid cut's value before the FP32 sums
+// (the term n * sum(d^2) - (sum d)^2 does not change under a common shift,
+// and the shifted sums stay small); out[q] is the chunk's FP64 lane sum.
+template <int NCH>
+__device__ void trial_partial(const Shared& S, const Roi& R, int t, uint32_t valid, int j0, int nch, int nS,
+                              int lane, double out[NCH])
+{
+    constexpr int G = NCH == 1 ? 4 : 2;  // cuts per step
+    const int n = __popc(valid);
+    float v0[NCH], s1[NCH], s2[NCH], kf[NCH];
+    bool act[NCH];
+#pragma unroll
+    for (int q = 0; q < NCH; ++q) {
+        const int k = (j0 + q) * kChunk + lane;
+        act[q] = j0 + q < nch && k < nS;
+        kf[q] = float(k);
+        v0[q] = s1[q] = s2[q] = 0.f;
+    }
+    if (n >= 2) {
         bool first = true;
         uint32_t m = valid;
         while (m) {
-            int c[4];
+            int c[G];
             int cnt = 0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                c[q] = m ? __ffs(m) - 1 : c[q > 0 ? q - 1 : 0];
+            for (int g = 0; g < G; ++g) {
+                c[g] = m ? __ffs(m) - 1 : c[g > 0 ? g - 1 : 0];
                 if (m) {
                     m &= m - 1;
                     ++cnt;
                 }
             }
-            float val[4];
+            float val[G][NCH];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) val[q] = cut_sample(S, R, t, c[q], kf, Hm);
+            for (int g = 0; g < G; ++g)
+#pragma unroll
+                for (int q = 0; q < NCH; ++q) val[g][q] = act[q] ? cut_sample(S, R, t, c[g], kf[q]) : 0.f;
             if (first) {
-                v0 = val[0];
+#pragma unroll
+                for (int q = 0; q < NCH; ++q) v0[q] = val[0][q];
                 first = false;
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (q < cnt) {
-                    const float d = val[q] - v0;
-                    s1 += d;
-                    s2 = fmaf(d, d, s2);
+            for (int g = 0; g < G; ++g) {
+                if (g < cnt) {
+#pragma unroll
+                    for (int q = 0; q < NCH; ++q) {
+                        const float d = __fsub_rn(val[g][q], v0[q]);
+                        s1[q] = __fadd_rn(s1[q], d);
+                        s2[q] = __fmaf_rn(d, d, s2[q]);
+                    }
                 }
             }
         }
-        acc = double(float(n) * s2 - s1 * s1);
     }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    return acc;
+    for (int q = 0; q < NCH; ++q) {
+        const double term =
+            (n >= 2 && act[q]) ? double(__fsub_rn(__fmul_rn(float(n), s2[q]), __fmul_rn(s1[q], s1[q]))) : 0.0;
+        out[q] = lane_sum(term);
+    }
 }
 
 // Identification.hpp:373-384
@@ -480,15 +529,19 @@ __device__ __forceinline__ void inverse_derivative(const float* Hi, const float*
 // Starts from the grid's center; a step that raises the cost is rejected and
 // the damping raised.  Stops when a step is below 1e-3 px, or after
 // gnIterations cost evaluations.
-template <class Cluster>
+template <int CL>
 __device__ void gn_refine(Shared& S, const IdentTask& T, const Roi& roi, const IdentParams& ip, uint32_t cutMask,
-                          int k0, int k1, Cluster& cluster)
+                          int crank)
 {
+    namespace cg = cooperative_groups;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int kWarps = kThreads / 32;
     const int nS = ip.nSamples;
+    const int nch = (nS + kChunk - 1) / kChunk;
     const float bs = ip.beginSig;
     const float den = float(nS) - 1.f;
+    // chunks of this block: all of them, or chunk `crank` in a cluster
+    const int j0 = CL == 1 ? 0 : crank;
+    const int j1 = CL == 1 ? nch : min(crank + 1, nch);
     if (tid == 0) {
         S.gTry[0] = S.cx;
         S.gTry[1] = S.cy;
@@ -528,96 +581,99 @@ __device__ void gn_refine(Shared& S, const IdentTask& T, const Roi& roi, const I
         }
         __syncthreads();
         const uint32_t valid = ~(S.oob | S.gOob) & cutMask;
-        // this block's samples: value and its derivatives along the center
-        const int k = k0 + lane;
-        for (int c = warp; c < T.ncuts; c += kWarps) {
-            if (!((valid >> c) & 1u) || k >= k1) continue;
-            float bx, by, db[2][2];
-            back_project(S.gHi, S.gdHi[0], S.gdHi[1], T.stop[c][0], T.stop[c][1], bx, by, db);
-            const float xs = bx * bs, ys = by * bs;
-            const float sx = (bx - xs) / den, sy = (by - ys) / den;
-            const float kf = float(k);
-            const float x = xs + kf * sx, y = ys + kf * sy;
-            const float t = bs + kf * (1.f - bs) / den;
-            const float* Hm = S.gH;
-            const float u = Hm[0] * x + Hm[1] * y + Hm[2];
-            const float v = Hm[3] * x + Hm[4] * y + Hm[5];
-            const float w = Hm[6] * x + Hm[7] * y + Hm[8];
-            const float r = __frcp_rn(w);
-            const float qx = u * r, qy = v * r;
-            float gx, gy;
-            const float val = bilinear_grad(roi, qx, qy, gx, gy);
-            float ds[2];
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const float* dH = S.gdH[q];
-                const float dxq = t * db[q][0], dyq = t * db[q][1];
-                const float du = dH[0] * x + dH[1] * y + dH[2] + Hm[0] * dxq + Hm[1] * dyq;
-                const float dv = dH[3] * x + dH[4] * y + dH[5] + Hm[3] * dxq + Hm[4] * dyq;
-                const float dw = dH[6] * x + dH[7] * y + dH[8] + Hm[6] * dxq + Hm[7] * dyq;
-                ds[q] = gx * (du - qx * dw) * r + gy * (dv - qy * dw) * r;
-            }
-            S.u.gn.s[c][lane] = val;
-            S.u.gn.dx[c][lane] = ds[0];
-            S.u.gn.dy[c][lane] = ds[1];
-        }
-        __syncthreads();
+        const int n = __popc(valid);
         const int par = it & 1;
-        if (warp == 0) {
-            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            const int n = __popc(valid);
-            if (k < k1 && n >= 2) {
-                float v0 = 0.f, s1 = 0.f, s2 = 0.f, a1 = 0.f, b1 = 0.f, aa = 0.f, ab = 0.f, bb = 0.f, ad = 0.f,
-                      bd = 0.f;
-                bool first = true;
-                uint32_t m = valid;
-                while (m) {
-                    const int c = __ffs(m) - 1;
-                    m &= m - 1;
-                    const float v = S.u.gn.s[c][lane], a = S.u.gn.dx[c][lane], b = S.u.gn.dy[c][lane];
-                    if (first) {
-                        v0 = v;
-                        first = false;
-                    }
-                    const float d = v - v0;
-                    s1 += d;
-                    s2 = fmaf(d, d, s2);
-                    a1 += a;
-                    b1 += b;
-                    aa = fmaf(a, a, aa);
-                    ab = fmaf(a, b, ab);
-                    bb = fmaf(b, b, bb);
-                    ad = fmaf(a, d, ad);
-                    bd = fmaf(b, d, bd);
+        for (int j = j0; j < j1; ++j) {
+            // this chunk's samples: value and its derivatives along the center
+            const int k = j * kChunk + lane;
+            for (int c = warp; c < T.ncuts; c += kWarps) {
+                if (!((valid >> c) & 1u) || k >= nS) continue;
+                float bx, by, db[2][2];
+                back_project(S.gHi, S.gdHi[0], S.gdHi[1], T.stop[c][0], T.stop[c][1], bx, by, db);
+                const float xs = bx * bs, ys = by * bs;
+                const float sx = (bx - xs) / den, sy = (by - ys) / den;
+                const float kf = float(k);
+                const float x = __fmaf_rn(kf, sx, xs), y = __fmaf_rn(kf, sy, ys);
+                const float t = bs + kf * (1.f - bs) / den;
+                const float* Hm = S.gH;
+                const float u = hrow(Hm, 0, x, y), v = hrow(Hm, 1, x, y), w = hrow(Hm, 2, x, y);
+                const float r = __frcp_rn(w);
+                const float qx = __fmul_rn(u, r), qy = __fmul_rn(v, r);
+                float gx, gy;
+                const float val = bilinear_grad(roi, qx, qy, gx, gy);
+                float ds[2];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const float* dH = S.gdH[q];
+                    const float dxq = __fmul_rn(t, db[q][0]), dyq = __fmul_rn(t, db[q][1]);
+                    const float du = __fmaf_rn(Hm[0], dxq, __fmaf_rn(Hm[1], dyq, hrow(dH, 0, x, y)));
+                    const float dv = __fmaf_rn(Hm[3], dxq, __fmaf_rn(Hm[4], dyq, hrow(dH, 1, x, y)));
+                    const float dw = __fmaf_rn(Hm[6], dxq, __fmaf_rn(Hm[7], dyq, hrow(dH, 2, x, y)));
+                    const float ex = __fmul_rn(__fmaf_rn(-qx, dw, du), r);
+                    const float ey = __fmul_rn(__fmaf_rn(-qy, dw, dv), r);
+                    ds[q] = __fmaf_rn(gx, ex, __fmul_rn(gy, ey));
                 }
-                const float fn = float(n);
-                acc[0] = double(fn * s2 - s1 * s1);
-                acc[1] = double(ad - a1 * s1 / fn);
-                acc[2] = double(bd - b1 * s1 / fn);
-                acc[3] = double(aa - a1 * a1 / fn);
-                acc[4] = double(ab - a1 * b1 / fn);
-                acc[5] = double(bb - b1 * b1 / fn);
+                S.u.gn.s[c][lane] = val;
+                S.u.gn.dx[c][lane] = ds[0];
+                S.u.gn.dy[c][lane] = ds[1];
             }
+            __syncthreads();
+            if (warp == 0) {
+                double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if (k < nS && n >= 2) {
+                    float v0 = 0.f, s1 = 0.f, s2 = 0.f, a1 = 0.f, b1 = 0.f, aa = 0.f, ab = 0.f, bb = 0.f, ad = 0.f,
+                          bd = 0.f;
+                    bool first = true;
+                    uint32_t m = valid;
+                    while (m) {
+                        const int c = __ffs(m) - 1;
+                        m &= m - 1;
+                        const float v = S.u.gn.s[c][lane], a = S.u.gn.dx[c][lane], b = S.u.gn.dy[c][lane];
+                        if (first) {
+                            v0 = v;
+                            first = false;
+                        }
+                        const float d = __fsub_rn(v, v0);
+                        s1 = __fadd_rn(s1, d);
+                        s2 = __fmaf_rn(d, d, s2);
+                        a1 = __fadd_rn(a1, a);
+                        b1 = __fadd_rn(b1, b);
+                        aa = __fmaf_rn(a, a, aa);
+                        ab = __fmaf_rn(a, b, ab);
+                        bb = __fmaf_rn(b, b, bb);
+                        ad = __fmaf_rn(a, d, ad);
+                        bd = __fmaf_rn(b, d, bd);
+                    }
+                    const float fn = float(n);
+                    acc[0] = double(__fsub_rn(__fmul_rn(fn, s2), __fmul_rn(s1, s1)));
+                    acc[1] = double(__fsub_rn(ad, __fdiv_rn(__fmul_rn(a1, s1), fn)));
+                    acc[2] = double(__fsub_rn(bd, __fdiv_rn(__fmul_rn(b1, s1), fn)));
+                    acc[3] = double(__fsub_rn(aa, __fdiv_rn(__fmul_rn(a1, a1), fn)));
+                    acc[4] = double(__fsub_rn(ab, __fdiv_rn(__fmul_rn(a1, b1), fn)));
+                    acc[5] = double(__fsub_rn(bb, __fdiv_rn(__fmul_rn(b1, b1), fn)));
+                }
 #pragma unroll
-            for (int j = 0; j < 6; ++j) {
+                for (int q = 0; q < 6; ++q) acc[q] = lane_sum(acc[q]);
+                if (lane == 0)
 #pragma unroll
-                for (int o = 16; o; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+                    for (int q = 0; q < 6; ++q) S.gPart[par][j][q] = acc[q];
             }
-            if (lane == 0)
-#pragma unroll
-                for (int j = 0; j < 6; ++j) S.gPart[par][j] = acc[j];
+            __syncthreads();
         }
-        // every block's sums are in; a parity's array is rewritten two
-        // evaluations later, past the next cluster barrier
-        cluster.sync();
+        // every chunk's sums are in; a parity's array is rewritten two
+        // evaluations later, past the next barrier of the cluster
+        if constexpr (CL > 1) cg::this_cluster().sync();
         if (warp == 0 && lane < 6) {
             double a = 0.0;
-            for (int q = 0; q < kCluster; ++q) a += cluster.map_shared_rank(&S.gPart[par][0], q)[lane];
+            for (int j = 0; j < nch; ++j) {
+                const double* src = &S.gPart[par][j][0];
+                if constexpr (CL > 1) src = cg::this_cluster().map_shared_rank(src, j);
+                a += src[lane];
+            }
             S.gSum[lane] = a;
         }
         __syncthreads();
         if (tid == 0) {
-            const int n = __popc(valid);
             const double cost = n >= 2 ? S.gSum[0] / (0.5 * double(n) * double(n - 1)) : DBL_MAX;
             ++S.iterations;
             if (n >= 2 && (!S.gHave || cost < S.gBest)) {
@@ -660,22 +716,25 @@ __device__ void gn_refine(Shared& S, const IdentTask& T, const Roi& roi, const I
 
 }  // namespace
 
-__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
+// CL = 1: one block per marker; CL = kCluster: a cluster of blocks per marker
+// (launched with that cluster dimension), block r on sample chunk r.
+template <int CL>
+__global__ void __launch_bounds__(kThreads)
     k_identify(const uint8_t* __restrict__ img, size_t pitch, const IdentTask* __restrict__ tasks, IdentResult* res,
                const float* __restrict__ bankInv, IdentParams ip)
 {
     namespace cg = cooperative_groups;
     __shared__ Shared S;
-    cg::cluster_group cluster = cg::this_cluster();
-    const int crank = int(cluster.block_rank());
-    const int marker = blockIdx.x / kCluster;
+    int crank = 0;
+    if constexpr (CL > 1) crank = int(cg::this_cluster().block_rank());
+    const int marker = blockIdx.x / CL;
     const IdentTask& T = tasks[marker];
     const Roi roi = make_roi(img, pitch, T);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nS = ip.nSamples;
-    // this block's samples along every cut (at most 32: one per lane)
-    const int chunk = (nS + kCluster - 1) / kCluster;
-    const int k0 = min(nS, crank * chunk), k1 = min(nS, k0 + chunk);
+    const int nch = (nS + kChunk - 1) / kChunk;
+    constexpr int NCH = CL == 1 ? kMaxChunks : 1;  // chunks this block evaluates
+    const int j0 = CL == 1 ? 0 : crank;
     const int gridN = ip.gridN;
     const int nTrials = gridN * gridN;
     const uint32_t cutMask = (T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u);
@@ -734,50 +793,71 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
             setup_trial(S, T, warp, px, py, ip, roi, lane);
         }
         __syncthreads();
-        if (tid == 0) {
-            uint32_t m = S.oob;
-            for (int t = 0; t < nTrials; ++t) {
-                m |= S.trialOob[t];
-                S.valid[t] = ~m & cutMask;
+        // sticky out-of-bounds flags in trial order: inclusive OR scan
+        if (warp == 0) {
+            uint32_t m = lane < nTrials ? S.trialOob[lane] : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, m, o);
+                if (lane >= o) m |= v;
             }
-            S.oob = m;
+            m |= S.oob;
+            if (lane < nTrials) S.valid[lane] = ~m & cutMask;
+            const uint32_t last = __shfl_sync(0xffffffffu, m, nTrials - 1);
+            __syncwarp();
+            if (lane == 0) S.oob = last;
         }
         __syncthreads();
         const int par = round & 1;
         if (warp < nTrials) {
-            const double c = trial_partial(S, roi, warp, S.valid[warp], k0, k1, lane);
-            if (lane == 0) S.part[par][warp] = c;
+            double c[NCH];
+            trial_partial<NCH>(S, roi, warp, S.valid[warp], j0, nch, nS, lane, c);
+            if (lane == 0)
+#pragma unroll
+                for (int q = 0; q < NCH; ++q)
+                    if (j0 + q < nch) S.part[par][j0 + q][warp] = c[q];
         }
-        // All blocks of the marker have their shares; a block reuses this
-        // parity's array two rounds later, after the next cluster barrier,
-        // when every block has finished reading it.
-        cluster.sync();
-        if (warp == 0 && lane < nTrials) {
+        // All chunks of the marker are in; a block rewrites this parity's
+        // array two rounds later, after the next cluster barrier, when every
+        // block has finished reading it.
+        if constexpr (CL > 1) cg::this_cluster().sync();
+        else __syncthreads();
+        if (warp == 0) {
             double acc = 0.0;
-            for (int r = 0; r < kCluster; ++r) acc += cluster.map_shared_rank(&S.part[par][0], r)[lane];
-            const int n = __popc(S.valid[lane]);
-            S.cost[lane] = n >= 2 ? float(acc / (0.5 * double(n) * double(n - 1))) : FLT_MAX;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            // imageCenterOptimizationGlob: first strict minimum in trial order.
-            float best = FLT_MAX;
-            int bi = -1;
-            bool readable = false;
-            for (int t = 0; t < nTrials; ++t) {
-                if (__popc(S.valid[t]) >= 2) readable = true;
-                if (S.cost[t] < best) {
-                    best = S.cost[t];
-                    bi = t;
+            if (lane < nTrials)
+                for (int j = 0; j < nch; ++j) {
+                    const double* src = &S.part[par][j][0];
+                    if constexpr (CL > 1) src = cg::this_cluster().map_shared_rank(src, j);
+                    acc += src[lane];
                 }
+            const int n = lane < nTrials ? __popc(S.valid[lane]) : 0;
+            const float cost = n >= 2 ? float(acc / (0.5 * double(n) * double(n - 1))) : FLT_MAX;
+            if (lane < nTrials) S.cost[lane] = cost;
+            // imageCenterOptimizationGlob: first strict minimum in trial order
+            // (costs below FLT_MAX; key = orderable cost bits, then index)
+            unsigned long long key = ~0ull;
+            if (lane < nTrials && cost < FLT_MAX) {
+                const uint32_t b = __float_as_uint(cost);
+                const uint32_t ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+                key = (static_cast<unsigned long long>(ord) << 32) | unsigned(lane);
             }
-            if (!readable || bi < 0) {
-                S.fail = 1;
-            } else {
-                S.cx = S.trialPt[bi][0];
-                S.cy = S.trialPt[bi][1];
-                for (int k = 0; k < 9; ++k) S.Hopt[k] = S.trialH[bi][k];
-                S.minRes = best;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+                key = k2 < key ? k2 : key;
+            }
+            const bool readable = __any_sync(0xffffffffu, n >= 2);
+            __syncwarp();
+            if (lane == 0) {
+                if (!readable || key == ~0ull) {
+                    S.fail = 1;
+                } else {
+                    const int bi = int(key & 0xffffffffull);
+                    S.cx = S.trialPt[bi][0];
+                    S.cy = S.trialPt[bi][1];
+                    for (int k = 0; k < 9; ++k) S.Hopt[k] = S.trialH[bi][k];
+                    S.minRes = S.cost[bi];
+                }
             }
         }
         __syncthreads();
@@ -785,11 +865,13 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
         ns /= float((gridN - 1) / 2);
     }
     if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON && !S.fail && S.rounds > 0)
-        gn_refine(S, T, roi, ip, cutMask, k0, k1, cluster);
+        gn_refine<CL>(S, T, roi, ip, cutMask, crank);
     // No block leaves while another may still read its shared memory; the
     // rest of the identification runs in the first block of the cluster.
-    cluster.sync();
-    if (crank != 0) return;
+    if constexpr (CL > 1) {
+        cg::this_cluster().sync();
+        if (crank != 0) return;
+    }
     IdentResult& R = res[marker];
     if (S.fail || S.rounds == 0) {
         if (tid == 0) {
@@ -806,7 +888,6 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
         return;
     }
     // Final signals with the optimal homography (getSignals, Identification.cpp:901).
-    constexpr int kWarps = kThreads / 32;
     for (int c = warp; c < T.ncuts; c += kWarps) {
         float Hi[9];
         mat_inv(S.Hopt, Hi);
@@ -1004,7 +1085,6 @@ __global__ void __launch_bounds__(kThreads) k_cut_cost(const uint8_t* __restrict
     const IdentTask& T = tasks[blockIdx.x];
     const Roi roi = make_roi(img, pitch, T);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int kWarps = kThreads / 32;
     const int nS = ip.nSamples;
     const float bs = ip.beginSig;
     const float den = float(nS) - 1.f;
@@ -1188,8 +1268,29 @@ void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_task
         throw Error{CCTAGB_BAD_ARG, "gnIterations must be in [1, 100]"};
     if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON && (ip.coarseRounds < 1 || ip.coarseRounds > 64))
         throw Error{CCTAGB_BAD_ARG, "gnCoarseRounds must be in [1, 64]"};
-    k_identify<<<n * kCluster, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_res, d_bank_inv, ip);
-    CCTAGB_CUDA(cudaGetLastError());
+    // Few markers: a cluster of blocks each, so that a launch spreads over
+    // the SMs; many: one block each (the per-chunk sums are the same bits).
+    int dev = 0, sms = 0;
+    CCTAGB_CUDA(cudaGetDevice(&dev));
+    CCTAGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (n * kCluster <= sms) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(n * kCluster));
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kCluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CCTAGB_CUDA(cudaLaunchKernelEx(&cfg, k_identify<kCluster>, d_img, pitch, d_tasks, d_res, d_bank_inv, ip));
+    } else {
+        k_identify<1><<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_res, d_bank_inv, ip);
+        CCTAGB_CUDA(cudaGetLastError());
+    }
 }
 
 void launch_cut_cost(const uint8_t* d_img, size_t pitch, const IdentTask* d_tasks, const float* d_centers,

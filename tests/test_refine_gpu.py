@@ -109,3 +109,17 @@ def test_task_outside_the_image_is_rejected(detector, scene):
     with pytest.raises(cctag_b200.CCTagError) as e:
         detector.identify_tasks(d.data_ptr(), 1280, 720, 1280, [bad], capi.REFINE_GRID)
     assert e.value.status == capi.BAD_ARG
+
+
+@pytest.mark.parametrize("mode", [capi.REFINE_GRID, capi.REFINE_GAUSS_NEWTON])
+def test_few_and_many_candidates_give_the_same_bits(detector, scene, mode):
+    """A handful of candidates runs as clusters of blocks, thousands as one
+    block each; both sum the same per-chunk terms in the same order."""
+    f, tasks = scene
+    d = to_device(f.image)
+    few = detector.identify_tasks(d.data_ptr(), 1280, 720, 1280, tasks, mode)
+    many = detector.identify_tasks(d.data_ptr(), 1280, 720, 1280, tasks * 64, mode)
+    for i, a in enumerate(few):
+        for b in many[i::len(tasks)]:
+            assert (a.status, a.id, a.x, a.y, a.residual, a.iterations) == \
+                (b.status, b.id, b.x, b.y, b.residual, b.iterations)
