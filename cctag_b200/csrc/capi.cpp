@@ -14,24 +14,21 @@
 #include "pipeline.hpp"
 
 struct cctagb_handle {
+    std::shared_ptr<cctagb::ThreadPool> pool;     // host workers shared by every slot
     std::unique_ptr<cctagb::Detector> det;        // slot 0: every single-frame call
     std::vector<std::unique_ptr<cctagb::Detector>> extra;  // slots 1..: cctagb_detect_batch
     cctagb_params params{};
     int max_w = 0, max_h = 0, max_batch = 1, device = 0;
     std::string last_error;
 
-    int slots() const { return std::max(1, std::min(max_batch, 8)); }
-    // Detection slots for a batch: own device buffers, stream and host pool,
-    // the host threads shared out between the slots.
-    static int workers_per_slot(int n)
-    {
-        const int hc = int(std::max(1u, std::thread::hardware_concurrency()));
-        return std::max(0, std::min(7, hc / n - 1));
-    }
+    int slots() const { return std::max(1, std::min(max_batch, kMaxSlots)); }
+    static constexpr int kMaxSlots = 32;
+    // Detection slots for a batch: own device buffers and stream, the host
+    // pool shared.
     void ensure_slots(int n)
     {
         while (int(extra.size()) + 1 < n) {
-            extra.emplace_back(new cctagb::Detector(params, max_w, max_h, 1, workers_per_slot(n)));
+            extra.emplace_back(new cctagb::Detector(params, max_w, max_h, 1, pool));
             copy_bank(*extra.back());
         }
     }
@@ -155,7 +152,10 @@ cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int ma
     h->max_h = max_h;
     h->max_batch = max_batch;
     cudaGetDevice(&h->device);
-    const cctagb_status s = guarded(h.get(), [&] { h->det.reset(new cctagb::Detector(*p, max_w, max_h, max_batch)); });
+    const cctagb_status s = guarded(h.get(), [&] {
+        h->pool = cctagb::make_host_pool();
+        h->det.reset(new cctagb::Detector(*p, max_w, max_h, max_batch, h->pool));
+    });
     if (s != CCTAGB_OK) return s;
     *out = h.release();
     return CCTAGB_OK;
@@ -339,8 +339,6 @@ cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)
     return guarded(h, [&] {
         const int S = std::min(n, h->slots());
         h->ensure_slots(S);
-        const int workers = cctagb_handle::workers_per_slot(S);
-        for (int s = 0; s < S; ++s) h->slot(s).set_host_workers(workers);
         for (int i = 0; i < n; ++i) {
             frames[i].n_out = 0;
             frames[i].status = CCTAGB_INTERNAL;
@@ -374,7 +372,6 @@ cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)
         for (int s = 1; s < S; ++s) threads.emplace_back(run, s);
         run(0);
         for (auto& t : threads) t.join();
-        h->det->set_host_workers(h->det->host_workers_max());
         for (int i = 0; i < n; ++i)
             if (frames[i].status != CCTAGB_OK)
                 throw cctagb::Error{frames[i].status, "frame " + std::to_string(i) + ": " + msg[size_t(i)]};

@@ -16,8 +16,8 @@
 
 namespace cctagb {
 
-Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, int host_workers)
-    : params_(p), pipe_(p, max_w, max_h, max_batch)
+Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, std::shared_ptr<ThreadPool> pool)
+    : params_(p), pipe_(p, max_w, max_h, max_batch), pool_(std::move(pool))
 {
     CCTAGB_CUDA(cudaMalloc(&d_bank_inv_, sizeof(float) * kMaxBankIds * kMaxBankRatios));
     if (p.nCrowns == 3) {
@@ -35,11 +35,7 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, 
     ensure_ident_capacity(256);
     hl_.resize(idxmaps_.size());
     es_.resize(idxmaps_.size());
-    if (host_workers < 0) {
-        const unsigned hc = std::thread::hardware_concurrency();
-        host_workers = int(std::min(7u, hc > 1 ? hc - 1 : 0u));
-    }
-    pool_.reset(new ThreadPool(host_workers));
+    if (!pool_) pool_ = make_host_pool();
 }
 
 Detector::~Detector()

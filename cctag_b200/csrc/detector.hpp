@@ -15,18 +15,15 @@ namespace cctagb {
 
 class Detector {
 public:
-    // host_workers: threads of the host candidate stage besides the caller
-    // (-1: min(7, cores - 1)).
-    Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, int host_workers = -1);
+    // pool: the host worker pool (shared by the detectors of a handle); null
+    // makes one with a thread per core besides the caller.
+    Detector(const cctagb_params& p, int max_w, int max_h, int max_batch,
+             std::shared_ptr<ThreadPool> pool = nullptr);
     ~Detector();
     Detector(const Detector&) = delete;
     Detector& operator=(const Detector&) = delete;
 
     Pipeline& pipeline() { return pipe_; }
-    // Host threads of the candidate stage besides the caller (at most the
-    // number the detector was created with).
-    void set_host_workers(int n) { pool_->set_active(n); }
-    int host_workers_max() const { return pool_->size(); }
     void set_bank(const float* ratios, int n_ids, int n_ratios);
     const std::vector<std::vector<float>>& bank() const { return bank_; }
 
@@ -57,7 +54,7 @@ private:
     std::vector<std::vector<int32_t>> idxmaps_;  // per level, -1 where no edge point
     std::vector<HostLevel> hl_;                  // per level, pinned downloads
     std::vector<EdgeSet> es_;                    // per level, candidate-stage state
-    std::unique_ptr<ThreadPool> pool_;
+    std::shared_ptr<ThreadPool> pool_;
     std::vector<uint8_t> frame_host_;
     float* d_bank_inv_ = nullptr;                // kMaxBankIds x kMaxBankRatios
     IdentTask* d_tasks_ = nullptr;

@@ -1,10 +1,15 @@
-// Small persistent worker pool for the host stages (one per handle).
+// Persistent worker pool for the host stages, shared by all detection slots
+// of a handle.  Several threads may run parallel_for at once: each call is a
+// job, its caller works on it, and idle workers take tasks from any job that
+// still has some (round robin), so a frame with more work left gets more
+// threads while other frames wait on the GPU.
 #pragma once
 
 #include <algorithm>
 #include <condition_variable>
 #include <exception>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -13,9 +18,9 @@ namespace cctagb {
 
 class ThreadPool {
 public:
-    explicit ThreadPool(int n) : active_(n)
+    explicit ThreadPool(int n)
     {
-        for (int i = 0; i < n; ++i) workers_.emplace_back([this, i] { loop(i); });
+        for (int i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
     }
     ~ThreadPool()
     {
@@ -26,90 +31,107 @@ public:
         cv_.notify_all();
         for (auto& t : workers_) t.join();
     }
+    ThreadPool(const ThreadPool&) = delete;
+    ThreadPool& operator=(const ThreadPool&) = delete;
     int size() const { return int(workers_.size()); }
-    // Only the first n workers take part in later parallel_for calls (the
-    // others stay idle); n is clamped to [0, size()].
-    void set_active(int n)
-    {
-        std::lock_guard<std::mutex> l(mu_);
-        active_ = std::max(0, std::min(n, size()));
-    }
 
-    // Runs fn(i) for i in [0, n) on the workers and the calling thread; the
-    // first exception thrown by a task is rethrown here.
+    // Runs fn(i) for i in [0, n) on the calling thread and idle workers; the
+    // first exception thrown by a task is rethrown here.  Tasks must not call
+    // parallel_for themselves.
     void parallel_for(int n, const std::function<void(int)>& fn)
     {
         if (n <= 0) return;
-        if (n == 1 || workers_.empty() || active_ == 0) {
+        if (n == 1 || workers_.empty()) {
             for (int i = 0; i < n; ++i) fn(i);
             return;
         }
+        Job job;
+        job.fn = &fn;
+        job.total = n;
         {
             std::lock_guard<std::mutex> l(mu_);
-            fn_ = &fn;
-            next_ = 0;
-            total_ = n;
-            done_ = 0;
-            err_ = nullptr;
-            ++gen_;
+            jobs_.push_back(&job);
         }
         cv_.notify_all();
-        work();
+        for (;;) {
+            int i;
+            {
+                std::lock_guard<std::mutex> l(mu_);
+                if (job.next >= job.total) break;
+                i = job.next++;
+            }
+            run(&job, i);
+        }
         std::unique_lock<std::mutex> l(mu_);
-        done_cv_.wait(l, [&] { return done_ == total_; });
-        fn_ = nullptr;
-        if (err_) std::rethrow_exception(err_);
+        job.cv.wait(l, [&] { return job.done == job.total; });
+        jobs_.erase(std::find(jobs_.begin(), jobs_.end(), &job));
+        if (job.err) std::rethrow_exception(job.err);
     }
 
 private:
-    void work()
+    struct Job {
+        const std::function<void(int)>* fn = nullptr;
+        int next = 0, total = 0, done = 0;
+        std::exception_ptr err;
+        std::condition_variable cv;
+    };
+
+    // Under the lock: a job with tasks left, starting after the last one
+    // served.
+    Job* pick()
     {
-        for (;;) {
-            int i;
-            const std::function<void(int)>* f;
-            {
-                std::lock_guard<std::mutex> l(mu_);
-                if (!fn_ || next_ >= total_) return;
-                i = next_++;
-                f = fn_;
-            }
-            try {
-                (*f)(i);
-            } catch (...) {
-                std::lock_guard<std::mutex> l(mu_);
-                if (!err_) err_ = std::current_exception();
-            }
-            {
-                std::lock_guard<std::mutex> l(mu_);
-                if (++done_ == total_) done_cv_.notify_all();
+        const size_t n = jobs_.size();
+        for (size_t k = 0; k < n; ++k) {
+            Job* j = jobs_[(rr_ + k) % n];
+            if (j->next < j->total) {
+                rr_ = (rr_ + k + 1) % n;
+                return j;
             }
         }
+        return nullptr;
     }
-    void loop(int index)
+
+    void run(Job* job, int i)
     {
-        unsigned seen = 0;
+        std::exception_ptr err;
+        try {
+            (*job->fn)(i);
+        } catch (...) {
+            err = std::current_exception();
+        }
+        std::lock_guard<std::mutex> l(mu_);
+        if (err && !job->err) job->err = err;
+        if (++job->done == job->total) job->cv.notify_all();
+    }
+
+    void loop()
+    {
         for (;;) {
-            bool take_part;
+            Job* job;
+            int i;
             {
                 std::unique_lock<std::mutex> l(mu_);
-                cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+                cv_.wait(l, [&] { return stop_ || (job = pick()) != nullptr; });
                 if (stop_) return;
-                seen = gen_;
-                take_part = index < active_;
+                i = job->next++;
             }
-            if (take_part) work();
+            run(job, i);
         }
     }
 
     std::vector<std::thread> workers_;
     std::mutex mu_;
-    std::condition_variable cv_, done_cv_;
-    const std::function<void(int)>* fn_ = nullptr;
-    int next_ = 0, total_ = 0, done_ = 0;
-    int active_ = 0;
-    unsigned gen_ = 0;
+    std::condition_variable cv_;
+    std::vector<Job*> jobs_;
+    size_t rr_ = 0;
     bool stop_ = false;
-    std::exception_ptr err_;
 };
+
+// A pool with one worker per core besides the caller (at most 63).
+inline std::shared_ptr<ThreadPool> make_host_pool()
+{
+    const unsigned hc = std::thread::hardware_concurrency();
+    return std::make_shared<ThreadPool>(int(std::min(63u, hc > 1 ? hc - 1 : 0u)));
+}
 
 }  // namespace cctagb

@@ -177,7 +177,7 @@ typedef struct cctagb_frame {
 } cctagb_frame;
 
 /* Detection of n independent frames (cameras), of any sizes up to the
- * handle's max_w x max_h.  The handle runs min(max_batch, 8) detection slots,
+ * handle's max_w x max_h.  The handle runs min(max_batch, 32) detection slots,
  * each with its own device buffers and stream, so one frame's host candidate
  * stage overlaps other frames' GPU stages; every frame's result equals that
  * of cctagb_detect on the same frame.  Returns CCTAGB_OK when every frame
