@@ -371,6 +371,27 @@ def run_b200(args, rank, world, local):
     return line
 
 
+def run_plain(args, torch, local):
+    """Single-frame detections of the configuration's frames, one per call
+    (cctagb_detect_device), for profiling one frame's kernels."""
+    import cctag_b200
+
+    frames = make_frames(args.config, n=max(1, min(args.steps, N_FRAMES)))
+    H, W = frames[0].shape
+    det = cctag_b200.Detector(max_w=W, max_h=H)
+    d = [torch.from_numpy(f).to(f"cuda:{local}") for f in frames]
+    for i in range(args.warmup):
+        det.detect_device(d[i % len(d)].data_ptr(), W, H, W)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        det.detect_device(d[i % len(d)].data_ptr(), W, H, W)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    det.close()
+    return {"frames": args.steps, "ms_per_frame_wall": round(dt * 1e3 / args.steps, 3), "frame": f"{W}x{H}"}
+
+
 def run_c5(args, torch):
     """Candidate refinement: 4096 candidates (256 distinct crops, r 8-150 px,
     tilt <= 70 deg, noise 2-12) in one atlas, identified per call with the
@@ -564,7 +585,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the multi-camera (mixed resolution) leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the candidate-refinement leg")
-    ap.add_argument("--leg", default="all", choices=["all", "c4", "c5"],
+    ap.add_argument("--leg", default="all", choices=["all", "plain", "c4", "c5"],
                     help="run one secondary leg alone and print its object (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -582,6 +603,8 @@ def main():
         torch.cuda.set_device(local)
         if args.leg == "c5":
             print(json.dumps({"c5_refine": run_c5(args, torch)}))
+        elif args.leg == "plain":
+            print(json.dumps({"plain": run_plain(args, torch, local)}))
         else:
             flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
             print(json.dumps({"c4_cameras": run_c4(args, flush, torch)}))
