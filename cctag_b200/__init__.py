@@ -27,6 +27,9 @@ class Detector:
         if st != capi.OK:
             raise CCTagError(st, f"cctagb_create failed: {self._lib.cctagb_status_string(st).decode()}")
         self._h = h
+        self.max_w, self.max_h = int(max_w), int(max_h)
+        self._tickets: dict = {}   # ticket -> key of the host frame kept alive until waited
+        self._inflight: dict = {}
 
     # -- lifecycle ---------------------------------------------------------
     def close(self):
@@ -182,6 +185,47 @@ class Detector:
             fr[i].cap = cap
         self._check(self._lib.cctagb_detect_batch(self._h, fr, n), "detect_batch")
         return [([outs[i][k] for k in range(fr[i].n_out)], fr[i].stats) for i in range(n)]
+
+    # -- streaming ingest --------------------------------------------------------
+    def host_frames(self, n: int):
+        """n pinned frame buffers owned by the handle, as (max_h, max_w) uint8 arrays."""
+        ptrs = (C.c_void_p * n)()
+        self._check(self._lib.cctagb_host_frames(self._h, n, ptrs), "host_frames")
+        size = self.max_w * self.max_h
+        return [np.ctypeslib.as_array((C.c_uint8 * size).from_address(p)).reshape(self.max_h, self.max_w)
+                for p in ptrs]
+
+    def submit(self, gray, frame_id: int = 0, w: int | None = None, h: int | None = None, pitch: int | None = None,
+               is_device: bool = False) -> int:
+        """cctagb_submit: a host numpy frame (kept alive until waited) or a
+        device pointer with w/h/pitch; returns the ticket."""
+        t = C.c_int()
+        if isinstance(gray, np.ndarray):
+            g = gray if gray.flags["C_CONTIGUOUS"] and gray.dtype == np.uint8 else np.ascontiguousarray(gray, np.uint8)
+            hh, ww = g.shape
+            ptr, pitch, is_device = g.ctypes.data, int(g.strides[0]), False
+            self._inflight[id(g)] = g
+        else:
+            ptr, ww, hh = int(gray), int(w), int(h)
+            pitch = int(pitch if pitch is not None else ww)
+        self._check(self._lib.cctagb_submit(self._h, C.c_void_p(ptr), ww, hh, pitch, int(is_device), frame_id,
+                                            C.byref(t)), "submit")
+        if isinstance(gray, np.ndarray):
+            self._tickets[t.value] = id(g)
+        return t.value
+
+    def wait(self, ticket: int, cap: int = 256):
+        """cctagb_wait: (markers, stats) of a submitted frame."""
+        out = (capi.Marker * cap)()
+        n = C.c_int()
+        stats = capi.Stats()
+        try:
+            self._check(self._lib.cctagb_wait(self._h, ticket, out, cap, C.byref(n), C.byref(stats)), "wait")
+        finally:
+            key = self._tickets.pop(ticket, None)
+            if key is not None:
+                self._inflight.pop(key, None)
+        return [out[i] for i in range(n.value)], stats
 
     # -- identification of caller-given candidates ---------------------------
     def last_tasks(self):

@@ -90,6 +90,9 @@ SIGNATURES = {
     "cctagb_detect": (_I, [_P, _P, _I, _I, _SZ, _I, _P, _I, C.POINTER(_I), _P]),
     "cctagb_detect_device": (_I, [_P, _P, _I, _I, _SZ, _I, _P, _I, C.POINTER(_I), _P]),
     "cctagb_detect_batch": (_I, [_P, _P, _I]),
+    "cctagb_host_frames": (_I, [_P, _I, C.POINTER(_P)]),
+    "cctagb_submit": (_I, [_P, _P, _I, _I, _SZ, _I, _I, C.POINTER(_I)]),
+    "cctagb_wait": (_I, [_P, _I, _P, _I, C.POINTER(_I), _P]),
     "cctagb_last_tasks": (_I, [_P, _P, _I, C.POINTER(_I)]),
     "cctagb_identify_tasks": (_I, [_P, _P, _I, _I, _SZ, _P, _I, _I, _P]),
     "cctagb_cut_cost": (_I, [_P, _P, _I, _I, _SZ, _P, _I, _P, _P, _P, _P]),

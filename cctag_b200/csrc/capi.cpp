@@ -2,8 +2,12 @@
 // status codes; nothing crosses the ABI as a C++ exception.
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -12,6 +16,24 @@
 #include "cctag_b200.h"
 #include "detector.hpp"
 #include "pipeline.hpp"
+
+namespace {
+
+// One frame handed to cctagb_submit, and what its detection returned.
+struct Ticket {
+    const uint8_t* gray = nullptr;
+    int w = 0, h = 0;
+    size_t pitch = 0;
+    int is_device = 0, frame_id = 0;
+    bool done = false;
+    cctagb_status status = CCTAGB_OK;
+    std::string msg;
+    std::vector<cctagb_marker> markers;
+    int n = 0;
+    cctagb_stats stats{};
+};
+
+}  // namespace
 
 struct cctagb_handle {
     std::shared_ptr<cctagb::ThreadPool> pool;     // host workers shared by every slot
@@ -41,6 +63,83 @@ struct cctagb_handle {
         d.set_bank(flat.data(), int(b.size()), int(b[0].size()));
     }
     cctagb::Detector& slot(int i) { return i == 0 ? *det : *extra[size_t(i - 1)]; }
+
+    // Streaming ingest (cctagb_submit / cctagb_wait): one worker thread per
+    // slot takes queued tickets in order.
+    std::vector<uint8_t*> host_frames;            // pinned, max_w * max_h bytes each
+    std::mutex smu;
+    std::condition_variable scv, sdone;
+    std::deque<int> queue;
+    std::map<int, std::shared_ptr<Ticket>> tickets;
+    std::vector<std::thread> sworkers;
+    int next_ticket = 1;
+    bool sstop = false;
+
+    void stream_worker(int s)
+    {
+        cudaSetDevice(device);
+        cctagb::Detector& d = slot(s);
+        for (;;) {
+            std::shared_ptr<Ticket> t;
+            {
+                std::unique_lock<std::mutex> l(smu);
+                scv.wait(l, [&] { return sstop || !queue.empty(); });
+                if (sstop) return;
+                t = tickets.at(queue.front());
+                queue.pop_front();
+            }
+            cctagb_status st = CCTAGB_OK;
+            std::string msg;
+            t->markers.resize(256);
+            for (int attempt = 0; attempt < 2; ++attempt) {
+                try {
+                    d.detect(t->gray, t->w, t->h, t->pitch, t->is_device != 0, t->frame_id, t->markers.data(),
+                             int(t->markers.size()), &t->n, &t->stats);
+                    st = CCTAGB_OK;
+                    msg.clear();
+                    break;
+                } catch (const cctagb::Error& e) {
+                    st = e.status;
+                    msg = e.msg;
+                    // more markers than the buffer holds: once more with room
+                    if (st != CCTAGB_BAD_ARG || t->n <= int(t->markers.size())) break;
+                    t->markers.resize(size_t(t->n));
+                } catch (const std::exception& e) {
+                    st = CCTAGB_INTERNAL;
+                    msg = e.what();
+                    break;
+                }
+            }
+            {
+                std::lock_guard<std::mutex> l(smu);
+                t->status = st;
+                t->msg = msg;
+                t->done = true;
+            }
+            sdone.notify_all();
+        }
+    }
+    void start_stream()
+    {
+        if (!sworkers.empty()) return;
+        const int S = slots();
+        ensure_slots(S);
+        for (int s = 0; s < S; ++s) sworkers.emplace_back([this, s] { stream_worker(s); });
+    }
+    bool streaming() const { return !tickets.empty(); }
+
+    ~cctagb_handle()
+    {
+        {
+            std::lock_guard<std::mutex> l(smu);
+            sstop = true;
+        }
+        scv.notify_all();
+        for (auto& t : sworkers) t.join();
+        if (det) cudaStreamSynchronize(det->pipeline().stream());
+        for (auto& d : extra) cudaStreamSynchronize(d->pipeline().stream());
+        for (uint8_t* p : host_frames) cudaFreeHost(p);
+    }
 };
 
 namespace {
@@ -65,6 +164,14 @@ cctagb_status guarded(cctagb_handle* h, F&& f)
         if (h) h->last_error = "unknown error";
         return CCTAGB_INTERNAL;
     }
+}
+
+// Slot 0 belongs to the streaming workers while tickets are outstanding.
+bool refuse_if_streaming(cctagb_handle* h)
+{
+    if (!h->streaming()) return false;
+    h->last_error = "tickets outstanding: wait for them first";
+    return true;
 }
 
 }  // namespace
@@ -173,6 +280,7 @@ const char* cctagb_last_error_string(const cctagb_handle* h) { return h ? h->las
 cctagb_status cctagb_set_bank(cctagb_handle* h, const float* ratios, int n_ids, int n_ratios)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] {
         h->det->set_bank(ratios, n_ids, n_ratios);
         for (auto& d : h->extra) d->set_bank(ratios, n_ids, n_ratios);
@@ -182,6 +290,7 @@ cctagb_status cctagb_set_bank(cctagb_handle* h, const float* ratios, int n_ids, 
 cctagb_status cctagb_image_stage(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int is_device)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->pipeline().image_stage(gray, w, hgt, pitch, is_device != 0); });
 }
 
@@ -270,6 +379,7 @@ cctagb_status cctagb_get_stream(cctagb_handle* h, void** stream)
 cctagb_status cctagb_set_stage_timing(cctagb_handle* h, int enable)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->pipeline().set_stage_timing(enable != 0); });
 }
 
@@ -289,6 +399,7 @@ cctagb_status cctagb_canny_from_derivatives(cctagb_handle* h, const int16_t* dx,
                                             uint8_t* edges)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->pipeline().canny_only(dx, dy, w, hgt, edges); });
 }
 
@@ -296,6 +407,7 @@ cctagb_status cctagb_detect(cctagb_handle* h, const uint8_t* gray, int w, int hg
                             cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->detect(gray, w, hgt, pitch, false, frame_id, out, cap, n_out, stats); });
 }
 
@@ -303,12 +415,82 @@ cctagb_status cctagb_detect_device(cctagb_handle* h, const uint8_t* d_gray, int 
                                    int frame_id, cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->detect(d_gray, w, hgt, pitch, true, frame_id, out, cap, n_out, stats); });
+}
+
+cctagb_status cctagb_host_frames(cctagb_handle* h, int n, uint8_t** out)
+{
+    if (!h || n < 0 || n > 64 || (n > 0 && !out)) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        const size_t bytes = size_t(h->max_w) * size_t(h->max_h);
+        while (int(h->host_frames.size()) < n) {
+            uint8_t* p = nullptr;
+            CCTAGB_CUDA(cudaMallocHost(&p, bytes));
+            h->host_frames.push_back(p);
+        }
+        for (int i = 0; i < n; ++i) out[i] = h->host_frames[size_t(i)];
+    });
+}
+
+cctagb_status cctagb_submit(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int is_device,
+                            int frame_id, int* ticket)
+{
+    if (!h || !gray || !ticket || w <= 0 || hgt <= 0 || pitch < size_t(w)) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        if (w > h->max_w || hgt > h->max_h) throw cctagb::Error{CCTAGB_TOO_LARGE, "frame larger than the handle"};
+        h->start_stream();
+        auto t = std::make_shared<Ticket>();
+        t->gray = gray;
+        t->w = w;
+        t->h = hgt;
+        t->pitch = pitch;
+        t->is_device = is_device;
+        t->frame_id = frame_id;
+        {
+            std::lock_guard<std::mutex> l(h->smu);
+            *ticket = h->next_ticket++;
+            h->tickets[*ticket] = t;
+            h->queue.push_back(*ticket);
+        }
+        h->scv.notify_one();
+    });
+}
+
+cctagb_status cctagb_wait(cctagb_handle* h, int ticket, cctagb_marker* out, int cap, int* n_out, cctagb_stats* stats)
+{
+    if (!h || !n_out || (cap > 0 && !out)) return CCTAGB_BAD_ARG;
+    std::shared_ptr<Ticket> t;
+    {
+        std::unique_lock<std::mutex> l(h->smu);
+        auto it = h->tickets.find(ticket);
+        if (it == h->tickets.end()) {
+            h->last_error = "unknown ticket";
+            return CCTAGB_BAD_ARG;
+        }
+        t = it->second;
+        h->sdone.wait(l, [&] { return t->done; });
+        h->tickets.erase(it);
+    }
+    *n_out = t->n;
+    if (stats) *stats = t->stats;
+    if (t->status != CCTAGB_OK) {
+        h->last_error = "frame " + std::to_string(t->frame_id) + ": " + t->msg;
+        return t->status;
+    }
+    if (t->n > cap) {
+        h->last_error = "marker output capacity too small";
+        return CCTAGB_BAD_ARG;
+    }
+    std::copy(t->markers.begin(), t->markers.begin() + t->n, out);
+    h->last_error.clear();
+    return CCTAGB_OK;
 }
 
 cctagb_status cctagb_last_tasks(cctagb_handle* h, cctagb_cut_task* out, int cap, int* n)
 {
     if (!h || !n || (cap > 0 && !out)) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] {
         const auto& t = h->det->last_tasks();
         *n = int(t.size());
@@ -321,6 +503,7 @@ cctagb_status cctagb_identify_tasks(cctagb_handle* h, const uint8_t* d_img, int 
                                     const cctagb_cut_task* tasks, int n, int refine_mode, cctagb_ident_result* out)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->identify_tasks(d_img, w, hgt, pitch, tasks, n, refine_mode, out); });
 }
 
@@ -329,12 +512,14 @@ cctagb_status cctagb_cut_cost(cctagb_handle* h, const uint8_t* d_img, int w, int
                               float* d_center, float* d_h)
 {
     if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->cut_cost(d_img, w, hgt, pitch, tasks, n, centers, cost, d_center, d_h); });
 }
 
 cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)
 {
     if (!h || n < 0 || (n > 0 && !frames)) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     if (n == 0) return CCTAGB_OK;
     return guarded(h, [&] {
         const int S = std::min(n, h->slots());

@@ -288,13 +288,17 @@ __device__ __forceinline__ void uf_union(int32_t* L, int a, int b, int32_t* err)
 // the local roots are written back as global indices.
 constexpr int kUfT = 32;
 
-__device__ __forceinline__ int uf_find_s(const int* L, int p)
+// Tile-local find with path halving (each visited node is pointed at its
+// grandparent; parents only decrease, so concurrent unions stay correct).
+__device__ __forceinline__ int uf_find_s(int* L, int p)
 {
-    int q = *(volatile const int*)&L[p];
+    int q = *(volatile int*)&L[p];
     int guard = 0;
     while (q != p && guard++ < kUfT * kUfT) {
+        const int g = *(volatile int*)&L[q];
+        if (g != q) *(volatile int*)&L[p] = g;
         p = q;
-        q = *(volatile const int*)&L[p];
+        q = g;
     }
     return p;
 }
@@ -312,39 +316,62 @@ __device__ __forceinline__ void uf_union_s(int* L, int a, int b)
     }
 }
 
+// Components inside one 32x32 tile, on horizontal runs: one warp per row
+// reads the row as a 32-bit candidate mask; every pixel takes its run's first
+// pixel as parent (no atomics within a row); rows are joined by unions of
+// runs.  A run of row y and a run of row y-1 that touch (8-connectivity) meet
+// at a pixel of one of them that starts its run, so a pixel only tries the
+// unions where it starts its run or its upper neighbour starts one.
 __global__ void __launch_bounds__(256) k_hyst_local(Levels lv)
 {
     __shared__ int s_lab[kUfT * kUfT];
-    __shared__ uint8_t s_cls[kUfT * kUfT];
+    __shared__ uint32_t s_mask[kUfT];
     int tile;
     const int l = level_of_block(lv, blockIdx.x, &LevelView::uf_tiles, tile);
     const LevelView& L = lv.l[l];
     const int x0 = (tile % L.uf_tx) * kUfT, y0 = (tile / L.uf_tx) * kUfT;
-    for (int i = threadIdx.x; i < kUfT * kUfT; i += 256) {
-        const int lx = i % kUfT, ly = i / kUfT, x = x0 + lx, y = y0 + ly;
-        const uint8_t c = (x < L.W && y < L.H) ? L.map[size_t(y) * L.W + x] : 0;
-        s_cls[i] = c;
-        s_lab[i] = c ? i : -1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = x0 + lane;
+    for (int r = warp; r < kUfT; r += 8) {
+        const int y = y0 + r;
+        const bool c = x < L.W && y < L.H && L.map[size_t(y) * L.W + x] != 0;
+        const uint32_t m = __ballot_sync(0xffffffffu, c);
+        if (lane == 0) s_mask[r] = m;
+        const uint32_t starts = m & ~(m << 1);
+        const int start = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
+        s_lab[r * kUfT + lane] = c ? r * kUfT + start : -1;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kUfT * kUfT; i += 256) {
-        if (!s_cls[i]) continue;
-        const int lx = i % kUfT, ly = i / kUfT;
-        if (lx > 0 && s_cls[i - 1]) uf_union_s(s_lab, i, i - 1);
-        if (ly > 0) {
-            const int u = i - kUfT;
-            if (lx > 0 && s_cls[u - 1]) uf_union_s(s_lab, i, u - 1);
-            if (s_cls[u]) uf_union_s(s_lab, i, u);
-            if (lx + 1 < kUfT && s_cls[u + 1]) uf_union_s(s_lab, i, u + 1);
+    for (int r = 1 + warp; r < kUfT; r += 8) {
+        const uint32_t m = s_mask[r], up = s_mask[r - 1];
+        if (!((m >> lane) & 1u)) continue;
+        const bool isStart = lane == 0 || !((m >> (lane - 1)) & 1u);
+        const uint32_t upStarts = up & ~(up << 1);
+        const int i = r * kUfT + lane;
+#pragma unroll
+        for (int d = -1; d <= 1; ++d) {
+            const int xx = lane + d;
+            if (xx < 0 || xx >= kUfT || !((up >> xx) & 1u)) continue;
+            if (isStart || ((upStarts >> xx) & 1u)) uf_union_s(s_lab, i, (r - 1) * kUfT + xx);
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kUfT * kUfT; i += 256) {
-        if (!s_cls[i]) continue;
-        const int r = uf_find_s(s_lab, i);
-        const int x = x0 + i % kUfT, y = y0 + i / kUfT;
+    // run starts resolve their roots; every pixel then reads its run's root
+    for (int r = warp; r < kUfT; r += 8) {
+        const uint32_t m = s_mask[r];
+        const bool isStart = ((m >> lane) & 1u) && (lane == 0 || !((m >> (lane - 1)) & 1u));
+        if (isStart) s_lab[r * kUfT + lane] = uf_find_s(s_lab, r * kUfT + lane);
+    }
+    __syncthreads();
+    for (int r = warp; r < kUfT; r += 8) {
+        const uint32_t m = s_mask[r];
+        if (!((m >> lane) & 1u)) continue;
+        const uint32_t starts = m & ~(m << 1);
+        const int start = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
+        const int root = s_lab[r * kUfT + start];
+        const int y = y0 + r;
         const size_t p = size_t(y) * L.W + x;
-        L.label[p] = (y0 + r / kUfT) * L.W + (x0 + r % kUfT);
+        L.label[p] = (y0 + root / kUfT) * L.W + (x0 + root % kUfT);
         L.sroot[p] = 0;
     }
 }

@@ -32,6 +32,8 @@
  *   cctagb_cut_cost        <- costFunctionGlob (forward only in the reference; here with its
  *                             gradient in the center and in H)   src/cctag/Identification.cpp:1122-1158
  *   cctagb_edges_noalloc   <- cvRecodedCanny + thin on caller buffers (no allocation)
+ *   cctagb_host_frames / cctagb_submit / cctagb_wait
+ *                          <- page-locked frames + async upload    src/cctag/cuda/frame.cu:110-148
  */
 #ifndef CCTAG_B200_H
 #define CCTAG_B200_H
@@ -186,6 +188,29 @@ typedef struct cctagb_frame {
  * one frame per cctagDetection call (ICCTag.hpp:125-131); this is the
  * multi-camera form of that call. */
 cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n);
+
+/* ---- Streaming ingest ----------------------------------------------------
+ * For cameras that deliver a frame at a time.  The reference keeps page-locked
+ * frame buffers and uploads them asynchronously (cuda/frame.cu:110-148); here
+ * the handle owns pinned buffers the caller may fill, and cctagb_submit queues
+ * a frame on the detection slots (min(max_batch, 32) of them) and returns at
+ * once, so that one frame's upload and GPU stages overlap another frame's
+ * host stage.  cctagb_wait(ticket) returns that frame's markers, exactly what
+ * cctagb_detect returns for it.  The frame memory must stay valid until its
+ * ticket has been waited for.  While tickets are outstanding, every other
+ * call that uses the handle's detection slots returns CCTAGB_BAD_ARG. */
+
+/* n (<= 64) pinned host buffers of max_w * max_h bytes owned by the handle
+ * (kept across calls; freed by cctagb_destroy); out[i] receives buffer i. */
+cctagb_status cctagb_host_frames(cctagb_handle* h, int n, uint8_t** out);
+
+cctagb_status cctagb_submit(cctagb_handle* h, const uint8_t* gray, int w, int hgt, size_t pitch, int is_device,
+                            int frame_id, int* ticket);
+
+/* Blocks until the ticket's detection is done; the ticket is then released.
+ * A frame's failure is returned here (and named by last_error_string). */
+cctagb_status cctagb_wait(cctagb_handle* h, int ticket, cctagb_marker* out, int cap, int* n_out,
+                          cctagb_stats* stats);
 
 /* Image stage only (pyramid, derivatives, Canny, thinning, edge points, vote,
  * seeds) on the handle's stream; results stay on the device and are read with

@@ -123,3 +123,27 @@ def test_detect_batch_reports_the_failing_frame(built_library):
         assert "frame 1" in str(e.value)
         ok = bd.detect_batch([small, small])
     assert len(ok) == 2 and _key(ok[0][0]) == _key(ok[1][0])
+
+
+def test_streaming_submit_wait_matches_detect(built_library, detector):
+    """Frames submitted to the streaming ingest (pinned buffers owned by the
+    handle, several in flight) come back with exactly cctagb_detect's result,
+    whatever order the tickets are waited in."""
+    from cctag_b200.synth import render_frame
+    frames = [render_frame(1280, 720, 3, (30.0, 90.0), 50, seed=600 + i, noise_sigma=5.0).image for i in range(6)]
+    want = [_key(detector.detect(f)[0]) for f in frames]
+    with cctag_b200.Detector(max_w=1280, max_h=720, max_batch=3) as sd:
+        bufs = sd.host_frames(3)
+        tickets = []
+        for i, f in enumerate(frames[:3]):
+            bufs[i][:, :] = f
+            tickets.append(sd.submit(bufs[i], frame_id=i))
+        tickets += [sd.submit(f, frame_id=3 + i) for i, f in enumerate(frames[3:])]
+        # another detection call is refused while tickets are outstanding
+        with pytest.raises(cctag_b200.CCTagError):
+            sd.detect(frames[0])
+        got = {t: _key(sd.wait(t)[0]) for t in reversed(tickets)}
+        assert [got[t] for t in tickets] == want
+        assert _key(sd.detect(frames[0])[0]) == want[0]   # usable again once drained
+        with pytest.raises(cctag_b200.CCTagError):
+            sd.wait(tickets[0])                           # a ticket is released by its wait
