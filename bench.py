@@ -47,7 +47,9 @@ N_FRAMES = BATCH
 
 
 # ------------------------------------------------------------------ helpers --
-def dist_setup():
+def dist_setup(backend: str | None = None):
+    """Rank, world size and local rank from the launcher's environment; the
+    process group is NCCL on GPUs (gloo when there is no GPU, for tests)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -57,8 +59,11 @@ def dist_setup():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -70,14 +75,21 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest of every rank's x (device times: the job takes the slowest rank)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def frame_seeds(rank, n):
+    """Seeds of a rank's frames: replicas work on their own frames."""
+    return [100 + i + 1000 * rank for i in range(n)]
 
 
 class ClockSampler:
@@ -131,10 +143,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def make_frames(config, n=N_FRAMES):
+def make_frames(config, n=N_FRAMES, rank=0):
     from cctag_b200.synth import config_frame
 
-    return [config_frame(config, seed=100 + i).image for i in range(n)]
+    return [config_frame(config, seed=sd).image for sd in frame_seeds(rank, n)]
 
 
 # -------------------------------------------------------- algorithmic bytes --
@@ -193,7 +205,7 @@ def run_b200(args, rank, world, local):
 
     torch.cuda.set_device(local)
     dev = f"cuda:{local}"
-    frames = make_frames(args.config)
+    frames = make_frames(args.config, rank=rank)
     H, W = frames[0].shape
     det = cctag_b200.Detector(max_w=W, max_h=H, max_batch=BATCH)
     stream = torch.cuda.ExternalStream(det.stream)
