@@ -14,7 +14,6 @@
 #include <deque>
 #include <limits>
 #include <stdexcept>
-#include <unordered_set>
 
 namespace cctagb {
 
@@ -173,6 +172,36 @@ bool solve5(double A[5][5], double b[5], double x[5])
     return true;
 }
 
+// geo::dist_point_ellipse over a point array, as a loop the compiler can
+// vectorise (same operations per point, so the same values).
+void dist_to_ellipse(const geo::Mat3& Q, const Pt* p, size_t n, float* out)
+{
+    const float q00 = Q.m[0][0], q01 = Q.m[0][1], q02 = Q.m[0][2], q11 = Q.m[1][1], q12 = Q.m[1][2], q22 = Q.m[2][2];
+    for (size_t i = 0; i < n; ++i) {
+        const float x = p[i].x, y = p[i].y;
+        const float aux0 = x * x, aux1 = 2 * x * y, aux2 = 2 * x, aux3 = y * y, aux4 = 2 * y;
+        const float t1 = x * q00 + y * q01 + q02;
+        const float t2 = x * q01 + y * q11 + q12;
+        const float denom = t1 * t1 + t2 * t2;
+        const float dot = aux0 * q00 + aux1 * q01 + aux2 * q02 + aux3 * q11 + aux4 * q12 + q22;
+        out[i] = dot * dot / denom;
+    }
+}
+
+// Whether median_ref(v) (the element of rank n/2) is below `bound`, without
+// selecting it: that holds exactly when at least n/2 + 1 elements are.  -1
+// when a NaN makes the ranks ill-defined (the caller then selects).
+int median_below(const float* v, size_t n, float bound)
+{
+    size_t below = 0, nan = 0;
+    for (size_t i = 0; i < n; ++i) {
+        below += v[i] < bound;
+        nan += v[i] != v[i];
+    }
+    if (nan) return -1;
+    return below >= n / 2 + 1 ? 1 : 0;
+}
+
 // Vote.cpp:414-576 outlierRemoval: LMedS ellipse from random 5-point subsets
 // of (a regular subsample of) the points; keeps the points whose (weighted)
 // distance is below threshold * median.  The reference retries forever when
@@ -237,11 +266,15 @@ void outlier_removal(const EdgeSet& es, const std::vector<int>& children, std::v
                 ++counter;
                 continue;
             }
-            for (size_t i = 0; i < pts.size(); ++i) dist[i] = geo::dist_point_ellipse(q.Q, pts[i].x, pts[i].y);
+            dist_to_ellipse(q.Q, pts.data(), pts.size(), dist.data());
             if (weightedType != kNoWeight)
                 for (size_t i = 0; i < dist.size(); ++i) dist[i] *= weights[i];
-            std::vector<float> tmp = dist;
-            const float S = geo::median_ref(tmp);
+            // most draws do not improve on Sm: decide that by counting
+            if (median_below(dist.data(), dist.size(), Sm) == 0) {
+                ++counter;
+                continue;
+            }
+            const float S = geo::median_ref(dist);
             if (S < Sm) {
                 counter = 0;
                 qm = q;
@@ -515,11 +548,21 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
     pts.resize(numCircles);
     for (int e : outer) pts.back().push_back({float(es.x(e)), float(es.y(e)), es.dx(e), es.dy(e)});
     // The reference marks visited points in a shared per-point flag and clears
-    // it on return; a per-call set gives the same visits and lets candidates
-    // run concurrently.
-    std::unordered_set<int> visited;
+    // it on return; a per-thread stamp (this call's token) gives the same
+    // visits and lets candidates run concurrently.
+    thread_local std::vector<uint32_t> stamp;
+    thread_local uint32_t token = 0;
+    if (stamp.size() < size_t(es.E)) stamp.assign(size_t(es.E), 0u);
+    if (++token == 0) {  // wrapped: clear the stamps
+        std::fill(stamp.begin(), stamp.end(), 0u);
+        token = 1;
+    }
+    auto first_visit = [&](int q) {
+        if (stamp[size_t(q)] == token) return false;
+        stamp[size_t(q)] = token;
+        return true;
+    };
     size_t nGradientOut = 0, nAdded = 0;
-    auto undo = [&]() { visited.clear(); };
     for (int p0 : fc) {
         int dir = -1;
         int p = p0;
@@ -529,10 +572,9 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
         for (size_t j = 1; j < numCircles; ++j) {
             p = dir == -1 ? es.before[p] : es.after[p];
             if (p < 0) {
-                undo();
                 throw std::out_of_range("EdgePointCollection: missing link");
             }
-            if (visited.insert(p).second) {
+            if (first_visit(p)) {
                 const float ng = std::sqrt(es.dx(p) * es.dx(p) + es.dy(p) * es.dy(p));
                 const float gx = es.dx(p) / ng, gy = es.dy(p) / ng;
                 float tx = oe.cx - float(es.x(p)), ty = oe.cy - float(es.y(p));
@@ -546,14 +588,12 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
                     if (j >= numCircles - 2) ++nAdded;
                 } else {
                     pts.clear();
-                    undo();
                     return false;
                 }
             }
             dir = -dir;
         }
     }
-    undo();
     if (float(nGradientOut) / float(nAdded) > 0.5f) {
         pts.clear();
         return false;
@@ -591,11 +631,16 @@ bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& ou
                 ++cnt;
                 continue;
             }
-            d.clear();
-            for (const Pt& r : P) d.push_back(geo::dist_point_ellipse(q.Q, r.x, r.y));
+            d.resize(P.size());
+            dist_to_ellipse(q.Q, P.data(), P.size(), d.data());
+            // S = S1 + S2 >= S1 (S2 >= 0): no improvement unless S1 < Sm
+            if (median_below(d.data(), d.size(), Sm) == 0) {
+                ++cnt;
+                continue;
+            }
             const float S1 = geo::median_ref(d);
-            d.clear();
-            for (const Pt& r : AP) d.push_back(geo::dist_point_ellipse(q.Q, r.x, r.y));
+            d.resize(AP.size());
+            dist_to_ellipse(q.Q, AP.data(), AP.size(), d.data());
             const float S2 = geo::median_ref(d);
             const float S = S1 + S2;
             if (S < Sm) {

@@ -372,42 +372,41 @@ __device__ void trial_partial(const Shared& S, const Roi& R, int t, uint32_t val
     for (int q = 0; q < NCH; ++q) {
         const int k = (j0 + q) * kChunk + lane;
         act[q] = j0 + q < nch && k < nS;
-        kf[q] = float(k);
+        // lanes past the last sample read the last one again (in bounds, no
+        // branch) and their terms are dropped below
+        kf[q] = float(min(k, nS - 1));
         v0[q] = s1[q] = s2[q] = 0.f;
     }
     if (n >= 2) {
-        bool first = true;
         uint32_t m = valid;
+        bool first = true;  // the same in every lane: a uniform branch
         while (m) {
             int c[G];
-            int cnt = 0;
+            float keep[G];
 #pragma unroll
             for (int g = 0; g < G; ++g) {
+                // past the last valid cut: repeat it, with weight 0
                 c[g] = m ? __ffs(m) - 1 : c[g > 0 ? g - 1 : 0];
-                if (m) {
-                    m &= m - 1;
-                    ++cnt;
-                }
+                keep[g] = m ? 1.f : 0.f;
+                m &= m - 1;
             }
             float val[G][NCH];
 #pragma unroll
             for (int g = 0; g < G; ++g)
 #pragma unroll
-                for (int q = 0; q < NCH; ++q) val[g][q] = act[q] ? cut_sample(S, R, t, c[g], kf[q]) : 0.f;
+                for (int q = 0; q < NCH; ++q) val[g][q] = cut_sample(S, R, t, c[g], kf[q]);
             if (first) {
 #pragma unroll
-                for (int q = 0; q < NCH; ++q) v0[q] = val[0][q];
+                for (int q = 0; q < NCH; ++q) v0[q] = val[0][q];  // first valid cut: the shift
                 first = false;
             }
 #pragma unroll
             for (int g = 0; g < G; ++g) {
-                if (g < cnt) {
 #pragma unroll
-                    for (int q = 0; q < NCH; ++q) {
-                        const float d = __fsub_rn(val[g][q], v0[q]);
-                        s1[q] = __fadd_rn(s1[q], d);
-                        s2[q] = __fmaf_rn(d, d, s2[q]);
-                    }
+                for (int q = 0; q < NCH; ++q) {
+                    const float d = __fmul_rn(__fsub_rn(val[g][q], v0[q]), keep[g]);
+                    s1[q] = __fadd_rn(s1[q], d);
+                    s2[q] = __fmaf_rn(d, d, s2[q]);
                 }
             }
         }
@@ -717,9 +716,12 @@ __device__ void gn_refine(Shared& S, const IdentTask& T, const Roi& roi, const I
 }  // namespace
 
 // CL = 1: one block per marker; CL = kCluster: a cluster of blocks per marker
-// (launched with that cluster dimension), block r on sample chunk r.
-template <int CL>
-__global__ void __launch_bounds__(kThreads)
+// (launched with that cluster dimension), block r on sample chunk r.  MB:
+// blocks per SM the registers are budgeted for (2 suits Gauss-Newton, whose
+// steps leave most warps waiting; the grid keeps every warp busy and prefers
+// the registers).
+template <int CL, int MB>
+__global__ void __launch_bounds__(kThreads, MB)
     k_identify(const uint8_t* __restrict__ img, size_t pitch, const IdentTask* __restrict__ tasks, IdentResult* res,
                const float* __restrict__ bankInv, IdentParams ip)
 {
@@ -733,8 +735,11 @@ __global__ void __launch_bounds__(kThreads)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nS = ip.nSamples;
     const int nch = (nS + kChunk - 1) / kChunk;
-    constexpr int NCH = CL == 1 ? kMaxChunks : 1;  // chunks this block evaluates
+    // chunks this block evaluates (all, or chunk `crank` in a cluster), NCH
+    // per pass (fewer live registers when two blocks share an SM)
+    constexpr int NCH = CL == 1 ? (MB == 1 ? kMaxChunks : kMaxChunks / 2) : 1;
     const int j0 = CL == 1 ? 0 : crank;
+    const int jEnd = CL == 1 ? nch : j0 + 1;
     const int gridN = ip.gridN;
     const int nTrials = gridN * gridN;
     const uint32_t cutMask = (T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u);
@@ -810,12 +815,14 @@ __global__ void __launch_bounds__(kThreads)
         __syncthreads();
         const int par = round & 1;
         if (warp < nTrials) {
-            double c[NCH];
-            trial_partial<NCH>(S, roi, warp, S.valid[warp], j0, nch, nS, lane, c);
-            if (lane == 0)
+            for (int jp = j0; jp < jEnd; jp += NCH) {
+                double c[NCH];
+                trial_partial<NCH>(S, roi, warp, S.valid[warp], jp, nch, nS, lane, c);
+                if (lane == 0)
 #pragma unroll
-                for (int q = 0; q < NCH; ++q)
-                    if (j0 + q < nch) S.part[par][j0 + q][warp] = c[q];
+                    for (int q = 0; q < NCH; ++q)
+                        if (jp + q < nch) S.part[par][jp + q][warp] = c[q];
+            }
         }
         // All chunks of the marker are in; a block rewrites this parity's
         // array two rounds later, after the next cluster barrier, when every
@@ -1286,9 +1293,12 @@ void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_task
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CCTAGB_CUDA(cudaLaunchKernelEx(&cfg, k_identify<kCluster>, d_img, pitch, d_tasks, d_res, d_bank_inv, ip));
+        CCTAGB_CUDA(cudaLaunchKernelEx(&cfg, k_identify<kCluster, 1>, d_img, pitch, d_tasks, d_res, d_bank_inv, ip));
+    } else if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON) {
+        k_identify<1, 2><<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_res, d_bank_inv, ip);
+        CCTAGB_CUDA(cudaGetLastError());
     } else {
-        k_identify<1><<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_res, d_bank_inv, ip);
+        k_identify<1, 1><<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_res, d_bank_inv, ip);
         CCTAGB_CUDA(cudaGetLastError());
     }
 }
