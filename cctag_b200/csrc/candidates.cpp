@@ -53,7 +53,12 @@ inline bool bit_test(const EdgeSet& es, int i, uint64_t m)
 // equal to the call's token is the same set.
 void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t window, float averageVoteMin)
 {
-    std::deque<float> phi;
+    // the last `window` gradient angles (the reference's deque), as a ring
+    thread_local std::vector<float> ring;
+    if (ring.size() < window + 1) ring.resize(window + 1);
+    size_t head = 0, count = 0;  // oldest entry, entries held
+    auto phi_front = [&]() { return ring[head]; };
+    auto phi_back = [&]() { return ring[(head + count - 1) % (window + 1)]; };
     size_t i = 0;
     bool found = true;
     int stop = 0;
@@ -62,8 +67,11 @@ void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t 
     static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
     while (i < maxLength && found && averageVote >= averageVoteMin) {
         const float angle = std::fmod(std::atan2(es.dy(p), es.dx(p)) + 2.0f * kPi, 2.0f * kPi);
-        phi.push_back(angle);
-        if (phi.size() > window) phi.pop_front();
+        ring[(head + count) % (window + 1)] = angle;
+        if (++count > window) {
+            head = (head + 1) % (window + 1);
+            --count;
+        }
         const int shifting = int(std::round(((angle + kPi / 4.0f) / (2.0f * kPi)) * 8.0f)) - 1;
         const int yoff[8] = {0, -dir, -dir, -dir, 0, dir, dir, dir};
         int j = 0;
@@ -77,8 +85,8 @@ void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t 
                 const int sy = es.y(p) + yoff[k];
                 if (sx >= 0 && sx < es.W && sy >= 0 && sy < es.H && es.at(sx, sy) >= 0 &&
                     es.link_stamp[es.at(sx, sy)] != es.link_token) {
-                    const float d = phi.back() - phi.front();
-                    if (phi.size() == window) {
+                    const float d = phi_back() - phi_front();
+                    if (count == window) {
                         if (float(dir) * std::sin(d) < 0.0f) stop = kConvexityLost;
                     } else {
                         const float s = float(dir) * std::sin(d);
