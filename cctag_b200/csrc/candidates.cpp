@@ -24,7 +24,6 @@ void EdgeSet::reset_state()
 {
     processed_in.assign(E, 0);
     processed_aux.assign(E, 0);
-    processed.assign(E, 0);
     n_segment_out.assign(E, -1);
     link_stamp.assign(E, 0);
     link_token = 0;
@@ -36,15 +35,24 @@ constexpr int kEdgeNotFound = -1;
 constexpr int kConvexityLost = -2;
 constexpr float kPi = 3.14159265358979323846f;
 
-// Per-point candidate masks of the ellipse growing (EdgePoint::_processed, one
-// bit per candidate of the second loop): candidates grow concurrently, each on
-// its own bit, so the word updates are atomic.
-inline void bit_set(EdgeSet& es, int i, uint64_t m) { __atomic_fetch_or(&es.processed[i], m, __ATOMIC_RELAXED); }
-inline void bit_clear(EdgeSet& es, int i, uint64_t m) { __atomic_fetch_and(&es.processed[i], ~m, __ATOMIC_RELAXED); }
-inline bool bit_test(const EdgeSet& es, int i, uint64_t m)
-{
-    return (__atomic_load_n(&es.processed[i], __ATOMIC_RELAXED) & m) != 0;
-}
+// The points one ellipse-growing run has marked (EdgePoint::_processed ==
+// runId in the reference, a test private to the run): a per-thread stamp
+// array, with a fresh token per run, so concurrent runs need no shared state.
+struct RunMarks {
+    std::vector<uint32_t> stamp;
+    uint32_t token = 0;
+    void begin(size_t E)
+    {
+        if (stamp.size() < E) stamp.assign(E, 0u);
+        if (++token == 0) {  // wrapped: clear the stamps
+            std::fill(stamp.begin(), stamp.end(), 0u);
+            token = 1;
+        }
+    }
+    void set(int i) { stamp[size_t(i)] = token; }
+    void clear(int i) { stamp[size_t(i)] = 0u; }
+    bool test(int i) const { return stamp[size_t(i)] == token; }
+};
 
 // Vote.cpp:272-394 edgeLinkingDir: follow the edge contour from p while the
 // gradient direction keeps turning one way (convexity).
@@ -367,7 +375,7 @@ bool ellipse_growing_init(const EdgeSet& es, const std::vector<int>& fc, Ellipse
 // EllipseGrowing.cpp:378-422 connectedPoint: depth-first growth through
 // 8-neighbours inside the hull whose gradient points away from the center.
 // Iterative form of the reference's recursion (same visiting order).
-void connected_point(std::vector<int>& pts, uint64_t mask, EdgeSet& es, const Ellipse& qIn, const Ellipse& qOut,
+void connected_point(std::vector<int>& pts, RunMarks& mk, EdgeSet& es, const Ellipse& qIn, const Ellipse& qOut,
                      int x, int y)
 {
     static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
@@ -375,7 +383,7 @@ void connected_point(std::vector<int>& pts, uint64_t mask, EdgeSet& es, const El
     using Frame = EdgeSet::DfsFrame;
     thread_local std::vector<Frame> st;  // reused across calls of this thread
     st.clear();
-    bit_set(es, es.at(x, y), mask);
+    mk.set(es.at(x, y));
     st.push_back({x, y, 0});
     while (!st.empty()) {
         Frame& f = st.back();
@@ -388,25 +396,25 @@ void connected_point(std::vector<int>& pts, uint64_t mask, EdgeSet& es, const El
         if (sx < 0 || sx >= es.W || sy < 0 || sy >= es.H) continue;
         const int e = es.at(sx, sy);
         if (e < 0) continue;
-        if (!geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e))) || bit_test(es, e, mask)) continue;
+        if (!geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e))) || mk.test(e)) continue;
         const float ox = qIn.cx - float(es.x(e)), oy = qIn.cy - float(es.y(e));
         if (es.dx(e) * ox + es.dy(e) * oy < 0) {
             pts.push_back(e);
-            bit_set(es, e, mask);
+            mk.set(e);
             st.push_back({sx, sy, 0});
         }
     }
 }
 
 // EllipseGrowing.cpp:443-457
-void ellipse_hull(EdgeSet& es, std::vector<int>& pts, const Ellipse& e, float delta, uint64_t mask)
+void ellipse_hull(EdgeSet& es, std::vector<int>& pts, const Ellipse& e, float delta, RunMarks& mk)
 {
     Ellipse qIn, qOut;
     geo::compute_hull(e, delta, qIn, qOut);
     const size_t init = pts.size();
     for (size_t i = 0; i < init; ++i) {
         const int p = pts[i];
-        connected_point(pts, mask, es, qIn, qOut, es.x(p), es.y(p));
+        connected_point(pts, mk, es, qIn, qOut, es.x(p), es.y(p));
     }
 }
 
@@ -422,11 +430,12 @@ size_t count_in_hull(const EdgeSet& es, const std::vector<int>& pts, const Ellip
 
 // EllipseGrowing.cpp:459-551 ellipseGrowing2
 void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>& outer, Ellipse& ellipse, float width,
-                      size_t runId, bool goodInit)
+                      bool goodInit)
 {
-    const uint64_t mask = uint64_t(1) << (runId & 63);
+    thread_local RunMarks mk;
+    mk.begin(size_t(es.E));
     outer = fc;
-    for (int c : fc) bit_set(es, c, mask);
+    for (int c : fc) mk.set(c);
     if (!goodInit) {
         int newSize = int(outer.size());
         int maxNb = newSize, nIterMax = 0, lastSize = 0, nIter = 0;
@@ -435,7 +444,7 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
         ++nIter;
         while (newSize - lastSize > 0) {
             lastSize = int(count_in_hull(es, outer, ellipse, width));
-            ellipse_hull(es, outer, ellipse, width, mask);
+            ellipse_hull(es, outer, ellipse, width, mk);
             sets.push_back(outer);
             ells.push_back(ellipse);
             ellipse = fit_circle_points(es, outer);
@@ -449,14 +458,14 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
         outer = sets[nIterMax];
         ellipse = ells[nIterMax];
         for (auto& s : sets)
-            for (int p : s) bit_clear(es, p, mask);
-        for (int p : outer) bit_set(es, p, mask);
+            for (int p : s) mk.clear(p);
+        for (int p : outer) mk.set(p);
     }
     ellipse = fit_points(es, outer);
     size_t lastSize = 0;
     while (outer.size() > lastSize) {
         lastSize = outer.size();
-        ellipse_hull(es, outer, ellipse, width, mask);
+        ellipse_hull(es, outer, ellipse, width, mk);
         ellipse = fit_points(es, outer);
     }
 }
@@ -510,11 +519,11 @@ void flow_component_label(Candidate& c, EdgeSet& es, size_t& nSegmentOut)
 }
 
 // Phase D: returns whether the candidate enters the second list.
-bool flow_component_grow(Candidate& c, EdgeSet& es, size_t runId, const cctagb_params& p)
+bool flow_component_grow(Candidate& c, EdgeSet& es, const cctagb_params& p)
 {
     try {
         const bool goodInit = ellipse_growing_init(es, c.filtered, c.outerEllipse);
-        ellipse_growing2(es, c.filtered, c.outer, c.outerEllipse, p.ellipseGrowingEllipticHullWidth, runId, goodInit);
+        ellipse_growing2(es, c.filtered, c.outer, c.outerEllipse, p.ellipseGrowingEllipticHullWidth, goodInit);
         std::vector<float> vd;
         vd.reserve(c.outer.size());
         for (int q : c.outer) vd.push_back(geo::dist_point_ellipse(c.outerEllipse.Q, float(es.x(q)), float(es.y(q))));
@@ -836,22 +845,11 @@ void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, cons
         for (size_t i = 0; i < st[l].keep.size(); ++i)
             if (st[l].keep[i]) flow_component_label(st[l].loop1[i], *jobs[l].es, nSegmentOut);
     }
-    // Phase D: ellipse growing (runId = index in loop 1, as the reference).
-    // A run only tests its own bit of the per-point masks, so candidates grow
-    // in groups of 64 indices with the masks cleared between groups.
-    size_t n2max = 0;
-    for (int l = 0; l < nl; ++l) n2max = std::max(n2max, st[l].keep.size());
-    for (size_t g0 = 0; g0 < n2max; g0 += 64) {
-        std::vector<std::pair<int, int>> group;
-        for (const auto& t : tasks)
-            if (size_t(t.second) >= g0 && size_t(t.second) < g0 + 64) group.push_back(t);
-        if (g0 > 0)
-            for (int l = 0; l < nl; ++l) std::fill(jobs[l].es->processed.begin(), jobs[l].es->processed.end(), 0);
-        pf(int(group.size()), [&](int t) {
-            const int l = group[t].first, i = group[t].second;
-            if (st[l].keep[i] && !flow_component_grow(st[l].loop1[i], *jobs[l].es, size_t(i), p)) st[l].keep[i] = 0;
-        });
-    }
+    // Phase D: ellipse growing, each run with its own point marks.
+    pf(int(tasks.size()), [&](int t) {
+        const int l = tasks[t].first, i = tasks[t].second;
+        if (st[l].keep[i] && !flow_component_grow(st[l].loop1[i], *jobs[l].es, p)) st[l].keep[i] = 0;
+    });
     tasks.clear();
     for (int l = 0; l < nl; ++l) {
         for (size_t i = 0; i < st[l].keep.size(); ++i)

@@ -27,7 +27,6 @@ struct EdgeSet {
     int32_t* idxmap = nullptr;  // W*H, -1 where no edge point (owned by the caller)
 
     std::vector<uint8_t> processed_in, processed_aux;
-    std::vector<uint64_t> processed;  // per-candidate bit masks (ellipse growing)
     std::vector<int32_t> n_segment_out;
     std::vector<uint32_t> link_stamp;  // edge linking: point visited in call `link_token`
     uint32_t link_token = 0;
