@@ -304,7 +304,7 @@ def run_b200(args, rank, world, local):
     # identification kernel, separate pass (not part of the timed region).
     det.set_stage_timing(True)
     acc = {}
-    id_ms, host_ms = [], []
+    id_ms, host_ms, dl_ms, cut_ms = [], [], [], []
     for i in range(max(3, min(args.steps, 20))):
         flush.zero_()
         torch.cuda.synchronize()
@@ -313,6 +313,8 @@ def run_b200(args, rank, world, local):
             acc.setdefault(k, []).append(v)
         id_ms.append(st.ms_identify)
         host_ms.append(st.ms_host_candidates)
+        dl_ms.append(st.ms_download)
+        cut_ms.append(st.ms_cut_selection)
     det.set_stage_timing(False)
     stage_ms = {k: statistics.median(v) for k, v in acc.items()}
 
@@ -333,7 +335,10 @@ def run_b200(args, rank, world, local):
     idm = statistics.median(id_ms)
     stages["identify"] = {"ms": round(idm, 5), "markers": n_ident, "bound": "fp32 SIMT + L2 gathers",
                           "GFLOP_s": round(ident_flops(n_ident) / (idm * 1e-3) / 1e9, 1) if idm > 0 else None}
-    stages["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++)"}
+    stages["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++), includes the "
+                                 "edge-point download"}
+    stages["download"] = {"ms": round(statistics.median(dl_ms), 4), "where": "D2H of the edge-point collections"}
+    stages["host_cut_selection"] = {"ms": round(statistics.median(cut_ms), 4), "where": "host CPU (C++)"}
     # Roofline object for the dominant HBM-class kernel group of the image stage.
     top = max(stage_ms, key=lambda k: stage_ms[k])
     traffic = profiled_traffic(args.config).get(top)

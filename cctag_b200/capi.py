@@ -53,7 +53,8 @@ class Stats(C.Structure):
     _fields_ = [("edge_points", C.c_int * 8), ("seeds", C.c_int * 8), ("candidates", C.c_int),
                 ("markers", C.c_int), ("ms_image_stage", C.c_float), ("ms_host_candidates", C.c_float),
                 ("ms_identify", C.c_float), ("ms_total", C.c_float), ("h2d_bytes", C.c_longlong),
-                ("d2h_bytes", C.c_longlong), ("kernel_launches", C.c_int)]
+                ("d2h_bytes", C.c_longlong), ("kernel_launches", C.c_int), ("ms_download", C.c_float),
+                ("ms_cut_selection", C.c_float)]
 
 
 class Frame(C.Structure):

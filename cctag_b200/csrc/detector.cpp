@@ -48,8 +48,19 @@ Detector::~Detector()
     if (d_res_) cudaFree(d_res_);
     if (h_tasks_) cudaFreeHost(h_tasks_);
     if (h_res_) cudaFreeHost(h_res_);
+    if (frame_pinned_) cudaFreeHost(frame_pinned_);
     if (ev_id0_) cudaEventDestroy(ev_id0_);
     if (ev_id1_) cudaEventDestroy(ev_id1_);
+}
+
+void Detector::ensure_frame_pinned(size_t bytes)
+{
+    if (bytes <= frame_pinned_cap_) return;
+    if (frame_pinned_) cudaFreeHost(frame_pinned_);
+    frame_pinned_ = nullptr;
+    frame_pinned_cap_ = 0;
+    CCTAGB_CUDA(cudaMallocHost(&frame_pinned_, bytes));
+    frame_pinned_cap_ = bytes;
 }
 
 void Detector::ensure_ident_capacity(int n)
@@ -267,7 +278,17 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     const auto t1 = clk::now();
     std::vector<HostLevel>& hl = hl_;
     std::vector<EdgeSet>& es = es_;
+    // A device frame is needed on the host for cut selection: its copy into
+    // pinned memory rides with the edge-point downloads.
+    const bool need_frame = params_.doIdentification && is_device;
+    if (need_frame) {
+        ensure_frame_pinned(size_t(w) * h);
+        CCTAGB_CUDA(cudaMemcpyAsync(frame_pinned_, pipe_.level0_src(), size_t(w) * h, cudaMemcpyDeviceToHost,
+                                    pipe_.stream()));
+        pipe_.add_io(0, (long long)w * h, 0);
+    }
     pipe_.download_levels(hl);
+    const auto t1d = clk::now();
     auto fill_level = [&](int l) {
         EdgeSet& e = es[l];
         const HostLevel& L = hl[l];
@@ -308,15 +329,12 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     const auto t2 = clk::now();
 
     // Identification.
-    float ms_ident = 0.f;
+    float ms_ident = 0.f, ms_cut = 0.f;
     if (params_.doIdentification && !markers.empty()) {
         const uint8_t* img = gray;
         size_t stride = pitch;
         if (is_device) {
-            frame_host_.resize(size_t(w) * h);
-            CCTAGB_CUDA(cudaMemcpy(frame_host_.data(), pipe_.level0_src(), frame_host_.size(), cudaMemcpyDeviceToHost));
-            pipe_.add_io(0, (long long)frame_host_.size(), 0);
-            img = frame_host_.data();
+            img = frame_pinned_;  // copied with the downloads
             stride = size_t(w);
         } else if (pitch != size_t(w)) {
             frame_host_.resize(size_t(w) * h);
@@ -326,10 +344,12 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         }
         (void)stride;
         std::vector<IdentTask> all(markers.size());
+        const auto tc0 = clk::now();
         pool_->parallel_for(int(markers.size()), [&](int i) {
             all[i] = IdentTask{};
             markers[i].status = identify_step1(markers[i], img, w, h, params_, all[i]);
         });
+        ms_cut = std::chrono::duration<float, std::milli>(clk::now() - tc0).count();
         std::vector<IdentTask> tasks;
         std::vector<int> task_of(markers.size(), -1);
         for (size_t i = 0; i < markers.size(); ++i) {
@@ -405,6 +425,8 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         stats->h2d_bytes = pipe_.h2d_bytes();
         stats->d2h_bytes = pipe_.d2h_bytes();
         stats->kernel_launches = pipe_.kernel_launches();
+        stats->ms_download = std::chrono::duration<float, std::milli>(t1d - t1).count();
+        stats->ms_cut_selection = ms_cut;
     }
 }
 

@@ -44,6 +44,7 @@ public:
 
 private:
     void ensure_ident_capacity(int n);
+    void ensure_frame_pinned(size_t bytes);
     IdentParams ident_params(int refine_mode) const;
     void identify_on(const uint8_t* d_img, size_t pitch, const IdentTask* tasks, int n, const IdentParams& ip,
                      IdentResult* out);
@@ -55,7 +56,9 @@ private:
     std::vector<HostLevel> hl_;                  // per level, pinned downloads
     std::vector<EdgeSet> es_;                    // per level, candidate-stage state
     std::shared_ptr<ThreadPool> pool_;
-    std::vector<uint8_t> frame_host_;
+    std::vector<uint8_t> frame_host_;            // pitched host frames made contiguous
+    uint8_t* frame_pinned_ = nullptr;            // device frames copied back for cut selection
+    size_t frame_pinned_cap_ = 0;
     float* d_bank_inv_ = nullptr;                // kMaxBankIds x kMaxBankRatios
     IdentTask* d_tasks_ = nullptr;
     IdentResult* d_res_ = nullptr;

@@ -141,6 +141,8 @@ typedef struct cctagb_stats {
     long long h2d_bytes;       /* host->device bytes copied by the call */
     long long d2h_bytes;       /* device->host bytes copied by the call */
     int kernel_launches;       /* kernels launched by the call         */
+    float ms_download;         /* host wall time of the edge-point downloads */
+    float ms_cut_selection;    /* host wall time of cut selection (identify_step_1) */
 } cctagb_stats;
 
 typedef struct cctagb_handle cctagb_handle;

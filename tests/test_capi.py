@@ -85,7 +85,7 @@ def test_binding_struct_layouts_match_the_header(tmp_path):
     checks = {
         "cctagb_params": (capi.Params, []),
         "cctagb_marker": (capi.Marker, ["outer", "homography", "quality", "scale"]),
-        "cctagb_stats": (capi.Stats, ["ms_image_stage", "h2d_bytes", "kernel_launches"]),
+        "cctagb_stats": (capi.Stats, ["ms_image_stage", "h2d_bytes", "kernel_launches", "ms_cut_selection"]),
         "cctagb_frame": (capi.Frame, ["pitch", "out", "n_out", "status", "stats"]),
         "cctagb_cut_task": (capi.CutTask, ["x0", "ncuts", "stop", "roi"]),
         "cctagb_ident_result": (capi.IdentResult, ["H", "residual", "nvalid", "iterations"]),
