@@ -43,6 +43,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "1080p frames/s + per-stage HBM GB/s; batched/adjoint vs plain at <=0.05 px"
 UNIT = "frames/s"
 BATCH = 16  # frames per step (distinct seeded frames)
+SLOTS = 8   # detection slots of the batch handle
 N_FRAMES = BATCH
 
 
@@ -207,7 +208,7 @@ def run_b200(args, rank, world, local):
     dev = f"cuda:{local}"
     frames = make_frames(args.config, rank=rank)
     H, W = frames[0].shape
-    det = cctag_b200.Detector(max_w=W, max_h=H, max_batch=BATCH)
+    det = cctag_b200.Detector(max_w=W, max_h=H, max_batch=SLOTS)
     stream = torch.cuda.ExternalStream(det.stream)
     d_frames = [torch.from_numpy(f).to(dev) for f in frames]
     h_frames = [torch.from_numpy(f).pin_memory() for f in frames]
@@ -359,7 +360,8 @@ def run_b200(args, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "u8/i16/f32", "data": "synthetic",
         "config": {"workload": f"{args.config}: full detection (pyramid .. identification, 3 crowns) of a batch "
                                f"of {BATCH} frames per step through cctagb_detect_batch",
-                   "frame": f"{W}x{H}", "frames_per_step": BATCH, "levels": levels, "edge_points": E,
+                   "frame": f"{W}x{H}", "frames_per_step": BATCH, "detection_slots": SLOTS,
+                   "host_threads": os.cpu_count(), "levels": levels, "edge_points": E,
                    "seeds": S, "markers_reliable": len(found), "candidates": stats.candidates,
                    "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}",
                    "batch_frame_p50_ms": round(statistics.median(batch_frame_ms), 3),
@@ -495,7 +497,7 @@ def run_c4(args, flush, torch):
     from cctag_b200.synth import camera_batch
 
     cams = [f.image for f in camera_batch(seed=0, n=BATCH)]
-    det = cctag_b200.Detector(max_w=3840, max_h=2160, max_batch=BATCH)
+    det = cctag_b200.Detector(max_w=3840, max_h=2160, max_batch=SLOTS)
     stream = torch.cuda.ExternalStream(det.stream)
     dev = torch.device("cuda", torch.cuda.current_device())
     d = [torch.from_numpy(c).to(dev) for c in cams]

@@ -34,7 +34,7 @@ class Params(C.Structure):
         ("imagedCenterNeighbourSize", C.c_float), ("minIdentProba", C.c_float), ("useLMDif", C.c_int),
         ("searchForAnotherSegment", C.c_int), ("writeOutput", C.c_int), ("doIdentification", C.c_int),
         ("maxEdges", C.c_uint32), ("refineMode", C.c_int), ("gnIterations", C.c_int),
-        ("gnCoarseRounds", C.c_int), ("edgeCapacityDivisor", C.c_int),
+        ("gnCoarseRounds", C.c_int), ("edgeCapacityDivisor", C.c_int), ("hostThreads", C.c_int),
     ]
 
 

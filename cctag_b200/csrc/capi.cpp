@@ -260,7 +260,7 @@ cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int ma
     h->max_batch = max_batch;
     cudaGetDevice(&h->device);
     const cctagb_status s = guarded(h.get(), [&] {
-        h->pool = cctagb::make_host_pool();
+        h->pool = cctagb::make_host_pool(p->hostThreads);
         h->det.reset(new cctagb::Detector(*p, max_w, max_h, max_batch, h->pool));
     });
     if (s != CCTAGB_OK) return s;

@@ -35,7 +35,7 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, 
     ensure_ident_capacity(256);
     hl_.resize(idxmaps_.size());
     es_.resize(idxmaps_.size());
-    if (!pool_) pool_ = make_host_pool();
+    if (!pool_) pool_ = make_host_pool(p.hostThreads);
 }
 
 Detector::~Detector()

@@ -7,10 +7,13 @@
 
 #include <algorithm>
 #include <condition_variable>
+#include <cstdlib>
 #include <exception>
+#include <fstream>
 #include <functional>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -127,11 +130,33 @@ private:
     bool stop_ = false;
 };
 
-// A pool with one worker per core besides the caller (at most 63).
-inline std::shared_ptr<ThreadPool> make_host_pool()
+// Physical cores available to the process: the logical CPUs scaled by
+// "cpu cores" / "siblings" of /proc/cpuinfo (two hardware threads of one core
+// share its floating-point units, and the host stages are FP-bound); the
+// logical count when that is unknown.
+inline int physical_cores()
 {
-    const unsigned hc = std::thread::hardware_concurrency();
-    return std::make_shared<ThreadPool>(int(std::min(63u, hc > 1 ? hc - 1 : 0u)));
+    const int logical = int(std::max(1u, std::thread::hardware_concurrency()));
+    std::ifstream f("/proc/cpuinfo");
+    std::string line;
+    int cores = 0, siblings = 0;
+    while (std::getline(f, line) && (!cores || !siblings)) {
+        const auto colon = line.find(':');
+        if (colon == std::string::npos) continue;
+        const std::string key = line.substr(0, line.find_last_not_of(" \t", colon - 1) + 1);
+        if (key == "cpu cores") cores = std::atoi(line.c_str() + colon + 1);
+        if (key == "siblings") siblings = std::atoi(line.c_str() + colon + 1);
+    }
+    if (cores <= 0 || siblings <= 0 || cores > siblings) return logical;
+    return std::max(1, logical * cores / siblings);
+}
+
+// A pool of `threads` host threads counting the caller (0: one per physical
+// core), that is threads - 1 workers, at most 63.
+inline std::shared_ptr<ThreadPool> make_host_pool(int threads = 0)
+{
+    if (threads <= 0) threads = physical_cores();
+    return std::make_shared<ThreadPool>(std::min(63, threads - 1));
 }
 
 }  // namespace cctagb
