@@ -902,9 +902,12 @@ bool intersect_line_two(int y, const Ellipse& qIn, const Ellipse& qOut, const Ed
 
 }  // namespace
 
-void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, geo::Pcg32& rng)
+void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, const ParallelFor& pf)
 {
-    for (MarkerCand& m : markers) {
+    pf(int(markers.size()), [&](int mi) {
+        MarkerCand& m = markers[size_t(mi)];
+        // each marker its own PCG32 stream, apart from the candidate loops'
+        geo::Pcg32 rng(271828, (uint64_t(1) << 62) | uint64_t(mi));
         if (m.level > 0) {
             const float scale = m.scale;
             Ellipse qIn, qOut;
@@ -917,11 +920,11 @@ void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, geo::Pcg32&
                 if (!intersect_line_two(y, qIn, qOut, es0, hull)) break;
             for (int y = minY; y >= 0; --y)
                 if (!intersect_line_two(y, qIn, qOut, es0, hull)) break;
-            if (hull.size() < 5) continue;
+            if (hull.size() < 5) return;
             std::vector<int> filtered;
             float SmFinal = 1e+10f;
             outlier_removal(es0, hull, filtered, SmFinal, 20.0f, kNoWeight, 60, rng);
-            if (filtered.size() < 5) continue;
+            if (filtered.size() < 5) return;
             try {
                 const Ellipse fitted = fit_points(es0, filtered);
                 std::vector<DirPoint> dp;
@@ -936,7 +939,7 @@ void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, geo::Pcg32&
         } else {
             m.rescaled_points = m.points.empty() ? std::vector<DirPoint>() : m.points.back();
         }
-    }
+    });
 }
 
 }  // namespace cctagb

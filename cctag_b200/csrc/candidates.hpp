@@ -84,7 +84,8 @@ using ParallelFor = std::function<void(int, const std::function<void(int)>&)>;
 // the same for any ParallelFor.
 void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf);
 
-// Level-0 re-fit of markers detected on coarser levels (Multiresolution.cpp:319-401).
-void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, geo::Pcg32& rng);
+// Level-0 re-fit of markers detected on coarser levels (Multiresolution.cpp:
+// 319-401), markers in parallel, each with its own PCG32 stream.
+void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, const ParallelFor& pf);
 
 }  // namespace cctagb

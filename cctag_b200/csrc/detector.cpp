@@ -48,19 +48,14 @@ Detector::~Detector()
     if (d_res_) cudaFree(d_res_);
     if (h_tasks_) cudaFreeHost(h_tasks_);
     if (h_res_) cudaFreeHost(h_res_);
-    if (frame_pinned_) cudaFreeHost(frame_pinned_);
+    if (d_cutin_) cudaFree(d_cutin_);
+    if (h_cutin_) cudaFreeHost(h_cutin_);
+    if (d_cutpts_) cudaFree(d_cutpts_);
+    if (h_cutpts_) cudaFreeHost(h_cutpts_);
+    if (d_st1_) cudaFree(d_st1_);
+    if (h_st1_) cudaFreeHost(h_st1_);
     if (ev_id0_) cudaEventDestroy(ev_id0_);
     if (ev_id1_) cudaEventDestroy(ev_id1_);
-}
-
-void Detector::ensure_frame_pinned(size_t bytes)
-{
-    if (bytes <= frame_pinned_cap_) return;
-    if (frame_pinned_) cudaFreeHost(frame_pinned_);
-    frame_pinned_ = nullptr;
-    frame_pinned_cap_ = 0;
-    CCTAGB_CUDA(cudaMallocHost(&frame_pinned_, bytes));
-    frame_pinned_cap_ = bytes;
 }
 
 void Detector::ensure_ident_capacity(int n)
@@ -131,6 +126,66 @@ void Detector::identify_on(const uint8_t* d_img, size_t pitch, const IdentTask* 
     CCTAGB_CUDA(cudaStreamSynchronize(s));
     std::memcpy(out, h_res_, sizeof(IdentResult) * n);
     pipe_.add_io((long long)sizeof(IdentTask) * n, (long long)sizeof(IdentResult) * n, 1);
+}
+
+void Detector::ensure_cut_capacity(int nm, int npts)
+{
+    ensure_ident_capacity(nm);
+    if (nm > cut_cap_) {
+        if (d_cutin_) cudaFree(d_cutin_);
+        if (h_cutin_) cudaFreeHost(h_cutin_);
+        if (d_st1_) cudaFree(d_st1_);
+        if (h_st1_) cudaFreeHost(h_st1_);
+        d_cutin_ = nullptr;
+        h_cutin_ = nullptr;
+        d_st1_ = nullptr;
+        h_st1_ = nullptr;
+        cut_cap_ = 0;
+        const int cap = std::max(nm, 256);
+        CCTAGB_CUDA(cudaMalloc(&d_cutin_, sizeof(CutSelectIn) * cap));
+        CCTAGB_CUDA(cudaMallocHost(&h_cutin_, sizeof(CutSelectIn) * cap));
+        CCTAGB_CUDA(cudaMalloc(&d_st1_, sizeof(int) * cap));
+        CCTAGB_CUDA(cudaMallocHost(&h_st1_, sizeof(int) * cap));
+        cut_cap_ = cap;
+    }
+    if (npts > pts_cap_) {
+        if (d_cutpts_) cudaFree(d_cutpts_);
+        if (h_cutpts_) cudaFreeHost(h_cutpts_);
+        d_cutpts_ = nullptr;
+        h_cutpts_ = nullptr;
+        pts_cap_ = 0;
+        const int cap = std::max(npts, 16384);
+        CCTAGB_CUDA(cudaMalloc(&d_cutpts_, sizeof(DirPoint) * cap));
+        CCTAGB_CUDA(cudaMallocHost(&h_cutpts_, sizeof(DirPoint) * cap));
+        pts_cap_ = cap;
+    }
+}
+
+void Detector::select_and_identify(int nm, int npts, int w, int h)
+{
+    if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
+    cudaStream_t s = pipe_.stream();
+    CCTAGB_CUDA(cudaMemcpyAsync(d_cutin_, h_cutin_, sizeof(CutSelectIn) * nm, cudaMemcpyHostToDevice, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(d_cutpts_, h_cutpts_, sizeof(DirPoint) * npts, cudaMemcpyHostToDevice, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(d_tasks_, h_tasks_, sizeof(IdentTask) * nm, cudaMemcpyHostToDevice, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(d_st1_, h_st1_, sizeof(int) * nm, cudaMemcpyHostToDevice, s));
+    CutSelectParams cp{};
+    cp.beginSig = begin_signal(params_.nCrowns);
+    cp.nSamples = std::min(params_.sampleCutLength, kMaxSamples);
+    cp.nRefine = params_.numSamplesOuterEdgePointsRefinement;
+    cp.maxSelect = std::min(params_.numCutsInIdentStep, kMaxCuts);
+    launch_cut_select(pipe_.level0_src(), w, h, d_cutin_, d_cutpts_, d_tasks_, d_st1_, nm, cp, s);
+    CCTAGB_CUDA(cudaEventRecord(ev_id0_, s));
+    launch_identify(pipe_.level0_src(), size_t(w), d_tasks_, d_res_, nm, d_bank_inv_,
+                    ident_params(params_.refineMode), s);
+    CCTAGB_CUDA(cudaEventRecord(ev_id1_, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(h_res_, d_res_, sizeof(IdentResult) * nm, cudaMemcpyDeviceToHost, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(h_st1_, d_st1_, sizeof(int) * nm, cudaMemcpyDeviceToHost, s));
+    CCTAGB_CUDA(cudaMemcpyAsync(h_tasks_, d_tasks_, sizeof(IdentTask) * nm, cudaMemcpyDeviceToHost, s));
+    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    pipe_.add_io((long long)(sizeof(CutSelectIn) + sizeof(IdentTask) + sizeof(int)) * nm +
+                     (long long)sizeof(DirPoint) * npts,
+                 (long long)(sizeof(IdentResult) + sizeof(int) + sizeof(IdentTask)) * nm, 2);
 }
 
 void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
@@ -278,15 +333,6 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     const auto t1 = clk::now();
     std::vector<HostLevel>& hl = hl_;
     std::vector<EdgeSet>& es = es_;
-    // A device frame is needed on the host for cut selection: its copy into
-    // pinned memory rides with the edge-point downloads.
-    const bool need_frame = params_.doIdentification && is_device;
-    if (need_frame) {
-        ensure_frame_pinned(size_t(w) * h);
-        CCTAGB_CUDA(cudaMemcpyAsync(frame_pinned_, pipe_.level0_src(), size_t(w) * h, cudaMemcpyDeviceToHost,
-                                    pipe_.stream()));
-        pipe_.add_io(0, (long long)w * h, 0);
-    }
     pipe_.download_levels(hl);
     const auto t1d = clk::now();
     auto fill_level = [&](int l) {
@@ -320,54 +366,75 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     std::vector<MarkerCand> markers;
     for (int l = nl - 1; l >= 0; --l)
         for (auto& m : jobs[l].out) markers.push_back(std::move(m));
-    geo::Pcg32 rng0(271828);
-    refit_on_level0(es[0], markers, rng0);
+    refit_on_level0(es[0], markers, [this](int n, const std::function<void(int)>& f) { pool_->parallel_for(n, f); });
     for (int l = 0; l < nl; ++l) {
         const HostLevel& L = hl[l];
         for (int i = 0; i < L.E; ++i) idxmaps_[l][size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = -1;
     }
     const auto t2 = clk::now();
 
-    // Identification.
+    // Identification: the outer points sorted by angle on the host, then cut
+    // selection and identification on the GPU, on the level-0 frame there.
     float ms_ident = 0.f, ms_cut = 0.f;
     if (params_.doIdentification && !markers.empty()) {
-        const uint8_t* img = gray;
-        size_t stride = pitch;
-        if (is_device) {
-            img = frame_pinned_;  // copied with the downloads
-            stride = size_t(w);
-        } else if (pitch != size_t(w)) {
-            frame_host_.resize(size_t(w) * h);
-            for (int y = 0; y < h; ++y) std::memcpy(&frame_host_[size_t(y) * w], gray + y * pitch, size_t(w));
-            img = frame_host_.data();
-            stride = size_t(w);
-        }
-        (void)stride;
-        std::vector<IdentTask> all(markers.size());
+        const int nm = int(markers.size());
         const auto tc0 = clk::now();
-        pool_->parallel_for(int(markers.size()), [&](int i) {
-            all[i] = IdentTask{};
-            markers[i].status = identify_step1(markers[i], img, w, h, params_, all[i]);
+        std::vector<std::vector<DirPoint>> outer(markers.size());
+        pool_->parallel_for(nm, [&](int i) {
+            outer[size_t(i)] = sorted_outer_points(markers[size_t(i)].rescaled, markers[size_t(i)].rescaled_points,
+                                                   size_t(params_.nSamplesOuterEllipse));
         });
+        int npts = 0;
+        for (const auto& o : outer) npts += int(o.size());
+        ensure_cut_capacity(nm, npts);
+        int first = 0;
+        for (int i = 0; i < nm; ++i) {
+            const MarkerCand& m = markers[size_t(i)];
+            const geo::Ellipse& e = m.rescaled;
+            const auto& o = outer[size_t(i)];
+            if (o.size() > size_t(kMaxOuterPoints))
+                throw Error{CCTAGB_BAD_ARG, "nSamplesOuterEllipse above " + std::to_string(kMaxOuterPoints)};
+            CutSelectIn& ci = h_cutin_[i];
+            ci.cx = e.cx;
+            ci.cy = e.cy;
+            ci.a = e.a;
+            ci.b = e.b;
+            ci.cosA = std::cos(e.angle);
+            ci.sinA = std::sin(e.angle);
+            ci.scale = m.scale;
+            ci.first = first;
+            ci.count = int(o.size());
+            std::copy(o.begin(), o.end(), h_cutpts_ + first);
+            first += int(o.size());
+            IdentTask& t = h_tasks_[i];
+            t = IdentTask{};
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) t.Q[r * 3 + c] = e.Q.m[r][c];
+            t.cx = e.cx;
+            t.cy = e.cy;
+            t.a = e.a;
+            t.b = e.b;
+            t.angle = e.angle;
+            t.x0 = m.cx_img;
+            t.y0 = m.cy_img;
+            t.roi[0] = 0;
+            t.roi[1] = 0;
+            t.roi[2] = w;
+            t.roi[3] = h;
+            h_st1_[i] = o.size() < 5 ? CCTAGB_TOO_FEW_OUTER_POINTS : CCTAGB_ID_RELIABLE;
+        }
         ms_cut = std::chrono::duration<float, std::milli>(clk::now() - tc0).count();
-        std::vector<IdentTask> tasks;
-        std::vector<int> task_of(markers.size(), -1);
-        for (size_t i = 0; i < markers.size(); ++i) {
-            if (markers[i].status == CCTAGB_ID_RELIABLE) {
-                task_of[i] = int(tasks.size());
-                tasks.push_back(all[i]);
+        select_and_identify(nm, npts, w, h);
+        CCTAGB_CUDA(cudaEventElapsedTime(&ms_ident, ev_id0_, ev_id1_));
+        for (int i = 0; i < nm; ++i)
+            if (h_st1_[i] == CCTAGB_ID_RELIABLE) last_tasks_.push_back(h_tasks_[i]);
+        for (int i = 0; i < nm; ++i) {
+            MarkerCand& m = markers[size_t(i)];
+            if (h_st1_[i] != CCTAGB_ID_RELIABLE) {
+                m.status = h_st1_[i];
+                continue;
             }
-        }
-        last_tasks_ = tasks;
-        std::vector<IdentResult> res(tasks.size());
-        if (!tasks.empty()) {
-            identify(tasks.data(), int(tasks.size()), res.data());
-            CCTAGB_CUDA(cudaEventElapsedTime(&ms_ident, ev_id0_, ev_id1_));
-        }
-        for (size_t i = 0; i < markers.size(); ++i) {
-            if (task_of[i] < 0) continue;
-            const IdentResult& r = res[task_of[i]];
-            MarkerCand& m = markers[i];
+            const IdentResult& r = h_res_[i];
             m.status = r.status;
             m.cx_img = r.x;
             m.cy_img = r.y;

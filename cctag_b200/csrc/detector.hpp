@@ -44,7 +44,10 @@ public:
 
 private:
     void ensure_ident_capacity(int n);
-    void ensure_frame_pinned(size_t bytes);
+    void ensure_cut_capacity(int nm, int npts);
+    // Cut selection and identification of the h_cutin_ / h_cutpts_ /
+    // h_tasks_ markers on the level-0 frame; results in h_res_, h_st1_.
+    void select_and_identify(int nm, int npts, int w, int h);
     IdentParams ident_params(int refine_mode) const;
     void identify_on(const uint8_t* d_img, size_t pitch, const IdentTask* tasks, int n, const IdentParams& ip,
                      IdentResult* out);
@@ -56,9 +59,13 @@ private:
     std::vector<HostLevel> hl_;                  // per level, pinned downloads
     std::vector<EdgeSet> es_;                    // per level, candidate-stage state
     std::shared_ptr<ThreadPool> pool_;
-    std::vector<uint8_t> frame_host_;            // pitched host frames made contiguous
-    uint8_t* frame_pinned_ = nullptr;            // device frames copied back for cut selection
-    size_t frame_pinned_cap_ = 0;
+    CutSelectIn* d_cutin_ = nullptr;             // cut selection inputs (device / pinned)
+    CutSelectIn* h_cutin_ = nullptr;
+    DirPoint* d_cutpts_ = nullptr;               // sorted outer points of all markers
+    DirPoint* h_cutpts_ = nullptr;
+    int* d_st1_ = nullptr;                       // cut selection status per marker
+    int* h_st1_ = nullptr;
+    int cut_cap_ = 0, pts_cap_ = 0;
     float* d_bank_inv_ = nullptr;                // kMaxBankIds x kMaxBankRatios
     IdentTask* d_tasks_ = nullptr;
     IdentResult* d_res_ = nullptr;

@@ -33,9 +33,34 @@ struct IdentParams {
     int coarseRounds;       // grid rounds before Gauss-Newton
 };
 
-// Cut selection of one marker (identify_step_1).  Returns the marker status
-// (CCTAGB_ID_RELIABLE when cuts were selected) and fills `task`.
-int identify_step1(const MarkerCand& m, const uint8_t* img, int W, int H, const cctagb_params& p, IdentTask& task);
+constexpr int kMaxOuterPoints = 256;    // outer points per marker (nSamplesOuterEllipse)
+constexpr int kMaxRefineSamples = 64;   // numSamplesOuterEdgePointsRefinement
+
+// Cut selection of one marker on the GPU (k_cut_select): its level-0 outer
+// ellipse and the outer points the host sorted by angle.
+struct CutSelectIn {
+    float cx, cy, a, b;     // the ellipse (cuts start at its center)
+    float cosA, sinA;       // cos / sin of its angle, computed on the host
+    float scale;            // the marker's pyramid scale (refinement length)
+    int first, count;       // its outer points in the point array
+};
+
+struct CutSelectParams {
+    float beginSig;
+    int nSamples;           // sampleCutLength
+    int nRefine;            // numSamplesOuterEdgePointsRefinement
+    int maxSelect;          // min(numCutsInIdentStep, kMaxCuts)
+};
+
+// geometry/Ellipse.cpp:259-300: up to `requested` outer points, sorted by the
+// angle around the ellipse center, uniformly subsampled.
+std::vector<DirPoint> sorted_outer_points(const geo::Ellipse& e, const std::vector<DirPoint>& pts, size_t requested);
+
+// Writes stop[] and ncuts of tasks[i] (the rest filled by the host) and
+// status[i] (CCTAGB_ID_RELIABLE, _NO_COLLECTED_CUTS or _NO_SELECTED_CUTS;
+// left alone for markers with fewer than 5 outer points).
+void launch_cut_select(const uint8_t* d_img, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
+                       IdentTask* d_tasks, int* d_status, int n, const CutSelectParams& cp, cudaStream_t s);
 
 // Signal start along the cut as a fraction of the unit radius.
 float begin_signal(int nCrowns);

@@ -743,6 +743,17 @@ __global__ void __launch_bounds__(kThreads, MB)
     const int gridN = ip.gridN;
     const int nTrials = gridN * gridN;
     const uint32_t cutMask = (T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u);
+    if (T.ncuts <= 0) {  // nothing to refine or read (identify_step_1 stopped it)
+        if (tid == 0 && crank == 0) {
+            IdentResult& R0 = res[marker];
+            R0 = IdentResult{};
+            R0.x = T.x0;
+            R0.y = T.y0;
+            R0.id = -1;
+            R0.status = CCTAGB_NO_SELECTED_CUTS;
+        }
+        return;
+    }
 
     if (tid == 0) {
         canonic_form(T.Q, S.C, S.Tp, S.Td);

@@ -166,6 +166,29 @@ def detect(gray: np.ndarray, params=None, fp64: bool = False, cap: int = 512):
     return [out[i] for i in range(min(n, cap))]
 
 
+def cut_selection(gray: np.ndarray, params=None, cap: int = 512):
+    """identify_step_1 of every candidate of a frame, in candidate order:
+    a list of (status, stops) with stops an (ncuts, 2) float32 array of the
+    selected cut ends (Identification.cpp:1172-1300)."""
+    from cctag_b200.capi import Params
+
+    lib = load()
+    lib.orc_cut_selection.argtypes = [_P, _I, _I, C.POINTER(Params), _P, _P, _P, _I, _I]
+    lib.orc_cut_selection.restype = _I
+    lib.orc_params_default.argtypes = [C.POINTER(Params), _I]
+    if params is None:
+        params = Params()
+        lib.orc_params_default(C.byref(params), 3)
+    g = np.ascontiguousarray(gray, dtype=np.uint8)
+    kc = 32
+    status = np.zeros(cap, np.int32)
+    ncuts = np.zeros(cap, np.int32)
+    stops = np.zeros((cap, kc, 2), np.float32)
+    n = lib.orc_cut_selection(_p(g), g.shape[1], g.shape[0], C.byref(params), _p(status), _p(ncuts), _p(stops), kc,
+                              cap)
+    return [(int(status[i]), stops[i, :ncuts[i]].copy()) for i in range(min(n, cap))]
+
+
 # ------------------------------------------------ batched identification --
 def _refine_sigs(lib):
     D = C.c_double

@@ -450,7 +450,8 @@ int identify_step1(const MarkerCand& m, const uint8_t* img, int W, int H, const 
         outer.push_back(pts[ang[i].second]);
     }
     if (outer.size() < 5) return CCTAGB_TOO_FEW_OUTER_POINTS;
-    const float beginSig = 1 - float(2 * p.nCrowns - 1) * 0.15f;
+    // Identification.cpp:1221-1235: the signal starts at startSig of the radius
+    const float beginSig = p.nCrowns == 3 ? 1 - float(2 * p.nCrowns - 1) * 0.15f : (p.nCrowns == 4 ? 0.26f : 0.f);
     const int n = p.sampleCutLength;
     std::vector<DirPoint> cstop;
     std::vector<float> cvar;
@@ -554,8 +555,15 @@ void update(std::vector<MarkerCand>& list, const MarkerCand& m)
 
 }  // namespace orc
 
-extern "C" int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params* pp, int fp64, orc_marker* out,
-                          int cap)
+namespace orc {
+struct StepOneRec {
+    int status;
+    std::vector<std::pair<float, float>> stops;
+};
+}  // namespace orc
+
+static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* pp, int fp64, orc_marker* out, int cap,
+                       std::vector<orc::StepOneRec>* rec)
 {
     using namespace orc;
     const cctagb_params& p = *pp;
@@ -642,13 +650,15 @@ extern "C" int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params
     });
     for (int l = nl - 1; l >= 0; --l)
         for (auto& m : jobs[l].out) markers.push_back(m);
-    geo::Pcg32 rng0(271828);
-    cctagb::refit_on_level0(es[0], markers, rng0);
+    cctagb::refit_on_level0(es[0], markers, [](int n, const std::function<void(int)>& f) {
+        for (int i = 0; i < n; ++i) f(i);
+    });
     if (p.doIdentification) {
         for (auto& m : markers) {
             std::vector<std::pair<float, float>> stops;
             const int st = identify_step1(m, gray, W, H, p, stops);
             m.status = st;
+            if (rec) rec->push_back({st, stops});
             if (st != CCTAGB_ID_RELIABLE) continue;
             IdentOut r;
             if (fp64) {
@@ -702,6 +712,32 @@ extern "C" int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params
 }
 
 // Parameters::Parameters(nCrowns) defaults (Params.hpp:27-66, Params.cpp:38-75).
+extern "C" int orc_detect(const uint8_t* gray, int W, int H, const cctagb_params* pp, int fp64, orc_marker* out,
+                          int cap)
+{
+    return detect_impl(gray, W, H, pp, fp64, out, cap, nullptr);
+}
+
+// The identify_step_1 outcome of every candidate, in candidate order: its
+// status and the selected cut ends (cap_cuts pairs per candidate).
+extern "C" int orc_cut_selection(const uint8_t* gray, int W, int H, const cctagb_params* pp, int* status, int* ncuts,
+                                 float* stops, int cap_cuts, int cap)
+{
+    std::vector<orc::StepOneRec> rec;
+    detect_impl(gray, W, H, pp, 0, nullptr, 0, &rec);
+    const int n = std::min(cap, int(rec.size()));
+    for (int i = 0; i < n; ++i) {
+        status[i] = rec[size_t(i)].status;
+        const int k = std::min(cap_cuts, int(rec[size_t(i)].stops.size()));
+        ncuts[i] = rec[size_t(i)].status == CCTAGB_ID_RELIABLE ? k : 0;
+        for (int j = 0; j < k; ++j) {
+            stops[(size_t(i) * cap_cuts + j) * 2] = rec[size_t(i)].stops[size_t(j)].first;
+            stops[(size_t(i) * cap_cuts + j) * 2 + 1] = rec[size_t(i)].stops[size_t(j)].second;
+        }
+    }
+    return int(rec.size());
+}
+
 extern "C" void orc_params_default(cctagb_params* p, int nCrowns)
 {
     std::memset(p, 0, sizeof(*p));

@@ -71,6 +71,22 @@ def test_detect_matches_oracle(detector, orc, name, seed):
             assert np.hypot(g.x - w.x, g.y - w.y) <= 0.05, (g.x, g.y, w.x, w.y)
 
 
+@pytest.mark.parametrize("name,seed", [("c1_720p", 1), ("c1_720p", 3), ("c2_1080p", 2), ("small", 4)])
+def test_cut_selection_matches_oracle_bits(detector, orc, name, seed):
+    """Cut collection, outer-edge refinement and uniform selection on the GPU
+    (identify_step_1 after the angular sort) select the same cut ends as the
+    oracle's restatement, bit for bit, for every candidate it keeps."""
+    fr = config_frame(name, seed=seed)
+    detector.detect(fr.image)
+    tasks = detector.last_tasks()
+    want = [stops for st, stops in orc.cut_selection(fr.image) if st == 1]
+    assert len(tasks) == len(want) and len(want) > 0
+    for t, w in zip(tasks, want):
+        got = np.array([[t.stop[k][0], t.stop[k][1]] for k in range(t.ncuts)], np.float32).reshape(-1, 2)
+        assert got.shape == w.shape, (got.shape, w.shape)
+        assert np.array_equal(got.view(np.uint32), w.view(np.uint32)), np.abs(got - w).max()
+
+
 def test_cpp_shim_example_runs(built_library, tmp_path):
     """The C++ drop-in example (reference-style cctagDetection) finds the
     markers of a rendered frame."""
