@@ -339,7 +339,7 @@ def run_b200(args, rank, world, local):
     stages["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++), includes the "
                                  "edge-point download"}
     stages["download"] = {"ms": round(statistics.median(dl_ms), 4), "where": "D2H of the edge-point collections"}
-    stages["host_cut_selection"] = {"ms": round(statistics.median(cut_ms), 4), "where": "host CPU (C++)"}
+    stages["host_outer_point_sort"] = {"ms": round(statistics.median(cut_ms), 4), "where": "host CPU (C++): outer points sorted by angle; cut selection then runs on the GPU just before identification"}
     # Roofline object for the dominant HBM-class kernel group of the image stage.
     top = max(stage_ms, key=lambda k: stage_ms[k])
     traffic = profiled_traffic(args.config).get(top)

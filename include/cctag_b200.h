@@ -143,7 +143,7 @@ typedef struct cctagb_stats {
     long long d2h_bytes;       /* device->host bytes copied by the call */
     int kernel_launches;       /* kernels launched by the call         */
     float ms_download;         /* host wall time of the edge-point downloads */
-    float ms_cut_selection;    /* host wall time of cut selection (identify_step_1) */
+    float ms_cut_selection;    /* host wall time of the cut-selection set-up (outer points sorted by angle, tasks filled); the cut selection itself then runs on the GPU, just before identification */
 } cctagb_stats;
 
 typedef struct cctagb_handle cctagb_handle;
