@@ -74,7 +74,7 @@ void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t 
     float averageVote = float(es.voters(p));
     static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
     while (i < maxLength && found && averageVote >= averageVoteMin) {
-        const float angle = std::fmod(std::atan2(es.dy(p), es.dx(p)) + 2.0f * kPi, 2.0f * kPi);
+        const float angle = std::fmod(pm::atan2f_(es.dy(p), es.dx(p)) + 2.0f * kPi, 2.0f * kPi);
         ring[(head + count) % (window + 1)] = angle;
         if (++count > window) {
             head = (head + 1) % (window + 1);
@@ -95,10 +95,10 @@ void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t 
                     es.link_stamp[es.at(sx, sy)] != es.link_token) {
                     const float d = phi_back() - phi_front();
                     if (count == window) {
-                        if (float(dir) * std::sin(d) < 0.0f) stop = kConvexityLost;
+                        if (float(dir) * pm::sinf_(d) < 0.0f) stop = kConvexityLost;
                     } else {
-                        const float s = float(dir) * std::sin(d);
-                        const float c = std::cos(d);
+                        const float s = float(dir) * pm::sinf_(d);
+                        const float c = pm::cosf_(d);
                         if ((s < -0.707f && c > 0.f) || (s < 0.f && c < 0.f)) stop = kConvexityLost;
                     }
                     if (stop == 0) {

@@ -11,21 +11,23 @@
 #include <stdexcept>
 #include <vector>
 
+#include "pmath.hpp"
+
 namespace cctagb {
 namespace geo {
 
 struct Mat3 {
     float m[3][3];
-    float& operator()(int r, int c) { return m[r][c]; }
-    float operator()(int r, int c) const { return m[r][c]; }
-    static Mat3 zero()
+    CCTAGB_HD float& operator()(int r, int c) { return m[r][c]; }
+    CCTAGB_HD float operator()(int r, int c) const { return m[r][c]; }
+    CCTAGB_HD static Mat3 zero()
     {
         Mat3 z;
         for (auto& r : z.m)
             for (float& v : r) v = 0.f;
         return z;
     }
-    static Mat3 eye()
+    CCTAGB_HD static Mat3 eye()
     {
         Mat3 z = zero();
         z.m[0][0] = z.m[1][1] = z.m[2][2] = 1.f;
@@ -33,7 +35,7 @@ struct Mat3 {
     }
 };
 
-inline Mat3 mul(const Mat3& a, const Mat3& b)
+CCTAGB_HD inline Mat3 mul(const Mat3& a, const Mat3& b)
 {
     Mat3 r;
     for (int i = 0; i < 3; ++i)
@@ -41,7 +43,7 @@ inline Mat3 mul(const Mat3& a, const Mat3& b)
     return r;
 }
 
-inline Mat3 transpose(const Mat3& a)
+CCTAGB_HD inline Mat3 transpose(const Mat3& a)
 {
     Mat3 r;
     for (int i = 0; i < 3; ++i)
@@ -85,6 +87,56 @@ inline void apply_h(const Mat3& H, float x, float y, float& ox, float& oy)
 }
 
 // ------------------------------------------------------------------ ellipse --
+// Ellipse.cpp:223-241: Q = R^-T diag(1/a^2, 1/b^2, -1) R^-1 with R the rigid
+// transform of the ellipse frame.
+CCTAGB_HD inline Mat3 conic_of_params(float cx, float cy, float a, float b, float angle)
+{
+    const float c = pm::cosf_(angle), s = pm::sinf_(angle);
+    Mat3 Ri;  // inverse of [c -s cx; s c cy; 0 0 1]
+    Ri.m[0][0] = c;  Ri.m[0][1] = s; Ri.m[0][2] = -(c * cx + s * cy);
+    Ri.m[1][0] = -s; Ri.m[1][1] = c; Ri.m[1][2] = s * cx - c * cy;
+    Ri.m[2][0] = 0;  Ri.m[2][1] = 0; Ri.m[2][2] = 1;
+    Mat3 D = Mat3::zero();
+    D.m[0][0] = 1.f / (a * a);
+    D.m[1][1] = 1.f / (b * b);
+    D.m[2][2] = -1.f;
+    return mul(transpose(Ri), mul(D, Ri));
+}
+
+// Ellipse.cpp:103-159: center, semi axes and angle of the conic Q.  All zero
+// when the conic is degenerate (Auu or Avv zero); returns false when a semi
+// axis comes out negative (the reference throws).
+CCTAGB_HD inline bool params_of_conic(const Mat3& Q, float& cx, float& cy, float& a, float& b, float& angle)
+{
+    const float p0 = Q.m[0][0], p1 = 2.f * Q.m[0][1], p2 = Q.m[1][1], p3 = 2.f * Q.m[0][2],
+                p4 = 2.f * Q.m[1][2], p5 = Q.m[2][2];
+    const float th = 0.5f * pm::atan2f_(p1, p0 - p2);
+    const float ct = pm::cosf_(th), st = pm::sinf_(th);
+    const float s2 = st * st, c2 = ct * ct, cs = st * ct;
+    const float Ao = p5;
+    const float Au = p3 * ct + p4 * st;
+    const float Av = -p3 * st + p4 * ct;
+    const float Auu = p0 * c2 + p2 * s2 + p1 * cs;
+    const float Avv = p0 * s2 + p2 * c2 - p1 * cs;
+    if (Auu == 0.f || Avv == 0.f) {
+        cx = cy = a = b = angle = 0.f;
+        return true;
+    }
+    const float tu = -Au / (2.f * Auu);
+    const float tv = -Av / (2.f * Avv);
+    const float wc = Ao - Auu * tu * tu - Avv * tv * tv;
+    cx = tu * ct - tv * st;
+    cy = tu * st + tv * ct;
+    const float Ru = -wc / Auu, Rv = -wc / Avv;
+    const float aa = ::sqrtf(::fabsf(Ru)) * float((Ru > 0) - (Ru < 0));
+    const float bb = ::sqrtf(::fabsf(Rv)) * float((Rv > 0) - (Rv < 0));
+    if (aa < 0.f || bb < 0.f) return false;
+    a = aa;
+    b = bb;
+    angle = th;
+    return true;
+}
+
 // geometry/Ellipse.cpp: an ellipse is held both as parameters (center, semi
 // axes, angle) and as its conic matrix Q (x^T Q x = 0, negative inside).
 struct Ellipse {
@@ -110,50 +162,10 @@ struct Ellipse {
         e.compute_parameters();
         return e;
     }
-    // Ellipse.cpp:223-241: Q = R^-T diag(1/a^2, 1/b^2, -1) R^-1 with R the
-    // rigid transform of the ellipse frame.
-    void compute_matrix()
-    {
-        const float c = std::cos(angle), s = std::sin(angle);
-        Mat3 Ri;  // inverse of [c -s cx; s c cy; 0 0 1]
-        Ri.m[0][0] = c;  Ri.m[0][1] = s; Ri.m[0][2] = -(c * cx + s * cy);
-        Ri.m[1][0] = -s; Ri.m[1][1] = c; Ri.m[1][2] = s * cx - c * cy;
-        Ri.m[2][0] = 0;  Ri.m[2][1] = 0; Ri.m[2][2] = 1;
-        Mat3 D = Mat3::zero();
-        D.m[0][0] = 1.f / (a * a);
-        D.m[1][1] = 1.f / (b * b);
-        D.m[2][2] = -1.f;
-        Q = mul(transpose(Ri), mul(D, Ri));
-    }
-    // Ellipse.cpp:103-159
+    void compute_matrix() { Q = conic_of_params(cx, cy, a, b, angle); }
     void compute_parameters()
     {
-        const float p0 = Q.m[0][0], p1 = 2.f * Q.m[0][1], p2 = Q.m[1][1], p3 = 2.f * Q.m[0][2],
-                    p4 = 2.f * Q.m[1][2], p5 = Q.m[2][2];
-        const float th = 0.5f * std::atan2(p1, p0 - p2);
-        const float ct = std::cos(th), st = std::sin(th);
-        const float s2 = st * st, c2 = ct * ct, cs = st * ct;
-        const float Ao = p5;
-        const float Au = p3 * ct + p4 * st;
-        const float Av = -p3 * st + p4 * ct;
-        const float Auu = p0 * c2 + p2 * s2 + p1 * cs;
-        const float Avv = p0 * s2 + p2 * c2 - p1 * cs;
-        if (Auu == 0.f || Avv == 0.f) {
-            cx = cy = a = b = angle = 0.f;
-            return;
-        }
-        const float tu = -Au / (2.f * Auu);
-        const float tv = -Av / (2.f * Avv);
-        const float wc = Ao - Auu * tu * tu - Avv * tv * tv;
-        cx = tu * ct - tv * st;
-        cy = tu * st + tv * ct;
-        const float Ru = -wc / Auu, Rv = -wc / Avv;
-        const float aa = std::sqrt(std::fabs(Ru)) * float((Ru > 0) - (Ru < 0));
-        const float bb = std::sqrt(std::fabs(Rv)) * float((Rv > 0) - (Rv < 0));
-        if (aa < 0.f || bb < 0.f) throw std::invalid_argument("Semi axes must be real positive!");
-        a = aa;
-        b = bb;
-        angle = th;
+        if (!params_of_conic(Q, cx, cy, a, b, angle)) throw std::invalid_argument("Semi axes must be real positive!");
     }
     // Ellipse.cpp:89-94: conic of the transformed ellipse, mT^T Q mT.
     Ellipse transform(const Mat3& mT) const { return from_matrix(mul(transpose(mT), mul(Q, mT))); }
@@ -164,8 +176,8 @@ struct Ellipse {
     {
         const float q1 = Q.m[0][0], q2 = Q.m[0][1], q3 = Q.m[0][2], q4 = Q.m[1][1], q5 = Q.m[1][2], q6 = Q.m[2][2];
         const float par1 = q1, par2 = 2 * q2, par3 = q4, par4 = 2 * q3, par5 = 2 * q5;
-        const float th = 0.5f * std::atan2(par2, par1 - par3);
-        const float ct = std::cos(th), st = std::sin(th);
+        const float th = 0.5f * pm::atan2f_(par2, par1 - par3);
+        const float ct = pm::cosf_(th), st = pm::sinf_(th);
         const float s2 = st * st, c2 = ct * ct, cs = st * ct;
         const float Au = par4 * ct + par5 * st;
         const float Av = -par4 * st + par5 * ct;
@@ -271,17 +283,17 @@ inline float round_half_away(float v) { return std::round(v); }
 inline int rasterize_perimeter(const Ellipse& e)
 {
     auto pt = [&](float t, float& x, float& y) {
-        const float ex = e.a * std::cos(t), ey = e.b * std::sin(t);
-        x = ex * std::cos(e.angle) - ey * std::sin(e.angle) + e.cx;
-        y = ex * std::sin(e.angle) + ey * std::cos(e.angle) + e.cy;
+        const float ex = e.a * pm::cosf_(t), ey = e.b * pm::sinf_(t);
+        x = ex * pm::cosf_(e.angle) - ey * pm::sinf_(e.angle) + e.cx;
+        y = ex * pm::sinf_(e.angle) + ey * pm::cosf_(e.angle) + e.cy;
     };
     const float pi = 3.14159265358979323846f;
-    float a = -e.b * std::sin(e.angle) - e.b * std::cos(e.angle);
-    float b = -e.a * std::cos(e.angle) + e.a * std::sin(e.angle);
-    const float t11 = std::atan2(-a, b), t12 = t11 + pi;
-    a = -e.b * std::sin(e.angle) + e.b * std::cos(e.angle);
-    b = -e.a * std::cos(e.angle) - e.a * std::sin(e.angle);
-    const float t21 = std::atan2(-a, b), t22 = t21 + pi;
+    float a = -e.b * pm::sinf_(e.angle) - e.b * pm::cosf_(e.angle);
+    float b = -e.a * pm::cosf_(e.angle) + e.a * pm::sinf_(e.angle);
+    const float t11 = pm::atan2f_(-a, b), t12 = t11 + pi;
+    a = -e.b * pm::sinf_(e.angle) + e.b * pm::cosf_(e.angle);
+    b = -e.a * pm::cosf_(e.angle) - e.a * pm::sinf_(e.angle);
+    const float t21 = pm::atan2f_(-a, b), t22 = t21 + pi;
     float x11, y11, x12, y12, x22, y22;
     (void)t21;
     pt(t11, x11, y11);
@@ -306,7 +318,7 @@ inline int rasterize_perimeter(const Ellipse& e)
 inline void point_on_ellipse(const Ellipse& e, float px, float py, float& ox, float& oy)
 {
     const float x = px - e.cx, y = py - e.cy;
-    const float c = std::cos(e.angle), s = std::sin(e.angle);
+    const float c = pm::cosf_(e.angle), s = pm::sinf_(e.angle);
     float tx = x * c + y * s;
     float ty = -x * s + y * c;
     const float cs = std::sqrt(tx * tx / (e.a * e.a) + ty * ty / (e.b * e.b));

@@ -1,0 +1,123 @@
+// Portable sine, cosine and arctangent for the candidate stage, which runs on
+// the host (C++) and on the GPU (CUDA) and must give the same bits on both.
+// Each function is evaluated in double precision -- argument reduction by a
+// three-part pi/2 (Cody-Waite) and a polynomial fitted by gen_pmath.py -- and
+// rounded once to float, so the float results are correctly rounded except
+// within ~1e-16 of a rounding boundary.  Only IEEE +, -, *, / and floor are
+// used, with no fused multiply-add (host: -ffp-contract=off; device: the
+// translation units that include this are built with --fmad=false), so both
+// compilers perform the same operations in the same order.
+#pragma once
+
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define CCTAGB_HD __host__ __device__
+#else
+#define CCTAGB_HD
+#endif
+
+namespace cctagb {
+namespace pm {
+
+// gen_pmath.py output
+static constexpr double kSinP[7] = {-0.16666666666666666,    0.008333333333333331,  -0.00019841269841265065,
+                                    2.7557319219339963e-06, -2.505210623269685e-08, 1.605853165490743e-10,
+                                    -7.586699058841919e-13};
+static constexpr double kCosQ[7] = {0.041666666666666664,  -0.0013888888888888887, 2.480158730158465e-05,
+                                    -2.755731922140322e-07, 2.0876755791205128e-09, -1.1470460905580259e-11,
+                                    4.745872873139979e-14};
+static constexpr double kAtanR[11] = {-0.3333333333333333,  0.19999999999995652,  -0.14285714284691378,
+                                      0.11111111017100195,  -0.0909090464769147,  0.07692184699290894,
+                                      -0.06664531368831207, 0.05858311803098606,  -0.05086254851324164,
+                                      0.03925369542082372,  -0.0192025282626767};
+static constexpr double kPio2Hi = 1.5707963267341256, kPio2Mid = 6.07710050359346e-11,
+                        kPio2Lo = 2.912732056093356e-20;
+static constexpr double kPi = 3.141592653589793, kPio2 = 1.5707963267948966, kPio4 = 0.7853981633974483,
+                        kTanPio8 = 0.41421356237309503, k2OverPi = 0.6366197723675814;
+
+CCTAGB_HD inline double horner(const double* c, int n, double u)
+{
+    double s = c[n - 1];
+    for (int i = n - 2; i >= 0; --i) s = s * u + c[i];
+    return s;
+}
+
+CCTAGB_HD inline bool sign_bit(double x) { return ::copysign(1.0, x) < 0.0; }
+
+// x - k pi/2 with k the nearest integer to x 2/pi; q = k mod 4.
+CCTAGB_HD inline double reduce_pio2(double x, int& q)
+{
+    const double k = ::floor(x * k2OverPi + 0.5);
+    q = int(static_cast<long long>(k) & 3);
+    return ((x - k * kPio2Hi) - k * kPio2Mid) - k * kPio2Lo;
+}
+
+CCTAGB_HD inline double sin_poly(double r)
+{
+    const double u = r * r;
+    return r + r * (u * horner(kSinP, 7, u));
+}
+
+CCTAGB_HD inline double cos_poly(double r)
+{
+    const double u = r * r;
+    return (1.0 - 0.5 * u) + (u * u) * horner(kCosQ, 7, u);
+}
+
+CCTAGB_HD inline double sin_d(double x)
+{
+    int q;
+    const double r = reduce_pio2(x, q);
+    switch (q) {
+    case 0: return sin_poly(r);
+    case 1: return cos_poly(r);
+    case 2: return -sin_poly(r);
+    default: return -cos_poly(r);
+    }
+}
+
+CCTAGB_HD inline double cos_d(double x)
+{
+    int q;
+    const double r = reduce_pio2(x, q);
+    switch (q) {
+    case 0: return cos_poly(r);
+    case 1: return -sin_poly(r);
+    case 2: return -cos_poly(r);
+    default: return sin_poly(r);
+    }
+}
+
+// atan t for t in [0, 1]
+CCTAGB_HD inline double atan_unit(double t)
+{
+    double base = 0.0, u = t;
+    if (t > kTanPio8) {
+        u = (t - 1.0) / (t + 1.0);
+        base = kPio4;
+    }
+    const double z = u * u;
+    return base + (u + u * (z * horner(kAtanR, 11, z)));
+}
+
+// atan2 with the IEEE special cases of the zeros' signs.
+CCTAGB_HD inline double atan2_d(double y, double x)
+{
+    if (x != x || y != y) return x + y;
+    const double ax = ::fabs(x), ay = ::fabs(y);
+    double r;
+    if (ay == 0.0) r = 0.0;
+    else if (ax == ay) r = kPio4;
+    else if (ay < ax) r = atan_unit(ay / ax);
+    else r = kPio2 - atan_unit(ax / ay);
+    if (sign_bit(x)) r = kPi - r;
+    return ::copysign(r, y);
+}
+
+CCTAGB_HD inline float sinf_(float x) { return float(sin_d(double(x))); }
+CCTAGB_HD inline float cosf_(float x) { return float(cos_d(double(x))); }
+CCTAGB_HD inline float atan2f_(float y, float x) { return float(atan2_d(double(y), double(x))); }
+
+}  // namespace pm
+}  // namespace cctagb
