@@ -8,6 +8,7 @@
 // candidate order between the two loops.  The result is therefore the same
 // for every thread count and schedule.
 #include "candidates.hpp"
+#include "cand_shared.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -31,9 +32,8 @@ void EdgeSet::reset_state()
 
 namespace {
 
-constexpr int kEdgeNotFound = -1;
-constexpr int kConvexityLost = -2;
-constexpr float kPi = 3.14159265358979323846f;
+using cand::kConvexityLost;
+using cand::kEdgeNotFound;
 
 // The points one ellipse-growing run has marked (EdgePoint::_processed ==
 // runId in the reference, a test private to the run): a per-thread stamp
@@ -74,13 +74,13 @@ void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t 
     float averageVote = float(es.voters(p));
     static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
     while (i < maxLength && found && averageVote >= averageVoteMin) {
-        const float angle = std::fmod(pm::atan2f_(es.dy(p), es.dx(p)) + 2.0f * kPi, 2.0f * kPi);
+        const float angle = cand::link_angle(es.dx(p), es.dy(p));
         ring[(head + count) % (window + 1)] = angle;
         if (++count > window) {
             head = (head + 1) % (window + 1);
             --count;
         }
-        const int shifting = int(std::round(((angle + kPi / 4.0f) / (2.0f * kPi)) * 8.0f)) - 1;
+        const int shifting = cand::link_shift(angle);
         const int yoff[8] = {0, -dir, -dir, -dir, 0, dir, dir, dir};
         int j = 0;
         stop = 0;
@@ -93,20 +93,14 @@ void edge_linking_dir(EdgeSet& es, int p, int dir, std::deque<int>& seg, size_t 
                 const int sy = es.y(p) + yoff[k];
                 if (sx >= 0 && sx < es.W && sy >= 0 && sy < es.H && es.at(sx, sy) >= 0 &&
                     es.link_stamp[es.at(sx, sy)] != es.link_token) {
-                    const float d = phi_back() - phi_front();
-                    if (count == window) {
-                        if (float(dir) * pm::sinf_(d) < 0.0f) stop = kConvexityLost;
-                    } else {
-                        const float s = float(dir) * pm::sinf_(d);
-                        const float c = pm::cosf_(d);
-                        if ((s < -0.707f && c > 0.f) || (s < 0.f && c < 0.f)) stop = kConvexityLost;
-                    }
+                    if (cand::link_convexity_lost(phi_front(), phi_back(), count == window, dir))
+                        stop = kConvexityLost;
                     if (stop == 0) {
                         es.link_stamp[p] = es.link_token;
                         p = es.at(sx, sy);
                         if (dir > 0) seg.push_back(p);
                         else seg.push_front(p);
-                        averageVote = (averageVote * float(seg.size()) + float(es.voters(p))) / (float(seg.size()) + 1.f);
+                        averageVote = cand::link_average_vote(averageVote, int(seg.size()), es.voters(p));
                         stop = 1;
                     }
                     es.link_stamp[p] = es.link_token;
@@ -160,34 +154,6 @@ void children_of(const EdgeSet& es, const std::deque<int>& seg, std::vector<int>
 
 enum Weight { kNoWeight = 0, kInvGradWeight = 1 };
 
-// 5x5 linear solve with partial pivoting (FP64); false if singular.
-bool solve5(double A[5][5], double b[5], double x[5])
-{
-    int perm[5] = {0, 1, 2, 3, 4};
-    for (int c = 0; c < 5; ++c) {
-        int piv = c;
-        for (int r = c + 1; r < 5; ++r)
-            if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
-        if (A[piv][c] == 0.0) return false;
-        if (piv != c) {
-            for (int k = 0; k < 5; ++k) std::swap(A[piv][k], A[c][k]);
-            std::swap(b[piv], b[c]);
-            std::swap(perm[piv], perm[c]);
-        }
-        for (int r = c + 1; r < 5; ++r) {
-            const double f = A[r][c] / A[c][c];
-            for (int k = c; k < 5; ++k) A[r][k] -= f * A[c][k];
-            b[r] -= f * b[c];
-        }
-    }
-    for (int r = 4; r >= 0; --r) {
-        double s = b[r];
-        for (int k = r + 1; k < 5; ++k) s -= A[r][k] * x[k];
-        x[r] = s / A[r][r];
-    }
-    return true;
-}
-
 // geo::dist_point_ellipse over a point array, as a loop the compiler can
 // vectorise (same operations per point, so the same values).
 void dist_to_ellipse(const geo::Mat3& Q, const Pt* p, size_t n, float* out)
@@ -204,18 +170,13 @@ void dist_to_ellipse(const geo::Mat3& Q, const Pt* p, size_t n, float* out)
     }
 }
 
-// Whether median_ref(v) (the element of rank n/2) is below `bound`, without
-// selecting it: that holds exactly when at least n/2 + 1 elements are.  -1
-// when a NaN makes the ranks ill-defined (the caller then selects).
-int median_below(const float* v, size_t n, float bound)
+// Whether median_ref(v) (the element of rank n/2, NaN last) is below `bound`,
+// without selecting it: that holds exactly when at least n/2 + 1 elements are.
+bool median_below(const float* v, size_t n, float bound)
 {
-    size_t below = 0, nan = 0;
-    for (size_t i = 0; i < n; ++i) {
-        below += v[i] < bound;
-        nan += v[i] != v[i];
-    }
-    if (nan) return -1;
-    return below >= n / 2 + 1 ? 1 : 0;
+    size_t below = 0;
+    for (size_t i = 0; i < n; ++i) below += v[i] < bound;
+    return below >= n / 2 + 1;
 }
 
 // Vote.cpp:414-576 outlierRemoval: LMedS ellipse from random 5-point subsets
@@ -250,55 +211,30 @@ void outlier_removal(const EdgeSet& es, const std::vector<int>& children, std::v
     while (counter < 70 && draws < 7000) {
         ++draws;
         rng.rand5(perm, pts.size());
-        double A[5][5], b[5], t[5];
-        for (int i = 0; i < 5; ++i) {
-            const double x = pts[perm[i]].x, y = pts[perm[i]].y;
-            A[i][0] = x * x;
-            A[i][1] = 2.0 * x * y;
-            A[i][2] = y * y;
-            A[i][3] = 2.0 * x;
-            A[i][4] = 2.0 * y;
-            b[i] = -1.0;
-        }
-        if (!solve5(A, b, t)) {
-            ++counter;
-            continue;
-        }
-        if (!(float(t[0]) * float(t[2]) - float(t[1]) * float(t[1]) > 0)) {
-            ++counter;
-            continue;
-        }
         geo::Mat3 Q;
-        Q.m[0][0] = float(t[0]);
-        Q.m[0][1] = Q.m[1][0] = float(t[1]);
-        Q.m[0][2] = Q.m[2][0] = float(t[3]);
-        Q.m[1][1] = float(t[2]);
-        Q.m[1][2] = Q.m[2][1] = float(t[4]);
-        Q.m[2][2] = 1.f;
-        try {
-            const Ellipse q = Ellipse::from_matrix(Q);
-            const float ratio = q.a / q.b;
-            if (ratio < 0.04f || ratio > 25) {
-                ++counter;
-                continue;
-            }
-            dist_to_ellipse(q.Q, pts.data(), pts.size(), dist.data());
+        const int kind = cand::lmeds_conic(pts.data(), perm, Q);
+        if (kind == 0) {
+            ++counter;
+            continue;
+        }
+        if (kind == 2) continue;  // the reference's exception: not counted
+        {
+            dist_to_ellipse(Q, pts.data(), pts.size(), dist.data());
             if (weightedType != kNoWeight)
                 for (size_t i = 0; i < dist.size(); ++i) dist[i] *= weights[i];
             // most draws do not improve on Sm: decide that by counting
-            if (median_below(dist.data(), dist.size(), Sm) == 0) {
+            if (!median_below(dist.data(), dist.size(), Sm)) {
                 ++counter;
                 continue;
             }
             const float S = geo::median_ref(dist);
             if (S < Sm) {
                 counter = 0;
-                qm = q;
+                qm.Q = Q;
                 Sm = S;
             } else {
                 ++counter;
             }
-        } catch (...) {
         }
     }
     std::vector<float> vd;
@@ -651,7 +587,7 @@ bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& ou
             d.resize(P.size());
             dist_to_ellipse(q.Q, P.data(), P.size(), d.data());
             // S = S1 + S2 >= S1 (S2 >= 0): no improvement unless S1 < Sm
-            if (median_below(d.data(), d.size(), Sm) == 0) {
+            if (!median_below(d.data(), d.size(), Sm)) {
                 ++cnt;
                 continue;
             }
@@ -810,7 +746,7 @@ void link_level(EdgeSet& es, const std::vector<int32_t>& seeds, const cctagb_par
 // candidates are spread over threads.
 geo::Pcg32 candidate_rng(int level, size_t index, int phase)
 {
-    return geo::Pcg32(271828, (uint64_t(level) << 32) | (uint64_t(index) << 1) | uint64_t(phase));
+    return cand::candidate_rng(level, uint64_t(index), phase);
 }
 
 }  // namespace

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <stdexcept>
 #include <vector>
 
@@ -235,7 +236,7 @@ inline void compute_hull(const Ellipse& e, float delta, Ellipse& qIn, Ellipse& q
 
 // geometry/Distance.cpp:18-43 (the scalar path): squared algebraic distance
 // normalised by the squared gradient norm of the conic at p.
-inline float dist_point_ellipse(const Mat3& Q, float x, float y)
+CCTAGB_HD inline float dist_point_ellipse(const Mat3& Q, float x, float y)
 {
     const float aux0 = x * x, aux1 = 2 * x * y, aux2 = 2 * x, aux3 = y * y, aux4 = 2 * y;
     const float t1 = x * Q.m[0][0] + y * Q.m[0][1] + Q.m[0][2];
@@ -351,21 +352,21 @@ struct Pcg32 {
     static constexpr uint64_t kMul = 6364136223846793005ULL;
     static constexpr uint64_t kInc = 1442695040888963407ULL;
     uint64_t inc = kInc;
-    explicit Pcg32(uint64_t seed = 271828) { reseed(seed); }
+    CCTAGB_HD explicit Pcg32(uint64_t seed = 271828) { reseed(seed); }
     // Stream `stream` of the generator (PCG's selectable increment).
-    Pcg32(uint64_t seed, uint64_t stream) : inc((stream << 1) | 1u)
+    CCTAGB_HD Pcg32(uint64_t seed, uint64_t stream) : inc((stream << 1) | 1u)
     {
         state = 0;
         state = state * kMul + inc;
         state += seed;
         state = state * kMul + inc;
     }
-    void reseed(uint64_t seed)
+    CCTAGB_HD void reseed(uint64_t seed)
     {
         inc = kInc;
         state = (seed + kInc) * kMul + kInc;
     }
-    uint32_t next()
+    CCTAGB_HD uint32_t next()
     {
         const uint64_t old = state;
         state = old * kMul + inc;
@@ -373,7 +374,7 @@ struct Pcg32 {
         const uint32_t rot = uint32_t(old >> 59);
         return (xs >> rot) | (xs << ((32u - rot) & 31u));
     }
-    uint32_t bounded(uint32_t n)
+    CCTAGB_HD uint32_t bounded(uint32_t n)
     {
         const uint32_t threshold = uint32_t(-n) % n;
         for (;;) {
@@ -382,25 +383,40 @@ struct Pcg32 {
         }
     }
     // Five distinct indices in [0, n) (Statistic.cpp:16-29).
-    void rand5(int perm[5], size_t n)
+    CCTAGB_HD void rand5(int perm[5], size_t n)
     {
         for (int i = 0; i < 5; ++i) perm[i] = -1;
         for (int i = 0; i < 5; ++i) {
             int r;
+            bool seen;
             do {
                 r = int(bounded(uint32_t(n)));
-            } while (std::find(perm, perm + i, r) != perm + i);
+                seen = false;
+                for (int j = 0; j < i; ++j) seen = seen || perm[j] == r;
+            } while (seen);
             perm[i] = r;
         }
     }
 };
 
+// Order key of a float with every NaN above +inf: the total order the
+// medians use, so that an array holding NaNs has one well-defined median on
+// every platform (the reference's nth_element leaves it unspecified).
+CCTAGB_HD inline uint32_t order_key(float v)
+{
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    if (v != v) return 0xffffffffu;
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
 // Statistic.hpp:112-117 (medianRef): the element at index size/2 of the
-// sorted values; nth_element yields the same element without a full sort.
-// The vector is reordered.
+// sorted values (NaN last); nth_element yields it without a full sort.  The
+// vector is reordered.
 inline float median_ref(std::vector<float>& v)
 {
-    std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
+    std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end(),
+                     [](float a, float b) { return order_key(a) < order_key(b); });
     return v[v.size() / 2];
 }
 
