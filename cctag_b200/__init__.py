@@ -13,6 +13,10 @@ import numpy as np
 from . import capi
 from .capi import CCTagError, Params, default_params
 
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
 __all__ = ["Detector", "CCTagError", "Params", "default_params", "capi"]
 
 
@@ -226,6 +230,24 @@ class Detector:
             if key is not None:
                 self._inflight.pop(key, None)
         return [out[i] for i in range(n.value)], stats
+
+    def level_loop_two(self, level: int):
+        """Loop-two inputs of one level from the last detect (GPU loop 1 and
+        outlier removal): (seed, score, keep, filtered) with filtered a list
+        of int32 arrays (empty for candidates not kept)."""
+        cap, fcap = 4096, 1 << 22
+        seed = np.zeros(cap, np.int32)
+        score = np.zeros(cap, np.int32)
+        keep = np.zeros(cap, np.int32)
+        nflt = np.zeros(cap, np.int32)
+        flt = np.zeros(fcap, np.int32)
+        n, nt = C.c_int(), C.c_int()
+        self._check(self._lib.cctagb_level_loop_two(self._h, level, cap, _ptr(seed), _ptr(score), _ptr(keep),
+                                                    _ptr(nflt), C.byref(n), fcap, _ptr(flt), C.byref(nt)),
+                    "level_loop_two")
+        k = n.value
+        offs = np.concatenate([[0], np.cumsum(nflt[:k])])
+        return seed[:k].copy(), score[:k].copy(), keep[:k].copy(), [flt[offs[i]:offs[i + 1]].copy() for i in range(k)]
 
     # -- identification of caller-given candidates ---------------------------
     def last_tasks(self):

@@ -24,6 +24,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function", "-ffp-contract=off"]
+# Translation units whose float arithmetic must equal the host restatement's
+# bit for bit: no contraction of a * b + c into a fused multiply-add.
+NO_FMAD = {"loop_one"}
 
 
 def _sources():
@@ -54,7 +57,8 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     objs = []
     for src in cu:
         obj = BUILD / (src.stem + ".cu.o")
-        _run([NVCC, *ARCH, *CUDA_FLAGS, *inc, "-c", src, "-o", obj], verbose)
+        extra = ["--fmad=false"] if src.stem in NO_FMAD else []
+        _run([NVCC, *ARCH, *CUDA_FLAGS, *extra, *inc, "-c", src, "-o", obj], verbose)
         objs.append(obj)
     for src in cpp:
         obj = BUILD / (src.stem + ".o")

@@ -104,6 +104,7 @@ SIGNATURES = {
     "cctagb_level_links": (_I, [_P, _I, _I, _P, _P]),
     "cctagb_level_votes": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _I, _P]),
     "cctagb_level_seeds": (_I, [_P, _I, _I, _P, C.POINTER(_I)]),
+    "cctagb_level_loop_two": (_I, [_P, _I, _I, _P, _P, _P, _P, C.POINTER(_I), _I, _P, C.POINTER(_I)]),
     "cctagb_canny_from_derivatives": (_I, [_P, _P, _P, _I, _I, _P]),
     "cctagb_get_stream": (_I, [_P, C.POINTER(_P)]),
     "cctagb_set_stage_timing": (_I, [_P, _I]),

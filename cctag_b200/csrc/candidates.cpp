@@ -751,30 +751,81 @@ geo::Pcg32 candidate_rng(int level, size_t index, int phase)
 
 }  // namespace
 
-void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf)
+namespace {
+
+struct LevelState {
+    std::vector<Candidate> loop1, loop2;
+    std::vector<uint8_t> keep;
+    std::vector<std::vector<MarkerCand>> out3;
+};
+
+// Phases A (loop 1, one task per level) and B (children and outlier removal,
+// one task per candidate).
+void phases_a_b(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
+                std::vector<LevelState>& st)
 {
     const int nl = int(jobs.size());
-    struct State {
-        std::vector<Candidate> loop1, loop2;
-        std::vector<uint8_t> keep;
-        std::vector<std::vector<MarkerCand>> out3;
-    };
-    std::vector<State> st(static_cast<size_t>(nl));
-    // Phase A: loop 1, one task per level.
     pf(nl, [&](int l) { link_level(*jobs[l].es, *jobs[l].seeds, p, st[l].loop1); });
-    // Flat task list over (level, candidate) of loop 2.
     std::vector<std::pair<int, int>> tasks;
     for (int l = 0; l < nl; ++l) {
         const size_t n2 = std::min(st[l].loop1.size(), size_t(p.maximumNbCandidatesLoopTwo));
         st[l].keep.assign(n2, 0);
         for (size_t i = 0; i < n2; ++i) tasks.emplace_back(l, int(i));
     }
-    // Phase B: children and outlier removal.
     pf(int(tasks.size()), [&](int t) {
         const int l = tasks[t].first, i = tasks[t].second;
         geo::Pcg32 rng = candidate_rng(jobs[l].level, size_t(i), 0);
         st[l].keep[i] = flow_component_filter(st[l].loop1[i], *jobs[l].es, p, rng) ? 1 : 0;
     });
+}
+
+}  // namespace
+
+void link_and_filter(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
+                     std::vector<LoopTwoIn>& out)
+{
+    std::vector<LevelState> st(jobs.size());
+    phases_a_b(jobs, p, pf, st);
+    out.assign(jobs.size(), {});
+    for (size_t l = 0; l < jobs.size(); ++l) {
+        LoopTwoIn& o = out[l];
+        o.foff.push_back(0);
+        for (size_t i = 0; i < st[l].keep.size(); ++i) {
+            const Candidate& c = st[l].loop1[i];
+            o.seed.push_back(c.seed);
+            o.score.push_back(c.score);
+            o.keep.push_back(st[l].keep[i]);
+            if (st[l].keep[i]) o.flt.insert(o.flt.end(), c.filtered.begin(), c.filtered.end());
+            o.foff.push_back(int32_t(o.flt.size()));
+        }
+    }
+}
+
+void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
+                       const std::vector<LoopTwoIn>* given)
+{
+    const int nl = int(jobs.size());
+    std::vector<LevelState> st(static_cast<size_t>(nl));
+    if (!given) {
+        phases_a_b(jobs, p, pf, st);
+    } else {
+        if (given->size() != jobs.size()) throw std::runtime_error("loop-two inputs do not match the levels");
+        for (int l = 0; l < nl; ++l) {
+            const LoopTwoIn& g = (*given)[size_t(l)];
+            const size_t n2 = g.seed.size();
+            st[l].loop1.resize(n2);
+            st[l].keep.assign(g.keep.begin(), g.keep.end());
+            for (size_t i = 0; i < n2; ++i) {
+                Candidate& c = st[l].loop1[i];
+                c.seed = g.seed[i];
+                c.score = g.score[i];
+                c.filtered.assign(g.flt.begin() + g.foff[i], g.flt.begin() + g.foff[i + 1]);
+            }
+        }
+    }
+    std::vector<std::pair<int, int>> tasks;
+    for (int l = 0; l < nl; ++l)
+        for (size_t i = 0; i < st[l].keep.size(); ++i) tasks.emplace_back(l, int(i));
     // Phase C: segment labels in candidate order.
     for (int l = 0; l < nl; ++l) {
         size_t nSegmentOut = 0;

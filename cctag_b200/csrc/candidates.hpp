@@ -77,12 +77,29 @@ struct LevelJob {
 // have finished.
 using ParallelFor = std::function<void(int, const std::function<void(int)>&)>;
 
+// One level's first maximumNbCandidatesLoopTwo loop-1 candidates (in loop-1
+// order) after the children collection and LMedS outlier removal of loop 2
+// (Detection.cpp:115-156): their seed, children count (score), whether they
+// go on to the ellipse growing (keep), and their filtered children.
+struct LoopTwoIn {
+    std::vector<int32_t> seed, score;
+    std::vector<uint8_t> keep;
+    std::vector<int32_t> foff;  // candidate i: flt[foff[i], foff[i + 1]) (empty unless kept)
+    std::vector<int32_t> flt;
+};
+
+// Loop 1 and the outlier removal of loop 2 on the host, per level.
+void link_and_filter(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
+                     std::vector<LoopTwoIn>& out);
+
 // Candidate markers of every level (cctagDetectionFromEdges, Detection.cpp:
 // 568-693).  Loop 1 runs per level in seed order; loops 2 and 3 run per
 // candidate (each with its own PCG32 stream, seed 271828), with the segment
 // labels of loop 2 assigned in candidate order between them, so the result is
-// the same for any ParallelFor.
-void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf);
+// the same for any ParallelFor.  With `given`, loop 1 and the outlier removal
+// are taken from it (computed on the GPU) instead of being run here.
+void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
+                       const std::vector<LoopTwoIn>* given = nullptr);
 
 // Level-0 re-fit of markers detected on coarser levels (Multiresolution.cpp:
 // 319-401), markers in parallel, each with its own PCG32 stream.

@@ -369,6 +369,30 @@ cctagb_status cctagb_level_seeds(cctagb_handle* h, int level, int cap, int32_t* 
     });
 }
 
+cctagb_status cctagb_level_loop_two(cctagb_handle* h, int level, int cap, int32_t* seed, int32_t* score,
+                                    int32_t* keep, int32_t* n_filtered, int* n, int filtered_cap,
+                                    int32_t* filtered, int* n_filtered_total)
+{
+    if (!h || !n || !n_filtered_total) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] {
+        const auto& all = h->det->last_loop_two();
+        if (level < 0 || level >= int(all.size())) throw cctagb::Error{CCTAGB_BAD_ARG, "level out of range"};
+        const cctagb::LoopTwoIn& g = all[size_t(level)];
+        *n = int(g.seed.size());
+        *n_filtered_total = int(g.flt.size());
+        if (*n > cap || *n_filtered_total > filtered_cap)
+            throw cctagb::Error{CCTAGB_BAD_ARG, "output capacity too small"};
+        for (int i = 0; i < *n; ++i) {
+            if (seed) seed[i] = g.seed[size_t(i)];
+            if (score) score[i] = g.score[size_t(i)];
+            if (keep) keep[i] = g.keep[size_t(i)];
+            if (n_filtered) n_filtered[i] = g.foff[size_t(i) + 1] - g.foff[size_t(i)];
+        }
+        if (filtered) std::copy(g.flt.begin(), g.flt.end(), filtered);
+    });
+}
+
 cctagb_status cctagb_get_stream(cctagb_handle* h, void** stream)
 {
     if (!h || !stream) return CCTAGB_BAD_ARG;

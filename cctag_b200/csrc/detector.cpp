@@ -36,6 +36,9 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, 
     hl_.resize(idxmaps_.size());
     es_.resize(idxmaps_.size());
     if (!pool_) pool_ = make_host_pool(p.hostThreads);
+    std::vector<int> caps;
+    for (int l = 0; l < p.numberOfProcessedMultiresLayers; ++l) caps.push_back(pipe_.level_capacity(l));
+    loop1_ = std::make_unique<LoopOneGpu>(p, max_h, caps);
 }
 
 Detector::~Detector()
@@ -335,6 +338,17 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     std::vector<EdgeSet>& es = es_;
     pipe_.download_levels(hl);
     const auto t1d = clk::now();
+    // Loop 1 and the outlier removal run on the GPU while the host indexes the
+    // edge points.
+    {
+        std::vector<const std::vector<int32_t>*> seeds(static_cast<size_t>(nl));
+        int E[kMaxLevels] = {};
+        for (int l = 0; l < nl; ++l) {
+            seeds[size_t(l)] = &hl[l].seeds;
+            E[l] = hl[l].E;
+        }
+        loop1_->launch(pipe_.level_views(), E, seeds, pipe_.stream());
+    }
     auto fill_level = [&](int l) {
         EdgeSet& e = es[l];
         const HostLevel& L = hl[l];
@@ -353,6 +367,8 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         e.reset_state();
     };
     pool_->parallel_for(nl, fill_level);
+    loop1_->collect(pipe_.stream(), loop2in_);
+    pipe_.add_io(loop1_->h2d_bytes(), loop1_->d2h_bytes(), loop1_->launches());
     std::vector<LevelJob> jobs(nl);
     for (int l = 0; l < nl; ++l) {
         jobs[l].es = &es[l];
@@ -360,8 +376,8 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         jobs[l].level = l;
         jobs[l].scale = float(1 << l);
     }
-    detect_from_edges(jobs, params_,
-                      [this](int n, const std::function<void(int)>& f) { pool_->parallel_for(n, f); });
+    detect_from_edges(
+        jobs, params_, [this](int n, const std::function<void(int)>& f) { pool_->parallel_for(n, f); }, &loop2in_);
     // Coarse levels first, as the reference's loop from the top level down.
     std::vector<MarkerCand> markers;
     for (int l = nl - 1; l >= 0; --l)

@@ -9,6 +9,7 @@
 #include "candidates.hpp"
 #include "thread_pool.hpp"
 #include "ident_host.hpp"
+#include "loop_one.hpp"
 #include "pipeline.hpp"
 
 namespace cctagb {
@@ -41,6 +42,8 @@ public:
                   const float* centers, float* cost, float* d_center, float* d_h);
     // Tasks handed to the identification kernel by the last detect().
     const std::vector<IdentTask>& last_tasks() const { return last_tasks_; }
+    // Loop-two inputs (GPU loop 1 + outlier removal) of the last detect().
+    const std::vector<LoopTwoIn>& last_loop_two() const { return loop2in_; }
 
 private:
     void ensure_ident_capacity(int n);
@@ -58,6 +61,8 @@ private:
     std::vector<std::vector<int32_t>> idxmaps_;  // per level, -1 where no edge point
     std::vector<HostLevel> hl_;                  // per level, pinned downloads
     std::vector<EdgeSet> es_;                    // per level, candidate-stage state
+    std::unique_ptr<LoopOneGpu> loop1_;          // loop 1 + outlier removal on the GPU
+    std::vector<LoopTwoIn> loop2in_;             // its results for the last frame
     std::shared_ptr<ThreadPool> pool_;
     CutSelectIn* d_cutin_ = nullptr;             // cut selection inputs (device / pinned)
     CutSelectIn* h_cutin_ = nullptr;

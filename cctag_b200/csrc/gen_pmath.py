@@ -34,7 +34,7 @@ def report(name, f, c, powers, xs):
         if fx != 0:
             err = max(err, float(abs((v - fx) / fx)))
     print("// %s: max relative error %.2e" % (name, err))
-    print("static constexpr double k%s[%d] = {%s};" % (name, len(c), ", ".join(repr(v) for v in c)))
+    print("%s = [%s]" % (name, ", ".join(repr(v) for v in c)))
 
 
 if __name__ == "__main__":

@@ -1,0 +1,98 @@
+// Loop 1 of the candidate stage (edge linking from the seeds,
+// Detection.cpp:69-113, 609-627, Vote.cpp:255-394) and the first half of
+// loop 2 (children collection and LMedS outlier removal, Detection.cpp:
+// 115-156, Vote.cpp:396-576) on the GPU, with the same results as the host
+// restatement in candidates.cpp (shared arithmetic in cand_shared.hpp).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "candidates.hpp"
+#include "common.hpp"
+
+namespace cctagb {
+
+constexpr int kSegHalf = 100;                 // points per linking direction (maxLength)
+constexpr int kSegSlot = 2 * kSegHalf + 1;    // one segment: front, seed, back
+constexpr int kChildCap = 32768;              // children of one loop-two candidate
+constexpr int kLmedsMaxPts = 64;              // subsampled points of one outlier removal
+
+// One level as the loop-one kernels see it (device pointers).
+struct LoopOneLevel {
+    int W, H, WW, E;
+    const int32_t* exy;
+    const int32_t* grad;
+    const int32_t* voff;
+    const int32_t* vlist;
+    const uint32_t* bitmap;
+    const int32_t* idxmap;
+    const int32_t* order;   // seeds in processing order, nProc of them
+    int nProc, slot0;       // seed slots [slot0, slot0 + nProc)
+    uint8_t* processed;     // E flags (processedIn), zeroed per frame
+    int level;
+};
+
+struct LoopOneArgs {
+    int nl;
+    LoopOneLevel lv[kMaxLevels];
+    int window;             // windowSizeOnInnerEllipticSegment
+    float averageVoteMin;
+    int n2max;              // maximumNbCandidatesLoopTwo
+    int minPoints;          // minPointsSegmentCandidate
+    float threshold;        // threshRobustEstimationOfOuterEllipse
+    int totalSlots;
+    int32_t* seg;           // totalSlots * kSegSlot: segment of each seed slot, seed at kSegHalf
+    int32_t* sinfo;         // totalSlots * 4: front length, back length, marks after +1, marks after -1
+    float* skey;            // totalSlots: averageReceivedVote
+    int32_t* made;          // nl * maxSlotsPerLevel: made candidates (seed slots), per level
+    int maxSlotsPerLevel;
+    int32_t* meta;          // nl * n2max * 4: seed slot, score, keep, filtered count; then nl: made count
+    int32_t* children;      // nl * n2max * kChildCap: children, then filtered in place
+    int32_t* err;           // error bits
+};
+
+constexpr int kLoopOneErrChildren = 1;
+constexpr int kLoopOneErrWindow = 2;
+constexpr int kLoopOneErrPoints = 4;
+
+void launch_loop_one(const LoopOneArgs& a, cudaStream_t s);
+
+// Device buffers of loop 1 / loop 2 (first half) for one detection slot.
+class LoopOneGpu {
+public:
+    // max_h: largest frame height; caps: edge-point capacity of each level.
+    LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>& caps);
+    ~LoopOneGpu();
+    LoopOneGpu(const LoopOneGpu&) = delete;
+    LoopOneGpu& operator=(const LoopOneGpu&) = delete;
+
+    // Uploads the seeds (processing order), launches the kernels on `s` and
+    // queues the download of the per-candidate counts.  `E` = edge points per
+    // level.  Returns immediately.
+    void launch(const Levels& lv, const int* E, const std::vector<const std::vector<int32_t>*>& seeds,
+                cudaStream_t s);
+    // Waits for launch()'s work and fills `out` (one LoopTwoIn per level).
+    void collect(cudaStream_t s, std::vector<LoopTwoIn>& out);
+    int launches() const { return 4; }
+    long long h2d_bytes() const { return h2d_; }
+    long long d2h_bytes() const { return d2h_; }
+
+private:
+    cctagb_params p_;
+    int nl_ = 0, n2max_ = 0, maxSlotsPerLevel_ = 0, totalSlots_ = 0;
+    LoopOneArgs args_{};
+    int32_t* d_order_ = nullptr;   // all levels' seed slots
+    int32_t* h_order_ = nullptr;   // pinned staging
+    uint8_t* d_processed_ = nullptr;
+    int32_t* d_packed_ = nullptr;  // kept candidates' filtered children
+    size_t processed_bytes_ = 0;
+    std::vector<int> caps_;
+    int32_t* h_meta_ = nullptr;    // pinned: meta + made counts + err
+    int32_t* h_flt_ = nullptr;     // pinned: filtered children, all candidates
+    size_t h_flt_cap_ = 0;
+    std::vector<void*> allocs_;
+    long long h2d_ = 0, d2h_ = 0;
+};
+
+}  // namespace cctagb

@@ -44,6 +44,10 @@ public:
     void canny_only(const int16_t* dx, const int16_t* dy, int w, int h, uint8_t* edges_out);
 
     int levels() const { return lv_.n; }
+    // Device views of the levels of the last image_stage().
+    const Levels& level_views() const { return lv_; }
+    // Edge-point capacity of level l (fixed at construction).
+    int level_capacity(int l) const { return la_[l].v.cap; }
     const uint8_t* level0_src() const { return lv_.l[0].src; }
     void level_size(int l, int* w, int* h) const;
     void copy_planes(int l, uint8_t* src, int16_t* dx, int16_t* dy, uint8_t* edges);

@@ -20,28 +20,24 @@
 namespace cctagb {
 namespace pm {
 
-// gen_pmath.py output
-static constexpr double kSinP[7] = {-0.16666666666666666,    0.008333333333333331,  -0.00019841269841265065,
-                                    2.7557319219339963e-06, -2.505210623269685e-08, 1.605853165490743e-10,
-                                    -7.586699058841919e-13};
-static constexpr double kCosQ[7] = {0.041666666666666664,  -0.0013888888888888887, 2.480158730158465e-05,
-                                    -2.755731922140322e-07, 2.0876755791205128e-09, -1.1470460905580259e-11,
-                                    4.745872873139979e-14};
-static constexpr double kAtanR[11] = {-0.3333333333333333,  0.19999999999995652,  -0.14285714284691378,
-                                      0.11111111017100195,  -0.0909090464769147,  0.07692184699290894,
-                                      -0.06664531368831207, 0.05858311803098606,  -0.05086254851324164,
-                                      0.03925369542082372,  -0.0192025282626767};
+// Polynomials fitted by gen_pmath.py, in Horner form.
+CCTAGB_HD inline double sin_p(double u)
+{
+    return -0.16666666666666666 + u * (0.008333333333333331 + u * (-0.00019841269841265065 + u * (2.7557319219339963e-06 + u * (-2.505210623269685e-08 + u * (1.605853165490743e-10 + u * (-7.586699058841919e-13))))));
+}
+CCTAGB_HD inline double cos_q(double u)
+{
+    return 0.041666666666666664 + u * (-0.0013888888888888887 + u * (2.480158730158465e-05 + u * (-2.755731922140322e-07 + u * (2.0876755791205128e-09 + u * (-1.1470460905580259e-11 + u * (4.745872873139979e-14))))));
+}
+CCTAGB_HD inline double atan_r(double u)
+{
+    return -0.3333333333333333 + u * (0.19999999999995652 + u * (-0.14285714284691378 + u * (0.11111111017100195 + u * (-0.0909090464769147 + u * (0.07692184699290894 + u * (-0.06664531368831207 + u * (0.05858311803098606 + u * (-0.05086254851324164 + u * (0.03925369542082372 + u * (-0.0192025282626767))))))))));
+}
+
 static constexpr double kPio2Hi = 1.5707963267341256, kPio2Mid = 6.07710050359346e-11,
                         kPio2Lo = 2.912732056093356e-20;
 static constexpr double kPi = 3.141592653589793, kPio2 = 1.5707963267948966, kPio4 = 0.7853981633974483,
                         kTanPio8 = 0.41421356237309503, k2OverPi = 0.6366197723675814;
-
-CCTAGB_HD inline double horner(const double* c, int n, double u)
-{
-    double s = c[n - 1];
-    for (int i = n - 2; i >= 0; --i) s = s * u + c[i];
-    return s;
-}
 
 CCTAGB_HD inline bool sign_bit(double x) { return ::copysign(1.0, x) < 0.0; }
 
@@ -56,13 +52,13 @@ CCTAGB_HD inline double reduce_pio2(double x, int& q)
 CCTAGB_HD inline double sin_poly(double r)
 {
     const double u = r * r;
-    return r + r * (u * horner(kSinP, 7, u));
+    return r + r * (u * sin_p(u));
 }
 
 CCTAGB_HD inline double cos_poly(double r)
 {
     const double u = r * r;
-    return (1.0 - 0.5 * u) + (u * u) * horner(kCosQ, 7, u);
+    return (1.0 - 0.5 * u) + (u * u) * cos_q(u);
 }
 
 CCTAGB_HD inline double sin_d(double x)
@@ -98,7 +94,7 @@ CCTAGB_HD inline double atan_unit(double t)
         base = kPio4;
     }
     const double z = u * u;
-    return base + (u + u * (z * horner(kAtanR, 11, z)));
+    return base + (u + u * (z * atan_r(z)));
 }
 
 // atan2 with the IEEE special cases of the zeros' signs.

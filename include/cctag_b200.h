@@ -29,6 +29,8 @@
  *   cctagb_identify_tasks  <- identify_step_2 / refineConicFamilyGlob + orazioDistanceRobust
  *                                                                  src/cctag/Identification.cpp:813-965,1318-1480
  *   cctagb_last_tasks      <- the cuts identify_step_1 selects     src/cctag/Identification.cpp:1172-1301
+ *   cctagb_level_loop_two  <- loop 1 + outlier removal of cctagDetectionFromEdges
+ *                                                                  src/cctag/Detection.cpp:69-156,609-627
  *   cctagb_cut_cost        <- costFunctionGlob (forward only in the reference; here with its
  *                             gradient in the center and in H)   src/cctag/Identification.cpp:1122-1158
  *   cctagb_edges_noalloc   <- cvRecodedCanny + thin on caller buffers (no allocation)
@@ -52,7 +54,7 @@ typedef enum cctagb_status {
     CCTAGB_NO_DEVICE = 3,          /* no CUDA device, or not an sm_100 device           */
     CCTAGB_OVERFLOW_EDGES = 4,     /* more edge points than the handle's capacity       */
     CCTAGB_OVERFLOW_SEEDS = 5,     /* more seeds than the handle's capacity             */
-    CCTAGB_OVERFLOW_VOTERS = 6,    /* reserved: voter list larger than capacity         */
+    CCTAGB_OVERFLOW_VOTERS = 6,    /* a candidate gathers more voters than its capacity */
     CCTAGB_HYST_NO_CONVERGE = 7,   /* hysteresis union-find exceeded its iteration cap  */
     CCTAGB_TOO_LARGE = 8,          /* frame larger than the handle was created for      */
     CCTAGB_BANK_ERROR = 9,         /* marker bank missing, empty or malformed           */
@@ -232,6 +234,20 @@ cctagb_status cctagb_level_votes(cctagb_handle* h, int level, int cap, int32_t* 
                                  int32_t* n_voters);
 /* Seeds in the reference's processing order (push order, then std::sort by votes). */
 cctagb_status cctagb_level_seeds(cctagb_handle* h, int level, int cap, int32_t* seeds, int* n);
+
+/* Loop-one candidates of level `level` in the last cctagb_detect /
+ * cctagb_detect_device call: the first maximumNbCandidatesLoopTwo of them in
+ * loop-one order (Detection.cpp:609-627), after the children collection and
+ * the LMedS outlier removal of loop two (Detection.cpp:115-156, Vote.cpp:
+ * 396-576), as the GPU computed them.  Per candidate: seed (edge-point index),
+ * score (number of children, 0 when too few), keep (1 when it goes on to the
+ * ellipse growing) and, for kept candidates, the number of filtered children;
+ * `filtered` receives the kept candidates' filtered children one after the
+ * other.  These lists are locals of cctagDetectionFromEdges in the reference;
+ * the call exposes them for parity checks. */
+cctagb_status cctagb_level_loop_two(cctagb_handle* h, int level, int cap, int32_t* seed, int32_t* score,
+                                    int32_t* keep, int32_t* n_filtered, int* n, int filtered_cap,
+                                    int32_t* filtered, int* n_filtered_total);
 
 /* The CUDA stream (cudaStream_t) on which the handle launches its work, so a
  * caller can order its own work or CUDA events against it. */

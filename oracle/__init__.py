@@ -189,6 +189,31 @@ def cut_selection(gray: np.ndarray, params=None, cap: int = 512):
     return [(int(status[i]), stops[i, :ncuts[i]].copy()) for i in range(min(n, cap))]
 
 
+def loop_two(gray: np.ndarray, level: int, params=None):
+    """Loop 1 and the outlier removal of loop 2 (host restatement) for one
+    level: (seed, score, keep, filtered) as Detector.level_loop_two."""
+    from cctag_b200.capi import Params
+
+    lib = load()
+    lib.orc_loop_two.argtypes = [_P, _I, _I, C.POINTER(Params), _I, _I, _P, _P, _P, _P, _I, _P, C.POINTER(_I)]
+    lib.orc_loop_two.restype = _I
+    lib.orc_params_default.argtypes = [C.POINTER(Params), _I]
+    if params is None:
+        params = Params()
+        lib.orc_params_default(C.byref(params), 3)
+    g = np.ascontiguousarray(gray, dtype=np.uint8)
+    cap, fcap = 4096, 1 << 22
+    seed, score, keep, nflt = (np.zeros(cap, np.int32) for _ in range(4))
+    flt = np.zeros(fcap, np.int32)
+    nt = C.c_int()
+    n = lib.orc_loop_two(_p(g), g.shape[1], g.shape[0], C.byref(params), level, cap, _p(seed), _p(score),
+                         _p(keep), _p(nflt), fcap, _p(flt), C.byref(nt))
+    if n < 0:
+        raise ValueError("orc_loop_two failed")
+    offs = np.concatenate([[0], np.cumsum(nflt[:n])])
+    return seed[:n].copy(), score[:n].copy(), keep[:n].copy(), [flt[offs[i]:offs[i + 1]].copy() for i in range(n)]
+
+
 # ------------------------------------------------ batched identification --
 def _refine_sigs(lib):
     D = C.c_double

@@ -563,7 +563,7 @@ struct StepOneRec {
 }  // namespace orc
 
 static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* pp, int fp64, orc_marker* out, int cap,
-                       std::vector<orc::StepOneRec>* rec)
+                       std::vector<orc::StepOneRec>* rec, std::vector<cctagb::LoopTwoIn>* l2 = nullptr)
 {
     using namespace orc;
     const cctagb_params& p = *pp;
@@ -644,6 +644,12 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
         jobs[l].seeds = &ld[l].seeds;
         jobs[l].level = l;
         jobs[l].scale = float(1 << l);
+    }
+    if (l2) {  // loop 1 and the outlier removal only
+        cctagb::link_and_filter(jobs, p, [](int n, const std::function<void(int)>& f) {
+            for (int i = 0; i < n; ++i) f(i);
+        }, *l2);
+        return 0;
     }
     cctagb::detect_from_edges(jobs, p, [](int n, const std::function<void(int)>& f) {
         for (int i = 0; i < n; ++i) f(i);
@@ -736,6 +742,29 @@ extern "C" int orc_cut_selection(const uint8_t* gray, int W, int H, const cctagb
         }
     }
     return int(rec.size());
+}
+
+// Loop 1 and the outlier removal of loop 2 (host restatement) for one level:
+// the layout of cctagb_level_loop_two.
+extern "C" int orc_loop_two(const uint8_t* gray, int W, int H, const cctagb_params* pp, int level, int cap,
+                            int32_t* seed, int32_t* score, int32_t* keep, int32_t* n_filtered, int filtered_cap,
+                            int32_t* filtered, int* n_filtered_total)
+{
+    std::vector<cctagb::LoopTwoIn> l2;
+    detect_impl(gray, W, H, pp, 0, nullptr, 0, nullptr, &l2);
+    if (level < 0 || level >= int(l2.size())) return -1;
+    const cctagb::LoopTwoIn& g = l2[size_t(level)];
+    const int n = int(g.seed.size());
+    if (n > cap || int(g.flt.size()) > filtered_cap) return -1;
+    for (int i = 0; i < n; ++i) {
+        seed[i] = g.seed[size_t(i)];
+        score[i] = g.score[size_t(i)];
+        keep[i] = g.keep[size_t(i)];
+        n_filtered[i] = g.foff[size_t(i) + 1] - g.foff[size_t(i)];
+    }
+    std::copy(g.flt.begin(), g.flt.end(), filtered);
+    *n_filtered_total = int(g.flt.size());
+    return n;
 }
 
 extern "C" void orc_params_default(cctagb_params* p, int nCrowns)
