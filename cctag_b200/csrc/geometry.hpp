@@ -370,9 +370,31 @@ struct Pcg32 {
     {
         const uint64_t old = state;
         state = old * kMul + inc;
-        const uint32_t xs = uint32_t(((old >> 18) ^ old) >> 27);
-        const uint32_t rot = uint32_t(old >> 59);
+        return output(old);
+    }
+    // Output of the generator at state s (XSH-RR).
+    CCTAGB_HD static uint32_t output(uint64_t s)
+    {
+        const uint32_t xs = uint32_t(((s >> 18) ^ s) >> 27);
+        const uint32_t rot = uint32_t(s >> 59);
         return (xs >> rot) | (xs << ((32u - rot) & 31u));
+    }
+    // Skips `delta` outputs in O(log delta): the LCG jump of F. Brown,
+    // "Random number generation with arbitrary strides" (1994), as PCG's
+    // advance function.
+    CCTAGB_HD void advance(uint64_t delta)
+    {
+        uint64_t curMul = kMul, curPlus = inc, accMul = 1u, accPlus = 0u;
+        while (delta > 0) {
+            if (delta & 1u) {
+                accMul *= curMul;
+                accPlus = accPlus * curMul + curPlus;
+            }
+            curPlus = (curMul + 1u) * curPlus;
+            curMul *= curMul;
+            delta >>= 1;
+        }
+        state = accMul * state + accPlus;
     }
     CCTAGB_HD uint32_t bounded(uint32_t n)
     {

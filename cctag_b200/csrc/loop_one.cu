@@ -3,16 +3,24 @@
 // expression here and in cand_shared.hpp is then evaluated with the same IEEE
 // operations as the host restatement, so the candidates are the same bits.
 //
-// k_link_seeds   one thread per seed: the two edge-linking walks
-//                (Vote.cpp:255-394), independent of the other seeds since
-//                each walk only avoids its own points;
-// k_link_resolve one warp per level: the seeds in processing order, skipping
-//                those an earlier segment marked processed (Detection.cpp:
-//                609-627), then the candidates ranked by averageReceivedVote;
-// k_filter       one warp per loop-two candidate: children (Vote.cpp:
-//                396-412) and the LMedS outlier removal (Vote.cpp:414-576),
-//                32 random draws evaluated at once and accepted in draw order;
-// k_pack         the kept candidates' filtered children, packed for download.
+// k_point_records one thread per edge point: position, gradient angle,
+//                 votes received and the 8 neighbouring edge points, so that
+//                 a linking step is one dependent load;
+// k_seed_slots    marks each seed's record with its processing slot;
+// k_link_seeds    one thread per seed: the two edge-linking walks
+//                 (Vote.cpp:255-394), independent of the other seeds since
+//                 each walk only avoids its own points; also lists the later
+//                 seeds its segment marks processed;
+// k_link_resolve  one block per level: the seeds in processing order,
+//                 skipping those an earlier segment marked (Detection.cpp:
+//                 609-627), in shared memory; then the candidates ranked by
+//                 averageReceivedVote;
+// k_filter        one block per loop-two candidate: children (Vote.cpp:
+//                 396-412) and the LMedS outlier removal (Vote.cpp:414-576),
+//                 128 random draws evaluated at once and accepted in draw
+//                 order; the draws' random stream is generated in parallel
+//                 with the PCG jump-ahead;
+// k_pack          the kept candidates' filtered children, packed for download.
 #include "loop_one.hpp"
 
 #include <algorithm>
@@ -26,6 +34,37 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kVisitSlots = 512;  // > 2 * kSegSlot
+constexpr int kResolveThreads = 256;
+constexpr int kResolveSmemMarks = 12288;
+
+// Record of edge point i: r0 = {x | y << 16, angle bits, votes received, seed
+// slot or -1}, r1 / r2 = the edge points at the 8 neighbours in the order of
+// Vote.cpp:283-286 for direction +1 (-1 where none).
+struct PointRec {
+    int4 r0, r1, r2;
+};
+
+__device__ __forceinline__ PointRec load_rec(const int4* rec, int i)
+{
+    PointRec r;
+    r.r0 = rec[3 * i];
+    r.r1 = rec[3 * i + 1];
+    r.r2 = rec[3 * i + 2];
+    return r;
+}
+__device__ __forceinline__ int nbr(const PointRec& r, int k)
+{
+    switch (k) {
+    case 0: return r.r1.x;
+    case 1: return r.r1.y;
+    case 2: return r.r1.z;
+    case 3: return r.r1.w;
+    case 4: return r.r2.x;
+    case 5: return r.r2.y;
+    case 6: return r.r2.z;
+    default: return r.r2.w;
+    }
+}
 
 __device__ __forceinline__ int px_(const LoopOneLevel& L, int i) { return L.exy[i] & 0xffff; }
 __device__ __forceinline__ int py_(const LoopOneLevel& L, int i) { return L.exy[i] >> 16; }
@@ -41,88 +80,125 @@ __device__ __forceinline__ float gnorm(const LoopOneLevel& L, int i)
 // the edge bitmap is set).
 __device__ __forceinline__ int at(const LoopOneLevel& L, int x, int y)
 {
+    if (x < 0 || x >= L.W || y < 0 || y >= L.H) return -1;
     const uint32_t w = L.bitmap[size_t(y) * L.WW + (x >> 5)];
     return ((w >> (x & 31)) & 1u) ? L.idxmap[size_t(y) * L.W + x] : -1;
 }
 
-// Points of one edge-linking call (the reference's set of visited positions).
-struct VisitSet {
-    int32_t k[kVisitSlots];
-    __device__ void clear()
-    {
-        for (int i = 0; i < kVisitSlots; ++i) k[i] = -1;
-    }
-    __device__ static uint32_t slot(int v) { return (uint32_t(v) * 2654435761u) >> 23; }
-    __device__ bool has(int v) const
-    {
-        for (uint32_t h = slot(v);; h = (h + 1) & (kVisitSlots - 1)) {
-            if (k[h] == v) return true;
-            if (k[h] == -1) return false;
-        }
-    }
-    __device__ void add(int v)
-    {
-        for (uint32_t h = slot(v);; h = (h + 1) & (kVisitSlots - 1)) {
-            if (k[h] == v) return;
-            if (k[h] == -1) {
-                k[h] = v;
-                return;
-            }
-        }
-    }
-};
-
-// Vote.cpp:272-394 edgeLinkingDir from the seed in direction dir.  The segment
-// is held around segc[0] = seed: the +1 walk appends at segc[1..], the -1 walk
-// prepends at segc[-1..].  Returns how many points, counted from the front of
-// the segment as it is when the walk ends, become processed.
-__device__ int link_walk(const LoopOneLevel& L, int seed, int dir, int32_t* segc, int& nf, int& nb, VisitSet& vis,
-                         int window, float averageVoteMin)
+__global__ void __launch_bounds__(256) k_point_records(LoopOneArgs a, int4 total)
 {
-    float ring[cand::kLinkMaxWindow + 1];
+    // total.x..w: cumulative point counts of levels 0..3
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cum[4] = {total.x, total.y, total.z, total.w};
+    int l = 0;
+    while (l < a.nl - 1 && t >= cum[l]) ++l;
+    if (t >= cum[a.nl - 1]) return;
+    const int i = t - (l ? cum[l - 1] : 0);
+    const LoopOneLevel& L = a.lv[l];
+    const int x = px_(L, i), y = py_(L, i);
+    const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+    const int yoff[8] = {0, -1, -1, -1, 0, 1, 1, 1};
+    int n[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) n[k] = at(L, x + xoff[k], y + yoff[k]);
+    const float angle = cand::link_angle(gdx(L, i), gdy(L, i));
+    int4* rec = L.rec + 3 * size_t(i);
+    rec[0] = make_int4(L.exy[i], __float_as_int(angle), voters(L, i), -1);
+    rec[1] = make_int4(n[0], n[1], n[2], n[3]);
+    rec[2] = make_int4(n[4], n[5], n[6], n[7]);
+}
+
+__global__ void __launch_bounds__(256) k_seed_slots(LoopOneArgs a)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int l = t / a.maxSlotsPerLevel, s = t % a.maxSlotsPerLevel;
+    if (l >= a.nl) return;
+    const LoopOneLevel& L = a.lv[l];
+    if (s >= L.nProc) return;
+    L.rec[3 * size_t(L.order[s])].w = s;
+}
+
+// Points of one edge-linking call (the reference's set of visited positions),
+// an open-addressing set in shared memory used by the 8 lanes of one seed.
+constexpr int kLinkThreads = 128;
+constexpr int kLinkGroups = kLinkThreads / 8;
+
+__device__ __forceinline__ uint32_t visit_slot(int v) { return (uint32_t(v) * 2654435761u) >> 23; }
+__device__ __forceinline__ bool visit_has(const int32_t* set, int v)
+{
+    for (uint32_t h = visit_slot(v);; h = (h + 1) & (kVisitSlots - 1)) {
+        const int k = set[h];
+        if (k == v) return true;
+        if (k == -1) return false;
+    }
+}
+__device__ __forceinline__ void visit_add(int32_t* set, int v)
+{
+    for (uint32_t h = visit_slot(v);; h = (h + 1) & (kVisitSlots - 1)) {
+        if (set[h] == v) return;
+        if (set[h] == -1) {
+            set[h] = v;
+            return;
+        }
+    }
+}
+
+// Vote.cpp:272-394 edgeLinkingDir from the seed in direction dir, by the 8
+// lanes of a group: lane j examines the j-th neighbour of the search order,
+// the first lane whose neighbour is an unvisited edge point decides the step.
+// The segment is held around segc[0] = seed: the +1 walk appends at
+// segc[1..], the -1 walk prepends at segc[-1..].  Returns how many points,
+// counted from the front of the segment as it is when the walk ends, become
+// processed.
+__device__ int link_walk(const int4* recs, int seed, int dir, int32_t* segc, int& nf, int& nb, int32_t* vis,
+                         float* ring, int window, float averageVoteMin, unsigned gmask, int j)
+{
     int head = 0, count = 0;
     int i = 0;
     bool found = true;
     int stop = 0;
-    int p = seed;
-    float averageVote = float(voters(L, p));
-    const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
-    const int yoff[8] = {0, -dir, -dir, -dir, 0, dir, dir, dir};
+    PointRec r = load_rec(recs, seed);
+    float averageVote = float(r.r0.z);
+    const int gbase = __ffs(gmask) - 1;
     while (i < cand::kLinkMaxLength && found && averageVote >= averageVoteMin) {
-        const float angle = cand::link_angle(gdx(L, p), gdy(L, p));
-        ring[(head + count) % (window + 1)] = angle;
+        const float angle = __int_as_float(r.r0.y);
+        // window of the last `window` angles (a ring of window + 1 entries)
+        if (j == 0) ring[head + count > window ? head + count - window - 1 : head + count] = angle;
         if (++count > window) {
-            head = (head + 1) % (window + 1);
+            head = head == window ? 0 : head + 1;
             --count;
         }
+        __syncwarp(gmask);
         const int shifting = cand::link_shift(angle);
-        int j = 0;
-        stop = 0;
-        while (!stop) {
-            if (j >= 8) {
-                stop = cand::kEdgeNotFound;
+        const int k = dir == 1 ? (8 - shifting + j) % 8 : (shifting + j) % 8;
+        // direction -1 mirrors the y offsets: neighbour (8 - k) % 8 of the +1 table
+        const int q = nbr(r, dir == 1 ? k : (8 - k) % 8);
+        const bool cand = q >= 0 && !visit_has(vis, q);
+        const unsigned hits = (__ballot_sync(gmask, cand) >> gbase) & 0xffu;
+        if (!hits) {
+            stop = cand::kEdgeNotFound;
+        } else {
+            const int jj = __ffs(hits) - 1;
+            const int qn = __shfl_sync(gmask, q, gbase + jj);
+            const float front = ring[head];
+            const float back = ring[head + count - 1 > window ? head + count - window - 2 : head + count - 1];
+            if (cand::link_convexity_lost(front, back, count == window, dir)) {
+                stop = cand::kConvexityLost;
             } else {
-                const int k = dir == 1 ? (8 - shifting + j) % 8 : (shifting + j) % 8;
-                const int sx = px_(L, p) + xoff[k];
-                const int sy = py_(L, p) + yoff[k];
-                if (sx >= 0 && sx < L.W && sy >= 0 && sy < L.H) {
-                    const int q = at(L, sx, sy);
-                    if (q >= 0 && !vis.has(q)) {
-                        const float front = ring[head], back = ring[(head + count - 1) % (window + 1)];
-                        if (cand::link_convexity_lost(front, back, count == window, dir)) stop = cand::kConvexityLost;
-                        if (stop == 0) {
-                            p = q;
-                            if (dir > 0) segc[++nb] = p;
-                            else segc[-(++nf)] = p;
-                            averageVote = cand::link_average_vote(averageVote, 1 + nf + nb, voters(L, p));
-                            stop = 1;
-                        }
-                        vis.add(p);
-                    }
+                if (dir > 0) {
+                    ++nb;
+                    if (j == 0) segc[nb] = qn;
+                } else {
+                    ++nf;
+                    if (j == 0) segc[-nf] = qn;
                 }
+                if (j == 0) visit_add(vis, qn);
+                r = load_rec(recs, qn);
+                averageVote = cand::link_average_vote(averageVote, 1 + nf + nb, r.r0.z);
+                stop = 1;
             }
-            ++j;
         }
+        __syncwarp(gmask);
         found = stop == 1;
         ++i;
     }
@@ -132,9 +208,14 @@ __device__ int link_walk(const LoopOneLevel& L, int seed, int dir, int32_t* segc
     return 0;
 }
 
-__global__ void __launch_bounds__(128) k_link_seeds(LoopOneArgs a)
+__global__ void __launch_bounds__(kLinkThreads) k_link_seeds(LoopOneArgs a)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ int32_t visAll[kLinkGroups][kVisitSlots];
+    __shared__ float ringAll[kLinkGroups][cand::kLinkMaxWindow + 1];
+    const int g = threadIdx.x >> 3, j = threadIdx.x & 7;
+    const int lane = threadIdx.x & 31;
+    const unsigned gmask = 0xffu << (lane & ~7);
+    const int t = blockIdx.x * kLinkGroups + g;
     if (t >= a.totalSlots) return;
     const int l = t / a.maxSlotsPerLevel, s = t % a.maxSlotsPerLevel;
     if (l >= a.nl) return;
@@ -142,67 +223,104 @@ __global__ void __launch_bounds__(128) k_link_seeds(LoopOneArgs a)
     if (s >= L.nProc) return;
     const int seed = L.order[s];
     int32_t* segc = a.seg + size_t(t) * kSegSlot + kSegHalf;
-    VisitSet vis;
-    vis.clear();
-    vis.add(seed);
-    segc[0] = seed;
+    int32_t* vis = visAll[g];
+    float* ring = ringAll[g];
+    for (int k = j; k < kVisitSlots; k += 8) vis[k] = -1;
+    __syncwarp(gmask);
+    if (j == 0) {
+        visit_add(vis, seed);
+        segc[0] = seed;
+    }
+    __syncwarp(gmask);
     int nf = 0, nb = 0;
-    const int m1 = link_walk(L, seed, 1, segc, nf, nb, vis, a.window, a.averageVoteMin);
-    const int m2 = link_walk(L, seed, -1, segc, nf, nb, vis, a.window, a.averageVoteMin);
+    const int m1 = link_walk(L.rec, seed, 1, segc, nf, nb, vis, ring, a.window, a.averageVoteMin, gmask, j);
+    const int m2 = link_walk(L.rec, seed, -1, segc, nf, nb, vis, ring, a.window, a.averageVoteMin, gmask, j);
+    __syncwarp(gmask);
+    if (j != 0) return;
     int nReceived = 0, nVoted = 0;
     for (int k = -nf; k <= nb; ++k) {
-        const int v = voters(L, segc[k]);
+        const int v = L.rec[3 * size_t(segc[k])].z;
         nReceived += v;
         if (v > 0) ++nVoted;
+    }
+    // later seeds the marks reach: points [0, m1) of (seed, back...) after the
+    // +1 walk, points [0, m2) of the whole segment after the -1 walk
+    int32_t* ml = a.mlist + size_t(t) * kMarkCap;
+    int nm = 0;
+    for (int k = 0; k < m1; ++k) {
+        const int sl = L.rec[3 * size_t(segc[k])].w;
+        if (sl > s) ml[nm++] = sl;
+    }
+    for (int k = 0; k < m2; ++k) {
+        const int sl = L.rec[3 * size_t(segc[-nf + k])].w;
+        if (sl > s) ml[nm++] = sl;
     }
     int32_t* info = a.sinfo + size_t(t) * 4;
     info[0] = nf;
     info[1] = nb;
-    info[2] = m1;
-    info[3] = m2;
+    info[2] = nm;
+    info[3] = 0;
     a.skey[t] = cand::received_vote_key(nReceived, nVoted);
 }
 
-__global__ void __launch_bounds__(32) k_link_resolve(LoopOneArgs a)
+__global__ void __launch_bounds__(kResolveThreads) k_link_resolve(LoopOneArgs a)
 {
     const int l = blockIdx.x;
     const LoopOneLevel& L = a.lv[l];
-    const int lane = threadIdx.x;
-    int32_t* made = a.made + size_t(l) * a.maxSlotsPerLevel;
-    int m = 0;
-    for (int s = 0; s < L.nProc; ++s) {
-        const int seed = L.order[s];
-        int flag = lane == 0 ? L.processed[seed] : 0;
-        flag = __shfl_sync(kFull, flag, 0);
-        if (flag) continue;
-        const int t = L.slot0 + s;
-        if (lane == 0) {
-            made[m] = s;
-            L.processed[seed] = 1;
-        }
-        ++m;
-        const int32_t* info = a.sinfo + size_t(t) * 4;
-        const int nf = info[0], m1 = info[2], m2 = info[3];
-        const int32_t* segc = a.seg + size_t(t) * kSegSlot + kSegHalf;
-        for (int k = lane; k < m1; k += 32) L.processed[segc[k]] = 1;
-        for (int k = lane; k < m2; k += 32) L.processed[segc[-nf + k]] = 1;
-        __syncwarp();
+    const int tid = threadIdx.x;
+    extern __shared__ int smem[];
+    // [flags: maxSlots][marks offsets: maxSlots + 1][marks: kResolveSmemMarks][keys: maxSlots]
+    int* flags = smem;
+    int* moff = flags + a.maxSlotsPerLevel;
+    int* marks = moff + a.maxSlotsPerLevel + 1;
+    float* keys = reinterpret_cast<float*>(marks + kResolveSmemMarks);
+    __shared__ int sM, sInSmem;
+    const int n = L.nProc;
+    for (int s = tid; s < n; s += blockDim.x) flags[s] = 0;
+    for (int s = tid; s < n; s += blockDim.x) moff[s + 1] = a.sinfo[size_t(L.slot0 + s) * 4 + 2];
+    __syncthreads();
+    if (tid == 0) {
+        moff[0] = 0;
+        for (int s = 0; s < n; ++s) moff[s + 1] += moff[s];
+        sInSmem = moff[n] <= kResolveSmemMarks;
     }
-    __syncwarp();
+    __syncthreads();
+    if (sInSmem)
+        for (int s = tid; s < n; s += blockDim.x) {
+            const int32_t* ml = a.mlist + size_t(L.slot0 + s) * kMarkCap;
+            for (int k = 0; k < moff[s + 1] - moff[s]; ++k) marks[moff[s] + k] = ml[k];
+        }
+    __syncthreads();
+    int32_t* made = a.made + size_t(l) * a.maxSlotsPerLevel;
+    if (tid == 0) {
+        int m = 0;
+        for (int s = 0; s < n; ++s) {
+            if (flags[s]) continue;
+            made[m++] = s;
+            const int cnt = moff[s + 1] - moff[s];
+            const int32_t* ml = sInSmem ? marks + moff[s] : a.mlist + size_t(L.slot0 + s) * kMarkCap;
+            for (int k = 0; k < cnt; ++k) flags[ml[k]] = 1;
+        }
+        sM = m;
+        a.meta[size_t(a.nl) * a.n2max * 4 + l] = m;
+    }
+    __syncthreads();
+    const int m = sM;
+    for (int i = tid; i < m; i += blockDim.x) keys[i] = a.skey[L.slot0 + made[i]];
+    __syncthreads();
     // Loop-1 order: averageReceivedVote descending, the newer candidate first
     // on equal keys (Detection.cpp:619-622).
     const int n2 = min(m, a.n2max);
     int32_t* meta = a.meta + size_t(l) * a.n2max * 4;
-    for (int i = lane; i < m; i += 32) {
-        const float ki = a.skey[L.slot0 + made[i]];
+    for (int i = tid; i < m; i += blockDim.x) {
+        const float ki = keys[i];
         int rank = 0;
         for (int j = 0; j < m; ++j) {
-            const float kj = a.skey[L.slot0 + made[j]];
+            const float kj = keys[j];
             rank += (kj > ki || (!(ki > kj) && j > i)) ? 1 : 0;
         }
         if (rank < n2) meta[rank * 4] = made[i];
     }
-    if (lane == 0) a.meta[size_t(a.nl) * a.n2max * 4 + l] = m;
 }
 
 // Value of rank k (NaN last) of n order keys, reordering them.
@@ -237,11 +355,17 @@ __device__ __forceinline__ float key_value(uint32_t k)
     return __uint_as_float(u);
 }
 
-__global__ void __launch_bounds__(32) k_filter(LoopOneArgs a)
+// Draw kinds after evaluation
+constexpr int kDrawFail = 0;      // counted: no usable ellipse
+constexpr int kDrawUsable = 1;    // S holds its median
+constexpr int kDrawNotReal = 2;   // the reference's exception: not counted
+constexpr int kDrawNoGain = 3;    // counted: its median cannot beat the best so far
+
+__global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
 {
     const int l = blockIdx.x / a.n2max, rank = blockIdx.x % a.n2max;
     const LoopOneLevel& L = a.lv[l];
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int madeCount = a.meta[size_t(a.nl) * a.n2max * 4 + l];
     if (rank >= min(madeCount, a.n2max)) return;
     int32_t* meta = a.meta + (size_t(l) * a.n2max + rank) * 4;
@@ -252,34 +376,60 @@ __global__ void __launch_bounds__(32) k_filter(LoopOneArgs a)
     const int32_t* segc = a.seg + size_t(t) * kSegSlot + kSegHalf;
     const int len = nf + 1 + nb;
     int32_t* children = a.children + size_t(blockIdx.x) * kChildCap;
-    __syncwarp();
-    if (lane == 0) meta[0] = L.order[s];
+
+    __shared__ geo::Pt pts[kLmedsMaxPts];
+    __shared__ float wts[kLmedsMaxPts];
+    __shared__ uint32_t raws[kRawPool];
+    __shared__ uint8_t mods[kRawPool];
+    __shared__ int8_t perms[kFilterThreads][5];
+    __shared__ int kinds[kFilterThreads];
+    __shared__ float svals[kFilterThreads];
+    __shared__ float sQ[kFilterThreads][9];
+    __shared__ float bestQ[9];
+    __shared__ int sNchild, sNpts, sDone, sNd, sCounter, sDraws, sWarpCnt[kFilterThreads / 32];
+    __shared__ float sSm;
+    __shared__ unsigned long long sState, sInc;
 
     // children (Vote.cpp:396-412): voters of the points with >= voteMax/14 votes
-    int vmax = 1;
-    for (int k = lane; k < len; k += 32) vmax = max(vmax, voters(L, segc[-nf + k]));
-    for (int o = 16; o; o >>= 1) vmax = max(vmax, __shfl_xor_sync(kFull, vmax, o));
-    int nchild = 0;
-    for (int c0 = 0; c0 < len; c0 += 32) {
-        const int pos = c0 + lane;
-        const int e = pos < len ? segc[-nf + pos] : -1;
-        const int n = e >= 0 ? voters(L, e) : 0;
-        const int cnt = (n > 0 && n >= vmax / 14) ? n : 0;
-        int incl = cnt;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += v;
+    if (warp == 0) {
+        int vmax = 1;
+        for (int k = lane; k < len; k += 32) vmax = max(vmax, voters(L, segc[-nf + k]));
+        for (int o = 16; o; o >>= 1) vmax = max(vmax, __shfl_xor_sync(kFull, vmax, o));
+        int nchild = 0;
+        for (int c0 = 0; c0 < len; c0 += 32) {
+            const int pos = c0 + lane;
+            const int e = pos < len ? segc[-nf + pos] : -1;
+            const int n = e >= 0 ? voters(L, e) : 0;
+            const int cnt = (n > 0 && n >= vmax / 14) ? n : 0;
+            int incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int excl = incl - cnt;
+            const int base = cnt ? L.voff[e] : 0;
+            const int tot = __shfl_sync(kFull, incl, 31);
+            // the chunk's voter lists, 32 entries at a time: entry o belongs to
+            // the first lane whose inclusive count exceeds o
+            for (int o0 = 0; o0 < tot; o0 += 32) {
+                const int o = o0 + lane;
+                int w = 0;
+                for (int b = 16; b > 0; b >>= 1)
+                    if (__shfl_sync(kFull, incl, w + b - 1) <= o) w += b;
+                const int wbase = __shfl_sync(kFull, base, w & 31);
+                const int wexcl = __shfl_sync(kFull, excl, w & 31);
+                if (o < tot && nchild + o < kChildCap) children[nchild + o] = L.vlist[wbase + (o - wexcl)];
+            }
+            nchild += tot;
         }
-        const int excl = incl - cnt;
-        if (cnt && nchild + incl <= kChildCap) {
-            const int32_t* src = L.vlist + L.voff[e];
-            for (int k = 0; k < cnt; ++k) children[nchild + excl + k] = src[k];
-        }
-        nchild += __shfl_sync(kFull, incl, 31);
+        if (lane == 0) sNchild = nchild;
     }
+    __syncthreads();
+    const int nchild = sNchild;
     if (nchild > kChildCap) {
-        if (lane == 0) {
+        if (tid == 0) {
             atomicOr(a.err, kLoopOneErrChildren);
+            meta[0] = L.order[s];
             meta[1] = nchild;
             meta[2] = 0;
             meta[3] = 0;
@@ -287,127 +437,199 @@ __global__ void __launch_bounds__(32) k_filter(LoopOneArgs a)
         return;
     }
     if (nchild < a.minPoints) {
-        if (lane == 0) {
+        if (tid == 0) {
+            meta[0] = L.order[s];
             meta[1] = 0;
             meta[2] = 0;
             meta[3] = 0;
         }
         return;
     }
-    __syncwarp();
 
     // outlierRemoval (Vote.cpp:414-576) with maxSize 60 and inverse-gradient
     // weights: a regular subsample of the children ...
-    __shared__ geo::Pt pts[kLmedsMaxPts];
-    __shared__ float wts[kLmedsMaxPts];
-    __shared__ int sPerm[32][5];
-    __shared__ int sKind[32];
-    __shared__ float sS[32];
-    __shared__ float sQ[32][9];
-    __shared__ float bestQ[9];
-    __shared__ int sNpts, sDone;
-    __shared__ float sSm;
+    // The reference scans the children and takes child i when i equals
+    // size_t(float(k) * step) for the next k: the taken indices are those
+    // targets while they increase strictly and stay below nchild.
     const int nSub = min(nchild, 60);
-    if (lane == 0) {
+    __shared__ long long sTarget[kLmedsMaxPts + 1];
+    if (nSub >= 5 && tid <= kLmedsMaxPts) {
+        const float step = float(nchild) / float(nSub);
+        sTarget[tid] = (long long)size_t(float(size_t(tid)) * step);
+    }
+    __syncthreads();
+    if (tid == 0) {
         int np = 0;
         if (nSub >= 5) {
-            const float step = float(nchild) / float(nSub);
-            size_t k = 0;
-            for (int i = 0; i < nchild; ++i) {
-                if (size_t(i) == size_t(float(k) * step)) {
-                    ++k;
-                    const int e = children[i];
-                    if (np < kLmedsMaxPts) {
-                        pts[np] = {float(px_(L, e)), float(py_(L, e))};
-                        wts[np] = 255.f / gnorm(L, e);
-                    }
-                    ++np;
-                }
-            }
+            while (np <= kLmedsMaxPts && sTarget[np] < nchild && (np == 0 || sTarget[np] > sTarget[np - 1])) ++np;
             if (np > kLmedsMaxPts) atomicOr(a.err, kLoopOneErrPoints);
         }
         sNpts = np;
         for (int k = 0; k < 9; ++k) bestQ[k] = 0.f;
         sSm = 10000000.0f;
         sDone = 0;
+        sCounter = 0;
+        sDraws = 0;
+        const geo::Pcg32 rng = cand::candidate_rng(L.level, uint64_t(rank), 0);
+        sState = rng.state;
+        sInc = rng.inc;
     }
-    __syncwarp();
+    __syncthreads();
     const int np = sNpts;
+    if (np <= kLmedsMaxPts && tid < np) {
+        const int e = children[sTarget[tid]];
+        pts[tid] = {float(px_(L, e)), float(py_(L, e))};
+        wts[tid] = 255.f / gnorm(L, e);
+    }
+    __syncthreads();
     if (nSub < 5 || np > kLmedsMaxPts) {
-        if (lane == 0) {
+        if (tid == 0) {
+            meta[0] = L.order[s];
             meta[1] = nchild;
             meta[2] = 0;
             meta[3] = 0;
         }
         return;
     }
-    // ... then random 5-point conics, 32 draws at a time, accepted in order.
-    geo::Pcg32 rng = cand::candidate_rng(L.level, uint64_t(rank), 0);
-    int counter = 0, draws = 0;
-    float Sm = 10000000.0f;
+    // ... then random 5-point conics, 128 draws at a time, accepted in order.
+    const uint32_t threshold = uint32_t(-uint32_t(np)) % uint32_t(np);
     uint32_t keys[kLmedsMaxPts];
     while (!sDone) {
-        if (lane == 0)
-            for (int j = 0; j < 32; ++j) rng.rand5(sPerm[j], size_t(np));
-        __syncwarp();
+        // the next kRawPool outputs of the candidate's stream, 8 per thread
         {
+            geo::Pcg32 g;
+            g.state = sState;
+            g.inc = sInc;
+            g.advance(uint64_t(tid) * (kRawPool / kFilterThreads));
+            for (int k = 0; k < kRawPool / kFilterThreads; ++k) {
+                const uint32_t r = g.next();
+                raws[tid * (kRawPool / kFilterThreads) + k] = r;
+                mods[tid * (kRawPool / kFilterThreads) + k] = uint8_t(r % uint32_t(np));
+            }
+        }
+        __syncthreads();
+        // Statistic.cpp:16-29 rand_5_k on that stream, as many whole draws as it holds
+        if (tid == 0) {
+            int ptr = 0, nd = 0;
+            while (nd < kFilterThreads) {
+                int perm[5] = {-1, -1, -1, -1, -1};
+                const int start = ptr;
+                bool complete = true;
+                for (int i = 0; i < 5 && complete; ++i) {
+                    for (;;) {
+                        if (ptr >= kRawPool) {
+                            complete = false;
+                            break;
+                        }
+                        const uint32_t raw = raws[ptr];
+                        const int r = mods[ptr];
+                        ++ptr;
+                        if (raw < threshold) continue;
+                        bool seen = false;
+                        for (int q = 0; q < i; ++q) seen = seen || perm[q] == r;
+                        if (seen) continue;
+                        perm[i] = r;
+                        break;
+                    }
+                }
+                if (!complete) {
+                    ptr = start;
+                    break;
+                }
+                for (int i = 0; i < 5; ++i) perms[nd][i] = int8_t(perm[i]);
+                ++nd;
+            }
+            if (nd == 0) atomicOr(a.err, kLoopOneErrRandom);
+            sNd = nd;
+            geo::Pcg32 g;
+            g.state = sState;
+            g.inc = sInc;
+            g.advance(uint64_t(ptr));
+            sState = g.state;
+        }
+        __syncthreads();
+        const int nd = sNd;
+        if (nd == 0) break;
+        const float SmStart = sSm;
+        if (tid < nd) {
+            int perm[5];
+            for (int i = 0; i < 5; ++i) perm[i] = perms[tid][i];
             geo::Mat3 Q;
-            const int kind = cand::lmeds_conic(pts, sPerm[lane], Q);
+            int kind = cand::lmeds_conic(pts, perm, Q);
             float S = 0.f;
-            if (kind == 1) {
+            if (kind == kDrawUsable) {
+                int below = 0;
                 for (int i = 0; i < np; ++i) {
                     const float d = geo::dist_point_ellipse(Q, pts[i].x, pts[i].y) * wts[i];
                     keys[i] = geo::order_key(d);
+                    below += d < SmStart;
                 }
-                S = key_value(select_key(keys, np, np / 2));
+                // no median below the best so far: it cannot improve (Sm only decreases)
+                if (below >= np / 2 + 1) S = key_value(select_key(keys, np, np / 2));
+                else kind = kDrawNoGain;
             }
-            sKind[lane] = kind;
-            sS[lane] = S;
-            for (int k = 0; k < 9; ++k) sQ[lane][k] = Q.m[k / 3][k % 3];
+            kinds[tid] = kind;
+            svals[tid] = S;
+            for (int k = 0; k < 9; ++k) sQ[tid][k] = Q.m[k / 3][k % 3];
         }
-        __syncwarp();
-        if (lane == 0) {
-            for (int j = 0; j < 32; ++j) {
+        __syncthreads();
+        if (tid == 0) {
+            int counter = sCounter, draws = sDraws, best = -1;
+            float Sm = sSm;
+            for (int j = 0; j < nd; ++j) {
                 if (!(counter < 70 && draws < 7000)) break;
                 ++draws;
-                if (sKind[j] == 0) {
+                const int kind = kinds[j];
+                if (kind == kDrawFail || kind == kDrawNoGain) {
                     ++counter;
-                } else if (sKind[j] == 1) {
-                    if (sS[j] < Sm) {
+                } else if (kind == kDrawNotReal) {
+                    // neither counted nor used
+                } else {
+                    if (svals[j] < Sm) {
                         counter = 0;
-                        Sm = sS[j];
-                        for (int k = 0; k < 9; ++k) bestQ[k] = sQ[j][k];
+                        Sm = svals[j];
+                        best = j;
                     } else {
                         ++counter;
                     }
                 }
             }
-            if (!(counter < 70 && draws < 7000)) sDone = 1;
+            if (best >= 0)
+                for (int k = 0; k < 9; ++k) bestQ[k] = sQ[best][k];
+            sCounter = counter;
+            sDraws = draws;
             sSm = Sm;
+            if (!(counter < 70 && draws < 7000)) sDone = 1;
         }
-        __syncwarp();
+        __syncthreads();
     }
-    // the children whose weighted distance is below threshold * median
+    // the children whose weighted distance is below threshold * median, in order
     geo::Mat3 Q;
     for (int k = 0; k < 9; ++k) Q.m[k / 3][k % 3] = bestQ[k];
     const float thr = a.threshold * sSm;
     int nflt = 0;
-    for (int c0 = 0; c0 < nchild; c0 += 32) {
-        const int i = c0 + lane;
-        bool pass = false;
+    for (int c0 = 0; c0 < nchild; c0 += kFilterThreads) {
+        const int i = c0 + tid;
         int e = -1;
-        if (i < nchild) {
-            e = children[i];
+        if (i < nchild) e = children[i];
+        __syncthreads();  // every element of the chunk read before any is overwritten
+        bool pass = false;
+        if (e >= 0) {
             float d = geo::dist_point_ellipse(Q, float(px_(L, e)), float(py_(L, e)));
             d = d * 255 / gnorm(L, e);
             pass = d < thr;
         }
         const unsigned mask = __ballot_sync(kFull, pass);
-        if (pass) children[nflt + __popc(mask & ((1u << lane) - 1u))] = e;
-        nflt += __popc(mask);
-        __syncwarp();
+        if (lane == 0) sWarpCnt[warp] = __popc(mask);
+        __syncthreads();
+        int off = nflt;
+        for (int w = 0; w < warp; ++w) off += sWarpCnt[w];
+        if (pass) children[off + __popc(mask & ((1u << lane) - 1u))] = e;
+        for (int w = 0; w < kFilterThreads / 32; ++w) nflt += sWarpCnt[w];
+        __syncthreads();
     }
-    if (lane == 0) {
+    if (tid == 0) {
+        meta[0] = L.order[s];
         meta[1] = nchild;
         meta[2] = nflt >= 5 ? 1 : 0;
         meta[3] = nflt;
@@ -461,12 +683,14 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
     // level 0 has the most rows
     maxSlotsPerLevel_ = std::max(max_h / 2, p.maximumNbSeeds);
     totalSlots_ = nl_ * maxSlotsPerLevel_;
+    size_t nrec = 0;
     for (int l = 0; l < nl_; ++l) {
         caps_.push_back(caps[size_t(l)]);
-        processed_bytes_ += size_t(caps[size_t(l)]);
+        nrec += size_t(caps[size_t(l)]);
     }
     args_.seg = dev_alloc<int32_t>(allocs_, size_t(totalSlots_) * kSegSlot);
     args_.sinfo = dev_alloc<int32_t>(allocs_, size_t(totalSlots_) * 4);
+    args_.mlist = dev_alloc<int32_t>(allocs_, size_t(totalSlots_) * kMarkCap);
     args_.skey = dev_alloc<float>(allocs_, size_t(totalSlots_));
     args_.made = dev_alloc<int32_t>(allocs_, size_t(totalSlots_));
     const size_t metaN = size_t(nl_) * n2max_ * 4 + nl_ + 1;
@@ -474,7 +698,7 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
     args_.err = args_.meta + size_t(nl_) * n2max_ * 4 + nl_;
     args_.children = dev_alloc<int32_t>(allocs_, size_t(nl_) * n2max_ * kChildCap);
     d_order_ = dev_alloc<int32_t>(allocs_, size_t(totalSlots_));
-    d_processed_ = dev_alloc<uint8_t>(allocs_, processed_bytes_);
+    d_rec_ = dev_alloc<int4>(allocs_, nrec * 3);
     d_packed_ = dev_alloc<int32_t>(allocs_, size_t(nl_) * n2max_ * kChildCap);
     CCTAGB_CUDA(cudaMallocHost(&h_order_, sizeof(int32_t) * std::max(totalSlots_, 1)));
     CCTAGB_CUDA(cudaMallocHost(&h_meta_, sizeof(int32_t) * metaN));
@@ -488,6 +712,20 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
     args_.n2max = n2max_;
     args_.minPoints = p.minPointsSegmentCandidate;
     args_.threshold = p.threshRobustEstimationOfOuterEllipse;
+    // The attribute is per kernel and shared by every handle: set it to what
+    // the device allows, so that no handle lowers it below another's need.
+    int dev = 0, optin = 0;
+    CCTAGB_CUDA(cudaGetDevice(&dev));
+    CCTAGB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const int maxSmem = optin - 1024;  // room for the kernel's static shared memory
+    if (resolve_smem() > maxSmem)
+        throw Error{CCTAGB_BAD_ARG, "maximumNbSeeds / frame height too large for the loop-one resolve kernel"};
+    CCTAGB_CUDA(cudaFuncSetAttribute(k_link_resolve, cudaFuncAttributeMaxDynamicSharedMemorySize, maxSmem));
+}
+
+int LoopOneGpu::resolve_smem() const
+{
+    return int(sizeof(int) * (3 * size_t(maxSlotsPerLevel_) + 1 + kResolveSmemMarks));
 }
 
 LoopOneGpu::~LoopOneGpu()
@@ -503,7 +741,8 @@ void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const 
 {
     if (lv.n != nl_ || int(seeds.size()) != nl_) throw Error{CCTAGB_BAD_ARG, "loop one: level count changed"};
     h2d_ = d2h_ = 0;
-    size_t poff = 0;
+    size_t roff = 0;
+    int cum[kMaxLevels] = {};
     for (int l = 0; l < nl_; ++l) {
         const LevelView& v = lv.l[l];
         LoopOneLevel& L = args_.lv[l];
@@ -524,21 +763,30 @@ void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const 
         L.order = d_order_ + L.slot0;
         std::copy(seeds[l]->begin(), seeds[l]->begin() + L.nProc, h_order_ + L.slot0);
         if (v.cap > caps_[size_t(l)]) throw Error{CCTAGB_INTERNAL, "loop one: level capacity changed"};
-        L.processed = d_processed_ + poff;
-        poff += size_t(caps_[size_t(l)]);
+        if (E[l] > caps_[size_t(l)]) throw Error{CCTAGB_INTERNAL, "loop one: more edge points than capacity"};
+        L.rec = d_rec_ + 3 * roff;
+        roff += size_t(caps_[size_t(l)]);
+        cum[l] = (l ? cum[l - 1] : 0) + E[l];
         if (L.nProc)
             CCTAGB_CUDA(cudaMemcpyAsync(d_order_ + L.slot0, h_order_ + L.slot0, sizeof(int32_t) * L.nProc,
                                         cudaMemcpyHostToDevice, s));
         h2d_ += 4LL * L.nProc;
     }
-    CCTAGB_CUDA(cudaMemsetAsync(d_processed_, 0, processed_bytes_, s));
+    for (int l = nl_; l < kMaxLevels; ++l) cum[l] = cum[nl_ - 1];
     const size_t metaN = size_t(nl_) * n2max_ * 4 + nl_ + 1;
     CCTAGB_CUDA(cudaMemsetAsync(args_.meta, 0, sizeof(int32_t) * metaN, s));
-    k_link_seeds<<<(totalSlots_ + 127) / 128, 128, 0, s>>>(args_);
+    const int npts = cum[nl_ - 1];
+    if (npts > 0) {
+        k_point_records<<<(npts + 255) / 256, 256, 0, s>>>(args_, make_int4(cum[0], cum[1], cum[2], cum[3]));
+        CCTAGB_CUDA(cudaGetLastError());
+    }
+    k_seed_slots<<<(totalSlots_ + 255) / 256, 256, 0, s>>>(args_);
     CCTAGB_CUDA(cudaGetLastError());
-    k_link_resolve<<<nl_, 32, 0, s>>>(args_);
+    k_link_seeds<<<(totalSlots_ + kLinkGroups - 1) / kLinkGroups, kLinkThreads, 0, s>>>(args_);
     CCTAGB_CUDA(cudaGetLastError());
-    k_filter<<<nl_ * n2max_, 32, 0, s>>>(args_);
+    k_link_resolve<<<nl_, kResolveThreads, resolve_smem(), s>>>(args_);
+    CCTAGB_CUDA(cudaGetLastError());
+    k_filter<<<nl_ * n2max_, kFilterThreads, 0, s>>>(args_);
     CCTAGB_CUDA(cudaGetLastError());
     k_pack<<<nl_ * n2max_, 256, 0, s>>>(args_, d_packed_);
     CCTAGB_CUDA(cudaGetLastError());

@@ -17,6 +17,9 @@ constexpr int kSegHalf = 100;                 // points per linking direction (m
 constexpr int kSegSlot = 2 * kSegHalf + 1;    // one segment: front, seed, back
 constexpr int kChildCap = 32768;              // children of one loop-two candidate
 constexpr int kLmedsMaxPts = 64;              // subsampled points of one outlier removal
+constexpr int kMarkCap = 2 * kSegSlot;        // later seeds one segment can mark processed
+constexpr int kFilterThreads = 128;           // LMedS draws evaluated at once per candidate
+constexpr int kRawPool = 1024;                // random outputs generated per batch of draws
 
 // One level as the loop-one kernels see it (device pointers).
 struct LoopOneLevel {
@@ -29,7 +32,7 @@ struct LoopOneLevel {
     const int32_t* idxmap;
     const int32_t* order;   // seeds in processing order, nProc of them
     int nProc, slot0;       // seed slots [slot0, slot0 + nProc)
-    uint8_t* processed;     // E flags (processedIn), zeroed per frame
+    int4* rec;              // E point records (3 int4 each): xy, angle, voters, seed slot; 8 neighbours
     int level;
 };
 
@@ -43,7 +46,8 @@ struct LoopOneArgs {
     float threshold;        // threshRobustEstimationOfOuterEllipse
     int totalSlots;
     int32_t* seg;           // totalSlots * kSegSlot: segment of each seed slot, seed at kSegHalf
-    int32_t* sinfo;         // totalSlots * 4: front length, back length, marks after +1, marks after -1
+    int32_t* sinfo;         // totalSlots * 4: front length, back length, number of marked later seeds
+    int32_t* mlist;         // totalSlots * kMarkCap: later seed slots the segment marks processed
     float* skey;            // totalSlots: averageReceivedVote
     int32_t* made;          // nl * maxSlotsPerLevel: made candidates (seed slots), per level
     int maxSlotsPerLevel;
@@ -55,6 +59,7 @@ struct LoopOneArgs {
 constexpr int kLoopOneErrChildren = 1;
 constexpr int kLoopOneErrWindow = 2;
 constexpr int kLoopOneErrPoints = 4;
+constexpr int kLoopOneErrRandom = 8;
 
 void launch_loop_one(const LoopOneArgs& a, cudaStream_t s);
 
@@ -74,19 +79,19 @@ public:
                 cudaStream_t s);
     // Waits for launch()'s work and fills `out` (one LoopTwoIn per level).
     void collect(cudaStream_t s, std::vector<LoopTwoIn>& out);
-    int launches() const { return 4; }
+    int launches() const { return 6; }
     long long h2d_bytes() const { return h2d_; }
     long long d2h_bytes() const { return d2h_; }
 
 private:
+    int resolve_smem() const;
     cctagb_params p_;
     int nl_ = 0, n2max_ = 0, maxSlotsPerLevel_ = 0, totalSlots_ = 0;
     LoopOneArgs args_{};
     int32_t* d_order_ = nullptr;   // all levels' seed slots
     int32_t* h_order_ = nullptr;   // pinned staging
-    uint8_t* d_processed_ = nullptr;
+    int4* d_rec_ = nullptr;        // point records of all levels
     int32_t* d_packed_ = nullptr;  // kept candidates' filtered children
-    size_t processed_bytes_ = 0;
     std::vector<int> caps_;
     int32_t* h_meta_ = nullptr;    // pinned: meta + made counts + err
     int32_t* h_flt_ = nullptr;     // pinned: filtered children, all candidates
