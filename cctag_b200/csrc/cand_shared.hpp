@@ -54,32 +54,50 @@ CCTAGB_HD inline float received_vote_key(int nReceived, int nVoted)
     return float(nReceived * nReceived) / float(nVoted);
 }
 
-// 5x5 linear solve with partial pivoting (FP64); false if singular.
+// 5x5 linear solve with partial pivoting (FP64); false if singular.  Loops
+// with constant bounds and constant-index row swaps, so that the GPU keeps
+// the system in registers; the operations are those of the textbook
+// elimination in the same order on both sides.
 CCTAGB_HD inline bool solve5(double A[5][5], double b[5], double x[5])
 {
+#pragma unroll
     for (int c = 0; c < 5; ++c) {
         int piv = c;
-        for (int r = c + 1; r < 5; ++r)
-            if (::fabs(A[r][c]) > ::fabs(A[piv][c])) piv = r;
-        if (A[piv][c] == 0.0) return false;
-        if (piv != c) {
-            for (int k = 0; k < 5; ++k) {
-                const double t = A[piv][k];
-                A[piv][k] = A[c][k];
-                A[c][k] = t;
+        double best = ::fabs(A[c][c]);
+#pragma unroll
+        for (int r = c + 1; r < 5; ++r) {
+            const double v = ::fabs(A[r][c]);
+            if (v > best) {
+                best = v;
+                piv = r;
             }
-            const double t = b[piv];
-            b[piv] = b[c];
-            b[c] = t;
         }
+        if (best == 0.0) return false;
+#pragma unroll
+        for (int r = c + 1; r < 5; ++r)
+            if (r == piv) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) {
+                    const double t = A[r][k];
+                    A[r][k] = A[c][k];
+                    A[c][k] = t;
+                }
+                const double t = b[r];
+                b[r] = b[c];
+                b[c] = t;
+            }
+#pragma unroll
         for (int r = c + 1; r < 5; ++r) {
             const double f = A[r][c] / A[c][c];
+#pragma unroll
             for (int k = c; k < 5; ++k) A[r][k] -= f * A[c][k];
             b[r] -= f * b[c];
         }
     }
+#pragma unroll
     for (int r = 4; r >= 0; --r) {
         double s = b[r];
+#pragma unroll
         for (int k = r + 1; k < 5; ++k) s -= A[r][k] * x[k];
         x[r] = s / A[r][r];
     }

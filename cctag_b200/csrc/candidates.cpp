@@ -889,20 +889,55 @@ bool intersect_line_two(int y, const Ellipse& qIn, const Ellipse& qOut, const Ed
 
 }  // namespace
 
+void refit_hull(const MarkerCand& m, RefitHull& h)
+{
+    Ellipse qIn, qOut;
+    geo::compute_hull(m.rescaled, m.scale, qIn, qOut);
+    for (int k = 0; k < 9; ++k) {
+        h.qin[k] = qIn.Q.m[k / 3][k % 3];
+        h.qout[k] = qOut.Q.m[k / 3][k % 3];
+    }
+    h.inCx = qIn.cx;
+    h.inCy = qIn.cy;
+    h.yc = m.rescaled.cy;
+}
+
+void refit_apply(const EdgeSet& es0, MarkerCand& m, const int32_t* filtered, size_t n)
+{
+    if (n < 5) return;
+    try {
+        std::vector<int> f(filtered, filtered + n);
+        const Ellipse fitted = fit_points(es0, f);
+        std::vector<DirPoint> dp;
+        dp.reserve(n);
+        for (int e : f) dp.push_back({float(es0.x(e)), float(es0.y(e)), es0.dx(e), es0.dy(e)});
+        m.cx_img *= m.scale;
+        m.cy_img *= m.scale;
+        m.rescaled = fitted;
+        m.rescaled_points = std::move(dp);
+    } catch (...) {
+    }
+}
+
 void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, const ParallelFor& pf)
 {
     pf(int(markers.size()), [&](int mi) {
         MarkerCand& m = markers[size_t(mi)];
-        // each marker its own PCG32 stream, apart from the candidate loops'
-        geo::Pcg32 rng(271828, (uint64_t(1) << 62) | uint64_t(mi));
         if (m.level > 0) {
-            const float scale = m.scale;
+            // each marker its own PCG32 stream, apart from the candidate loops'
+            geo::Pcg32 rng = refit_rng(mi);
+            RefitHull h;
+            refit_hull(m, h);
             Ellipse qIn, qOut;
-            geo::compute_hull(m.rescaled, scale, qIn, qOut);
+            qIn.cx = h.inCx;
+            qIn.cy = h.inCy;
+            for (int k = 0; k < 9; ++k) {
+                qIn.Q.m[k / 3][k % 3] = h.qin[k];
+                qOut.Q.m[k / 3][k % 3] = h.qout[k];
+            }
             std::vector<int> hull;
-            const float yc = m.rescaled.cy;
-            const int maxY = std::max(int(yc), 0);
-            const int minY = std::min(int(yc), es0.H - 1);
+            const int maxY = std::max(int(h.yc), 0);
+            const int minY = std::min(int(h.yc), es0.H - 1);
             for (int y = maxY; y < es0.H; ++y)
                 if (!intersect_line_two(y, qIn, qOut, es0, hull)) break;
             for (int y = minY; y >= 0; --y)
@@ -911,18 +946,7 @@ void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, const Paral
             std::vector<int> filtered;
             float SmFinal = 1e+10f;
             outlier_removal(es0, hull, filtered, SmFinal, 20.0f, kNoWeight, 60, rng);
-            if (filtered.size() < 5) return;
-            try {
-                const Ellipse fitted = fit_points(es0, filtered);
-                std::vector<DirPoint> dp;
-                dp.reserve(filtered.size());
-                for (int e : filtered) dp.push_back({float(es0.x(e)), float(es0.y(e)), es0.dx(e), es0.dy(e)});
-                m.cx_img *= scale;
-                m.cy_img *= scale;
-                m.rescaled = fitted;
-                m.rescaled_points = std::move(dp);
-            } catch (...) {
-            }
+            refit_apply(es0, m, filtered.data(), filtered.size());
         } else {
             m.rescaled_points = m.points.empty() ? std::vector<DirPoint>() : m.points.back();
         }

@@ -105,4 +105,18 @@ void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, cons
 // 319-401), markers in parallel, each with its own PCG32 stream.
 void refit_on_level0(EdgeSet& es0, std::vector<MarkerCand>& markers, const ParallelFor& pf);
 
+// Pieces of the re-fit: the hull of a coarse-level marker (Multiresolution.cpp:
+// 331-336: conics of its inner and outer ellipse, the inner center for the
+// gradient test, the rescaled center row) ...
+struct RefitHull {
+    float qin[9], qout[9];
+    float inCx, inCy, yc;
+};
+void refit_hull(const MarkerCand& m, RefitHull& h);
+// ... the random stream of marker mi's outlier removal ...
+inline geo::Pcg32 refit_rng(int mi) { return geo::Pcg32(271828, (uint64_t(1) << 62) | uint64_t(mi)); }
+// ... and the ellipse fit to the filtered hull points (Multiresolution.cpp:
+// 360-401), which updates the marker when n >= 5 and the fit succeeds.
+void refit_apply(const EdgeSet& es0, MarkerCand& m, const int32_t* filtered, size_t n);
+
 }  // namespace cctagb

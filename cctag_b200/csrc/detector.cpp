@@ -382,7 +382,39 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     std::vector<MarkerCand> markers;
     for (int l = nl - 1; l >= 0; --l)
         for (auto& m : jobs[l].out) markers.push_back(std::move(m));
-    refit_on_level0(es[0], markers, [this](int n, const std::function<void(int)>& f) { pool_->parallel_for(n, f); });
+    // Level-0 re-fit of coarse-level markers: hull and outlier removal on the
+    // GPU, the ellipse fit on the host.
+    {
+        std::vector<RefitTask> rt;
+        std::vector<int> rtIdx;
+        for (size_t mi = 0; mi < markers.size(); ++mi) {
+            MarkerCand& m = markers[mi];
+            if (m.level > 0) {
+                RefitHull h;
+                refit_hull(m, h);
+                RefitTask t;
+                std::copy(h.qin, h.qin + 9, t.qin);
+                std::copy(h.qout, h.qout + 9, t.qout);
+                t.inCx = h.inCx;
+                t.inCy = h.inCy;
+                t.yc = h.yc;
+                t.marker = int(mi);
+                rt.push_back(t);
+                rtIdx.push_back(int(mi));
+            } else {
+                m.rescaled_points = m.points.empty() ? std::vector<DirPoint>() : m.points.back();
+            }
+        }
+        if (!rt.empty()) {
+            std::vector<std::vector<int32_t>> flt;
+            const long long h0 = loop1_->h2d_bytes(), d0 = loop1_->d2h_bytes();
+            loop1_->refit(pipe_.level_views(), rt, pipe_.stream(), flt);
+            pipe_.add_io(loop1_->h2d_bytes() - h0, loop1_->d2h_bytes() - d0, loop1_->refit_launches());
+            pool_->parallel_for(int(rt.size()), [&](int k) {
+                refit_apply(es[0], markers[size_t(rtIdx[size_t(k)])], flt[size_t(k)].data(), flt[size_t(k)].size());
+            });
+        }
+    }
     for (int l = 0; l < nl; ++l) {
         const HostLevel& L = hl[l];
         for (int i = 0; i < L.E; ++i) idxmaps_[l][size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = -1;

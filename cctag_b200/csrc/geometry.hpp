@@ -249,10 +249,9 @@ CCTAGB_HD inline float dist_point_ellipse(const Mat3& Q, float x, float y)
 
 // EllipseFromPoints.cpp:124-154: intersections of the conic with y = const
 // (horizontal) or x = const (vertical).
-inline int intersect_line(const Ellipse& e, float y, bool horizontal, float out[2])
+CCTAGB_HD inline int intersect_line_q(const Mat3& C, float y, bool horizontal, float out[2])
 {
     out[0] = out[1] = 0.f;
-    const Mat3& C = e.Q;
     float a, b, c;
     if (horizontal) {
         a = C.m[0][0];
@@ -265,7 +264,7 @@ inline int intersect_line(const Ellipse& e, float y, bool horizontal, float out[
     }
     const float disc = b * b / 4.0f - a * c;
     if (disc > 0.f) {
-        const float sd = std::sqrt(disc);
+        const float sd = ::sqrtf(disc);
         out[0] = (-b / 2.0f - sd) / a;
         out[1] = (-b / 2.0f + sd) / a;
         return 2;
@@ -275,6 +274,11 @@ inline int intersect_line(const Ellipse& e, float y, bool horizontal, float out[
         return 1;
     }
     return 0;
+}
+
+inline int intersect_line(const Ellipse& e, float y, bool horizontal, float out[2])
+{
+    return intersect_line_q(e.Q, y, horizontal, out);
 }
 
 inline float round_half_away(float v) { return std::round(v); }

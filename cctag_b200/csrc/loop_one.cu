@@ -323,20 +323,23 @@ __global__ void __launch_bounds__(kResolveThreads) k_link_resolve(LoopOneArgs a)
     }
 }
 
-// Value of rank k (NaN last) of n order keys, reordering them.
-__device__ uint32_t select_key(uint32_t* v, int n, int k)
+// Value of rank k (NaN last) of the n order keys v[0], v[kFilterThreads],
+// v[2 kFilterThreads], ... (one thread's column of a shared array), by
+// quickselect; the keys are reordered.
+__device__ uint32_t select_key_strided(uint32_t* v, int n, int k)
 {
+    auto at_ = [&](int i) -> uint32_t& { return v[i * kFilterThreads]; };
     int lo = 0, hi = n - 1;
     while (lo < hi) {
-        const uint32_t pivot = v[(lo + hi) >> 1];
+        const uint32_t pivot = at_((lo + hi) >> 1);
         int i = lo, j = hi;
         while (i <= j) {
-            while (v[i] < pivot) ++i;
-            while (v[j] > pivot) --j;
+            while (at_(i) < pivot) ++i;
+            while (at_(j) > pivot) --j;
             if (i <= j) {
-                const uint32_t t = v[i];
-                v[i] = v[j];
-                v[j] = t;
+                const uint32_t t = at_(i);
+                at_(i) = at_(j);
+                at_(j) = t;
                 ++i;
                 --j;
             }
@@ -345,7 +348,7 @@ __device__ uint32_t select_key(uint32_t* v, int n, int k)
         else if (k >= i) lo = i;
         else break;
     }
-    return v[k];
+    return at_(k);
 }
 
 __device__ __forceinline__ float key_value(uint32_t k)
@@ -360,6 +363,299 @@ constexpr int kDrawFail = 0;      // counted: no usable ellipse
 constexpr int kDrawUsable = 1;    // S holds its median
 constexpr int kDrawNotReal = 2;   // the reference's exception: not counted
 constexpr int kDrawNoGain = 3;    // counted: its median cannot beat the best so far
+
+// Five distinct residues read from mods[p0...] (rand_5_k without rejected
+// outputs); returns the position after the last one read, or -1 when the
+// pool ends first.  Registers only.
+__device__ __forceinline__ int draw_from(const uint8_t* mods, int p0, int g[5])
+{
+    int n = 0, q = p0;
+    int g0 = -1, g1 = -1, g2 = -1, g3 = -1, g4 = -1;
+    while (n < 5) {
+        if (q >= kRawPool) return -1;
+        const int r = mods[q++];
+        const bool seen = r == g0 || r == g1 || r == g2 || r == g3;
+        if (seen) continue;
+        if (n == 0) g0 = r;
+        else if (n == 1) g1 = r;
+        else if (n == 2) g2 = r;
+        else if (n == 3) g3 = r;
+        else g4 = r;
+        ++n;
+    }
+    g[0] = g0;
+    g[1] = g1;
+    g[2] = g2;
+    g[3] = g3;
+    g[4] = g4;
+    return q;
+}
+
+// Whether the (weighted) distance d(Q, p) * w of dist_point_ellipse is below
+// S, decided exactly: an estimate with the fast reciprocal settles the cases
+// that are more than 2^-16 (relative) away from S; the rest are computed with
+// the IEEE expression.
+__device__ __forceinline__ bool dist_below(const geo::Mat3& Q, float x, float y, bool weighted, float w, float S)
+{
+    const float aux0 = x * x, aux1 = 2 * x * y, aux2 = 2 * x, aux3 = y * y, aux4 = 2 * y;
+    const float t1 = x * Q.m[0][0] + y * Q.m[0][1] + Q.m[0][2];
+    const float t2 = x * Q.m[0][1] + y * Q.m[1][1] + Q.m[1][2];
+    const float denom = t1 * t1 + t2 * t2;
+    const float dot = aux0 * Q.m[0][0] + aux1 * Q.m[0][1] + aux2 * Q.m[0][2] + aux3 * Q.m[1][1] + aux4 * Q.m[1][2] +
+                      Q.m[2][2];
+    const float dd = dot * dot;
+    float v = dd * __frcp_rn(denom);
+    if (weighted) v *= w;
+    if (v < S * 0.99998f) return true;
+    if (v > S * 1.00002f && v <= 3.4e38f) return false;  // an infinite estimate is settled exactly
+    float d = dd / denom;
+    if (weighted) d *= w;
+    return d < S;
+}
+
+// Block-wide outlierRemoval (Vote.cpp:414-576) with maxSize 60 over the n
+// edge points idx[0, n) of level L: LMedS ellipse from random 5-point subsets
+// of a regular subsample, drawn from `rng`, kDrawsPerBatch at a time and
+// accepted in draw order; then idx is compacted in place (order kept) to the
+// points whose distance (times 255 / |gradient| when weighted) is below
+// threshold * the best median.  Returns their number (0 when fewer than 5
+// points are subsampled).  Every thread of the block must call it.
+__device__ int lmeds_outliers(const LoopOneLevel& L, int32_t* idx, int n, bool weighted, float threshold,
+                              const geo::Pcg32 rng0, int32_t* err)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ geo::Pt pts[kLmedsMaxPts];
+    __shared__ float wts[kLmedsMaxPts];
+    __shared__ uint32_t raws[kRawPool];
+    __shared__ uint8_t mods[kRawPool];
+    __shared__ int16_t lens[kRawPool];
+    __shared__ uint32_t keysAll[kLmedsMaxPts * kFilterThreads];
+    __shared__ int16_t starts[kFilterThreads];
+    __shared__ int8_t perms[kFilterThreads][5];
+    __shared__ int kinds[kFilterThreads];
+    __shared__ float svals[kFilterThreads];
+    __shared__ float sQ[kFilterThreads][9];
+    __shared__ float bestQ[9];
+    __shared__ int sNpts, sDone, sNd, sCounter, sDraws, sWarpCnt[kFilterThreads / 32];
+    __shared__ float sSm;
+    __shared__ unsigned long long sState, sInc;
+    const int nchild = n;
+    int32_t* children = idx;
+    // The reference scans the children and takes child i when i equals
+    // size_t(float(k) * step) for the next k: the taken indices are those
+    // targets while they increase strictly and stay below nchild.
+    const int nSub = min(nchild, 60);
+    __shared__ long long sTarget[kLmedsMaxPts + 1];
+    if (nSub >= 5 && tid <= kLmedsMaxPts) {
+        const float step = float(nchild) / float(nSub);
+        sTarget[tid] = (long long)size_t(float(size_t(tid)) * step);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int np = 0;
+        if (nSub >= 5) {
+            while (np <= kLmedsMaxPts && sTarget[np] < nchild && (np == 0 || sTarget[np] > sTarget[np - 1])) ++np;
+            if (np > kLmedsMaxPts) atomicOr(err, kLoopOneErrPoints);
+        }
+        sNpts = np;
+        for (int k = 0; k < 9; ++k) bestQ[k] = 0.f;
+        sSm = 10000000.0f;
+        sDone = 0;
+        sCounter = 0;
+        sDraws = 0;
+        sState = rng0.state;
+        sInc = rng0.inc;
+    }
+    __syncthreads();
+    const int np = sNpts;
+    if (np <= kLmedsMaxPts && tid < np) {
+        const int e = children[sTarget[tid]];
+        pts[tid] = {float(px_(L, e)), float(py_(L, e))};
+        wts[tid] = 255.f / gnorm(L, e);
+    }
+    __syncthreads();
+    if (nSub < 5 || np > kLmedsMaxPts) return 0;
+    // ... then random 5-point conics, 128 draws at a time, accepted in order.
+    const uint32_t rejectBelow = uint32_t(-uint32_t(np)) % uint32_t(np);
+    while (!sDone) {
+        // the next kRawPool outputs of the candidate's stream, 8 per thread
+        {
+            geo::Pcg32 g;
+            g.state = sState;
+            g.inc = sInc;
+            g.advance(uint64_t(tid) * (kRawPool / kFilterThreads));
+            for (int k = 0; k < kRawPool / kFilterThreads; ++k) {
+                const uint32_t r = g.next();
+                raws[tid * (kRawPool / kFilterThreads) + k] = r;
+                mods[tid * (kRawPool / kFilterThreads) + k] = uint8_t(r % uint32_t(np));
+            }
+        }
+        // Statistic.cpp:16-29 rand_5_k on that stream, as many whole draws as
+        // it holds.  A bounded draw rejects an output only below 2^32 mod np
+        // (< 64 of 2^32 values): when the pool holds none, a draw consumes
+        // outputs until it has 5 distinct residues, so each position's draw
+        // length is found in parallel and the draws chained from position 0.
+        bool rejects = false;
+        for (int k = 0; k < kRawPool / kFilterThreads; ++k)
+            rejects = rejects || raws[tid * (kRawPool / kFilterThreads) + k] < rejectBelow;
+        rejects = __syncthreads_or(rejects);
+        if (!rejects) {
+            for (int k = 0; k < kRawPool / kFilterThreads; ++k) {
+                const int p0 = tid * (kRawPool / kFilterThreads) + k;
+                int g[5];
+                const int q = draw_from(mods, p0, g);
+                lens[p0] = int16_t(q > 0 ? q - p0 : -1);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int ptr = 0, nd = 0;
+                while (nd < kFilterThreads && ptr < kRawPool && lens[ptr] > 0) {
+                    starts[nd++] = int16_t(ptr);
+                    ptr += lens[ptr];
+                }
+                if (nd == 0) atomicOr(err, kLoopOneErrRandom);
+                sNd = nd;
+                geo::Pcg32 g;
+                g.state = sState;
+                g.inc = sInc;
+                g.advance(uint64_t(ptr));
+                sState = g.state;
+            }
+            __syncthreads();
+            if (tid < sNd) {
+                int g[5];
+                draw_from(mods, starts[tid], g);
+#pragma unroll
+                for (int i = 0; i < 5; ++i) perms[tid][i] = int8_t(g[i]);
+            }
+        } else if (tid == 0) {
+            int ptr = 0, nd = 0;
+            while (nd < kFilterThreads) {
+                int perm[5] = {-1, -1, -1, -1, -1};
+                const int start = ptr;
+                bool complete = true;
+                for (int i = 0; i < 5 && complete; ++i) {
+                    for (;;) {
+                        if (ptr >= kRawPool) {
+                            complete = false;
+                            break;
+                        }
+                        const uint32_t raw = raws[ptr];
+                        const int r = mods[ptr];
+                        ++ptr;
+                        if (raw < rejectBelow) continue;
+                        bool seen = false;
+                        for (int q = 0; q < i; ++q) seen = seen || perm[q] == r;
+                        if (seen) continue;
+                        perm[i] = r;
+                        break;
+                    }
+                }
+                if (!complete) {
+                    ptr = start;
+                    break;
+                }
+                for (int i = 0; i < 5; ++i) perms[nd][i] = int8_t(perm[i]);
+                ++nd;
+            }
+            if (nd == 0) atomicOr(err, kLoopOneErrRandom);
+            sNd = nd;
+            geo::Pcg32 g;
+            g.state = sState;
+            g.inc = sInc;
+            g.advance(uint64_t(ptr));
+            sState = g.state;
+        }
+        __syncthreads();
+        const int nd = sNd;
+        if (nd == 0) break;
+        const float SmStart = sSm;
+        if (tid < nd) {
+            int perm[5];
+            for (int i = 0; i < 5; ++i) perm[i] = perms[tid][i];
+            geo::Mat3 Q;
+            int kind = cand::lmeds_conic(pts, perm, Q);
+            float S = 0.f;
+            if (kind == kDrawUsable) {
+                int below = 0;
+#pragma unroll 4
+                for (int i = 0; i < np; ++i) below += dist_below(Q, pts[i].x, pts[i].y, weighted, wts[i], SmStart);
+                // no median below the best so far: it cannot improve (Sm only decreases)
+                if (below >= np / 2 + 1) {
+                    uint32_t* keys = keysAll + tid;  // column tid of a [kLmedsMaxPts][kFilterThreads] array
+                    for (int i = 0; i < np; ++i) {
+                        float d = geo::dist_point_ellipse(Q, pts[i].x, pts[i].y);
+                        if (weighted) d *= wts[i];
+                        keys[i * kFilterThreads] = geo::order_key(d);
+                    }
+                    S = key_value(select_key_strided(keys, np, np / 2));
+                } else {
+                    kind = kDrawNoGain;
+                }
+            }
+            kinds[tid] = kind;
+            svals[tid] = S;
+            for (int k = 0; k < 9; ++k) sQ[tid][k] = Q.m[k / 3][k % 3];
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int counter = sCounter, draws = sDraws, best = -1;
+            float Sm = sSm;
+            for (int j = 0; j < nd; ++j) {
+                if (!(counter < 70 && draws < 7000)) break;
+                ++draws;
+                const int kind = kinds[j];
+                if (kind == kDrawFail || kind == kDrawNoGain) {
+                    ++counter;
+                } else if (kind == kDrawNotReal) {
+                    // neither counted nor used
+                } else {
+                    if (svals[j] < Sm) {
+                        counter = 0;
+                        Sm = svals[j];
+                        best = j;
+                    } else {
+                        ++counter;
+                    }
+                }
+            }
+            if (best >= 0)
+                for (int k = 0; k < 9; ++k) bestQ[k] = sQ[best][k];
+            sCounter = counter;
+            sDraws = draws;
+            sSm = Sm;
+            if (!(counter < 70 && draws < 7000)) sDone = 1;
+        }
+        __syncthreads();
+    }
+    // the children whose weighted distance is below threshold * median, in order
+    geo::Mat3 Q;
+    for (int k = 0; k < 9; ++k) Q.m[k / 3][k % 3] = bestQ[k];
+    const float thr = threshold * sSm;
+    int nflt = 0;
+    for (int c0 = 0; c0 < nchild; c0 += kFilterThreads) {
+        const int i = c0 + tid;
+        int e = -1;
+        if (i < nchild) e = children[i];
+        __syncthreads();  // every element of the chunk read before any is overwritten
+        bool pass = false;
+        if (e >= 0) {
+            float d = geo::dist_point_ellipse(Q, float(px_(L, e)), float(py_(L, e)));
+            if (weighted) d = d * 255 / gnorm(L, e);
+            pass = d < thr;
+        }
+        const unsigned mask = __ballot_sync(kFull, pass);
+        if (lane == 0) sWarpCnt[warp] = __popc(mask);
+        __syncthreads();
+        int off = nflt;
+        for (int w = 0; w < warp; ++w) off += sWarpCnt[w];
+        if (pass) children[off + __popc(mask & ((1u << lane) - 1u))] = e;
+        for (int w = 0; w < kFilterThreads / 32; ++w) nflt += sWarpCnt[w];
+        __syncthreads();
+    }
+    return nflt;
+}
+
 
 __global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
 {
@@ -377,18 +673,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
     const int len = nf + 1 + nb;
     int32_t* children = a.children + size_t(blockIdx.x) * kChildCap;
 
-    __shared__ geo::Pt pts[kLmedsMaxPts];
-    __shared__ float wts[kLmedsMaxPts];
-    __shared__ uint32_t raws[kRawPool];
-    __shared__ uint8_t mods[kRawPool];
-    __shared__ int8_t perms[kFilterThreads][5];
-    __shared__ int kinds[kFilterThreads];
-    __shared__ float svals[kFilterThreads];
-    __shared__ float sQ[kFilterThreads][9];
-    __shared__ float bestQ[9];
-    __shared__ int sNchild, sNpts, sDone, sNd, sCounter, sDraws, sWarpCnt[kFilterThreads / 32];
-    __shared__ float sSm;
-    __shared__ unsigned long long sState, sInc;
+    __shared__ int sNchild;
 
     // children (Vote.cpp:396-412): voters of the points with >= voteMax/14 votes
     if (warp == 0) {
@@ -446,194 +731,167 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
         return;
     }
 
-    // outlierRemoval (Vote.cpp:414-576) with maxSize 60 and inverse-gradient
-    // weights: a regular subsample of the children ...
-    // The reference scans the children and takes child i when i equals
-    // size_t(float(k) * step) for the next k: the taken indices are those
-    // targets while they increase strictly and stay below nchild.
-    const int nSub = min(nchild, 60);
-    __shared__ long long sTarget[kLmedsMaxPts + 1];
-    if (nSub >= 5 && tid <= kLmedsMaxPts) {
-        const float step = float(nchild) / float(nSub);
-        sTarget[tid] = (long long)size_t(float(size_t(tid)) * step);
-    }
-    __syncthreads();
-    if (tid == 0) {
-        int np = 0;
-        if (nSub >= 5) {
-            while (np <= kLmedsMaxPts && sTarget[np] < nchild && (np == 0 || sTarget[np] > sTarget[np - 1])) ++np;
-            if (np > kLmedsMaxPts) atomicOr(a.err, kLoopOneErrPoints);
-        }
-        sNpts = np;
-        for (int k = 0; k < 9; ++k) bestQ[k] = 0.f;
-        sSm = 10000000.0f;
-        sDone = 0;
-        sCounter = 0;
-        sDraws = 0;
-        const geo::Pcg32 rng = cand::candidate_rng(L.level, uint64_t(rank), 0);
-        sState = rng.state;
-        sInc = rng.inc;
-    }
-    __syncthreads();
-    const int np = sNpts;
-    if (np <= kLmedsMaxPts && tid < np) {
-        const int e = children[sTarget[tid]];
-        pts[tid] = {float(px_(L, e)), float(py_(L, e))};
-        wts[tid] = 255.f / gnorm(L, e);
-    }
-    __syncthreads();
-    if (nSub < 5 || np > kLmedsMaxPts) {
-        if (tid == 0) {
-            meta[0] = L.order[s];
-            meta[1] = nchild;
-            meta[2] = 0;
-            meta[3] = 0;
-        }
-        return;
-    }
-    // ... then random 5-point conics, 128 draws at a time, accepted in order.
-    const uint32_t threshold = uint32_t(-uint32_t(np)) % uint32_t(np);
-    uint32_t keys[kLmedsMaxPts];
-    while (!sDone) {
-        // the next kRawPool outputs of the candidate's stream, 8 per thread
-        {
-            geo::Pcg32 g;
-            g.state = sState;
-            g.inc = sInc;
-            g.advance(uint64_t(tid) * (kRawPool / kFilterThreads));
-            for (int k = 0; k < kRawPool / kFilterThreads; ++k) {
-                const uint32_t r = g.next();
-                raws[tid * (kRawPool / kFilterThreads) + k] = r;
-                mods[tid * (kRawPool / kFilterThreads) + k] = uint8_t(r % uint32_t(np));
-            }
-        }
-        __syncthreads();
-        // Statistic.cpp:16-29 rand_5_k on that stream, as many whole draws as it holds
-        if (tid == 0) {
-            int ptr = 0, nd = 0;
-            while (nd < kFilterThreads) {
-                int perm[5] = {-1, -1, -1, -1, -1};
-                const int start = ptr;
-                bool complete = true;
-                for (int i = 0; i < 5 && complete; ++i) {
-                    for (;;) {
-                        if (ptr >= kRawPool) {
-                            complete = false;
-                            break;
-                        }
-                        const uint32_t raw = raws[ptr];
-                        const int r = mods[ptr];
-                        ++ptr;
-                        if (raw < threshold) continue;
-                        bool seen = false;
-                        for (int q = 0; q < i; ++q) seen = seen || perm[q] == r;
-                        if (seen) continue;
-                        perm[i] = r;
-                        break;
-                    }
-                }
-                if (!complete) {
-                    ptr = start;
-                    break;
-                }
-                for (int i = 0; i < 5; ++i) perms[nd][i] = int8_t(perm[i]);
-                ++nd;
-            }
-            if (nd == 0) atomicOr(a.err, kLoopOneErrRandom);
-            sNd = nd;
-            geo::Pcg32 g;
-            g.state = sState;
-            g.inc = sInc;
-            g.advance(uint64_t(ptr));
-            sState = g.state;
-        }
-        __syncthreads();
-        const int nd = sNd;
-        if (nd == 0) break;
-        const float SmStart = sSm;
-        if (tid < nd) {
-            int perm[5];
-            for (int i = 0; i < 5; ++i) perm[i] = perms[tid][i];
-            geo::Mat3 Q;
-            int kind = cand::lmeds_conic(pts, perm, Q);
-            float S = 0.f;
-            if (kind == kDrawUsable) {
-                int below = 0;
-                for (int i = 0; i < np; ++i) {
-                    const float d = geo::dist_point_ellipse(Q, pts[i].x, pts[i].y) * wts[i];
-                    keys[i] = geo::order_key(d);
-                    below += d < SmStart;
-                }
-                // no median below the best so far: it cannot improve (Sm only decreases)
-                if (below >= np / 2 + 1) S = key_value(select_key(keys, np, np / 2));
-                else kind = kDrawNoGain;
-            }
-            kinds[tid] = kind;
-            svals[tid] = S;
-            for (int k = 0; k < 9; ++k) sQ[tid][k] = Q.m[k / 3][k % 3];
-        }
-        __syncthreads();
-        if (tid == 0) {
-            int counter = sCounter, draws = sDraws, best = -1;
-            float Sm = sSm;
-            for (int j = 0; j < nd; ++j) {
-                if (!(counter < 70 && draws < 7000)) break;
-                ++draws;
-                const int kind = kinds[j];
-                if (kind == kDrawFail || kind == kDrawNoGain) {
-                    ++counter;
-                } else if (kind == kDrawNotReal) {
-                    // neither counted nor used
-                } else {
-                    if (svals[j] < Sm) {
-                        counter = 0;
-                        Sm = svals[j];
-                        best = j;
-                    } else {
-                        ++counter;
-                    }
-                }
-            }
-            if (best >= 0)
-                for (int k = 0; k < 9; ++k) bestQ[k] = sQ[best][k];
-            sCounter = counter;
-            sDraws = draws;
-            sSm = Sm;
-            if (!(counter < 70 && draws < 7000)) sDone = 1;
-        }
-        __syncthreads();
-    }
-    // the children whose weighted distance is below threshold * median, in order
-    geo::Mat3 Q;
-    for (int k = 0; k < 9; ++k) Q.m[k / 3][k % 3] = bestQ[k];
-    const float thr = a.threshold * sSm;
-    int nflt = 0;
-    for (int c0 = 0; c0 < nchild; c0 += kFilterThreads) {
-        const int i = c0 + tid;
-        int e = -1;
-        if (i < nchild) e = children[i];
-        __syncthreads();  // every element of the chunk read before any is overwritten
-        bool pass = false;
-        if (e >= 0) {
-            float d = geo::dist_point_ellipse(Q, float(px_(L, e)), float(py_(L, e)));
-            d = d * 255 / gnorm(L, e);
-            pass = d < thr;
-        }
-        const unsigned mask = __ballot_sync(kFull, pass);
-        if (lane == 0) sWarpCnt[warp] = __popc(mask);
-        __syncthreads();
-        int off = nflt;
-        for (int w = 0; w < warp; ++w) off += sWarpCnt[w];
-        if (pass) children[off + __popc(mask & ((1u << lane) - 1u))] = e;
-        for (int w = 0; w < kFilterThreads / 32; ++w) nflt += sWarpCnt[w];
-        __syncthreads();
-    }
+    // outlierRemoval with inverse-gradient weights (Detection.cpp:131-133)
+    const int nflt = lmeds_outliers(L, children, nchild, true, a.threshold,
+                                    cand::candidate_rng(L.level, uint64_t(rank), 0), a.err);
     if (tid == 0) {
         meta[0] = L.order[s];
         meta[1] = nchild;
         meta[2] = nflt >= 5 ? 1 : 0;
         meta[3] = nflt;
     }
+}
+
+// float -> int as the host's conversion does it on x86-64: out of range and
+// NaN give INT_MIN (the device instruction would saturate instead).
+__device__ __forceinline__ int host_int(float f)
+{
+    return (f >= -2147483648.0f && f < 2147483648.0f) ? int(f) : int(0x80000000u);
+}
+
+// Multiresolution.cpp:43-142 intersectLineToTwoEllipses for row y: whether the
+// row counts, and up to two x ranges to scan.
+__device__ bool refit_row(const geo::Mat3& Qi, const geo::Mat3& Qo, int W, int y, int& nr, int xb[2], int xe[2])
+{
+    float io[2], ii[2];
+    const int no = geo::intersect_line_q(Qo, float(y), true, io);
+    const int ni = geo::intersect_line_q(Qi, float(y), true, ii);
+    nr = 0;
+    if (no == 2 && ni == 2) {
+        nr = 2;
+        xb[0] = max(0, host_int(io[0]));
+        xe[0] = min(W - 1, host_int(ii[0]));
+        xb[1] = max(0, host_int(ii[1]));
+        xe[1] = min(W - 1, host_int(io[1]));
+    } else if (no == 2 && ni <= 1) {
+        nr = 1;
+        xb[0] = max(0, host_int(io[0]));
+        xe[0] = min(W - 1, host_int(io[1]));
+    } else if (no == 1 && ni == 0) {
+        if (io[0] >= 0 && io[0] < float(W)) {
+            nr = 1;
+            xb[0] = xe[0] = host_int(io[0]);
+        }
+    } else {
+        return false;
+    }
+    return true;
+}
+
+// Edge points of row y taken into the hull, in x order: written at out[]
+// when out is not null; returns their number.
+__device__ int refit_row_takes(const LoopOneLevel& L, const geo::Mat3& Qi, const geo::Mat3& Qo, float inCx,
+                               float inCy, int y, int32_t* out)
+{
+    int nr, xb[2], xe[2];
+    if (!refit_row(Qi, Qo, L.W, y, nr, xb, xe)) return 0;
+    int n = 0;
+    for (int r = 0; r < nr; ++r)
+        for (int x = xb[r]; x <= xe[r]; ++x) {
+            const int e = at(L, x, y);
+            if (e < 0) continue;
+            const float cx = inCx - float(px_(L, e)), cy = inCy - float(py_(L, e));
+            if (gdx(L, e) * cx + gdy(L, e) * cy < 0) {
+                if (out) out[n] = e;
+                ++n;
+            }
+        }
+    return n;
+}
+
+// Multiresolution.cpp:319-401: level-0 hull of one coarse-level marker (rows
+// from the center row down the image until one misses the hull, then from
+// the center row up), then the outlier removal without weights.
+__global__ void __launch_bounds__(kFilterThreads) k_refit(LoopOneLevel L, const RefitTask* tasks, int32_t* hullAll,
+                                                        int32_t* rowsAll, int rowStride, int32_t* counts)
+{
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const RefitTask& T = tasks[b];
+    int32_t* hull = hullAll + size_t(b) * kChildCap;
+    int32_t* rowOff = rowsAll + size_t(b) * rowStride;
+    int32_t* err = counts + gridDim.x;
+    geo::Mat3 Qi, Qo;
+    for (int k = 0; k < 9; ++k) {
+        Qi.m[k / 3][k % 3] = T.qin[k];
+        Qo.m[k / 3][k % 3] = T.qout[k];
+    }
+    const int maxY = max(host_int(T.yc), 0);
+    const int minY = min(host_int(T.yc), L.H - 1);
+    __shared__ int sUpEnd, sDownEnd, sTotal;
+    __shared__ int sPart[kFilterThreads];
+    if (tid == 0) {
+        sUpEnd = L.H;
+        sDownEnd = -1;
+    }
+    __syncthreads();
+    int nr, xb[2], xe[2];
+    for (int y = maxY + tid; y < L.H; y += blockDim.x)
+        if (!refit_row(Qi, Qo, L.W, y, nr, xb, xe)) atomicMin(&sUpEnd, y);
+    for (int y = minY - tid; y >= 0; y -= blockDim.x)
+        if (!refit_row(Qi, Qo, L.W, y, nr, xb, xe)) atomicMax(&sDownEnd, y);
+    __syncthreads();
+    const int rUp = max(sUpEnd - maxY, 0), rDown = max(minY - sDownEnd, 0);
+    const int R = rUp + rDown;
+    auto row_y = [&](int r) { return r < rUp ? maxY + r : minY - (r - rUp); };
+    // per-row counts in processing order, contiguous chunks per thread
+    const int chunk = (R + blockDim.x - 1) / blockDim.x;
+    const int r0 = min(R, tid * chunk), r1 = min(R, r0 + chunk);
+    int part = 0;
+    for (int r = r0; r < r1; ++r) {
+        const int c = refit_row_takes(L, Qi, Qo, T.inCx, T.inCy, row_y(r), nullptr);
+        rowOff[r] = c;
+        part += c;
+    }
+    sPart[tid] = part;
+    __syncthreads();
+    if (tid == 0) {
+        int acc = 0;
+        for (int k = 0; k < int(blockDim.x); ++k) {
+            const int v = sPart[k];
+            sPart[k] = acc;
+            acc += v;
+        }
+        sTotal = acc;
+    }
+    __syncthreads();
+    const int total = sTotal;
+    if (total > kChildCap) {
+        if (tid == 0) {
+            atomicOr(err, kLoopOneErrChildren);
+            counts[b] = -1;
+        }
+        return;
+    }
+    int off = sPart[tid];
+    for (int r = r0; r < r1; ++r) {
+        const int c = rowOff[r];
+        refit_row_takes(L, Qi, Qo, T.inCx, T.inCy, row_y(r), hull + off);
+        off += c;
+    }
+    __syncthreads();
+    if (total < 5) {
+        if (tid == 0) counts[b] = -1;
+        return;
+    }
+    const geo::Pcg32 rng(271828, (uint64_t(1) << 62) | uint64_t(T.marker));
+    const int nflt = lmeds_outliers(L, hull, total, false, 20.0f, rng, err);
+    if (tid == 0) counts[b] = nflt;
+}
+
+__global__ void __launch_bounds__(256) k_refit_pack(const int32_t* hullAll, const int32_t* counts, int32_t* packed)
+{
+    const int b = blockIdx.x;
+    __shared__ int sOff;
+    const int n = counts[b];
+    if (n <= 0) return;
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int q = 0; q < b; ++q) off += max(counts[q], 0);
+        sOff = off;
+    }
+    __syncthreads();
+    const int32_t* src = hullAll + size_t(b) * kChildCap;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) packed[sOff + i] = src[i];
 }
 
 // Kept candidates' filtered children, in candidate order, into one array.
@@ -682,6 +940,7 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
     // seeds processed per level: max(rows / 2, maximumNbSeeds) (Detection.cpp:603-605);
     // level 0 has the most rows
     maxSlotsPerLevel_ = std::max(max_h / 2, p.maximumNbSeeds);
+    maxH_ = max_h;
     totalSlots_ = nl_ * maxSlotsPerLevel_;
     size_t nrec = 0;
     for (int l = 0; l < nl_; ++l) {
@@ -731,6 +990,12 @@ int LoopOneGpu::resolve_smem() const
 LoopOneGpu::~LoopOneGpu()
 {
     for (void* q : allocs_) cudaFree(q);
+    for (void* q : {static_cast<void*>(d_rtask_), static_cast<void*>(d_rhull_), static_cast<void*>(d_rrows_),
+                    static_cast<void*>(d_rcount_), static_cast<void*>(d_rpacked_)})
+        if (q) cudaFree(q);
+    if (h_rtask_) cudaFreeHost(h_rtask_);
+    if (h_rcount_) cudaFreeHost(h_rcount_);
+    if (h_rpacked_) cudaFreeHost(h_rpacked_);
     if (h_order_) cudaFreeHost(h_order_);
     if (h_meta_) cudaFreeHost(h_meta_);
     if (h_flt_) cudaFreeHost(h_flt_);
@@ -839,6 +1104,76 @@ void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
             }
             o.foff.push_back(int32_t(o.flt.size()));
         }
+    }
+}
+
+void LoopOneGpu::ensure_refit_capacity(int n)
+{
+    if (n <= refitCap_) return;
+    for (void* q : {static_cast<void*>(d_rtask_), static_cast<void*>(d_rhull_), static_cast<void*>(d_rrows_),
+                    static_cast<void*>(d_rcount_), static_cast<void*>(d_rpacked_)})
+        if (q) cudaFree(q);
+    if (h_rtask_) cudaFreeHost(h_rtask_);
+    if (h_rcount_) cudaFreeHost(h_rcount_);
+    d_rtask_ = nullptr;
+    d_rhull_ = d_rrows_ = d_rcount_ = d_rpacked_ = nullptr;
+    h_rtask_ = nullptr;
+    h_rcount_ = nullptr;
+    refitCap_ = 0;
+    const int cap = std::max(n, 64);
+    CCTAGB_CUDA(cudaMalloc(&d_rtask_, sizeof(RefitTask) * cap));
+    CCTAGB_CUDA(cudaMalloc(&d_rhull_, sizeof(int32_t) * size_t(cap) * kChildCap));
+    CCTAGB_CUDA(cudaMalloc(&d_rrows_, sizeof(int32_t) * size_t(cap) * (maxH_ + 2)));
+    CCTAGB_CUDA(cudaMalloc(&d_rcount_, sizeof(int32_t) * (cap + 1)));
+    CCTAGB_CUDA(cudaMalloc(&d_rpacked_, sizeof(int32_t) * size_t(cap) * kChildCap));
+    CCTAGB_CUDA(cudaMallocHost(&h_rtask_, sizeof(RefitTask) * cap));
+    CCTAGB_CUDA(cudaMallocHost(&h_rcount_, sizeof(int32_t) * (cap + 1)));
+    refitCap_ = cap;
+}
+
+void LoopOneGpu::refit(const Levels& lv, const std::vector<RefitTask>& tasks, cudaStream_t s,
+                       std::vector<std::vector<int32_t>>& filtered)
+{
+    const int n = int(tasks.size());
+    filtered.assign(size_t(n), {});
+    if (n == 0) return;
+    ensure_refit_capacity(n);
+    const LevelView& v = lv.l[0];
+    if (v.H > maxH_) throw Error{CCTAGB_INTERNAL, "refit: frame taller than the handle"};
+    LoopOneLevel L = args_.lv[0];  // level-0 view of the frame loop one ran on
+    std::copy(tasks.begin(), tasks.end(), h_rtask_);
+    CCTAGB_CUDA(cudaMemcpyAsync(d_rtask_, h_rtask_, sizeof(RefitTask) * n, cudaMemcpyHostToDevice, s));
+    CCTAGB_CUDA(cudaMemsetAsync(d_rcount_ + n, 0, sizeof(int32_t), s));
+    k_refit<<<n, kFilterThreads, 0, s>>>(L, d_rtask_, d_rhull_, d_rrows_, maxH_ + 2, d_rcount_);
+    CCTAGB_CUDA(cudaGetLastError());
+    k_refit_pack<<<n, 256, 0, s>>>(d_rhull_, d_rcount_, d_rpacked_);
+    CCTAGB_CUDA(cudaGetLastError());
+    CCTAGB_CUDA(cudaMemcpyAsync(h_rcount_, d_rcount_, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    const int err = h_rcount_[n];
+    if (err & kLoopOneErrChildren)
+        throw Error{CCTAGB_OVERFLOW_VOTERS, "a re-fit hull holds more than 32768 edge points"};
+    if (err) throw Error{CCTAGB_INTERNAL, "refit: error bits " + std::to_string(err)};
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) total += size_t(std::max(h_rcount_[i], 0));
+    if (total > h_rpacked_cap_) {
+        if (h_rpacked_) cudaFreeHost(h_rpacked_);
+        h_rpacked_ = nullptr;
+        h_rpacked_cap_ = 0;
+        CCTAGB_CUDA(cudaMallocHost(&h_rpacked_, sizeof(int32_t) * std::max<size_t>(total, 4096)));
+        h_rpacked_cap_ = std::max<size_t>(total, 4096);
+    }
+    if (total) {
+        CCTAGB_CUDA(cudaMemcpyAsync(h_rpacked_, d_rpacked_, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, s));
+        CCTAGB_CUDA(cudaStreamSynchronize(s));
+    }
+    h2d_ += (long long)sizeof(RefitTask) * n;
+    d2h_ += 4LL * (n + 1) + 4LL * (long long)total;
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        const int c = std::max(h_rcount_[i], 0);
+        filtered[size_t(i)].assign(h_rpacked_ + off, h_rpacked_ + off + c);
+        off += size_t(c);
     }
 }
 

@@ -61,6 +61,15 @@ constexpr int kLoopOneErrWindow = 2;
 constexpr int kLoopOneErrPoints = 4;
 constexpr int kLoopOneErrRandom = 8;
 
+// One coarse-level marker to re-fit on level 0 (Multiresolution.cpp:319-401):
+// the hull's inner and outer conics, the inner center, the center row, and
+// the marker's index in the frame (its random stream).
+struct RefitTask {
+    float qin[9], qout[9];
+    float inCx, inCy, yc;
+    int marker;
+};
+
 void launch_loop_one(const LoopOneArgs& a, cudaStream_t s);
 
 // Device buffers of loop 1 / loop 2 (first half) for one detection slot.
@@ -79,12 +88,19 @@ public:
                 cudaStream_t s);
     // Waits for launch()'s work and fills `out` (one LoopTwoIn per level).
     void collect(cudaStream_t s, std::vector<LoopTwoIn>& out);
+    // Level-0 hull collection and outlier removal of the re-fit of `tasks`
+    // on level 0 of `lv` (synchronous): per task, the filtered hull points
+    // (fewer than 5 when the marker keeps its coarse-level ellipse).
+    void refit(const Levels& lv, const std::vector<RefitTask>& tasks, cudaStream_t s,
+               std::vector<std::vector<int32_t>>& filtered);
     int launches() const { return 6; }
+    int refit_launches() const { return 2; }
     long long h2d_bytes() const { return h2d_; }
     long long d2h_bytes() const { return d2h_; }
 
 private:
     int resolve_smem() const;
+    void ensure_refit_capacity(int n);
     cctagb_params p_;
     int nl_ = 0, n2max_ = 0, maxSlotsPerLevel_ = 0, totalSlots_ = 0;
     LoopOneArgs args_{};
@@ -93,6 +109,17 @@ private:
     int4* d_rec_ = nullptr;        // point records of all levels
     int32_t* d_packed_ = nullptr;  // kept candidates' filtered children
     std::vector<int> caps_;
+    int maxH_ = 0;
+    int refitCap_ = 0;
+    RefitTask* d_rtask_ = nullptr;
+    RefitTask* h_rtask_ = nullptr;
+    int32_t* d_rhull_ = nullptr;    // refitCap_ * kChildCap
+    int32_t* d_rrows_ = nullptr;    // refitCap_ * (maxH_ + 2) per-row offsets
+    int32_t* d_rcount_ = nullptr;   // refitCap_ + 1 (last: error bits)
+    int32_t* h_rcount_ = nullptr;
+    int32_t* d_rpacked_ = nullptr;  // refitCap_ * kChildCap
+    int32_t* h_rpacked_ = nullptr;
+    size_t h_rpacked_cap_ = 0;
     int32_t* h_meta_ = nullptr;    // pinned: meta + made counts + err
     int32_t* h_flt_ = nullptr;     // pinned: filtered children, all candidates
     size_t h_flt_cap_ = 0;
