@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256) k_seed_slots(LoopOneArgs a)
 // Points of one edge-linking call (the reference's set of visited positions),
 // an open-addressing set in shared memory used by the 8 lanes of one seed.
 constexpr int kLinkThreads = 128;
-constexpr int kLinkGroups = kLinkThreads / 8;
+constexpr int kLinkGroups = kLinkThreads / 32;  // one seed per warp (lanes 0-7): seeds do not diverge each other
 
 __device__ __forceinline__ uint32_t visit_slot(int v) { return (uint32_t(v) * 2654435761u) >> 23; }
 __device__ __forceinline__ bool visit_has(const int32_t* set, int v)
@@ -141,6 +141,27 @@ __device__ __forceinline__ void visit_add(int32_t* set, int v)
             return;
         }
     }
+}
+
+__device__ __forceinline__ int4 shfl_int4(unsigned mask, int4 v, int src)
+{
+    return make_int4(__shfl_sync(mask, v.x, src), __shfl_sync(mask, v.y, src), __shfl_sync(mask, v.z, src),
+                     __shfl_sync(mask, v.w, src));
+}
+
+// cand::link_convexity_lost, decided from the fast sine and cosine where they
+// are more than 1e-3 away from every threshold of the test (their error is
+// below 1e-5 for |d| < 2 pi) and from the exact test elsewhere.
+__device__ __forceinline__ bool convexity_lost(float front, float back, bool full, int dir)
+{
+    const float d = back - front;
+    const float s = float(dir) * __sinf(d), c = __cosf(d);
+    if (full) {
+        if (fabsf(s) > 1e-3f) return s < 0.0f;
+    } else if (fabsf(s) > 1e-3f && fabsf(s + 0.707f) > 1e-3f && fabsf(c) > 1e-3f) {
+        return (s < -0.707f && c > 0.f) || (s < 0.f && c < 0.f);
+    }
+    return cand::link_convexity_lost(front, back, full, dir);
 }
 
 // Vote.cpp:272-394 edgeLinkingDir from the seed in direction dir, by the 8
@@ -173,6 +194,9 @@ __device__ int link_walk(const int4* recs, int seed, int dir, int32_t* segc, int
         const int k = dir == 1 ? (8 - shifting + j) % 8 : (shifting + j) % 8;
         // direction -1 mirrors the y offsets: neighbour (8 - k) % 8 of the +1 table
         const int q = nbr(r, dir == 1 ? k : (8 - k) % 8);
+        // every lane fetches its neighbour's record now; the step keeps one
+        PointRec rq = r;
+        if (q >= 0) rq = load_rec(recs, q);
         const bool cand = q >= 0 && !visit_has(vis, q);
         const unsigned hits = (__ballot_sync(gmask, cand) >> gbase) & 0xffu;
         if (!hits) {
@@ -182,7 +206,7 @@ __device__ int link_walk(const int4* recs, int seed, int dir, int32_t* segc, int
             const int qn = __shfl_sync(gmask, q, gbase + jj);
             const float front = ring[head];
             const float back = ring[head + count - 1 > window ? head + count - window - 2 : head + count - 1];
-            if (cand::link_convexity_lost(front, back, count == window, dir)) {
+            if (convexity_lost(front, back, count == window, dir)) {
                 stop = cand::kConvexityLost;
             } else {
                 if (dir > 0) {
@@ -193,7 +217,9 @@ __device__ int link_walk(const int4* recs, int seed, int dir, int32_t* segc, int
                     if (j == 0) segc[-nf] = qn;
                 }
                 if (j == 0) visit_add(vis, qn);
-                r = load_rec(recs, qn);
+                r.r0 = shfl_int4(gmask, rq.r0, gbase + jj);
+                r.r1 = shfl_int4(gmask, rq.r1, gbase + jj);
+                r.r2 = shfl_int4(gmask, rq.r2, gbase + jj);
                 averageVote = cand::link_average_vote(averageVote, 1 + nf + nb, r.r0.z);
                 stop = 1;
             }
@@ -212,9 +238,9 @@ __global__ void __launch_bounds__(kLinkThreads) k_link_seeds(LoopOneArgs a)
 {
     __shared__ int32_t visAll[kLinkGroups][kVisitSlots];
     __shared__ float ringAll[kLinkGroups][cand::kLinkMaxWindow + 1];
-    const int g = threadIdx.x >> 3, j = threadIdx.x & 7;
-    const int lane = threadIdx.x & 31;
-    const unsigned gmask = 0xffu << (lane & ~7);
+    const int g = threadIdx.x >> 5, j = threadIdx.x & 31;
+    if (j >= 8) return;
+    const unsigned gmask = 0xffu;
     const int t = blockIdx.x * kLinkGroups + g;
     if (t >= a.totalSlots) return;
     const int l = t / a.maxSlotsPerLevel, s = t % a.maxSlotsPerLevel;
@@ -324,31 +350,25 @@ __global__ void __launch_bounds__(kResolveThreads) k_link_resolve(LoopOneArgs a)
 }
 
 // Value of rank k (NaN last) of the n order keys v[0], v[kFilterThreads],
-// v[2 kFilterThreads], ... (one thread's column of a shared array), by
-// quickselect; the keys are reordered.
-__device__ uint32_t select_key_strided(uint32_t* v, int n, int k)
+// v[2 kFilterThreads], ... (one thread's column of a shared array): the key
+// with fewer than k + 1 smaller keys and more than k smaller-or-equal ones.
+// Branch-free with a fixed trip count, so that the lanes of a warp selecting
+// at the same time do not diverge.
+__device__ uint32_t rank_key_strided(const uint32_t* v, int n, int k)
 {
-    auto at_ = [&](int i) -> uint32_t& { return v[i * kFilterThreads]; };
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const uint32_t pivot = at_((lo + hi) >> 1);
-        int i = lo, j = hi;
-        while (i <= j) {
-            while (at_(i) < pivot) ++i;
-            while (at_(j) > pivot) --j;
-            if (i <= j) {
-                const uint32_t t = at_(i);
-                at_(i) = at_(j);
-                at_(j) = t;
-                ++i;
-                --j;
-            }
+    uint32_t res = 0;
+    for (int i = 0; i < n; ++i) {
+        const uint32_t ki = v[i * kFilterThreads];
+        int lt = 0, le = 0;
+#pragma unroll 8
+        for (int j = 0; j < n; ++j) {
+            const uint32_t kj = v[j * kFilterThreads];
+            lt += kj < ki;
+            le += kj <= ki;
         }
-        if (k <= j) hi = j;
-        else if (k >= i) lo = i;
-        else break;
+        res = (lt <= k && k < le) ? ki : res;
     }
-    return at_(k);
+    return res;
 }
 
 __device__ __forceinline__ float key_value(uint32_t k)
@@ -588,7 +608,7 @@ __device__ int lmeds_outliers(const LoopOneLevel& L, int32_t* idx, int n, bool w
                         if (weighted) d *= wts[i];
                         keys[i * kFilterThreads] = geo::order_key(d);
                     }
-                    S = key_value(select_key_strided(keys, np, np / 2));
+                    S = key_value(rank_key_strided(keys, np, np / 2));
                 } else {
                     kind = kDrawNoGain;
                 }
@@ -598,33 +618,67 @@ __device__ int lmeds_outliers(const LoopOneLevel& L, int32_t* idx, int n, bool w
             for (int k = 0; k < 9; ++k) sQ[tid][k] = Q.m[k / 3][k % 3];
         }
         __syncthreads();
-        if (tid == 0) {
+        // Acceptance in draw order (Vote.cpp:478-545) by warp 0, 32 draws at a
+        // time: draw j improves when its median is below the best before it,
+        // which is the minimum of the carried best and every usable median
+        // before j; the no-gain counter restarts at each improvement, and the
+        // loop stops before the first draw at which it has reached 70 (or the
+        // draws 7000).
+        if (warp == 0) {
             int counter = sCounter, draws = sDraws, best = -1;
             float Sm = sSm;
-            for (int j = 0; j < nd; ++j) {
-                if (!(counter < 70 && draws < 7000)) break;
-                ++draws;
-                const int kind = kinds[j];
-                if (kind == kDrawFail || kind == kDrawNoGain) {
-                    ++counter;
-                } else if (kind == kDrawNotReal) {
-                    // neither counted nor used
-                } else {
-                    if (svals[j] < Sm) {
-                        counter = 0;
-                        Sm = svals[j];
-                        best = j;
-                    } else {
-                        ++counter;
-                    }
+            bool stopped = false;
+            for (int c0 = 0; c0 < nd && !stopped; c0 += 32) {
+                const int j = c0 + lane;
+                const bool valid = j < nd;
+                const int kind = valid ? kinds[j] : kDrawNotReal;
+                const bool usable = valid && kind == kDrawUsable;
+                const float Sj = usable ? svals[j] : __int_as_float(0x7f800000);
+                float incl = Sj;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const float v = __shfl_up_sync(kFull, incl, o);
+                    if (lane >= o) incl = fminf(incl, v);
                 }
+                float excl = __shfl_up_sync(kFull, incl, 1);
+                if (lane == 0) excl = __int_as_float(0x7f800000);
+                const bool improving = usable && Sj < fminf(Sm, excl);
+                const bool counted = valid && (kind == kDrawFail || kind == kDrawNoGain || (usable && !improving));
+                const unsigned impM = __ballot_sync(kFull, improving);
+                const unsigned cntM = __ballot_sync(kFull, counted);
+                const unsigned lower = (1u << lane) - 1u;
+                const unsigned impBefore = impM & lower;
+                int cb;
+                if (impBefore) {
+                    const int last = 31 - __clz(impBefore);
+                    cb = __popc(cntM & lower & ~((2u << last) - 1u));
+                } else {
+                    cb = counter + __popc(cntM & lower);
+                }
+                const bool stopHere = valid && !(cb < 70 && draws + lane < 7000);
+                const unsigned stopM = __ballot_sync(kFull, stopHere);
+                const int n = min(nd - c0, 32);
+                const int js = stopM ? __ffs(stopM) - 1 : n;
+                const unsigned proc = js >= 32 ? 0xffffffffu : ((1u << js) - 1u);
+                const unsigned impP = impM & proc;
+                if (impP) {
+                    const int last = 31 - __clz(impP);
+                    best = c0 + last;
+                    Sm = __shfl_sync(kFull, Sj, last);
+                    counter = __popc(cntM & proc & ~((2u << last) - 1u));
+                } else {
+                    counter += __popc(cntM & proc);
+                }
+                draws += js;
+                stopped = stopM != 0;
             }
-            if (best >= 0)
-                for (int k = 0; k < 9; ++k) bestQ[k] = sQ[best][k];
-            sCounter = counter;
-            sDraws = draws;
-            sSm = Sm;
-            if (!(counter < 70 && draws < 7000)) sDone = 1;
+            if (lane == 0) {
+                if (best >= 0)
+                    for (int k = 0; k < 9; ++k) bestQ[k] = sQ[best][k];
+                sCounter = counter;
+                sDraws = draws;
+                sSm = Sm;
+                if (stopped || !(counter < 70 && draws < 7000)) sDone = 1;
+            }
         }
         __syncthreads();
     }
