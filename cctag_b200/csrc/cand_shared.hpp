@@ -10,6 +10,12 @@
 #include "geometry.hpp"
 #include "pmath.hpp"
 
+#if defined(__CUDACC__)
+#define CCTAGB_UNROLL _Pragma("unroll")
+#else
+#define CCTAGB_UNROLL
+#endif
+
 namespace cctagb {
 namespace cand {
 
@@ -60,11 +66,11 @@ CCTAGB_HD inline float received_vote_key(int nReceived, int nVoted)
 // elimination in the same order on both sides.
 CCTAGB_HD inline bool solve5(double A[5][5], double b[5], double x[5])
 {
-#pragma unroll
+CCTAGB_UNROLL
     for (int c = 0; c < 5; ++c) {
         int piv = c;
         double best = ::fabs(A[c][c]);
-#pragma unroll
+CCTAGB_UNROLL
         for (int r = c + 1; r < 5; ++r) {
             const double v = ::fabs(A[r][c]);
             if (v > best) {
@@ -73,10 +79,10 @@ CCTAGB_HD inline bool solve5(double A[5][5], double b[5], double x[5])
             }
         }
         if (best == 0.0) return false;
-#pragma unroll
+CCTAGB_UNROLL
         for (int r = c + 1; r < 5; ++r)
             if (r == piv) {
-#pragma unroll
+CCTAGB_UNROLL
                 for (int k = 0; k < 5; ++k) {
                     const double t = A[r][k];
                     A[r][k] = A[c][k];
@@ -86,18 +92,18 @@ CCTAGB_HD inline bool solve5(double A[5][5], double b[5], double x[5])
                 b[r] = b[c];
                 b[c] = t;
             }
-#pragma unroll
+CCTAGB_UNROLL
         for (int r = c + 1; r < 5; ++r) {
             const double f = A[r][c] / A[c][c];
-#pragma unroll
+CCTAGB_UNROLL
             for (int k = c; k < 5; ++k) A[r][k] -= f * A[c][k];
             b[r] -= f * b[c];
         }
     }
-#pragma unroll
+CCTAGB_UNROLL
     for (int r = 4; r >= 0; --r) {
         double s = b[r];
-#pragma unroll
+CCTAGB_UNROLL
         for (int k = r + 1; k < 5; ++k) s -= A[r][k] * x[k];
         x[r] = s / A[r][r];
     }

@@ -21,6 +21,25 @@ namespace cctagb {
 using geo::Ellipse;
 using geo::Pt;
 
+void EdgeSet::index_points()
+{
+    const size_t nw = (size_t(W) * size_t(H) + 63) / 64;
+    ebits.assign(nw, 0);
+    erank.resize(nw);
+    long long last = -1;
+    for (int i = 0; i < E; ++i) {
+        const long long pos = (long long)(exy[i] >> 16) * W + (exy[i] & 0xffff);
+        if (pos <= last || pos >= (long long)W * H) throw std::runtime_error("edge points not in raster order");
+        last = pos;
+        ebits[size_t(pos) >> 6] |= uint64_t(1) << (pos & 63);
+    }
+    int32_t r = 0;
+    for (size_t k = 0; k < nw; ++k) {
+        erank[k] = r;
+        r += int32_t(__builtin_popcountll(ebits[k]));
+    }
+}
+
 void EdgeSet::reset_state()
 {
     processed_in.assign(E, 0);
@@ -332,7 +351,7 @@ void connected_point(std::vector<int>& pts, RunMarks& mk, EdgeSet& es, const Ell
         if (sx < 0 || sx >= es.W || sy < 0 || sy >= es.H) continue;
         const int e = es.at(sx, sy);
         if (e < 0) continue;
-        if (!geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e))) || mk.test(e)) continue;
+        if (mk.test(e) || !geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e)))) continue;
         const float ox = qIn.cx - float(es.x(e)), oy = qIn.cy - float(es.y(e));
         if (es.dx(e) * ox + es.dy(e) * oy < 0) {
             pts.push_back(e);

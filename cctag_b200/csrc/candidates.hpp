@@ -24,7 +24,12 @@ struct EdgeSet {
     const int32_t* voff = nullptr;
     const int32_t* vlist = nullptr;
     const float* flow = nullptr;
-    int32_t* idxmap = nullptr;  // W*H, -1 where no edge point (owned by the caller)
+    // Point index of a pixel: the points are in raster order, so a pixel's
+    // index is its rank among the edge pixels.  ebits holds the edge pixels
+    // (bit x + y W), erank the number of points before each 64-bit word: 1/16
+    // of the bytes of a dense W x H index map, so lookups stay in cache.
+    std::vector<uint64_t> ebits;
+    std::vector<int32_t> erank;
 
     std::vector<uint8_t> processed_in, processed_aux;
     std::vector<int32_t> n_segment_out;
@@ -41,7 +46,15 @@ struct EdgeSet {
     float dy(int i) const { return float(int16_t(grad[i] >> 16)); }
     float norm(int i) const { return std::sqrt(dx(i) * dx(i) + dy(i) * dy(i)); }
     int voters(int i) const { return voff[i + 1] - voff[i]; }
-    int at(int px, int py) const { return idxmap[size_t(py) * W + px]; }
+    int at(int px, int py) const
+    {
+        const size_t pos = size_t(py) * size_t(W) + size_t(px);
+        const uint64_t w = ebits[pos >> 6], bit = uint64_t(1) << (pos & 63);
+        return (w & bit) ? erank[pos >> 6] + __builtin_popcountll(w & (bit - 1)) : -1;
+    }
+    // Builds ebits / erank from exy[0, E); throws unless the points are in
+    // strict raster order.
+    void index_points();
     void reset_state();
 };
 

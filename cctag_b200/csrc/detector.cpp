@@ -24,17 +24,11 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, 
         for (const auto& row : kThreeCrownsBank) bank_.emplace_back(row, row + 5);
         upload_bank(bank_, d_bank_inv_);
     }
-    int w = max_w, h = max_h;
-    for (int l = 0; l < p.numberOfProcessedMultiresLayers; ++l) {
-        idxmaps_.emplace_back(size_t(w) * h, -1);
-        w /= 2;
-        h /= 2;
-    }
     CCTAGB_CUDA(cudaEventCreate(&ev_id0_));
     CCTAGB_CUDA(cudaEventCreate(&ev_id1_));
     ensure_ident_capacity(256);
-    hl_.resize(idxmaps_.size());
-    es_.resize(idxmaps_.size());
+    hl_.resize(size_t(p.numberOfProcessedMultiresLayers));
+    es_.resize(size_t(p.numberOfProcessedMultiresLayers));
     if (!pool_) pool_ = make_host_pool(p.hostThreads);
     std::vector<int> caps;
     for (int l = 0; l < p.numberOfProcessedMultiresLayers; ++l) caps.push_back(pipe_.level_capacity(l));
@@ -362,8 +356,7 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         e.voff = L.voff;
         e.vlist = L.vlist;
         e.flow = L.flow;
-        e.idxmap = idxmaps_[l].data();
-        for (int i = 0; i < L.E; ++i) e.idxmap[size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = i;
+        e.index_points();
         e.reset_state();
     };
     pool_->parallel_for(nl, fill_level);
@@ -414,10 +407,6 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
                 refit_apply(es[0], markers[size_t(rtIdx[size_t(k)])], flt[size_t(k)].data(), flt[size_t(k)].size());
             });
         }
-    }
-    for (int l = 0; l < nl; ++l) {
-        const HostLevel& L = hl[l];
-        for (int i = 0; i < L.E; ++i) idxmaps_[l][size_t(L.exy[i] >> 16) * L.W + (L.exy[i] & 0xffff)] = -1;
     }
     const auto t2 = clk::now();
 

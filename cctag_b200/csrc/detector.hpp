@@ -58,7 +58,6 @@ private:
     cctagb_params params_;
     Pipeline pipe_;
     std::vector<std::vector<float>> bank_;
-    std::vector<std::vector<int32_t>> idxmaps_;  // per level, -1 where no edge point
     std::vector<HostLevel> hl_;                  // per level, pinned downloads
     std::vector<EdgeSet> es_;                    // per level, candidate-stage state
     std::unique_ptr<LoopOneGpu> loop1_;          // loop 1 + outlier removal on the GPU

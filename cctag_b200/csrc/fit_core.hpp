@@ -1,0 +1,302 @@
+// Direct least-squares ellipse fit (Fitting.cpp:89-200 of the reference: the
+// Halir-Flusser reduction of Fitzgibbon's fit, eigen decomposition of the 3x3
+// reduced scatter matrix) written once for the host and the GPU.  The
+// reference solves the eigenproblem with Eigen; here the characteristic cubic
+// is solved in real arithmetic (Cardano with a portable cube root, or the
+// trigonometric form for three real roots), each root polished by Newton, and
+// the eigenvectors taken from cross products of (M - lambda I), in complex
+// arithmetic for a complex pair (the real part, as Eigen's eigenvectors().real()).
+// Only +, -, *, /, sqrt and the portable pmath functions are used.
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+#include <cstddef>
+
+#include "pmath.hpp"
+
+namespace cctagb {
+namespace geo {
+
+enum FitStatus {
+    kFitOk = 0,
+    kFitTooFewPoints,      // fewer than 5 points
+    kFitDependent,         // the points appear to be linearly dependent
+    kFitDegenerate,        // no eigenvector satisfies the ellipse constraint
+    kFitSingular1,         // to_ellipse: singularity 1
+    kFitSingular2,         // to_ellipse: singularity 2
+    kFitLineOrPoint,       // degenerate ellipse (line or point)
+};
+
+struct FitCplx {
+    double re, im;
+};
+
+CCTAGB_HD inline FitCplx cx_mul(FitCplx a, FitCplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+CCTAGB_HD inline FitCplx cx_sub(FitCplx a, FitCplx b) { return {a.re - b.re, a.im - b.im}; }
+CCTAGB_HD inline FitCplx cx_add(FitCplx a, FitCplx b) { return {a.re + b.re, a.im + b.im}; }
+CCTAGB_HD inline double cx_norm(FitCplx a) { return a.re * a.re + a.im * a.im; }
+CCTAGB_HD inline FitCplx cx_div(FitCplx a, FitCplx b)
+{
+    const double d = b.re * b.re + b.im * b.im;
+    return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+}
+
+// Real cube root (sign kept): Newton's iteration from an estimate of the right
+// binary magnitude, to convergence.
+CCTAGB_HD inline double cbrt_d(double y)
+{
+    if (y == 0.0 || !(y == y) || ::fabs(y) > DBL_MAX) return y;
+    const double a = ::fabs(y);
+    // estimate: 2^(floor(log2 a) / 3) by halving / doubling
+    double x = 1.0, t = a;
+    while (t >= 8.0) {
+        t *= 0.125;
+        x *= 2.0;
+    }
+    while (t < 1.0) {
+        t *= 8.0;
+        x *= 0.5;
+    }
+    for (int it = 0; it < 60; ++it) {
+        const double nx = x - (x * x * x - a) / (3.0 * x * x);
+        if (nx == x) break;
+        x = nx;
+    }
+    return y < 0.0 ? -x : x;
+}
+
+// Roots of x^3 + a x^2 + b x + c: three real, or one real and a complex pair.
+CCTAGB_HD inline void cubic_roots_real(double a, double b, double c, FitCplx r[3])
+{
+    const double p = b - a * a / 3.0;
+    const double q = 2.0 * a * a * a / 27.0 - a * b / 3.0 + c;
+    const double disc = q * q / 4.0 + p * p * p / 27.0;
+    const double shift = a / 3.0;
+    if (disc > 0.0) {
+        const double s = ::sqrt(disc);
+        const double u = cbrt_d(-q / 2.0 + s), v = cbrt_d(-q / 2.0 - s);
+        r[0] = {u + v - shift, 0.0};
+        const double re = -(u + v) / 2.0 - shift, im = (u - v) * 0.8660254037844386;
+        r[1] = {re, im};
+        r[2] = {re, -im};
+    } else if (p == 0.0) {
+        r[0] = r[1] = r[2] = {-shift, 0.0};
+    } else {
+        const double m = 2.0 * ::sqrt(-p / 3.0);
+        double arg = 3.0 * q / (p * m);
+        arg = arg > 1.0 ? 1.0 : (arg < -1.0 ? -1.0 : arg);
+        const double th = pm::atan2_d(::sqrt((1.0 - arg) * (1.0 + arg)), arg) / 3.0;
+        for (int k = 0; k < 3; ++k) r[k] = {m * pm::cos_d(th - 2.0943951023931957 * double(k)) - shift, 0.0};
+    }
+    // Newton polish on the original cubic (complex arithmetic for a complex root)
+    for (int k = 0; k < 3; ++k) {
+        for (int it = 0; it < 3; ++it) {
+            const FitCplx x = r[k];
+            const FitCplx f = cx_add(cx_mul(cx_add(cx_mul(cx_add(x, {a, 0.0}), x), {b, 0.0}), x), {c, 0.0});
+            const FitCplx df = cx_add(cx_mul(cx_add({3.0 * x.re, 3.0 * x.im}, {2.0 * a, 0.0}), x), {b, 0.0});
+            if (!(cx_norm(df) > 0.0)) break;
+            r[k] = cx_sub(x, cx_div(f, df));
+        }
+    }
+}
+
+// Unit eigenvector of M for eigenvalue lam: the largest cross product of two
+// rows of (M - lam I), phase fixed so that its largest component is real, real
+// part returned (Eigen's EigenSolver().eigenvectors().real() convention).
+CCTAGB_HD inline void eigvec_real(const double M[3][3], FitCplx lam, double out[3])
+{
+    FitCplx A[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) A[i][j] = {M[i][j] - (i == j ? lam.re : 0.0), i == j ? -lam.im : 0.0};
+    FitCplx best[3] = {{0, 0}, {0, 0}, {0, 0}};
+    double bn = -1.0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = i + 1; j < 3; ++j) {
+            const FitCplx c0 = cx_sub(cx_mul(A[i][1], A[j][2]), cx_mul(A[i][2], A[j][1]));
+            const FitCplx c1 = cx_sub(cx_mul(A[i][2], A[j][0]), cx_mul(A[i][0], A[j][2]));
+            const FitCplx c2 = cx_sub(cx_mul(A[i][0], A[j][1]), cx_mul(A[i][1], A[j][0]));
+            const double n = cx_norm(c0) + cx_norm(c1) + cx_norm(c2);
+            if (n > bn) {
+                bn = n;
+                best[0] = c0;
+                best[1] = c1;
+                best[2] = c2;
+            }
+        }
+    const double nrm = ::sqrt(bn > 0.0 ? bn : 0.0);
+    if (!(nrm > 0.0)) {
+        out[0] = out[1] = out[2] = 0.0;
+        return;
+    }
+    int kmax = 0;
+    for (int k = 1; k < 3; ++k)
+        if (cx_norm(best[k]) > cx_norm(best[kmax])) kmax = k;
+    const double am = ::sqrt(cx_norm(best[kmax]));
+    const FitCplx ph = am > 0.0 ? FitCplx{best[kmax].re / am, -best[kmax].im / am} : FitCplx{1.0, 0.0};
+    for (int k = 0; k < 3; ++k) out[k] = cx_mul(best[k], ph).re / nrm;
+}
+
+CCTAGB_HD inline bool inv3_d(const double a[3][3], double r[3][3])
+{
+    const double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
+    const double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
+    const double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
+    const double det = a[0][0] * c00 + a[0][1] * c01 + a[0][2] * c02;
+    double scale = 0.0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) scale = ::fmax(scale, ::fabs(a[i][j]));
+    if (det == 0.0 || !(::fabs(det) <= DBL_MAX) || ::fabs(det) <= 1e-14 * scale * scale * scale) return false;
+    const double id = 1.0 / det;
+    r[0][0] = c00 * id;
+    r[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) * id;
+    r[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) * id;
+    r[1][0] = c01 * id;
+    r[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) * id;
+    r[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) * id;
+    r[2][0] = c02 * id;
+    r[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) * id;
+    r[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) * id;
+    return true;
+}
+
+// Symmetric 2x2 eigen decomposition by Jacobi rotations, eigenvectors in columns.
+CCTAGB_HD inline void jacobi2(double A[2][2], double V[2][2], double d[2])
+{
+    V[0][0] = V[1][1] = 1.0;
+    V[0][1] = V[1][0] = 0.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        if (A[0][1] * A[0][1] < 1e-300) break;
+        if (::fabs(A[0][1]) < 1e-300) break;
+        const double theta = (A[1][1] - A[0][0]) / (2.0 * A[0][1]);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (::fabs(theta) + ::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / ::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < 2; ++k) {
+            const double akp = A[k][0], akq = A[k][1];
+            A[k][0] = c * akp - s * akq;
+            A[k][1] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 2; ++k) {
+            const double apk = A[0][k], aqk = A[1][k];
+            A[0][k] = c * apk - s * aqk;
+            A[1][k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < 2; ++k) {
+            const double vkp = V[k][0], vkq = V[k][1];
+            V[k][0] = c * vkp - s * vkq;
+            V[k][1] = s * vkp + c * vkq;
+        }
+    }
+    d[0] = A[0][0];
+    d[1] = A[1][1];
+}
+
+// The fit on n points (x[i], y[i]) read through `pt(i, x, y)`; on success the
+// ellipse parameters (center, semi axes, angle) as the reference's
+// Ellipse(center, r0, r1, angle) receives them.  The sums run in point order.
+template <class PointAt>
+CCTAGB_HD inline int fit_ellipse_core(PointAt pt, size_t n, float& ocx, float& ocy, float& oa, float& ob,
+                                      float& oangle)
+{
+    if (n < 5) return kFitTooFewPoints;
+    // Fitting.cpp:37-45 offset (mean), :47-71 scatter matrices
+    double ox = 0, oy = 0;
+    for (size_t i = 0; i < n; ++i) {
+        float x, y;
+        pt(i, x, y);
+        ox += x;
+        oy += y;
+    }
+    ox /= double(n);
+    oy /= double(n);
+    double S1[3][3] = {}, S2[3][3] = {}, S3[3][3] = {};
+    for (size_t i = 0; i < n; ++i) {
+        float xf, yf;
+        pt(i, xf, yf);
+        const double x = xf - ox, y = yf - oy;
+        const double q[3] = {x * x, x * y, y * y};
+        const double l[3] = {x, y, 1.0};
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                S1[r][c] += q[r] * q[c];
+                S2[r][c] += q[r] * l[c];
+                S3[r][c] += l[r] * l[c];
+            }
+    }
+    double S3i[3][3];
+    if (!inv3_d(S3, S3i)) return kFitDependent;
+    // T = -S3^-1 S2^T ; M = C1^-1 (S1 + S2 T), C1^-1 = [0 0 .5; 0 -1 0; .5 0 0]
+    double T[3][3], R[3][3], M[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += S3i[r][k] * S2[c][k];
+            T[r][c] = -s;
+        }
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            double s = S1[r][c];
+            for (int k = 0; k < 3; ++k) s += S2[r][k] * T[k][c];
+            R[r][c] = s;
+        }
+    for (int c = 0; c < 3; ++c) {
+        M[0][c] = 0.5 * R[2][c];
+        M[1][c] = -R[1][c];
+        M[2][c] = 0.5 * R[0][c];
+    }
+    // eigenvector with the smallest positive 4 v0 v2 - v1^2 (Fitting.cpp:102-128)
+    const double tr = M[0][0] + M[1][1] + M[2][2];
+    const double m2 = M[0][0] * M[1][1] - M[0][1] * M[1][0] + M[0][0] * M[2][2] - M[0][2] * M[2][0] +
+                      M[1][1] * M[2][2] - M[1][2] * M[2][1];
+    const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
+                       M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+    FitCplx lam[3];
+    cubic_roots_real(-tr, m2, -det, lam);
+    const double eps = double(FLT_EPSILON);
+    int imin = -1;
+    double minv = DBL_MAX;
+    double vecs[3][3];
+    for (int i = 0; i < 3; ++i) {
+        eigvec_real(M, lam[i], vecs[i]);
+        const double cond = 4 * vecs[i][0] * vecs[i][2] - vecs[i][1] * vecs[i][1];
+        if (cond > eps && cond < minv) {
+            imin = i;
+            minv = cond;
+        }
+    }
+    if (imin < 0) return kFitDegenerate;
+    double coef[6];
+    for (int k = 0; k < 3; ++k) coef[k] = vecs[imin][k];
+    for (int k = 0; k < 3; ++k) coef[3 + k] = T[k][0] * coef[0] + T[k][1] * coef[1] + T[k][2] * coef[2];
+    // to_ellipse, Fitting.cpp:131-169
+    double idet = coef[0] * coef[2] - coef[1] * coef[1] / 4;
+    idet = idet > eps ? 1.0 / idet : 0.0;
+    const double scale = ::sqrt(idet / 4);
+    if (scale < eps) return kFitSingular1;
+    for (double& v : coef) v *= scale;
+    const double aa = coef[0], bb = coef[1], cc = coef[2], dd = coef[3], ee = coef[4];
+    double ff = coef[5];
+    const double cxo = 2 * (-dd * cc + ee * bb / 2), cyo = 2 * (-aa * ee + dd * bb / 2);
+    ff += aa * cxo * cxo + bb * cxo * cyo + cc * cyo * cyo + dd * cxo + ee * cyo;
+    if (::fabs(ff) < eps) return kFitSingular2;
+    double S[2][2] = {{aa / -ff, bb / 2 / -ff}, {bb / 2 / -ff, cc / -ff}};
+    double V[2][2], d[2];
+    jacobi2(S, V, d);
+    // singular values in decreasing order, with their left singular vectors
+    const int i0 = ::fabs(d[0]) >= ::fabs(d[1]) ? 0 : 1, i1 = 1 - i0;
+    const double s0 = ::fabs(d[i0]), s1 = ::fabs(d[i1]);
+    const double u01 = V[0][i1], u11 = V[1][i1];
+    const double r0 = ::sqrt(1.0 / s0), r1 = ::sqrt(1.0 / s1);
+    const double angle = pm::kPi - pm::atan2_d(u01, u11);
+    if (!(r0 > 0) || !(r1 > 0) || !(r0 <= DBL_MAX) || !(r1 <= DBL_MAX)) return kFitLineOrPoint;
+    ocx = float(cxo + ox);
+    ocy = float(cyo + oy);
+    oa = float(r0);
+    ob = float(r1);
+    oangle = float(angle);
+    return kFitOk;
+}
+
+}  // namespace geo
+}  // namespace cctagb

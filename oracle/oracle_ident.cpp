@@ -582,7 +582,7 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
         pyramid_down(lvl[l - 1].data(), lw[l - 1], lh[l - 1], lvl[l].data(), lw[l], lh[l]);
     }
     struct LevelData {
-        std::vector<int32_t> exy, grad, before, after, voff, vlist, seeds, idxmap;
+        std::vector<int32_t> exy, grad, before, after, voff, vlist, seeds;
         std::vector<float> flow;
         int E = 0;
     };
@@ -622,8 +622,6 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
         L.vlist.assign(vl.begin(), vl.begin() + vo[E]);
         L.flow.assign(fl.begin(), fl.begin() + E);
         L.seeds.assign(ss.begin(), ss.begin() + ns);
-        L.idxmap.assign(size_t(w) * h, -1);
-        for (int i = 0; i < E; ++i) L.idxmap[size_t(y[i]) * w + x[i]] = i;
         cctagb::EdgeSet& S = es[l];
         S.W = w;
         S.H = h;
@@ -635,7 +633,7 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
         S.voff = L.voff.data();
         S.vlist = L.vlist.data();
         S.flow = L.flow.data();
-        S.idxmap = L.idxmap.data();
+        S.index_points();
         S.reset_state();
     }
     std::vector<cctagb::LevelJob> jobs(nl);
