@@ -42,10 +42,10 @@ void EdgeSet::index_points()
 
 void EdgeSet::reset_state()
 {
-    processed_in.assign(E, 0);
-    processed_aux.assign(E, 0);
-    n_segment_out.assign(E, -1);
-    link_stamp.assign(E, 0);
+    // segment labels stay -1 between frames (phase C restores the ones it set)
+    if (n_segment_out.size() < size_t(E)) n_segment_out.assign(size_t(E), -1);
+    processed_in.clear();
+    link_stamp.clear();
     link_token = 0;
 }
 
@@ -729,6 +729,9 @@ namespace {
 void link_level(EdgeSet& es, const std::vector<int32_t>& seeds, const cctagb_params& p, std::vector<Candidate>& loop1)
 {
     loop1.clear();
+    es.processed_in.assign(size_t(es.E), 0);
+    es.link_stamp.assign(size_t(es.E), 0u);
+    es.link_token = 0;
     if (seeds.empty()) return;
     const size_t nMax = size_t(std::max(es.H / 2, p.maximumNbSeeds));
     const size_t nProc = std::min(seeds.size(), nMax);
@@ -851,6 +854,12 @@ void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, cons
         for (size_t i = 0; i < st[l].keep.size(); ++i)
             if (st[l].keep[i]) flow_component_label(st[l].loop1[i], *jobs[l].es, nSegmentOut);
     }
+    // The labels are kept in the candidates (nLabel): put the per-point ones
+    // back to -1 for the next frame.
+    for (int l = 0; l < nl; ++l)
+        for (size_t i = 0; i < st[l].keep.size(); ++i)
+            if (st[l].keep[i])
+                for (int q : st[l].loop1[i].filtered) jobs[l].es->n_segment_out[q] = -1;
     // Phase D: ellipse growing, each run with its own point marks.
     pf(int(tasks.size()), [&](int t) {
         const int l = tasks[t].first, i = tasks[t].second;

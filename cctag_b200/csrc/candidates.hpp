@@ -31,7 +31,7 @@ struct EdgeSet {
     std::vector<uint64_t> ebits;
     std::vector<int32_t> erank;
 
-    std::vector<uint8_t> processed_in, processed_aux;
+    std::vector<uint8_t> processed_in;  // loop 1 on the host
     std::vector<int32_t> n_segment_out;
     std::vector<uint32_t> link_stamp;  // edge linking: point visited in call `link_token`
     uint32_t link_token = 0;

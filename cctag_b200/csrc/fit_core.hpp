@@ -209,20 +209,42 @@ CCTAGB_HD inline int fit_ellipse_core(PointAt pt, size_t n, float& ocx, float& o
     }
     ox /= double(n);
     oy /= double(n);
-    double S1[3][3] = {}, S2[3][3] = {}, S3[3][3] = {};
+    // S1 = sum q q^T, S2 = sum q l^T, S3 = sum l l^T with q = (x^2, xy, y^2) and
+    // l = (x, y, 1): the symmetric entries once (a product and its transpose
+    // are the same double), the products by 1 left out (exact).
+    double a00 = 0, a01 = 0, a02 = 0, a11 = 0, a12 = 0, a22 = 0;  // S1
+    double b00 = 0, b01 = 0, b02 = 0, b10 = 0, b11 = 0, b12 = 0, b20 = 0, b21 = 0, b22 = 0;  // S2
+    double c00 = 0, c01 = 0, c02 = 0, c11 = 0, c12 = 0, c22 = 0;  // S3
     for (size_t i = 0; i < n; ++i) {
         float xf, yf;
         pt(i, xf, yf);
         const double x = xf - ox, y = yf - oy;
-        const double q[3] = {x * x, x * y, y * y};
-        const double l[3] = {x, y, 1.0};
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c) {
-                S1[r][c] += q[r] * q[c];
-                S2[r][c] += q[r] * l[c];
-                S3[r][c] += l[r] * l[c];
-            }
+        const double q0 = x * x, q1 = x * y, q2 = y * y;
+        a00 += q0 * q0;
+        a01 += q0 * q1;
+        a02 += q0 * q2;
+        a11 += q1 * q1;
+        a12 += q1 * q2;
+        a22 += q2 * q2;
+        b00 += q0 * x;
+        b01 += q0 * y;
+        b02 += q0;
+        b10 += q1 * x;
+        b11 += q1 * y;
+        b12 += q1;
+        b20 += q2 * x;
+        b21 += q2 * y;
+        b22 += q2;
+        c00 += x * x;
+        c01 += x * y;
+        c02 += x;
+        c11 += y * y;
+        c12 += y;
+        c22 += 1.0;
     }
+    const double S1[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
+    const double S2[3][3] = {{b00, b01, b02}, {b10, b11, b12}, {b20, b21, b22}};
+    const double S3[3][3] = {{c00, c01, c02}, {c01, c11, c12}, {c02, c12, c22}};
     double S3i[3][3];
     if (!inv3_d(S3, S3i)) return kFitDependent;
     // T = -S3^-1 S2^T ; M = C1^-1 (S1 + S2 T), C1^-1 = [0 0 .5; 0 -1 0; .5 0 0]
