@@ -434,6 +434,7 @@ struct Candidate {
     int score = 0;
     size_t nLabel = 0;
     float averageReceivedVote = 0.f;
+    float flow = 0.f;  // flow length of the seed
 };
 
 float quality_of(size_t npts, const Ellipse& e) { return float(npts) / float(geo::rasterize_perimeter(e)); }
@@ -649,13 +650,13 @@ void flow_component_assembling(EdgeSet& es, float& quality, size_t ci, const std
     const Candidate& c = loop2[ci];
     int score = -1;
     size_t iMax = 0;
-    const float r = es.flow[c.seed] * 2.5f;
+    const float r = c.flow * 2.5f;
     const Ellipse area = Ellipse::from_params(float(es.x(c.seed)), float(es.y(c.seed)), r, r, 0.f);
     for (size_t i = 0; i < loop2.size(); ++i) {
         if (i == ci) continue;
         const Candidate& o = loop2[i];
         if (c.nLabel == o.nLabel) continue;
-        const float ratio = es.flow[o.seed] / es.flow[c.seed];
+        const float ratio = o.flow / c.flow;
         if (!(ratio > 0.666f && ratio < 1.5f)) continue;
         if (in_ellipse(area, float(es.x(o.seed)), float(es.y(o.seed)))) {
             if (o.score > score) {
@@ -742,6 +743,7 @@ void link_level(EdgeSet& es, const std::vector<int32_t>& seeds, const cctagb_par
         if (es.processed_in[seed]) continue;
         Candidate c;
         c.seed = seed;
+        c.flow = es.flow[seed];
         edge_linking(es, c.segment, seed, size_t(p.windowSizeOnInnerEllipticSegment), p.averageVoteMin);
         int nReceived = 0, nVoted = 0;
         for (int q : c.segment) {
@@ -815,6 +817,7 @@ void link_and_filter(std::vector<LevelJob>& jobs, const cctagb_params& p, const 
         for (size_t i = 0; i < st[l].keep.size(); ++i) {
             const Candidate& c = st[l].loop1[i];
             o.seed.push_back(c.seed);
+            o.flow.push_back(c.flow);
             o.score.push_back(c.score);
             o.keep.push_back(st[l].keep[i]);
             if (st[l].keep[i]) o.flt.insert(o.flt.end(), c.filtered.begin(), c.filtered.end());
@@ -840,6 +843,7 @@ void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, cons
             for (size_t i = 0; i < n2; ++i) {
                 Candidate& c = st[l].loop1[i];
                 c.seed = g.seed[i];
+                c.flow = g.flow[i];
                 c.score = g.score[i];
                 c.filtered.assign(g.flt.begin() + g.foff[i], g.flt.begin() + g.foff[i + 1]);
             }

@@ -96,6 +96,7 @@ using ParallelFor = std::function<void(int, const std::function<void(int)>&)>;
 // go on to the ellipse growing (keep), and their filtered children.
 struct LoopTwoIn {
     std::vector<int32_t> seed, score;
+    std::vector<float> flow;  // flow length of the seed (Vote.cpp:232)
     std::vector<uint8_t> keep;
     std::vector<int32_t> foff;  // candidate i: flt[foff[i], foff[i + 1]) (empty unless kept)
     std::vector<int32_t> flt;

@@ -41,6 +41,7 @@ struct LevelView {
     int seedcap;
     int32_t* seed_idx;       // seedcap
     int32_t* seed_key;       // seedcap: index of the voter that made it a seed
+    int32_t* seed_votes;     // seedcap: votes the seed received
     int32_t* bigq;           // cap: points whose voter list needs a block sort
     // launch geometry of the tiled kernels
     int nms_tx, nms_tiles;   // 30x30 output tiles

@@ -330,7 +330,7 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     const auto t1 = clk::now();
     std::vector<HostLevel>& hl = hl_;
     std::vector<EdgeSet>& es = es_;
-    pipe_.download_levels(hl);
+    pipe_.download_levels(hl, false);
     const auto t1d = clk::now();
     // Loop 1 and the outlier removal run on the GPU while the host indexes the
     // edge points.

@@ -810,6 +810,7 @@ __device__ __forceinline__ void finish_point(const LevelView& L, LevelCounters& 
         if (s < L.seedcap) {
             L.seed_idx[s] = c;
             L.seed_key[s] = list[vp.minVotes - 1];
+            L.seed_votes[s] = n;
         } else {
             atomicOr(&cnt.err, kErrSeedOverflow);
         }

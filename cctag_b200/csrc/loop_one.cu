@@ -726,6 +726,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
     const int32_t* segc = a.seg + size_t(t) * kSegSlot + kSegHalf;
     const int len = nf + 1 + nb;
     int32_t* children = a.children + size_t(blockIdx.x) * kChildCap;
+    if (threadIdx.x == 0) a.cflow[blockIdx.x] = L.flow[L.order[s]];
 
     __shared__ int sNchild;
 
@@ -1008,6 +1009,7 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
     args_.made = dev_alloc<int32_t>(allocs_, size_t(totalSlots_));
     const size_t metaN = size_t(nl_) * n2max_ * 4 + nl_ + 1;
     args_.meta = dev_alloc<int32_t>(allocs_, metaN);
+    args_.cflow = dev_alloc<float>(allocs_, size_t(nl_) * n2max_);
     args_.err = args_.meta + size_t(nl_) * n2max_ * 4 + nl_;
     args_.children = dev_alloc<int32_t>(allocs_, size_t(nl_) * n2max_ * kChildCap);
     d_order_ = dev_alloc<int32_t>(allocs_, size_t(totalSlots_));
@@ -1015,6 +1017,7 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
     d_packed_ = dev_alloc<int32_t>(allocs_, size_t(nl_) * n2max_ * kChildCap);
     CCTAGB_CUDA(cudaMallocHost(&h_order_, sizeof(int32_t) * std::max(totalSlots_, 1)));
     CCTAGB_CUDA(cudaMallocHost(&h_meta_, sizeof(int32_t) * metaN));
+    CCTAGB_CUDA(cudaMallocHost(&h_cflow_, sizeof(float) * size_t(nl_) * n2max_));
     h_flt_cap_ = size_t(nl_) * n2max_ * 512;
     CCTAGB_CUDA(cudaMallocHost(&h_flt_, sizeof(int32_t) * h_flt_cap_));
     args_.maxSlotsPerLevel = maxSlotsPerLevel_;
@@ -1052,6 +1055,7 @@ LoopOneGpu::~LoopOneGpu()
     if (h_rpacked_) cudaFreeHost(h_rpacked_);
     if (h_order_) cudaFreeHost(h_order_);
     if (h_meta_) cudaFreeHost(h_meta_);
+    if (h_cflow_) cudaFreeHost(h_cflow_);
     if (h_flt_) cudaFreeHost(h_flt_);
 }
 
@@ -1075,6 +1079,7 @@ void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const 
         L.vlist = v.vlist;
         L.bitmap = v.bitmap;
         L.idxmap = v.idxmap;
+        L.flow = v.flow;
         L.level = l;
         L.slot0 = l * maxSlotsPerLevel_;
         const size_t nMax = size_t(std::max(v.H / 2, p_.maximumNbSeeds));
@@ -1110,7 +1115,9 @@ void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const 
     k_pack<<<nl_ * n2max_, 256, 0, s>>>(args_, d_packed_);
     CCTAGB_CUDA(cudaGetLastError());
     CCTAGB_CUDA(cudaMemcpyAsync(h_meta_, args_.meta, sizeof(int32_t) * metaN, cudaMemcpyDeviceToHost, s));
-    d2h_ += 4LL * metaN;
+    CCTAGB_CUDA(cudaMemcpyAsync(h_cflow_, args_.cflow, sizeof(float) * size_t(nl_) * n2max_,
+                                cudaMemcpyDeviceToHost, s));
+    d2h_ += 4LL * metaN + 4LL * nl_ * n2max_;
 }
 
 void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
@@ -1150,6 +1157,7 @@ void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
         for (int r = 0; r < n2; ++r) {
             const int32_t* m = h_meta_ + (size_t(l) * n2max_ + r) * 4;
             o.seed.push_back(m[0]);
+            o.flow.push_back(h_cflow_[size_t(l) * n2max_ + r]);
             o.score.push_back(m[1]);
             o.keep.push_back(uint8_t(m[2]));
             if (m[2]) {

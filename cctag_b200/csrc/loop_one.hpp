@@ -33,6 +33,7 @@ struct LoopOneLevel {
     const int32_t* order;   // seeds in processing order, nProc of them
     int nProc, slot0;       // seed slots [slot0, slot0 + nProc)
     int4* rec;              // E point records (3 int4 each): xy, angle, voters, seed slot; 8 neighbours
+    const float* flow;      // E flow lengths (Vote.cpp:232)
     int level;
 };
 
@@ -52,6 +53,7 @@ struct LoopOneArgs {
     int32_t* made;          // nl * maxSlotsPerLevel: made candidates (seed slots), per level
     int maxSlotsPerLevel;
     int32_t* meta;          // nl * n2max * 4: seed slot, score, keep, filtered count; then nl: made count
+    float* cflow;           // nl * n2max: flow length of each loop-two candidate's seed
     int32_t* children;      // nl * n2max * kChildCap: children, then filtered in place
     int32_t* err;           // error bits
 };
@@ -121,6 +123,7 @@ private:
     int32_t* h_rpacked_ = nullptr;
     size_t h_rpacked_cap_ = 0;
     int32_t* h_meta_ = nullptr;    // pinned: meta + made counts + err
+    float* h_cflow_ = nullptr;     // pinned: seeds' flow lengths
     int32_t* h_flt_ = nullptr;     // pinned: filtered children, all candidates
     size_t h_flt_cap_ = 0;
     std::vector<void*> allocs_;

@@ -108,6 +108,7 @@ void Pipeline::alloc(int max_w, int max_h)
         v.seedcap = a.seedcap;
         v.seed_idx = dev_alloc<int32_t>(allocs_, a.seedcap);
         v.seed_key = dev_alloc<int32_t>(allocs_, a.seedcap);
+        v.seed_votes = dev_alloc<int32_t>(allocs_, a.seedcap);
         v.bigq = dev_alloc<int32_t>(allocs_, a.cap);
         auto pinned = [&](size_t n) {
             void* q = nullptr;
@@ -124,6 +125,7 @@ void Pipeline::alloc(int max_w, int max_h)
         a.h_flow = static_cast<float*>(pinned(a.cap));
         a.h_sidx = static_cast<int32_t*>(pinned(a.seedcap));
         a.h_skey = static_cast<int32_t*>(pinned(a.seedcap));
+        a.h_svotes = static_cast<int32_t*>(pinned(a.seedcap));
         w /= 2;
         h /= 2;
         if (w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "frame too small for the number of pyramid levels"};
@@ -276,7 +278,7 @@ void Pipeline::copy_planes(int l, uint8_t* src, int16_t* dx, int16_t* dy, uint8_
     }
 }
 
-void Pipeline::issue_level_download(int l)
+void Pipeline::issue_level_download(int l, bool voters)
 {
     const LevelView& v = lv_.l[l];
     const LevelCounters& c = h_cnt_[l];
@@ -290,15 +292,18 @@ void Pipeline::issue_level_download(int l)
     d2h(a.h_grad, v.grad, size_t(E) * 4);
     d2h(a.h_before, v.before, size_t(E) * 4);
     d2h(a.h_after, v.after, size_t(E) * 4);
-    d2h(a.h_voff, v.voff, size_t(E + 1) * 4);
-    d2h(a.h_vlist, v.vlist, size_t(c.V) * 4);
-    d2h(a.h_flow, v.flow, size_t(E) * 4);
+    if (voters) {
+        d2h(a.h_voff, v.voff, size_t(E + 1) * 4);
+        d2h(a.h_vlist, v.vlist, size_t(c.V) * 4);
+        d2h(a.h_flow, v.flow, size_t(E) * 4);
+    }
     d2h(a.h_sidx, v.seed_idx, size_t(S) * 4);
     d2h(a.h_skey, v.seed_key, size_t(S) * 4);
-    d2h_bytes_ += (long long)E * 24 + 4 + (long long)c.V * 4 + (long long)S * 8;
+    d2h(a.h_svotes, v.seed_votes, size_t(S) * 4);
+    d2h_bytes_ += (long long)E * 16 + (voters ? (long long)E * 8 + 4 + (long long)c.V * 4 : 0) + (long long)S * 12;
 }
 
-void Pipeline::finish_level_download(int l, HostLevel& out)
+void Pipeline::finish_level_download(int l, HostLevel& out, bool voters)
 {
     const LevelView& v = lv_.l[l];
     const LevelCounters& c = h_cnt_[l];
@@ -311,39 +316,48 @@ void Pipeline::finish_level_download(int l, HostLevel& out)
     out.grad = a.h_grad;
     out.before = a.h_before;
     out.after = a.h_after;
-    out.voff = a.h_voff;
-    out.vlist = a.h_vlist;
-    out.flow = a.h_flow;
+    out.voff = voters ? a.h_voff : nullptr;
+    out.vlist = voters ? a.h_vlist : nullptr;
+    out.flow = voters ? a.h_flow : nullptr;
     const int S = std::min(c.S, v.seedcap);
     // Seeds in the order vote() appends them (the voter that brings a point to
     // minVotes, Vote.cpp:236-241), then std::sort by votes received, as
     // Multiresolution.cpp:239-242 does (same comparator, same libstdc++ sort).
-    std::vector<std::pair<int32_t, int32_t>> ks(S);
-    for (int i = 0; i < S; ++i) ks[i] = {a.h_skey[i], a.h_sidx[i]};
-    std::sort(ks.begin(), ks.end());
-    out.seeds.resize(S);
-    for (int i = 0; i < S; ++i) out.seeds[i] = ks[i].second;
-    const int32_t* voff = a.h_voff;
+    // (The element sorted second carries its vote count along; std::sort's
+    // permutation depends only on the comparisons, so it is the one of
+    // sorting the indices with a vote-count comparator.)
+    struct SeedRec {
+        int32_t key, idx, votes;
+    };
+    std::vector<SeedRec> ks(static_cast<size_t>(S));
+    for (int i = 0; i < S; ++i) ks[size_t(i)] = {a.h_skey[i], a.h_sidx[i], a.h_svotes[i]};
+    std::sort(ks.begin(), ks.end(),
+              [](const SeedRec& x, const SeedRec& y) { return x.key < y.key || (x.key == y.key && x.idx < y.idx); });
+    std::vector<std::pair<int32_t, int32_t>> sv(static_cast<size_t>(S));
+    for (int i = 0; i < S; ++i) sv[size_t(i)] = {ks[size_t(i)].idx, ks[size_t(i)].votes};
     if (S > 1)
-        std::sort(out.seeds.begin(), out.seeds.end(), [voff](int32_t x, int32_t y) {
-            return (voff[x + 1] - voff[x]) > (voff[y + 1] - voff[y]);
-        });
+        std::sort(sv.begin(), sv.end(),
+                  [](const std::pair<int32_t, int32_t>& x, const std::pair<int32_t, int32_t>& y) {
+                      return x.second > y.second;
+                  });
+    out.seeds.resize(S);
+    for (int i = 0; i < S; ++i) out.seeds[size_t(i)] = sv[size_t(i)].first;
 }
 
 void Pipeline::download_level(int l, HostLevel& out)
 {
     if (l < 0 || l >= lv_.n) throw Error{CCTAGB_BAD_ARG, "level out of range"};
-    issue_level_download(l);
+    issue_level_download(l, true);
     CCTAGB_CUDA(cudaStreamSynchronize(stream_));
-    finish_level_download(l, out);
+    finish_level_download(l, out, true);
 }
 
-void Pipeline::download_levels(std::vector<HostLevel>& out)
+void Pipeline::download_levels(std::vector<HostLevel>& out, bool voters)
 {
     out.resize(lv_.n);
-    for (int l = 0; l < lv_.n; ++l) issue_level_download(l);
+    for (int l = 0; l < lv_.n; ++l) issue_level_download(l, voters);
     CCTAGB_CUDA(cudaStreamSynchronize(stream_));
-    for (int l = 0; l < lv_.n; ++l) finish_level_download(l, out[l]);
+    for (int l = 0; l < lv_.n; ++l) finish_level_download(l, out[l], voters);
 }
 
 }  // namespace cctagb

@@ -54,8 +54,11 @@ public:
     const LevelCounters& counters(int l) const { return h_cnt_[l]; }
     // Downloads one level's edge-point collection (after image_stage).
     void download_level(int l, HostLevel& out);
-    // Downloads every level with one synchronisation.
-    void download_levels(std::vector<HostLevel>& out);
+    // Downloads every level with one synchronisation; without `voters` the
+    // voter lists, their offsets and the flow lengths stay on the device
+    // (out.voff / vlist / flow null: the GPU's loop one is their only reader
+    // in a detection, and it hands the seeds' flow lengths over itself).
+    void download_levels(std::vector<HostLevel>& out, bool voters = true);
     float last_image_stage_ms() const { return last_ms_; }
     // Transfers and kernel launches since the last image_stage() began.
     long long h2d_bytes() const { return h2d_bytes_; }
@@ -96,10 +99,11 @@ private:
         float* h_flow = nullptr;
         int32_t* h_sidx = nullptr;
         int32_t* h_skey = nullptr;
+        int32_t* h_svotes = nullptr;
     } la_[kMaxLevels];
     std::vector<void*> host_allocs_;
-    void issue_level_download(int l);
-    void finish_level_download(int l, HostLevel& out);
+    void issue_level_download(int l, bool voters);
+    void finish_level_download(int l, HostLevel& out, bool voters);
     Levels lv_{};
     LevelCounters* d_cnt_ = nullptr;  // + scan partials
     LevelCounters* h_cnt_ = nullptr;  // pinned
