@@ -330,8 +330,7 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     const auto t1 = clk::now();
     std::vector<HostLevel>& hl = hl_;
     std::vector<EdgeSet>& es = es_;
-    pipe_.download_levels(hl, false);
-    const auto t1d = clk::now();
+    pipe_.download_seeds_then_points(hl);
     // Loop 1 and the outlier removal run on the GPU while the host indexes the
     // edge points.
     {
@@ -343,6 +342,8 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
         }
         loop1_->launch(pipe_.level_views(), E, seeds, pipe_.stream());
     }
+    pipe_.wait_points(hl);
+    const auto t1d = clk::now();
     auto fill_level = [&](int l) {
         EdgeSet& e = es[l];
         const HostLevel& L = hl[l];

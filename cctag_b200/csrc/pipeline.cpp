@@ -46,6 +46,7 @@ Pipeline::Pipeline(const cctagb_params& p, int max_w, int max_h, int max_batch) 
     vp_.low = int(std::floor(lo));
     vp_.high = int(std::floor(hi));
     CCTAGB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CCTAGB_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
     CCTAGB_CUDA(cudaEventCreate(&ev0_));
     CCTAGB_CUDA(cudaEventCreate(&ev1_));
     upload_constants(nullptr, 0, 0);
@@ -63,6 +64,7 @@ Pipeline::~Pipeline()
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
+    if (copy_stream_) cudaStreamDestroy(copy_stream_);
 }
 
 void Pipeline::alloc(int max_w, int max_h)
@@ -350,6 +352,46 @@ void Pipeline::download_level(int l, HostLevel& out)
     issue_level_download(l, true);
     CCTAGB_CUDA(cudaStreamSynchronize(stream_));
     finish_level_download(l, out, true);
+}
+
+void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
+{
+    out.resize(lv_.n);
+    for (int l = 0; l < lv_.n; ++l) {
+        const LevelView& v = lv_.l[l];
+        const LevelCounters& c = h_cnt_[l];
+        LevelAlloc& a = la_[l];
+        const int E = c.E;
+        const int S = std::min(c.S, v.seedcap);
+        auto d2h = [&](void* dst, const void* src, size_t bytes, cudaStream_t st) {
+            if (bytes) CCTAGB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+        };
+        d2h(a.h_sidx, v.seed_idx, size_t(S) * 4, stream_);
+        d2h(a.h_skey, v.seed_key, size_t(S) * 4, stream_);
+        d2h(a.h_svotes, v.seed_votes, size_t(S) * 4, stream_);
+        d2h(a.h_exy, v.exy, size_t(E) * 4, copy_stream_);
+        d2h(a.h_grad, v.grad, size_t(E) * 4, copy_stream_);
+        d2h(a.h_before, v.before, size_t(E) * 4, copy_stream_);
+        d2h(a.h_after, v.after, size_t(E) * 4, copy_stream_);
+        d2h_bytes_ += (long long)E * 16 + (long long)S * 12;
+    }
+    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    for (int l = 0; l < lv_.n; ++l) {
+        finish_level_download(l, out[l], false);
+        out[l].exy = out[l].grad = out[l].before = out[l].after = nullptr;  // until wait_points()
+    }
+}
+
+void Pipeline::wait_points(std::vector<HostLevel>& out)
+{
+    CCTAGB_CUDA(cudaStreamSynchronize(copy_stream_));
+    for (int l = 0; l < lv_.n; ++l) {
+        const LevelAlloc& a = la_[l];
+        out[l].exy = a.h_exy;
+        out[l].grad = a.h_grad;
+        out[l].before = a.h_before;
+        out[l].after = a.h_after;
+    }
 }
 
 void Pipeline::download_levels(std::vector<HostLevel>& out, bool voters)

@@ -59,6 +59,13 @@ public:
     // (out.voff / vlist / flow null: the GPU's loop one is their only reader
     // in a detection, and it hands the seeds' flow lengths over itself).
     void download_levels(std::vector<HostLevel>& out, bool voters = true);
+    // The detection's form: the seeds (sorted, returned once they are on the
+    // host) on the pipeline stream, and the edge points' positions,
+    // gradients and links on a copy stream, so that they travel while the
+    // GPU's loop one runs; wait_points() waits for them and sets
+    // out.exy / grad / before / after.
+    void download_seeds_then_points(std::vector<HostLevel>& out);
+    void wait_points(std::vector<HostLevel>& out);
     float last_image_stage_ms() const { return last_ms_; }
     // Transfers and kernel launches since the last image_stage() began.
     long long h2d_bytes() const { return h2d_bytes_; }
@@ -83,6 +90,7 @@ private:
     VoteParamsDev vp_{};
     int max_w_ = 0, max_h_ = 0;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t copy_stream_ = nullptr;  // edge-point downloads of a detection
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     std::vector<void*> allocs_;
     struct LevelAlloc {
