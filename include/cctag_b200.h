@@ -113,7 +113,7 @@ typedef struct cctagb_params {
     int gnIterations;                           /* 10: cost evaluations at most in REFINE_GAUSS_NEWTON */
     int gnCoarseRounds;                         /* 2: grid rounds before Gauss-Newton */
     int edgeCapacityDivisor;                    /* 4: edge capacity per level = W*H/divisor */
-    int hostThreads;                            /* 0: host threads of the candidate stage, 0 = one per physical core */
+    int hostThreads;                            /* 0: host threads of the candidate stage; 0 = one per physical core, less one per detection slot beyond the first */
 } cctagb_params;
 
 typedef struct cctagb_ellipse {
