@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
     const int nf = info[0], nb = info[1];
     const int32_t* segc = a.seg + size_t(t) * kSegSlot + kSegHalf;
     const int len = nf + 1 + nb;
-    int32_t* children = a.children + size_t(blockIdx.x) * kChildCap;
+    int32_t* children = a.children + size_t(blockIdx.x) * a.childCap;
     if (threadIdx.x == 0) a.cflow[blockIdx.x] = L.flow[L.order[s]];
 
     __shared__ int sNchild;
@@ -758,7 +758,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
                     if (__shfl_sync(kFull, incl, w + b - 1) <= o) w += b;
                 const int wbase = __shfl_sync(kFull, base, w & 31);
                 const int wexcl = __shfl_sync(kFull, excl, w & 31);
-                if (o < tot && nchild + o < kChildCap) children[nchild + o] = L.vlist[wbase + (o - wexcl)];
+                if (o < tot && nchild + o < a.childCap) children[nchild + o] = L.vlist[wbase + (o - wexcl)];
             }
             nchild += tot;
         }
@@ -766,7 +766,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(LoopOneArgs a)
     }
     __syncthreads();
     const int nchild = sNchild;
-    if (nchild > kChildCap) {
+    if (nchild > a.childCap) {
         if (tid == 0) {
             atomicOr(a.err, kLoopOneErrChildren);
             meta[0] = L.order[s];
@@ -858,11 +858,11 @@ __device__ int refit_row_takes(const LoopOneLevel& L, const geo::Mat3& Qi, const
 // from the center row down the image until one misses the hull, then from
 // the center row up), then the outlier removal without weights.
 __global__ void __launch_bounds__(kFilterThreads) k_refit(LoopOneLevel L, const RefitTask* tasks, int32_t* hullAll,
-                                                        int32_t* rowsAll, int rowStride, int32_t* counts)
+                                                        int hullCap, int32_t* rowsAll, int rowStride, int32_t* counts)
 {
     const int b = blockIdx.x, tid = threadIdx.x;
     const RefitTask& T = tasks[b];
-    int32_t* hull = hullAll + size_t(b) * kChildCap;
+    int32_t* hull = hullAll + size_t(b) * hullCap;
     int32_t* rowOff = rowsAll + size_t(b) * rowStride;
     int32_t* err = counts + gridDim.x;
     geo::Mat3 Qi, Qo;
@@ -910,7 +910,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_refit(LoopOneLevel L, const 
     }
     __syncthreads();
     const int total = sTotal;
-    if (total > kChildCap) {
+    if (total > hullCap) {
         if (tid == 0) {
             atomicOr(err, kLoopOneErrChildren);
             counts[b] = -1;
@@ -933,7 +933,8 @@ __global__ void __launch_bounds__(kFilterThreads) k_refit(LoopOneLevel L, const 
     if (tid == 0) counts[b] = nflt;
 }
 
-__global__ void __launch_bounds__(256) k_refit_pack(const int32_t* hullAll, const int32_t* counts, int32_t* packed)
+__global__ void __launch_bounds__(256) k_refit_pack(const int32_t* hullAll, int hullCap, const int32_t* counts,
+                                                    int32_t* packed)
 {
     const int b = blockIdx.x;
     __shared__ int sOff;
@@ -945,7 +946,7 @@ __global__ void __launch_bounds__(256) k_refit_pack(const int32_t* hullAll, cons
         sOff = off;
     }
     __syncthreads();
-    const int32_t* src = hullAll + size_t(b) * kChildCap;
+    const int32_t* src = hullAll + size_t(b) * hullCap;
     for (int i = threadIdx.x; i < n; i += blockDim.x) packed[sOff + i] = src[i];
 }
 
@@ -969,7 +970,7 @@ __global__ void __launch_bounds__(256) k_pack(LoopOneArgs a, int32_t* packed)
         sOff = off;
     }
     __syncthreads();
-    const int32_t* src = a.children + size_t(b) * kChildCap;
+    const int32_t* src = a.children + size_t(b) * a.childCap;
     for (int i = threadIdx.x; i < meta[3]; i += blockDim.x) packed[sOff + i] = src[i];
 }
 
@@ -1011,10 +1012,11 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
     args_.meta = dev_alloc<int32_t>(allocs_, metaN);
     args_.cflow = dev_alloc<float>(allocs_, size_t(nl_) * n2max_);
     args_.err = args_.meta + size_t(nl_) * n2max_ * 4 + nl_;
-    args_.children = dev_alloc<int32_t>(allocs_, size_t(nl_) * n2max_ * kChildCap);
+
     d_order_ = dev_alloc<int32_t>(allocs_, size_t(totalSlots_));
     d_rec_ = dev_alloc<int4>(allocs_, nrec * 3);
-    d_packed_ = dev_alloc<int32_t>(allocs_, size_t(nl_) * n2max_ * kChildCap);
+    for (int l = 0; l < nl_; ++l) maxCap_ = std::max(maxCap_, size_t(caps[size_t(l)]));
+    grow_children(std::min<size_t>(kChildCap, maxCap_ + 1));
     CCTAGB_CUDA(cudaMallocHost(&h_order_, sizeof(int32_t) * std::max(totalSlots_, 1)));
     CCTAGB_CUDA(cudaMallocHost(&h_meta_, sizeof(int32_t) * metaN));
     CCTAGB_CUDA(cudaMallocHost(&h_cflow_, sizeof(float) * size_t(nl_) * n2max_));
@@ -1047,6 +1049,8 @@ int LoopOneGpu::resolve_smem() const
 LoopOneGpu::~LoopOneGpu()
 {
     for (void* q : allocs_) cudaFree(q);
+    if (args_.children) cudaFree(args_.children);
+    if (d_packed_) cudaFree(d_packed_);
     for (void* q : {static_cast<void*>(d_rtask_), static_cast<void*>(d_rhull_), static_cast<void*>(d_rrows_),
                     static_cast<void*>(d_rcount_), static_cast<void*>(d_rpacked_)})
         if (q) cudaFree(q);
@@ -1097,11 +1101,31 @@ void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const 
         h2d_ += 4LL * L.nProc;
     }
     for (int l = nl_; l < kMaxLevels; ++l) cum[l] = cum[nl_ - 1];
+    cum_ = make_int4(cum[0], cum[1], cum[2], cum[3]);
+    run_kernels(s);
+}
+
+void LoopOneGpu::grow_children(size_t cap)
+{
+    if (args_.children) cudaFree(args_.children);
+    if (d_packed_) cudaFree(d_packed_);
+    args_.children = nullptr;
+    d_packed_ = nullptr;
+    args_.childCap = 0;
+    const size_t n = size_t(nl_) * n2max_ * cap;
+    CCTAGB_CUDA(cudaMalloc(&args_.children, sizeof(int32_t) * n));
+    CCTAGB_CUDA(cudaMalloc(&d_packed_, sizeof(int32_t) * n));
+    args_.childCap = int(cap);
+}
+
+void LoopOneGpu::run_kernels(cudaStream_t s)
+{
     const size_t metaN = size_t(nl_) * n2max_ * 4 + nl_ + 1;
     CCTAGB_CUDA(cudaMemsetAsync(args_.meta, 0, sizeof(int32_t) * metaN, s));
-    const int npts = cum[nl_ - 1];
+    const int cumv[kMaxLevels] = {cum_.x, cum_.y, cum_.z, cum_.w};
+    const int npts = nl_ > 0 ? cumv[nl_ - 1] : 0;
     if (npts > 0) {
-        k_point_records<<<(npts + 255) / 256, 256, 0, s>>>(args_, make_int4(cum[0], cum[1], cum[2], cum[3]));
+        k_point_records<<<(npts + 255) / 256, 256, 0, s>>>(args_, cum_);
         CCTAGB_CUDA(cudaGetLastError());
     }
     k_seed_slots<<<(totalSlots_ + 255) / 256, 256, 0, s>>>(args_);
@@ -1124,9 +1148,16 @@ void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
 {
     CCTAGB_CUDA(cudaStreamSynchronize(s));
     const int32_t* made = h_meta_ + size_t(nl_) * n2max_ * 4;
+    // a candidate with more voters than the room: more room, same kernels
+    // (no list can hold more points than its level)
+    while ((made[nl_] & kLoopOneErrChildren) && size_t(args_.childCap) <= maxCap_) {
+        grow_children(std::min(size_t(args_.childCap) * 4, maxCap_ + 1));
+        run_kernels(s);
+        CCTAGB_CUDA(cudaStreamSynchronize(s));
+    }
     const int err = made[nl_];
     if (err & kLoopOneErrChildren)
-        throw Error{CCTAGB_OVERFLOW_VOTERS, "a loop-two candidate gathers more than 32768 voters"};
+        throw Error{CCTAGB_OVERFLOW_VOTERS, "a loop-two candidate gathers more voters than its level has points"};
     if (err) throw Error{CCTAGB_INTERNAL, "loop one: error bits " + std::to_string(err)};
     size_t total = 0;
     for (int l = 0; l < nl_; ++l) {
@@ -1184,10 +1215,10 @@ void LoopOneGpu::ensure_refit_capacity(int n)
     refitCap_ = 0;
     const int cap = std::max(n, 64);
     CCTAGB_CUDA(cudaMalloc(&d_rtask_, sizeof(RefitTask) * cap));
-    CCTAGB_CUDA(cudaMalloc(&d_rhull_, sizeof(int32_t) * size_t(cap) * kChildCap));
+    CCTAGB_CUDA(cudaMalloc(&d_rhull_, sizeof(int32_t) * size_t(cap) * hullCap_));
     CCTAGB_CUDA(cudaMalloc(&d_rrows_, sizeof(int32_t) * size_t(cap) * (maxH_ + 2)));
     CCTAGB_CUDA(cudaMalloc(&d_rcount_, sizeof(int32_t) * (cap + 1)));
-    CCTAGB_CUDA(cudaMalloc(&d_rpacked_, sizeof(int32_t) * size_t(cap) * kChildCap));
+    CCTAGB_CUDA(cudaMalloc(&d_rpacked_, sizeof(int32_t) * size_t(cap) * hullCap_));
     CCTAGB_CUDA(cudaMallocHost(&h_rtask_, sizeof(RefitTask) * cap));
     CCTAGB_CUDA(cudaMallocHost(&h_rcount_, sizeof(int32_t) * (cap + 1)));
     refitCap_ = cap;
@@ -1205,16 +1236,28 @@ void LoopOneGpu::refit(const Levels& lv, const std::vector<RefitTask>& tasks, cu
     LoopOneLevel L = args_.lv[0];  // level-0 view of the frame loop one ran on
     std::copy(tasks.begin(), tasks.end(), h_rtask_);
     CCTAGB_CUDA(cudaMemcpyAsync(d_rtask_, h_rtask_, sizeof(RefitTask) * n, cudaMemcpyHostToDevice, s));
-    CCTAGB_CUDA(cudaMemsetAsync(d_rcount_ + n, 0, sizeof(int32_t), s));
-    k_refit<<<n, kFilterThreads, 0, s>>>(L, d_rtask_, d_rhull_, d_rrows_, maxH_ + 2, d_rcount_);
-    CCTAGB_CUDA(cudaGetLastError());
-    k_refit_pack<<<n, 256, 0, s>>>(d_rhull_, d_rcount_, d_rpacked_);
-    CCTAGB_CUDA(cudaGetLastError());
-    CCTAGB_CUDA(cudaMemcpyAsync(h_rcount_, d_rcount_, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
-    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    // the hull of one marker holds at most every level-0 point and a row twice
+    const size_t hullMax = size_t(L.E) + size_t(L.W) + 1;
+    for (;;) {
+        CCTAGB_CUDA(cudaMemsetAsync(d_rcount_ + n, 0, sizeof(int32_t), s));
+        k_refit<<<n, kFilterThreads, 0, s>>>(L, d_rtask_, d_rhull_, hullCap_, d_rrows_, maxH_ + 2, d_rcount_);
+        CCTAGB_CUDA(cudaGetLastError());
+        k_refit_pack<<<n, 256, 0, s>>>(d_rhull_, hullCap_, d_rcount_, d_rpacked_);
+        CCTAGB_CUDA(cudaGetLastError());
+        CCTAGB_CUDA(cudaMemcpyAsync(h_rcount_, d_rcount_, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+        CCTAGB_CUDA(cudaStreamSynchronize(s));
+        if (!(h_rcount_[n] & kLoopOneErrChildren) || size_t(hullCap_) > hullMax) break;
+        // more room for the hulls, same kernels
+        hullCap_ = int(std::min(size_t(hullCap_) * 4, hullMax + 1));
+        const int keep = refitCap_;
+        refitCap_ = 0;
+        ensure_refit_capacity(keep);
+        std::copy(tasks.begin(), tasks.end(), h_rtask_);
+        CCTAGB_CUDA(cudaMemcpyAsync(d_rtask_, h_rtask_, sizeof(RefitTask) * n, cudaMemcpyHostToDevice, s));
+    }
     const int err = h_rcount_[n];
     if (err & kLoopOneErrChildren)
-        throw Error{CCTAGB_OVERFLOW_VOTERS, "a re-fit hull holds more than 32768 edge points"};
+        throw Error{CCTAGB_OVERFLOW_VOTERS, "a re-fit hull holds more points than level 0"};
     if (err) throw Error{CCTAGB_INTERNAL, "refit: error bits " + std::to_string(err)};
     size_t total = 0;
     for (int i = 0; i < n; ++i) total += size_t(std::max(h_rcount_[i], 0));

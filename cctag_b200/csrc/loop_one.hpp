@@ -15,7 +15,7 @@ namespace cctagb {
 
 constexpr int kSegHalf = 100;                 // points per linking direction (maxLength)
 constexpr int kSegSlot = 2 * kSegHalf + 1;    // one segment: front, seed, back
-constexpr int kChildCap = 32768;              // children of one loop-two candidate
+constexpr int kChildCap = 32768;              // initial room for the children of one loop-two candidate
 constexpr int kLmedsMaxPts = 64;              // subsampled points of one outlier removal
 constexpr int kMarkCap = 2 * kSegSlot;        // later seeds one segment can mark processed
 constexpr int kFilterThreads = 128;           // LMedS draws evaluated at once per candidate
@@ -54,7 +54,8 @@ struct LoopOneArgs {
     int maxSlotsPerLevel;
     int32_t* meta;          // nl * n2max * 4: seed slot, score, keep, filtered count; then nl: made count
     float* cflow;           // nl * n2max: flow length of each loop-two candidate's seed
-    int32_t* children;      // nl * n2max * kChildCap: children, then filtered in place
+    int32_t* children;      // nl * n2max * childCap: children, then filtered in place
+    int childCap;           // room per candidate (grown and re-run on overflow)
     int32_t* err;           // error bits
 };
 
@@ -102,24 +103,29 @@ public:
 
 private:
     int resolve_smem() const;
+    void run_kernels(cudaStream_t s);    // the loop-one kernels and the count download
+    void grow_children(size_t cap);     // children / packed buffers for `cap` per candidate
     void ensure_refit_capacity(int n);
     cctagb_params p_;
     int nl_ = 0, n2max_ = 0, maxSlotsPerLevel_ = 0, totalSlots_ = 0;
     LoopOneArgs args_{};
+    int4 cum_{};                   // cumulative edge points of the levels (last launch)
     int32_t* d_order_ = nullptr;   // all levels' seed slots
     int32_t* h_order_ = nullptr;   // pinned staging
     int4* d_rec_ = nullptr;        // point records of all levels
     int32_t* d_packed_ = nullptr;  // kept candidates' filtered children
     std::vector<int> caps_;
     int maxH_ = 0;
+    size_t maxCap_ = 0;             // largest level capacity: no list can exceed it
     int refitCap_ = 0;
     RefitTask* d_rtask_ = nullptr;
     RefitTask* h_rtask_ = nullptr;
-    int32_t* d_rhull_ = nullptr;    // refitCap_ * kChildCap
+    int hullCap_ = kChildCap;       // room for one marker's hull points
+    int32_t* d_rhull_ = nullptr;    // refitCap_ * hullCap_
     int32_t* d_rrows_ = nullptr;    // refitCap_ * (maxH_ + 2) per-row offsets
     int32_t* d_rcount_ = nullptr;   // refitCap_ + 1 (last: error bits)
     int32_t* h_rcount_ = nullptr;
-    int32_t* d_rpacked_ = nullptr;  // refitCap_ * kChildCap
+    int32_t* d_rpacked_ = nullptr;  // refitCap_ * hullCap_
     int32_t* h_rpacked_ = nullptr;
     size_t h_rpacked_cap_ = 0;
     int32_t* h_meta_ = nullptr;    // pinned: meta + made counts + err
