@@ -349,26 +349,28 @@ __global__ void __launch_bounds__(kResolveThreads) k_link_resolve(LoopOneArgs a)
     }
 }
 
-// Value of rank k (NaN last) of the n order keys v[0], v[kFilterThreads],
-// v[2 kFilterThreads], ... (one thread's column of a shared array): the key
-// with fewer than k + 1 smaller keys and more than k smaller-or-equal ones.
-// Branch-free with a fixed trip count, so that the lanes of a warp selecting
-// at the same time do not diverge.
-__device__ uint32_t rank_key_strided(const uint32_t* v, int n, int k)
+// Ascending bitonic sort of 64 keys held by a warp, key `lane` in a and key
+// `lane + 32` in b.
+__device__ __forceinline__ void bitonic64(uint32_t& a, uint32_t& b, int lane)
 {
-    uint32_t res = 0;
-    for (int i = 0; i < n; ++i) {
-        const uint32_t ki = v[i * kFilterThreads];
-        int lt = 0, le = 0;
-#pragma unroll 8
-        for (int j = 0; j < n; ++j) {
-            const uint32_t kj = v[j * kFilterThreads];
-            lt += kj < ki;
-            le += kj <= ki;
+#pragma unroll
+    for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j == 32) {  // partners lane and lane + 32, both ascending at k = 64
+                const uint32_t lo = min(a, b), hi = max(a, b);
+                a = lo;
+                b = hi;
+            } else {
+                const uint32_t ya = __shfl_xor_sync(kFull, a, j), yb = __shfl_xor_sync(kFull, b, j);
+                const int ea = lane, eb = lane + 32;
+                const bool keepLowA = ((ea & j) == 0) == ((ea & k) == 0);
+                const bool keepLowB = ((eb & j) == 0) == ((eb & k) == 0);
+                a = keepLowA ? min(a, ya) : max(a, ya);
+                b = keepLowB ? min(b, yb) : max(b, yb);
+            }
         }
-        res = (lt <= k && k < le) ? ki : res;
     }
-    return res;
 }
 
 __device__ __forceinline__ float key_value(uint32_t k)
@@ -590,32 +592,52 @@ __device__ int lmeds_outliers(const LoopOneLevel& L, int32_t* idx, int n, bool w
         const int nd = sNd;
         if (nd == 0) break;
         const float SmStart = sSm;
-        if (tid < nd) {
-            int perm[5];
-            for (int i = 0; i < 5; ++i) perm[i] = perms[tid][i];
-            geo::Mat3 Q;
-            int kind = cand::lmeds_conic(pts, perm, Q);
-            float S = 0.f;
-            if (kind == kDrawUsable) {
-                int below = 0;
+        {
+            const bool valid = tid < nd;
+            geo::Mat3 Q = geo::Mat3::zero();
+            int kind = kDrawNotReal;
+            bool needS = false;
+            if (valid) {
+                int perm[5];
+                for (int i = 0; i < 5; ++i) perm[i] = perms[tid][i];
+                kind = cand::lmeds_conic(pts, perm, Q);
+                if (kind == kDrawUsable) {
+                    int below = 0;
 #pragma unroll 4
-                for (int i = 0; i < np; ++i) below += dist_below(Q, pts[i].x, pts[i].y, weighted, wts[i], SmStart);
-                // no median below the best so far: it cannot improve (Sm only decreases)
-                if (below >= np / 2 + 1) {
-                    uint32_t* keys = keysAll + tid;  // column tid of a [kLmedsMaxPts][kFilterThreads] array
-                    for (int i = 0; i < np; ++i) {
-                        float d = geo::dist_point_ellipse(Q, pts[i].x, pts[i].y);
-                        if (weighted) d *= wts[i];
-                        keys[i * kFilterThreads] = geo::order_key(d);
+                    for (int i = 0; i < np; ++i) below += dist_below(Q, pts[i].x, pts[i].y, weighted, wts[i], SmStart);
+                    // no median below the best so far: it cannot improve (Sm only decreases)
+                    if (below >= np / 2 + 1) {
+                        needS = true;
+                        uint32_t* keys = keysAll + tid;  // column tid of a [kLmedsMaxPts][kFilterThreads] array
+                        for (int i = 0; i < np; ++i) {
+                            float d = geo::dist_point_ellipse(Q, pts[i].x, pts[i].y);
+                            if (weighted) d *= wts[i];
+                            keys[i * kFilterThreads] = geo::order_key(d);
+                        }
+                    } else {
+                        kind = kDrawNoGain;
                     }
-                    S = key_value(rank_key_strided(keys, np, np / 2));
-                } else {
-                    kind = kDrawNoGain;
                 }
             }
-            kinds[tid] = kind;
-            svals[tid] = S;
-            for (int k = 0; k < 9; ++k) sQ[tid][k] = Q.m[k / 3][k % 3];
+            // medians (rank np / 2, NaN last) of the draws that need one, a draw at
+            // a time by the whole warp: a 64-key bitonic sort of its column
+            __syncwarp();
+            float S = 0.f;
+            for (unsigned m = __ballot_sync(kFull, needS); m; m &= m - 1) {
+                const int src = __ffs(m) - 1;
+                const uint32_t* col = keysAll + (warp * 32 + src);
+                uint32_t ka = lane < np ? col[lane * kFilterThreads] : 0xffffffffu;
+                uint32_t kb = lane + 32 < np ? col[(lane + 32) * kFilterThreads] : 0xffffffffu;
+                bitonic64(ka, kb, lane);
+                const int r = np / 2;
+                const uint32_t v = __shfl_sync(kFull, r < 32 ? ka : kb, r & 31);
+                if (lane == src) S = key_value(v);
+            }
+            if (valid) {
+                kinds[tid] = kind;
+                svals[tid] = S;
+                for (int k = 0; k < 9; ++k) sQ[tid][k] = Q.m[k / 3][k % 3];
+            }
         }
         __syncthreads();
         // Acceptance in draw order (Vote.cpp:478-545) by warp 0, 32 draws at a
