@@ -863,16 +863,27 @@ __device__ int refit_row_takes(const LoopOneLevel& L, const geo::Mat3& Qi, const
     int nr, xb[2], xe[2];
     if (!refit_row(Qi, Qo, L.W, y, nr, xb, xe)) return 0;
     int n = 0;
-    for (int r = 0; r < nr; ++r)
-        for (int x = xb[r]; x <= xe[r]; ++x) {
-            const int e = at(L, x, y);
-            if (e < 0) continue;
-            const float cx = inCx - float(px_(L, e)), cy = inCy - float(py_(L, e));
-            if (gdx(L, e) * cx + gdy(L, e) * cy < 0) {
-                if (out) out[n] = e;
-                ++n;
+    // the edge pixels of each x range, a bitmap word at a time, in x order
+    const uint32_t* row = L.bitmap + size_t(y) * L.WW;
+    for (int r = 0; r < nr; ++r) {
+        if (xb[r] > xe[r]) continue;
+        for (int wx = xb[r] >> 5; wx <= xe[r] >> 5; ++wx) {
+            const int lo = wx << 5;
+            uint32_t w = row[wx];
+            if (xb[r] > lo) w &= 0xffffffffu << (xb[r] - lo);
+            if (xe[r] < lo + 31) w &= 0xffffffffu >> (31 - (xe[r] - lo));
+            while (w) {
+                const int x = lo + __ffs(w) - 1;
+                w &= w - 1;
+                const int e = L.idxmap[size_t(y) * L.W + x];
+                const float cx = inCx - float(px_(L, e)), cy = inCy - float(py_(L, e));
+                if (gdx(L, e) * cx + gdy(L, e) * cy < 0) {
+                    if (out) out[n] = e;
+                    ++n;
+                }
             }
         }
+    }
     return n;
 }
 
