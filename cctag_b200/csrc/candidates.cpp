@@ -535,6 +535,12 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
         stamp[size_t(q)] = token;
         return true;
     };
+    for (auto& v : pts) v.reserve(v.size() + fc.size());
+    // in_ellipse's transformed center, the same for every point
+    const geo::Mat3& Q = oe.Q;
+    const float qc0 = Q.m[0][0] * oe.cx + Q.m[0][1] * oe.cy + Q.m[0][2];
+    const float qc1 = Q.m[1][0] * oe.cx + Q.m[1][1] * oe.cy + Q.m[1][2];
+    const float qc2 = Q.m[2][0] * oe.cx + Q.m[2][1] * oe.cy + Q.m[2][2];
     size_t nGradientOut = 0, nAdded = 0;
     for (int p0 : fc) {
         int dir = -1;
@@ -548,15 +554,19 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
                 throw std::out_of_range("EdgePointCollection: missing link");
             }
             if (first_visit(p)) {
-                const float ng = std::sqrt(es.dx(p) * es.dx(p) + es.dy(p) * es.dy(p));
-                const float gx = es.dx(p) / ng, gy = es.dy(p) / ng;
-                float tx = oe.cx - float(es.x(p)), ty = oe.cy - float(es.y(p));
-                const float dc = std::sqrt(tx * tx + ty * ty);
-                tx /= dc;
-                ty /= dc;
                 const DirPoint q{float(es.x(p)), float(es.y(p)), es.dx(p), es.dy(p)};
-                if (in_ellipse(oe, q.x, q.y) && same_side(ox, oy, q.x, q.y, line)) {
-                    if (float(-dir) * (gx * tx + gy * ty) < -0.5f && j >= numCircles - 2) ++nGradientOut;
+                const bool inside = geo::qform(Q, q.x, q.y) * (q.x * qc0 + q.y * qc1 + qc2) > 0;
+                if (inside && same_side(ox, oy, q.x, q.y, line)) {
+                    if (j >= numCircles - 2) {
+                        // gradient against the direction to the center (the last two circles only)
+                        const float ng = std::sqrt(q.dx * q.dx + q.dy * q.dy);
+                        const float gx = q.dx / ng, gy = q.dy / ng;
+                        float tx = oe.cx - q.x, ty = oe.cy - q.y;
+                        const float dc = std::sqrt(tx * tx + ty * ty);
+                        tx /= dc;
+                        ty /= dc;
+                        if (float(-dir) * (gx * tx + gy * ty) < -0.5f) ++nGradientOut;
+                    }
                     pts[numCircles - j - 1].push_back(q);
                     if (j >= numCircles - 2) ++nAdded;
                 } else {
