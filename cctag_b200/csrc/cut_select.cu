@@ -56,19 +56,39 @@ __device__ bool cut_stats(const uint8_t* img, int W, int H, float sx, float sy, 
     const float stepX = fd(fs(ex, xs), den), stepY = fd(fs(ey, ys), den);
     float x = xs, y = ys;
     float mean = 0.f, var = 0.f;
-    for (int i = 0; i < n; ++i) {
-        if (!(x >= 1.f && x < float(W - 1) && y >= 1.f && y < float(H - 1))) return false;
-        const float v = bilinear_host(img, W, x, y);
-        if (sig) sig[i] = v;
-        // MeanVar::add
-        const int c = i + 1;
-        mean = fd(fa(fm(mean, float(c - 1)), v), float(c));
-        if (c > 1) {
-            const float t = fs(v, mean);
-            var = fa(fd(fm(var, float(c - 1)), float(c)), fd(fm(t, t), float(c - 1)));
-        }
-        x = fa(x, stepX);
-        y = fa(y, stepY);
+    // 8 samples at a time: their positions (the same running sums) and bounds
+    // first, then the 8 bilinear reads, which overlap, then the running mean
+    // and variance in sample order
+    constexpr int kGroup = 8;
+    for (int i0 = 0; i0 < n; i0 += kGroup) {
+        float gx[kGroup], gy[kGroup], gv[kGroup];
+        bool inside = true;
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+            if (i0 + k < n) {
+                gx[k] = x;
+                gy[k] = y;
+                inside = inside && (x >= 1.f && x < float(W - 1) && y >= 1.f && y < float(H - 1));
+                x = fa(x, stepX);
+                y = fa(y, stepY);
+            }
+        if (!inside) return false;
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+            if (i0 + k < n) gv[k] = bilinear_host(img, W, gx[k], gy[k]);
+#pragma unroll
+        for (int k = 0; k < kGroup; ++k)
+            if (i0 + k < n) {
+                const float v = gv[k];
+                if (sig) sig[i0 + k] = v;
+                // MeanVar::add
+                const int c = i0 + k + 1;
+                mean = fd(fa(fm(mean, float(c - 1)), v), float(c));
+                if (c > 1) {
+                    const float t = fs(v, mean);
+                    var = fa(fd(fm(var, float(c - 1)), float(c)), fd(fm(t, t), float(c - 1)));
+                }
+            }
     }
     *var_out = var;
     return true;
