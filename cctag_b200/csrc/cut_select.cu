@@ -19,6 +19,8 @@ namespace cctagb {
 namespace {
 
 constexpr int kCutThreads = kMaxOuterPoints;
+constexpr int kCutWarps = kCutThreads / 32;
+static_assert(kCutThreads % 32 == 0, "whole warps");
 
 __device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
@@ -157,10 +159,15 @@ __global__ void __launch_bounds__(kCutThreads) k_cut_select(const uint8_t* __res
                                                             const DirPoint* __restrict__ pts, IdentTask* tasks,
                                                             int* status, CutSelectParams cp)
 {
-    __shared__ uint8_t s_ok[kCutThreads], s_ref[kCutThreads];
-    __shared__ float s_var[kCutThreads], s_x[kCutThreads], s_y[kCutThreads];
+    __shared__ float s_x[kCutThreads], s_y[kCutThreads], s_wmax[kCutWarps];
+    __shared__ int s_keep[kCutThreads], s_wcnt[kCutWarps];
     const CutSelectIn in = ins[blockIdx.x];
     const int i = threadIdx.x;
+    IdentTask& T = tasks[blockIdx.x];
+    if (in.count < 5) {  // the host decided TOO_FEW_OUTER_POINTS
+        if (i == 0) T.ncuts = 0;
+        return;
+    }
     bool ok = false, ref = false;
     float var = 0.f, sx = 0.f, sy = 0.f;
     if (i < in.count) {
@@ -179,50 +186,57 @@ __global__ void __launch_bounds__(kCutThreads) k_cut_select(const uint8_t* __res
             ref = refine_stop(sx, sy, op.dx, op.dy, img, W, H, in.scale, cp.nRefine);
         }
     }
-    s_ok[i] = ok;
-    s_ref[i] = ref;
-    s_var[i] = var;
     s_x[i] = sx;
     s_y[i] = sy;
-    __syncthreads();
-    if (i != 0) return;
-    IdentTask& T = tasks[blockIdx.x];
-    if (in.count < 5) {  // the host decided TOO_FEW_OUTER_POINTS
-        T.ncuts = 0;
-        return;
-    }
-    // selectCutCheapUniform over the collected (in-image) cuts, in order
-    int nOk = 0;
-    float varMax = 0.f;
-    for (int j = 0; j < in.count; ++j)
-        if (s_ok[j]) {
-            if (nOk == 0 || s_var[j] > varMax) varMax = s_var[j];
-            ++nOk;
-        }
+    // selectCutCheapUniform over the collected (in-image) cuts, in order,
+    // block-parallel.  The variances are finite and >= +0 (means and squares
+    // of finite samples), so the largest one has a single bit pattern and any
+    // reduction order gives the serial first-max.
+    const int lane = i & 31, warp = i >> 5;
+    float vm = ok ? var : -1.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vm = fmaxf(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+    if (lane == 0) s_wmax[warp] = vm;
+    const int nOk = __syncthreads_count(ok);
     if (nOk == 0) {
-        T.ncuts = 0;
-        status[blockIdx.x] = CCTAGB_NO_COLLECTED_CUTS;
+        if (i == 0) {
+            T.ncuts = 0;
+            status[blockIdx.x] = CCTAGB_NO_COLLECTED_CUTS;
+        }
         return;
     }
-    int keep[kCutThreads];
-    int nKeep = 0;
-    for (int j = 0; j < in.count; ++j)
-        if (s_ok[j] && s_ref[j] && fd(s_var[j], varMax) > 0.5f) keep[nKeep++] = j;
+    float varMax = s_wmax[0];
+#pragma unroll
+    for (int w = 1; w < kCutWarps; ++w) varMax = fmaxf(varMax, s_wmax[w]);
+    // the kept cuts, compacted in point order: rank = kept cuts before i
+    const bool kp = ok && ref && fd(var, varMax) > 0.5f;
+    const unsigned kb = __ballot_sync(0xffffffffu, kp);
+    if (lane == 0) s_wcnt[warp] = __popc(kb);
+    __syncthreads();
+    int rank = __popc(kb & ((1u << lane) - 1u)), nKeep = 0;
+#pragma unroll
+    for (int w = 0; w < kCutWarps; ++w) {
+        rank += w < warp ? s_wcnt[w] : 0;
+        nKeep += s_wcnt[w];
+    }
+    if (kp) s_keep[rank] = i;
+    __syncthreads();
+    // The serial loop's k-th pick is keep[int(k * step)] while k < selectSize
+    // and that index < nKeep; the index is non-decreasing in k, so the picks
+    // are the prefix of k where both hold, one thread per k.
     const int selectSize = min(cp.maxSelect, nOk);
     const float step = fmaxf(1.f, fd(float(nKeep), float(selectSize)));
-    int nsel = 0;
-    for (int k = 0;; ++k) {
-        const int j = int(fm(float(k), step));
-        if (j < nKeep && nsel < selectSize) {
-            T.stop[nsel][0] = s_x[keep[j]];
-            T.stop[nsel][1] = s_y[keep[j]];
-            ++nsel;
-        } else {
-            break;
-        }
+    const int j = int(fm(float(i), step));
+    const bool pick = i < selectSize && j < nKeep;
+    if (pick) {
+        T.stop[i][0] = s_x[s_keep[j]];
+        T.stop[i][1] = s_y[s_keep[j]];
     }
-    T.ncuts = nsel;
-    status[blockIdx.x] = nsel == 0 ? CCTAGB_NO_SELECTED_CUTS : CCTAGB_ID_RELIABLE;
+    const int nsel = __syncthreads_count(pick);
+    if (i == 0) {
+        T.ncuts = nsel;
+        status[blockIdx.x] = nsel == 0 ? CCTAGB_NO_SELECTED_CUTS : CCTAGB_ID_RELIABLE;
+    }
 }
 
 void launch_cut_select(const uint8_t* d_img, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
