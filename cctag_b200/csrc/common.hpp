@@ -107,6 +107,18 @@ void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t 
                         cudaEvent_t* ev = nullptr);
 void launch_canny_only(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s);
 void launch_gate(cudaStream_t s, int us);
+
+// Device arrays of 32-bit words copied back to back into one buffer, so that
+// a download is one copy instead of one per array (seeds and edge points of
+// every level: 7 arrays per level).
+constexpr int kMaxPackSegs = 7 * kMaxLevels;
+struct PackSegs {
+    const int32_t* src[kMaxPackSegs];
+    long long off[kMaxPackSegs + 1];  // word offsets in dst; off[n] = total
+    int n;
+};
+// Returns the number of kernels launched (0 when every segment is empty).
+int launch_pack(const PackSegs& p, int32_t* dst, cudaStream_t s);
 void launch_edge_level(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, uint8_t* edges_out,
                        int32_t* status_out);
 

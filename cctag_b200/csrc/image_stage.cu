@@ -12,6 +12,7 @@
 //  * edge order: raster order, Canny.cpp:15-31
 //  * walk: Bresenham.cpp:18-209, vote: Vote.cpp:58-247 (no FMA contraction,
 //    IEEE division and square root, same accumulation order)
+#include <algorithm>
 #include <cstdint>
 
 #include "common.hpp"
@@ -978,6 +979,28 @@ __global__ void k_gate(int us)
 }
 
 void launch_gate(cudaStream_t s, int us) { k_gate<<<1, 1, 0, s>>>(us); }
+
+// Segment blockIdx.y of p to dst[p.off[y] ...], grid-stride over its words.
+__global__ void __launch_bounds__(256) k_pack_words(PackSegs p, int32_t* __restrict__ dst)
+{
+    const int g = blockIdx.y;
+    const long long o = p.off[g], n = p.off[g + 1] - o;
+    const int32_t* __restrict__ src = p.src[g];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[o + i] = __ldg(src + i);
+}
+
+int launch_pack(const PackSegs& p, int32_t* dst, cudaStream_t s)
+{
+    if (p.n <= 0 || p.n > kMaxPackSegs) return 0;
+    long long longest = 0;
+    for (int g = 0; g < p.n; ++g) longest = std::max(longest, p.off[g + 1] - p.off[g]);
+    if (longest == 0) return 0;
+    const int bx = int(std::min<long long>((longest + 1023) / 1024, 148));
+    k_pack_words<<<dim3(bx, p.n), 256, 0, s>>>(p, dst);
+    CCTAGB_CUDA(cudaGetLastError());
+    return 1;
+}
 
 static void launch_edges(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, int write_derivs,
                          cudaEvent_t* ev)

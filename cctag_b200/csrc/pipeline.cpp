@@ -45,10 +45,19 @@ Pipeline::Pipeline(const cctagb_params& p, int max_w, int max_h, int max_batch) 
     if (lo > hi) std::swap(lo, hi);
     vp_.low = int(std::floor(lo));
     vp_.high = int(std::floor(hi));
-    CCTAGB_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    CCTAGB_CUDA(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    // The image stage (full-GPU, bandwidth-bound grids) runs at the lowest
+    // stream priority and the later latency-bound kernels of a detection at
+    // the highest, so that with several detections in flight a frame past its
+    // image stage gets SMs ahead of the next frame's image stage.
+    int least = 0, greatest = 0;
+    CCTAGB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CCTAGB_CUDA(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, greatest));
+    CCTAGB_CUDA(cudaStreamCreateWithPriority(&stage_stream_, cudaStreamNonBlocking, least));
+    CCTAGB_CUDA(cudaStreamCreateWithPriority(&copy_stream_, cudaStreamNonBlocking, greatest));
     CCTAGB_CUDA(cudaEventCreate(&ev0_));
     CCTAGB_CUDA(cudaEventCreate(&ev1_));
+    CCTAGB_CUDA(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming));
+    CCTAGB_CUDA(cudaEventCreateWithFlags(&ev_pack_, cudaEventDisableTiming));
     upload_constants(nullptr, 0, 0);
     alloc(max_w, max_h);
 }
@@ -63,7 +72,10 @@ Pipeline::~Pipeline()
     if (h_cnt_) cudaFreeHost(h_cnt_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
+    if (ev_in_) cudaEventDestroy(ev_in_);
+    if (ev_pack_) cudaEventDestroy(ev_pack_);
     if (stream_) cudaStreamDestroy(stream_);
+    if (stage_stream_) cudaStreamDestroy(stage_stream_);
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
 }
 
@@ -132,6 +144,12 @@ void Pipeline::alloc(int max_w, int max_h)
         h /= 2;
         if (w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "frame too small for the number of pyramid levels"};
     }
+    // Compact download staging: seeds and edge points of every level.
+    pack_words_ = 0;
+    for (int l = 0; l < nl; ++l) pack_words_ += 3LL * la_[l].seedcap + 4LL * la_[l].cap;
+    d_pack_ = dev_alloc<int32_t>(allocs_, size_t(pack_words_));
+    CCTAGB_CUDA(cudaMallocHost(&h_pack_, size_t(pack_words_) * 4));
+    host_allocs_.push_back(h_pack_);
     // Counters followed by the partial sums of the voter-count scan.
     const size_t cnt_bytes = sizeof(LevelCounters) * kMaxLevels + sizeof(int32_t) * kMaxLevels * 148;
     d_cnt_ = reinterpret_cast<LevelCounters*>(dev_alloc<uint8_t>(allocs_, cnt_bytes));
@@ -168,8 +186,12 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
 {
     if (!gray || w < 1 || h < 1 || pitch < size_t(w)) throw Error{CCTAGB_BAD_ARG, "bad frame arguments"};
     set_views(w, h, params_.numberOfProcessedMultiresLayers);
+    // the stage stream starts after all earlier work of the pipeline stream
+    cudaStream_t st = stage_stream_;
+    CCTAGB_CUDA(cudaEventRecord(ev_in_, stream_));
+    CCTAGB_CUDA(cudaStreamWaitEvent(st, ev_in_, 0));
     CCTAGB_CUDA(cudaMemcpy2DAsync(lv_.l[0].src, w, gray, pitch, w, h,
-                                  is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+                                  is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     const bool fused = (w % 8 == 0) && (h % 8 == 0) && lv_.n == 4;
     h2d_bytes_ = is_device ? 0 : (long long)w * h;
     d2h_bytes_ = 0;
@@ -178,11 +200,11 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
     if (timing_) {
         // Per-stage timing: eager launches queued behind a ~2 ms gate so the
         // GPU never waits for the host between two stage events.
-        launch_gate(stream_, 2000);
-        CCTAGB_CUDA(cudaEventRecord(ev0_, stream_));
-        launch_image_stage(lv_, vp_, stream_, fused, st_ev_);
-        CCTAGB_CUDA(cudaEventRecord(ev1_, stream_));
-        sync_counters();
+        launch_gate(st, 2000);
+        CCTAGB_CUDA(cudaEventRecord(ev0_, st));
+        launch_image_stage(lv_, vp_, st, fused, st_ev_);
+        CCTAGB_CUDA(cudaEventRecord(ev1_, st));
+        sync_counters(st);
         CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
         for (int k = 0; k < kStageCount; ++k) CCTAGB_CUDA(cudaEventElapsedTime(&stage_ms_[k], st_ev_[k], st_ev_[k + 1]));
         return;
@@ -193,25 +215,25 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
             graph_ = nullptr;
         }
         cudaGraph_t g = nullptr;
-        CCTAGB_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        CCTAGB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         try {
-            launch_image_stage(lv_, vp_, stream_, fused, nullptr);
+            launch_image_stage(lv_, vp_, st, fused, nullptr);
         } catch (...) {
-            cudaStreamEndCapture(stream_, &g);
+            cudaStreamEndCapture(st, &g);
             if (g) cudaGraphDestroy(g);
             throw;
         }
-        CCTAGB_CUDA(cudaStreamEndCapture(stream_, &g));
+        CCTAGB_CUDA(cudaStreamEndCapture(st, &g));
         const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
         cudaGraphDestroy(g);
         CCTAGB_CUDA(e);
         graph_w_ = w;
         graph_h_ = h;
     }
-    CCTAGB_CUDA(cudaEventRecord(ev0_, stream_));
-    CCTAGB_CUDA(cudaGraphLaunch(graph_, stream_));
-    CCTAGB_CUDA(cudaEventRecord(ev1_, stream_));
-    sync_counters();
+    CCTAGB_CUDA(cudaEventRecord(ev0_, st));
+    CCTAGB_CUDA(cudaGraphLaunch(graph_, st));
+    CCTAGB_CUDA(cudaEventRecord(ev1_, st));
+    sync_counters(st);
     CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
 }
 
@@ -224,11 +246,11 @@ void Pipeline::set_stage_timing(bool on)
     std::fill(stage_ms_, stage_ms_ + kStageCount, 0.f);
 }
 
-void Pipeline::sync_counters()
+void Pipeline::sync_counters(cudaStream_t s)
 {
-    CCTAGB_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(LevelCounters) * kMaxLevels, cudaMemcpyDeviceToHost, stream_));
+    CCTAGB_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(LevelCounters) * kMaxLevels, cudaMemcpyDeviceToHost, s));
     d2h_bytes_ += sizeof(LevelCounters) * kMaxLevels;
-    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    CCTAGB_CUDA(cudaStreamSynchronize(s));
     for (int l = 0; l < lv_.n; ++l) {
         const int err = h_cnt_[l].err;
         if (err & kErrUnionFind) throw Error{CCTAGB_HYST_NO_CONVERGE, "hysteresis union-find exceeded its cap"};
@@ -247,7 +269,7 @@ void Pipeline::canny_only(const int16_t* dx, const int16_t* dy, int w, int h, ui
     CCTAGB_CUDA(cudaMemcpyAsync(lv_.l[0].dx, dx, px * 2, cudaMemcpyHostToDevice, stream_));
     CCTAGB_CUDA(cudaMemcpyAsync(lv_.l[0].dy, dy, px * 2, cudaMemcpyHostToDevice, stream_));
     launch_canny_only(lv_, vp_, stream_);
-    sync_counters();
+    sync_counters(stream_);
     copy_planes(0, nullptr, nullptr, nullptr, edges_out);
     graph_w_ = graph_h_ = -1;  // views were narrowed; force a fresh capture next frame
 }
@@ -307,6 +329,13 @@ void Pipeline::issue_level_download(int l, bool voters)
 
 void Pipeline::finish_level_download(int l, HostLevel& out, bool voters)
 {
+    const LevelAlloc& a = la_[l];
+    finish_level(l, out, voters, a.h_sidx, a.h_skey, a.h_svotes);
+}
+
+void Pipeline::finish_level(int l, HostLevel& out, bool voters, const int32_t* sidx, const int32_t* skey,
+                            const int32_t* svotes)
+{
     const LevelView& v = lv_.l[l];
     const LevelCounters& c = h_cnt_[l];
     const LevelAlloc& a = la_[l];
@@ -332,7 +361,7 @@ void Pipeline::finish_level_download(int l, HostLevel& out, bool voters)
         int32_t key, idx, votes;
     };
     std::vector<SeedRec> ks(static_cast<size_t>(S));
-    for (int i = 0; i < S; ++i) ks[size_t(i)] = {a.h_skey[i], a.h_sidx[i], a.h_svotes[i]};
+    for (int i = 0; i < S; ++i) ks[size_t(i)] = {skey[i], sidx[i], svotes[i]};
     std::sort(ks.begin(), ks.end(),
               [](const SeedRec& x, const SeedRec& y) { return x.key < y.key || (x.key == y.key && x.idx < y.idx); });
     std::vector<std::pair<int32_t, int32_t>> sv(static_cast<size_t>(S));
@@ -357,27 +386,59 @@ void Pipeline::download_level(int l, HostLevel& out)
 void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
 {
     out.resize(lv_.n);
+    // One compacting launch and two copies: the seeds of every level (index,
+    // key, votes) on the pipeline stream, then the edge points' positions,
+    // gradients and links on the copy stream.
+    PackSegs ps{};
+    long long off = 0;
+    auto seg = [&](const int32_t* src, long long n) {
+        ps.src[ps.n] = src;
+        ps.off[ps.n] = off;
+        ++ps.n;
+        off += n;
+    };
     for (int l = 0; l < lv_.n; ++l) {
         const LevelView& v = lv_.l[l];
-        const LevelCounters& c = h_cnt_[l];
-        LevelAlloc& a = la_[l];
-        const int E = c.E;
-        const int S = std::min(c.S, v.seedcap);
-        auto d2h = [&](void* dst, const void* src, size_t bytes, cudaStream_t st) {
-            if (bytes) CCTAGB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
-        };
-        d2h(a.h_sidx, v.seed_idx, size_t(S) * 4, stream_);
-        d2h(a.h_skey, v.seed_key, size_t(S) * 4, stream_);
-        d2h(a.h_svotes, v.seed_votes, size_t(S) * 4, stream_);
-        d2h(a.h_exy, v.exy, size_t(E) * 4, copy_stream_);
-        d2h(a.h_grad, v.grad, size_t(E) * 4, copy_stream_);
-        d2h(a.h_before, v.before, size_t(E) * 4, copy_stream_);
-        d2h(a.h_after, v.after, size_t(E) * 4, copy_stream_);
-        d2h_bytes_ += (long long)E * 16 + (long long)S * 12;
+        const long long S = std::min(h_cnt_[l].S, v.seedcap);
+        seg(v.seed_idx, S);
+        seg(v.seed_key, S);
+        seg(v.seed_votes, S);
+    }
+    const long long nseed = off;
+    for (int l = 0; l < lv_.n; ++l) {
+        const LevelView& v = lv_.l[l];
+        const long long E = h_cnt_[l].E;
+        seg(v.exy, E);
+        seg(v.grad, E);
+        seg(v.before, E);
+        seg(v.after, E);
+    }
+    ps.off[ps.n] = off;
+    if (off > pack_words_) throw Error{CCTAGB_INTERNAL, "download staging too small"};
+    launches_ += launch_pack(ps, d_pack_, stream_);
+    CCTAGB_CUDA(cudaEventRecord(ev_pack_, stream_));
+    if (nseed)
+        CCTAGB_CUDA(cudaMemcpyAsync(h_pack_, d_pack_, size_t(nseed) * 4, cudaMemcpyDeviceToHost, stream_));
+    CCTAGB_CUDA(cudaStreamWaitEvent(copy_stream_, ev_pack_, 0));
+    if (off > nseed)
+        CCTAGB_CUDA(cudaMemcpyAsync(h_pack_ + nseed, d_pack_ + nseed, size_t(off - nseed) * 4,
+                                    cudaMemcpyDeviceToHost, copy_stream_));
+    d2h_bytes_ += off * 4;
+    for (int l = 0; l < lv_.n; ++l) {
+        Packed& k = pk_[l];
+        k.sidx = h_pack_ + ps.off[3 * l];
+        k.skey = h_pack_ + ps.off[3 * l + 1];
+        k.svotes = h_pack_ + ps.off[3 * l + 2];
+        const int p = 3 * lv_.n + 4 * l;
+        k.exy = h_pack_ + ps.off[p];
+        k.grad = h_pack_ + ps.off[p + 1];
+        k.before = h_pack_ + ps.off[p + 2];
+        k.after = h_pack_ + ps.off[p + 3];
     }
     CCTAGB_CUDA(cudaStreamSynchronize(stream_));
     for (int l = 0; l < lv_.n; ++l) {
-        finish_level_download(l, out[l], false);
+        const Packed& k = pk_[l];
+        finish_level(l, out[l], false, k.sidx, k.skey, k.svotes);
         out[l].exy = out[l].grad = out[l].before = out[l].after = nullptr;  // until wait_points()
     }
 }
@@ -386,11 +447,11 @@ void Pipeline::wait_points(std::vector<HostLevel>& out)
 {
     CCTAGB_CUDA(cudaStreamSynchronize(copy_stream_));
     for (int l = 0; l < lv_.n; ++l) {
-        const LevelAlloc& a = la_[l];
-        out[l].exy = a.h_exy;
-        out[l].grad = a.h_grad;
-        out[l].before = a.h_before;
-        out[l].after = a.h_after;
+        const Packed& k = pk_[l];
+        out[l].exy = k.exy;
+        out[l].grad = k.grad;
+        out[l].before = k.before;
+        out[l].after = k.after;
     }
 }
 

@@ -84,14 +84,16 @@ public:
 private:
     void alloc(int max_w, int max_h);
     void set_views(int w, int h, int nlevels);
-    void sync_counters();
+    void sync_counters(cudaStream_t s);  // counters to the host; s synchronised
 
     cctagb_params params_;
     VoteParamsDev vp_{};
     int max_w_ = 0, max_h_ = 0;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t stage_stream_ = nullptr; // upload + image stage, lowest priority
     cudaStream_t copy_stream_ = nullptr;  // edge-point downloads of a detection
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaEvent_t ev_in_ = nullptr;         // orders the stage stream after stream_
     std::vector<void*> allocs_;
     struct LevelAlloc {
         size_t px = 0;  // pixel capacity
@@ -112,6 +114,18 @@ private:
     std::vector<void*> host_allocs_;
     void issue_level_download(int l, bool voters);
     void finish_level_download(int l, HostLevel& out, bool voters);
+    // Fills out from the counters and the downloaded seed arrays (sorted into
+    // processing order); the point pointers are the per-level staging's.
+    void finish_level(int l, HostLevel& out, bool voters, const int32_t* sidx, const int32_t* skey,
+                      const int32_t* svotes);
+    // compact staging of download_seeds_then_points and its per-level views
+    int32_t* d_pack_ = nullptr;
+    int32_t* h_pack_ = nullptr;  // pinned
+    long long pack_words_ = 0;
+    struct Packed {
+        const int32_t *sidx, *skey, *svotes, *exy, *grad, *before, *after;
+    } pk_[kMaxLevels] = {};
+    cudaEvent_t ev_pack_ = nullptr;  // the pack launch, for the copy stream
     Levels lv_{};
     LevelCounters* d_cnt_ = nullptr;  // + scan partials
     LevelCounters* h_cnt_ = nullptr;  // pinned
