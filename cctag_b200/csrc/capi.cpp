@@ -37,6 +37,7 @@ struct Ticket {
 
 struct cctagb_handle {
     std::shared_ptr<cctagb::ThreadPool> pool;     // host workers shared by every slot
+    std::shared_ptr<cctagb::StageOrder> order;    // image stages of the slots, in submission order
     std::unique_ptr<cctagb::Detector> det;        // slot 0: every single-frame call
     std::vector<std::unique_ptr<cctagb::Detector>> extra;  // slots 1..: cctagb_detect_batch
     cctagb_params params{};
@@ -51,6 +52,7 @@ struct cctagb_handle {
     {
         while (int(extra.size()) + 1 < n) {
             extra.emplace_back(new cctagb::Detector(params, max_w, max_h, 1, pool));
+            extra.back()->pipeline().set_stage_order(order);
             copy_bank(*extra.back());
         }
     }
@@ -268,6 +270,8 @@ cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int ma
         if (threads <= 0) threads = std::max(2, cctagb::physical_cores() - (h->slots() - 1));
         h->pool = cctagb::make_host_pool(threads);
         h->det.reset(new cctagb::Detector(*p, max_w, max_h, max_batch, h->pool));
+        h->order = std::make_shared<cctagb::StageOrder>();
+        h->det->pipeline().set_stage_order(h->order);
     });
     if (s != CCTAGB_OK) return s;
     *out = h.release();

@@ -8,12 +8,12 @@
 // roundings in the same order (no contraction into FMAs), so the selected
 // cut ends are the same bits as the host's.  The cosine and sine of the
 // ellipse angle come from the host (they are the only transcendental values).
-#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
 #include "common.hpp"
 #include "ident_host.hpp"
+#include "pmath.hpp"
 
 namespace cctagb {
 
@@ -28,29 +28,25 @@ __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); 
 __device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fd(float a, float b) { return __fdiv_rn(a, b); }
 
-// Identification.hpp:197-219, as the host: ((p0 w1 + p1 w2) + p2 w3 + p3 w4) / 2.
-// The gather at (px + 1, py + 1) returns the 2x2 footprint whose top-left
-// texel is (px, py), as x = (px, py+1), y = (px+1, py+1), z = (px+1, py),
-// w = (px, py); the coordinates are exact small integers, so the footprint
-// is the host's.
-__device__ __forceinline__ float bilinear_host(cudaTextureObject_t img, float x, float y)
+// Identification.hpp:197-219, as the host: ((p0 w1 + p1 w2) + p2 w3 + p3 w4) / 2
+__device__ __forceinline__ float bilinear_host(const uint8_t* img, int W, float x, float y)
 {
     const int px = int(x), py = int(y);
-    const uchar4 q = tex2Dgather<uchar4>(img, float(px) + 1.0f, float(py) + 1.0f, 0);
+    const uint8_t* p0 = img + px + size_t(py) * W;
     const float fx = fs(x, float(px)), fy = fs(y, float(py));
     const float fx1 = fs(1.0f, fx), fy1 = fs(1.0f, fy);
     const float w1 = fm(fx1, fy1), w2 = fm(fx, fy1), w3 = fm(fx1, fy), w4 = fm(fx, fy);
-    float t = fm(float(q.w), w1);
-    t = fa(t, fm(float(q.z), w2));
-    t = fa(t, fm(float(q.x), w3));
-    t = fa(t, fm(float(q.y), w4));
-    return fd(t, 2.f);
+    float t = fm(float(p0[0]), w1);
+    t = fa(t, fm(float(p0[1]), w2));
+    t = fa(t, fm(float(p0[W]), w3));
+    t = fa(t, fm(float(p0[W + 1]), w4));
+    return fm(t, 0.5f);  // the division by 2, exact
 }
 
 // cutInterpolated from (sx, sy) to (ex, ey): the samples' Boost-style mean /
 // variance when every sample stays in [1, W-1) x [1, H-1); sig (optional)
 // receives the samples.
-__device__ bool cut_stats(cudaTextureObject_t img, int W, int H, float sx, float sy, float ex, float ey, float beginSig,
+__device__ bool cut_stats(const uint8_t* img, int W, int H, float sx, float sy, float ex, float ey, float beginSig,
                           int n, float* var_out, float* sig)
 {
     const float dX = fs(ex, sx), dY = fs(ey, sy);
@@ -62,7 +58,7 @@ __device__ bool cut_stats(cudaTextureObject_t img, int W, int H, float sx, float
     const float den = fs(float(n), 1.f);
     const float stepX = fd(fs(ex, xs), den), stepY = fd(fs(ey, ys), den);
     float x = xs, y = ys;
-    float mean = 0.f, var = 0.f;
+    float mean = 0.f, var = 0.f, rprev = 1.f;
     // 8 samples at a time: their positions (the same running sums) and bounds
     // first, then the 8 bilinear reads, which overlap, then the running mean
     // and variance in sample order
@@ -82,19 +78,22 @@ __device__ bool cut_stats(cudaTextureObject_t img, int W, int H, float sx, float
         if (!inside) return false;
 #pragma unroll
         for (int k = 0; k < kGroup; ++k)
-            if (i0 + k < n) gv[k] = bilinear_host(img, gx[k], gy[k]);
+            if (i0 + k < n) gv[k] = bilinear_host(img, W, gx[k], gy[k]);
 #pragma unroll
         for (int k = 0; k < kGroup; ++k)
             if (i0 + k < n) {
                 const float v = gv[k];
                 if (sig) sig[i0 + k] = v;
-                // MeanVar::add
+                // MeanVar::add; the divisions by the counts are correctly
+                // rounded (div_small: the operands here are zero or normal)
                 const int c = i0 + k + 1;
-                mean = fd(fa(fm(mean, float(c - 1)), v), float(c));
+                const float fc = float(c), fc1 = float(c - 1), rc = __frcp_rn(fc);
+                mean = pm::div_small(fa(fm(mean, fc1), v), fc, rc);
                 if (c > 1) {
                     const float t = fs(v, mean);
-                    var = fa(fd(fm(var, float(c - 1)), float(c)), fd(fm(t, t), float(c - 1)));
+                    var = fa(pm::div_small(fm(var, fc1), fc, rc), pm::div_small(fm(t, t), fc1, rprev));
                 }
+                rprev = rc;
             }
     }
     *var_out = var;
@@ -121,7 +120,7 @@ __device__ void conv_cut(const float* k, const float* sig, int n, float& best, i
 
 // outerEdgeRefinement: the cut end moves to the strongest derivative
 // response along its gradient; false when that cut leaves the image.
-__device__ bool refine_stop(float& x, float& y, float dx, float dy, cudaTextureObject_t img, int W, int H, float scale,
+__device__ bool refine_stop(float& x, float& y, float dx, float dy, const uint8_t* img, int W, int H, float scale,
                             int nRefine)
 {
     const float len = fm(fm(3.f, __fsqrt_rn(2.f)), scale);
@@ -159,7 +158,7 @@ __device__ bool refine_stop(float& x, float& y, float dx, float dy, cudaTextureO
 
 }  // namespace
 
-__global__ void __launch_bounds__(kCutThreads) k_cut_select(cudaTextureObject_t img, int W, int H,
+__global__ void __launch_bounds__(kCutThreads) k_cut_select(const uint8_t* __restrict__ img, int W, int H,
                                                             const CutSelectIn* __restrict__ ins,
                                                             const DirPoint* __restrict__ pts, IdentTask* tasks,
                                                             int* status, CutSelectParams cp)
@@ -244,50 +243,14 @@ __global__ void __launch_bounds__(kCutThreads) k_cut_select(cudaTextureObject_t 
     }
 }
 
-FrameTexture::~FrameTexture() { release(); }
-
-void FrameTexture::release()
-{
-    if (tex_) cudaDestroyTextureObject(tex_);
-    if (arr_) cudaFreeArray(arr_);
-    tex_ = 0;
-    arr_ = nullptr;
-    w_ = h_ = 0;
-}
-
-cudaTextureObject_t FrameTexture::fill(const uint8_t* d_src, int W, int H, cudaStream_t s)
-{
-    if (W > w_ || H > h_) {
-        CCTAGB_CUDA(cudaStreamSynchronize(s));  // no launch still reads the old array
-        const int w = std::max(W, w_), h = std::max(H, h_);
-        release();
-        const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<unsigned char>();
-        CCTAGB_CUDA(cudaMallocArray(&arr_, &fmt, size_t(w), size_t(h), cudaArrayTextureGather));
-        cudaResourceDesc rd{};
-        rd.resType = cudaResourceTypeArray;
-        rd.res.array.array = arr_;
-        cudaTextureDesc td{};
-        td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
-        td.filterMode = cudaFilterModePoint;
-        td.readMode = cudaReadModeElementType;
-        td.normalizedCoords = 0;
-        CCTAGB_CUDA(cudaCreateTextureObject(&tex_, &rd, &td, nullptr));
-        w_ = w;
-        h_ = h;
-    }
-    CCTAGB_CUDA(cudaMemcpy2DToArrayAsync(arr_, 0, 0, d_src, size_t(W), size_t(W), size_t(H),
-                                         cudaMemcpyDeviceToDevice, s));
-    return tex_;
-}
-
-void launch_cut_select(cudaTextureObject_t frame, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
+void launch_cut_select(const uint8_t* d_img, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
                        IdentTask* d_tasks, int* d_status, int n, const CutSelectParams& cp, cudaStream_t s)
 {
     if (n <= 0) return;
     if (cp.nSamples < 2 || cp.nSamples > kMaxSamples) throw Error{CCTAGB_BAD_ARG, "sampleCutLength out of range"};
     if (cp.nRefine < 2 || cp.nRefine > kMaxRefineSamples)
         throw Error{CCTAGB_BAD_ARG, "numSamplesOuterEdgePointsRefinement out of range"};
-    k_cut_select<<<n, kCutThreads, 0, s>>>(frame, W, H, d_ins, d_pts, d_tasks, d_status, cp);
+    k_cut_select<<<n, kCutThreads, 0, s>>>(d_img, W, H, d_ins, d_pts, d_tasks, d_status, cp);
     CCTAGB_CUDA(cudaGetLastError());
 }
 

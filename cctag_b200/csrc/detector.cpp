@@ -171,7 +171,7 @@ void Detector::select_and_identify(int nm, int npts, int w, int h)
     cp.nSamples = std::min(params_.sampleCutLength, kMaxSamples);
     cp.nRefine = params_.numSamplesOuterEdgePointsRefinement;
     cp.maxSelect = std::min(params_.numCutsInIdentStep, kMaxCuts);
-    launch_cut_select(frame_tex_.fill(pipe_.level0_src(), w, h, s), w, h, d_cutin_, d_cutpts_, d_tasks_, d_st1_, nm, cp, s);
+    launch_cut_select(pipe_.level0_src(), w, h, d_cutin_, d_cutpts_, d_tasks_, d_st1_, nm, cp, s);
     CCTAGB_CUDA(cudaEventRecord(ev_id0_, s));
     launch_identify(pipe_.level0_src(), size_t(w), d_tasks_, d_res_, nm, d_bank_inv_,
                     ident_params(params_.refineMode), s);

@@ -63,7 +63,6 @@ private:
     std::unique_ptr<LoopOneGpu> loop1_;          // loop 1 + outlier removal on the GPU
     std::vector<LoopTwoIn> loop2in_;             // its results for the last frame
     std::shared_ptr<ThreadPool> pool_;
-    FrameTexture frame_tex_;                     // level-0 frame for k_cut_select
     CutSelectIn* d_cutin_ = nullptr;             // cut selection inputs (device / pinned)
     CutSelectIn* h_cutin_ = nullptr;
     DirPoint* d_cutpts_ = nullptr;               // sorted outer points of all markers

@@ -56,30 +56,10 @@ struct CutSelectParams {
 // angle around the ellipse center, uniformly subsampled.
 std::vector<DirPoint> sorted_outer_points(const geo::Ellipse& e, const std::vector<DirPoint>& pts, size_t requested);
 
-// The level-0 frame as a gather texture: k_cut_select reads the four pixels
-// of each bilinear sample with one tex2Dgather instead of four scattered
-// byte loads.  A CUDA array (2D-local layout) grown to the largest frame.
-class FrameTexture {
-public:
-    FrameTexture() = default;
-    FrameTexture(const FrameTexture&) = delete;
-    FrameTexture& operator=(const FrameTexture&) = delete;
-    ~FrameTexture();
-    // Copies the W x H frame (rows W bytes apart) into the array on stream s.
-    cudaTextureObject_t fill(const uint8_t* d_src, int W, int H, cudaStream_t s);
-
-private:
-    void release();
-    cudaArray_t arr_ = nullptr;
-    cudaTextureObject_t tex_ = 0;
-    int w_ = 0, h_ = 0;
-};
-
 // Writes stop[] and ncuts of tasks[i] (the rest filled by the host) and
 // status[i] (CCTAGB_ID_RELIABLE, _NO_COLLECTED_CUTS or _NO_SELECTED_CUTS;
-// left alone for markers with fewer than 5 outer points).  frame is the
-// W x H level-0 image as filled by FrameTexture.
-void launch_cut_select(cudaTextureObject_t frame, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
+// left alone for markers with fewer than 5 outer points).
+void launch_cut_select(const uint8_t* d_img, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
                        IdentTask* d_tasks, int* d_status, int n, const CutSelectParams& cp, cudaStream_t s);
 
 // Signal start along the cut as a fraction of the unit radius.

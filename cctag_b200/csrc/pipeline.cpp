@@ -79,6 +79,13 @@ Pipeline::~Pipeline()
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
 }
 
+StageOrder::StageOrder() { CCTAGB_CUDA(cudaEventCreateWithFlags(&last, cudaEventDisableTiming)); }
+
+StageOrder::~StageOrder()
+{
+    if (last) cudaEventDestroy(last);
+}
+
 void Pipeline::alloc(int max_w, int max_h)
 {
     if (max_w < 1 || max_h < 1 || max_w > 16384 || max_h > 16384)
@@ -230,9 +237,18 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
         graph_w_ = w;
         graph_h_ = h;
     }
-    CCTAGB_CUDA(cudaEventRecord(ev0_, st));
-    CCTAGB_CUDA(cudaGraphLaunch(graph_, st));
-    CCTAGB_CUDA(cudaEventRecord(ev1_, st));
+    if (order_) {
+        std::lock_guard<std::mutex> lock(order_->m);
+        CCTAGB_CUDA(cudaStreamWaitEvent(st, order_->last, 0));
+        CCTAGB_CUDA(cudaEventRecord(ev0_, st));
+        CCTAGB_CUDA(cudaGraphLaunch(graph_, st));
+        CCTAGB_CUDA(cudaEventRecord(ev1_, st));
+        CCTAGB_CUDA(cudaEventRecord(order_->last, st));
+    } else {
+        CCTAGB_CUDA(cudaEventRecord(ev0_, st));
+        CCTAGB_CUDA(cudaGraphLaunch(graph_, st));
+        CCTAGB_CUDA(cudaEventRecord(ev1_, st));
+    }
     sync_counters(st);
     CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
 }

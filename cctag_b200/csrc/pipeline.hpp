@@ -1,6 +1,8 @@
 // Host orchestration of one detection pipeline (one handle).
 #pragma once
 
+#include <mutex>
+#include <memory>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -28,6 +30,21 @@ struct HostLevel {
     std::vector<int32_t> seeds;  // processing order (Multiresolution.cpp:239-242)
 };
 
+// Orders the image stages of the detectors of one handle on the GPU: each
+// stage waits for the one submitted before it, so that the full-GPU stages
+// run one after the other in submission order.  The first frames of a batch
+// then leave their image stage early and their latency-bound kernels and host
+// phases overlap the later frames' stages, instead of every stage
+// interleaving with the others and all finishing together.
+struct StageOrder {
+    StageOrder();
+    ~StageOrder();
+    StageOrder(const StageOrder&) = delete;
+    StageOrder& operator=(const StageOrder&) = delete;
+    std::mutex m;
+    cudaEvent_t last = nullptr;  // end of the last submitted image stage
+};
+
 class Pipeline {
 public:
     Pipeline(const cctagb_params& p, int max_w, int max_h, int max_batch);
@@ -37,6 +54,8 @@ public:
 
     const cctagb_params& params() const { return params_; }
     cudaStream_t stream() const { return stream_; }
+    // Shares the image-stage order of the other detectors of a handle.
+    void set_stage_order(std::shared_ptr<StageOrder> o) { order_ = std::move(o); }
 
     // Pyramid .. seeds for one frame; results stay on the device.
     void image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool is_device);
@@ -94,6 +113,7 @@ private:
     cudaStream_t copy_stream_ = nullptr;  // edge-point downloads of a detection
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaEvent_t ev_in_ = nullptr;         // orders the stage stream after stream_
+    std::shared_ptr<StageOrder> order_;
     std::vector<void*> allocs_;
     struct LevelAlloc {
         size_t px = 0;  // pixel capacity
