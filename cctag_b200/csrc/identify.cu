@@ -28,6 +28,7 @@
 
 #include "common.hpp"
 #include "ident_host.hpp"
+#include "pmath.hpp"
 
 namespace cctagb {
 
@@ -419,15 +420,12 @@ __device__ void trial_partial(const Shared& S, const Roi& R, int t, uint32_t val
     }
 }
 
-// Identification.hpp:373-384
-__device__ __forceinline__ float dis(float sig, float val, float mub, float muw, float var)
+// Identification.hpp:373-384, with val = +1 (white: even ratio count) or -1
+// and the division by 2 var done as a product with rvar2 = 1 / double(2 var).
+__device__ __forceinline__ float dis_r(float sig, bool white, float mub, float muw, double rvar2)
 {
-    if (val == -1.f) {
-        const float d = fmaxf(sig - mub, 0.f);
-        return d * d / (2.0f * var);
-    }
-    const float d = fminf(sig - muw, 0.f);
-    return d * d / (2.0f * var);
+    const float d = white ? fminf(__fsub_rn(sig, muw), 0.f) : fmaxf(__fsub_rn(sig, mub), 0.f);
+    return float(double(__fmul_rn(d, d)) * rvar2);
 }
 
 
@@ -953,17 +951,22 @@ __global__ void __launch_bounds__(kThreads, MB)
         if (!((valid >> c) & 1u)) continue;
         const float* sg = S.sig[c];
         // statistics over samples [30, n): Boost immediate mean / variance
+        // (the divisions by the counts correctly rounded by div_small)
         float mean = 0.f, var = 0.f;
         {
             int cnt = 0;
+            float rprev = 1.f;
             for (int k = 30; k < nS; ++k) {
                 ++cnt;
                 const float x = sg[k];
-                mean = (mean * float(cnt - 1) + x) / float(cnt);
+                const float fc = float(cnt), fc1 = float(cnt - 1), rc = __frcp_rn(fc);
+                mean = pm::div_small(__fmaf_rn(mean, fc1, x), fc, rc);
                 if (cnt > 1) {
-                    const float t = x - mean;
-                    var = var * float(cnt - 1) / float(cnt) + t * t / float(cnt - 1);
+                    const float t = __fsub_rn(x, mean);
+                    var = __fadd_rn(pm::div_small(__fmul_rn(var, fc1), fc, rc),
+                                    pm::div_small(__fmul_rn(t, t), fc1, rprev));
                 }
+                rprev = rc;
             }
         }
         float mub = 0.f, muw = 0.f;
@@ -976,14 +979,20 @@ __global__ void __launch_bounds__(kThreads, MB)
                 if (acc) {
                     if (x < mean) {
                         ++ni;
-                        mub = (mub * float(ni - 1) + x) / float(ni);
+                        mub = pm::div_small(__fmaf_rn(mub, float(ni - 1), x), float(ni), __frcp_rn(float(ni)));
                     } else {
                         ++nsup;
-                        muw = (muw * float(nsup - 1) + x) / float(nsup);
+                        muw = pm::div_small(__fmaf_rn(muw, float(nsup - 1), x), float(nsup),
+                                            __frcp_rn(float(nsup)));
                     }
                 }
             }
         }
+        // dis()'s division by 2 var: a float quotient through the double
+        // reciprocal is correctly rounded for a normal result (its relative
+        // error, 2^-52, is below the 2^-49 that separates a quotient of floats
+        // from a float rounding midpoint), so each term is the IEEE quotient.
+        const double rvar2 = 1.0 / double(2.0f * var);
         const float stepX = (1.f - ip.beginSig) / (float(nS) - 1.f);
         // std::map<float, id> keeps, for equal keys, the id inserted last: the
         // winner is the largest v, ties to the largest id.  v >= 0, so its bit
@@ -999,11 +1008,12 @@ __global__ void __launch_bounds__(kThreads, MB)
                 for (int r = 0; r < kMaxBankRatios; ++r)
                     inv[r] = r < ip.nRatios ? __ldg(&bankInv[idc * kMaxBankRatios + r]) : FLT_MAX;
                 float x = ip.beginSig, dist = 0.f;
+#pragma unroll 4
                 for (int k = 0; k < nS; ++k) {
                     int ldum = 0;
 #pragma unroll
                     for (int r = 0; r < kMaxBankRatios; ++r) ldum += (inv[r] <= x) ? 1 : 0;
-                    dist += dis(sg[k], float(-(ldum % 2) * 2 + 1), mub, muw, var);
+                    dist += dis_r(sg[k], (ldum & 1) == 0, mub, muw, rvar2);
                     x += stepX;
                 }
                 const float v = expf(-dist);

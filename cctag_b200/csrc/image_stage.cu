@@ -980,24 +980,26 @@ __global__ void k_gate(int us)
 
 void launch_gate(cudaStream_t s, int us) { k_gate<<<1, 1, 0, s>>>(us); }
 
-// Segment blockIdx.y of p to dst[p.off[y] ...], grid-stride over its words.
+// The segments of p back to back into dst: a flat grid-stride loop over the
+// total, each thread advancing its segment cursor as its index grows.
 __global__ void __launch_bounds__(256) k_pack_words(PackSegs p, int32_t* __restrict__ dst)
 {
-    const int g = blockIdx.y;
-    const long long o = p.off[g], n = p.off[g + 1] - o;
-    const int32_t* __restrict__ src = p.src[g];
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        dst[o + i] = __ldg(src + i);
+    const long long total = p.off[p.n];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int g = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        while (i >= p.off[g + 1]) ++g;  // i < off[n], so g < n
+        dst[i] = __ldg(p.src[g] + (i - p.off[g]));
+    }
 }
 
 int launch_pack(const PackSegs& p, int32_t* dst, cudaStream_t s)
 {
     if (p.n <= 0 || p.n > kMaxPackSegs) return 0;
-    long long longest = 0;
-    for (int g = 0; g < p.n; ++g) longest = std::max(longest, p.off[g + 1] - p.off[g]);
-    if (longest == 0) return 0;
-    const int bx = int(std::min<long long>((longest + 1023) / 1024, 148));
-    k_pack_words<<<dim3(bx, p.n), 256, 0, s>>>(p, dst);
+    const long long total = p.off[p.n];
+    if (total <= 0) return 0;
+    const int blocks = int(std::min<long long>((total + 255) / 256, 148 * 4));
+    k_pack_words<<<blocks, 256, 0, s>>>(p, dst);
     CCTAGB_CUDA(cudaGetLastError());
     return 1;
 }
