@@ -164,6 +164,29 @@ __device__ __forceinline__ bool convexity_lost(float front, float back, bool ful
     return cand::link_convexity_lost(front, back, full, dir);
 }
 
+// cand::link_shift without a division where it is safe: the quotient by
+// 2 pi through a float reciprocal is within 1e-6 of the exact one after the
+// scaling by 8, so wherever that product is more than 1e-5 away from a
+// rounding boundary (k + 1/2) both round to the same integer; elsewhere (and
+// for a non-finite angle) the exact form decides.
+__device__ __forceinline__ int link_shift_fast(float angle)
+{
+    const float a = __fadd_rn(angle, cand::kPiF / 4.0f);
+    const float p = __fmul_rn(__fmul_rn(a, 0.159154943f), 8.0f);
+    if (fabsf(__fsub_rn(__fsub_rn(p, floorf(p)), 0.5f)) > 1e-5f) return int(rintf(p)) - 1;
+    return cand::link_shift(angle);
+}
+
+// cand::link_average_vote with the division by the segment size + 1 (an
+// integer up to 2 kLinkMaxLength + 2) correctly rounded by div_small.
+__device__ __forceinline__ float link_average_vote_fast(float average, int segSize, int voters)
+{
+    const float n = __fadd_rn(__fmul_rn(average, float(segSize)), float(voters));
+    const float d = float(segSize) + 1.f;
+    if (segSize + 1 > 256) return n / d;
+    return pm::div_small(n, d, __frcp_rn(d));
+}
+
 // Vote.cpp:272-394 edgeLinkingDir from the seed in direction dir, by the 8
 // lanes of a group: lane j examines the j-th neighbour of the search order,
 // the first lane whose neighbour is an unvisited edge point decides the step.
@@ -190,7 +213,7 @@ __device__ int link_walk(const int4* recs, int seed, int dir, int32_t* segc, int
             --count;
         }
         __syncwarp(gmask);
-        const int shifting = cand::link_shift(angle);
+        const int shifting = link_shift_fast(angle);
         const int k = dir == 1 ? (8 - shifting + j) % 8 : (shifting + j) % 8;
         // direction -1 mirrors the y offsets: neighbour (8 - k) % 8 of the +1 table
         const int q = nbr(r, dir == 1 ? k : (8 - k) % 8);
@@ -220,7 +243,7 @@ __device__ int link_walk(const int4* recs, int seed, int dir, int32_t* segc, int
                 r.r0 = shfl_int4(gmask, rq.r0, gbase + jj);
                 r.r1 = shfl_int4(gmask, rq.r1, gbase + jj);
                 r.r2 = shfl_int4(gmask, rq.r2, gbase + jj);
-                averageVote = cand::link_average_vote(averageVote, 1 + nf + nb, r.r0.z);
+                averageVote = link_average_vote_fast(averageVote, 1 + nf + nb, r.r0.z);
                 stop = 1;
             }
         }
