@@ -185,13 +185,6 @@ void Detector::select_and_identify(int nm, int npts, int w, int h)
                  (long long)(sizeof(IdentResult) + sizeof(int) + sizeof(IdentTask)) * nm, 2);
 }
 
-void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
-{
-    int W, H;
-    pipe_.level_size(0, &W, &H);
-    identify_on(pipe_.level0_src(), size_t(W), tasks, n, ident_params(params_.refineMode), out);
-}
-
 namespace {
 
 // Caller-given tasks must stay inside the image and within the kernel's limits.
@@ -214,6 +207,14 @@ void check_tasks(const IdentTask* tasks, int n, int w, int h, size_t pitch)
 }
 
 }  // namespace
+
+void Detector::identify(const IdentTask* tasks, int n, IdentResult* out)
+{
+    int W, H;
+    pipe_.level_size(0, &W, &H);
+    check_tasks(tasks, n, W, H, size_t(W));
+    identify_on(pipe_.level0_src(), size_t(W), tasks, n, ident_params(params_.refineMode), out);
+}
 
 void Detector::identify_tasks(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
                               int refine_mode, IdentResult* out)
