@@ -717,9 +717,13 @@ __device__ void gn_refine(Shared& S, const IdentTask& T, const Roi& roi, const I
 // (launched with that cluster dimension), block r on sample chunk r.  MB:
 // blocks per SM the registers are budgeted for (2 suits Gauss-Newton, whose
 // steps leave most warps waiting; the grid keeps every warp busy and prefers
-// the registers).
+// the registers).  The register caps follow from the 25 warps of a block
+// spread over the SM's four 16 K-register partitions (7 warps on one): 72 for
+// one block per SM, 32 for two; 64 for the cluster form (the detection's),
+// which needs no spill at 64 and so leaves room in every partition for a
+// block of another stream's kernel.
 template <int CL, int MB>
-__global__ void __launch_bounds__(kThreads, MB)
+__global__ void __maxnreg__(CL > 1 ? 64 : (MB == 1 ? 72 : 32))
     k_identify(const uint8_t* __restrict__ img, size_t pitch, const IdentTask* __restrict__ tasks, IdentResult* res,
                const float* __restrict__ bankInv, IdentParams ip)
 {
