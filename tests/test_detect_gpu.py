@@ -121,11 +121,18 @@ def test_detect_batch_matches_single_frames(built_library, detector):
     with cctag_b200.Detector(max_w=1920, max_h=1080, max_batch=4) as bd:
         got = bd.detect_batch(frames)
         again = bd.detect_batch(frames[::-1])[::-1]
-    for f, (m, st), (m2, _) in zip(frames, got, again):
+    # two slots for six frames: each slot runs three in turn, and a single
+    # call afterwards is unaffected
+    with cctag_b200.Detector(max_w=1920, max_h=1080, max_batch=2) as bd2:
+        turns = bd2.detect_batch(frames)
+        after, _ = bd2.detect(frames[0])
+    for f, (m, st), (m2, _), (m3, _) in zip(frames, got, again, turns):
         want, _ = detector.detect(f)
         assert _key(m) == _key(want)
         assert _key(m2) == _key(want)
+        assert _key(m3) == _key(want)
         assert st.markers == len(m)
+    assert _key(after) == _key(detector.detect(frames[0])[0])
 
 
 def test_detect_batch_reports_the_failing_frame(built_library):
