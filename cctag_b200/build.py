@@ -32,7 +32,7 @@ NO_FMAD = {"loop_one"}
 def _sources():
     cu = sorted(CSRC.glob("*.cu"))
     cpp = sorted(CSRC.glob("*.cpp"))
-    hdr = sorted(CSRC.glob("*.hpp")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.rglob("*.h"))
+    hdr = sorted(CSRC.glob("*.hpp")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.rglob("*.h")) + sorted(INCLUDE.rglob("*.hpp"))
     return cu, cpp, hdr
 
 

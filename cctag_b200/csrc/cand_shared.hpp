@@ -8,7 +8,7 @@
 #include <cstdint>
 
 #include "geometry.hpp"
-#include "pmath.hpp"
+#include "cctag_b200/portable/pmath.hpp"
 
 #if defined(__CUDACC__)
 #define CCTAGB_UNROLL _Pragma("unroll")

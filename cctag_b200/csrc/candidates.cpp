@@ -486,9 +486,10 @@ bool flow_component_grow(Candidate& c, EdgeSet& es, const cctagb_params& p)
         if (vd.empty()) return false;
         const float SmFinal = geo::median_ref(vd);
         if (SmFinal > p.thrMedianDistanceEllipse) return false;
-        if (quality_of(c.outer.size(), c.outerEllipse) > 1.1f) return false;
+        // the reference's literals are doubles: a float compares with 1.1, 0.05 as a double
+        if (quality_of(c.outer.size(), c.outerEllipse) > 1.1) return false;
         const float ratio = c.outerEllipse.a / c.outerEllipse.b;
-        if (ratio < 0.05f || ratio > 20) return false;
+        if (ratio < 0.05 || ratio > 20) return false;
         return true;
     } catch (...) {
         return false;
@@ -607,10 +608,14 @@ bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& ou
         for (int i = 0; i < 4; ++i) pp[i] = P[perm[i]];
         rng.rand5(perm, aout.size());
         for (int i = 0; i < 4; ++i) pp[4 + i] = AP[perm[i]];
+        // The fit of the eight points sits outside the reference's try block
+        // (Vote.cpp:640-645): a fit that throws ends the whole loop-3
+        // iteration of this candidate, not just the draw.
+        const Ellipse fit8 = geo::fit_ellipse(pp, 8);
         try {
-            const Ellipse q = Ellipse::from_matrix(geo::fit_ellipse(pp, 8).Q);
+            const Ellipse q = Ellipse::from_matrix(fit8.Q);
             const float ratio = q.a / q.b;
-            if (ratio < 0.12f || ratio > 8) {
+            if (ratio < 0.12 || ratio > 8) {
                 ++cnt;
                 continue;
             }
@@ -641,7 +646,7 @@ bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& ou
     std::vector<int> merged = outer;
     merged.insert(merged.end(), aout.begin(), aout.end());
     const Ellipse fitted = fit_points(es, merged);
-    if (!(quality_of(merged.size(), fitted) < 1.1f)) return false;
+    if (!(quality_of(merged.size(), fitted) < 1.1)) return false;
     d.clear();
     for (int q : merged) d.push_back(geo::dist_point_ellipse(fitted.Q, float(es.x(q)), float(es.y(q))));
     const float SmFinal = geo::median_ref(d);
@@ -667,7 +672,7 @@ void flow_component_assembling(EdgeSet& es, float& quality, size_t ci, const std
         const Candidate& o = loop2[i];
         if (c.nLabel == o.nLabel) continue;
         const float ratio = o.flow / c.flow;
-        if (!(ratio > 0.666f && ratio < 1.5f)) continue;
+        if (!(ratio > 0.666 && ratio < 1.5)) continue;
         if (in_ellipse(area, float(es.x(o.seed)), float(es.y(o.seed)))) {
             if (o.score > score) {
                 score = o.score;
@@ -692,12 +697,12 @@ void loop_two_iteration(EdgeSet& es, const std::vector<Candidate>& loop2, size_t
     std::vector<std::vector<DirPoint>> pts;
     try {
         float quality = quality_of(outer.size(), oe);
-        if (p.searchForAnotherSegment && quality > 0.25f && quality < 0.7f)
+        if (p.searchForAnotherSegment && quality > 0.25 && quality < 0.7)
             flow_component_assembling(es, quality, ci, loop2, oe, outer, pts, p, rng);
         if (!add_candidate_flow(es, c.filtered, c.outer, oe, pts, size_t(p.nCrowns) * 2)) return;
         const Ellipse rescale = Ellipse::from_params(oe.cx, oe.cy, oe.a * scale, oe.b * scale, oe.angle);
         const float realSize = quality * float(geo::rasterize_perimeter(rescale));
-        if ((quality <= 0.35f && realSize >= 300.0f) ||
+        if ((quality <= 0.35 && realSize >= 300.0f) ||
             (quality <= 0.45f && realSize >= 200.0f && realSize < 300.0f) ||
             (quality <= 0.5f && realSize >= 100.0f && realSize < 200.0f) ||
             (quality <= 0.5f && realSize >= 70.0f && realSize < 100.0f) ||

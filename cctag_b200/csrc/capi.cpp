@@ -504,17 +504,20 @@ cctagb_status cctagb_wait(cctagb_handle* h, int ticket, cctagb_marker* out, int 
         }
         t = it->second;
         h->sdone.wait(l, [&] { return t->done; });
-        h->tickets.erase(it);
+        // a buffer too small for the markers keeps the ticket: the caller
+        // can wait on it again with *n_out places
+        if (t->status == CCTAGB_OK && t->n > cap) {
+            *n_out = t->n;
+            h->last_error = "marker output capacity too small";
+            return CCTAGB_BAD_ARG;
+        }
+        h->tickets.erase(h->tickets.find(ticket));
     }
     *n_out = t->n;
     if (stats) *stats = t->stats;
     if (t->status != CCTAGB_OK) {
         h->last_error = "frame " + std::to_string(t->frame_id) + ": " + t->msg;
         return t->status;
-    }
-    if (t->n > cap) {
-        h->last_error = "marker output capacity too small";
-        return CCTAGB_BAD_ARG;
     }
     std::copy(t->markers.begin(), t->markers.begin() + t->n, out);
     h->last_error.clear();

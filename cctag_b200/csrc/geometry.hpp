@@ -12,7 +12,7 @@
 #include <stdexcept>
 #include <vector>
 
-#include "pmath.hpp"
+#include "cctag_b200/portable/pmath.hpp"
 
 namespace cctagb {
 namespace geo {
@@ -256,11 +256,11 @@ CCTAGB_HD inline int intersect_line_q(const Mat3& C, float y, bool horizontal, f
     if (horizontal) {
         a = C.m[0][0];
         b = 2 * (y * C.m[0][1] + C.m[0][2]);
-        c = C.m[1][1] * y * y + 2 * y * C.m[2][1] + C.m[2][2];
+        c = C.m[1][1] * (y * y) + 2 * y * C.m[2][1] + C.m[2][2];  // pow<2>(y) first
     } else {
         a = C.m[1][1];
         b = 2 * (y * C.m[0][1] + C.m[1][2]);
-        c = C.m[0][0] * y * y + 2 * y * C.m[0][2] + C.m[2][2];
+        c = C.m[0][0] * (y * y) + 2 * y * C.m[0][2] + C.m[2][2];
     }
     const float disc = b * b / 4.0f - a * c;
     if (disc > 0.f) {

@@ -15,6 +15,10 @@ std::vector<DirPoint> sorted_outer_points(const geo::Ellipse& e, const std::vect
     for (size_t i = 0; i < pts.size(); ++i) ang.emplace_back(std::atan2(pts[i].y - e.cy, pts[i].x - e.cx), i);
     std::sort(ang.begin(), ang.end());
     const size_t nOuter = std::min(requested, pts.size());
+    // With one point the reference's step is a division by zero and the
+    // index size_t(0 * inf) is undefined (on x86 it selects nothing); no cut
+    // can come from fewer than two points, so nothing is selected.
+    if (nOuter < 2) return {};
     const float step = std::max(1.f, float(pts.size()) / float(nOuter - 1));
     std::vector<DirPoint> res;
     res.reserve(nOuter);

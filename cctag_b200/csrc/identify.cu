@@ -28,7 +28,7 @@
 
 #include "common.hpp"
 #include "ident_host.hpp"
-#include "pmath.hpp"
+#include "cctag_b200/portable/pmath.hpp"
 
 namespace cctagb {
 

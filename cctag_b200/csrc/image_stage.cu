@@ -19,8 +19,48 @@
 
 namespace cctagb {
 
-__constant__ float cK[9][9];         // kerneldX of cvRecode.cpp:74-83
-__constant__ uint32_t cThin[2][16];  // thinning tables as bitsets
+// kerneldX of cvRecode.cpp:74-83
+__constant__ float cK[9][9] = {
+    {-0.000000143284235f, -0.000003558691641f, -0.000028902492951f, -0.000064765993382f, 0.f, 0.000064765993382f, 0.000028902492951f, 0.000003558691641f, 0.000000143284235f},
+    {-0.000004744922188f, -0.000117847682078f, -0.000957119116802f, -0.002144755142391f, 0.f, 0.002144755142391f, 0.000957119116802f, 0.000117847682078f, 0.000004744922188f},
+    {-0.000057804985902f, -0.001435678675203f, -0.011660097860113f, -0.026128466569370f, 0.f, 0.026128466569370f, 0.011660097860113f, 0.001435678675203f, 0.000057804985902f},
+    {-0.000259063973527f, -0.006434265427174f, -0.052256933138740f, -0.117099663048638f, 0.f, 0.117099663048638f, 0.052256933138740f, 0.006434265427174f, 0.000259063973527f},
+    {-0.000427124283626f, -0.010608310271112f, -0.086157117207395f, -0.193064705260108f, 0.f, 0.193064705260108f, 0.086157117207395f, 0.010608310271112f, 0.000427124283626f},
+    {-0.000259063973527f, -0.006434265427174f, -0.052256933138740f, -0.117099663048638f, 0.f, 0.117099663048638f, 0.052256933138740f, 0.006434265427174f, 0.000259063973527f},
+    {-0.000057804985902f, -0.001435678675203f, -0.011660097860113f, -0.026128466569370f, 0.f, 0.026128466569370f, 0.011660097860113f, 0.001435678675203f, 0.000057804985902f},
+    {-0.000004744922188f, -0.000117847682078f, -0.000957119116802f, -0.002144755142391f, 0.f, 0.002144755142391f, 0.000957119116802f, 0.000117847682078f, 0.000004744922188f},
+    {-0.000000143284235f, -0.000003558691641f, -0.000028902492951f, -0.000064765993382f, 0.f, 0.000064765993382f, 0.000028902492951f, 0.000003558691641f, 0.000000143284235f}};
+
+// Lam-Lee-Suen sub-iteration tables as bitsets (index = the 3x3 neighbourhood
+// with the weights of thinning.cpp: (x-1,y-1)=1 ... (x+1,y+1)=256): bit set
+// where the pixel stays.  Derived from the thinning conditions at compile time.
+struct ThinTables {
+    uint32_t bits[2][16];
+};
+constexpr ThinTables make_thin_tables()
+{
+    ThinTables t{};
+    for (int pass = 1; pass <= 2; ++pass)
+        for (int idx = 0; idx < 512; ++idx) {
+            if (!(idx & 16)) continue;
+            int x[10] = {0, (idx & 128) ? 1 : 0, (idx & 64) ? 1 : 0, (idx & 8) ? 1 : 0, (idx & 1) ? 1 : 0,
+                         (idx & 2) ? 1 : 0, (idx & 4) ? 1 : 0, (idx & 32) ? 1 : 0, (idx & 256) ? 1 : 0, 0};
+            x[9] = x[1];
+            int xh = 0, n1 = 0, n2 = 0;
+            for (int i = 1; i <= 4; ++i) {
+                xh += (x[2 * i - 1] == 0 && (x[2 * i] == 1 || x[2 * i + 1] == 1)) ? 1 : 0;
+                n1 += x[2 * i - 1] | x[2 * i];
+                n2 += x[2 * i] | x[2 * i + 1];
+            }
+            const int mn = n1 < n2 ? n1 : n2;
+            const bool g1 = xh == 1, g2 = mn >= 2 && mn <= 3;
+            const bool g3 = pass == 1 ? (((x[2] | x[3] | (1 - x[8])) & x[1]) == 0)
+                                      : (((x[6] | x[7] | (1 - x[4])) & x[5]) == 0);
+            if (!(g1 && g2 && g3)) t.bits[pass - 1][idx >> 5] |= 1u << (idx & 31);
+        }
+    return t;
+}
+__constant__ ThinTables cThinTab = make_thin_tables();
 
 // ------------------------------------------------------------------ utils --
 __device__ __forceinline__ int level_of_block(const Levels& lv, int b, int LevelView::*tiles, int& local)
@@ -435,7 +475,7 @@ __global__ void __launch_bounds__(kThX * kThY) k_final_thin(Levels lv)
     const int x0 = (tile % L.thin_tx) * kThX;
     const int y0 = (tile / L.thin_tx) * kThY;
     const int t = threadIdx.y * kThX + threadIdx.x;
-    if (t < 32) s_lut[t >> 4][t & 15] = cThin[t >> 4][t & 15];
+    if (t < 32) s_lut[t >> 4][t & 15] = cThinTab.bits[t >> 4][t & 15];
     for (int i = t; i < (kThY + 4) * (kThX + 4); i += kThX * kThY) {
         const int r = i / (kThX + 4), c = i % (kThX + 4);
         const int x = x0 - 2 + c, y = y0 - 2 + r;
@@ -907,37 +947,9 @@ static int total_of(const Levels& lv, int LevelView::*f)
 
 void upload_constants(const float*, int, int)
 {
-    static const float K[9][9] = {
-        {-0.000000143284235f, -0.000003558691641f, -0.000028902492951f, -0.000064765993382f, 0.f, 0.000064765993382f, 0.000028902492951f, 0.000003558691641f, 0.000000143284235f},
-        {-0.000004744922188f, -0.000117847682078f, -0.000957119116802f, -0.002144755142391f, 0.f, 0.002144755142391f, 0.000957119116802f, 0.000117847682078f, 0.000004744922188f},
-        {-0.000057804985902f, -0.001435678675203f, -0.011660097860113f, -0.026128466569370f, 0.f, 0.026128466569370f, 0.011660097860113f, 0.001435678675203f, 0.000057804985902f},
-        {-0.000259063973527f, -0.006434265427174f, -0.052256933138740f, -0.117099663048638f, 0.f, 0.117099663048638f, 0.052256933138740f, 0.006434265427174f, 0.000259063973527f},
-        {-0.000427124283626f, -0.010608310271112f, -0.086157117207395f, -0.193064705260108f, 0.f, 0.193064705260108f, 0.086157117207395f, 0.010608310271112f, 0.000427124283626f},
-        {-0.000259063973527f, -0.006434265427174f, -0.052256933138740f, -0.117099663048638f, 0.f, 0.117099663048638f, 0.052256933138740f, 0.006434265427174f, 0.000259063973527f},
-        {-0.000057804985902f, -0.001435678675203f, -0.011660097860113f, -0.026128466569370f, 0.f, 0.026128466569370f, 0.011660097860113f, 0.001435678675203f, 0.000057804985902f},
-        {-0.000004744922188f, -0.000117847682078f, -0.000957119116802f, -0.002144755142391f, 0.f, 0.002144755142391f, 0.000957119116802f, 0.000117847682078f, 0.000004744922188f},
-        {-0.000000143284235f, -0.000003558691641f, -0.000028902492951f, -0.000064765993382f, 0.f, 0.000064765993382f, 0.000028902492951f, 0.000003558691641f, 0.000000143284235f}};
-    CCTAGB_CUDA(cudaMemcpyToSymbol(cK, K, sizeof(K)));
-    // Lam-Lee-Suen sub-iteration tables (see thin_lut in the host code).
-    uint32_t bits[2][16] = {};
-    for (int pass = 1; pass <= 2; ++pass)
-        for (int idx = 0; idx < 512; ++idx) {
-            auto bit = [&](int w) { return (idx & w) ? 1 : 0; };
-            if (!bit(16)) continue;
-            const int x[10] = {0, bit(128), bit(64), bit(8), bit(1), bit(2), bit(4), bit(32), bit(256), bit(128)};
-            int xh = 0, n1 = 0, n2 = 0;
-            for (int i = 1; i <= 4; ++i) {
-                xh += (x[2 * i - 1] == 0 && (x[2 * i] == 1 || x[2 * i + 1] == 1)) ? 1 : 0;
-                n1 += x[2 * i - 1] | x[2 * i];
-                n2 += x[2 * i] | x[2 * i + 1];
-            }
-            const int mn = n1 < n2 ? n1 : n2;
-            const bool g1 = xh == 1, g2 = mn >= 2 && mn <= 3;
-            const bool g3 = pass == 1 ? (((x[2] | x[3] | (1 - x[8])) & x[1]) == 0)
-                                      : (((x[6] | x[7] | (1 - x[4])) & x[5]) == 0);
-            if (!(g1 && g2 && g3)) bits[pass - 1][idx >> 5] |= 1u << (idx & 31);
-        }
-    CCTAGB_CUDA(cudaMemcpyToSymbol(cThin, bits, sizeof(bits)));
+    // The tables are initialised statically with the module (cK, cThinTab);
+    // nothing is uploaded, so a context that reloads the module after a
+    // device reset sees them too.
 }
 
 static void launch_pyramid(const Levels& lv, cudaStream_t s, bool fused)

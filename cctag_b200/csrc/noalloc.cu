@@ -17,9 +17,11 @@
 //    CCTAGB_TOO_LARGE;
 //  * the array (about 6.4 MB) is held by every GPU that loads the library,
 //    until the process exits;
-//  * the first call on a device resolves the array's device address
-//    (cudaGetSymbolAddress) and uploads the filter constants, with that device
-//    current; make that first call before any stream capture;
+//  * the first call on a device (in each CUDA context: after a
+//    cudaDeviceReset the next call does it again) resolves the array's device
+//    address with cudaGetSymbolAddress, with that device current; make that
+//    first call before any stream capture.  The filter tables are
+//    initialised statically with the module, so nothing is uploaded;
 //  * all calls share the one array and it keeps the last call's contents:
 //    calls whose GPU work overlaps (different streams, or host threads) race
 //    and give wrong results; serialise them on one stream.
@@ -53,9 +55,29 @@ constexpr size_t kScratchBytes = align_up(kOffBitmap + sizeof(uint32_t) * kBitma
 constexpr int kMaxDevices = 64;
 
 struct DeviceSlot {
-    bool ready = false;
+    void* ctx = nullptr;  // the context the address was resolved in
     uint8_t* base = nullptr;
 };
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link to the
+// driver library): the current context, or nullptr when it cannot be read.
+void* current_context()
+{
+    using GetCtx = int (*)(void**);
+    static GetCtx fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            f = nullptr;
+        }
+        return reinterpret_cast<GetCtx>(f);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 
 std::mutex g_mu;
 DeviceSlot g_slots[kMaxDevices];
@@ -64,8 +86,9 @@ DeviceSlot g_slots[kMaxDevices];
 
 static __device__ __align__(256) uint8_t g_edge_scratch[kScratchBytes];
 
-// Resolves the device address of the scratch array on the current device
-// (once per device) and uploads the filter constants there.
+// Resolves the device address of the scratch array on the current device,
+// once per device and context (a new context after a device reset resolves it
+// again; where the context cannot be read, every call resolves it).
 static uint8_t* scratch_for_current_device(cctagb_status& st)
 {
     int dev = 0;
@@ -74,9 +97,10 @@ static uint8_t* scratch_for_current_device(cctagb_status& st)
         st = CCTAGB_NO_DEVICE;
         return nullptr;
     }
+    void* ctx = current_context();
     std::lock_guard<std::mutex> lock(g_mu);
     DeviceSlot& s = g_slots[dev];
-    if (!s.ready) {
+    if (!s.base || !ctx || s.ctx != ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_edge_scratch);
         if (e != cudaSuccess || !p) {
@@ -84,14 +108,9 @@ static uint8_t* scratch_for_current_device(cctagb_status& st)
             st = CCTAGB_CUDA_ERROR;
             return nullptr;
         }
-        try {
-            upload_constants(nullptr, 0, 0);
-        } catch (const Error& err) {
-            st = err.status;
-            return nullptr;
-        }
+        // the first call may have created the context: read it again
+        s.ctx = ctx ? ctx : current_context();
         s.base = static_cast<uint8_t*>(p);
-        s.ready = true;
     }
     st = CCTAGB_OK;
     return s.base;

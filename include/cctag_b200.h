@@ -33,7 +33,8 @@
  *                                                                  src/cctag/Detection.cpp:69-156,609-627
  *   cctagb_cut_cost        <- costFunctionGlob (forward only in the reference; here with its
  *                             gradient in the center and in H)   src/cctag/Identification.cpp:1122-1158
- *   cctagb_edges_noalloc   <- cvRecodedCanny + thin on caller buffers (no allocation)
+ *   cctagb_edges_noalloc   <- no reference counterpart (the edge stage on caller buffers,
+ *                             allocating nothing)
  *   cctagb_host_frames / cctagb_submit / cctagb_wait
  *                          <- page-locked frames + async upload    src/cctag/cuda/frame.cu:110-148
  */
@@ -202,7 +203,9 @@ cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)
  * once, so that one frame's upload and GPU stages overlap another frame's
  * host stage.  cctagb_wait(ticket) returns that frame's markers, exactly what
  * cctagb_detect returns for it.  The frame memory must stay valid until its
- * ticket has been waited for.  While tickets are outstanding, every other
+ * ticket has been waited for.  When `cap` is smaller than the frame's marker
+ * count, cctagb_wait returns CCTAGB_BAD_ARG with *n_out set to that count and
+ * keeps the ticket, so the caller can wait on it again with a larger buffer.  While tickets are outstanding, every other
  * call that uses the handle's detection slots returns CCTAGB_BAD_ARG. */
 
 /* n (<= 64) pinned host buffers of max_w * max_h bytes owned by the handle

@@ -1,11 +1,23 @@
+// FP64 cores of the two point fits of the candidate stage, written once for
+// the host and the GPU, and the arithmetic that pins them: the reference
+// solves their small eigen / singular-value problems with Eigen, whose last
+// bits depend on the platform, so this header fixes one sequence of IEEE
+// operations for them.  The library and the CPU oracle both use it; each
+// restates the algorithm around it (point selection, conic parameters,
+// thresholds) on its own.
+//
 // Direct least-squares ellipse fit (Fitting.cpp:89-200 of the reference: the
 // Halir-Flusser reduction of Fitzgibbon's fit, eigen decomposition of the 3x3
-// reduced scatter matrix) written once for the host and the GPU.  The
-// reference solves the eigenproblem with Eigen; here the characteristic cubic
-// is solved in real arithmetic (Cardano with a portable cube root, or the
-// trigonometric form for three real roots), each root polished by Newton, and
-// the eigenvectors taken from cross products of (M - lambda I), in complex
-// arithmetic for a complex pair (the real part, as Eigen's eigenvectors().real()).
+// reduced scatter matrix).  The characteristic cubic is solved in real
+// arithmetic (Cardano with a portable cube root, or the trigonometric form for
+// three real roots), each root polished by Newton, and the eigenvectors taken
+// from cross products of (M - lambda I), in complex arithmetic for a complex
+// pair (the real part, as Eigen's eigenvectors().real()).
+//
+// Algebraic circle fit (Fitting.cpp:329-360): the smallest right singular
+// vector of [x y 1 x^2+y^2], as the eigenvector of the smallest eigenvalue of
+// the 4x4 normal matrix, by cyclic Jacobi rotations.
+//
 // Only +, -, *, /, sqrt and the portable pmath functions are used.
 #pragma once
 
@@ -318,6 +330,75 @@ CCTAGB_HD inline int fit_ellipse_core(PointAt pt, size_t n, float& ocx, float& o
     ob = float(r1);
     oangle = float(angle);
     return kFitOk;
+}
+
+// Symmetric Jacobi eigen decomposition (n <= 4), eigenvectors in columns:
+// cyclic sweeps over (p, q) in row order until the off-diagonal mass is below
+// 1e-28 of the diagonal's (or 1e-300), at most 100 sweeps.
+template <int N>
+CCTAGB_HD inline void jacobi_sym(double A[N][N], double V[N][N], double d[N])
+{
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) V[i][j] = (i == j) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < N; ++i) {
+            diag += A[i][i] * A[i][i];
+            for (int j = i + 1; j < N; ++j) off += A[i][j] * A[i][j];
+        }
+        // converged: off-diagonal below 1e-14 of the diagonal (the absolute
+        // test alone never fires once rounding noise is all that is left)
+        if (off < 1e-300 || off <= 1e-28 * diag) break;
+        for (int p = 0; p < N; ++p)
+            for (int q = p + 1; q < N; ++q) {
+                if (::fabs(A[p][q]) < 1e-300) continue;
+                const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (::fabs(theta) + ::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / ::sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < N; ++k) {
+                    const double akp = A[k][p], akq = A[k][q];
+                    A[k][p] = c * akp - s * akq;
+                    A[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < N; ++k) {
+                    const double apk = A[p][k], aqk = A[q][k];
+                    A[p][k] = c * apk - s * aqk;
+                    A[q][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < N; ++k) {
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for (int i = 0; i < N; ++i) d[i] = A[i][i];
+}
+
+// The circle fit on n points read through `pt(i, x, y)`: center and radius in
+// FP64; false when the radius is not positive (the reference throws).  The
+// normal matrix is summed in point order.
+template <class PointAt>
+CCTAGB_HD inline bool fit_circle_core(PointAt pt, size_t n, double& xc, double& yc, double& r)
+{
+    double A[4][4] = {};
+    for (size_t i = 0; i < n; ++i) {
+        float xf, yf;
+        pt(i, xf, yf);
+        const double row[4] = {xf, yf, 1.0, double(xf) * xf + double(yf) * yf};
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) A[a][b] += row[a] * row[b];
+    }
+    double V[4][4], d[4];
+    jacobi_sym<4>(A, V, d);
+    int k = 0;
+    for (int i = 1; i < 4; ++i)
+        if (d[i] < d[k]) k = i;
+    const double v0 = V[0][k], v1 = V[1][k], v2 = V[2][k], v3 = V[3][k];
+    xc = -0.5 * v0 / v3;
+    yc = -0.5 * v1 / v3;
+    r = ::sqrt(xc * xc + yc * yc - v2 / v3);
+    return r > 0.0;
 }
 
 }  // namespace geo

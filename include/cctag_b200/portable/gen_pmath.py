@@ -7,7 +7,7 @@ polynomial fitted here (least squares on Chebyshev nodes against 50-digit
 mpmath values), then rounds once to float; both compilers then perform the
 same IEEE operations in the same order.
 
-    python cctag_b200/csrc/gen_pmath.py      # prints the coefficient tables
+    python include/cctag_b200/portable/gen_pmath.py      # prints the coefficient tables
 """
 import mpmath
 import numpy as np

@@ -17,12 +17,12 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
-# The host candidate stage is shared with the product library (it is host
-# code in both); its sources are compiled in from the package.
-PKG_CSRC = HERE.parent / "cctag_b200" / "csrc"
-SOURCES = sorted(HERE.glob("*.cpp")) + [PKG_CSRC / "candidates.cpp", PKG_CSRC / "geometry.cpp"]
-HEADERS = sorted(HERE.glob("*.h")) + sorted(HERE.glob("*.hpp")) + sorted(PKG_CSRC.glob("*.hpp"))
+# Only this directory's sources; from include/ the public C header (the
+# parameter struct and status codes) and the FP64 fit cores of
+# include/cctag_b200/portable/ (the arithmetic that stands in for Eigen).
+SOURCES = sorted(HERE.glob("*.cpp"))
 INCLUDE = HERE.parent / "include"
+HEADERS = sorted(HERE.glob("*.h")) + sorted(HERE.glob("*.hpp")) + sorted(INCLUDE.rglob("*.h*"))
 FLAGS = ["-O3", "-std=c++17", "-fPIC", "-shared", "-mavx2", "-mfma", "-ffp-contract=off", "-Wall", "-pthread"]
 
 

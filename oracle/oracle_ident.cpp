@@ -8,10 +8,8 @@
 // oracle image stage and vote (oracle_image.cpp), the candidate stage, this
 // identification, duplicate removal and sort (Detection.cpp:773-999).
 //
-// The candidate stage (flow components, ellipse growing and fitting) is host
-// code that the product library also runs on the CPU; it is compiled in here
-// from the product's own source (cctag_b200/csrc/candidates.cpp), so the
-// oracle's end-to-end result checks the GPU stages, not that host stage.
+// The candidate stage (flow components, ellipse growing and fitting) is the
+// oracle's own restatement (oracle_candidates.cpp).
 //
 // Identification is a template on the scalar type: with float it follows the
 // reference's FP32 arithmetic and evaluation order (pairwise cut differences
@@ -27,14 +25,13 @@
 
 #include "oracle.h"
 #include "oracle_internal.hpp"
-#include "../cctag_b200/csrc/bank_data.hpp"
-#include "../cctag_b200/csrc/candidates.hpp"
+#include "oracle_bank.hpp"
+#include "oracle_cand.hpp"
 
 namespace orc {
 
-using cctagb::DirPoint;
-using cctagb::MarkerCand;
-namespace geo = cctagb::geo;
+using DirPoint = DPt;
+using MarkerCand = Marker;
 
 template <class T>
 struct M3T {
@@ -435,13 +432,14 @@ bool cut_interp(const uint8_t* img, int W, int H, float sx, float sy, float ex, 
 int identify_step1(const MarkerCand& m, const uint8_t* img, int W, int H, const cctagb_params& p,
                    std::vector<std::pair<float, float>>& stops)
 {
-    const geo::Ellipse& e = m.rescaled;
+    const gm::Ellipse& e = m.rescaled;
     const auto& pts = m.rescaled_points;
     // Ellipse.cpp:259-300
     std::vector<std::pair<float, size_t>> ang;
     for (size_t i = 0; i < pts.size(); ++i) ang.emplace_back(std::atan2(pts[i].y - e.cy, pts[i].x - e.cx), i);
     std::sort(ang.begin(), ang.end());
     const size_t nOuter = std::min(size_t(p.nSamplesOuterEllipse), pts.size());
+    if (nOuter < 2) return CCTAGB_TOO_FEW_OUTER_POINTS;  // the step would divide by zero
     const float stepO = std::max(1.f, float(pts.size()) / float(nOuter - 1));
     std::vector<DirPoint> outer;
     for (size_t k = 0;; ++k) {
@@ -531,12 +529,12 @@ int identify_step1(const MarkerCand& m, const uint8_t* img, int W, int H, const 
 // CCTag::isEqual (CCTag.cpp:42-57) and update (Multiresolution.cpp:172-193)
 bool overlap(const MarkerCand& A, const MarkerCand& B)
 {
-    auto inside = [](const geo::Ellipse& big, float x, float y) {
-        const geo::Ellipse e = geo::Ellipse::from_params(big.cx, big.cy, big.b * 0.5f, big.b * 0.5f, big.angle);
-        const float s1 = geo::qform(e.Q, x, y);
-        const float q0 = e.Q.m[0][0] * e.cx + e.Q.m[0][1] * e.cy + e.Q.m[0][2];
-        const float q1 = e.Q.m[1][0] * e.cx + e.Q.m[1][1] * e.cy + e.Q.m[1][2];
-        const float q2 = e.Q.m[2][0] * e.cx + e.Q.m[2][1] * e.cy + e.Q.m[2][2];
+    auto inside = [](const gm::Ellipse& big, float x, float y) {
+        const gm::Ellipse e = gm::ellipse_from_params(big.cx, big.cy, big.b * 0.5f, big.b * 0.5f, big.angle);
+        const float s1 = gm::quad(e.Q, x, y);
+        const float q0 = e.Q.v[0][0] * e.cx + e.Q.v[0][1] * e.cy + e.Q.v[0][2];
+        const float q1 = e.Q.v[1][0] * e.cx + e.Q.v[1][1] * e.cy + e.Q.v[1][2];
+        const float q2 = e.Q.v[2][0] * e.cx + e.Q.v[2][1] * e.cy + e.Q.v[2][2];
         return s1 * (x * q0 + y * q1 + q2) > 0;
     };
     return inside(A.rescaled, B.rescaled.cx, B.rescaled.cy) || inside(B.rescaled, A.rescaled.cx, A.rescaled.cy);
@@ -563,12 +561,12 @@ struct StepOneRec {
 }  // namespace orc
 
 static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* pp, int fp64, orc_marker* out, int cap,
-                       std::vector<orc::StepOneRec>* rec, std::vector<cctagb::LoopTwoIn>* l2 = nullptr)
+                       std::vector<orc::StepOneRec>* rec, std::vector<orc::LoopTwoRecord>* l2 = nullptr)
 {
     using namespace orc;
     const cctagb_params& p = *pp;
     std::vector<std::vector<float>> bank;
-    for (const auto& row : cctagb::kThreeCrownsBank) bank.emplace_back(row, row + 5);
+    for (const auto& row : kBankThreeCrowns) bank.emplace_back(row, row + 5);
     const int nl = p.numberOfProcessedMultiresLayers;
     std::vector<std::vector<uint8_t>> lvl(nl);
     std::vector<int> lw(nl), lh(nl);
@@ -581,13 +579,8 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
         lvl[l].resize(size_t(lw[l]) * lh[l]);
         pyramid_down(lvl[l - 1].data(), lw[l - 1], lh[l - 1], lvl[l].data(), lw[l], lh[l]);
     }
-    struct LevelData {
-        std::vector<int32_t> exy, grad, before, after, voff, vlist, seeds;
-        std::vector<float> flow;
-        int E = 0;
-    };
-    std::vector<LevelData> ld(nl);
-    std::vector<cctagb::EdgeSet> es(nl);
+    std::vector<EdgeCollection> ec(static_cast<size_t>(nl));
+    std::vector<std::vector<int>> seeds(static_cast<size_t>(nl));
     std::vector<MarkerCand> markers;
     const float lo = p.cannyThrLow * 256.f, hi = p.cannyThrHigh * 256.f;
     for (int l = 0; l < nl; ++l) {
@@ -607,56 +600,21 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
         const int E = vote(e.data(), dx.data(), dy.data(), w, h, vp, cap_e, x.data(), y.data(), b.data(), a.data(),
                            ch.data(), tot.data(), nv.data(), im.data(), fl.data(), vo.data(), vl.data(), sp.data(),
                            ss.data(), &ns);
-        LevelData& L = ld[l];
-        L.E = E;
-        L.exy.resize(E);
-        L.grad.resize(E);
-        for (int i = 0; i < E; ++i) {
-            L.exy[i] = x[i] | (y[i] << 16);
-            const size_t q = size_t(y[i]) * w + x[i];
-            L.grad[i] = int32_t(uint16_t(dx[q])) | (int32_t(dy[q]) << 16);
-        }
-        L.before.assign(b.begin(), b.begin() + E);
-        L.after.assign(a.begin(), a.begin() + E);
-        L.voff.assign(vo.begin(), vo.begin() + E + 1);
-        L.vlist.assign(vl.begin(), vl.begin() + vo[E]);
-        L.flow.assign(fl.begin(), fl.begin() + E);
-        L.seeds.assign(ss.begin(), ss.begin() + ns);
-        cctagb::EdgeSet& S = es[l];
-        S.W = w;
-        S.H = h;
-        S.E = E;
-        S.exy = L.exy.data();
-        S.grad = L.grad.data();
-        S.before = L.before.data();
-        S.after = L.after.data();
-        S.voff = L.voff.data();
-        S.vlist = L.vlist.data();
-        S.flow = L.flow.data();
-        S.index_points();
-        S.reset_state();
-    }
-    std::vector<cctagb::LevelJob> jobs(nl);
-    for (int l = 0; l < nl; ++l) {
-        jobs[l].es = &es[l];
-        jobs[l].seeds = &ld[l].seeds;
-        jobs[l].level = l;
-        jobs[l].scale = float(1 << l);
+        ec[size_t(l)].build(w, h, x.data(), y.data(), dx.data(), dy.data(), E, b.data(), a.data(), vo.data(), vl.data(),
+                            fl.data());
+        seeds[size_t(l)].assign(ss.begin(), ss.begin() + ns);
     }
     if (l2) {  // loop 1 and the outlier removal only
-        cctagb::link_and_filter(jobs, p, [](int n, const std::function<void(int)>& f) {
-            for (int i = 0; i < n; ++i) f(i);
-        }, *l2);
+        l2->assign(size_t(nl), {});
+        std::vector<MarkerCand> none;
+        for (int l = 0; l < nl; ++l)
+            candidates_from_edges(ec[size_t(l)], seeds[size_t(l)], l, float(1 << l), p, none, &(*l2)[size_t(l)]);
         return 0;
     }
-    cctagb::detect_from_edges(jobs, p, [](int n, const std::function<void(int)>& f) {
-        for (int i = 0; i < n; ++i) f(i);
-    });
+    // Multiresolution.cpp:272-300: levels from the coarsest down
     for (int l = nl - 1; l >= 0; --l)
-        for (auto& m : jobs[l].out) markers.push_back(m);
-    cctagb::refit_on_level0(es[0], markers, [](int n, const std::function<void(int)>& f) {
-        for (int i = 0; i < n; ++i) f(i);
-    });
+        candidates_from_edges(ec[size_t(l)], seeds[size_t(l)], l, float(1 << l), p, markers, nullptr);
+    refit_on_level0(ec[0], markers);
     if (p.doIdentification) {
         for (auto& m : markers) {
             std::vector<std::pair<float, float>> stops;
@@ -667,7 +625,7 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
             IdentOut r;
             if (fp64) {
                 Ell<double> e{m.rescaled.cx, m.rescaled.cy, m.rescaled.a, m.rescaled.b, m.rescaled.angle, {}};
-                for (int k = 0; k < 9; ++k) e.Q.m[k] = m.rescaled.Q.m[k / 3][k % 3];
+                for (int k = 0; k < 9; ++k) e.Q.m[k] = m.rescaled.Q.v[k / 3][k % 3];
                 // recompute the conic in FP64 from the parameters
                 {
                     const double c = std::cos(e.angle), s = std::sin(e.angle);
@@ -683,7 +641,7 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
                 r = identify_step2<double>(gray, W, H, e, m.cx_img, m.cy_img, stops, p, bank);
             } else {
                 Ell<float> e{m.rescaled.cx, m.rescaled.cy, m.rescaled.a, m.rescaled.b, m.rescaled.angle, {}};
-                for (int k = 0; k < 9; ++k) e.Q.m[k] = m.rescaled.Q.m[k / 3][k % 3];
+                for (int k = 0; k < 9; ++k) e.Q.m[k] = m.rescaled.Q.v[k / 3][k % 3];
                 r = identify_step2<float>(gray, W, H, e, m.cx_img, m.cy_img, stops, p, bank);
             }
             m.status = r.status;
@@ -691,7 +649,7 @@ static int detect_impl(const uint8_t* gray, int W, int H, const cctagb_params* p
             m.cy_img = float(r.y);
             m.quality = float(1.0 / r.residual);
             if (r.status != CCTAGB_OPTI_HAS_DIVERGED) m.id = r.id;
-            for (int k = 0; k < 9; ++k) m.H.m[k / 3][k % 3] = float(r.H[k]);
+            for (int k = 0; k < 9; ++k) m.H[k] = float(r.H[k]);
         }
     }
     std::vector<MarkerCand> pre, fin;
@@ -748,10 +706,10 @@ extern "C" int orc_loop_two(const uint8_t* gray, int W, int H, const cctagb_para
                             int32_t* seed, int32_t* score, int32_t* keep, int32_t* n_filtered, int filtered_cap,
                             int32_t* filtered, int* n_filtered_total)
 {
-    std::vector<cctagb::LoopTwoIn> l2;
+    std::vector<orc::LoopTwoRecord> l2;
     detect_impl(gray, W, H, pp, 0, nullptr, 0, nullptr, &l2);
     if (level < 0 || level >= int(l2.size())) return -1;
-    const cctagb::LoopTwoIn& g = l2[size_t(level)];
+    const orc::LoopTwoRecord& g = l2[size_t(level)];
     const int n = int(g.seed.size());
     if (n > cap || int(g.flt.size()) > filtered_cap) return -1;
     for (int i = 0; i < n; ++i) {

@@ -6,7 +6,7 @@
 #include <cstdio>
 #include <cstring>
 
-#include "pmath.hpp"
+#include "cctag_b200/portable/pmath.hpp"
 
 int main()
 {

@@ -8,7 +8,7 @@
 #include <cstring>
 #include <random>
 
-#include "pmath.hpp"
+#include "cctag_b200/portable/pmath.hpp"
 
 using namespace cctagb::pm;
 

@@ -1,17 +1,21 @@
 """Regenerate the golden fixtures in this directory.
 
 Sources:
-  * the reference CCTag sources (read as text, when present): the two thinning
-    tables of ``src/cctag/filter/thinning.cpp:12-13`` and the 3-crown bank of
-    ``src/cctag/CCTagMarkersBank.cpp:120-152``;
+  * the reference CCTag sources, read as text: the two thinning tables of
+    ``src/cctag/filter/thinning.cpp:12-13``, the 3-crown bank of
+    ``src/cctag/CCTagMarkersBank.cpp:120-152``, and the point sets and expected
+    outcomes of the reference's ellipse-fit and ellipse-representation unit
+    tests (``src/cctag/test/fitEllipse.cpp``,
+    ``src/cctag/geometry/test/ellipse.cpp``);
   * OpenCV (``cv2``, the installed stand-in for the reference's OpenCV 4.5.3):
     ``cv2.filter2D`` with the reference's 9x9 derivative kernel and
     ``cv2.resize`` (INTER_LINEAR), on seeded images.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference
 """
 from __future__ import annotations
 
+import json
 import re
 import sys
 from pathlib import Path
@@ -19,7 +23,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+REF: Path = Path(".")
 
 KERNEL_ROWS = """
 -0.000000143284235 -0.000003558691641 -0.000028902492951 -0.000064765993382 0 0.000064765993382 0.000028902492951 0.000003558691641 0.000000143284235
@@ -71,11 +75,49 @@ def opencv_cases():
     return cases
 
 
+def _points(body):
+    return [[float(x), float(y)] for x, y in re.findall(r"emplace_back\(\s*([-0-9.]+)f?\s*,\s*([-0-9.]+)f?\s*\)", body)]
+
+
+def reference_fit_cases():
+    """The reference's fit known-answer tests: for each case its points and
+    whether the fit must succeed with the points' mass center inside the
+    ellipse ("inside") or throw std::domain_error ("throw")."""
+    src = (REF / "src/cctag/test/fitEllipse.cpp").read_text()
+    cases = []
+    for name, body in re.findall(r"BOOST_AUTO_TEST_CASE\((\w+)\)\s*\{(.*?)\n\}", src, re.S):
+        live = "\n".join(l for l in body.splitlines() if not l.strip().startswith("//"))
+        if name == "test_throw_5points":  # 0 to 4 copies of (5, 0)
+            for i in range(5):
+                cases.append({"name": f"{name}_{i}", "points": [[5.0, 0.0]] * i, "expect": "throw"})
+            continue
+        if "fit_and_check_ellipse" in live:
+            expect = "inside"
+        elif "THROW" in live:
+            expect = "throw"
+        else:
+            continue  # the case the reference disabled (its assertion is commented out)
+        pts = _points(body)
+        loop = re.search(r"for \(int j = 0; j < (\d+); \+\+j\)", live)
+        if loop and len(pts) == 1:  # one point pushed in a loop
+            pts = pts * int(loop.group(1))
+        cases.append({"name": name, "points": pts, "expect": expect})
+    ell = (REF / "src/cctag/geometry/test/ellipse.cpp").read_text()
+    gt = {k: float(v) for k, v in re.findall(r"const float (\w+GT) = ([-0-9.]+)f;", ell)}
+    return {"fit": cases, "representation": {"points": _points(ell), "aGT": gt["aGT"], "bGT": gt["bGT"],
+                                             "cxGT": gt["cxGT"], "cyGT": gt["cyGT"], "numTrials": 10}}
+
+
 def main():
+    global REF
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    REF = Path(sys.argv[1])
+    (HERE / "reference_geometry_cases.json").write_text(json.dumps(reference_fit_cases(), indent=1))
     lut1, lut2, bank = reference_tables()
     np.savez_compressed(HERE / "reference_tables.npz", lutthin1=lut1, lutthin2=lut2, idThreeCrowns=bank)
     np.savez_compressed(HERE / "opencv_cases.npz", **opencv_cases())
-    print("wrote", HERE / "reference_tables.npz", HERE / "opencv_cases.npz")
+    print("wrote", HERE / "reference_tables.npz", HERE / "opencv_cases.npz", HERE / "reference_geometry_cases.json")
 
 
 if __name__ == "__main__":

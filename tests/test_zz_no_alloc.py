@@ -63,6 +63,21 @@ def test_edges_noalloc_matches_image_stage_twice(built_library):
             np.testing.assert_array_equal(g, e, err_msg=name)
 
 
+def test_edges_noalloc_at_the_size_limits(built_library):
+    """Frames of exactly the maximum pixel count with one side at the maximum
+    (4096 x 256 and 256 x 4096), where the scratch array's bitmap words and
+    row counts are at their bounds."""
+    import torch
+
+    stream = torch.cuda.Stream()
+    for w, h in ((4096, 256), (256, 4096)):
+        img = render_frame(w, h, 3, (20, 60), 45, seed=w + h, noise_sigma=6.0).image
+        want = _handle_edges(img)
+        got = _noalloc_edges(img, stream)
+        for name, g, e in zip(("dx", "dy", "edges"), got, want):
+            np.testing.assert_array_equal(g, e, err_msg=f"{w}x{h} {name}")
+
+
 def test_edges_noalloc_rejects_oversized_frames(built_library):
     import torch
 
@@ -72,6 +87,8 @@ def test_edges_noalloc_rejects_oversized_frames(built_library):
     buf = torch.empty(16, dtype=torch.uint8, device="cuda")
     p = C.c_void_p(buf.data_ptr())
     st = lib.cctagb_edges_noalloc(p, 2048, 1024, 2048, C.c_float(0.01), C.c_float(0.04), p, p, p, None, None)
+    assert st == capi.TOO_LARGE
+    st = lib.cctagb_edges_noalloc(p, 4097, 200, 4097, C.c_float(0.01), C.c_float(0.04), p, p, p, None, None)
     assert st == capi.TOO_LARGE
     st = lib.cctagb_edges_noalloc(p, 100, 100, 128, C.c_float(0.01), C.c_float(0.04), p, p, p, None, None)
     assert st == capi.BAD_ARG
