@@ -144,6 +144,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def host_pool():
+    """Process pool (spawn: safe after CUDA is initialised) to render the
+    synthetic inputs over the host cores."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    return ProcessPoolExecutor(max_workers=os.cpu_count() or 1, mp_context=mp.get_context("spawn"))
+
+
 def make_frames(config, n=N_FRAMES, rank=0):
     from cctag_b200.synth import config_frame
 
@@ -348,6 +357,7 @@ def run_b200(args, rank, world, local):
                 "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": peak_src,
                 "note": "achieved = algorithmic bytes / CUDA-event time of the kernel group, frac of measured"}
 
+    c3 = run_c3(args, flush, torch, peak, peak_src) if rank == 0 and not args.no_c3 else None
     c4 = run_c4(args, flush, torch) if rank == 0 and not args.no_c4 else None
     c5 = run_c5(args, torch) if rank == 0 and not args.no_c5 else None
 
@@ -380,6 +390,8 @@ def run_b200(args, rank, world, local):
                         + int(stats.kernel_launches + stats_h.kernel_launches) * n_plain,
         "clocks": clk.summary(),
     }
+    if c3 is not None:
+        line["c3_clutter"] = c3
     if c4 is not None:
         line["c4_cameras"] = c4
     if c5 is not None:
@@ -412,17 +424,22 @@ def run_plain(args, torch, local):
 
 
 def run_c5(args, torch):
-    """Candidate refinement: 4096 candidates (256 distinct crops, r 8-150 px,
-    tilt <= 70 deg, noise 2-12) in one atlas, identified per call with the
-    reference's grid and with Gauss-Newton, and the cost adjoint."""
+    """Candidate refinement (C5): 4096 distinct candidates (crops r 8-150 px,
+    tilt <= 70 deg, noise sigma 2-12) in one device atlas, identified per call
+    with the reference's grid refinement and with Gauss-Newton, their center
+    error against the FP64 oracle (grid continued to 1e-4 px), the cost
+    adjoint's rate, and the adjoint's accuracy (FP64 kernel against central
+    differences of the FP64 oracle cost)."""
     import cctag_b200
+    import oracle
     from cctag_b200 import capi
     from cctag_b200.synth import cut_task_from_marker, refine_atlas
 
-    atlas, crops = refine_atlas(seed=0, n_crops=256)
-    base = [cut_task_from_marker(m, roi, offset=roi[:2]) for m, roi in crops]
-    n_total = 4096
-    tasks = [base[i % len(base)] for i in range(n_total)]
+    with host_pool() as pool:
+        atlas, crops = refine_atlas(seed=0, n_crops=args.c5_candidates,
+                                    map_fn=lambda f, j: pool.map(f, j, chunksize=32))
+    tasks = [cut_task_from_marker(m, roi, local=True) for m, roi in crops]
+    n_total = len(tasks)
     H, W = atlas.shape
     det = cctag_b200.Detector(max_w=640, max_h=480)
     stream = torch.cuda.ExternalStream(det.stream)
@@ -461,33 +478,144 @@ def run_c5(args, torch):
     ms_grid, res_grid = timed(lambda: ident(capi.REFINE_GRID), steps)
     ms_gn, res_gn = timed(lambda: ident(capi.REFINE_GAUSS_NEWTON), steps)
     ms_adj, _ = timed(adjoint, steps)
-    det.close()
-    # agreement of the two refinements on the distinct candidates (the FP64
-    # reference comparison is in the test-suite)
-    egn = [float(np.hypot(a[2] - b[2], a[3] - b[3])) for a, b in zip(res_grid[:len(base)], res_gn[:len(base)])
-           if a[0] == 1 and b[0] == 1]
+
+    # centers against the FP64 oracle, on every candidate
+    dense = [oracle.refine_grid(atlas, t, 1e-4) for t in tasks]
+
+    def errs(res):
+        return [float(np.hypot(r[2] - q[0], r[3] - q[1])) for r, q in zip(res, dense) if r[0] == 1 and q is not None]
 
     def stats(v):
         return {"median_px": round(float(np.median(v)), 4), "p95_px": round(float(np.percentile(v, 95)), 4),
-                "max_px": round(float(np.max(v)), 4)} if v else None
+                "max_px": round(float(np.max(v)), 4), "over_0.02_px": int(sum(x > 0.02 for x in v)),
+                "n": len(v)} if v else None
 
-    ok_grid = sum(1 for r in res_grid[:len(base)] if r[0] == 1)
-    ok_gn = sum(1 for r in res_gn[:len(base)] if r[0] == 1)
-    same_id = sum(1 for a, b in zip(res_grid[:len(base)], res_gn[:len(base)]) if a[0] == 1 and b[0] == 1
-                  and a[1] == b[1])
+    egn_grid = [float(np.hypot(a[2] - b[2], a[3] - b[3])) for a, b in zip(res_grid, res_gn)
+                if a[0] == 1 and b[0] == 1]
+    # adjoint accuracy: the FP64 kernel's center gradient against central
+    # differences (h = 1e-5 px) of the FP64 oracle cost, and the FP32 kernel's
+    # against the FP64 kernel's, on the first 256 candidates off their start
+    nb = min(256, n_total)
+    cen = centers[:nb] + np.float32([0.6, -0.4])
+    c64, g64, h64 = det.cut_cost(d.data_ptr(), W, H, W, tasks[:nb], cen, fp64=True)
+    c32, g32, h32 = det.cut_cost(d.data_ptr(), W, H, W, tasks[:nb], cen)
+    rel_fd, rel_32 = [], []
+    for i, t in enumerate(tasks[:nb]):
+        x, y = float(cen[i, 0]), float(cen[i, 1])
+        fd = []
+        for ddx, ddy in ((1e-5, 0.0), (0.0, 1e-5)):
+            a = oracle.cut_cost(atlas, t, x + ddx, y + ddy)[0]
+            b = oracle.cut_cost(atlas, t, x - ddx, y - ddy)[0]
+            fd.append(None if a is None or b is None else (a - b) / 2e-5)
+        if None in fd or c64[i] >= np.finfo(np.float32).max:
+            continue
+        fd = np.array(fd)
+        rel_fd.append(float(np.linalg.norm(g64[i] - fd) / np.linalg.norm(fd)))
+        rel_32.append(float(np.linalg.norm(g32[i] - g64[i]) / np.linalg.norm(g64[i])))
+    det.close()
+
+    ok_grid = sum(1 for r in res_grid if r[0] == 1)
+    ok_gn = sum(1 for r in res_gn if r[0] == 1)
+    same_id = sum(1 for a, b in zip(res_grid, res_gn) if a[0] == 1 and b[0] == 1 and a[1] == b[1])
     return {
-        "candidates_per_call": n_total, "distinct": len(base), "atlas": f"{W}x{H}",
+        "candidates_per_call": n_total, "distinct": n_total, "atlas": f"{W}x{H}",
         "grid": {"candidates_per_s": round(n_total / (ms_grid * 1e-3), 1), "ms_per_call": round(ms_grid, 3),
-                 "identified": ok_grid},
+                 "identified": ok_grid, "vs_fp64_oracle": stats(errs(res_grid)),
+                 "mean_rounds": round(float(np.mean([r[4] for r in res_grid])), 2)},
         "gauss_newton": {"candidates_per_s": round(n_total / (ms_gn * 1e-3), 1), "ms_per_call": round(ms_gn, 3),
-                         "identified": ok_gn, "vs_grid": stats(egn),
+                         "identified": ok_gn, "vs_fp64_oracle": stats(errs(res_gn)), "vs_grid": stats(egn_grid),
                          "same_id_as_grid": same_id,
-                         "mean_iterations": round(float(np.mean([r[4] for r in res_gn[:len(base)]])), 2)},
+                         "mean_evaluations": round(float(np.mean([r[4] for r in res_gn])), 2)},
         "adjoint": {"candidates_per_s": round(n_total / (ms_adj * 1e-3), 1), "ms_per_call": round(ms_adj, 3),
-                    "note": "cctagb_cut_cost: cost + d/dcenter + d/dH per candidate"},
+                    "note": "cctagb_cut_cost: cost + d/dcenter + d/dH per candidate (FP32)",
+                    "fp64_kernel_vs_central_differences": {
+                        "median_rel": float(f"{np.median(rel_fd):.3g}"), "max_rel": float(f"{np.max(rel_fd):.3g}"),
+                        "n": len(rel_fd), "h_px": 1e-5},
+                    "fp32_kernel_vs_fp64_kernel": {"median_rel": float(f"{np.median(rel_32):.3g}"),
+                                                   "max_rel": float(f"{np.max(rel_32):.3g}")}},
         "speedup_gn_vs_grid": round(ms_grid / ms_gn, 2),
-        "note": "cctagb_identify_tasks on one device atlas; tasks from the rendered outer ellipses (22 cuts)",
+        "note": "cctagb_identify_tasks on one device atlas of distinct rendered crops; tasks from the rendered "
+                "outer ellipses (22 cuts), started at the ellipse center",
     }
+
+
+def _c3_frame(seed):
+    from cctag_b200.synth import config_frame
+
+    return config_frame("c3_4k_clutter", seed=seed).image
+
+
+def run_c3(args, flush, torch, peak, peak_src):
+    """4K clutter (C3): 3840x2160 frames with 30 markers, 200 distractor
+    ellipses and 300 line segments (1-3 M Canny edge points).  Frames/s of a
+    4-frame batch per call, the edge points and votes, per-stage GB/s and the
+    roofline of the dominant image-stage kernel group, and the CPU baseline."""
+    import cctag_b200
+    from cctag_b200 import capi
+
+    seeds = [300, 301, 302, 303]
+    with host_pool() as pool:
+        frames = list(pool.map(_c3_frame, seeds))
+    H, W = frames[0].shape
+    det = cctag_b200.Detector(max_w=W, max_h=H, max_batch=SLOTS)
+    stream = torch.cuda.ExternalStream(det.stream)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d = [torch.from_numpy(f).to(dev) for f in frames]
+    cap = 512
+    outs = [(capi.Marker * cap)() for _ in frames]
+    fr = (capi.Frame * len(frames))()
+    for i, t in enumerate(d):
+        fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch, fr[i].is_device, fr[i].frame_id = t.data_ptr(), W, H, W, 1, i
+        fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
+        fr[i].cap = cap
+    for _ in range(args.warmup):
+        det._check(det._lib.cctagb_detect_batch(det._h, fr, len(frames)), "detect_batch")
+    steps = max(5, min(args.steps, 20))
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        det._check(det._lib.cctagb_detect_batch(det._h, fr, len(frames)), "detect_batch")
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    fps = steps * len(frames) / (total * 1e-3)
+    # per-stage device times of one frame's image stage (separate eager pass)
+    det.set_stage_timing(True)
+    acc = {}
+    for i in range(max(3, min(args.steps, 10))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        _, st = det.detect_device(d[i % len(d)].data_ptr(), W, H, W)
+        for k, v in det.stage_times().items():
+            acc.setdefault(k, []).append(v)
+    det.set_stage_timing(False)
+    _, st = det.detect_device(d[0].data_ptr(), W, H, W)
+    levels = [det.level_size(l) for l in range(4)]
+    E = [st.edge_points[l] for l in range(4)]
+    S = [st.seeds[l] for l in range(4)]
+    V = [int(len(det.votes(l)["vlist"])) for l in range(4)]
+    det.close()
+    stage_ms = {k: statistics.median(v) for k, v in acc.items()}
+    sb = stage_bytes(levels, E, S, V)
+    stages = {k: {"ms": round(stage_ms[k], 5), "bytes": sb[k],
+                  "GB_s": round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) if stage_ms[k] > 0 else None}
+              for k in sb}
+    top = max(stage_ms, key=lambda k: stage_ms[k])
+    ach = sb[top] / (stage_ms[top] * 1e-3) / 1e9
+    out = {"value": round(fps, 2), "unit": UNIT, "steps": steps, "frames_per_step": len(frames),
+           "frame": f"{W}x{H}", "edge_points": E, "votes": V, "seeds": S,
+           "markers": int(sum(fr[i].n_out for i in range(len(frames)))),
+           "image_stage_ms": round(sum(stage_ms.values()), 4), "stages": stages,
+           "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(ach / peak, 4), "peak_source": peak_src},
+           "note": "cctagb_detect_batch of 4 distinct frames per call, frames in device memory"}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(frames[:2], budget_s=min(args.cpu_budget, 10.0), threads=1)
+    return out
 
 
 def run_c4(args, flush, torch):
@@ -496,39 +624,48 @@ def run_c4(args, flush, torch):
     from cctag_b200 import capi
     from cctag_b200.synth import camera_batch
 
-    cams = [f.image for f in camera_batch(seed=0, n=BATCH)]
+    with host_pool() as pool:
+        batches = [[f.image for f in camera_batch(seed=s, n=BATCH, map_fn=pool.map)] for s in range(2)]
     det = cctag_b200.Detector(max_w=3840, max_h=2160, max_batch=SLOTS)
     stream = torch.cuda.ExternalStream(det.stream)
     dev = torch.device("cuda", torch.cuda.current_device())
-    d = [torch.from_numpy(c).to(dev) for c in cams]
     cap = 512
-    outs = [(capi.Marker * cap)() for _ in cams]
-    fr = (capi.Frame * len(cams))()
-    for i, t in enumerate(d):
-        h, w = t.shape
-        fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch, fr[i].is_device, fr[i].frame_id = t.data_ptr(), w, h, w, 1, i
-        fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
-        fr[i].cap = cap
-    for _ in range(args.warmup):
-        det._check(det._lib.cctagb_detect_batch(det._h, fr, len(cams)), "detect_batch")
-    steps = max(3, min(args.steps, 10))
-    total, per_frame = 0.0, []
-    for _ in range(steps):
+    dev_batches, frs, outs = [], [], []
+    for cams in batches:
+        d = [torch.from_numpy(c).to(dev) for c in cams]
+        o = [(capi.Marker * cap)() for _ in cams]
+        fr = (capi.Frame * len(cams))()
+        for i, t in enumerate(d):
+            h, w = t.shape
+            fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch, fr[i].is_device, fr[i].frame_id = t.data_ptr(), w, h, w, 1, i
+            fr[i].out = C.cast(o[i], C.POINTER(capi.Marker))
+            fr[i].cap = cap
+        dev_batches.append(d)
+        frs.append(fr)
+        outs.append(o)
+    for k in range(args.warmup):
+        for fr in frs:
+            det._check(det._lib.cctagb_detect_batch(det._h, fr, BATCH), "detect_batch")
+    steps = max(100, args.steps)
+    total, per_frame, markers = 0.0, [], 0
+    for k in range(steps):
+        fr = frs[k % len(frs)]
         flush.zero_()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        det._check(det._lib.cctagb_detect_batch(det._h, fr, len(cams)), "detect_batch")
+        det._check(det._lib.cctagb_detect_batch(det._h, fr, BATCH), "detect_batch")
         e1.record(stream)
         e1.synchronize()
         total += e0.elapsed_time(e1)
-        per_frame += [fr[i].stats.ms_total for i in range(len(cams))]
+        per_frame += [fr[i].stats.ms_total for i in range(BATCH)]
+        markers += int(sum(fr[i].n_out for i in range(BATCH)))
     det.close()
-    sizes = sorted({f"{c.shape[1]}x{c.shape[0]}" for c in cams})
-    return {"value": round(steps * len(cams) / (total * 1e-3), 2), "unit": UNIT, "steps": steps,
-            "frames_per_step": len(cams), "resolutions": sizes,
-            "markers": int(sum(fr[i].n_out for i in range(len(cams)))),
+    sizes = sorted({f"{c.shape[1]}x{c.shape[0]}" for cams in batches for c in cams})
+    return {"value": round(steps * BATCH / (total * 1e-3), 2), "unit": UNIT, "steps": steps,
+            "frames_per_step": BATCH, "distinct_frames": BATCH * len(batches), "resolutions": sizes,
+            "markers_per_step": round(markers / steps, 1),
             "frame_p50_ms": round(statistics.median(per_frame), 3),
             "frame_p99_ms": round(float(np.percentile(per_frame, 99)), 3),
             "note": "cctagb_detect_batch, frames in device memory; per-frame latency = host wall time of the "
@@ -604,7 +741,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the multi-camera (mixed resolution) leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the candidate-refinement leg")
-    ap.add_argument("--leg", default="all", choices=["all", "plain", "c4", "c5"],
+    ap.add_argument("--no-c3", action="store_true", help="skip the 4K clutter leg")
+    ap.add_argument("--c5-candidates", type=int, default=4096, help="distinct candidates of the refinement leg")
+    ap.add_argument("--leg", default="all", choices=["all", "plain", "c3", "c4", "c5"],
                     help="run one secondary leg alone and print its object (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -624,6 +763,12 @@ def main():
             print(json.dumps({"c5_refine": run_c5(args, torch)}))
         elif args.leg == "plain":
             print(json.dumps({"plain": run_plain(args, torch, local)}))
+        elif args.leg == "c3":
+            flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+            peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \
+                if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+            print(json.dumps({"c3_clutter": run_c3(args, flush, torch, peaks.get("hbm_gbs", 6650.0),
+                                                   "measured" if "hbm_gbs" in peaks else "fallback")}))
         else:
             flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
             print(json.dumps({"c4_cameras": run_c4(args, flush, torch)}))

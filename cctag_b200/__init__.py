@@ -267,16 +267,17 @@ class Detector:
                                                     out), "identify_tasks")
         return list(out)
 
-    def cut_cost(self, dptr: int, w: int, h: int, pitch: int, tasks, centers: np.ndarray):
-        """cctagb_cut_cost: (cost[n], d_center[n,2], d_h[n,9])."""
+    def cut_cost(self, dptr: int, w: int, h: int, pitch: int, tasks, centers: np.ndarray, fp64: bool = False):
+        """cctagb_cut_cost (or cctagb_cut_cost_f64): (cost[n], d_center[n,2], d_h[n,9])."""
         n = len(tasks)
         arr = (capi.CutTask * n)(*tasks)
         c = np.ascontiguousarray(centers, dtype=np.float32).reshape(n, 2)
         cost = np.zeros(n, np.float32)
         dc = np.zeros((n, 2), np.float32)
         dh = np.zeros((n, 9), np.float32)
-        self._check(self._lib.cctagb_cut_cost(self._h, C.c_void_p(dptr), w, h, pitch, arr, n, capi.ptr(c),
-                                              capi.ptr(cost), capi.ptr(dc), capi.ptr(dh)), "cut_cost")
+        fn = self._lib.cctagb_cut_cost_f64 if fp64 else self._lib.cctagb_cut_cost
+        self._check(fn(self._h, C.c_void_p(dptr), w, h, pitch, arr, n, capi.ptr(c), capi.ptr(cost), capi.ptr(dc),
+                       capi.ptr(dh)), "cut_cost")
         return cost, dc, dh
 
     def detect(self, gray: np.ndarray, frame_id: int = 0, cap: int = 256):

@@ -35,6 +35,7 @@ class Params(C.Structure):
         ("searchForAnotherSegment", C.c_int), ("writeOutput", C.c_int), ("doIdentification", C.c_int),
         ("maxEdges", C.c_uint32), ("refineMode", C.c_int), ("gnIterations", C.c_int),
         ("gnCoarseRounds", C.c_int), ("edgeCapacityDivisor", C.c_int), ("hostThreads", C.c_int),
+        ("gnCoarseGrid", C.c_int), ("gnCoarseNeighbourSize", C.c_float),
     ]
 
 
@@ -69,7 +70,7 @@ MAX_CUTS = 32
 class CutTask(C.Structure):
     _fields_ = [("Q", C.c_float * 9), ("cx", C.c_float), ("cy", C.c_float), ("a", C.c_float), ("b", C.c_float),
                 ("angle", C.c_float), ("x0", C.c_float), ("y0", C.c_float), ("ncuts", C.c_int),
-                ("stop", (C.c_float * 2) * MAX_CUTS), ("roi", C.c_int * 4)]
+                ("stop", (C.c_float * 2) * MAX_CUTS), ("roi", C.c_int * 4), ("local", C.c_int)]
 
 
 class IdentResult(C.Structure):
@@ -97,6 +98,7 @@ SIGNATURES = {
     "cctagb_last_tasks": (_I, [_P, _P, _I, C.POINTER(_I)]),
     "cctagb_identify_tasks": (_I, [_P, _P, _I, _I, _SZ, _P, _I, _I, _P]),
     "cctagb_cut_cost": (_I, [_P, _P, _I, _I, _SZ, _P, _I, _P, _P, _P, _P]),
+    "cctagb_cut_cost_f64": (_I, [_P, _P, _I, _I, _SZ, _P, _I, _P, _P, _P, _P]),
     "cctagb_image_stage": (_I, [_P, _P, _I, _I, _SZ, _I]),
     "cctagb_level_size": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_I)]),
     "cctagb_level_planes": (_I, [_P, _I, _P, _P, _P, _P]),

@@ -218,8 +218,10 @@ void cctagb_params_default(cctagb_params* p, int nCrowns)
     p->maxEdges = 20000;
     p->refineMode = CCTAGB_REFINE_GRID;
     p->gnIterations = 10;
-    p->gnCoarseRounds = 2;
+    p->gnCoarseRounds = 1;
     p->edgeCapacityDivisor = 4;
+    p->gnCoarseGrid = 3;
+    p->gnCoarseNeighbourSize = 0.1f;
 }
 
 const char* cctagb_status_string(cctagb_status s)
@@ -551,6 +553,15 @@ cctagb_status cctagb_cut_cost(cctagb_handle* h, const uint8_t* d_img, int w, int
     if (!h) return CCTAGB_BAD_ARG;
     if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     return guarded(h, [&] { h->det->cut_cost(d_img, w, hgt, pitch, tasks, n, centers, cost, d_center, d_h); });
+}
+
+cctagb_status cctagb_cut_cost_f64(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
+                                  const cctagb_cut_task* tasks, int n, const float* centers, float* cost,
+                                  float* d_center, float* d_h)
+{
+    if (!h) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
+    return guarded(h, [&] { h->det->cut_cost(d_img, w, hgt, pitch, tasks, n, centers, cost, d_center, d_h, true); });
 }
 
 cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)

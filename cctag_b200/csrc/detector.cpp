@@ -104,6 +104,11 @@ IdentParams Detector::ident_params(int refine_mode) const
     ip.refineMode = refine_mode;
     ip.gnIterations = params_.gnIterations;
     ip.coarseRounds = params_.gnCoarseRounds;
+    if (refine_mode == CCTAGB_REFINE_GAUSS_NEWTON) {
+        // the coarse rounds only pick the basin Gauss-Newton then descends
+        ip.gridN = params_.gnCoarseGrid;
+        ip.neighbourSize = params_.gnCoarseNeighbourSize;
+    }
     return ip;
 }
 
@@ -225,7 +230,7 @@ void Detector::identify_tasks(const uint8_t* d_img, int w, int h, size_t pitch, 
 }
 
 void Detector::cut_cost(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
-                        const float* centers, float* cost, float* d_center, float* d_h)
+                        const float* centers, float* cost, float* d_center, float* d_h, bool fp64)
 {
     if (!d_img || (n > 0 && !centers)) throw Error{CCTAGB_BAD_ARG, "bad image or center pointer"};
     check_tasks(tasks, n, w, h, pitch);
@@ -249,7 +254,7 @@ void Detector::cut_cost(const uint8_t* d_img, int w, int h, size_t pitch, const 
     cudaStream_t s = pipe_.stream();
     CCTAGB_CUDA(cudaMemcpyAsync(d_tasks_, h_tasks_, sizeof(IdentTask) * n, cudaMemcpyHostToDevice, s));
     CCTAGB_CUDA(cudaMemcpyAsync(d_centers_, h_cost_, sizeof(float) * 2 * size_t(n), cudaMemcpyHostToDevice, s));
-    launch_cut_cost(d_img, pitch, d_tasks_, d_centers_, d_cost_, n, ident_params(params_.refineMode), s);
+    launch_cut_cost(d_img, pitch, d_tasks_, d_centers_, d_cost_, n, ident_params(params_.refineMode), s, fp64);
     CCTAGB_CUDA(cudaMemcpyAsync(h_cost_, d_cost_, sizeof(float) * 12 * size_t(n), cudaMemcpyDeviceToHost, s));
     CCTAGB_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n; ++i) {

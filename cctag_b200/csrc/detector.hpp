@@ -39,7 +39,7 @@ public:
     void identify_tasks(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
                         int refine_mode, IdentResult* out);
     void cut_cost(const uint8_t* d_img, int w, int h, size_t pitch, const IdentTask* tasks, int n,
-                  const float* centers, float* cost, float* d_center, float* d_h);
+                  const float* centers, float* cost, float* d_center, float* d_h, bool fp64 = false);
     // Tasks handed to the identification kernel by the last detect().
     const std::vector<IdentTask>& last_tasks() const { return last_tasks_; }
     // Loop-two inputs (GPU loop 1 + outlier removal) of the last detect().

@@ -73,7 +73,8 @@ void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_task
                      const float* d_bank_inv, const IdentParams& ip, cudaStream_t s);
 // Cost and adjoints at given centers (cctagb_cut_cost): out is 12 floats per
 // task (cost, d/dcenter x2, d/dH x9).
+// fp64: every step in double precision (the check form of the adjoint).
 void launch_cut_cost(const uint8_t* d_img, size_t pitch, const IdentTask* d_tasks, const float* d_centers,
-                     float* d_out, int n, const IdentParams& ip, cudaStream_t s);
+                     float* d_out, int n, const IdentParams& ip, cudaStream_t s, bool fp64 = false);
 
 }  // namespace cctagb

@@ -95,6 +95,8 @@ struct Roi {
 
 __device__ __forceinline__ Roi make_roi(const uint8_t* img, size_t pitch, const IdentTask& T)
 {
+    if (T.local)  // coordinates relative to the rectangle's corner
+        return Roi{img + size_t(T.roi[1]) * pitch + size_t(T.roi[0]), pitch, 0, 0, T.roi[2], T.roi[3]};
     return Roi{img, pitch, T.roi[0], T.roi[1], T.roi[0] + T.roi[2], T.roi[1] + T.roi[3]};
 }
 
@@ -516,6 +518,82 @@ __device__ __forceinline__ void inverse_derivative(const float* Hi, const float*
     for (int k = 0; k < 9; ++k) dHi[k] = -dHi[k];
 }
 
+// Sample k of a cut for Gauss-Newton at the trial homography S.gH: its value
+// and, in ds, its derivatives along the two center coordinates (through H, and
+// through the back-projected cut end (bx, by) whose derivatives are db).
+__device__ __forceinline__ float gn_sample(const Shared& S, const Roi& roi, float bs, float den, float bx, float by,
+                                          const float db[2][2], int k, float ds[2])
+{
+    const float xs = bx * bs, ys = by * bs;
+    const float sx = (bx - xs) / den, sy = (by - ys) / den;
+    const float kf = float(k);
+    const float x = __fmaf_rn(kf, sx, xs), y = __fmaf_rn(kf, sy, ys);
+    const float t = bs + kf * (1.f - bs) / den;
+    const float* Hm = S.gH;
+    const float u = hrow(Hm, 0, x, y), v = hrow(Hm, 1, x, y), w = hrow(Hm, 2, x, y);
+    const float r = __frcp_rn(w);
+    const float qx = __fmul_rn(u, r), qy = __fmul_rn(v, r);
+    float gx, gy;
+    const float val = bilinear_grad(roi, qx, qy, gx, gy);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const float* dH = S.gdH[q];
+        const float dxq = __fmul_rn(t, db[q][0]), dyq = __fmul_rn(t, db[q][1]);
+        const float du = __fmaf_rn(Hm[0], dxq, __fmaf_rn(Hm[1], dyq, hrow(dH, 0, x, y)));
+        const float dv = __fmaf_rn(Hm[3], dxq, __fmaf_rn(Hm[4], dyq, hrow(dH, 1, x, y)));
+        const float dw = __fmaf_rn(Hm[6], dxq, __fmaf_rn(Hm[7], dyq, hrow(dH, 2, x, y)));
+        const float ex = __fmul_rn(__fmaf_rn(-qx, dw, du), r);
+        const float ey = __fmul_rn(__fmaf_rn(-qy, dw, dv), r);
+        ds[q] = __fmaf_rn(gx, ex, __fmul_rn(gy, ey));
+    }
+    return val;
+}
+
+// The Gauss-Newton sums of one chunk (lane = sample): cost, J^T r and J^T J
+// of the residuals s_ik - mean_k, from per-lane shifted FP32 sums over the
+// valid cuts in cut order, then FP64 over the lanes.  at(c, v, a, b) reads
+// sample value v and its center derivatives a, b of cut c.
+template <class At>
+__device__ __forceinline__ void gn_chunk_sums(uint32_t valid, int n, bool live, double acc[6], At at)
+{
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+    if (live && n >= 2) {
+        float v0 = 0.f, s1 = 0.f, s2 = 0.f, a1 = 0.f, b1 = 0.f, aa = 0.f, ab = 0.f, bb = 0.f, ad = 0.f, bd = 0.f;
+        bool first = true;
+        uint32_t m = valid;
+        while (m) {
+            const int c = __ffs(m) - 1;
+            m &= m - 1;
+            float v, a, b;
+            at(c, v, a, b);
+            if (first) {
+                v0 = v;
+                first = false;
+            }
+            const float d = __fsub_rn(v, v0);
+            s1 = __fadd_rn(s1, d);
+            s2 = __fmaf_rn(d, d, s2);
+            a1 = __fadd_rn(a1, a);
+            b1 = __fadd_rn(b1, b);
+            aa = __fmaf_rn(a, a, aa);
+            ab = __fmaf_rn(a, b, ab);
+            bb = __fmaf_rn(b, b, bb);
+            ad = __fmaf_rn(a, d, ad);
+            bd = __fmaf_rn(b, d, bd);
+        }
+        const float fn = float(n);
+        acc[0] = double(__fsub_rn(__fmul_rn(fn, s2), __fmul_rn(s1, s1)));
+        acc[1] = double(__fsub_rn(ad, __fdiv_rn(__fmul_rn(a1, s1), fn)));
+        acc[2] = double(__fsub_rn(bd, __fdiv_rn(__fmul_rn(b1, s1), fn)));
+        acc[3] = double(__fsub_rn(aa, __fdiv_rn(__fmul_rn(a1, a1), fn)));
+        acc[4] = double(__fsub_rn(ab, __fdiv_rn(__fmul_rn(a1, b1), fn)));
+        acc[5] = double(__fsub_rn(bb, __fdiv_rn(__fmul_rn(b1, b1), fn)));
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] = lane_sum(acc[q]);
+}
+
 // Levenberg-Marquardt on the cut-consistency cost (CCTAGB_REFINE_GAUSS_NEWTON):
 // residuals r_ik = s_ik - mean_k over the valid cuts i and samples k, whose
 // sum of squares is the reference's pair cost up to the factor n / pairs;
@@ -580,82 +658,67 @@ __device__ void gn_refine(Shared& S, const IdentTask& T, const Roi& roi, const I
         const uint32_t valid = ~(S.oob | S.gOob) & cutMask;
         const int n = __popc(valid);
         const int par = it & 1;
-        for (int j = j0; j < j1; ++j) {
-            // this chunk's samples: value and its derivatives along the center
-            const int k = j * kChunk + lane;
+        // One block doing every chunk, with room for all samples: each warp
+        // computes its cuts' samples of every chunk (the back-projected end
+        // once per cut), then warp j sums chunk j.  The per-chunk sums are
+        // the same operations in the same order as the chunk-at-a-time path,
+        // so both give the same bits.
+        const bool whole = CL == 1 && 2 * T.ncuts * nS <= int(sizeof(S.u) / sizeof(float));
+        if (whole) {
+            float* gdx = reinterpret_cast<float*>(&S.u);
+            float* gdy = gdx + T.ncuts * nS;
             for (int c = warp; c < T.ncuts; c += kWarps) {
-                if (!((valid >> c) & 1u) || k >= nS) continue;
+                if (!((valid >> c) & 1u)) continue;
                 float bx, by, db[2][2];
                 back_project(S.gHi, S.gdHi[0], S.gdHi[1], T.stop[c][0], T.stop[c][1], bx, by, db);
-                const float xs = bx * bs, ys = by * bs;
-                const float sx = (bx - xs) / den, sy = (by - ys) / den;
-                const float kf = float(k);
-                const float x = __fmaf_rn(kf, sx, xs), y = __fmaf_rn(kf, sy, ys);
-                const float t = bs + kf * (1.f - bs) / den;
-                const float* Hm = S.gH;
-                const float u = hrow(Hm, 0, x, y), v = hrow(Hm, 1, x, y), w = hrow(Hm, 2, x, y);
-                const float r = __frcp_rn(w);
-                const float qx = __fmul_rn(u, r), qy = __fmul_rn(v, r);
-                float gx, gy;
-                const float val = bilinear_grad(roi, qx, qy, gx, gy);
-                float ds[2];
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    const float* dH = S.gdH[q];
-                    const float dxq = __fmul_rn(t, db[q][0]), dyq = __fmul_rn(t, db[q][1]);
-                    const float du = __fmaf_rn(Hm[0], dxq, __fmaf_rn(Hm[1], dyq, hrow(dH, 0, x, y)));
-                    const float dv = __fmaf_rn(Hm[3], dxq, __fmaf_rn(Hm[4], dyq, hrow(dH, 1, x, y)));
-                    const float dw = __fmaf_rn(Hm[6], dxq, __fmaf_rn(Hm[7], dyq, hrow(dH, 2, x, y)));
-                    const float ex = __fmul_rn(__fmaf_rn(-qx, dw, du), r);
-                    const float ey = __fmul_rn(__fmaf_rn(-qy, dw, dv), r);
-                    ds[q] = __fmaf_rn(gx, ex, __fmul_rn(gy, ey));
+                for (int k = lane; k < nS; k += kChunk) {
+                    float ds[2];
+                    S.sig[c][k] = gn_sample(S, roi, bs, den, bx, by, db, k, ds);
+                    gdx[c * nS + k] = ds[0];
+                    gdy[c * nS + k] = ds[1];
                 }
-                S.u.gn.s[c][lane] = val;
-                S.u.gn.dx[c][lane] = ds[0];
-                S.u.gn.dy[c][lane] = ds[1];
             }
             __syncthreads();
-            if (warp == 0) {
-                double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                if (k < nS && n >= 2) {
-                    float v0 = 0.f, s1 = 0.f, s2 = 0.f, a1 = 0.f, b1 = 0.f, aa = 0.f, ab = 0.f, bb = 0.f, ad = 0.f,
-                          bd = 0.f;
-                    bool first = true;
-                    uint32_t m = valid;
-                    while (m) {
-                        const int c = __ffs(m) - 1;
-                        m &= m - 1;
-                        const float v = S.u.gn.s[c][lane], a = S.u.gn.dx[c][lane], b = S.u.gn.dy[c][lane];
-                        if (first) {
-                            v0 = v;
-                            first = false;
-                        }
-                        const float d = __fsub_rn(v, v0);
-                        s1 = __fadd_rn(s1, d);
-                        s2 = __fmaf_rn(d, d, s2);
-                        a1 = __fadd_rn(a1, a);
-                        b1 = __fadd_rn(b1, b);
-                        aa = __fmaf_rn(a, a, aa);
-                        ab = __fmaf_rn(a, b, ab);
-                        bb = __fmaf_rn(b, b, bb);
-                        ad = __fmaf_rn(a, d, ad);
-                        bd = __fmaf_rn(b, d, bd);
-                    }
-                    const float fn = float(n);
-                    acc[0] = double(__fsub_rn(__fmul_rn(fn, s2), __fmul_rn(s1, s1)));
-                    acc[1] = double(__fsub_rn(ad, __fdiv_rn(__fmul_rn(a1, s1), fn)));
-                    acc[2] = double(__fsub_rn(bd, __fdiv_rn(__fmul_rn(b1, s1), fn)));
-                    acc[3] = double(__fsub_rn(aa, __fdiv_rn(__fmul_rn(a1, a1), fn)));
-                    acc[4] = double(__fsub_rn(ab, __fdiv_rn(__fmul_rn(a1, b1), fn)));
-                    acc[5] = double(__fsub_rn(bb, __fdiv_rn(__fmul_rn(b1, b1), fn)));
-                }
-#pragma unroll
-                for (int q = 0; q < 6; ++q) acc[q] = lane_sum(acc[q]);
+            if (warp < nch) {
+                const int k = warp * kChunk + lane;
+                double acc[6];
+                gn_chunk_sums(valid, n, k < nS, acc, [&](int c, float& v, float& a, float& b) {
+                    v = S.sig[c][k];
+                    a = gdx[c * nS + k];
+                    b = gdy[c * nS + k];
+                });
                 if (lane == 0)
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) S.gPart[par][j][q] = acc[q];
+                    for (int q = 0; q < 6; ++q) S.gPart[par][warp][q] = acc[q];
             }
             __syncthreads();
+        } else {
+            for (int j = j0; j < j1; ++j) {
+                // this chunk's samples: value and its derivatives along the center
+                const int k = j * kChunk + lane;
+                for (int c = warp; c < T.ncuts; c += kWarps) {
+                    if (!((valid >> c) & 1u) || k >= nS) continue;
+                    float bx, by, db[2][2];
+                    back_project(S.gHi, S.gdHi[0], S.gdHi[1], T.stop[c][0], T.stop[c][1], bx, by, db);
+                    float ds[2];
+                    S.u.gn.s[c][lane] = gn_sample(S, roi, bs, den, bx, by, db, k, ds);
+                    S.u.gn.dx[c][lane] = ds[0];
+                    S.u.gn.dy[c][lane] = ds[1];
+                }
+                __syncthreads();
+                if (warp == 0) {
+                    double acc[6];
+                    gn_chunk_sums(valid, n, k < nS, acc, [&](int c, float& v, float& a, float& b) {
+                        v = S.u.gn.s[c][lane];
+                        a = S.u.gn.dx[c][lane];
+                        b = S.u.gn.dy[c][lane];
+                    });
+                    if (lane == 0)
+#pragma unroll
+                        for (int q = 0; q < 6; ++q) S.gPart[par][j][q] = acc[q];
+                }
+                __syncthreads();
+            }
         }
         // every chunk's sums are in; a parity's array is rewritten two
         // evaluations later, past the next barrier of the cluster
@@ -1277,6 +1340,308 @@ __global__ void __launch_bounds__(kThreads) k_cut_cost(const uint8_t* __restrict
     }
 }
 
+namespace {
+
+// ---------------------------------------------------- FP64 check form --
+// The same cost and adjoint as k_cut_cost, every step in double precision:
+// the canonic form, the trial homography with its center derivatives, the
+// back-projected cut ends, the sample positions and the bilinear reads.  It
+// exists to check the adjoint's derivation against central differences at a
+// precision the FP32 kernel cannot reach (FP32 sample positions alone move
+// the cost by ~1e-4 of itself); the refinement kernels do not use it.
+struct D2d {
+    double v, a, b;
+};
+__device__ __forceinline__ D2d operator+(D2d p, D2d q) { return D2d{p.v + q.v, p.a + q.a, p.b + q.b}; }
+__device__ __forceinline__ D2d operator-(D2d p, D2d q) { return D2d{p.v - q.v, p.a - q.a, p.b - q.b}; }
+__device__ __forceinline__ D2d operator*(D2d p, D2d q)
+{
+    return D2d{p.v * q.v, p.a * q.v + p.v * q.a, p.b * q.v + p.v * q.b};
+}
+__device__ __forceinline__ D2d operator/(D2d p, D2d q)
+{
+    const double r = p.v / q.v;
+    return D2d{r, (p.a - r * q.a) / q.v, (p.b - r * q.b) / q.v};
+}
+__device__ __forceinline__ D2d sqrt_d2(D2d p)
+{
+    const double r = sqrt(p.v);
+    return D2d{r, p.a / (2.0 * r), p.b / (2.0 * r)};
+}
+__device__ __forceinline__ D2d cst_d2(double v) { return D2d{v, 0.0, 0.0}; }
+
+__device__ void canonic_form_d(const float* Qf, double* C, double* Tp, double* Td)
+{
+    const double q1 = Qf[0], q2 = Qf[1], q3 = Qf[2], q4 = Qf[4], q5 = Qf[5], q6 = Qf[8];
+    const double par1 = q1, par2 = 2 * q2, par3 = q4, par4 = 2 * q3, par5 = 2 * q5;
+    const double th = 0.5 * atan2(par2, par1 - par3);
+    const double ct = cos(th), st = sin(th);
+    const double s2 = st * st, c2 = ct * ct, cs = st * ct;
+    const double Au = par4 * ct + par5 * st, Av = -par4 * st + par5 * ct;
+    const double Auu = par1 * c2 + par3 * s2 + par2 * cs, Avv = par1 * s2 + par3 * c2 - par2 * cs;
+    const double tu = -Au / (2 * Auu), tv = -Av / (2 * Avv);
+    const double uc = tu * ct - tv * st, vc = tu * st + tv * ct;
+    const double t1 = ct * (ct * q1 + q2 * st) + st * (ct * q2 + q4 * st);
+    const double t2 = ct * (ct * q2 + q4 * st) - st * (ct * q1 + q2 * st);
+    const double t3 = ct * q3 + q5 * st + uc * (ct * q1 + q2 * st) + vc * (ct * q2 + q4 * st);
+    const double t4 = ct * (ct * q4 - q2 * st) - st * (ct * q2 - q1 * st);
+    const double t5 = ct * q5 - q3 * st + uc * (ct * q2 - q1 * st) + vc * (ct * q4 - q2 * st);
+    const double t6 = q6 + uc * (q3 + q1 * uc + q2 * vc) + vc * (q5 + q2 * uc + q4 * vc) + q3 * uc + q5 * vc;
+    const double c[9] = {t1, t2, t3, t2, t4, t5, t3, t5, t6};
+    const double tp[9] = {ct, st, -ct * uc - st * vc, -st, ct, st * uc - ct * vc, 0, 0, ct * ct + st * st};
+    const double td[9] = {ct, -st, uc, st, ct, vc, 0, 0, 1};
+    for (int k = 0; k < 9; ++k) {
+        C[k] = c[k];
+        Tp[k] = tp[k];
+        Td[k] = td[k];
+    }
+}
+
+// homography_from_center in double, with d/d(x, y).
+__device__ void homography_center_derivs_d(const double* C, const double* Tp, const double* Td, double x, double y,
+                                           double* H, double* dHx, double* dHy)
+{
+    const D2d X{x, 1.0, 0.0}, Y{y, 0.0, 1.0};
+    const D2d u = X * cst_d2(Tp[0]) + Y * cst_d2(Tp[1]) + cst_d2(Tp[2]);
+    const D2d v = X * cst_d2(Tp[3]) + Y * cst_d2(Tp[4]) + cst_d2(Tp[5]);
+    const D2d w = X * cst_d2(Tp[6]) + Y * cst_d2(Tp[7]) + cst_d2(Tp[8]);
+    const D2d xc = u / w, yc = v / w;
+    const D2d Q11 = cst_d2(C[0]), Q22 = cst_d2(C[4]), Q33 = cst_d2(C[8]), z = cst_d2(0.0);
+    D2d h[9] = {Q33,          Q22 * xc * yc,           z - Q33 * xc,
+                z,            z - Q11 * xc * xc - Q33, z - Q33 * yc,
+                z - Q11 * xc, Q22 * yc,                z - Q33};
+    const D2d d0 = sqrt_d2(Q22 * Q33 / Q11 * (Q11 * xc * xc + Q22 * yc * yc + Q33));
+    const D2d d2 = sqrt_d2(z - Q22 * (Q11 * xc * xc + Q33));
+    for (int i = 0; i < 3; ++i) {
+        h[i * 3 + 0] = h[i * 3 + 0] * d0;
+        h[i * 3 + 1] = h[i * 3 + 1] * Q33;
+        h[i * 3 + 2] = h[i * 3 + 2] * d2;
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const D2d r = h[j] * cst_d2(Td[i * 3]) + h[3 + j] * cst_d2(Td[i * 3 + 1]) + h[6 + j] * cst_d2(Td[i * 3 + 2]);
+            H[i * 3 + j] = r.v;
+            dHx[i * 3 + j] = r.a;
+            dHy[i * 3 + j] = r.b;
+        }
+}
+
+__device__ bool mat_inv_d(const double* a, double* r)
+{
+    const double c00 = a[4] * a[8] - a[5] * a[7];
+    const double c01 = a[5] * a[6] - a[3] * a[8];
+    const double c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    if (det == 0.0 || !isfinite(det)) return false;
+    const double id = 1.0 / det;
+    r[0] = c00 * id;
+    r[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    r[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    r[3] = c01 * id;
+    r[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    r[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    r[6] = c02 * id;
+    r[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    r[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    return true;
+}
+
+__device__ __forceinline__ bool inside_d(const Roi& R, double x, double y)
+{
+    return x >= double(R.x0) && x < double(R.x1 - 1) && y >= double(R.y0) && y < double(R.y1 - 1);
+}
+
+// Identification.hpp:197-219 and its gradient, in double.
+__device__ __forceinline__ double bilinear_d(const Roi& R, double x, double y, double& gx, double& gy)
+{
+    const int px = int(x), py = int(y);
+    const uint8_t* p0 = R.img + px + size_t(py) * R.pitch;
+    const double fx = x - double(px), fy = y - double(py);
+    const double p1 = __ldg(p0), p2 = __ldg(p0 + 1), p3 = __ldg(p0 + R.pitch), p4 = __ldg(p0 + R.pitch + 1);
+    gx = ((p2 - p1) * (1.0 - fy) + (p4 - p3) * fy) * 0.5;
+    gy = ((p3 - p1) * (1.0 - fx) + (p4 - p2) * fx) * 0.5;
+    return (p1 * (1.0 - fx) * (1.0 - fy) + p2 * fx * (1.0 - fy) + p3 * (1.0 - fx) * fy + p4 * fx * fy) * 0.5;
+}
+
+struct CostSharedD {
+    double C[9], Tp[9], Td[9];
+    double H[9], Hi[9], dH[2][9];
+    double sig[kMaxCuts][kMaxSamples];
+    double mean[kMaxSamples];
+    double dz[kMaxCuts][3];
+    double red[kThreads / 32][10];
+    uint32_t oob;
+    int bad;
+};
+
+}  // namespace
+
+// k_cut_cost in double precision (one block per task).
+__global__ void __launch_bounds__(kThreads) k_cut_cost_f64(const uint8_t* __restrict__ img, size_t pitch,
+                                                           const IdentTask* __restrict__ tasks,
+                                                           const float* __restrict__ centers, float* out,
+                                                           IdentParams ip)
+{
+    __shared__ CostSharedD S;
+    const IdentTask& T = tasks[blockIdx.x];
+    const Roi roi = make_roi(img, pitch, T);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nS = ip.nSamples;
+    const double bs = ip.beginSig;
+    const double den = double(nS) - 1.0;
+    float* o = out + 12 * size_t(blockIdx.x);
+    const uint32_t cutMask = (T.ncuts >= 32) ? 0xffffffffu : ((1u << T.ncuts) - 1u);
+    if (tid == 0) {
+        canonic_form_d(T.Q, S.C, S.Tp, S.Td);
+        homography_center_derivs_d(S.C, S.Tp, S.Td, centers[2 * blockIdx.x], centers[2 * blockIdx.x + 1], S.H,
+                                   S.dH[0], S.dH[1]);
+        S.bad = mat_inv_d(S.H, S.Hi) ? 0 : 1;
+        S.oob = 0u;
+    }
+    if (tid < kMaxCuts * 3) S.dz[tid / 3][tid % 3] = 0.0;
+    __syncthreads();
+    if (S.bad) {
+        if (tid == 0) write_cost(o, FLT_MAX);
+        return;
+    }
+    for (int c = warp; c < T.ncuts; c += kWarps) {
+        const double px = T.stop[c][0], py = T.stop[c][1];
+        const double z0 = S.Hi[0] * px + S.Hi[1] * py + S.Hi[2];
+        const double z1 = S.Hi[3] * px + S.Hi[4] * py + S.Hi[5];
+        const double z2 = S.Hi[6] * px + S.Hi[7] * py + S.Hi[8];
+        const double bx = z0 / z2, by = z1 / z2;
+        const double xs = bx * bs, ys = by * bs;
+        const double sx = (bx - xs) / den, sy = (by - ys) / den;
+        bool bad = false;
+        for (int k = lane; k < nS; k += 32) {
+            const double x = xs + double(k) * sx, y = ys + double(k) * sy;
+            const double u = S.H[0] * x + S.H[1] * y + S.H[2];
+            const double v = S.H[3] * x + S.H[4] * y + S.H[5];
+            const double w = S.H[6] * x + S.H[7] * y + S.H[8];
+            const double qx = u / w, qy = v / w;
+            double gx, gy;
+            if (inside_d(roi, qx, qy)) S.sig[c][k] = bilinear_d(roi, qx, qy, gx, gy);
+            else bad = true;
+        }
+        if (__ballot_sync(0xffffffffu, bad) && lane == 0) atomicOr(&S.oob, 1u << c);
+    }
+    __syncthreads();
+    const uint32_t valid = ~S.oob & cutMask;
+    const int n = __popc(valid);
+    if (n < 2) {
+        if (tid == 0) write_cost(o, FLT_MAX);
+        return;
+    }
+    const double pairs = 0.5 * double(n) * double(n - 1);
+    double costPart = 0.0;
+    for (int k = tid; k < nS; k += kThreads) {
+        double s1 = 0.0, s2 = 0.0;
+        uint32_t m = valid;
+        while (m) {
+            const int c = __ffs(m) - 1;
+            m &= m - 1;
+            const double v = S.sig[c][k];
+            s1 += v;
+            s2 += v * v;
+        }
+        S.mean[k] = s1 / double(n);
+        costPart += double(n) * s2 - s1 * s1;
+    }
+    __syncthreads();
+    double gH[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double coef = 2.0 * double(n) / pairs;
+    const double* Hm = S.H;
+    for (int c = warp; c < T.ncuts; c += kWarps) {
+        if (!((valid >> c) & 1u)) continue;
+        const double px = T.stop[c][0], py = T.stop[c][1];
+        const double z0 = S.Hi[0] * px + S.Hi[1] * py + S.Hi[2];
+        const double z1 = S.Hi[3] * px + S.Hi[4] * py + S.Hi[5];
+        const double z2 = S.Hi[6] * px + S.Hi[7] * py + S.Hi[8];
+        const double bx = z0 / z2, by = z1 / z2;
+        const double xs = bx * bs, ys = by * bs;
+        const double sx = (bx - xs) / den, sy = (by - ys) / den;
+        double gbx = 0.0, gby = 0.0;
+        for (int k = lane; k < nS; k += 32) {
+            const double x = xs + double(k) * sx, y = ys + double(k) * sy;
+            const double u = Hm[0] * x + Hm[1] * y + Hm[2];
+            const double v = Hm[3] * x + Hm[4] * y + Hm[5];
+            const double w = Hm[6] * x + Hm[7] * y + Hm[8];
+            const double rw = 1.0 / w;
+            const double qx = u / w, qy = v / w;
+            double gx, gy;
+            (void)bilinear_d(roi, qx, qy, gx, gy);
+            const double lam = coef * (S.sig[c][k] - S.mean[k]);
+            const double fx = lam * gx, fy = lam * gy;
+            const double fw = -(fx * qx + fy * qy);
+            const double y3[3] = {x, y, 1.0};
+            for (int j = 0; j < 3; ++j) {
+                gH[j] += fx * rw * y3[j];
+                gH[3 + j] += fy * rw * y3[j];
+                gH[6 + j] += fw * rw * y3[j];
+            }
+            const double fX = (fx * (Hm[0] - qx * Hm[6]) + fy * (Hm[3] - qy * Hm[6])) * rw;
+            const double fY = (fx * (Hm[1] - qx * Hm[7]) + fy * (Hm[4] - qy * Hm[7])) * rw;
+            const double t = bs + double(k) * (1.0 - bs) / den;
+            gbx += t * fX;
+            gby += t * fY;
+        }
+        for (int off = 16; off; off >>= 1) {
+            gbx += __shfl_xor_sync(0xffffffffu, gbx, off);
+            gby += __shfl_xor_sync(0xffffffffu, gby, off);
+        }
+        if (lane == 0) {
+            S.dz[c][0] = gbx / z2;
+            S.dz[c][1] = gby / z2;
+            S.dz[c][2] = -(gbx * bx + gby * by) / z2;
+        }
+    }
+    double red[10];
+    red[0] = costPart;
+    for (int j = 0; j < 9; ++j) red[1 + j] = gH[j];
+    for (int j = 0; j < 10; ++j)
+        for (int off = 16; off; off >>= 1) red[j] += __shfl_xor_sync(0xffffffffu, red[j], off);
+    if (lane == 0)
+        for (int j = 0; j < 10; ++j) S.red[warp][j] = red[j];
+    __syncthreads();
+    if (tid == 0) {
+        double cost = 0.0, G[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int w = 0; w < kWarps; ++w) {
+            cost += S.red[w][0];
+            for (int j = 0; j < 9; ++j) G[j] += S.red[w][1 + j];
+        }
+        cost /= pairs;
+        double GHi[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int c = 0; c < T.ncuts; ++c) {
+            const double p3[3] = {T.stop[c][0], T.stop[c][1], 1.0};
+            for (int r = 0; r < 3; ++r)
+                for (int q = 0; q < 3; ++q) GHi[r * 3 + q] += S.dz[c][r] * p3[q];
+        }
+        double M[9], Mt[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double a = 0.0;
+                for (int q = 0; q < 3; ++q) a += GHi[i * 3 + q] * S.Hi[j * 3 + q];
+                M[i * 3 + j] = a;
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double a = 0.0;
+                for (int q = 0; q < 3; ++q) a += S.Hi[q * 3 + i] * M[q * 3 + j];
+                Mt[i * 3 + j] = a;
+            }
+        double dc[2] = {0.0, 0.0};
+        for (int j = 0; j < 9; ++j) {
+            G[j] -= Mt[j];
+            dc[0] += G[j] * S.dH[0][j];
+            dc[1] += G[j] * S.dH[1][j];
+        }
+        o[0] = float(cost);
+        o[1] = float(dc[0]);
+        o[2] = float(dc[1]);
+        for (int j = 0; j < 9; ++j) o[3 + j] = float(G[j]);
+    }
+}
+
 void upload_bank(const std::vector<std::vector<float>>& bank, float* d_bank_inv)
 {
     std::vector<float> inv(size_t(kMaxBankIds) * kMaxBankRatios, 0.f);
@@ -1292,7 +1657,7 @@ void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_task
 {
     if (n <= 0) return;
     if (ip.gridN * ip.gridN > kMaxTrials || ip.gridN < 3 || (ip.gridN & 1) == 0)
-        throw Error{CCTAGB_BAD_ARG, "imagedCenterNGridSample must be 3 or 5"};
+        throw Error{CCTAGB_BAD_ARG, "imagedCenterNGridSample (gnCoarseGrid in Gauss-Newton) must be 3 or 5"};
     if (ip.nSamples > kMaxSamples || ip.nSamples < 32) throw Error{CCTAGB_BAD_ARG, "sampleCutLength out of range"};
     if (ip.refineMode != CCTAGB_REFINE_GRID && ip.refineMode != CCTAGB_REFINE_GAUSS_NEWTON)
         throw Error{CCTAGB_BAD_ARG, "unknown refineMode"};
@@ -1329,11 +1694,15 @@ void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_task
 }
 
 void launch_cut_cost(const uint8_t* d_img, size_t pitch, const IdentTask* d_tasks, const float* d_centers,
-                     float* d_out, int n, const IdentParams& ip, cudaStream_t s)
+                     float* d_out, int n, const IdentParams& ip, cudaStream_t s, bool fp64)
 {
     if (n <= 0) return;
     if (ip.nSamples > kMaxSamples || ip.nSamples < 32) throw Error{CCTAGB_BAD_ARG, "sampleCutLength out of range"};
-    k_cut_cost<<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_centers, d_out, ip);
+    if (fp64) {
+        k_cut_cost_f64<<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_centers, d_out, ip);
+    } else {
+        k_cut_cost<<<n, kThreads, 0, s>>>(d_img, pitch, d_tasks, d_centers, d_out, ip);
+    }
     CCTAGB_CUDA(cudaGetLastError());
 }
 

@@ -261,18 +261,23 @@ def config_frame(name: str, seed: int = 0) -> Frame:
 CAMERA_SIZES = ((640, 480), (1280, 720), (1920, 1080), (3840, 2160))
 
 
-def camera_batch(seed: int = 0, n: int = 16) -> list:
+def _camera_frame(job):
+    w, h, n_markers, rmax, seed, noise = job
+    return render_frame(w, h, n_markers, (15.0, rmax), 60, seed=seed, noise_sigma=noise, blur_sigma=1.0)
+
+
+def camera_batch(seed: int = 0, n: int = 16, map_fn=map) -> list:
     """Multi-camera step: n frames, each of a resolution drawn uniformly from
     CAMERA_SIZES, with 0-20 markers (outer radius up to a quarter of the
-    shorter side), tilt <= 60 deg, noise sigma 4-8."""
+    shorter side), tilt <= 60 deg, noise sigma 4-8.  map_fn renders the frames
+    (a process pool's map spreads them over the host cores; same result)."""
     rng = np.random.default_rng(seed + 7000)
-    out = []
+    jobs = []
     for i in range(n):
         w, h = CAMERA_SIZES[int(rng.integers(len(CAMERA_SIZES)))]
         rmax = min(200.0, min(w, h) / 4.0)
-        out.append(render_frame(w, h, int(rng.integers(0, 21)), (15.0, rmax), 60, seed=seed * 1000 + i,
-                                noise_sigma=float(rng.uniform(4.0, 8.0)), blur_sigma=1.0))
-    return out
+        jobs.append((w, h, int(rng.integers(0, 21)), rmax, seed * 1000 + i, float(rng.uniform(4.0, 8.0))))
+    return list(map_fn(_camera_frame, jobs))
 
 
 def ellipse_of_conic(Q: np.ndarray):
@@ -287,14 +292,16 @@ def ellipse_of_conic(Q: np.ndarray):
     return float(c[0]), float(c[1]), float(a), float(b), ang
 
 
-def cut_task_from_marker(m: Marker, roi, n_cuts: int = 22, offset=(0.0, 0.0), start=None):
+def cut_task_from_marker(m: Marker, roi, n_cuts: int = 22, offset=(0.0, 0.0), start=None, local=False):
     """A cctagb_cut_task for a rendered marker: its true outer ellipse, cut
     stops spread evenly on it, the ellipse center as the initial imaged center
     (as detection starts), all shifted by `offset` (an atlas placement);
-    `roi` = (x, y, w, h) in the shifted image."""
+    `roi` = (x, y, w, h) in the shifted image.  local: the geometry stays in
+    the marker's own frame (the task's coordinates are relative to the roi
+    corner; `offset` is then only the roi's placement)."""
     from .capi import CutTask
 
-    ox, oy = offset
+    ox, oy = (0.0, 0.0) if local else offset
     T = np.array([[1, 0, -ox], [0, 1, -oy], [0, 0, 1.0]])
     Q = T.T @ m.outer_conic @ T          # conic in shifted coordinates
     Q = Q / np.abs(Q).max()
@@ -312,23 +319,29 @@ def cut_task_from_marker(m: Marker, roi, n_cuts: int = 22, offset=(0.0, 0.0), st
         t.stop[i][1] = cy + a * np.cos(th) * sa + b * np.sin(th) * ca
     for k in range(4):
         t.roi[k] = int(roi[k])
+    t.local = int(bool(local))
     return t
 
 
-def refine_atlas(seed: int = 0, n_crops: int = 256, width: int = 4096):
+def _refine_crop(job):
+    """One crop of refine_atlas (module level so that a process pool can run it)."""
+    seed, i, r, noise = job
+    s = int(np.ceil(4.2 * r + 12))
+    return render_frame(s, s, 1, (r, r), 70, seed=seed * 100000 + i, noise_sigma=noise, blur_sigma=1.0)
+
+
+def refine_atlas(seed: int = 0, n_crops: int = 256, width: int = 4096, map_fn=map):
     """Candidate-refinement workload: n_crops single-marker crops (outer radius
     8-150 px, tilt <= 70 deg, noise sigma 2-12) packed row by row into one
-    atlas image.  Returns (atlas, [(marker in atlas coordinates, roi)]), roi =
-    (x, y, w, h) of the crop in the atlas."""
+    atlas image.  Returns (atlas, [(marker in its crop's coordinates, roi)]), roi =
+    (x, y, w, h) of the crop in the atlas.  map_fn renders the crops (a
+    process pool's map spreads them over the host cores; same result)."""
     rng = np.random.default_rng(seed + 9000)
-    crops = []
+    jobs = []
     for i in range(n_crops):
         r = float(rng.uniform(8.0, 150.0))
-        s = int(np.ceil(4.2 * r + 12))
-        f = render_frame(s, s, 1, (r, r), 70, seed=seed * 100000 + i, noise_sigma=float(rng.uniform(2.0, 12.0)),
-                         blur_sigma=1.0)
-        if f.markers:
-            crops.append(f)
+        jobs.append((seed, i, r, float(rng.uniform(2.0, 12.0))))
+    crops = [f for f in map_fn(_refine_crop, jobs) if f.markers]
     # shelf packing
     x = y = shelf = 0
     places = []

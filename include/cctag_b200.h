@@ -33,6 +33,7 @@
  *                                                                  src/cctag/Detection.cpp:69-156,609-627
  *   cctagb_cut_cost        <- costFunctionGlob (forward only in the reference; here with its
  *                             gradient in the center and in H)   src/cctag/Identification.cpp:1122-1158
+ *   cctagb_cut_cost_f64    <- the same in double precision (a check form; no reference counterpart)
  *   cctagb_edges_noalloc   <- no reference counterpart (the edge stage on caller buffers,
  *                             allocating nothing)
  *   cctagb_host_frames / cctagb_submit / cctagb_wait
@@ -112,9 +113,11 @@ typedef struct cctagb_params {
     /* B200-specific */
     int refineMode;                             /* CCTAGB_REFINE_GRID */
     int gnIterations;                           /* 10: cost evaluations at most in REFINE_GAUSS_NEWTON */
-    int gnCoarseRounds;                         /* 2: grid rounds before Gauss-Newton */
+    int gnCoarseRounds;                         /* 1: grid rounds before Gauss-Newton */
     int edgeCapacityDivisor;                    /* 4: edge capacity per level = W*H/divisor */
     int hostThreads;                            /* 0: host threads of the candidate stage; 0 = one per physical core, less one per detection slot beyond the first */
+    int gnCoarseGrid;                           /* 3: trial grid (3 or 5 per side) of the coarse rounds of REFINE_GAUSS_NEWTON */
+    float gnCoarseNeighbourSize;                /* 0.1: their neighbourhood, as imagedCenterNeighbourSize */
 } cctagb_params;
 
 typedef struct cctagb_ellipse {
@@ -306,6 +309,12 @@ typedef struct cctagb_cut_task {
     int roi[4];                     /* x, y, w, h: the candidate's image rectangle;
                                        a sample outside it drops its cut, as the
                                        image border does in the reference        */
+    int local;                      /* 0: Q, cx, cy, x0, y0 and stop are image
+                                       coordinates; nonzero: they are relative to
+                                       the rectangle's corner (roi[0], roi[1]),
+                                       and so are the results.  Candidates from
+                                       a large atlas keep their FP32 positions
+                                       as precise as in a frame that way.         */
 } cctagb_cut_task;
 
 typedef struct cctagb_ident_result {
@@ -345,6 +354,15 @@ cctagb_status cctagb_identify_tasks(cctagb_handle* h, const uint8_t* d_img, int 
 cctagb_status cctagb_cut_cost(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
                               const cctagb_cut_task* tasks, int n, const float* centers, float* cost,
                               float* d_center, float* d_h);
+
+/* cctagb_cut_cost with every step in double precision on the GPU (canonic
+ * form, homography and its center derivatives, cut ends, sample positions,
+ * bilinear reads, sums).  It has no counterpart in the reference: it exists
+ * to check the adjoint against central differences below the ~1e-4 relative
+ * noise that FP32 sample positions put on the cost.  Same arguments. */
+cctagb_status cctagb_cut_cost_f64(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
+                                  const cctagb_cut_task* tasks, int n, const float* centers, float* cost,
+                                  float* d_center, float* d_h);
 
 #ifdef __cplusplus
 }

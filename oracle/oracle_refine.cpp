@@ -160,6 +160,8 @@ struct Img {
 
 Img image_of(const uint8_t* img, size_t pitch, const cctagb_cut_task& t)
 {
+    if (t.local)  // coordinates relative to the rectangle's corner
+        return Img{img + size_t(t.roi[1]) * pitch + size_t(t.roi[0]), pitch, 0, 0, t.roi[2], t.roi[3]};
     return Img{img, pitch, t.roi[0], t.roi[1], t.roi[0] + t.roi[2], t.roi[1] + t.roi[3]};
 }
 
@@ -360,7 +362,7 @@ int orc_refine_grid(const uint8_t* img, size_t pitch, const cctagb_cut_task* t, 
     double ns = neighbourSize;
     const double maxSemi = std::max(double(t->a), double(t->b));
     bool any = false;
-    while (ns * maxSemi > stop_width) {
+    for (int round = 0; ns * maxSemi > stop_width && round < 64; ++round) {  // 64: the kernel's bound
         const double size = ns * std::max(ca, cb);
         const double half = size / 2, step = size / (gridN - 1);
         const double ccx = mT.m[0] * cx + mT.m[1] * cy + mT.m[2];
