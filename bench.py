@@ -43,7 +43,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "1080p frames/s + per-stage HBM GB/s; batched/adjoint vs plain at <=0.05 px"
 UNIT = "frames/s"
 BATCH = 16  # frames per step (distinct seeded frames)
-SLOTS = 8   # detection slots of the batch handle
+SLOTS = 16  # detection slots of the batch handle (one wave of 16 frames per step)
 N_FRAMES = BATCH
 
 
@@ -219,6 +219,9 @@ def run_b200(args, rank, world, local):
     H, W = frames[0].shape
     det = cctag_b200.Detector(max_w=W, max_h=H, max_batch=SLOTS)
     stream = torch.cuda.ExternalStream(det.stream)
+    # single-frame calls on a handle of their own (one slot: the whole host pool)
+    det1 = cctag_b200.Detector(max_w=W, max_h=H)
+    stream1 = torch.cuda.ExternalStream(det1.stream)
     d_frames = [torch.from_numpy(f).to(dev) for f in frames]
     h_frames = [torch.from_numpy(f).pin_memory() for f in frames]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -248,17 +251,17 @@ def run_b200(args, rank, world, local):
 
     def step_device(i):
         t = d_frames[i % len(d_frames)]
-        return det.detect_device(t.data_ptr(), W, H, W, frame_id=i)
+        return det1.detect_device(t.data_ptr(), W, H, W, frame_id=i)
 
     def step_host(i):
         t = h_frames[i % len(h_frames)]
         n = C.c_int()
         st = capi.Stats()
-        det._check(det._lib.cctagb_detect(det._h, C.c_void_p(t.data_ptr()), W, H, W, i, out1, cap, C.byref(n),
-                                          C.byref(st)), "detect")
+        det1._check(det1._lib.cctagb_detect(det1._h, C.c_void_p(t.data_ptr()), W, H, W, i, out1, cap, C.byref(n),
+                                            C.byref(st)), "detect")
         return [out1[k] for k in range(n.value)], st
 
-    def timed(step_fn, steps):
+    def timed(step_fn, steps, stream=stream):
         total = 0.0
         last = None
         per = []
@@ -291,8 +294,8 @@ def run_b200(args, rank, world, local):
         ms_e2e, fr_last_h, _ = timed(step_batch(fr_host), args.steps)
         torch.cuda.synchronize()
         barrier(world)
-        ms_plain, (markers, stats), per_plain = timed(step_device, n_plain)
-        ms_plain_h, (_, stats_h), _ = timed(step_host, n_plain)
+        ms_plain, (markers, stats), per_plain = timed(step_device, n_plain, stream1)
+        ms_plain_h, (_, stats_h), _ = timed(step_host, n_plain, stream1)
     torch.cuda.synchronize()
     barrier(world)
     ms_dev = max_over_ranks(ms_dev, world)
@@ -306,56 +309,92 @@ def run_b200(args, rank, world, local):
     d2h = sum(fr_last_h[i].stats.d2h_bytes for i in range(BATCH))
     # Batched and single-frame paths return the same markers for a frame.
     same = all(
-        [(m.id, m.status, m.x, m.y) for m in det.detect(frames[i])[0]]
+        [(m.id, m.status, m.x, m.y) for m in det1.detect(frames[i])[0]]
         == [(outs[i][k].id, outs[i][k].status, outs[i][k].x, outs[i][k].y) for k in range(fr_last_h[i].n_out)]
         for i in range(min(4, BATCH)))
 
-    # Per-stage device times (events between the image-stage kernels) and the
-    # identification kernel, separate pass (not part of the timed region).
-    det.set_stage_timing(True)
+    # Per-stage device times of the batched image stage with the step's 16
+    # frames in one wave (one launch per kernel over all of them; events
+    # between the kernels, eager, nothing else running), separate pass.
+    pt = cctag_b200.default_params(3)
+    pt.batchWaveFrames = BATCH
+    det_t = cctag_b200.Detector(pt, max_w=W, max_h=H, max_batch=BATCH)
+    det_t.set_stage_timing(True)
+    bacc = {}
+    for i in range(max(3, min(args.steps, 10))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        det_t._check(det_t._lib.cctagb_detect_batch(det_t._h, fr_dev, BATCH), "detect_batch")
+        for k, v in det_t.stage_times().items():
+            bacc.setdefault(k, []).append(v)
+    det_t.close()
+    batch_stage_ms = {k: statistics.median(v) for k, v in bacc.items()}
+    # per-frame edge points, seeds and votes of the batch's frames
+    bE, bS, bV, blevels = [], [], [], []
+    for i in range(BATCH):
+        _, st_i = step_device(i)
+        blevels.append([det1.level_size(l) for l in range(4)])
+        bE.append([st_i.edge_points[l] for l in range(4)])
+        bS.append([st_i.seeds[l] for l in range(4)])
+        bV.append([int(len(det1.votes(l)["vlist"])) for l in range(4)])
+    # Per-stage device times of one frame's image stage and the
+    # identification kernel (single-frame path), separate pass.
+    det1.set_stage_timing(True)
     acc = {}
     id_ms, host_ms, dl_ms, cut_ms = [], [], [], []
     for i in range(max(3, min(args.steps, 20))):
         flush.zero_()
         torch.cuda.synchronize()
         _, st = step_device(i)
-        for k, v in det.stage_times().items():
+        for k, v in det1.stage_times().items():
             acc.setdefault(k, []).append(v)
         id_ms.append(st.ms_identify)
         host_ms.append(st.ms_host_candidates)
         dl_ms.append(st.ms_download)
         cut_ms.append(st.ms_cut_selection)
-    det.set_stage_timing(False)
+    det1.set_stage_timing(False)
     stage_ms = {k: statistics.median(v) for k, v in acc.items()}
 
-    levels = [det.level_size(l) for l in range(4)]
+    levels = [det1.level_size(l) for l in range(4)]
     E = [stats.edge_points[l] for l in range(4)]
     S = [stats.seeds[l] for l in range(4)]
-    V = [int(len(det.votes(l)["vlist"])) for l in range(4)]
+    V = [int(len(det1.votes(l)["vlist"])) for l in range(4)]
     sb = stage_bytes(levels, E, S, V)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    stages = {k: {"ms": round(stage_ms[k], 5), "bytes": sb[k],
-                  "GB_s": round(sb[k] / (stage_ms[k] * 1e-3) / 1e9, 1) if stage_ms[k] > 0 else None,
-                  "frac_of_measured_hbm": round(sb[k] / (stage_ms[k] * 1e-3) / 1e9 / peak, 4) if stage_ms[k] > 0
-                  else None}
-              for k in sb}
+
+    def stage_table(ms_by, bytes_by):
+        return {k: {"ms": round(ms_by[k], 5), "bytes": bytes_by[k],
+                    "GB_s": round(bytes_by[k] / (ms_by[k] * 1e-3) / 1e9, 1) if ms_by[k] > 0 else None,
+                    "frac_of_measured_hbm": round(bytes_by[k] / (ms_by[k] * 1e-3) / 1e9 / peak, 4)
+                    if ms_by[k] > 0 else None}
+                for k in bytes_by}
+
+    # algorithmic bytes of the batched launch: the sum over its frames
+    bsb = {}
+    for i in range(BATCH):
+        for k, v in stage_bytes(blevels[i], bE[i], bS[i], bV[i]).items():
+            bsb[k] = bsb.get(k, 0) + v
+    stages = stage_table(batch_stage_ms, bsb)
+    stages_single = stage_table(stage_ms, sb)
     n_ident = sum(1 for m in markers if m.status in (1, -4))
     idm = statistics.median(id_ms)
-    stages["identify"] = {"ms": round(idm, 5), "markers": n_ident, "bound": "fp32 SIMT + L2 gathers",
+    stages_single["identify"] = {"ms": round(idm, 5), "markers": n_ident, "bound": "fp32 SIMT + L2 gathers",
                           "GFLOP_s": round(ident_flops(n_ident) / (idm * 1e-3) / 1e9, 1) if idm > 0 else None}
-    stages["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++), includes the "
+    stages_single["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++), includes the "
                                  "edge-point download"}
-    stages["download"] = {"ms": round(statistics.median(dl_ms), 4), "where": "D2H of the edge-point collections"}
-    stages["host_outer_point_sort"] = {"ms": round(statistics.median(cut_ms), 4), "where": "host CPU (C++): outer points sorted by angle; cut selection then runs on the GPU just before identification"}
-    # Roofline object for the dominant HBM-class kernel group of the image stage.
-    top = max(stage_ms, key=lambda k: stage_ms[k])
+    stages_single["download"] = {"ms": round(statistics.median(dl_ms), 4), "where": "D2H of the edge-point collections"}
+    stages_single["host_outer_point_sort"] = {"ms": round(statistics.median(cut_ms), 4), "where": "host CPU (C++): outer points sorted by angle; cut selection then runs on the GPU just before identification"}
+    # Roofline object for the dominant HBM-class kernel group of the batched
+    # image stage (one launch over the step's 16 frames).
+    top = max(batch_stage_ms, key=lambda k: batch_stage_ms[k])
     traffic = profiled_traffic(args.config).get(top)
-    ach = sb[top] / (stage_ms[top] * 1e-3) / 1e9
+    ach = bsb[top] / (batch_stage_ms[top] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": traffic, "peak_source": peak_src,
-                "note": "achieved = algorithmic bytes / CUDA-event time of the kernel group, frac of measured"}
+                "launch": f"one launch per kernel over the image stages of the {BATCH} frames of a step",
+                "note": "achieved = algorithmic bytes of the launch / its CUDA-event time, frac of measured"}
 
     c3 = run_c3(args, flush, torch, peak, peak_src) if rank == 0 and not args.no_c3 else None
     c4 = run_c4(args, flush, torch) if rank == 0 and not args.no_c4 else None
@@ -385,6 +424,7 @@ def run_b200(args, rank, world, local):
                   "p99_ms": round(float(np.percentile(per_plain, 99)), 3),
                   "note": "one frame per call (cctagb_detect_device / cctagb_detect)"},
         "stages": stages,
+        "stages_single_frame": stages_single,
         "roofline": roofline,
         "gpu_launches": int(launches_batch + launches_batch_h) * args.steps
                         + int(stats.kernel_launches + stats_h.kernel_launches) * n_plain,
@@ -399,6 +439,7 @@ def run_b200(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(frames[:2], budget_s=args.cpu_budget, threads=1)
     det.close()
+    det1.close()
     return line
 
 

@@ -35,7 +35,7 @@ class Params(C.Structure):
         ("searchForAnotherSegment", C.c_int), ("writeOutput", C.c_int), ("doIdentification", C.c_int),
         ("maxEdges", C.c_uint32), ("refineMode", C.c_int), ("gnIterations", C.c_int),
         ("gnCoarseRounds", C.c_int), ("edgeCapacityDivisor", C.c_int), ("hostThreads", C.c_int),
-        ("gnCoarseGrid", C.c_int), ("gnCoarseNeighbourSize", C.c_float),
+        ("gnCoarseGrid", C.c_int), ("gnCoarseNeighbourSize", C.c_float), ("batchWaveFrames", C.c_int),
     ]
 
 

@@ -2,9 +2,11 @@
 // status codes; nothing crosses the ABI as a C++ exception.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -130,6 +132,31 @@ struct cctagb_handle {
     }
     bool streaming() const { return !tickets.empty(); }
 
+    // Batched image stage of cctagb_detect_batch: one launch per kernel for
+    // the frames of a wave, on its own (lowest-priority) stream.
+    // One batch-stage state and completion event per wave in flight.
+    std::vector<std::unique_ptr<cctagb::BatchStage>> batch;
+    std::vector<cudaEvent_t> bdone;
+    cudaStream_t bstream = nullptr;
+    bool batch_timing = false;
+    bool last_timed_batch = false;  // stage times: of the last batch, else of the last single frame
+    int last_batch = 0;             // the wave state whose stage times are the last batch's
+    void ensure_batch(int d)
+    {
+        if (!bstream) {
+            int least = 0, greatest = 0;
+            CCTAGB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+            CCTAGB_CUDA(cudaStreamCreateWithPriority(&bstream, cudaStreamNonBlocking, least));
+        }
+        while (int(batch.size()) < d) {
+            cudaEvent_t e = nullptr;
+            CCTAGB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            bdone.push_back(e);
+            batch.push_back(std::make_unique<cctagb::BatchStage>());
+            batch.back()->set_stage_timing(batch_timing);
+        }
+    }
+
     ~cctagb_handle()
     {
         {
@@ -140,6 +167,10 @@ struct cctagb_handle {
         for (auto& t : sworkers) t.join();
         if (det) cudaStreamSynchronize(det->pipeline().stream());
         for (auto& d : extra) cudaStreamSynchronize(d->pipeline().stream());
+        if (bstream) cudaStreamSynchronize(bstream);
+        batch.clear();
+        for (cudaEvent_t e : bdone) cudaEventDestroy(e);
+        if (bstream) cudaStreamDestroy(bstream);
         for (uint8_t* p : host_frames) cudaFreeHost(p);
     }
 };
@@ -222,6 +253,7 @@ void cctagb_params_default(cctagb_params* p, int nCrowns)
     p->edgeCapacityDivisor = 4;
     p->gnCoarseGrid = 3;
     p->gnCoarseNeighbourSize = 0.1f;
+    p->batchWaveFrames = 4;
 }
 
 const char* cctagb_status_string(cctagb_status s)
@@ -416,7 +448,12 @@ cctagb_status cctagb_set_stage_timing(cctagb_handle* h, int enable)
 {
     if (!h) return CCTAGB_BAD_ARG;
     if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
-    return guarded(h, [&] { h->det->pipeline().set_stage_timing(enable != 0); });
+    return guarded(h, [&] {
+        h->det->pipeline().set_stage_timing(enable != 0);
+        h->batch_timing = enable != 0;
+        for (auto& b : h->batch) b->set_stage_timing(enable != 0);
+        h->last_timed_batch = false;
+    });
 }
 
 cctagb_status cctagb_stage_times(cctagb_handle* h, int cap, float* ms, int* n)
@@ -424,7 +461,8 @@ cctagb_status cctagb_stage_times(cctagb_handle* h, int cap, float* ms, int* n)
     if (!h || !n) return CCTAGB_BAD_ARG;
     *n = cctagb::kStageCount;
     if (cap < cctagb::kStageCount || !ms) return CCTAGB_BAD_ARG;
-    const float* src = h->det->pipeline().stage_ms();
+    const float* src = h->last_timed_batch && !h->batch.empty() ? h->batch[size_t(h->last_batch)]->stage_ms()
+                                                                : h->det->pipeline().stage_ms();
     std::copy(src, src + cctagb::kStageCount, ms);
     return CCTAGB_OK;
 }
@@ -444,6 +482,7 @@ cctagb_status cctagb_detect(cctagb_handle* h, const uint8_t* gray, int w, int hg
 {
     if (!h) return CCTAGB_BAD_ARG;
     if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
+    h->last_timed_batch = false;
     return guarded(h, [&] { h->det->detect(gray, w, hgt, pitch, false, frame_id, out, cap, n_out, stats); });
 }
 
@@ -452,6 +491,7 @@ cctagb_status cctagb_detect_device(cctagb_handle* h, const uint8_t* d_gray, int 
 {
     if (!h) return CCTAGB_BAD_ARG;
     if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
+    h->last_timed_batch = false;
     return guarded(h, [&] { h->det->detect(d_gray, w, hgt, pitch, true, frame_id, out, cap, n_out, stats); });
 }
 
@@ -570,41 +610,91 @@ cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)
     if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
     if (n == 0) return CCTAGB_OK;
     return guarded(h, [&] {
-        const int S = std::min(n, h->slots());
-        h->ensure_slots(S);
+        // Waves of wf frames: the image stages of a wave's frames run as one
+        // batched launch per kernel (on the lowest-priority batch stream, in
+        // wave order), then frame j of the wave continues on its detection
+        // slot.  The slots hold D = slots / wf waves in flight: wave k reuses
+        // the slots (and batch-stage state) of wave k - D once that wave's
+        // frames are done, so later waves' stages overlap earlier frames'
+        // GPU and host stages.  A frame's result does not depend on the wave
+        // or slot that ran it.
+        const int S = h->slots();
+        const int wf = std::max(1, std::min({h->params.batchWaveFrames, cctagb::kMaxBatchFrames, S, n}));
+        const int D = std::max(1, std::min(S / wf, (n + wf - 1) / wf));
+        h->ensure_slots(D * wf);
+        h->ensure_batch(D);
         for (int i = 0; i < n; ++i) {
             frames[i].n_out = 0;
             frames[i].status = CCTAGB_INTERNAL;
         }
         std::vector<std::string> msg(static_cast<size_t>(n));
-        std::atomic<int> next{0};
-        // Each slot takes the next frame until none is left; a frame's result
-        // does not depend on the slot that ran it.
-        auto run = [&](int s) {
-            cudaSetDevice(h->device);
-            cctagb::Detector& d = h->slot(s);
-            for (int i; (i = next.fetch_add(1)) < n;) {
-                cctagb_frame& f = frames[i];
+        std::mutex msg_mu;
+        auto fail = [&](int i, cctagb_status st, std::string m) {
+            std::lock_guard<std::mutex> l(msg_mu);
+            frames[i].status = st;
+            msg[size_t(i)] = std::move(m);
+        };
+        std::vector<std::vector<std::thread>> inflight(static_cast<size_t>(D));
+        auto drain = [&](int d) {
+            for (auto& t : inflight[size_t(d)]) t.join();
+            inflight[size_t(d)].clear();
+        };
+        struct Joiner {  // every started frame is joined, also when a launch throws
+            std::function<void()> f;
+            ~Joiner() { f(); }
+        } joiner{[&] {
+            for (int d = 0; d < D; ++d) drain(d);
+        }};
+        for (int k = 0, w0 = 0; w0 < n; ++k, w0 += wf) {
+            const int d = k % D, nw = std::min(wf, n - w0);
+            drain(d);  // the wave that last used these slots is done
+            const auto t0 = std::chrono::steady_clock::now();
+            std::vector<cctagb::Pipeline*> pipes;
+            std::vector<int> started;  // wave frame j -> its slot, -1 if it failed to start
+            for (int j = 0; j < nw; ++j) {
+                cctagb_frame& f = frames[w0 + j];
+                const int s = d * wf + j;
                 try {
-                    d.detect(f.gray, f.w, f.h, f.pitch, f.is_device != 0, f.frame_id, f.out, f.cap, &f.n_out,
-                             &f.stats);
-                    f.status = CCTAGB_OK;
+                    h->slot(s).pipeline().prepare_batched(f.gray, f.w, f.h, f.pitch, f.is_device != 0, h->bstream);
+                    pipes.push_back(&h->slot(s).pipeline());
+                    started.push_back(s);
                 } catch (const cctagb::Error& e) {
-                    f.status = e.status;
-                    msg[size_t(i)] = e.msg;
-                } catch (const std::exception& e) {
-                    f.status = CCTAGB_INTERNAL;
-                    msg[size_t(i)] = e.what();
-                } catch (...) {
-                    f.status = CCTAGB_INTERNAL;
-                    msg[size_t(i)] = "unknown error";
+                    fail(w0 + j, e.status, e.msg);
+                    started.push_back(-1);
                 }
             }
-        };
-        std::vector<std::thread> threads;
-        for (int s = 1; s < S; ++s) threads.emplace_back(run, s);
-        run(0);
-        for (auto& t : threads) t.join();
+            if (pipes.empty()) continue;
+            cctagb::BatchStage& bs = *h->batch[size_t(d)];
+            bs.run(pipes, h->bstream);
+            CCTAGB_CUDA(cudaEventRecord(h->bdone[size_t(d)], h->bstream));
+            h->last_timed_batch = h->batch_timing;
+            h->last_batch = d;
+            const cudaEvent_t done = h->bdone[size_t(d)];
+            bool first = true;
+            for (int j = 0; j < nw; ++j) {
+                const int s = started[size_t(j)];
+                if (s < 0) continue;
+                const int launches = first ? bs.launches() : 0;
+                first = false;
+                inflight[size_t(d)].emplace_back([&, s, j, w0, t0, done, launches, d] {
+                    cudaSetDevice(h->device);
+                    cctagb_frame& f = frames[w0 + j];
+                    try {
+                        h->slot(s).detect_batched(done, -1.f, launches, t0, f.out, f.cap, &f.n_out, &f.stats);
+                        f.stats.ms_image_stage = h->batch[size_t(d)]->elapsed_ms();
+                        f.status = CCTAGB_OK;
+                    } catch (const cctagb::Error& e) {
+                        fail(w0 + j, e.status, e.msg);
+                    } catch (const std::exception& e) {
+                        fail(w0 + j, CCTAGB_INTERNAL, e.what());
+                    } catch (...) {
+                        fail(w0 + j, CCTAGB_INTERNAL, "unknown error");
+                    }
+                });
+            }
+        }
+        joiner.f();
+        joiner.f = [] {};
         for (int i = 0; i < n; ++i)
             if (frames[i].status != CCTAGB_OK)
                 throw cctagb::Error{frames[i].status, "frame " + std::to_string(i) + ": " + msg[size_t(i)]};

@@ -11,7 +11,10 @@
 
 namespace cctagb {
 
-constexpr int kMaxLevels = 4;
+constexpr int kMaxLevels = 4;         // pyramid levels of one frame
+constexpr int kMaxBatchFrames = 16;   // frames whose image stages share one launch per kernel
+constexpr int kMaxLaunchLevels = kMaxLevels * kMaxBatchFrames;
+constexpr int kScanBlocksPerLevel = 148;  // blocks of the voter-count scan (its partial sums per level)
 
 // One pyramid level as the kernels see it.  All pointers are device memory.
 struct LevelView {
@@ -20,8 +23,10 @@ struct LevelView {
     int16_t* dx;             // W*H
     int16_t* dy;             // W*H
     uint8_t* map;            // W*H: 0 no edge, 1 weak candidate, 2 strong candidate
-    int32_t* label;          // W*H union-find parents (valid at candidates)
-    uint8_t* sroot;          // W*H strong-component flags (valid at roots)
+    uint32_t* hbits;         // 3 * WW*H: hysteresis planes C (candidates), R (tile-local strong closure), H (result)
+    uint8_t* blab;           // uf_tiles * 128: border-position -> tile component (0xff none)
+    int32_t* tcomp;          // uf_tiles * 64: union-find parents over (tile, component) ids
+    int32_t* tflag;          // uf_tiles * 64: bit 0 holds a strong pixel, bit 1 (at roots) its set does
     uint32_t* bitmap;        // WW*H final thinned edges, bit x&31 of word x>>5
     int32_t* idxmap;         // W*H edge index (valid where the bitmap is set)
     int32_t* row_count;      // H
@@ -47,7 +52,7 @@ struct LevelView {
     int nms_tx, nms_tiles;   // 30x30 output tiles
     int thin_tx, thin_tiles; // 32x16 output tiles
     int pix_blocks;          // 256-pixel blocks
-    int uf_tx, uf_tiles;     // 32x32 union-find tiles
+    int uf_tx, uf_tiles;     // 32x32 hysteresis tiles
 };
 
 struct LevelCounters {
@@ -63,10 +68,15 @@ constexpr int kErrEdgeOverflow = 1;
 constexpr int kErrSeedOverflow = 2;
 constexpr int kErrUnionFind = 4;
 
+// The levels one launch of the image-stage kernels covers: the pyramid of one
+// frame, or those of several frames back to back (frame f's level k is
+// l[f * (n / frames) + k]).  Every kernel maps its blocks over all of them.
 struct Levels {
     int n;
-    LevelView l[kMaxLevels];
-    LevelCounters* cnt;  // device, n entries
+    int frames;              // frames in the launch; n / frames levels each
+    LevelView l[kMaxLaunchLevels];
+    LevelCounters* cnt;      // device, n entries
+    int32_t* partial;        // device, n * kScanBlocksPerLevel: voter-count scan partial sums
 };
 
 struct VoteParamsDev {
@@ -121,5 +131,11 @@ struct PackSegs {
 int launch_pack(const PackSegs& p, int32_t* dst, cudaStream_t s);
 void launch_edge_level(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, uint8_t* edges_out,
                        int32_t* status_out);
+// Copies counters src[0, n) of a batched launch to each level's own (dst[i]).
+struct CounterTargets {
+    LevelCounters* dst[kMaxLaunchLevels];
+    int n;
+};
+void launch_scatter_counters(const LevelCounters* src, const CounterTargets& t, cudaStream_t s);
 
 }  // namespace cctagb

@@ -324,10 +324,29 @@ void Detector::detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_d
     (void)frame_id;
     if (!n_out || (cap > 0 && !out)) throw Error{CCTAGB_BAD_ARG, "bad output arguments"};
     if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
-    using clk = std::chrono::steady_clock;
-    const auto t0 = clk::now();
+    const auto t0 = std::chrono::steady_clock::now();
     last_tasks_.clear();
     pipe_.image_stage(gray, w, h, pitch, is_device);
+    after_image_stage(t0, w, h, out, cap, n_out, stats);
+}
+
+void Detector::detect_batched(cudaEvent_t stage_done, float stage_ms, int stage_launches,
+                              std::chrono::steady_clock::time_point t0, cctagb_marker* out, int cap, int* n_out,
+                              cctagb_stats* stats)
+{
+    if (!n_out || (cap > 0 && !out)) throw Error{CCTAGB_BAD_ARG, "bad output arguments"};
+    if (bank_.empty()) throw Error{CCTAGB_BANK_ERROR, "no marker bank for this number of crowns"};
+    last_tasks_.clear();
+    pipe_.finish_batched(stage_done, stage_ms, stage_launches);
+    int w = 0, h = 0;
+    pipe_.level_size(0, &w, &h);
+    after_image_stage(t0, w, h, out, cap, n_out, stats);
+}
+
+void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w, int h, cctagb_marker* out, int cap,
+                                 int* n_out, cctagb_stats* stats)
+{
+    using clk = std::chrono::steady_clock;
     const int nl = pipe_.levels();
 
     // Candidate stage on the host worker pool: the per-level edge sets are

@@ -3,6 +3,8 @@
 // Detection.cpp:773-999).
 #pragma once
 
+#include <chrono>
+
 #include <memory>
 #include <vector>
 
@@ -30,6 +32,12 @@ public:
 
     void detect(const uint8_t* gray, int w, int h, size_t pitch, bool is_device, int frame_id, cctagb_marker* out,
                 int cap, int* n_out, cctagb_stats* stats);
+    // The rest of a detection whose image stage ran in a batched launch
+    // (Pipeline::prepare_batched, BatchStage::run, event stage_done); t0 is
+    // the start of the frame's call, for the statistics.
+    void detect_batched(cudaEvent_t stage_done, float stage_ms, int stage_launches,
+                        std::chrono::steady_clock::time_point t0, cctagb_marker* out, int cap, int* n_out,
+                        cctagb_stats* stats);
 
     // Identification of caller-given markers (ellipse + initial center + cuts)
     // on the frame last passed to the image stage.
@@ -46,6 +54,8 @@ public:
     const std::vector<LoopTwoIn>& last_loop_two() const { return loop2in_; }
 
 private:
+    void after_image_stage(std::chrono::steady_clock::time_point t0, int w, int h, cctagb_marker* out, int cap,
+                           int* n_out, cctagb_stats* stats);
     void ensure_ident_capacity(int n);
     void ensure_cut_capacity(int nm, int npts);
     // Cut selection and identification of the h_cutin_ / h_cutpts_ /

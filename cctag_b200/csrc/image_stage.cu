@@ -93,7 +93,8 @@ __device__ __forceinline__ bool edge_bit(const LevelView& L, int x, int y)
 // levels 1..3.
 __global__ void k_pyramid3(Levels lv)
 {
-    const LevelView& L0 = lv.l[0];
+    const int base = blockIdx.z * (lv.n / lv.frames);  // this frame's level 0
+    const LevelView& L0 = lv.l[base];
     const int W3 = L0.W >> 3, H3 = L0.H >> 3;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -120,9 +121,9 @@ __global__ void k_pyramid3(Levels lv)
         for (int c = 0; c < 2; ++c)
             q2[r][c] = (q1[2 * r][2 * c] + q1[2 * r][2 * c + 1] + q1[2 * r + 1][2 * c] + q1[2 * r + 1][2 * c + 1] + 2) >> 2;
     const uint32_t q3 = (q2[0][0] + q2[0][1] + q2[1][0] + q2[1][1] + 2) >> 2;
-    const LevelView& L1 = lv.l[1];
-    const LevelView& L2 = lv.l[2];
-    const LevelView& L3 = lv.l[3];
+    const LevelView& L1 = lv.l[base + 1];
+    const LevelView& L2 = lv.l[base + 2];
+    const LevelView& L3 = lv.l[base + 3];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
         *reinterpret_cast<uint32_t*>(L1.src + size_t(4 * y + r) * L1.W + 4 * x) =
@@ -294,9 +295,25 @@ __global__ void __launch_bounds__(128) k_deriv_nms(Levels lv, VoteParamsDev vp, 
 // ------------------------------------------------------------- hysteresis --
 // The reference's stack hysteresis (cvRecode.cpp:362-394) keeps exactly the
 // 8-connected components of NMS candidates that contain a strong pixel.  Here
-// the components come from a lock-free union-find (parent <= self invariant,
-// roots linked by atomicMin), which gives the same set in any schedule.
+// the image is cut into 32x32 tiles, one warp each, lane r holding row r of
+// the tile as 32-bit masks (candidates C, strong S):
+//  1. k_hyst_tiles: the closure of S within C inside the tile (R, bit-parallel
+//     dilation: rows shifted by one bit, neighbour rows by shuffles), and the
+//     components that touch the tile border, one flood fill each, labelled
+//     per border position, with whether they hold a strong pixel;
+//  2. k_hyst_unions / k_hyst_roots: those border components joined across
+//     tile borders by a lock-free union-find over (tile, component) ids
+//     (parent <= self, roots linked by atomicMin, so any schedule gives the
+//     same sets), and each set marked strong at its root if a member is;
+//  3. k_hyst_final: per tile, R plus the border pixels of strong sets, closed
+//     within C again: the hysteresis result H, one bit per pixel.
+// A pixel is in H exactly when its component holds a strong pixel: a path to
+// one either stays in the tile (step 1) or leaves it through a border pixel
+// of its tile component, whose set is then strong (steps 2-3).
 constexpr int kUfCap = 1 << 22;
+constexpr int kTile = 32;          // hysteresis tile side
+constexpr int kBorderPos = 128;    // border positions of a tile (4 x 32, some unused)
+constexpr int kTileComps = 64;     // border components per tile (at most 62: runs on a 124-pixel cycle)
 
 __device__ __forceinline__ int uf_find(const int32_t* L, int p)
 {
@@ -323,140 +340,205 @@ __device__ __forceinline__ void uf_union(int32_t* L, int a, int b, int32_t* err)
     atomicOr(err, kErrUnionFind);
 }
 
-// Components inside one 32x32 tile, with a shared-memory union-find over
-// tile-local indices.  Tile-local row-major order is the global order
-// restricted to the tile, so the parent <= self invariant carries over when
-// the local roots are written back as global indices.
-constexpr int kUfT = 32;
-
-// Tile-local find with path halving (each visited node is pointed at its
-// grandparent; parents only decrease, so concurrent unions stay correct).
-__device__ __forceinline__ int uf_find_s(int* L, int p)
+// The closure of `seed` (a subset of c) within c, 8-connected, over the
+// warp's tile (lane = row).  Each round adds a pixel or ends the loop, so it
+// ends within the tile's 1024 pixels.
+__device__ __forceinline__ uint32_t tile_closure(uint32_t seed, uint32_t c, int lane)
 {
-    int q = *(volatile int*)&L[p];
-    int guard = 0;
-    while (q != p && guard++ < kUfT * kUfT) {
-        const int g = *(volatile int*)&L[q];
-        if (g != q) *(volatile int*)&L[p] = g;
-        p = q;
-        q = g;
+    uint32_t r = seed & c;
+    for (int it = 0; it <= kTile * kTile; ++it) {
+        uint32_t up = __shfl_up_sync(0xffffffffu, r, 1);
+        uint32_t dn = __shfl_down_sync(0xffffffffu, r, 1);
+        if (lane == 0) up = 0u;
+        if (lane == kTile - 1) dn = 0u;
+        const uint32_t v = r | up | dn;
+        const uint32_t nb = (v | (v << 1) | (v >> 1)) & c;
+        if (!__any_sync(0xffffffffu, nb != r)) break;
+        r = nb;
     }
-    return p;
+    return r;
 }
 
-__device__ __forceinline__ void uf_union_s(int* L, int a, int b)
+// Border position of tile pixel (x, y) (tile coordinates), -1 inside:
+// row 0 -> x, row 31 -> 32 + x, column 0 -> 64 + y, column 31 -> 96 + y.
+__device__ __forceinline__ int border_pos(int x, int y)
 {
-    for (int it = 0; it < kUfT * kUfT; ++it) {
-        a = uf_find_s(L, a);
-        b = uf_find_s(L, b);
-        if (a == b) return;
-        if (a > b) { const int tmp = a; a = b; b = tmp; }
-        const int old = atomicMin(&L[b], a);
-        if (old == b) return;
-        b = old;
-    }
+    if (y == 0) return x;
+    if (y == kTile - 1) return kTile + x;
+    if (x == 0) return 2 * kTile + y;
+    if (x == kTile - 1) return 3 * kTile + y;
+    return -1;
 }
 
-// Components inside one 32x32 tile, on horizontal runs: one warp per row
-// reads the row as a 32-bit candidate mask; every pixel takes its run's first
-// pixel as parent (no atomics within a row); rows are joined by unions of
-// runs.  A run of row y and a run of row y-1 that touch (8-connectivity) meet
-// at a pixel of one of them that starts its run, so a pixel only tries the
-// unions where it starts its run or its upper neighbour starts one.
-__global__ void __launch_bounds__(256) k_hyst_local(Levels lv)
+// Warp w of the launch: its level and tile (tiles of all levels back to back).
+__device__ __forceinline__ int level_of_tile(const Levels& lv, int g, int& tile)
 {
-    __shared__ int s_lab[kUfT * kUfT];
-    __shared__ uint32_t s_mask[kUfT];
-    int tile;
-    const int l = level_of_block(lv, blockIdx.x, &LevelView::uf_tiles, tile);
-    const LevelView& L = lv.l[l];
-    const int x0 = (tile % L.uf_tx) * kUfT, y0 = (tile / L.uf_tx) * kUfT;
+    int l = 0;
+    while (l < lv.n - 1 && g >= lv.l[l].uf_tiles) {
+        g -= lv.l[l].uf_tiles;
+        ++l;
+    }
+    tile = g;
+    return l;
+}
+
+__device__ __forceinline__ uint32_t* plane_c(const LevelView& L) { return L.hbits; }
+__device__ __forceinline__ uint32_t* plane_r(const LevelView& L) { return L.hbits + size_t(L.WW) * L.H; }
+__device__ __forceinline__ uint32_t* plane_h(const LevelView& L) { return L.hbits + 2 * size_t(L.WW) * L.H; }
+
+constexpr int kHystWarps = 4;
+
+__global__ void __launch_bounds__(32 * kHystWarps) k_hyst_tiles(Levels lv, int total_tiles)
+{
+    __shared__ uint8_t s_lab[kHystWarps][kBorderPos];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = x0 + lane;
-    for (int r = warp; r < kUfT; r += 8) {
-        const int y = y0 + r;
-        const bool c = x < L.W && y < L.H && L.map[size_t(y) * L.W + x] != 0;
-        const uint32_t m = __ballot_sync(0xffffffffu, c);
-        if (lane == 0) s_mask[r] = m;
-        const uint32_t starts = m & ~(m << 1);
-        const int start = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
-        s_lab[r * kUfT + lane] = c ? r * kUfT + start : -1;
-    }
-    __syncthreads();
-    for (int r = 1 + warp; r < kUfT; r += 8) {
-        const uint32_t m = s_mask[r], up = s_mask[r - 1];
-        if (!((m >> lane) & 1u)) continue;
-        const bool isStart = lane == 0 || !((m >> (lane - 1)) & 1u);
-        const uint32_t upStarts = up & ~(up << 1);
-        const int i = r * kUfT + lane;
-#pragma unroll
-        for (int d = -1; d <= 1; ++d) {
-            const int xx = lane + d;
-            if (xx < 0 || xx >= kUfT || !((up >> xx) & 1u)) continue;
-            if (isStart || ((upStarts >> xx) & 1u)) uf_union_s(s_lab, i, (r - 1) * kUfT + xx);
+    const int g = blockIdx.x * kHystWarps + warp;
+    if (g >= total_tiles) return;
+    int tile;
+    const int l = level_of_tile(lv, g, tile);
+    const LevelView& L = lv.l[l];
+    const int tx = tile % L.uf_tx, ty = tile / L.uf_tx;
+    const int x0 = tx * kTile, y0 = ty * kTile;
+    const int rows = min(kTile, L.H - y0), cols = min(kTile, L.W - x0);
+    // row masks of the tile: lane r keeps row r
+    uint32_t c = 0u, st = 0u;
+#pragma unroll 4
+    for (int r = 0; r < kTile; ++r) {
+        uint8_t v = 0;
+        if (r < rows && lane < cols) v = L.map[size_t(y0 + r) * L.W + x0 + lane];
+        const uint32_t cm = __ballot_sync(0xffffffffu, v != 0), sm = __ballot_sync(0xffffffffu, v == 2);
+        if (lane == r) {
+            c = cm;
+            st = sm;
         }
     }
-    __syncthreads();
-    // run starts resolve their roots; every pixel then reads its run's root
-    for (int r = warp; r < kUfT; r += 8) {
-        const uint32_t m = s_mask[r];
-        const bool isStart = ((m >> lane) & 1u) && (lane == 0 || !((m >> (lane - 1)) & 1u));
-        if (isStart) s_lab[r * kUfT + lane] = uf_find_s(s_lab, r * kUfT + lane);
+    const uint32_t R = tile_closure(st, c, lane);
+    if (lane < rows) {
+        const size_t w = size_t(y0 + lane) * L.WW + tx;
+        plane_c(L)[w] = c;
+        plane_r(L)[w] = R;
     }
-    __syncthreads();
-    for (int r = warp; r < kUfT; r += 8) {
-        const uint32_t m = s_mask[r];
-        if (!((m >> lane) & 1u)) continue;
-        const uint32_t starts = m & ~(m << 1);
-        const int start = 31 - __clz(starts & (0xffffffffu >> (31 - lane)));
-        const int root = s_lab[r * kUfT + start];
-        const int y = y0 + r;
-        const size_t p = size_t(y) * L.W + x;
-        L.label[p] = (y0 + root / kUfT) * L.W + (x0 + root % kUfT);
-        L.sroot[p] = 0;
+    for (int i = lane; i < kBorderPos; i += 32) s_lab[warp][i] = 0xff;
+    __syncwarp();
+    // border components, one flood fill each from an unlabelled border pixel
+    const uint32_t bmask = (lane == 0 || lane == kTile - 1) ? c : (c & (1u | (1u << (kTile - 1))));
+    uint32_t unl = bmask;
+    uint64_t strong = 0ull;
+    int ncomp = 0;
+    while (__any_sync(0xffffffffu, unl != 0u)) {
+        const uint32_t have = __ballot_sync(0xffffffffu, unl != 0u);
+        const int sl = __ffs(have) - 1;
+        const uint32_t sb = __shfl_sync(0xffffffffu, unl & (0u - unl), sl);
+        const uint32_t m = tile_closure(lane == sl ? sb : 0u, c, lane);
+        if (ncomp >= kTileComps) {  // cannot happen (<= 62 components); flagged, not silent
+            if (lane == 0) atomicOr(&lv.cnt[l].err, kErrUnionFind);
+            break;
+        }
+        if (__any_sync(0xffffffffu, (m & R) != 0u)) strong |= 1ull << ncomp;
+        uint32_t bm = m & bmask;
+        while (bm) {
+            const int b = __ffs(bm) - 1;
+            bm &= bm - 1;
+            s_lab[warp][border_pos(b, lane)] = uint8_t(ncomp);
+        }
+        unl &= ~m;
+        ++ncomp;
     }
+    __syncwarp();
+    const size_t base = size_t(tile) * kTileComps;
+    for (int k = lane; k < kTileComps; k += 32) {
+        L.tcomp[base + k] = int32_t(base + k);
+        L.tflag[base + k] = (k < ncomp && ((strong >> k) & 1ull)) ? 1 : 0;
+    }
+    for (int i = lane; i < kBorderPos; i += 32) L.blab[size_t(tile) * kBorderPos + i] = s_lab[warp][i];
 }
 
-// 8-connections that cross a tile border: the first row and column of a tile
-// look up/left, the last column looks up-right.  96 threads per tile.
-__global__ void __launch_bounds__(96) k_hyst_border(Levels lv)
+// The (tile, component) id of border pixel (x, y) of the level.
+__device__ __forceinline__ int border_comp(const LevelView& L, int x, int y)
+{
+    const int tile = (y / kTile) * L.uf_tx + x / kTile;
+    const int lab = L.blab[size_t(tile) * kBorderPos + border_pos(x % kTile, y % kTile)];
+    return tile * kTileComps + lab;
+}
+
+__device__ __forceinline__ bool cand_bit(const LevelView& L, int x, int y)
+{
+    return (plane_c(L)[size_t(y) * L.WW + (x >> 5)] >> (x & 31)) & 1u;
+}
+
+// Unions across tile borders: the first row of a tile with the row above
+// (three neighbours each), the first column with the column to the left.
+// Every 8-neighbour pair that straddles a tile border meets here.
+__global__ void __launch_bounds__(64) k_hyst_unions(Levels lv)
 {
     int tile;
     const int l = level_of_block(lv, blockIdx.x, &LevelView::uf_tiles, tile);
     const LevelView& L = lv.l[l];
-    const int x0 = (tile % L.uf_tx) * kUfT, y0 = (tile / L.uf_tx) * kUfT;
+    const int x0 = (tile % L.uf_tx) * kTile, y0 = (tile / L.uf_tx) * kTile;
     const int t = threadIdx.x;
-    int x, y;
-    if (t < 32) { x = x0 + t; y = y0; }                 // first row
-    else if (t < 64) { x = x0; y = y0 + (t - 32); }     // first column
-    else { x = x0 + kUfT - 1; y = y0 + (t - 64); }      // last column
+    const bool row = t < 32;
+    const int x = row ? x0 + t : x0, y = row ? y0 : y0 + (t - 32);
     if (x >= L.W || y >= L.H) return;
-    const int W = L.W;
-    const int p = y * W + x;
-    if (!L.map[p]) return;
+    if (row ? y == 0 : x == 0) return;
+    if (!cand_bit(L, x, y)) return;
     int32_t* err = &lv.cnt[l].err;
-    const bool firstRow = (y == y0), firstCol = (x == x0), lastCol = (x == x0 + kUfT - 1);
-    if (firstCol && x > 0 && L.map[p - 1]) uf_union(L.label, p, p - 1, err);
-    if (y > 0) {
-        const int u = p - W;
-        if (x > 0 && (firstRow || firstCol) && L.map[u - 1]) uf_union(L.label, p, u - 1, err);
-        if (firstRow && L.map[u]) uf_union(L.label, p, u, err);
-        if (x + 1 < W && (firstRow || lastCol) && L.map[u + 1]) uf_union(L.label, p, u + 1, err);
+    const int a = border_comp(L, x, y);
+    for (int d = -1; d <= 1; ++d) {
+        const int qx = row ? x + d : x - 1, qy = row ? y - 1 : y + d;
+        if (qx < 0 || qx >= L.W || qy < 0 || qy >= L.H) continue;
+        if (qx / kTile == x / kTile && qy / kTile == y / kTile) continue;  // same tile: joined in step 1
+        if (cand_bit(L, qx, qy)) uf_union(L.tcomp, a, border_comp(L, qx, qy), err);
     }
 }
 
-__global__ void k_hyst_compress_mark(Levels lv)
+// Each set with a strong member is marked strong at its root.
+__global__ void __launch_bounds__(kTileComps) k_hyst_roots(Levels lv)
 {
-    int blk;
-    const int l = level_of_block(lv, blockIdx.x, &LevelView::pix_blocks, blk);
+    int tile;
+    const int l = level_of_block(lv, blockIdx.x, &LevelView::uf_tiles, tile);
     const LevelView& L = lv.l[l];
-    const int p = blk * blockDim.x + threadIdx.x;
-    if (p >= L.W * L.H) return;
-    const uint8_t cls = L.map[p];
-    if (!cls) return;
-    const int r = uf_find(L.label, p);
-    L.label[p] = r;
-    if (cls == 2) L.sroot[r] = 1;
+    const int id = tile * kTileComps + threadIdx.x;
+    if (L.tflag[id] & 1) atomicOr(&L.tflag[uf_find(L.tcomp, id)], 2);
+}
+
+__global__ void __launch_bounds__(32 * kHystWarps) k_hyst_final(Levels lv, int total_tiles)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = blockIdx.x * kHystWarps + warp;
+    if (g >= total_tiles) return;
+    int tile;
+    const int l = level_of_tile(lv, g, tile);
+    const LevelView& L = lv.l[l];
+    const int tx = tile % L.uf_tx, ty = tile / L.uf_tx;
+    const int y0 = ty * kTile;
+    const int rows = min(kTile, L.H - y0);
+    uint32_t c = 0u, R = 0u;
+    if (lane < rows) {
+        const size_t w = size_t(y0 + lane) * L.WW + tx;
+        c = plane_c(L)[w];
+        R = plane_r(L)[w];
+    }
+    // which of the tile's components belong to a strong set (two per lane,
+    // the finds side by side; unused components are their own roots, flag 0)
+    const int base = tile * kTileComps;
+    const bool s0 = L.tflag[uf_find(L.tcomp, base + lane)] & 2;
+    const bool s1 = L.tflag[uf_find(L.tcomp, base + 32 + lane)] & 2;
+    const uint64_t strongSets =
+        uint64_t(__ballot_sync(0xffffffffu, s0)) | (uint64_t(__ballot_sync(0xffffffffu, s1)) << 32);
+    // border pixels of those components seed the closure
+    __shared__ uint32_t s_lab[kHystWarps][kBorderPos / 4];
+    s_lab[warp][lane] = reinterpret_cast<const uint32_t*>(L.blab + size_t(tile) * kBorderPos)[lane];
+    __syncwarp();
+    const uint8_t* lab = reinterpret_cast<const uint8_t*>(s_lab[warp]);
+    const uint32_t bmask = (lane == 0 || lane == kTile - 1) ? c : (c & (1u | (1u << (kTile - 1))));
+    uint32_t seed = 0u, bm = strongSets ? (bmask & ~R) : 0u;
+    while (bm) {
+        const int b = __ffs(bm) - 1;
+        bm &= bm - 1;
+        if ((strongSets >> lab[border_pos(b, lane)]) & 1ull) seed |= 1u << b;
+    }
+    const uint32_t H = __any_sync(0xffffffffu, seed != 0u) ? tile_closure(R | seed, c, lane) : R;
+    if (lane < rows) plane_h(L)[size_t(y0 + lane) * L.WW + tx] = H;
 }
 
 // ------------------------------------------------ final edges + thinning --
@@ -480,10 +562,7 @@ __global__ void __launch_bounds__(kThX * kThY) k_final_thin(Levels lv)
         const int r = i / (kThX + 4), c = i % (kThX + 4);
         const int x = x0 - 2 + c, y = y0 - 2 + r;
         uint8_t e = 0;
-        if (x >= 0 && x < W && y >= 0 && y < H) {
-            const size_t p = size_t(y) * W + x;
-            if (L.map[p]) e = L.sroot[L.label[p]];
-        }
+        if (x >= 0 && x < W && y >= 0 && y < H) e = (plane_h(L)[size_t(y) * L.WW + (x >> 5)] >> (x & 31)) & 1u;
         s_e[r][c] = e;
     }
     __syncthreads();
@@ -759,7 +838,7 @@ __global__ void k_vote(Levels lv, VoteParamsDev vp)
 
 // ----------------------------------------------------- voter lists (CSR) --
 // Chunked exclusive scan of nvotes[0, E) into voff, all levels, fixed grid.
-constexpr int kScanBlocks = 148;
+constexpr int kScanBlocks = kScanBlocksPerLevel;
 constexpr int kScanThreads = 1024;
 
 __global__ void __launch_bounds__(kScanThreads) k_vscan_partial(Levels lv, int32_t* partial)
@@ -952,21 +1031,31 @@ void upload_constants(const float*, int, int)
     // device reset sees them too.
 }
 
+// fused: every frame has 4 levels and sides that are multiples of 8 (one
+// k_pyramid3 launch, blockIdx.z = frame); else one resize launch per level.
 static void launch_pyramid(const Levels& lv, cudaStream_t s, bool fused)
 {
-    if (lv.n < 2) return;
-    if (fused && lv.n == 4) {
+    const int lpf = lv.n / lv.frames;
+    if (lpf < 2) return;
+    if (fused && lpf == 4) {
+        int w8 = 0, h8 = 0;
+        for (int f = 0; f < lv.frames; ++f) {
+            w8 = std::max(w8, lv.l[f * lpf].W / 8);
+            h8 = std::max(h8, lv.l[f * lpf].H / 8);
+        }
         const dim3 blk(32, 8);
-        const dim3 grd((lv.l[0].W / 8 + 31) / 32, (lv.l[0].H / 8 + 7) / 8);
+        const dim3 grd((w8 + 31) / 32, (h8 + 7) / 8, lv.frames);
         k_pyramid3<<<grd, blk, 0, s>>>(lv);
         return;
     }
-    for (int l = 1; l < lv.n; ++l) {
-        const dim3 blk(32, 8);
-        const dim3 grd((lv.l[l].W + 31) / 32, (lv.l[l].H + 7) / 8);
-        k_resize_level<<<grd, blk, 0, s>>>(lv.l[l - 1].src, lv.l[l - 1].W, lv.l[l - 1].H, lv.l[l].src, lv.l[l].W,
-                                           lv.l[l].H);
-    }
+    for (int f = 0; f < lv.frames; ++f)
+        for (int k = 1; k < lpf; ++k) {
+            const LevelView& a = lv.l[f * lpf + k - 1];
+            const LevelView& b = lv.l[f * lpf + k];
+            const dim3 blk(32, 8);
+            const dim3 grd((b.W + 31) / 32, (b.H + 7) / 8);
+            k_resize_level<<<grd, blk, 0, s>>>(a.src, a.W, a.H, b.src, b.W, b.H);
+        }
 }
 
 const char* stage_name(int k)
@@ -1021,11 +1110,13 @@ static void launch_edges(const Levels& lv, const VoteParamsDev& vp, cudaStream_t
 {
     k_deriv_nms<<<total_of(lv, &LevelView::nms_tiles), 128, 0, s>>>(lv, vp, write_derivs);
     mark(ev, kStDerivNms + 1, s);
-    const int pb = total_of(lv, &LevelView::pix_blocks);
-    k_hyst_local<<<total_of(lv, &LevelView::uf_tiles), 256, 0, s>>>(lv);
-    k_hyst_border<<<total_of(lv, &LevelView::uf_tiles), 96, 0, s>>>(lv);
+    const int tiles = total_of(lv, &LevelView::uf_tiles);
+    const int hb = (tiles + kHystWarps - 1) / kHystWarps;
+    k_hyst_tiles<<<hb, 32 * kHystWarps, 0, s>>>(lv, tiles);
+    k_hyst_unions<<<tiles, 64, 0, s>>>(lv);
     mark(ev, kStHystMerge + 1, s);
-    k_hyst_compress_mark<<<pb, 256, 0, s>>>(lv);
+    k_hyst_roots<<<tiles, kTileComps, 0, s>>>(lv);
+    k_hyst_final<<<hb, 32 * kHystWarps, 0, s>>>(lv, tiles);
     mark(ev, kStHystCompress + 1, s);
     k_final_thin<<<total_of(lv, &LevelView::thin_tiles), dim3(kThX, kThY), 0, s>>>(lv);
     mark(ev, kStFinalThin + 1, s);
@@ -1037,12 +1128,10 @@ static void launch_edges(const Levels& lv, const VoteParamsDev& vp, cudaStream_t
     mark(ev, kStEmit + 1, s);
 }
 
-// The partial sums of the voter-count scan live in the counters allocation
-// (see Pipeline): cnt + 8 ints per level, then kMaxLevels*kScanBlocks ints.
 void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s, bool fused_pyramid,
                         cudaEvent_t* ev)
 {
-    CCTAGB_CUDA(cudaMemsetAsync(lv.cnt, 0, sizeof(LevelCounters) * kMaxLevels, s));
+    CCTAGB_CUDA(cudaMemsetAsync(lv.cnt, 0, sizeof(LevelCounters) * lv.n, s));
     mark(ev, 0, s);
     launch_pyramid(lv, s, fused_pyramid);
     mark(ev, kStPyramid + 1, s);
@@ -1052,9 +1141,8 @@ void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t 
     mark(ev, kStWalk + 1, s);
     k_vote<<<G, 256, 0, s>>>(lv, vp);
     mark(ev, kStVote + 1, s);
-    int32_t* partial = reinterpret_cast<int32_t*>(lv.cnt + kMaxLevels);
-    k_vscan_partial<<<kScanBlocks, kScanThreads, 0, s>>>(lv, partial);
-    k_vscan_final<<<kScanBlocks, kScanThreads, 0, s>>>(lv, partial);
+    k_vscan_partial<<<kScanBlocks, kScanThreads, 0, s>>>(lv, lv.partial);
+    k_vscan_final<<<kScanBlocks, kScanThreads, 0, s>>>(lv, lv.partial);
     mark(ev, kStVoterScan + 1, s);
     k_vfill<<<G, 256, 0, s>>>(lv);
     mark(ev, kStVoterFill + 1, s);
@@ -1066,7 +1154,7 @@ void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t 
 
 void launch_canny_only(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s)
 {
-    CCTAGB_CUDA(cudaMemsetAsync(lv.cnt, 0, sizeof(LevelCounters) * kMaxLevels, s));
+    CCTAGB_CUDA(cudaMemsetAsync(lv.cnt, 0, sizeof(LevelCounters) * lv.n, s));
     launch_edges(lv, vp, s, 0, nullptr);
     CCTAGB_CUDA(cudaGetLastError());
 }
@@ -1084,6 +1172,18 @@ __global__ void k_bitmap_to_bytes(Levels lv, uint8_t* out)
     }
 }
 
+__global__ void k_scatter_counters(const LevelCounters* __restrict__ src, CounterTargets t)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < t.n) *t.dst[i] = src[i];
+}
+
+void launch_scatter_counters(const LevelCounters* src, const CounterTargets& t, cudaStream_t s)
+{
+    k_scatter_counters<<<1, kMaxLaunchLevels, 0, s>>>(src, t);
+    CCTAGB_CUDA(cudaGetLastError());
+}
+
 __global__ void k_copy_status(const LevelCounters* cnt, int32_t* status)
 {
     *status = cnt->err;
@@ -1094,9 +1194,11 @@ void launch_edge_level(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s
 {
     const LevelView& L = lv.l[0];
     k_deriv_nms<<<L.nms_tiles, 128, 0, s>>>(lv, vp, 1);
-    k_hyst_local<<<L.uf_tiles, 256, 0, s>>>(lv);
-    k_hyst_border<<<L.uf_tiles, 96, 0, s>>>(lv);
-    k_hyst_compress_mark<<<L.pix_blocks, 256, 0, s>>>(lv);
+    const int hb = (L.uf_tiles + kHystWarps - 1) / kHystWarps;
+    k_hyst_tiles<<<hb, 32 * kHystWarps, 0, s>>>(lv, L.uf_tiles);
+    k_hyst_unions<<<L.uf_tiles, 64, 0, s>>>(lv);
+    k_hyst_roots<<<L.uf_tiles, kTileComps, 0, s>>>(lv);
+    k_hyst_final<<<hb, 32 * kHystWarps, 0, s>>>(lv, L.uf_tiles);
     k_final_thin<<<L.thin_tiles, dim3(kThX, kThY), 0, s>>>(lv);
     k_bitmap_to_bytes<<<148 * 4, 256, 0, s>>>(lv, edges_out);
     if (status_out) k_copy_status<<<1, 1, 0, s>>>(lv.cnt, status_out);

@@ -7,7 +7,7 @@
 // has no handle and only owns the frame and output buffers.  This entry point
 // runs the edge stage of one frame (9x9 derivatives, Canny NMS, hysteresis,
 // thinning) with the caller's input and output buffers and keeps its own
-// scratch (class map, union-find labels, strong-component flags, edge bitmap,
+// scratch (class map, hysteresis bit planes and tile components, edge bitmap,
 // row counts, counters) in the file-scope device array below.  It calls no
 // cudaMalloc, cudaFree or allocating library routine.
 //
@@ -15,7 +15,7 @@
 //  * at most kNoAllocMaxPixels pixels and kNoAllocMaxSide per side, frame rows
 //    contiguous (pitch == width); larger frames are rejected with
 //    CCTAGB_TOO_LARGE;
-//  * the array (about 6.4 MB) is held by every GPU that loads the library,
+//  * the array (about 2.5 MB) is held by every GPU that loads the library,
 //    until the process exits;
 //  * the first call on a device (in each CUDA context: after a
 //    cudaDeviceReset the next call does it again) resolves the array's device
@@ -45,11 +45,16 @@ constexpr size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign;
 // Layout of the scratch array.
 constexpr size_t kOffCounters = 0;
 constexpr size_t kOffRowCount = align_up(kOffCounters + sizeof(LevelCounters));
-constexpr size_t kOffMap = align_up(kOffRowCount + sizeof(int32_t) * kNoAllocMaxSide);
-constexpr size_t kOffLabel = align_up(kOffMap + size_t(kNoAllocMaxPixels));
-constexpr size_t kOffSroot = align_up(kOffLabel + sizeof(int32_t) * size_t(kNoAllocMaxPixels));
-constexpr size_t kOffBitmap = align_up(kOffSroot + size_t(kNoAllocMaxPixels));
+// bitmap words of one plane: ceil(w / 32) * h <= w h / 32 + h
 constexpr size_t kBitmapWords = size_t(kNoAllocMaxPixels) / 32 + kNoAllocMaxSide;
+// 32x32 tiles: ceil(w / 32) ceil(h / 32) <= w h / 1024 + (w + h) / 32 + 1
+constexpr size_t kMaxTiles = size_t(kNoAllocMaxPixels) / 1024 + 2 * kNoAllocMaxSide / 32 + 1;
+constexpr size_t kOffMap = align_up(kOffRowCount + sizeof(int32_t) * kNoAllocMaxSide);
+constexpr size_t kOffHyst = align_up(kOffMap + size_t(kNoAllocMaxPixels));           // 3 bitmap planes
+constexpr size_t kOffBlab = align_up(kOffHyst + 3 * sizeof(uint32_t) * kBitmapWords);  // 128 B per tile
+constexpr size_t kOffTcomp = align_up(kOffBlab + 128 * kMaxTiles);                     // 64 ints per tile
+constexpr size_t kOffTflag = align_up(kOffTcomp + 64 * sizeof(int32_t) * kMaxTiles);  // 64 ints per tile
+constexpr size_t kOffBitmap = align_up(kOffTflag + 64 * sizeof(int32_t) * kMaxTiles);
 constexpr size_t kScratchBytes = align_up(kOffBitmap + sizeof(uint32_t) * kBitmapWords);
 
 constexpr int kMaxDevices = 64;
@@ -139,6 +144,7 @@ extern "C" cctagb_status cctagb_edges_noalloc(const uint8_t* d_gray, int w, int 
     }
     Levels lv{};
     lv.n = 1;
+    lv.frames = 1;
     lv.cnt = reinterpret_cast<LevelCounters*>(base + kOffCounters);
     LevelView& L = lv.l[0];
     L.W = w;
@@ -148,8 +154,10 @@ extern "C" cctagb_status cctagb_edges_noalloc(const uint8_t* d_gray, int w, int 
     L.dx = d_dx;
     L.dy = d_dy;
     L.map = base + kOffMap;
-    L.label = reinterpret_cast<int32_t*>(base + kOffLabel);
-    L.sroot = base + kOffSroot;
+    L.hbits = reinterpret_cast<uint32_t*>(base + kOffHyst);
+    L.blab = base + kOffBlab;
+    L.tcomp = reinterpret_cast<int32_t*>(base + kOffTcomp);
+    L.tflag = reinterpret_cast<int32_t*>(base + kOffTflag);
     L.bitmap = reinterpret_cast<uint32_t*>(base + kOffBitmap);
     L.row_count = reinterpret_cast<int32_t*>(base + kOffRowCount);
     L.nms_tx = (w + 29) / 30;

@@ -107,8 +107,11 @@ void Pipeline::alloc(int max_w, int max_h)
         v.dx = dev_alloc<int16_t>(allocs_, px);
         v.dy = dev_alloc<int16_t>(allocs_, px);
         v.map = dev_alloc<uint8_t>(allocs_, px);
-        v.label = dev_alloc<int32_t>(allocs_, px);
-        v.sroot = dev_alloc<uint8_t>(allocs_, px);
+        const size_t tiles = size_t((w + 31) / 32) * size_t((h + 31) / 32);
+        v.hbits = dev_alloc<uint32_t>(allocs_, 3 * size_t((w + 31) / 32) * h);
+        v.blab = dev_alloc<uint8_t>(allocs_, tiles * 128);
+        v.tcomp = dev_alloc<int32_t>(allocs_, tiles * 64);
+        v.tflag = dev_alloc<int32_t>(allocs_, tiles * 64);
         v.bitmap = dev_alloc<uint32_t>(allocs_, size_t((w + 31) / 32) * h);
         v.idxmap = dev_alloc<int32_t>(allocs_, px);
         v.row_count = dev_alloc<int32_t>(allocs_, h);
@@ -158,7 +161,7 @@ void Pipeline::alloc(int max_w, int max_h)
     CCTAGB_CUDA(cudaMallocHost(&h_pack_, size_t(pack_words_) * 4));
     host_allocs_.push_back(h_pack_);
     // Counters followed by the partial sums of the voter-count scan.
-    const size_t cnt_bytes = sizeof(LevelCounters) * kMaxLevels + sizeof(int32_t) * kMaxLevels * 148;
+    const size_t cnt_bytes = sizeof(LevelCounters) * kMaxLevels + sizeof(int32_t) * kMaxLevels * kScanBlocksPerLevel;
     d_cnt_ = reinterpret_cast<LevelCounters*>(dev_alloc<uint8_t>(allocs_, cnt_bytes));
     CCTAGB_CUDA(cudaMemset(d_cnt_, 0, cnt_bytes));
     CCTAGB_CUDA(cudaMallocHost(&h_cnt_, sizeof(LevelCounters) * kMaxLevels));
@@ -169,7 +172,9 @@ void Pipeline::set_views(int w, int h, int nl)
 {
     if (w > max_w_ || h > max_h_) throw Error{CCTAGB_TOO_LARGE, "frame larger than the handle's maximum"};
     lv_.n = nl;
+    lv_.frames = 1;
     lv_.cnt = d_cnt_;
+    lv_.partial = reinterpret_cast<int32_t*>(d_cnt_ + kMaxLevels);
     for (int l = 0; l < nl; ++l) {
         if (w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "frame too small for the number of pyramid levels"};
         LevelView v = la_[l].v;
@@ -251,6 +256,127 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
     }
     sync_counters(st);
     CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
+}
+
+void Pipeline::prepare_batched(const uint8_t* gray, int w, int h, size_t pitch, bool is_device, cudaStream_t s)
+{
+    if (!gray || w < 1 || h < 1 || pitch < size_t(w)) throw Error{CCTAGB_BAD_ARG, "bad frame arguments"};
+    set_views(w, h, params_.numberOfProcessedMultiresLayers);
+    // the batch stream starts after all earlier work of this pipeline
+    CCTAGB_CUDA(cudaEventRecord(ev_in_, stream_));
+    CCTAGB_CUDA(cudaStreamWaitEvent(s, ev_in_, 0));
+    CCTAGB_CUDA(cudaMemcpy2DAsync(lv_.l[0].src, w, gray, pitch, w, h,
+                                  is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    h2d_bytes_ = is_device ? 0 : (long long)w * h;
+    d2h_bytes_ = 0;
+    launches_ = 0;
+}
+
+void Pipeline::finish_batched(cudaEvent_t done, float stage_ms, int launches)
+{
+    CCTAGB_CUDA(cudaStreamWaitEvent(stream_, done, 0));
+    sync_counters(stream_);
+    last_ms_ = stage_ms;
+    launches_ = launches;
+}
+
+// ---------------------------------------------------------------- batches --
+BatchStage::BatchStage()
+{
+    CCTAGB_CUDA(cudaMalloc(&d_cnt_, sizeof(LevelCounters) * kMaxLaunchLevels));
+    CCTAGB_CUDA(cudaMalloc(&d_partial_, sizeof(int32_t) * kMaxLaunchLevels * kScanBlocksPerLevel));
+    CCTAGB_CUDA(cudaEventCreate(&ev0_));
+    CCTAGB_CUDA(cudaEventCreate(&ev1_));
+}
+
+BatchStage::~BatchStage()
+{
+    if (graph_) cudaGraphExecDestroy(graph_);
+    for (cudaEvent_t e : st_ev_)
+        if (e) cudaEventDestroy(e);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (d_cnt_) cudaFree(d_cnt_);
+    if (d_partial_) cudaFree(d_partial_);
+}
+
+void BatchStage::set_stage_timing(bool on)
+{
+    if (on && !st_ev_[0])
+        for (cudaEvent_t& e : st_ev_) CCTAGB_CUDA(cudaEventCreate(&e));
+    timing_ = on;
+    std::fill(stage_ms_, stage_ms_ + kStageCount, 0.f);
+}
+
+void BatchStage::run(const std::vector<Pipeline*>& pipes, cudaStream_t s)
+{
+    const int nf = int(pipes.size());
+    if (nf < 1 || nf > kMaxBatchFrames) throw Error{CCTAGB_INTERNAL, "batched image stage: bad frame count"};
+    lv_.n = 0;
+    lv_.frames = nf;
+    lv_.cnt = d_cnt_;
+    lv_.partial = d_partial_;
+    CounterTargets tg{};
+    bool fused = true;
+    std::vector<Key> key;
+    for (Pipeline* p : pipes) {
+        const Levels& v = p->level_views();
+        if (v.n != pipes[0]->level_views().n) throw Error{CCTAGB_INTERNAL, "batched frames differ in level count"};
+        fused = fused && v.n == 4 && v.l[0].W % 8 == 0 && v.l[0].H % 8 == 0;
+        for (int l = 0; l < v.n; ++l) {
+            tg.dst[lv_.n] = p->device_counters() + l;
+            lv_.l[lv_.n++] = v.l[l];
+        }
+        key.push_back({p, v.l[0].W, v.l[0].H});
+    }
+    tg.n = lv_.n;
+    const VoteParamsDev& vp = pipes[0]->vote_params();
+    // kernels: pyramid (1 fused or one per level), 14 image-stage kernels, the counter scatter
+    launches_ = (fused ? 1 : lv_.n - nf) + 14 + 1;
+    if (timing_) {
+        launch_gate(s, 2000);
+        CCTAGB_CUDA(cudaEventRecord(ev0_, s));
+        launch_image_stage(lv_, vp, s, fused, st_ev_);
+        launch_scatter_counters(d_cnt_, tg, s);
+        CCTAGB_CUDA(cudaEventRecord(ev1_, s));
+        CCTAGB_CUDA(cudaEventSynchronize(ev1_));
+        CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
+        for (int k = 0; k < kStageCount; ++k) CCTAGB_CUDA(cudaEventElapsedTime(&stage_ms_[k], st_ev_[k], st_ev_[k + 1]));
+        return;
+    }
+    if (!graph_ || key != key_) {
+        if (graph_) {
+            cudaGraphExecDestroy(graph_);
+            graph_ = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        CCTAGB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        try {
+            launch_image_stage(lv_, vp, s, fused, nullptr);
+            launch_scatter_counters(d_cnt_, tg, s);
+        } catch (...) {
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        CCTAGB_CUDA(cudaStreamEndCapture(s, &g));
+        const cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+        cudaGraphDestroy(g);
+        CCTAGB_CUDA(e);
+        key_ = key;
+    }
+    CCTAGB_CUDA(cudaEventRecord(ev0_, s));
+    CCTAGB_CUDA(cudaGraphLaunch(graph_, s));
+    CCTAGB_CUDA(cudaEventRecord(ev1_, s));
+}
+
+float BatchStage::finish_ms()
+{
+    if (!timing_) {
+        CCTAGB_CUDA(cudaEventSynchronize(ev1_));
+        CCTAGB_CUDA(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
+    }
+    return last_ms_;
 }
 
 void Pipeline::set_stage_timing(bool on)

@@ -59,6 +59,14 @@ public:
 
     // Pyramid .. seeds for one frame; results stay on the device.
     void image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool is_device);
+    // The batched form of image_stage (see BatchStage): the views of a w x h
+    // frame and its upload on the batch stream s ...
+    void prepare_batched(const uint8_t* gray, int w, int h, size_t pitch, bool is_device, cudaStream_t s);
+    // ... and, once the batched launch has recorded `done`, this frame's
+    // counters on the host (stage_ms and launches go to the statistics).
+    void finish_batched(cudaEvent_t done, float stage_ms, int launches);
+    LevelCounters* device_counters() const { return d_cnt_; }
+    const VoteParamsDev& vote_params() const { return vp_; }
     // Canny + thinning from caller derivatives (level 0 buffers).
     void canny_only(const int16_t* dx, const int16_t* dy, int w, int h, uint8_t* edges_out);
 
@@ -157,6 +165,57 @@ private:
     bool timing_ = false;
     cudaEvent_t st_ev_[kStageCount + 1] = {};
     float stage_ms_[kStageCount] = {};
+};
+
+// The image stages of several frames (each prepared in its own Pipeline's
+// buffers) with one launch per kernel: the kernels map their blocks over the
+// levels of all the frames, so a batch of 1080p frames fills the GPU where
+// one frame's stage leaves it latency-bound.  The launches are captured into
+// a CUDA graph, re-captured when the frames' pipelines or sizes change.
+class BatchStage {
+public:
+    BatchStage();
+    ~BatchStage();
+    BatchStage(const BatchStage&) = delete;
+    BatchStage& operator=(const BatchStage&) = delete;
+
+    // Queues the stages of the prepared frames of `pipes` (at most
+    // kMaxBatchFrames) on s; afterwards each pipeline's device counters hold
+    // its frame's.  Record an event on s to hand the frames on.
+    void run(const std::vector<Pipeline*>& pipes, cudaStream_t s);
+    // Device time of the last run (waits for it) ...
+    float finish_ms();
+    // ... or, once the run is known complete, without waiting or writing.
+    float elapsed_ms() const
+    {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev0_, ev1_) != cudaSuccess) cudaGetLastError();
+        return ms;
+    }
+    int launches() const { return launches_; }
+    // Per-stage timing of the batched launch (eager, events between kernels).
+    void set_stage_timing(bool on);
+    bool stage_timing() const { return timing_; }
+    const float* stage_ms() const { return stage_ms_; }
+
+private:
+    struct Key {
+        const Pipeline* p;
+        int w, h;
+        bool operator==(const Key& o) const { return p == o.p && w == o.w && h == o.h; }
+        bool operator!=(const Key& o) const { return !(*this == o); }
+    };
+    Levels lv_{};
+    LevelCounters* d_cnt_ = nullptr;
+    int32_t* d_partial_ = nullptr;
+    cudaGraphExec_t graph_ = nullptr;
+    std::vector<Key> key_;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaEvent_t st_ev_[kStageCount + 1] = {};
+    bool timing_ = false;
+    float stage_ms_[kStageCount] = {};
+    float last_ms_ = 0.f;
+    int launches_ = 0;
 };
 
 }  // namespace cctagb

@@ -118,6 +118,7 @@ typedef struct cctagb_params {
     int hostThreads;                            /* 0: host threads of the candidate stage; 0 = one per physical core, less one per detection slot beyond the first */
     int gnCoarseGrid;                           /* 3: trial grid (3 or 5 per side) of the coarse rounds of REFINE_GAUSS_NEWTON */
     float gnCoarseNeighbourSize;                /* 0.1: their neighbourhood, as imagedCenterNeighbourSize */
+    int batchWaveFrames;                        /* 4: frames whose image stages share one launch in cctagb_detect_batch (1..16) */
 } cctagb_params;
 
 typedef struct cctagb_ellipse {
@@ -188,10 +189,13 @@ typedef struct cctagb_frame {
 } cctagb_frame;
 
 /* Detection of n independent frames (cameras), of any sizes up to the
- * handle's max_w x max_h.  The handle runs min(max_batch, 32) detection slots,
- * each with its own device buffers and stream, so one frame's host candidate
- * stage overlaps other frames' GPU stages; every frame's result equals that
- * of cctagb_detect on the same frame.  Returns CCTAGB_OK when every frame
+ * handle's max_w x max_h.  Frames go in waves of params.batchWaveFrames: the
+ * image stages (pyramid .. seeds) of a wave's frames run as one launch per
+ * kernel over all their levels, then each frame continues on its own
+ * detection slot (device buffers and stream); min(max_batch, 32) slots keep
+ * several waves in flight, so later waves' image stages overlap earlier
+ * frames' GPU and host stages.  Every frame's result equals that of
+ * cctagb_detect on the same frame.  Returns CCTAGB_OK when every frame
  * succeeded, else the status of the first failing frame (last_error_string
  * names it); per-frame statuses are in frames[i].status.  The reference runs
  * one frame per cctagDetection call (ICCTag.hpp:125-131); this is the
@@ -279,11 +283,11 @@ cctagb_status cctagb_canny_from_derivatives(cctagb_handle* h, const int16_t* dx,
  * (w*hgt bytes, 0/255) are device buffers owned by the caller; d_status (one
  * int, may be null) receives 0 or an internal error bit.  Runs asynchronously
  * on `stream` (a cudaStream_t; null = legacy default stream).  Its scratch is a
- * fixed device array inside the library (about 6.4 MB on every GPU that loads
+ * fixed device array inside the library (about 2.5 MB on every GPU that loads
  * it): frames are limited to 1,048,576 pixels and 4096 per side
- * (CCTAGB_TOO_LARGE beyond).  The first call on a device sets the array up
- * (resolves its address, uploads filter constants) with that device current:
- * make it before any stream capture.  Calls share the array: calls whose GPU
+ * (CCTAGB_TOO_LARGE beyond).  The first call on a device (in each CUDA
+ * context) sets the array up (resolves its device address) with that device
+ * current: make it before any stream capture.  Calls share the array: calls whose GPU
  * work overlaps race; serialise them on one stream. */
 cctagb_status cctagb_edges_noalloc(const uint8_t* d_gray, int w, int hgt, size_t pitch, float cannyThrLow,
                                    float cannyThrHigh, int16_t* d_dx, int16_t* d_dy, uint8_t* d_edges,
