@@ -50,7 +50,7 @@ struct LevelView {
     int32_t* bigq;           // cap: points whose voter list needs a block sort
     // launch geometry of the tiled kernels
     int nms_tx, nms_tiles;   // 30x30 output tiles
-    int thin_tx, thin_tiles; // 32x16 output tiles
+    int thin_tx, thin_tiles; // thinning: 32-pixel word columns x 28-row strips
     int pix_blocks;          // 256-pixel blocks
     int uf_tx, uf_tiles;     // 32x32 hysteresis tiles
 };

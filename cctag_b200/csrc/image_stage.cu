@@ -542,64 +542,82 @@ __global__ void __launch_bounds__(32 * kHystWarps) k_hyst_final(Levels lv, int t
 }
 
 // ------------------------------------------------ final edges + thinning --
-// Output tile 32 x 16 (one warp per row, so a ballot is one bitmap word).
-constexpr int kThX = 32, kThY = 16;
+// thin() (thinning.cpp:12-51): two Lam-Lee-Suen sub-iterations over the
+// hysteresis result, interior pixels only, the image border keeping its
+// Canny value.  Evaluated bit-parallel: a warp takes one 32-pixel word column
+// and 28 output rows, lane r holding row y0 - 2 + r as a 64-bit window
+// (x0 - 16 .. x0 + 47) built from three words of the H plane.  The neighbour
+// masks are the window shifted by one bit and the rows above and below
+// (shuffles); each sub-iteration's "delete" condition is the conjunction of
+// G1 (exactly one of four 0 -> 1 transitions), G2 (2 <= min(n1, n2) <= 3) and
+// the sub-iteration's G3, in bitwise form -- the same function as the
+// reference's 512-entry tables (checked entry by entry in the tests).  Rows
+// and columns two away from the output are enough for the two passes.
+constexpr int kThinRows = 28;
+constexpr int kThinWarps = 4;
 
-__global__ void __launch_bounds__(kThX * kThY) k_final_thin(Levels lv)
+__device__ __forceinline__ uint64_t atl2(uint64_t a, uint64_t b, uint64_t c, uint64_t d)
 {
-    __shared__ uint8_t s_e[kThY + 4][kThX + 4];
-    __shared__ uint8_t s_t[kThY + 2][kThX + 2];
-    __shared__ uint32_t s_lut[2][16];
-    int tile;
-    const int l = level_of_block(lv, blockIdx.x, &LevelView::thin_tiles, tile);
+    return ((a | b) & (c | d)) | (a & b) | (c & d);
+}
+
+// Pixels of plane P that one sub-iteration keeps (pass 1 or 2), as a mask;
+// up / dn are the rows above and below.
+__device__ __forceinline__ uint64_t thin_keep(uint64_t P, uint64_t up, uint64_t dn, int pass)
+{
+    const uint64_t x1 = P >> 1, x2 = up >> 1, x3 = up, x4 = up << 1;  // E, NE, N, NW
+    const uint64_t x5 = P << 1, x6 = dn << 1, x7 = dn, x8 = dn >> 1;  // W, SW, S, SE
+    const uint64_t b1 = ~x1 & (x2 | x3), b2 = ~x3 & (x4 | x5), b3 = ~x5 & (x6 | x7), b4 = ~x7 & (x8 | x1);
+    const uint64_t g1 = (b1 | b2 | b3 | b4) & ~atl2(b1, b2, b3, b4);
+    const uint64_t a1 = x1 | x2, a2 = x3 | x4, a3 = x5 | x6, a4 = x7 | x8;
+    const uint64_t c1 = x2 | x3, c2 = x4 | x5, c3 = x6 | x7, c4 = x8 | x1;
+    const uint64_t g2 = atl2(a1, a2, a3, a4) & atl2(c1, c2, c3, c4) & ~((a1 & a2 & a3 & a4) & (c1 & c2 & c3 & c4));
+    const uint64_t g3 = pass == 1 ? ~((x2 | x3 | ~x8) & x1) : ~((x6 | x7 | ~x4) & x5);
+    return P & ~(g1 & g2 & g3);
+}
+
+// Bits of the window (bit i = column x0 - 16 + i) whose column lies in [lo, hi].
+__device__ __forceinline__ uint64_t col_range(int x0, int lo, int hi)
+{
+    const int a = max(lo - (x0 - 16), 0), b = min(hi - (x0 - 16), 63);
+    if (b < a) return 0ull;
+    const uint64_t upto = b == 63 ? ~0ull : ((1ull << (b + 1)) - 1ull);
+    return upto & ~((1ull << a) - 1ull);
+}
+
+__global__ void __launch_bounds__(32 * kThinWarps) k_final_thin(Levels lv, int total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int g = blockIdx.x * kThinWarps + warp;
+    if (g >= total) return;
+    int l = 0;
+    while (l < lv.n - 1 && g >= lv.l[l].thin_tiles) {
+        g -= lv.l[l].thin_tiles;
+        ++l;
+    }
     const LevelView& L = lv.l[l];
-    const int W = L.W, H = L.H;
-    const int x0 = (tile % L.thin_tx) * kThX;
-    const int y0 = (tile / L.thin_tx) * kThY;
-    const int t = threadIdx.y * kThX + threadIdx.x;
-    if (t < 32) s_lut[t >> 4][t & 15] = cThinTab.bits[t >> 4][t & 15];
-    for (int i = t; i < (kThY + 4) * (kThX + 4); i += kThX * kThY) {
-        const int r = i / (kThX + 4), c = i % (kThX + 4);
-        const int x = x0 - 2 + c, y = y0 - 2 + r;
-        uint8_t e = 0;
-        if (x >= 0 && x < W && y >= 0 && y < H) e = (plane_h(L)[size_t(y) * L.WW + (x >> 5)] >> (x & 31)) & 1u;
-        s_e[r][c] = e;
+    const int W = L.W, H = L.H, WW = L.WW;
+    const int wx = g % WW, y0 = (g / WW) * kThinRows;
+    const int x0 = wx * 32;
+    const int y = y0 - 2 + lane;
+    uint64_t P = 0ull;
+    if (y >= 0 && y < H) {
+        const uint32_t* row = plane_h(L) + size_t(y) * WW;
+        const uint32_t wl = wx > 0 ? row[wx - 1] : 0u, wc = row[wx], wr = wx + 1 < WW ? row[wx + 1] : 0u;
+        P = uint64_t((wl >> 16) | (wc << 16)) | (uint64_t((wc >> 16) | (wr << 16)) << 32);
     }
-    __syncthreads();
-    auto lut = [&](int k, int idx) -> uint8_t { return (s_lut[k][idx >> 5] >> (idx & 31)) & 1u; };
-    for (int i = t; i < (kThY + 2) * (kThX + 2); i += kThX * kThY) {
-        const int r = i / (kThX + 2), c = i % (kThX + 2);
-        const int x = x0 - 1 + c, y = y0 - 1 + r;
-        uint8_t v = 0;
-        if (x >= 1 && x < W - 1 && y >= 1 && y < H - 1 && s_e[r + 1][c + 1]) {
-            const int rr = r + 1, cc = c + 1;
-            const int idx = s_e[rr - 1][cc - 1] * 1 + s_e[rr][cc - 1] * 2 + s_e[rr + 1][cc - 1] * 4 +
-                            s_e[rr - 1][cc] * 8 + 16 + s_e[rr + 1][cc] * 32 +
-                            s_e[rr - 1][cc + 1] * 64 + s_e[rr][cc + 1] * 128 + s_e[rr + 1][cc + 1] * 256;
-            v = lut(0, idx);
-        }
-        s_t[r][c] = v;
-    }
-    __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    bool on = false;
-    if (x < W && y < H) {
-        if (x == 0 || y == 0 || x == W - 1 || y == H - 1) {
-            on = s_e[threadIdx.y + 2][threadIdx.x + 2];
-        } else {
-            const int rr = threadIdx.y + 1, cc = threadIdx.x + 1;
-            if (s_t[rr][cc]) {
-                const int idx = s_t[rr - 1][cc - 1] * 1 + s_t[rr][cc - 1] * 2 + s_t[rr + 1][cc - 1] * 4 +
-                                s_t[rr - 1][cc] * 8 + 16 + s_t[rr + 1][cc] * 32 +
-                                s_t[rr - 1][cc + 1] * 64 + s_t[rr][cc + 1] * 128 + s_t[rr + 1][cc + 1] * 256;
-                on = lut(1, idx);
-            }
-        }
-    }
-    const uint32_t mask = __ballot_sync(0xffffffffu, on);
-    if (threadIdx.x == 0 && y < H) {
-        L.bitmap[size_t(y) * L.WW + (x0 >> 5)] = mask;
-        if (mask) atomicAdd(&L.row_count[y], __popc(mask));
+    const bool rowInterior = y >= 1 && y <= H - 2;
+    const uint64_t interior = rowInterior ? col_range(x0, 1, W - 2) : 0ull;
+    uint64_t up = __shfl_up_sync(0xffffffffu, P, 1), dn = __shfl_down_sync(0xffffffffu, P, 1);
+    const uint64_t T = thin_keep(P, up, dn, 1) & interior;
+    up = __shfl_up_sync(0xffffffffu, T, 1);
+    dn = __shfl_down_sync(0xffffffffu, T, 1);
+    const uint64_t inImage = (y >= 0 && y < H) ? col_range(x0, 0, W - 1) : 0ull;
+    const uint64_t out = (thin_keep(T, up, dn, 2) & interior) | (P & inImage & ~interior);
+    if (lane >= 2 && lane < 2 + kThinRows && y < H) {
+        const uint32_t word = uint32_t(out >> 16);
+        L.bitmap[size_t(y) * WW + wx] = word;
+        if (word) atomicAdd(&L.row_count[y], __popc(word));
     }
 }
 
@@ -1118,7 +1136,8 @@ static void launch_edges(const Levels& lv, const VoteParamsDev& vp, cudaStream_t
     k_hyst_roots<<<tiles, kTileComps, 0, s>>>(lv);
     k_hyst_final<<<hb, 32 * kHystWarps, 0, s>>>(lv, tiles);
     mark(ev, kStHystCompress + 1, s);
-    k_final_thin<<<total_of(lv, &LevelView::thin_tiles), dim3(kThX, kThY), 0, s>>>(lv);
+    const int tt = total_of(lv, &LevelView::thin_tiles);
+    k_final_thin<<<(tt + kThinWarps - 1) / kThinWarps, 32 * kThinWarps, 0, s>>>(lv, tt);
     mark(ev, kStFinalThin + 1, s);
     k_row_scan<<<lv.n, 1024, 0, s>>>(lv);
     mark(ev, kStRowScan + 1, s);
@@ -1199,7 +1218,7 @@ void launch_edge_level(const Levels& lv, const VoteParamsDev& vp, cudaStream_t s
     k_hyst_unions<<<L.uf_tiles, 64, 0, s>>>(lv);
     k_hyst_roots<<<L.uf_tiles, kTileComps, 0, s>>>(lv);
     k_hyst_final<<<hb, 32 * kHystWarps, 0, s>>>(lv, L.uf_tiles);
-    k_final_thin<<<L.thin_tiles, dim3(kThX, kThY), 0, s>>>(lv);
+    k_final_thin<<<(L.thin_tiles + kThinWarps - 1) / kThinWarps, 32 * kThinWarps, 0, s>>>(lv, L.thin_tiles);
     k_bitmap_to_bytes<<<148 * 4, 256, 0, s>>>(lv, edges_out);
     if (status_out) k_copy_status<<<1, 1, 0, s>>>(lv.cnt, status_out);
     CCTAGB_CUDA(cudaGetLastError());

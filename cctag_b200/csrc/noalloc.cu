@@ -163,7 +163,7 @@ extern "C" cctagb_status cctagb_edges_noalloc(const uint8_t* d_gray, int w, int 
     L.nms_tx = (w + 29) / 30;
     L.nms_tiles = L.nms_tx * ((h + 29) / 30);
     L.thin_tx = (w + 31) / 32;
-    L.thin_tiles = L.thin_tx * ((h + 15) / 16);
+    L.thin_tiles = L.thin_tx * ((h + 27) / 28);  // word columns x 28-row strips
     L.pix_blocks = int((size_t(w) * h + 255) / 256);
     L.uf_tx = (w + 31) / 32;
     L.uf_tiles = L.uf_tx * ((h + 31) / 32);

@@ -184,7 +184,7 @@ void Pipeline::set_views(int w, int h, int nl)
         v.nms_tx = (w + 29) / 30;
         v.nms_tiles = v.nms_tx * ((h + 29) / 30);
         v.thin_tx = (w + 31) / 32;
-        v.thin_tiles = v.thin_tx * ((h + 15) / 16);
+        v.thin_tiles = v.thin_tx * ((h + 27) / 28);  // word columns x 28-row strips
         v.pix_blocks = int((size_t(w) * h + 255) / 256);
         v.uf_tx = (w + 31) / 32;
         v.uf_tiles = v.uf_tx * ((h + 31) / 32);
