@@ -443,6 +443,32 @@ def run_b200(args, rank, world, local):
     return line
 
 
+def run_batch_only(args, torch, local):
+    """The step's 16 frames through cctagb_detect_batch in one wave (one
+    batched image-stage launch per kernel), `steps` times, for profiling."""
+    import cctag_b200
+    from cctag_b200 import capi
+
+    frames = make_frames(args.config)
+    H, W = frames[0].shape
+    p = cctag_b200.default_params(3)
+    p.batchWaveFrames = BATCH
+    det = cctag_b200.Detector(p, max_w=W, max_h=H, max_batch=BATCH)
+    d = [torch.from_numpy(f).to(f"cuda:{local}") for f in frames]
+    cap = 512
+    outs = [(capi.Marker * cap)() for _ in frames]
+    fr = (capi.Frame * len(frames))()
+    for i, t in enumerate(d):
+        fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch, fr[i].is_device, fr[i].frame_id = t.data_ptr(), W, H, W, 1, i
+        fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
+        fr[i].cap = cap
+    for _ in range(args.warmup + args.steps):
+        det._check(det._lib.cctagb_detect_batch(det._h, fr, len(frames)), "detect_batch")
+    torch.cuda.synchronize()
+    det.close()
+    return {"frames_per_call": len(frames), "calls": args.warmup + args.steps, "frame": f"{W}x{H}"}
+
+
 def run_plain(args, torch, local):
     """Single-frame detections of the configuration's frames, one per call
     (cctagb_detect_device), for profiling one frame's kernels."""
@@ -784,7 +810,7 @@ def main():
     ap.add_argument("--no-c5", action="store_true", help="skip the candidate-refinement leg")
     ap.add_argument("--no-c3", action="store_true", help="skip the 4K clutter leg")
     ap.add_argument("--c5-candidates", type=int, default=4096, help="distinct candidates of the refinement leg")
-    ap.add_argument("--leg", default="all", choices=["all", "plain", "c3", "c4", "c5"],
+    ap.add_argument("--leg", default="all", choices=["all", "plain", "batch", "c3", "c4", "c5"],
                     help="run one secondary leg alone and print its object (for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -804,6 +830,8 @@ def main():
             print(json.dumps({"c5_refine": run_c5(args, torch)}))
         elif args.leg == "plain":
             print(json.dumps({"plain": run_plain(args, torch, local)}))
+        elif args.leg == "batch":
+            print(json.dumps({"batch": run_batch_only(args, torch, local)}))
         elif args.leg == "c3":
             flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
             peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) \

@@ -733,9 +733,11 @@ __device__ int gradient_walk(const LevelView& L, int px, int py, int gdx, int gd
     const bool y_major = fabsf(dy) > fabsf(dx);
     int x = px, y = py, stpX = 0, stpY = 0, n = 0;
     const int W = L.W, H = L.H;
+    // |dmin / dmaj| is the same before and after the re-orientation (both
+    // signs flip), so the division is done once
+    const float a = fabsf(__fdiv_rn(y_major ? dx : dy, y_major ? dy : dx));
     auto step = [&]() {
         const float dmaj = y_major ? dy : dx, dmin = y_major ? dx : dy;
-        const float a = fabsf(__fdiv_rn(dmin, dmaj));
         const int smaj = sgn_i(int(dmaj)), smin = sgn_i(int(dmin));
         e = __fadd_rn(e, a);
         if (y_major) { stpY = smaj; stpX = smin; y += smaj; } else { stpX = smaj; stpY = smin; x += smaj; }
@@ -745,6 +747,10 @@ __device__ int gradient_walk(const LevelView& L, int px, int py, int gdx, int gd
         }
         ++n;
     };
+    auto inside = [&](int qx, int qy) { return qx >= 0 && qx < W && qy >= 0 && qy < H; };
+    auto word = [&](int qx, int qy) -> uint32_t {
+        return inside(qx, qy) ? __ldg(&L.bitmap[size_t(qy) * L.WW + (qx >> 5)]) : 0u;
+    };
     step();
     if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > float(thr)) {
         const float v = __fadd_rn(__fmul_rn(float(gdx), dxRef), __fmul_rn(float(gdy), dyRef));
@@ -753,16 +759,16 @@ __device__ int gradient_walk(const LevelView& L, int px, int py, int gdx, int gd
         dy = float(d * gdy);
     }
     step();
-    if (x < 0 || x >= W || y < 0 || y >= H) return -1;
-    if (edge_bit(L, x, y)) return L.idxmap[size_t(y) * W + x];
+    if (!inside(x, y)) return -1;
+    if ((word(x, y) >> (x & 31)) & 1u) return L.idxmap[size_t(y) * W + x];
     while (n <= nmax) {
         step();
-        if (x < 0 || x >= W || y < 0 || y >= H) return -1;
-        if (edge_bit(L, x, y)) return L.idxmap[size_t(y) * W + x];
+        if (!inside(x, y)) return -1;
+        if ((word(x, y) >> (x & 31)) & 1u) return L.idxmap[size_t(y) * W + x];
         const int bx = y_major ? x : x - stpX;
         const int by = y_major ? y - stpY : y;
-        if (bx < 0 || bx >= W || by < 0 || by >= H) return -1;
-        if (edge_bit(L, bx, by)) return L.idxmap[size_t(by) * W + bx];
+        if (!inside(bx, by)) return -1;
+        if ((word(bx, by) >> (bx & 31)) & 1u) return L.idxmap[size_t(by) * W + bx];
     }
     return -1;
 }
@@ -857,29 +863,29 @@ __global__ void k_vote(Levels lv, VoteParamsDev vp)
 // ----------------------------------------------------- voter lists (CSR) --
 // Chunked exclusive scan of nvotes[0, E) into voff, all levels, fixed grid.
 constexpr int kScanBlocks = kScanBlocksPerLevel;
-constexpr int kScanThreads = 1024;
+constexpr int kScanThreads = 256;
+constexpr int kScanChunks = 32;  // chunks per level (partial sums at stride kScanBlocks)
 
+// Voter-count scan: level blockIdx.y, chunk blockIdx.x of kScanChunks.
 __global__ void __launch_bounds__(kScanThreads) k_vscan_partial(Levels lv, int32_t* partial)
 {
-    __shared__ int s_red[32];
-    for (int l = 0; l < lv.n; ++l) {
-        const LevelView& L = lv.l[l];
-        const int E = lv.cnt[l].E;
-        const int chunk = (E + kScanBlocks - 1) / kScanBlocks;
-        const int b0 = blockIdx.x * chunk, b1 = min(E, b0 + chunk);
-        int s = 0;
-        for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) s += L.nvotes[i];
+    __shared__ int s_red[kScanThreads / 32];
+    const int l = blockIdx.y;
+    const LevelView& L = lv.l[l];
+    const int E = lv.cnt[l].E;
+    const int chunk = (E + kScanChunks - 1) / kScanChunks;
+    const int b0 = blockIdx.x * chunk, b1 = min(E, b0 + chunk);
+    int s = 0;
+    for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) s += L.nvotes[i];
 #pragma unroll
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = s;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            int v = s_red[threadIdx.x];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int v = threadIdx.x < kScanThreads / 32 ? s_red[threadIdx.x] : 0;
 #pragma unroll
-            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (threadIdx.x == 0) partial[l * kScanBlocks + blockIdx.x] = v;
-        }
-        __syncthreads();
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) partial[l * kScanBlocks + blockIdx.x] = v;
     }
 }
 
@@ -887,33 +893,31 @@ __global__ void __launch_bounds__(kScanThreads) k_vscan_final(Levels lv, const i
 {
     __shared__ int s_warp[33];
     __shared__ int s_base;
-    for (int l = 0; l < lv.n; ++l) {
-        const LevelView& L = lv.l[l];
-        const int E = lv.cnt[l].E;
-        const int chunk = (E + kScanBlocks - 1) / kScanBlocks;
-        const int b0 = blockIdx.x * chunk, b1 = min(E, b0 + chunk);
-        if (threadIdx.x == 0) {
-            int b = 0;
-            for (int k = 0; k < int(blockIdx.x); ++k) b += partial[l * kScanBlocks + k];
-            s_base = b;
-        }
-        __syncthreads();
-        int carry = s_base;
-        for (int base = b0; base < b1; base += blockDim.x) {
-            const int i = base + threadIdx.x;
-            const int v = i < b1 ? L.nvotes[i] : 0;
-            int total;
-            const int ex = block_excl_scan(v, s_warp, &total);
-            if (i < b1) L.voff[i] = carry + ex;
-            carry += total;
-        }
-        if (blockIdx.x == kScanBlocks - 1 && threadIdx.x == 0) {
-            int V = 0;
-            for (int k = 0; k < kScanBlocks; ++k) V += partial[l * kScanBlocks + k];
-            L.voff[E] = V;
-            lv.cnt[l].V = V;
-        }
-        __syncthreads();
+    const int l = blockIdx.y;
+    const LevelView& L = lv.l[l];
+    const int E = lv.cnt[l].E;
+    const int chunk = (E + kScanChunks - 1) / kScanChunks;
+    const int b0 = blockIdx.x * chunk, b1 = min(E, b0 + chunk);
+    if (threadIdx.x == 0) {
+        int b = 0;
+        for (int k = 0; k < int(blockIdx.x); ++k) b += partial[l * kScanBlocks + k];
+        s_base = b;
+    }
+    __syncthreads();
+    int carry = s_base;
+    for (int base = b0; base < b1; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < b1 ? L.nvotes[i] : 0;
+        int total;
+        const int ex = block_excl_scan(v, s_warp, &total);
+        if (i < b1) L.voff[i] = carry + ex;
+        carry += total;
+    }
+    if (blockIdx.x == kScanChunks - 1 && threadIdx.x == 0) {
+        int V = 0;
+        for (int k = 0; k < kScanChunks; ++k) V += partial[l * kScanBlocks + k];
+        L.voff[E] = V;
+        lv.cnt[l].V = V;
     }
 }
 
@@ -1160,8 +1164,8 @@ void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t 
     mark(ev, kStWalk + 1, s);
     k_vote<<<G, 256, 0, s>>>(lv, vp);
     mark(ev, kStVote + 1, s);
-    k_vscan_partial<<<kScanBlocks, kScanThreads, 0, s>>>(lv, lv.partial);
-    k_vscan_final<<<kScanBlocks, kScanThreads, 0, s>>>(lv, lv.partial);
+    k_vscan_partial<<<dim3(kScanChunks, lv.n), kScanThreads, 0, s>>>(lv, lv.partial);
+    k_vscan_final<<<dim3(kScanChunks, lv.n), kScanThreads, 0, s>>>(lv, lv.partial);
     mark(ev, kStVoterScan + 1, s);
     k_vfill<<<G, 256, 0, s>>>(lv);
     mark(ev, kStVoterFill + 1, s);

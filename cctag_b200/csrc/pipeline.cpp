@@ -207,8 +207,8 @@ void Pipeline::image_stage(const uint8_t* gray, int w, int h, size_t pitch, bool
     const bool fused = (w % 8 == 0) && (h % 8 == 0) && lv_.n == 4;
     h2d_bytes_ = is_device ? 0 : (long long)w * h;
     d2h_bytes_ = 0;
-    // kernels of one image stage: pyramid (1 fused or one per level), 14 others
-    launches_ = (fused ? 1 : lv_.n - 1) + 14;
+    // kernels of one image stage: pyramid (1 fused or one per level), 15 others
+    launches_ = (fused ? 1 : lv_.n - 1) + 15;
     if (timing_) {
         // Per-stage timing: eager launches queued behind a ~2 ms gate so the
         // GPU never waits for the host between two stage events.
@@ -331,8 +331,8 @@ void BatchStage::run(const std::vector<Pipeline*>& pipes, cudaStream_t s)
     }
     tg.n = lv_.n;
     const VoteParamsDev& vp = pipes[0]->vote_params();
-    // kernels: pyramid (1 fused or one per level), 14 image-stage kernels, the counter scatter
-    launches_ = (fused ? 1 : lv_.n - nf) + 14 + 1;
+    // kernels: pyramid (1 fused or one per level), 15 image-stage kernels, the counter scatter
+    launches_ = (fused ? 1 : lv_.n - nf) + 15 + 1;
     if (timing_) {
         launch_gate(s, 2000);
         CCTAGB_CUDA(cudaEventRecord(ev0_, s));
