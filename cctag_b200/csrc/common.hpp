@@ -28,7 +28,7 @@ struct LevelView {
     int32_t* tcomp;          // uf_tiles * 64: union-find parents over (tile, component) ids
     int32_t* tflag;          // uf_tiles * 64: bit 0 holds a strong pixel, bit 1 (at roots) its set does
     uint32_t* bitmap;        // WW*H final thinned edges, bit x&31 of word x>>5
-    int32_t* idxmap;         // W*H edge index (valid where the bitmap is set)
+    uint2* bitidx;           // WW*H: (bitmap word, edge index of the word's first set bit)
     int32_t* row_count;      // H
     int32_t* row_off;        // H+1
     int cap;                 // edge-point capacity

@@ -682,8 +682,10 @@ __global__ void __launch_bounds__(1024) k_row_scan(Levels lv)
     }
 }
 
-// One block (4 warps) per image row: raster-order edge list, index map,
-// per-point state reset.  EdgePointCollection::add_point, Types.cpp:40-61.
+// One block (4 warps) per image row: raster-order edge list, per-point state
+// reset, and per bitmap word the word with the index of its first edge point
+// (an edge pixel's index is that plus the word's set bits below it).
+// EdgePointCollection::add_point, Types.cpp:40-61.
 __global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
 {
     __shared__ int s_warp[4];
@@ -702,8 +704,10 @@ __global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
     __syncthreads();
     int base = L.row_off[y];
     for (int k = 0; k < wid; ++k) base += s_warp[k];
+    uint2* bi = L.bitidx + size_t(y) * L.WW;
     for (int w = w0; w < w1; ++w) {
         const uint32_t m = row[w];
+        if (lane == 0) bi[w] = make_uint2(m, uint32_t(base));
         if (!m) continue;
         if ((m >> lane) & 1u) {
             const int idx = base + __popc(m & ((1u << lane) - 1u));
@@ -712,7 +716,6 @@ __global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
                 const size_t p = size_t(y) * L.W + x;
                 L.exy[idx] = x | (y << 16);
                 L.grad[idx] = int32_t(uint16_t(L.dx[p])) | (int32_t(L.dy[p]) << 16);
-                L.idxmap[p] = idx;
                 L.nvotes[idx] = 0;
                 L.fill[idx] = 0;
             }
@@ -722,71 +725,132 @@ __global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
 }
 
 // ------------------------------------------------------ gradient walk --
-// Bresenham.cpp:18-209.  Returns the index of the first edge point met, or -1.
+// Bresenham.cpp:18-209: from an edge point, follow the gradient (dir = -1
+// backward, +1 forward) for up to distSearch steps and return the index of the
+// first edge point met, or -1.  Walk lengths spread widely (most stop within
+// two or three steps, a few run the full distance), so a warp does not run
+// one walk per lane to the end of its longest: each lane takes the next walk
+// of the warp's chunk as soon as its current one stops.  One iteration of the
+// loop below is one step of a lane's walk, with the probes the reference makes
+// after that step; the steps and probes of every walk are those of the
+// reference in the same order, so the results do not depend on the schedule.
+constexpr int kWalkWarps = 8;
+constexpr int kWalkChunk = 512;  // walks (two per point) a warp takes at once
+
 __device__ __forceinline__ int sgn_i(int v) { return (v > 0) - (v < 0); }
 
-__device__ int gradient_walk(const LevelView& L, int px, int py, int gdx, int gdy, int dir, int nmax, int thr)
+__global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsDev vp)
 {
-    float e = 0.f;
-    float dx = float(dir * gdx), dy = float(dir * gdy);
-    const float dxRef = dx, dyRef = dy;
-    const bool y_major = fabsf(dy) > fabsf(dx);
-    int x = px, y = py, stpX = 0, stpY = 0, n = 0;
-    const int W = L.W, H = L.H;
-    // |dmin / dmaj| is the same before and after the re-orientation (both
-    // signs flip), so the division is done once
-    const float a = fabsf(__fdiv_rn(y_major ? dx : dy, y_major ? dy : dx));
-    auto step = [&]() {
-        const float dmaj = y_major ? dy : dx, dmin = y_major ? dx : dy;
-        const int smaj = sgn_i(int(dmaj)), smin = sgn_i(int(dmin));
-        e = __fadd_rn(e, a);
-        if (y_major) { stpY = smaj; stpX = smin; y += smaj; } else { stpX = smaj; stpY = smin; x += smaj; }
-        if (e >= 0.5f) {
-            if (y_major) x += smin; else y += smin;
-            e = __fadd_rn(e, -1.f);
-        }
-        ++n;
-    };
-    auto inside = [&](int qx, int qy) { return qx >= 0 && qx < W && qy >= 0 && qy < H; };
-    auto word = [&](int qx, int qy) -> uint32_t {
-        return inside(qx, qy) ? __ldg(&L.bitmap[size_t(qy) * L.WW + (qx >> 5)]) : 0u;
-    };
-    step();
-    if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > float(thr)) {
-        const float v = __fadd_rn(__fmul_rn(float(gdx), dxRef), __fmul_rn(float(gdy), dyRef));
-        const int d = (v > 0.f) - (v < 0.f);
-        dx = float(d * gdx);
-        dy = float(d * gdy);
-    }
-    step();
-    if (!inside(x, y)) return -1;
-    if ((word(x, y) >> (x & 31)) & 1u) return L.idxmap[size_t(y) * W + x];
-    while (n <= nmax) {
-        step();
-        if (!inside(x, y)) return -1;
-        if ((word(x, y) >> (x & 31)) & 1u) return L.idxmap[size_t(y) * W + x];
-        const int bx = y_major ? x : x - stpX;
-        const int by = y_major ? y - stpY : y;
-        if (!inside(bx, by)) return -1;
-        if ((word(bx, by) >> (bx & 31)) & 1u) return L.idxmap[size_t(by) * W + bx];
-    }
-    return -1;
-}
-
-__global__ void k_walk(Levels lv, VoteParamsDev vp)
-{
-    const int stride = gridDim.x * blockDim.x;
+    __shared__ int s_xy[kWalkWarps][kWalkChunk / 2];
+    __shared__ int s_g[kWalkWarps][kWalkChunk / 2];
+    __shared__ float s_a[kWalkWarps][kWalkChunk / 2];
+    __shared__ int s_res[kWalkWarps][kWalkChunk];
+    const unsigned kAll = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    const int gw = blockIdx.x * kWalkWarps + wid, NW = gridDim.x * kWalkWarps;
+    const int nmax = vp.distSearch;
+    const float thr = float(vp.thrGradient);
+    int first = 0;  // global number of the level's first chunk
     for (int l = 0; l < lv.n; ++l) {
         const LevelView& L = lv.l[l];
         const int E = lv.cnt[l].E;
-        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * E; t += stride) {
-            const int p = t >> 1;
-            const int dir = (t & 1) ? 1 : -1;
-            const int xy = L.exy[p], g = L.grad[p];
-            const int px = xy & 0xffff, py = xy >> 16;
-            const int gdx = int16_t(g & 0xffff), gdy = g >> 16;
-            const int hit = gradient_walk(L, px, py, gdx, gdy, dir, vp.distSearch, vp.thrGradient);
-            if (dir < 0) L.before[p] = hit; else L.after[p] = hit;
+        const int W = L.W, H = L.H, WW = L.WW;
+        const int nch = (2 * E + kWalkChunk - 1) / kWalkChunk;
+        int c = (gw - first % NW + NW) % NW;
+        first += nch;
+        for (; c < nch; c += NW) {
+            const int t0 = c * kWalkChunk, t1 = min(2 * E, t0 + kWalkChunk);
+            const int p0 = t0 >> 1, np = (t1 - t0) >> 1;
+            // the chunk's points, and |dmin / dmaj| per point (the same for
+            // both directions and before and after the re-orientation: the
+            // signs of both components flip together)
+            for (int i = lane; i < np; i += 32) {
+                const int xy = L.exy[p0 + i], g = L.grad[p0 + i];
+                const float gx = float(int16_t(g & 0xffff)), gy = float(g >> 16);
+                const bool ym = fabsf(gy) > fabsf(gx);
+                s_xy[wid][i] = xy;
+                s_g[wid][i] = g;
+                s_a[wid][i] = fabsf(__fdiv_rn(ym ? gx : gy, ym ? gy : gx));
+            }
+            __syncwarp();
+            int q = t0, t = 0, x = 0, y = 0, stpX = 0, stpY = 0, n = 0, gdx = 0, gdy = 0;
+            float e = 0.f, dx = 0.f, dy = 0.f, a = 0.f;
+            bool act = false, ymaj = false;
+            while (true) {
+                const unsigned idle = __ballot_sync(kAll, !act);
+                if (!act) {
+                    const int k = q + __popc(idle & below);
+                    if (k < t1) {
+                        t = k;
+                        act = true;
+                        const int i = (k - t0) >> 1;
+                        const int xy = s_xy[wid][i], g = s_g[wid][i];
+                        const int dir = (k & 1) ? 1 : -1;
+                        x = xy & 0xffff;
+                        y = xy >> 16;
+                        gdx = int16_t(g & 0xffff);
+                        gdy = g >> 16;
+                        dx = float(dir * gdx);
+                        dy = float(dir * gdy);
+                        ymaj = fabsf(dy) > fabsf(dx);
+                        a = s_a[wid][i];
+                        e = 0.f;
+                        n = 0;
+                        stpX = stpY = 0;
+                    }
+                }
+                q += __popc(idle);
+                if (!__any_sync(kAll, act)) break;
+                if (!act) continue;
+                int res = -2;  // -2: the walk goes on
+                if (n >= 2 && n > nmax) {
+                    res = -1;
+                } else {
+                    const float dmaj = ymaj ? dy : dx, dmin = ymaj ? dx : dy;
+                    const int smaj = sgn_i(int(dmaj)), smin = sgn_i(int(dmin));
+                    e = __fadd_rn(e, a);
+                    if (ymaj) { stpY = smaj; stpX = smin; y += smaj; } else { stpX = smaj; stpY = smin; x += smaj; }
+                    if (e >= 0.5f) {
+                        if (ymaj) x += smin; else y += smin;
+                        e = __fadd_rn(e, -1.f);
+                    }
+                    ++n;
+                    if (n == 1) {
+                        // after the first step: re-orient along the gradient
+                        // when the direction is long enough
+                        if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > thr) {
+                            const float v = __fadd_rn(__fmul_rn(float(gdx), dx), __fmul_rn(float(gdy), dy));
+                            const int d = (v > 0.f) - (v < 0.f);
+                            dx = float(d * gdx);
+                            dy = float(d * gdy);
+                        }
+                    } else {
+                        // -1 outside the level, -2 no edge pixel, else its
+                        // index (-1 past a clamped edge count)
+                        auto probe = [&](int qx, int qy) -> int {
+                            if (qx < 0 || qx >= W || qy < 0 || qy >= H) return -1;
+                            const uint2 v = __ldg(&L.bitidx[size_t(qy) * WW + (qx >> 5)]);
+                            const uint32_t bit = 1u << (qx & 31);
+                            if (!(v.x & bit)) return -2;
+                            const int idx = int(v.y) + __popc(v.x & (bit - 1u));
+                            return idx < E ? idx : -1;
+                        };
+                        res = probe(x, y);
+                        if (res == -2 && n > 2) res = probe(ymaj ? x : x - stpX, ymaj ? y - stpY : y);
+                    }
+                }
+                if (res != -2) {
+                    s_res[wid][t - t0] = res;
+                    act = false;
+                }
+            }
+            __syncwarp();
+            for (int i = lane; i < np; i += 32) {
+                L.before[p0 + i] = s_res[wid][2 * i];
+                L.after[p0 + i] = s_res[wid][2 * i + 1];
+            }
+            __syncwarp();
         }
     }
 }
@@ -1160,7 +1224,7 @@ void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t 
     mark(ev, kStPyramid + 1, s);
     launch_edges(lv, vp, s, 1, ev);
     const int G = 148 * 8;
-    k_walk<<<G, 256, 0, s>>>(lv, vp);
+    k_walk<<<148 * 5, 32 * kWalkWarps, 0, s>>>(lv, vp);  // 5 resident per SM (48 registers, 40 KB)
     mark(ev, kStWalk + 1, s);
     k_vote<<<G, 256, 0, s>>>(lv, vp);
     mark(ev, kStVote + 1, s);

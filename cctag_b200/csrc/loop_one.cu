@@ -76,13 +76,15 @@ __device__ __forceinline__ float gnorm(const LoopOneLevel& L, int i)
     const float dx = gdx(L, i), dy = gdy(L, i);
     return sqrtf(dx * dx + dy * dy);
 }
-// Edge point at pixel (x, y), -1 if none (the index map is valid only where
-// the edge bitmap is set).
+// Edge point at pixel (x, y), -1 if none: the word's first index plus its
+// set bits below x.
 __device__ __forceinline__ int at(const LoopOneLevel& L, int x, int y)
 {
     if (x < 0 || x >= L.W || y < 0 || y >= L.H) return -1;
-    const uint32_t w = L.bitmap[size_t(y) * L.WW + (x >> 5)];
-    return ((w >> (x & 31)) & 1u) ? L.idxmap[size_t(y) * L.W + x] : -1;
+    const uint2 v = L.bitidx[size_t(y) * L.WW + (x >> 5)];
+    const uint32_t bit = 1u << (x & 31);
+    const int i = int(v.y) + __popc(v.x & (bit - 1u));
+    return (v.x & bit) && i < L.E ? i : -1;
 }
 
 __global__ void __launch_bounds__(256) k_point_records(LoopOneArgs a, int4 total)
@@ -887,18 +889,20 @@ __device__ int refit_row_takes(const LoopOneLevel& L, const geo::Mat3& Qi, const
     if (!refit_row(Qi, Qo, L.W, y, nr, xb, xe)) return 0;
     int n = 0;
     // the edge pixels of each x range, a bitmap word at a time, in x order
-    const uint32_t* row = L.bitmap + size_t(y) * L.WW;
+    const uint2* row = L.bitidx + size_t(y) * L.WW;
     for (int r = 0; r < nr; ++r) {
         if (xb[r] > xe[r]) continue;
         for (int wx = xb[r] >> 5; wx <= xe[r] >> 5; ++wx) {
             const int lo = wx << 5;
-            uint32_t w = row[wx];
+            const uint2 word = row[wx];
+            uint32_t w = word.x;
             if (xb[r] > lo) w &= 0xffffffffu << (xb[r] - lo);
             if (xe[r] < lo + 31) w &= 0xffffffffu >> (31 - (xe[r] - lo));
             while (w) {
-                const int x = lo + __ffs(w) - 1;
+                const int b = __ffs(w) - 1;
                 w &= w - 1;
-                const int e = L.idxmap[size_t(y) * L.W + x];
+                const int e = int(word.y) + __popc(word.x & ((1u << b) - 1u));
+                if (e >= L.E) break;  // past a clamped edge count
                 const float cx = inCx - float(px_(L, e)), cy = inCy - float(py_(L, e));
                 if (gdx(L, e) * cx + gdy(L, e) * cy < 0) {
                     if (out) out[n] = e;
@@ -1137,8 +1141,7 @@ void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const 
         L.grad = v.grad;
         L.voff = v.voff;
         L.vlist = v.vlist;
-        L.bitmap = v.bitmap;
-        L.idxmap = v.idxmap;
+        L.bitidx = v.bitidx;
         L.flow = v.flow;
         L.level = l;
         L.slot0 = l * maxSlotsPerLevel_;

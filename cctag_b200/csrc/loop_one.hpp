@@ -28,8 +28,7 @@ struct LoopOneLevel {
     const int32_t* grad;
     const int32_t* voff;
     const int32_t* vlist;
-    const uint32_t* bitmap;
-    const int32_t* idxmap;
+    const uint2* bitidx;     // WW*H: (edge bitmap word, edge index of its first set bit)
     const int32_t* order;   // seeds in processing order, nProc of them
     int nProc, slot0;       // seed slots [slot0, slot0 + nProc)
     int4* rec;              // E point records (3 int4 each): xy, angle, voters, seed slot; 8 neighbours

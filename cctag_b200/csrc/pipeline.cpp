@@ -35,6 +35,8 @@ Pipeline::Pipeline(const cctagb_params& p, int max_w, int max_h, int max_batch) 
         throw Error{CCTAGB_BAD_ARG, "numberOfProcessedMultiresLayers must be in [1, 4]"};
     if (p.nCrowns < 1 || 2 * p.nCrowns - 1 > 16) throw Error{CCTAGB_BAD_ARG, "nCrowns out of range"};
     if (p.edgeCapacityDivisor < 1) throw Error{CCTAGB_BAD_ARG, "edgeCapacityDivisor must be >= 1"};
+    // a walk that does not move (zero gradient) runs distSearch steps
+    if (p.distSearch < 0 || p.distSearch > 16384) throw Error{CCTAGB_BAD_ARG, "distSearch must be in [0, 16384]"};
     vp_.distSearch = p.distSearch;
     vp_.thrGradient = p.thrGradientMagInVote;
     vp_.angleVoting = p.angleVoting;
@@ -113,7 +115,7 @@ void Pipeline::alloc(int max_w, int max_h)
         v.tcomp = dev_alloc<int32_t>(allocs_, tiles * 64);
         v.tflag = dev_alloc<int32_t>(allocs_, tiles * 64);
         v.bitmap = dev_alloc<uint32_t>(allocs_, size_t((w + 31) / 32) * h);
-        v.idxmap = dev_alloc<int32_t>(allocs_, px);
+        v.bitidx = dev_alloc<uint2>(allocs_, size_t((w + 31) / 32) * h);
         v.row_count = dev_alloc<int32_t>(allocs_, h);
         v.row_off = dev_alloc<int32_t>(allocs_, h + 1);
         CCTAGB_CUDA(cudaMemset(v.row_count, 0, sizeof(int32_t) * h));

@@ -114,6 +114,11 @@ def test_errors_are_status_codes(built_library):
         assert ei.value.status == cctag_b200.capi.OVERFLOW_EDGES
         # the handle stays usable after an error
         d.image_stage(np.full((120, 160), 5, np.uint8))
+    p = cctag_b200.default_params(3)
+    p.distSearch = 1 << 20
+    with pytest.raises(cctag_b200.CCTagError) as ei:
+        cctag_b200.Detector(p, max_w=64, max_h=64)
+    assert ei.value.status == cctag_b200.capi.BAD_ARG
 
 
 def test_stage_timing_mode_gives_same_results(detector, orc):
