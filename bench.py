@@ -153,6 +153,25 @@ def host_pool():
     return ProcessPoolExecutor(max_workers=os.cpu_count() or 1, mp_context=mp.get_context("spawn"))
 
 
+def tune_cache_path():
+    """The autotuner's JSON cache: $CCTAG_B200_TUNE_CACHE, else a file in the
+    user's cache directory."""
+    p = Path(os.environ.get("CCTAG_B200_TUNE_CACHE") or Path.home() / ".cache" / "cctag_b200" / "tune.json")
+    p.parent.mkdir(parents=True, exist_ok=True)
+    return p
+
+
+def autotune(det, fr, reps=3):
+    """Batch configuration of `det` for the frames of `fr` (cctagb_autotune)."""
+    import cctag_b200
+    from cctag_b200 import capi
+
+    ch = capi.TuneChoice()
+    det._check(det._lib.cctagb_autotune(det._h, fr, len(fr), str(tune_cache_path()).encode(), reps, C.byref(ch)),
+               "autotune")
+    return cctag_b200.tune_choice_dict(ch)
+
+
 def make_frames(config, n=N_FRAMES, rank=0):
     from cctag_b200.synth import config_frame
 
@@ -240,6 +259,8 @@ def run_b200(args, rank, world, local):
 
     fr_dev = batch_struct(d_frames, True)
     fr_host = batch_struct(h_frames, False)
+    # wave size and identification layout for this GPU and workload
+    tune = autotune(det, fr_dev)
 
     def step_batch(fr):
         def run(i):
@@ -415,7 +436,10 @@ def run_b200(args, rank, world, local):
                    "l2": "flushed between steps (256 MiB write, untimed)", "parallelism": f"replicas x{world}",
                    "batch_frame_p50_ms": round(statistics.median(batch_frame_ms), 3),
                    "batch_frame_p99_ms": round(float(np.percentile(batch_frame_ms, 99)), 3),
-                   "batched_equals_single": bool(same)},
+                   "batched_equals_single": bool(same),
+                   "batch_config": {"batchWaveFrames": tune["batchWaveFrames"],
+                                    "identLayout": ["auto", "block"][tune["identLayout"]]}},
+        "autotune": tune,
         "e2e": {"value": round(fps_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "plain": {"value": round(world * n_plain / (ms_plain * 1e-3), 2),
@@ -710,6 +734,7 @@ def run_c4(args, flush, torch):
         dev_batches.append(d)
         frs.append(fr)
         outs.append(o)
+    tune = autotune(det, frs[0])
     for k in range(args.warmup):
         for fr in frs:
             det._check(det._lib.cctagb_detect_batch(det._h, fr, BATCH), "detect_batch")
@@ -735,6 +760,7 @@ def run_c4(args, flush, torch):
             "markers_per_step": round(markers / steps, 1),
             "frame_p50_ms": round(statistics.median(per_frame), 3),
             "frame_p99_ms": round(float(np.percentile(per_frame, 99)), 3),
+            "autotune": tune,
             "note": "cctagb_detect_batch, frames in device memory; per-frame latency = host wall time of the "
                     "frame's detection inside the batch"}
 

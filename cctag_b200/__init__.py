@@ -165,12 +165,10 @@ class Detector:
                                                    C.byref(n), C.byref(stats)), "detect_device")
         return [out[i] for i in range(n.value)], stats
 
-    def detect_batch(self, frames, cap: int = 256):
-        """Detection of several independent frames (cctagb_detect_batch).
-
-        `frames` holds uint8 numpy arrays (host) or ``(device_ptr, w, h, pitch)``
-        tuples (device memory).  Returns one ``(markers, stats)`` pair per frame.
-        """
+    @staticmethod
+    def _frame_array(frames, cap):
+        """cctagb_frame array of uint8 numpy arrays (host) or ``(device_ptr,
+        w, h, pitch)`` tuples (device memory), with the buffers it points to."""
         n = len(frames)
         fr = (capi.Frame * n)()
         outs = [(capi.Marker * cap)() for _ in range(n)]
@@ -187,8 +185,30 @@ class Detector:
             fr[i].frame_id = i
             fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
             fr[i].cap = cap
+        return fr, outs, keep
+
+    def detect_batch(self, frames, cap: int = 256):
+        """Detection of several independent frames (cctagb_detect_batch).
+
+        `frames` holds uint8 numpy arrays (host) or ``(device_ptr, w, h, pitch)``
+        tuples (device memory).  Returns one ``(markers, stats)`` pair per frame.
+        """
+        fr, outs, _keep = self._frame_array(frames, cap)
+        n = len(frames)
         self._check(self._lib.cctagb_detect_batch(self._h, fr, n), "detect_batch")
         return [([outs[i][k] for k in range(fr[i].n_out)], fr[i].stats) for i in range(n)]
+
+    def autotune(self, frames, cache_path: str | None = None, reps: int = 3, cap: int = 256) -> dict:
+        """Choose and set the batch configuration for these frames
+        (cctagb_autotune): from the cache file when it holds the key, else
+        measured on the frames and written to the cache file."""
+        fr, _outs, _keep = self._frame_array(frames, cap)
+        ch = capi.TuneChoice()
+        path = None if cache_path is None else str(cache_path).encode()
+        self._check(self._lib.cctagb_autotune(self._h, fr, len(frames), path, int(reps), C.byref(ch)), "autotune")
+        self.params.batchWaveFrames = ch.batchWaveFrames
+        self.params.identLayout = ch.identLayout
+        return tune_choice_dict(ch)
 
     # -- streaming ingest --------------------------------------------------------
     def host_frames(self, n: int):
@@ -289,3 +309,35 @@ class Detector:
         self._check(self._lib.cctagb_detect(self._h, capi.ptr(g), W, H, W, frame_id, out, cap, C.byref(n),
                                             C.byref(stats)), "detect")
         return [out[i] for i in range(n.value)], stats
+
+
+def tune_choice_dict(ch: capi.TuneChoice) -> dict:
+    return {"batchWaveFrames": ch.batchWaveFrames, "identLayout": ch.identLayout,
+            "ms_per_frame": round(float(ch.ms_per_frame), 4), "from_cache": bool(ch.from_cache),
+            "tried": [{"batchWaveFrames": ch.tried_wave[i], "identLayout": ch.tried_layout[i],
+                       "ms_per_frame": round(float(ch.tried_ms_per_frame[i]), 4)} for i in range(ch.n_tried)]}
+
+
+def tune_key(gpu_name: str, sm_count: int, w: int, h: int, frames: int, n_crowns: int) -> str:
+    """Cache key of a batch configuration (cctagb_tune_key)."""
+    buf = C.create_string_buffer(512)
+    st = capi.load().cctagb_tune_key(gpu_name.encode(), sm_count, w, h, frames, n_crowns, buf, len(buf))
+    if st != capi.OK:
+        raise CCTagError(st, "tune_key")
+    return buf.value.decode()
+
+
+def tune_cache_get(cache_path: str, key: str) -> dict | None:
+    """The cache file's entry for `key` (cctagb_tune_cache_get), None if absent."""
+    ch = capi.TuneChoice()
+    st = capi.load().cctagb_tune_cache_get(str(cache_path).encode(), key.encode(), C.byref(ch))
+    return tune_choice_dict(ch) if st == capi.OK else None
+
+
+def tune_cache_put(cache_path: str, key: str, batch_wave_frames: int, ident_layout: int, ms_per_frame: float = 0.0):
+    """Add or replace the cache file's entry for `key` (cctagb_tune_cache_put)."""
+    ch = capi.TuneChoice()
+    ch.batchWaveFrames, ch.identLayout, ch.ms_per_frame = batch_wave_frames, ident_layout, ms_per_frame
+    st = capi.load().cctagb_tune_cache_put(str(cache_path).encode(), key.encode(), C.byref(ch))
+    if st != capi.OK:
+        raise CCTagError(st, "tune_cache_put")

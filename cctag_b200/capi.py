@@ -16,6 +16,8 @@ OVERFLOW_EDGES, OVERFLOW_SEEDS, OVERFLOW_VOTERS, HYST_NO_CONVERGE = 4, 5, 6, 7
 TOO_LARGE, BANK_ERROR, INTERNAL = 8, 9, 10
 
 REFINE_GRID, REFINE_GAUSS_NEWTON = 0, 1
+IDENT_AUTO, IDENT_BLOCK = 0, 1
+TUNE_MAX_TRIED = 16
 
 
 class Params(C.Structure):
@@ -36,7 +38,15 @@ class Params(C.Structure):
         ("maxEdges", C.c_uint32), ("refineMode", C.c_int), ("gnIterations", C.c_int),
         ("gnCoarseRounds", C.c_int), ("edgeCapacityDivisor", C.c_int), ("hostThreads", C.c_int),
         ("gnCoarseGrid", C.c_int), ("gnCoarseNeighbourSize", C.c_float), ("batchWaveFrames", C.c_int),
+        ("identLayout", C.c_int),
     ]
+
+
+class TuneChoice(C.Structure):
+    """Mirror of ``cctagb_tune_choice``."""
+    _fields_ = [("batchWaveFrames", C.c_int), ("identLayout", C.c_int), ("ms_per_frame", C.c_float),
+                ("from_cache", C.c_int), ("n_tried", C.c_int), ("tried_wave", C.c_int * TUNE_MAX_TRIED),
+                ("tried_layout", C.c_int * TUNE_MAX_TRIED), ("tried_ms_per_frame", C.c_float * TUNE_MAX_TRIED)]
 
 
 class Ellipse(C.Structure):
@@ -113,6 +123,10 @@ SIGNATURES = {
     "cctagb_stage_times": (_I, [_P, _I, _P, C.POINTER(_I)]),
     "cctagb_stage_name": (C.c_char_p, [_I]),
     "cctagb_edges_noalloc": (_I, [_P, _I, _I, _SZ, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
+    "cctagb_autotune": (_I, [_P, _P, _I, C.c_char_p, _I, C.POINTER(TuneChoice)]),
+    "cctagb_tune_key": (_I, [C.c_char_p, _I, _I, _I, _I, _I, C.c_char_p, _I]),
+    "cctagb_tune_cache_get": (_I, [C.c_char_p, C.c_char_p, C.POINTER(TuneChoice)]),
+    "cctagb_tune_cache_put": (_I, [C.c_char_p, C.c_char_p, C.POINTER(TuneChoice)]),
 }
 
 _lib = None

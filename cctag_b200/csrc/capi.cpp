@@ -15,6 +15,7 @@
 #include <thread>
 #include <vector>
 
+#include "autotune.hpp"
 #include "cctag_b200.h"
 #include "detector.hpp"
 #include "pipeline.hpp"
@@ -67,6 +68,15 @@ struct cctagb_handle {
         d.set_bank(flat.data(), int(b.size()), int(b[0].size()));
     }
     cctagb::Detector& slot(int i) { return i == 0 ? *det : *extra[size_t(i - 1)]; }
+    // Batch configuration (cctagb_autotune): on the handle's parameters and
+    // on every slot made so far (later slots copy the parameters).
+    void set_batch_config(int wave, int layout)
+    {
+        params.batchWaveFrames = wave;
+        params.identLayout = layout;
+        det->set_ident_layout(layout);
+        for (auto& d : extra) d->set_ident_layout(layout);
+    }
 
     // Streaming ingest (cctagb_submit / cctagb_wait): one worker thread per
     // slot takes queued tickets in order.
@@ -254,6 +264,7 @@ void cctagb_params_default(cctagb_params* p, int nCrowns)
     p->gnCoarseGrid = 3;
     p->gnCoarseNeighbourSize = 0.1f;
     p->batchWaveFrames = 4;
+    p->identLayout = CCTAGB_IDENT_AUTO;
 }
 
 const char* cctagb_status_string(cctagb_status s)
@@ -290,6 +301,7 @@ cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int ma
         cudaGetLastError();
         return CCTAGB_NO_DEVICE;
     }
+    if (p->identLayout != CCTAGB_IDENT_AUTO && p->identLayout != CCTAGB_IDENT_BLOCK) return CCTAGB_BAD_ARG;
     h->params = *p;
     h->max_w = max_w;
     h->max_h = max_h;
@@ -699,6 +711,107 @@ cctagb_status cctagb_detect_batch(cctagb_handle* h, cctagb_frame* frames, int n)
             if (frames[i].status != CCTAGB_OK)
                 throw cctagb::Error{frames[i].status, "frame " + std::to_string(i) + ": " + msg[size_t(i)]};
     });
+}
+
+cctagb_status cctagb_tune_key(const char* gpu_name, int sm_count, int w, int hgt, int frames, int nCrowns, char* out,
+                              int cap)
+{
+    if (!gpu_name || !out || cap < 1) return CCTAGB_BAD_ARG;
+    const std::string k = cctagb::tune::key(gpu_name, sm_count, w, hgt, frames, nCrowns);
+    if (k.size() + 1 > size_t(cap)) return CCTAGB_BAD_ARG;
+    std::memcpy(out, k.c_str(), k.size() + 1);
+    return CCTAGB_OK;
+}
+
+cctagb_status cctagb_tune_cache_get(const char* cache_path, const char* key, cctagb_tune_choice* out)
+{
+    if (!cache_path || !key || !out) return CCTAGB_BAD_ARG;
+    try {
+        cctagb_tune_choice c{};
+        if (!cctagb::tune::cache_get(cache_path, key, c)) return CCTAGB_BAD_ARG;
+        *out = c;
+        return CCTAGB_OK;
+    } catch (...) {
+        return CCTAGB_INTERNAL;
+    }
+}
+
+cctagb_status cctagb_tune_cache_put(const char* cache_path, const char* key, const cctagb_tune_choice* c)
+{
+    if (!cache_path || !key || !c) return CCTAGB_BAD_ARG;
+    if (c->batchWaveFrames < 1 || c->batchWaveFrames > cctagb::kMaxBatchFrames) return CCTAGB_BAD_ARG;
+    if (c->identLayout != CCTAGB_IDENT_AUTO && c->identLayout != CCTAGB_IDENT_BLOCK) return CCTAGB_BAD_ARG;
+    return guarded(nullptr, [&] { cctagb::tune::cache_put(cache_path, key, *c); });
+}
+
+cctagb_status cctagb_autotune(cctagb_handle* h, cctagb_frame* frames, int n, const char* cache_path, int reps,
+                              cctagb_tune_choice* out)
+{
+    if (!h || !frames || n < 1 || !out || reps < 1 || reps > 100) return CCTAGB_BAD_ARG;
+    if (refuse_if_streaming(h)) return CCTAGB_BAD_ARG;
+    bool uniform = true;
+    long long total_px = 0;
+    for (int i = 0; i < n; ++i) {
+        uniform = uniform && frames[i].w == frames[0].w && frames[i].h == frames[0].h;
+        total_px += (long long)frames[i].w * frames[i].h;
+    }
+    std::string key;
+    const cctagb_status ks = guarded(h, [&] {
+        cudaDeviceProp prop{};
+        CCTAGB_CUDA(cudaGetDeviceProperties(&prop, h->device));
+        key = uniform ? cctagb::tune::key(prop.name, prop.multiProcessorCount, frames[0].w, frames[0].h, n,
+                                          h->params.nCrowns)
+                      : cctagb::tune::key_mixed(prop.name, prop.multiProcessorCount, total_px, n, h->params.nCrowns);
+    });
+    if (ks != CCTAGB_OK) return ks;
+    cctagb_tune_choice best{};
+    if (cache_path && cctagb::tune::cache_get(cache_path, key, best)) {
+        h->set_batch_config(best.batchWaveFrames, best.identLayout);
+        *out = best;
+        return CCTAGB_OK;
+    }
+    // Candidates: wave sizes 1, 2, 4, .. up to the frames (and slots) of a
+    // call, each with both identification layouts; the least median wall
+    // time of a cctagb_detect_batch call wins.
+    const int maxWave = std::max(1, std::min({n, h->slots(), cctagb::kMaxBatchFrames}));
+    std::vector<std::pair<int, int>> cand;
+    for (int wf = 1; wf <= maxWave; wf *= 2)
+        for (int layout : {CCTAGB_IDENT_AUTO, CCTAGB_IDENT_BLOCK}) cand.emplace_back(wf, layout);
+    if (int(cand.size()) > CCTAGB_TUNE_MAX_TRIED) cand.resize(CCTAGB_TUNE_MAX_TRIED);
+    const cctagb_params saved = h->params;
+    cctagb_tune_choice res{};
+    float bestMs = 0.f;
+    for (const auto& c : cand) {
+        h->set_batch_config(c.first, c.second);
+        cctagb_status st = cctagb_detect_batch(h, frames, n);  // untimed: graphs, slots, caches
+        std::vector<float> ms;
+        for (int r = 0; r < reps && st == CCTAGB_OK; ++r) {
+            const auto t0 = std::chrono::steady_clock::now();
+            st = cctagb_detect_batch(h, frames, n);
+            ms.push_back(std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count());
+        }
+        if (st != CCTAGB_OK) {
+            h->set_batch_config(saved.batchWaveFrames, saved.identLayout);
+            return st;
+        }
+        std::sort(ms.begin(), ms.end());
+        const float perFrame = ms[ms.size() / 2] / float(n);
+        const int k = res.n_tried++;
+        res.tried_wave[k] = c.first;
+        res.tried_layout[k] = c.second;
+        res.tried_ms_per_frame[k] = perFrame;
+        if (k == 0 || perFrame < bestMs) {
+            bestMs = perFrame;
+            res.batchWaveFrames = c.first;
+            res.identLayout = c.second;
+        }
+    }
+    res.ms_per_frame = bestMs;
+    res.from_cache = 0;
+    h->set_batch_config(res.batchWaveFrames, res.identLayout);
+    *out = res;
+    if (cache_path) return guarded(h, [&] { cctagb::tune::cache_put(cache_path, key, res); });
+    return CCTAGB_OK;
 }
 
 }  // extern "C"

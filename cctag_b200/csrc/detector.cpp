@@ -104,6 +104,7 @@ IdentParams Detector::ident_params(int refine_mode) const
     ip.refineMode = refine_mode;
     ip.gnIterations = params_.gnIterations;
     ip.coarseRounds = params_.gnCoarseRounds;
+    ip.layout = params_.identLayout;
     if (refine_mode == CCTAGB_REFINE_GAUSS_NEWTON) {
         // the coarse rounds only pick the basin Gauss-Newton then descends
         ip.gridN = params_.gnCoarseGrid;

@@ -27,6 +27,7 @@ public:
     Detector& operator=(const Detector&) = delete;
 
     Pipeline& pipeline() { return pipe_; }
+    void set_ident_layout(int layout) { params_.identLayout = layout; }
     void set_bank(const float* ratios, int n_ids, int n_ratios);
     const std::vector<std::vector<float>>& bank() const { return bank_; }
 

@@ -31,6 +31,7 @@ struct IdentParams {
     int refineMode;         // CCTAGB_REFINE_GRID / CCTAGB_REFINE_GAUSS_NEWTON
     int gnIterations;       // Gauss-Newton cost evaluations at most
     int coarseRounds;       // grid rounds before Gauss-Newton
+    int layout;             // CCTAGB_IDENT_AUTO / CCTAGB_IDENT_BLOCK
 };
 
 constexpr int kMaxOuterPoints = 256;    // outer points per marker (nSamplesOuterEllipse)

@@ -1666,11 +1666,13 @@ void launch_identify(const uint8_t* d_img, size_t pitch, const IdentTask* d_task
     if (ip.refineMode == CCTAGB_REFINE_GAUSS_NEWTON && (ip.coarseRounds < 1 || ip.coarseRounds > 64))
         throw Error{CCTAGB_BAD_ARG, "gnCoarseRounds must be in [1, 64]"};
     // Few markers: a cluster of blocks each, so that a launch spreads over
-    // the SMs; many: one block each (the per-chunk sums are the same bits).
+    // the SMs; many (or the block layout asked for): one block each, which
+    // takes about half the SM time per marker (the per-chunk sums are the
+    // same bits).
     int dev = 0, sms = 0;
     CCTAGB_CUDA(cudaGetDevice(&dev));
     CCTAGB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    if (n * kCluster <= sms) {
+    if (ip.layout != CCTAGB_IDENT_BLOCK && n * kCluster <= sms) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(unsigned(n * kCluster));
         cfg.blockDim = dim3(kThreads);

@@ -36,6 +36,10 @@
  *   cctagb_cut_cost_f64    <- the same in double precision (a check form; no reference counterpart)
  *   cctagb_edges_noalloc   <- no reference counterpart (the edge stage on caller buffers,
  *                             allocating nothing)
+ *   cctagb_autotune / cctagb_tune_*
+ *                          <- no reference counterpart (the reference fixes its batch layout,
+ *                             one host thread and stream per pyramid level, at build time:
+ *                                                                  src/cctag/cuda/tag_threads.cu:19-91)
  *   cctagb_host_frames / cctagb_submit / cctagb_wait
  *                          <- page-locked frames + async upload    src/cctag/cuda/frame.cu:110-148
  */
@@ -119,7 +123,12 @@ typedef struct cctagb_params {
     int gnCoarseGrid;                           /* 3: trial grid (3 or 5 per side) of the coarse rounds of REFINE_GAUSS_NEWTON */
     float gnCoarseNeighbourSize;                /* 0.1: their neighbourhood, as imagedCenterNeighbourSize */
     int batchWaveFrames;                        /* 4: frames whose image stages share one launch in cctagb_detect_batch (1..16) */
+    int identLayout;                            /* CCTAGB_IDENT_AUTO: block layout of the identification kernel */
 } cctagb_params;
+
+/* Block layouts of the identification kernel (the results are the same bits). */
+#define CCTAGB_IDENT_AUTO 0     /* a cluster of 4 blocks per marker when a call's markers fit the SMs (least latency for one frame), else one block each */
+#define CCTAGB_IDENT_BLOCK 1    /* one block per marker (least SM time: for several frames in flight) */
 
 typedef struct cctagb_ellipse {
     float cx, cy, a, b, angle; /* parameters (Ellipse.hpp)            */
@@ -367,6 +376,47 @@ cctagb_status cctagb_cut_cost(cctagb_handle* h, const uint8_t* d_img, int w, int
 cctagb_status cctagb_cut_cost_f64(cctagb_handle* h, const uint8_t* d_img, int w, int hgt, size_t pitch,
                                   const cctagb_cut_task* tasks, int n, const float* centers, float* cost,
                                   float* d_center, float* d_h);
+
+/* ---- batch autotuning ---------------------------------------------------- */
+
+#define CCTAGB_TUNE_MAX_TRIED 16
+
+/* A batch configuration and how it was chosen. */
+typedef struct cctagb_tune_choice {
+    int batchWaveFrames;       /* frames per batched image-stage launch   */
+    int identLayout;           /* CCTAGB_IDENT_AUTO / CCTAGB_IDENT_BLOCK   */
+    float ms_per_frame;        /* median batch time / frames, when measured */
+    int from_cache;            /* 1: read from the cache file; 0: measured by this call */
+    int n_tried;               /* configurations measured by this call    */
+    int tried_wave[CCTAGB_TUNE_MAX_TRIED];
+    int tried_layout[CCTAGB_TUNE_MAX_TRIED];
+    float tried_ms_per_frame[CCTAGB_TUNE_MAX_TRIED];
+} cctagb_tune_choice;
+
+/* Picks the configuration of cctagb_detect_batch (params.batchWaveFrames and
+ * params.identLayout) for this handle's GPU, the frames' size and count and
+ * the number of crowns, and sets it on the handle.  With a cache file that
+ * holds an entry for that key (cctagb_tune_key), the entry is used; otherwise
+ * every candidate configuration detects the given frames `reps` times (after
+ * one untimed call) and the one with the least median time wins, and is
+ * written to the cache file when cache_path is not NULL.  Frames of several
+ * sizes are keyed by their total pixel count.  When measuring, the frames'
+ * markers and statistics are written as by cctagb_detect_batch. */
+cctagb_status cctagb_autotune(cctagb_handle* h, cctagb_frame* frames, int n, const char* cache_path, int reps,
+                              cctagb_tune_choice* out);
+
+/* Cache key of a configuration: the GPU's name and SM count, the frame size,
+ * frames per call, crowns and the cache format version.  Host only. */
+cctagb_status cctagb_tune_key(const char* gpu_name, int sm_count, int w, int hgt, int frames, int nCrowns, char* out,
+                              int cap);
+/* The cache is a JSON object {"version": V, "entries": {key: {...}}}.
+ * cctagb_tune_cache_get returns CCTAGB_OK and fills *out (from_cache = 1) when
+ * the file holds the key; CCTAGB_BAD_ARG when the file or key is absent, of
+ * another version or malformed.  cctagb_tune_cache_put adds or replaces the
+ * key's entry (other entries are kept) by writing a temporary file and
+ * renaming it over the cache file.  Host only. */
+cctagb_status cctagb_tune_cache_get(const char* cache_path, const char* key, cctagb_tune_choice* out);
+cctagb_status cctagb_tune_cache_put(const char* cache_path, const char* key, const cctagb_tune_choice* c);
 
 #ifdef __cplusplus
 }
