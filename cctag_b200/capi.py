@@ -38,7 +38,8 @@ class Params(C.Structure):
         ("maxEdges", C.c_uint32), ("refineMode", C.c_int), ("gnIterations", C.c_int),
         ("gnCoarseRounds", C.c_int), ("edgeCapacityDivisor", C.c_int), ("hostThreads", C.c_int),
         ("gnCoarseGrid", C.c_int), ("gnCoarseNeighbourSize", C.c_float), ("batchWaveFrames", C.c_int),
-        ("identLayout", C.c_int),
+        ("identLayout", C.c_int), ("hostSpinMicros", C.c_int), ("gpuEllipseGrowing", C.c_int),
+        ("gpuGrowMaxPoints", C.c_int),
     ]
 
 
@@ -65,7 +66,7 @@ class Stats(C.Structure):
                 ("markers", C.c_int), ("ms_image_stage", C.c_float), ("ms_host_candidates", C.c_float),
                 ("ms_identify", C.c_float), ("ms_total", C.c_float), ("h2d_bytes", C.c_longlong),
                 ("d2h_bytes", C.c_longlong), ("kernel_launches", C.c_int), ("ms_download", C.c_float),
-                ("ms_cut_selection", C.c_float)]
+                ("ms_cut_selection", C.c_float), ("grown_gpu", C.c_int), ("grown_host", C.c_int)]
 
 
 class Frame(C.Structure):

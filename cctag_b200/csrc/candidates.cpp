@@ -842,8 +842,9 @@ void link_and_filter(std::vector<LevelJob>& jobs, const cctagb_params& p, const 
 }
 
 void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
-                       const std::vector<LoopTwoIn>* given)
+                       const std::vector<LoopTwoIn>* given, const GrowFn* grow, int* grown)
 {
+    if (grown) grown[0] = grown[1] = 0;
     const int nl = int(jobs.size());
     std::vector<LevelState> st(static_cast<size_t>(nl));
     if (!given) {
@@ -880,10 +881,43 @@ void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, cons
             if (st[l].keep[i])
                 for (int q : st[l].loop1[i].filtered) jobs[l].es->n_segment_out[q] = -1;
     // Phase D: ellipse growing, each run with its own point marks.
-    pf(int(tasks.size()), [&](int t) {
-        const int l = tasks[t].first, i = tasks[t].second;
-        if (st[l].keep[i] && !flow_component_grow(st[l].loop1[i], *jobs[l].es, p)) st[l].keep[i] = 0;
-    });
+    if (grow) {
+        std::vector<GrowJob> gj;
+        std::vector<std::pair<int, int>> idx;
+        for (const auto& t : tasks) {
+            Candidate& c = st[t.first].loop1[size_t(t.second)];
+            if (!st[t.first].keep[size_t(t.second)]) continue;
+            GrowJob g;
+            g.level = t.first;
+            g.filtered = &c.filtered;
+            g.outer = &c.outer;
+            g.ellipse = &c.outerEllipse;
+            gj.push_back(g);
+            idx.push_back(t);
+        }
+        (*grow)(gj);
+        std::vector<int> rest;  // not grown there
+        for (size_t k = 0; k < gj.size(); ++k) {
+            if (gj[k].status == 2) rest.push_back(int(k));
+            else if (gj[k].status == 0) st[idx[k].first].keep[size_t(idx[k].second)] = 0;
+        }
+        pf(int(rest.size()), [&](int r) {
+            const auto& t = idx[size_t(rest[size_t(r)])];
+            if (!flow_component_grow(st[t.first].loop1[size_t(t.second)], *jobs[t.first].es, p))
+                st[t.first].keep[size_t(t.second)] = 0;
+        });
+        if (grown) {
+            grown[0] = int(gj.size() - rest.size());
+            grown[1] = int(rest.size());
+        }
+    } else {
+        if (grown)
+            for (const auto& t : tasks) grown[1] += st[t.first].keep[size_t(t.second)] ? 1 : 0;
+        pf(int(tasks.size()), [&](int t) {
+            const int l = tasks[t].first, i = tasks[t].second;
+            if (st[l].keep[i] && !flow_component_grow(st[l].loop1[i], *jobs[l].es, p)) st[l].keep[i] = 0;
+        });
+    }
     tasks.clear();
     for (int l = 0; l < nl; ++l) {
         for (size_t i = 0; i < st[l].keep.size(); ++i)

@@ -106,14 +106,29 @@ struct LoopTwoIn {
 void link_and_filter(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
                      std::vector<LoopTwoIn>& out);
 
+// Ellipse growing of one candidate done elsewhere (on the GPU): its level and
+// filtered points in; its outer points, ellipse and status out (0 it leaves
+// the list, 1 it stays, 2 not grown there: the host grows it).
+struct GrowJob {
+    int level = 0;
+    const std::vector<int>* filtered = nullptr;
+    std::vector<int>* outer = nullptr;
+    geo::Ellipse* ellipse = nullptr;
+    int status = 2;
+};
+using GrowFn = std::function<void(std::vector<GrowJob>&)>;
+
 // Candidate markers of every level (cctagDetectionFromEdges, Detection.cpp:
 // 568-693).  Loop 1 runs per level in seed order; loops 2 and 3 run per
 // candidate (each with its own PCG32 stream, seed 271828), with the segment
 // labels of loop 2 assigned in candidate order between them, so the result is
 // the same for any ParallelFor.  With `given`, loop 1 and the outlier removal
-// are taken from it (computed on the GPU) instead of being run here.
+// are taken from it (computed on the GPU) instead of being run here; with
+// `grow`, the ellipse growing of the candidates goes to it.
+// `grown` (optional) receives the candidates grown by `grow` and by the host.
 void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, const ParallelFor& pf,
-                       const std::vector<LoopTwoIn>* given = nullptr);
+                       const std::vector<LoopTwoIn>* given = nullptr, const GrowFn* grow = nullptr,
+                       int* grown = nullptr);
 
 // Level-0 re-fit of markers detected on coarser levels (Multiresolution.cpp:
 // 319-401), markers in parallel, each with its own PCG32 stream.

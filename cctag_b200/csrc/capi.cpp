@@ -265,6 +265,9 @@ void cctagb_params_default(cctagb_params* p, int nCrowns)
     p->gnCoarseNeighbourSize = 0.1f;
     p->batchWaveFrames = 4;
     p->identLayout = CCTAGB_IDENT_AUTO;
+    p->hostSpinMicros = -1;
+    p->gpuEllipseGrowing = 0;
+    p->gpuGrowMaxPoints = 2048;
 }
 
 const char* cctagb_status_string(cctagb_status s)

@@ -1,6 +1,7 @@
 // Shared definitions of the B200 CCTag library (host and device).
 #pragma once
 
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -102,6 +103,42 @@ struct Error {
             throw ::cctagb::Error{CCTAGB_CUDA_ERROR, std::string(#call) + ": " +             \
                                                          cudaGetErrorString(e__)};          \
     } while (0)
+
+// A host thread's waits on its stream: a spin on an event for at most
+// spin_us microseconds, then a blocking wait (the event is created with
+// cudaEventBlockingSync), so that a thread whose frame waits on the GPU gives
+// its core to the host stages of other frames.  spin_us < 0 spins throughout.
+class HostWaiter {
+public:
+    HostWaiter() = default;
+    ~HostWaiter()
+    {
+        if (ev_) cudaEventDestroy(ev_);
+    }
+    HostWaiter(const HostWaiter&) = delete;
+    HostWaiter& operator=(const HostWaiter&) = delete;
+    void init(int spin_us)
+    {
+        spin_us_ = spin_us;
+        if (!ev_) CCTAGB_CUDA(cudaEventCreateWithFlags(&ev_, cudaEventBlockingSync | cudaEventDisableTiming));
+    }
+    void wait(cudaStream_t s) const
+    {
+        CCTAGB_CUDA(cudaEventRecord(ev_, s));
+        const auto t0 = std::chrono::steady_clock::now();
+        for (;;) {
+            const cudaError_t q = cudaEventQuery(ev_);
+            if (q == cudaSuccess) return;
+            if (q != cudaErrorNotReady) CCTAGB_CUDA(q);
+            if (spin_us_ >= 0 && std::chrono::steady_clock::now() - t0 >= std::chrono::microseconds(spin_us_)) break;
+        }
+        CCTAGB_CUDA(cudaEventSynchronize(ev_));
+    }
+
+private:
+    cudaEvent_t ev_ = nullptr;
+    int spin_us_ = -1;
+};
 
 // Optional per-stage timing: when `ev` is non-null the launcher records
 // ev[k] after stage k (ev[0] before the first stage), kStageCount+1 events.

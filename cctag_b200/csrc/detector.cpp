@@ -33,6 +33,7 @@ Detector::Detector(const cctagb_params& p, int max_w, int max_h, int max_batch, 
     std::vector<int> caps;
     for (int l = 0; l < p.numberOfProcessedMultiresLayers; ++l) caps.push_back(pipe_.level_capacity(l));
     loop1_ = std::make_unique<LoopOneGpu>(p, max_h, caps);
+    if (p.gpuEllipseGrowing) grow_ = std::make_unique<GrowGpu>(p.hostSpinMicros, p.gpuGrowMaxPoints);
 }
 
 Detector::~Detector()
@@ -126,7 +127,7 @@ void Detector::identify_on(const uint8_t* d_img, size_t pitch, const IdentTask* 
     launch_identify(d_img, pitch, d_tasks_, d_res_, n, d_bank_inv_, ip, s);
     CCTAGB_CUDA(cudaEventRecord(ev_id1_, s));
     CCTAGB_CUDA(cudaMemcpyAsync(h_res_, d_res_, sizeof(IdentResult) * n, cudaMemcpyDeviceToHost, s));
-    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    pipe_.host_wait(s);
     std::memcpy(out, h_res_, sizeof(IdentResult) * n);
     pipe_.add_io((long long)sizeof(IdentTask) * n, (long long)sizeof(IdentResult) * n, 1);
 }
@@ -185,7 +186,7 @@ void Detector::select_and_identify(int nm, int npts, int w, int h)
     CCTAGB_CUDA(cudaMemcpyAsync(h_res_, d_res_, sizeof(IdentResult) * nm, cudaMemcpyDeviceToHost, s));
     CCTAGB_CUDA(cudaMemcpyAsync(h_st1_, d_st1_, sizeof(int) * nm, cudaMemcpyDeviceToHost, s));
     CCTAGB_CUDA(cudaMemcpyAsync(h_tasks_, d_tasks_, sizeof(IdentTask) * nm, cudaMemcpyDeviceToHost, s));
-    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    pipe_.host_wait(s);
     pipe_.add_io((long long)(sizeof(CutSelectIn) + sizeof(IdentTask) + sizeof(int)) * nm +
                      (long long)sizeof(DirPoint) * npts,
                  (long long)(sizeof(IdentResult) + sizeof(int) + sizeof(IdentTask)) * nm, 2);
@@ -257,7 +258,7 @@ void Detector::cut_cost(const uint8_t* d_img, int w, int h, size_t pitch, const 
     CCTAGB_CUDA(cudaMemcpyAsync(d_centers_, h_cost_, sizeof(float) * 2 * size_t(n), cudaMemcpyHostToDevice, s));
     launch_cut_cost(d_img, pitch, d_tasks_, d_centers_, d_cost_, n, ident_params(params_.refineMode), s, fp64);
     CCTAGB_CUDA(cudaMemcpyAsync(h_cost_, d_cost_, sizeof(float) * 12 * size_t(n), cudaMemcpyDeviceToHost, s));
-    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    pipe_.host_wait(s);
     for (int i = 0; i < n; ++i) {
         const float* o = h_cost_ + 12 * size_t(i);
         if (cost) cost[i] = o[0];
@@ -396,8 +397,38 @@ void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w
         jobs[l].level = l;
         jobs[l].scale = float(1 << l);
     }
+    // Ellipse growing of the candidates on the GPU: their filtered points up,
+    // outer points and ellipses down.
+    GrowFn growFn = [&](std::vector<GrowJob>& gj) {
+        std::vector<GrowTask> tasks(gj.size());
+        std::vector<int32_t> pts;
+        for (size_t k = 0; k < gj.size(); ++k) {
+            tasks[k].level = gj[k].level;
+            tasks[k].first = int(pts.size());
+            tasks[k].count = int(gj[k].filtered->size());
+            pts.insert(pts.end(), gj[k].filtered->begin(), gj[k].filtered->end());
+        }
+        int E[kMaxLevels] = {};
+        for (int l = 0; l < nl; ++l) E[l] = hl[l].E;
+        std::vector<GrowResult> res;
+        std::vector<int32_t> outer;
+        int stride = 0;
+        grow_->run(pipe_.level_views(), E, tasks, pts, params_.ellipseGrowingEllipticHullWidth,
+                   params_.thrMedianDistanceEllipse, pipe_.stream(), res, outer, stride);
+        pipe_.add_io(grow_->h2d_bytes(), grow_->d2h_bytes(), grow_->launches());
+        for (size_t k = 0; k < gj.size(); ++k) {
+            const GrowResult& r = res[k];
+            gj[k].status = r.status == kGrowKeep ? 1 : r.status == kGrowDrop ? 0 : 2;
+            if (r.status != kGrowKeep) continue;
+            const int32_t* o = outer.data() + k * size_t(stride);
+            gj[k].outer->assign(o, o + r.nOuter);
+            *gj[k].ellipse = geo::Ellipse::from_params(r.cx, r.cy, r.a, r.b, r.angle);
+        }
+    };
+    int grown[2] = {};
     detect_from_edges(
-        jobs, params_, [this](int n, const std::function<void(int)>& f) { pool_->parallel_for(n, f); }, &loop2in_);
+        jobs, params_, [this](int n, const std::function<void(int)>& f) { pool_->parallel_for(n, f); }, &loop2in_,
+        grow_ ? &growFn : nullptr, grown);
     // Coarse levels first, as the reference's loop from the top level down.
     std::vector<MarkerCand> markers;
     for (int l = nl - 1; l >= 0; --l)
@@ -558,6 +589,8 @@ void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w
         stats->kernel_launches = pipe_.kernel_launches();
         stats->ms_download = std::chrono::duration<float, std::milli>(t1d - t1).count();
         stats->ms_cut_selection = ms_cut;
+        stats->grown_gpu = grown[0];
+        stats->grown_host = grown[1];
     }
 }
 

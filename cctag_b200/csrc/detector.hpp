@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "candidates.hpp"
+#include "grow.hpp"
 #include "thread_pool.hpp"
 #include "ident_host.hpp"
 #include "loop_one.hpp"
@@ -72,6 +73,7 @@ private:
     std::vector<HostLevel> hl_;                  // per level, pinned downloads
     std::vector<EdgeSet> es_;                    // per level, candidate-stage state
     std::unique_ptr<LoopOneGpu> loop1_;          // loop 1 + outlier removal on the GPU
+    std::unique_ptr<GrowGpu> grow_;              // ellipse growing on the GPU (gpuEllipseGrowing)
     std::vector<LoopTwoIn> loop2in_;             // its results for the last frame
     std::shared_ptr<ThreadPool> pool_;
     CutSelectIn* d_cutin_ = nullptr;             // cut selection inputs (device / pinned)

@@ -207,7 +207,7 @@ struct Ellipse {
 };
 
 // Quadratic form p^T Q p for p = (x, y, 1).
-inline float qform(const Mat3& Q, float x, float y)
+CCTAGB_HD inline float qform(const Mat3& Q, float x, float y)
 {
     const float r0 = Q.m[0][0] * x + Q.m[0][1] * y + Q.m[0][2];
     const float r1 = Q.m[1][0] * x + Q.m[1][1] * y + Q.m[1][2];
@@ -222,9 +222,13 @@ inline bool is_in_ellipse(const Ellipse& e, float x, float y)
 }
 
 // EllipseGrowing.hpp:60-72: strictly between the two conics.
+CCTAGB_HD inline bool is_in_hull_q(const Mat3& qIn, const Mat3& qOut, float x, float y)
+{
+    return qform(qIn, x, y) * qform(qOut, x, y) < 0.f;
+}
 inline bool is_in_hull(const Ellipse& qIn, const Ellipse& qOut, float x, float y)
 {
-    return qform(qIn.Q, x, y) * qform(qOut.Q, x, y) < 0.f;
+    return is_in_hull_q(qIn.Q, qOut.Q, x, y);
 }
 
 // EllipseGrowing.cpp:424-441
@@ -281,12 +285,16 @@ inline int intersect_line(const Ellipse& e, float y, bool horizontal, float out[
     return intersect_line_q(e.Q, y, horizontal, out);
 }
 
-inline float round_half_away(float v) { return std::round(v); }
+CCTAGB_HD inline float round_half_away(float v) { return ::roundf(v); }
 
 // EllipseFromPoints.cpp:64-99 (computeIntermediatePoints) and :193-230
-// (rasterizeEllipsePerimeter): pixel length of the rasterised perimeter.
-inline int rasterize_perimeter(const Ellipse& e)
+// (rasterizeEllipsePerimeter): pixel length of the rasterised perimeter of
+// the ellipse (center, semi axes, angle).
+CCTAGB_HD inline int rasterize_perimeter_p(float ecx, float ecy, float ea, float eb, float eangle)
 {
+    struct {
+        float cx, cy, a, b, angle;
+    } e{ecx, ecy, ea, eb, eangle};
     auto pt = [&](float t, float& x, float& y) {
         const float ex = e.a * pm::cosf_(t), ey = e.b * pm::sinf_(t);
         x = ex * pm::cosf_(e.angle) - ey * pm::sinf_(e.angle) + e.cx;
@@ -309,15 +317,16 @@ inline int rasterize_perimeter(const Ellipse& e)
     const int p22x = int(round_half_away(x22)), p22y = int(round_half_away(y22));
     float d1, d2;
     {
-        const float mx = float(std::abs(p22x - p11x)), my = float(std::abs(p22y - p11y));
+        const float mx = float(::abs(p22x - p11x)), my = float(::abs(p22y - p11y));
         d1 = mx > my ? mx : my;
     }
     {
-        const float mx = float(std::abs(p12x - p22x)), my = float(std::abs(p12y - p22y));
+        const float mx = float(::abs(p12x - p22x)), my = float(::abs(p12y - p22y));
         d2 = mx > my ? mx : my;
     }
     return int((d1 + d2) * 2.f);
 }
+inline int rasterize_perimeter(const Ellipse& e) { return rasterize_perimeter_p(e.cx, e.cy, e.a, e.b, e.angle); }
 
 // EllipseFromPoints.cpp:29-48: radial projection of p onto the ellipse.
 inline void point_on_ellipse(const Ellipse& e, float px, float py, float& ox, float& oy)

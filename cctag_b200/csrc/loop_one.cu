@@ -1053,6 +1053,7 @@ LoopOneGpu::LoopOneGpu(const cctagb_params& p, int max_h, const std::vector<int>
         throw Error{CCTAGB_BAD_ARG, "maximumNbCandidatesLoopTwo must be in [1, 1024]"};
     nl_ = int(caps.size());
     n2max_ = p.maximumNbCandidatesLoopTwo;
+    waiter_.init(p.hostSpinMicros);
     // seeds processed per level: max(rows / 2, maximumNbSeeds) (Detection.cpp:603-605);
     // level 0 has the most rows
     maxSlotsPerLevel_ = std::max(max_h / 2, p.maximumNbSeeds);
@@ -1205,14 +1206,14 @@ void LoopOneGpu::run_kernels(cudaStream_t s)
 
 void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
 {
-    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    waiter_.wait(s);
     const int32_t* made = h_meta_ + size_t(nl_) * n2max_ * 4;
     // a candidate with more voters than the room: more room, same kernels
     // (no list can hold more points than its level)
     while ((made[nl_] & kLoopOneErrChildren) && size_t(args_.childCap) <= maxCap_) {
         grow_children(std::min(size_t(args_.childCap) * 4, maxCap_ + 1));
         run_kernels(s);
-        CCTAGB_CUDA(cudaStreamSynchronize(s));
+        waiter_.wait(s);
     }
     const int err = made[nl_];
     if (err & kLoopOneErrChildren)
@@ -1235,7 +1236,7 @@ void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
     }
     if (total) {
         CCTAGB_CUDA(cudaMemcpyAsync(h_flt_, d_packed_, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, s));
-        CCTAGB_CUDA(cudaStreamSynchronize(s));
+        waiter_.wait(s);
     }
     d2h_ += 4LL * total;
     out.assign(size_t(nl_), {});
@@ -1304,7 +1305,7 @@ void LoopOneGpu::refit(const Levels& lv, const std::vector<RefitTask>& tasks, cu
         k_refit_pack<<<n, 256, 0, s>>>(d_rhull_, hullCap_, d_rcount_, d_rpacked_);
         CCTAGB_CUDA(cudaGetLastError());
         CCTAGB_CUDA(cudaMemcpyAsync(h_rcount_, d_rcount_, sizeof(int32_t) * (n + 1), cudaMemcpyDeviceToHost, s));
-        CCTAGB_CUDA(cudaStreamSynchronize(s));
+        waiter_.wait(s);
         if (!(h_rcount_[n] & kLoopOneErrChildren) || size_t(hullCap_) > hullMax) break;
         // more room for the hulls, same kernels
         hullCap_ = int(std::min(size_t(hullCap_) * 4, hullMax + 1));
@@ -1329,7 +1330,7 @@ void LoopOneGpu::refit(const Levels& lv, const std::vector<RefitTask>& tasks, cu
     }
     if (total) {
         CCTAGB_CUDA(cudaMemcpyAsync(h_rpacked_, d_rpacked_, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, s));
-        CCTAGB_CUDA(cudaStreamSynchronize(s));
+        waiter_.wait(s);
     }
     h2d_ += (long long)sizeof(RefitTask) * n;
     d2h_ += 4LL * (n + 1) + 4LL * (long long)total;

@@ -106,6 +106,7 @@ private:
     void grow_children(size_t cap);     // children / packed buffers for `cap` per candidate
     void ensure_refit_capacity(int n);
     cctagb_params p_;
+    HostWaiter waiter_;            // waits of the calling thread on its stream
     int nl_ = 0, n2max_ = 0, maxSlotsPerLevel_ = 0, totalSlots_ = 0;
     LoopOneArgs args_{};
     int4 cum_{};                   // cumulative edge points of the levels (last launch)

@@ -61,6 +61,7 @@ Pipeline::Pipeline(const cctagb_params& p, int max_w, int max_h, int max_batch) 
     CCTAGB_CUDA(cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming));
     CCTAGB_CUDA(cudaEventCreateWithFlags(&ev_pack_, cudaEventDisableTiming));
     upload_constants(nullptr, 0, 0);
+    waiter_.init(p.hostSpinMicros);
     alloc(max_w, max_h);
 }
 
@@ -394,7 +395,7 @@ void Pipeline::sync_counters(cudaStream_t s)
 {
     CCTAGB_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(LevelCounters) * kMaxLevels, cudaMemcpyDeviceToHost, s));
     d2h_bytes_ += sizeof(LevelCounters) * kMaxLevels;
-    CCTAGB_CUDA(cudaStreamSynchronize(s));
+    waiter_.wait(s);
     for (int l = 0; l < lv_.n; ++l) {
         const int err = h_cnt_[l].err;
         if (err & kErrUnionFind) throw Error{CCTAGB_HYST_NO_CONVERGE, "hysteresis union-find exceeded its cap"};
@@ -438,7 +439,7 @@ void Pipeline::copy_planes(int l, uint8_t* src, int16_t* dx, int16_t* dy, uint8_
         bits.resize(size_t(v.WW) * v.H);
         CCTAGB_CUDA(cudaMemcpyAsync(bits.data(), v.bitmap, bits.size() * 4, cudaMemcpyDeviceToHost, stream_));
     }
-    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    waiter_.wait(stream_);
     if (edges) {
         for (int y = 0; y < v.H; ++y)
             for (int x = 0; x < v.W; ++x)
@@ -523,7 +524,7 @@ void Pipeline::download_level(int l, HostLevel& out)
 {
     if (l < 0 || l >= lv_.n) throw Error{CCTAGB_BAD_ARG, "level out of range"};
     issue_level_download(l, true);
-    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    waiter_.wait(stream_);
     finish_level_download(l, out, true);
 }
 
@@ -579,7 +580,7 @@ void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
         k.before = h_pack_ + ps.off[p + 2];
         k.after = h_pack_ + ps.off[p + 3];
     }
-    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    waiter_.wait(stream_);
     for (int l = 0; l < lv_.n; ++l) {
         const Packed& k = pk_[l];
         finish_level(l, out[l], false, k.sidx, k.skey, k.svotes);
@@ -589,7 +590,7 @@ void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
 
 void Pipeline::wait_points(std::vector<HostLevel>& out)
 {
-    CCTAGB_CUDA(cudaStreamSynchronize(copy_stream_));
+    waiter_.wait(copy_stream_);
     for (int l = 0; l < lv_.n; ++l) {
         const Packed& k = pk_[l];
         out[l].exy = k.exy;
@@ -603,7 +604,7 @@ void Pipeline::download_levels(std::vector<HostLevel>& out, bool voters)
 {
     out.resize(lv_.n);
     for (int l = 0; l < lv_.n; ++l) issue_level_download(l, voters);
-    CCTAGB_CUDA(cudaStreamSynchronize(stream_));
+    waiter_.wait(stream_);
     for (int l = 0; l < lv_.n; ++l) finish_level_download(l, out[l], voters);
 }
 

@@ -65,6 +65,8 @@ public:
     // ... and, once the batched launch has recorded `done`, this frame's
     // counters on the host (stage_ms and launches go to the statistics).
     void finish_batched(cudaEvent_t done, float stage_ms, int launches);
+    // Waits for the work queued on s (this pipeline's streams).
+    void host_wait(cudaStream_t s) const { waiter_.wait(s); }
     LevelCounters* device_counters() const { return d_cnt_; }
     const VoteParamsDev& vote_params() const { return vp_; }
     // Canny + thinning from caller derivatives (level 0 buffers).
@@ -120,6 +122,7 @@ private:
     cudaStream_t stage_stream_ = nullptr; // upload + image stage, lowest priority
     cudaStream_t copy_stream_ = nullptr;  // edge-point downloads of a detection
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    HostWaiter waiter_;                   // waits of the calling thread on stream_ / copy_stream_
     cudaEvent_t ev_in_ = nullptr;         // orders the stage stream after stream_
     std::shared_ptr<StageOrder> order_;
     std::vector<void*> allocs_;

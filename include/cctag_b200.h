@@ -124,6 +124,9 @@ typedef struct cctagb_params {
     float gnCoarseNeighbourSize;                /* 0.1: their neighbourhood, as imagedCenterNeighbourSize */
     int batchWaveFrames;                        /* 4: frames whose image stages share one launch in cctagb_detect_batch (1..16) */
     int identLayout;                            /* CCTAGB_IDENT_AUTO: block layout of the identification kernel */
+    int hostSpinMicros;                         /* -1: a host thread waiting on the GPU spins this long (microseconds), then sleeps until the GPU is done; < 0 spins throughout (least latency; sleeping frees the core for other work) */
+    int gpuEllipseGrowing;                      /* 0: the candidates' ellipse growing runs on the host; 1: on the GPU, one block per candidate (the same results bit for bit, but slower on B200: its fits are serial FP64 sums in point order) */
+    int gpuGrowMaxPoints;                       /* 2048: outer points a candidate may reach on the GPU (16..2048); a larger one grows on the host */
 } cctagb_params;
 
 /* Block layouts of the identification kernel (the results are the same bits). */
@@ -160,6 +163,8 @@ typedef struct cctagb_stats {
     int kernel_launches;       /* kernels launched by the call         */
     float ms_download;         /* host wall time of the edge-point downloads */
     float ms_cut_selection;    /* host wall time of the cut-selection set-up (outer points sorted by angle, tasks filled); the cut selection itself then runs on the GPU, just before identification */
+    int grown_gpu;             /* candidates whose ellipse growing ran on the GPU */
+    int grown_host;            /* ... on the host (gpuEllipseGrowing 0, or too many outer points for the kernel) */
 } cctagb_stats;
 
 typedef struct cctagb_handle cctagb_handle;
