@@ -438,7 +438,8 @@ def run_b200(args, rank, world, local):
                    "batch_frame_p99_ms": round(float(np.percentile(batch_frame_ms, 99)), 3),
                    "batched_equals_single": bool(same),
                    "batch_config": {"batchWaveFrames": tune["batchWaveFrames"],
-                                    "identLayout": ["auto", "block"][tune["identLayout"]]}},
+                                    "identLayout": ["auto", "block"][tune["identLayout"]],
+                                    "hostThreads": tune["hostThreads"] or "default"}},
         "autotune": tune,
         "e2e": {"value": round(fps_e2e, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},

@@ -208,6 +208,7 @@ class Detector:
         self._check(self._lib.cctagb_autotune(self._h, fr, len(frames), path, int(reps), C.byref(ch)), "autotune")
         self.params.batchWaveFrames = ch.batchWaveFrames
         self.params.identLayout = ch.identLayout
+        self.params.hostThreads = ch.hostThreads
         return tune_choice_dict(ch)
 
     # -- streaming ingest --------------------------------------------------------
@@ -312,9 +313,10 @@ class Detector:
 
 
 def tune_choice_dict(ch: capi.TuneChoice) -> dict:
-    return {"batchWaveFrames": ch.batchWaveFrames, "identLayout": ch.identLayout,
+    return {"batchWaveFrames": ch.batchWaveFrames, "identLayout": ch.identLayout, "hostThreads": ch.hostThreads,
             "ms_per_frame": round(float(ch.ms_per_frame), 4), "from_cache": bool(ch.from_cache),
             "tried": [{"batchWaveFrames": ch.tried_wave[i], "identLayout": ch.tried_layout[i],
+                       "hostThreads": ch.tried_threads[i],
                        "ms_per_frame": round(float(ch.tried_ms_per_frame[i]), 4)} for i in range(ch.n_tried)]}
 
 
@@ -334,10 +336,12 @@ def tune_cache_get(cache_path: str, key: str) -> dict | None:
     return tune_choice_dict(ch) if st == capi.OK else None
 
 
-def tune_cache_put(cache_path: str, key: str, batch_wave_frames: int, ident_layout: int, ms_per_frame: float = 0.0):
+def tune_cache_put(cache_path: str, key: str, batch_wave_frames: int, ident_layout: int, ms_per_frame: float = 0.0,
+                   host_threads: int = 0):
     """Add or replace the cache file's entry for `key` (cctagb_tune_cache_put)."""
     ch = capi.TuneChoice()
     ch.batchWaveFrames, ch.identLayout, ch.ms_per_frame = batch_wave_frames, ident_layout, ms_per_frame
+    ch.hostThreads = host_threads
     st = capi.load().cctagb_tune_cache_put(str(cache_path).encode(), key.encode(), C.byref(ch))
     if st != capi.OK:
         raise CCTagError(st, "tune_cache_put")

@@ -47,7 +47,8 @@ class TuneChoice(C.Structure):
     """Mirror of ``cctagb_tune_choice``."""
     _fields_ = [("batchWaveFrames", C.c_int), ("identLayout", C.c_int), ("ms_per_frame", C.c_float),
                 ("from_cache", C.c_int), ("n_tried", C.c_int), ("tried_wave", C.c_int * TUNE_MAX_TRIED),
-                ("tried_layout", C.c_int * TUNE_MAX_TRIED), ("tried_ms_per_frame", C.c_float * TUNE_MAX_TRIED)]
+                ("tried_layout", C.c_int * TUNE_MAX_TRIED), ("tried_ms_per_frame", C.c_float * TUNE_MAX_TRIED),
+                ("hostThreads", C.c_int), ("tried_threads", C.c_int * TUNE_MAX_TRIED)]
 
 
 class Ellipse(C.Structure):

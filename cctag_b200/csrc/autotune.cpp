@@ -273,6 +273,7 @@ bool cache_get(const std::string& path, const std::string& k, cctagb_tune_choice
     cctagb_tune_choice c{};
     if (!int_field(it->second, "batchWaveFrames", 1, kMaxBatchFrames, c.batchWaveFrames)) return false;
     if (!int_field(it->second, "identLayout", CCTAGB_IDENT_AUTO, CCTAGB_IDENT_BLOCK, c.identLayout)) return false;
+    if (!int_field(it->second, "hostThreads", 0, 64, c.hostThreads)) return false;
     auto ms = it->second.obj.find("ms_per_frame");
     if (ms != it->second.obj.end() && ms->second.kind == Value::Number) c.ms_per_frame = float(ms->second.num);
     c.from_cache = 1;
@@ -294,6 +295,7 @@ void cache_put(const std::string& path, const std::string& k, const cctagb_tune_
     };
     e.obj["batchWaveFrames"] = num(c.batchWaveFrames);
     e.obj["identLayout"] = num(c.identLayout);
+    e.obj["hostThreads"] = num(c.hostThreads);
     e.obj["ms_per_frame"] = num(c.ms_per_frame);
     entries[k] = e;
     std::ostringstream o;

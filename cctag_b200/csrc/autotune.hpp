@@ -11,7 +11,7 @@
 namespace cctagb {
 namespace tune {
 
-constexpr int kCacheVersion = 1;
+constexpr int kCacheVersion = 2;
 
 std::string key(const char* gpu_name, int sm_count, int w, int h, int frames, int n_crowns);
 // Frames of several sizes: named by their total pixel count.

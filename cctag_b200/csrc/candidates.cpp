@@ -328,18 +328,22 @@ bool ellipse_growing_init(const EdgeSet& es, const std::vector<int>& fc, Ellipse
 }
 
 // EllipseGrowing.cpp:378-422 connectedPoint: depth-first growth through
-// 8-neighbours inside the hull whose gradient points away from the center.
-// Iterative form of the reference's recursion (same visiting order).
-void connected_point(std::vector<int>& pts, RunMarks& mk, EdgeSet& es, const Ellipse& qIn, const Ellipse& qOut,
-                     int x, int y)
+// 8-neighbours inside the hull whose gradient points away from the center,
+// from listed point p.  Iterative form of the reference's recursion (same
+// visiting order).  Returns whether p is saturated: every edge pixel around
+// it is marked, so no later pass can grow anything from it (marks only grow
+// until the growing loop resets them).
+bool connected_point(std::vector<int>& pts, RunMarks& mk, EdgeSet& es, const Ellipse& qIn, const Ellipse& qOut,
+                     int p)
 {
     static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
     static const int yoff[8] = {0, -1, -1, -1, 0, 1, 1, 1};
     using Frame = EdgeSet::DfsFrame;
     thread_local std::vector<Frame> st;  // reused across calls of this thread
     st.clear();
-    mk.set(es.at(x, y));
-    st.push_back({x, y, 0});
+    mk.set(p);  // the reference marks the start point; a listed point already is
+    st.push_back({es.x(p), es.y(p), 0});
+    bool saturated = true;
     while (!st.empty()) {
         Frame& f = st.back();
         if (f.k >= 8) {
@@ -347,30 +351,39 @@ void connected_point(std::vector<int>& pts, RunMarks& mk, EdgeSet& es, const Ell
             continue;
         }
         const int k = f.k++;
+        const bool start = st.size() == 1;
         const int sx = f.x + xoff[k], sy = f.y + yoff[k];
         if (sx < 0 || sx >= es.W || sy < 0 || sy >= es.H) continue;
         const int e = es.at(sx, sy);
         if (e < 0) continue;
-        if (mk.test(e) || !geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e)))) continue;
-        const float ox = qIn.cx - float(es.x(e)), oy = qIn.cy - float(es.y(e));
-        if (es.dx(e) * ox + es.dy(e) * oy < 0) {
+        if (mk.test(e)) continue;
+        bool grow = geo::is_in_hull(qIn, qOut, float(es.x(e)), float(es.y(e)));
+        if (grow) {
+            const float ox = qIn.cx - float(es.x(e)), oy = qIn.cy - float(es.y(e));
+            grow = es.dx(e) * ox + es.dy(e) * oy < 0;
+        }
+        if (grow) {
             pts.push_back(e);
             mk.set(e);
             st.push_back({sx, sy, 0});
+        } else if (start) {
+            saturated = false;  // an unmarked edge pixel another hull may take
         }
     }
+    return saturated;
 }
 
-// EllipseGrowing.cpp:443-457
-void ellipse_hull(EdgeSet& es, std::vector<int>& pts, const Ellipse& e, float delta, RunMarks& mk)
+// EllipseGrowing.cpp:443-457.  sat[i]: list point i is saturated (skipped:
+// it would add nothing and mark nothing).
+void ellipse_hull(EdgeSet& es, std::vector<int>& pts, const Ellipse& e, float delta, RunMarks& mk,
+                  std::vector<uint8_t>& sat)
 {
     Ellipse qIn, qOut;
     geo::compute_hull(e, delta, qIn, qOut);
     const size_t init = pts.size();
-    for (size_t i = 0; i < init; ++i) {
-        const int p = pts[i];
-        connected_point(pts, mk, es, qIn, qOut, es.x(p), es.y(p));
-    }
+    sat.resize(init, 0);
+    for (size_t i = 0; i < init; ++i)
+        if (!sat[i] && connected_point(pts, mk, es, qIn, qOut, pts[i])) sat[i] = 1;
 }
 
 size_t count_in_hull(const EdgeSet& es, const std::vector<int>& pts, const Ellipse& e, float width)
@@ -388,7 +401,9 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
                       bool goodInit)
 {
     thread_local RunMarks mk;
+    thread_local std::vector<uint8_t> sat;  // saturated list points (connected_point)
     mk.begin(size_t(es.E));
+    sat.clear();
     outer = fc;
     for (int c : fc) mk.set(c);
     if (!goodInit) {
@@ -399,7 +414,7 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
         ++nIter;
         while (newSize - lastSize > 0) {
             lastSize = int(count_in_hull(es, outer, ellipse, width));
-            ellipse_hull(es, outer, ellipse, width, mk);
+            ellipse_hull(es, outer, ellipse, width, mk, sat);
             sets.push_back(outer);
             ells.push_back(ellipse);
             ellipse = fit_circle_points(es, outer);
@@ -415,12 +430,13 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
         for (auto& s : sets)
             for (int p : s) mk.clear(p);
         for (int p : outer) mk.set(p);
+        sat.clear();  // marks were taken back
     }
     ellipse = fit_points(es, outer);
     size_t lastSize = 0;
     while (outer.size() > lastSize) {
         lastSize = outer.size();
-        ellipse_hull(es, outer, ellipse, width, mk);
+        ellipse_hull(es, outer, ellipse, width, mk, sat);
         ellipse = fit_points(es, outer);
     }
 }

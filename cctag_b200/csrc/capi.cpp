@@ -1,6 +1,7 @@
 // C ABI of the library (include/cctag_b200.h).  Converts exceptions into
 // status codes; nothing crosses the ABI as a C++ exception.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -45,6 +46,7 @@ struct cctagb_handle {
     std::vector<std::unique_ptr<cctagb::Detector>> extra;  // slots 1..: cctagb_detect_batch
     cctagb_params params{};
     int max_w = 0, max_h = 0, max_batch = 1, device = 0;
+    int pool_threads = 0;                         // the host pool's size, counting the caller
     std::string last_error;
 
     int slots() const { return std::max(1, std::min(max_batch, kMaxSlots)); }
@@ -70,13 +72,26 @@ struct cctagb_handle {
     cctagb::Detector& slot(int i) { return i == 0 ? *det : *extra[size_t(i - 1)]; }
     // Batch configuration (cctagb_autotune): on the handle's parameters and
     // on every slot made so far (later slots copy the parameters).
-    void set_batch_config(int wave, int layout)
+    void set_batch_config(int wave, int layout, int threads)
     {
         params.batchWaveFrames = wave;
         params.identLayout = layout;
         det->set_ident_layout(layout);
         for (auto& d : extra) d->set_ident_layout(layout);
+        const int t = threads > 0 ? threads : default_pool_threads();
+        if (t != pool_threads) {
+            pool = cctagb::make_host_pool(t);
+            det->set_pool(pool);
+            for (auto& d : extra) d->set_pool(pool);
+            pool_threads = t;
+        }
+        params.hostThreads = threads;
     }
+    // One thread per physical core, less one per detection slot beyond the
+    // first -- a slot's own thread works in its frame's parallel loops and
+    // spins while it waits on the GPU (measured on a 16-core host with 8
+    // slots: 8 pool threads 1.09-1.13 k frames/s, 16 threads 0.99 k).
+    int default_pool_threads() const { return std::max(2, cctagb::physical_cores() - (slots() - 1)); }
 
     // Streaming ingest (cctagb_submit / cctagb_wait): one worker thread per
     // slot takes queued tickets in order.
@@ -311,13 +326,9 @@ cctagb_status cctagb_create(const cctagb_params* p, int max_w, int max_h, int ma
     h->max_batch = max_batch;
     cudaGetDevice(&h->device);
     const cctagb_status s = guarded(h.get(), [&] {
-        // Default pool size: one thread per physical core, less one per extra
-        // detection slot -- a slot's own thread works in its frame's parallel
-        // loops and spins while it waits on the GPU (measured on a 16-core host
-        // with 8 slots: 8 pool threads 1.09-1.13 k frames/s, 16 threads 0.99 k).
-        int threads = p->hostThreads;
-        if (threads <= 0) threads = std::max(2, cctagb::physical_cores() - (h->slots() - 1));
+        const int threads = p->hostThreads > 0 ? p->hostThreads : h->default_pool_threads();
         h->pool = cctagb::make_host_pool(threads);
+        h->pool_threads = threads;
         h->det.reset(new cctagb::Detector(*p, max_w, max_h, max_batch, h->pool));
         h->order = std::make_shared<cctagb::StageOrder>();
         h->det->pipeline().set_stage_order(h->order);
@@ -744,6 +755,7 @@ cctagb_status cctagb_tune_cache_put(const char* cache_path, const char* key, con
     if (!cache_path || !key || !c) return CCTAGB_BAD_ARG;
     if (c->batchWaveFrames < 1 || c->batchWaveFrames > cctagb::kMaxBatchFrames) return CCTAGB_BAD_ARG;
     if (c->identLayout != CCTAGB_IDENT_AUTO && c->identLayout != CCTAGB_IDENT_BLOCK) return CCTAGB_BAD_ARG;
+    if (c->hostThreads < 0 || c->hostThreads > 64) return CCTAGB_BAD_ARG;
     return guarded(nullptr, [&] { cctagb::tune::cache_put(cache_path, key, *c); });
 }
 
@@ -769,49 +781,68 @@ cctagb_status cctagb_autotune(cctagb_handle* h, cctagb_frame* frames, int n, con
     if (ks != CCTAGB_OK) return ks;
     cctagb_tune_choice best{};
     if (cache_path && cctagb::tune::cache_get(cache_path, key, best)) {
-        h->set_batch_config(best.batchWaveFrames, best.identLayout);
+        const cctagb_status st = guarded(h, [&] { h->set_batch_config(best.batchWaveFrames, best.identLayout,
+                                                                      best.hostThreads); });
+        if (st != CCTAGB_OK) return st;
         *out = best;
         return CCTAGB_OK;
     }
     // Candidates: wave sizes 1, 2, 4, .. up to the frames (and slots) of a
-    // call, each with both identification layouts; the least median wall
-    // time of a cctagb_detect_batch call wins.
+    // call, each with both identification layouts, at the handle's pool
+    // size; then, with the best of those, pools of 4, 8 and 16 threads.  The
+    // least median wall time of a cctagb_detect_batch call wins.
     const int maxWave = std::max(1, std::min({n, h->slots(), cctagb::kMaxBatchFrames}));
-    std::vector<std::pair<int, int>> cand;
+    const int threads0 = h->params.hostThreads;
+    std::vector<std::array<int, 3>> cand;
     for (int wf = 1; wf <= maxWave; wf *= 2)
-        for (int layout : {CCTAGB_IDENT_AUTO, CCTAGB_IDENT_BLOCK}) cand.emplace_back(wf, layout);
-    if (int(cand.size()) > CCTAGB_TUNE_MAX_TRIED) cand.resize(CCTAGB_TUNE_MAX_TRIED);
+        for (int layout : {CCTAGB_IDENT_AUTO, CCTAGB_IDENT_BLOCK}) cand.push_back({wf, layout, threads0});
     const cctagb_params saved = h->params;
     cctagb_tune_choice res{};
     float bestMs = 0.f;
-    for (const auto& c : cand) {
-        h->set_batch_config(c.first, c.second);
-        cctagb_status st = cctagb_detect_batch(h, frames, n);  // untimed: graphs, slots, caches
+    auto measure = [&](const std::array<int, 3>& c) -> cctagb_status {
+        if (res.n_tried >= CCTAGB_TUNE_MAX_TRIED) return CCTAGB_OK;
+        cctagb_status st = guarded(h, [&] { h->set_batch_config(c[0], c[1], c[2]); });
+        if (st == CCTAGB_OK) st = cctagb_detect_batch(h, frames, n);  // untimed: graphs, slots, caches
         std::vector<float> ms;
         for (int r = 0; r < reps && st == CCTAGB_OK; ++r) {
             const auto t0 = std::chrono::steady_clock::now();
             st = cctagb_detect_batch(h, frames, n);
             ms.push_back(std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count());
         }
-        if (st != CCTAGB_OK) {
-            h->set_batch_config(saved.batchWaveFrames, saved.identLayout);
-            return st;
-        }
+        if (st != CCTAGB_OK) return st;
         std::sort(ms.begin(), ms.end());
         const float perFrame = ms[ms.size() / 2] / float(n);
         const int k = res.n_tried++;
-        res.tried_wave[k] = c.first;
-        res.tried_layout[k] = c.second;
+        res.tried_wave[k] = c[0];
+        res.tried_layout[k] = c[1];
+        res.tried_threads[k] = c[2];
         res.tried_ms_per_frame[k] = perFrame;
         if (k == 0 || perFrame < bestMs) {
             bestMs = perFrame;
-            res.batchWaveFrames = c.first;
-            res.identLayout = c.second;
+            res.batchWaveFrames = c[0];
+            res.identLayout = c[1];
+            res.hostThreads = c[2];
         }
+        return CCTAGB_OK;
+    };
+    cctagb_status st = CCTAGB_OK;
+    for (const auto& c : cand)
+        if (st == CCTAGB_OK) st = measure(c);
+    const int base = h->default_pool_threads();
+    for (int t : {4, 8, 16})
+        if (st == CCTAGB_OK && t != (threads0 > 0 ? threads0 : base))
+            st = measure({res.batchWaveFrames, res.identLayout, t});
+    if (st != CCTAGB_OK) {
+        guarded(h, [&] { h->set_batch_config(saved.batchWaveFrames, saved.identLayout, saved.hostThreads); });
+        return st;
     }
     res.ms_per_frame = bestMs;
     res.from_cache = 0;
-    h->set_batch_config(res.batchWaveFrames, res.identLayout);
+    {
+        const cctagb_status s2 = guarded(h, [&] { h->set_batch_config(res.batchWaveFrames, res.identLayout,
+                                                                       res.hostThreads); });
+        if (s2 != CCTAGB_OK) return s2;
+    }
     *out = res;
     if (cache_path) return guarded(h, [&] { cctagb::tune::cache_put(cache_path, key, res); });
     return CCTAGB_OK;

@@ -29,6 +29,7 @@ public:
 
     Pipeline& pipeline() { return pipe_; }
     void set_ident_layout(int layout) { params_.identLayout = layout; }
+    void set_pool(std::shared_ptr<ThreadPool> pool) { pool_ = std::move(pool); }
     void set_bank(const float* ratios, int n_ids, int n_ratios);
     const std::vector<std::vector<float>>& bank() const { return bank_; }
 

@@ -396,11 +396,14 @@ typedef struct cctagb_tune_choice {
     int tried_wave[CCTAGB_TUNE_MAX_TRIED];
     int tried_layout[CCTAGB_TUNE_MAX_TRIED];
     float tried_ms_per_frame[CCTAGB_TUNE_MAX_TRIED];
+    int hostThreads;           /* host worker pool size (params.hostThreads) */
+    int tried_threads[CCTAGB_TUNE_MAX_TRIED];
 } cctagb_tune_choice;
 
-/* Picks the configuration of cctagb_detect_batch (params.batchWaveFrames and
- * params.identLayout) for this handle's GPU, the frames' size and count and
- * the number of crowns, and sets it on the handle.  With a cache file that
+/* Picks the configuration of cctagb_detect_batch (params.batchWaveFrames,
+ * params.identLayout, then the host pool size params.hostThreads) for this
+ * handle's GPU, the frames' size and count and the number of crowns, and sets
+ * it on the handle.  With a cache file that
  * holds an entry for that key (cctagb_tune_key), the entry is used; otherwise
  * every candidate configuration detects the given frames `reps` times (after
  * one untimed call) and the one with the least median time wins, and is

@@ -26,7 +26,8 @@ def test_put_then_get_round_trip(built_library, tmp_path):
     assert got["batchWaveFrames"] == 8 and got["identLayout"] == capi.IDENT_BLOCK
     assert got["from_cache"] and abs(got["ms_per_frame"] - 0.625) < 1e-6
     doc = json.loads(f.read_text())
-    assert doc["version"] == 1 and doc["entries"]["k1"]["batchWaveFrames"] == 8
+    assert doc["version"] == 2 and doc["entries"]["k1"]["batchWaveFrames"] == 8
+    assert doc["entries"]["k1"]["hostThreads"] == 0
 
 
 def test_other_entries_are_kept_and_replaced_in_place(built_library, tmp_path):
@@ -43,14 +44,17 @@ def test_other_entries_are_kept_and_replaced_in_place(built_library, tmp_path):
 
 
 @pytest.mark.parametrize("text", [
-    "", "{", "[]", '{"version": 2, "entries": {"k": {"batchWaveFrames": 4, "identLayout": 0}}}',
-    '{"version": 1, "entries": []}',
-    '{"version": 1, "entries": {"k": {"batchWaveFrames": 0, "identLayout": 0}}}',
-    '{"version": 1, "entries": {"k": {"batchWaveFrames": 17, "identLayout": 0}}}',
-    '{"version": 1, "entries": {"k": {"batchWaveFrames": 4.5, "identLayout": 0}}}',
-    '{"version": 1, "entries": {"k": {"batchWaveFrames": 4, "identLayout": 2}}}',
-    '{"version": 1, "entries": {"k": {"batchWaveFrames": "4", "identLayout": 0}}}',
-    '{"version": 1, "entries": {"k": {"identLayout": 0}}} trailing',
+    "", "{", "[]",
+    '{"version": 1, "entries": {"k": {"batchWaveFrames": 4, "identLayout": 0, "hostThreads": 0}}}',
+    '{"version": 2, "entries": []}',
+    '{"version": 2, "entries": {"k": {"batchWaveFrames": 0, "identLayout": 0, "hostThreads": 0}}}',
+    '{"version": 2, "entries": {"k": {"batchWaveFrames": 17, "identLayout": 0, "hostThreads": 0}}}',
+    '{"version": 2, "entries": {"k": {"batchWaveFrames": 4.5, "identLayout": 0, "hostThreads": 0}}}',
+    '{"version": 2, "entries": {"k": {"batchWaveFrames": 4, "identLayout": 2, "hostThreads": 0}}}',
+    '{"version": 2, "entries": {"k": {"batchWaveFrames": 4, "identLayout": 0, "hostThreads": 65}}}',
+    '{"version": 2, "entries": {"k": {"batchWaveFrames": 4, "identLayout": 0}}}',
+    '{"version": 2, "entries": {"k": {"batchWaveFrames": "4", "identLayout": 0, "hostThreads": 0}}}',
+    '{"version": 2, "entries": {"k": {"identLayout": 0, "hostThreads": 0}}} trailing',
     "[" * 100 + "]" * 100,
 ])
 def test_malformed_foreign_or_out_of_range_entries_are_misses(built_library, tmp_path, text):
@@ -72,9 +76,9 @@ def test_escaped_keys_round_trip(built_library, tmp_path):
 
 def test_put_rejects_out_of_range_choices(built_library, tmp_path):
     f = tmp_path / "tune.json"
-    for wave, layout in ((0, 0), (17, 0), (4, 2), (4, -1)):
+    for wave, layout, threads in ((0, 0, 0), (17, 0, 0), (4, 2, 0), (4, -1, 0), (4, 0, -1), (4, 0, 65)):
         with pytest.raises(cctag_b200.CCTagError):
-            cctag_b200.tune_cache_put(f, "k", wave, layout)
+            cctag_b200.tune_cache_put(f, "k", wave, layout, host_threads=threads)
     assert not f.exists()
     with pytest.raises(cctag_b200.CCTagError):
         cctag_b200.tune_cache_put(tmp_path / "no_such_dir" / "tune.json", "k", 4, 0)
@@ -90,17 +94,19 @@ def test_autotune_measures_then_reads_the_cache(built_library, tmp_path):
     with cctag_b200.Detector(max_w=w, max_h=h, max_batch=4) as det:
         want = [[(m.id, m.status, m.x, m.y) for m in r[0]] for r in det.detect_batch(frames)]
         first = det.autotune(frames, cache_path=f, reps=2)
-        assert not first["from_cache"] and len(first["tried"]) == 6  # waves 1, 2, 4 x two layouts
-        assert (first["batchWaveFrames"], first["identLayout"]) in \
-            {(t["batchWaveFrames"], t["identLayout"]) for t in first["tried"]}
+        # waves 1, 2, 4 x two layouts, then pool sizes at the best of those
+        assert not first["from_cache"] and 6 < len(first["tried"]) <= 9
+        assert (first["batchWaveFrames"], first["identLayout"], first["hostThreads"]) in \
+            {(t["batchWaveFrames"], t["identLayout"], t["hostThreads"]) for t in first["tried"]}
         assert det.params.batchWaveFrames == first["batchWaveFrames"]
+        assert det.params.hostThreads == first["hostThreads"]
         got = [[(m.id, m.status, m.x, m.y) for m in r[0]] for r in det.detect_batch(frames)]
         assert got == want
     with cctag_b200.Detector(max_w=w, max_h=h, max_batch=4) as det:
         second = det.autotune(frames, cache_path=f)
         assert second["from_cache"] and second["tried"] == []
-        assert (second["batchWaveFrames"], second["identLayout"]) == \
-            (first["batchWaveFrames"], first["identLayout"])
+        assert (second["batchWaveFrames"], second["identLayout"], second["hostThreads"]) == \
+            (first["batchWaveFrames"], first["identLayout"], first["hostThreads"])
         got = [[(m.id, m.status, m.x, m.y) for m in r[0]] for r in det.detect_batch(frames)]
         assert got == want
 
