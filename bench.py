@@ -161,7 +161,7 @@ def tune_cache_path():
     return p
 
 
-def autotune(det, fr, reps=3):
+def autotune(det, fr, reps=5):
     """Batch configuration of `det` for the frames of `fr` (cctagb_autotune)."""
     import cctag_b200
     from cctag_b200 import capi
@@ -188,11 +188,12 @@ def stage_bytes(levels, E, S, V):
     return {
         "pyramid": n[0] + sum(n[1:]),                 # read level 0, write levels 1..3
         "deriv_nms": 6 * nt,                          # 1 B in, dx+dy 4 B + class map 1 B out
-        "hyst_merge": 1 * nt,                         # class map in (labels are its own output)
-        "hyst_compress": 1 * nt,                      # class map in
-        "final_thin": 1 * nt + nt // 8,               # hysteresis result in, edge bitmap out
+        "hyst_merge": 1 * nt,                         # class map in (tile bit planes are its own output)
+        "hyst_compress": 3 * nt // 8,                 # two tile bit planes in, result bit plane out
+        "final_thin": nt // 4,                        # result bit plane in, edge bitmap out
         "row_scan": 8 * sum(h for (_, h) in levels),
-        "emit": nt // 8 + 4 * Et + 4 * Et + 4 * Et,   # bitmap in, dx/dy gathers, points + index map out
+        # bitmap in, word + first-index plane out, dx/dy gathers, points, gradients, vote counters out
+        "emit": nt // 8 + nt // 4 + 4 * Et + 16 * Et,
         "walk": 8 * Et + 8 * Et + nt // 8,            # points + gradients in, links out, bitmap once
         "vote": 8 * Et + 8 * Et,                      # links in, chosen + length out
         "voter_scan": 4 * Et + 4 * Et,
@@ -209,10 +210,11 @@ def ident_flops(n_markers, rounds=10, trials=25, cuts=22, samples=100):
 
 
 def profiled_traffic(config):
-    """DRAM bytes per launch of each image-stage kernel group, from the ncu
-    summary of this workload under profiles/ (cold-cache capture; the
-    `stage: bytes` lines of its last code block)."""
-    name = {"c2_1080p": "dram_image_stage_c2_1080p.md"}.get(config)
+    """DRAM bytes per launch of each image-stage kernel group (one launch over
+    the 16 frames of a step), from the ncu summary of this workload under
+    profiles/ (cold-cache capture; the `stage: bytes` lines of its last code
+    block)."""
+    name = {"c2_1080p": "dram_image_stage_c2_1080p_batch16.md"}.get(config)
     f = ROOT / "profiles" / name if name else None
     if not f or not f.exists():
         return {}

@@ -735,7 +735,7 @@ __global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
 // after that step; the steps and probes of every walk are those of the
 // reference in the same order, so the results do not depend on the schedule.
 constexpr int kWalkWarps = 8;
-constexpr int kWalkChunk = 512;  // walks (two per point) a warp takes at once
+constexpr int kWalkChunk = 512;  // walks (two per point) a warp takes at once, at most
 
 __device__ __forceinline__ int sgn_i(int v) { return (v > 0) - (v < 0); }
 
@@ -751,16 +751,22 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
     const int gw = blockIdx.x * kWalkWarps + wid, NW = gridDim.x * kWalkWarps;
     const int nmax = vp.distSearch;
     const float thr = float(vp.thrGradient);
+    // chunk size: the launch's walks spread over its warps (a multiple of 32,
+    // 32 .. kWalkChunk), the same in every block
+    long long walks = 0;
+    for (int l = 0; l < lv.n; ++l) walks += 2LL * lv.cnt[l].E;
+    long long per = (walks / NW + 31) / 32 * 32;
+    const int chunk = per < 32 ? 32 : per > kWalkChunk ? kWalkChunk : int(per);
     int first = 0;  // global number of the level's first chunk
     for (int l = 0; l < lv.n; ++l) {
         const LevelView& L = lv.l[l];
         const int E = lv.cnt[l].E;
         const int W = L.W, H = L.H, WW = L.WW;
-        const int nch = (2 * E + kWalkChunk - 1) / kWalkChunk;
+        const int nch = (2 * E + chunk - 1) / chunk;
         int c = (gw - first % NW + NW) % NW;
         first += nch;
         for (; c < nch; c += NW) {
-            const int t0 = c * kWalkChunk, t1 = min(2 * E, t0 + kWalkChunk);
+            const int t0 = c * chunk, t1 = min(2 * E, t0 + chunk);
             const int p0 = t0 >> 1, np = (t1 - t0) >> 1;
             // the chunk's points, and |dmin / dmaj| per point (the same for
             // both directions and before and after the re-orientation: the
