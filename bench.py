@@ -408,7 +408,7 @@ def run_b200(args, rank, world, local):
     stages_single["host_candidates"] = {"ms": round(statistics.median(host_ms), 4), "where": "host CPU (C++), includes the "
                                  "edge-point download"}
     stages_single["download"] = {"ms": round(statistics.median(dl_ms), 4), "where": "D2H of the edge-point collections"}
-    stages_single["host_outer_point_sort"] = {"ms": round(statistics.median(cut_ms), 4), "where": "host CPU (C++): outer points sorted by angle; cut selection then runs on the GPU just before identification"}
+    stages_single["host_cut_setup"] = {"ms": round(statistics.median(cut_ms), 4), "where": "host CPU (C++): outer points and tasks staged for upload; the angular sort, subsampling and cut selection run on the GPU just before identification"}
     # Roofline object for the dominant HBM-class kernel group of the batched
     # image stage (one launch over the step's 16 frames).
     top = max(batch_stage_ms, key=lambda k: batch_stage_ms[k])

@@ -26,7 +26,7 @@ CUDA_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-r
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function", "-ffp-contract=off", "-mpopcnt"]
 # Translation units whose float arithmetic must equal the host restatement's
 # bit for bit: no contraction of a * b + c into a fused multiply-add.
-NO_FMAD = {"loop_one", "grow"}
+NO_FMAD = {"loop_one", "grow", "outer_select"}
 
 
 def _sources():

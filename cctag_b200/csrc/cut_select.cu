@@ -160,7 +160,9 @@ __device__ bool refine_stop(float& x, float& y, float dx, float dy, const uint8_
 
 __global__ void __launch_bounds__(kCutThreads) k_cut_select(const uint8_t* __restrict__ img, int W, int H,
                                                             const CutSelectIn* __restrict__ ins,
-                                                            const DirPoint* __restrict__ pts, IdentTask* tasks,
+                                                            const DirPoint* __restrict__ pts,
+                                                            const int16_t* __restrict__ sel,
+                                                            const int* __restrict__ nsel, IdentTask* tasks,
                                                             int* status, CutSelectParams cp)
 {
     __shared__ float s_x[kCutThreads], s_y[kCutThreads], s_wmax[kCutWarps];
@@ -168,14 +170,19 @@ __global__ void __launch_bounds__(kCutThreads) k_cut_select(const uint8_t* __res
     const CutSelectIn in = ins[blockIdx.x];
     const int i = threadIdx.x;
     IdentTask& T = tasks[blockIdx.x];
-    if (in.count < 5) {  // the host decided TOO_FEW_OUTER_POINTS
-        if (i == 0) T.ncuts = 0;
+    // the outer points sorted by angle and subsampled (k_outer_select)
+    const int count = nsel[blockIdx.x];
+    if (count < 5) {  // identify_step_1's TOO_FEW_OUTER_POINTS
+        if (i == 0) {
+            T.ncuts = 0;
+            status[blockIdx.x] = CCTAGB_TOO_FEW_OUTER_POINTS;
+        }
         return;
     }
     bool ok = false, ref = false;
     float var = 0.f, sx = 0.f, sy = 0.f;
-    if (i < in.count) {
-        const DirPoint op = pts[in.first + i];
+    if (i < count) {
+        const DirPoint op = pts[in.first + sel[size_t(blockIdx.x) * kMaxOuterPoints + i]];
         ok = cut_stats(img, W, H, in.cx, in.cy, op.x, op.y, cp.beginSig, cp.nSamples, &var, nullptr);
         if (ok) {
             // pointOnEllipse with the host's cos / sin of the angle
@@ -236,21 +243,22 @@ __global__ void __launch_bounds__(kCutThreads) k_cut_select(const uint8_t* __res
         T.stop[i][0] = s_x[s_keep[j]];
         T.stop[i][1] = s_y[s_keep[j]];
     }
-    const int nsel = __syncthreads_count(pick);
+    const int nCuts = __syncthreads_count(pick);
     if (i == 0) {
-        T.ncuts = nsel;
-        status[blockIdx.x] = nsel == 0 ? CCTAGB_NO_SELECTED_CUTS : CCTAGB_ID_RELIABLE;
+        T.ncuts = nCuts;
+        status[blockIdx.x] = nCuts == 0 ? CCTAGB_NO_SELECTED_CUTS : CCTAGB_ID_RELIABLE;
     }
 }
 
 void launch_cut_select(const uint8_t* d_img, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
-                       IdentTask* d_tasks, int* d_status, int n, const CutSelectParams& cp, cudaStream_t s)
+                       const int16_t* d_sel, const int* d_nsel, IdentTask* d_tasks, int* d_status, int n,
+                       const CutSelectParams& cp, cudaStream_t s)
 {
     if (n <= 0) return;
     if (cp.nSamples < 2 || cp.nSamples > kMaxSamples) throw Error{CCTAGB_BAD_ARG, "sampleCutLength out of range"};
     if (cp.nRefine < 2 || cp.nRefine > kMaxRefineSamples)
         throw Error{CCTAGB_BAD_ARG, "numSamplesOuterEdgePointsRefinement out of range"};
-    k_cut_select<<<n, kCutThreads, 0, s>>>(d_img, W, H, d_ins, d_pts, d_tasks, d_status, cp);
+    k_cut_select<<<n, kCutThreads, 0, s>>>(d_img, W, H, d_ins, d_pts, d_sel, d_nsel, d_tasks, d_status, cp);
     CCTAGB_CUDA(cudaGetLastError());
 }
 

@@ -52,6 +52,8 @@ Detector::~Detector()
     if (h_cutpts_) cudaFreeHost(h_cutpts_);
     if (d_st1_) cudaFree(d_st1_);
     if (h_st1_) cudaFreeHost(h_st1_);
+    if (d_sel_) cudaFree(d_sel_);
+    if (d_nsel_) cudaFree(d_nsel_);
     if (ev_id0_) cudaEventDestroy(ev_id0_);
     if (ev_id1_) cudaEventDestroy(ev_id1_);
 }
@@ -140,16 +142,22 @@ void Detector::ensure_cut_capacity(int nm, int npts)
         if (h_cutin_) cudaFreeHost(h_cutin_);
         if (d_st1_) cudaFree(d_st1_);
         if (h_st1_) cudaFreeHost(h_st1_);
+        if (d_sel_) cudaFree(d_sel_);
+        if (d_nsel_) cudaFree(d_nsel_);
         d_cutin_ = nullptr;
         h_cutin_ = nullptr;
         d_st1_ = nullptr;
         h_st1_ = nullptr;
+        d_sel_ = nullptr;
+        d_nsel_ = nullptr;
         cut_cap_ = 0;
         const int cap = std::max(nm, 256);
         CCTAGB_CUDA(cudaMalloc(&d_cutin_, sizeof(CutSelectIn) * cap));
         CCTAGB_CUDA(cudaMallocHost(&h_cutin_, sizeof(CutSelectIn) * cap));
         CCTAGB_CUDA(cudaMalloc(&d_st1_, sizeof(int) * cap));
         CCTAGB_CUDA(cudaMallocHost(&h_st1_, sizeof(int) * cap));
+        CCTAGB_CUDA(cudaMalloc(&d_sel_, sizeof(int16_t) * kMaxOuterPoints * size_t(cap)));
+        CCTAGB_CUDA(cudaMalloc(&d_nsel_, sizeof(int) * cap));
         cut_cap_ = cap;
     }
     if (npts > pts_cap_) {
@@ -172,13 +180,14 @@ void Detector::select_and_identify(int nm, int npts, int w, int h)
     CCTAGB_CUDA(cudaMemcpyAsync(d_cutin_, h_cutin_, sizeof(CutSelectIn) * nm, cudaMemcpyHostToDevice, s));
     CCTAGB_CUDA(cudaMemcpyAsync(d_cutpts_, h_cutpts_, sizeof(DirPoint) * npts, cudaMemcpyHostToDevice, s));
     CCTAGB_CUDA(cudaMemcpyAsync(d_tasks_, h_tasks_, sizeof(IdentTask) * nm, cudaMemcpyHostToDevice, s));
-    CCTAGB_CUDA(cudaMemcpyAsync(d_st1_, h_st1_, sizeof(int) * nm, cudaMemcpyHostToDevice, s));
     CutSelectParams cp{};
     cp.beginSig = begin_signal(params_.nCrowns);
     cp.nSamples = std::min(params_.sampleCutLength, kMaxSamples);
     cp.nRefine = params_.numSamplesOuterEdgePointsRefinement;
     cp.maxSelect = std::min(params_.numCutsInIdentStep, kMaxCuts);
-    launch_cut_select(pipe_.level0_src(), w, h, d_cutin_, d_cutpts_, d_tasks_, d_st1_, nm, cp, s);
+    cp.nOuter = params_.nSamplesOuterEllipse;
+    launch_outer_select(d_cutin_, d_cutpts_, cp.nOuter, d_sel_, d_nsel_, nm, s);
+    launch_cut_select(pipe_.level0_src(), w, h, d_cutin_, d_cutpts_, d_sel_, d_nsel_, d_tasks_, d_st1_, nm, cp, s);
     CCTAGB_CUDA(cudaEventRecord(ev_id0_, s));
     launch_identify(pipe_.level0_src(), size_t(w), d_tasks_, d_res_, nm, d_bank_inv_,
                     ident_params(params_.refineMode), s);
@@ -187,9 +196,8 @@ void Detector::select_and_identify(int nm, int npts, int w, int h)
     CCTAGB_CUDA(cudaMemcpyAsync(h_st1_, d_st1_, sizeof(int) * nm, cudaMemcpyDeviceToHost, s));
     CCTAGB_CUDA(cudaMemcpyAsync(h_tasks_, d_tasks_, sizeof(IdentTask) * nm, cudaMemcpyDeviceToHost, s));
     pipe_.host_wait(s);
-    pipe_.add_io((long long)(sizeof(CutSelectIn) + sizeof(IdentTask) + sizeof(int)) * nm +
-                     (long long)sizeof(DirPoint) * npts,
-                 (long long)(sizeof(IdentResult) + sizeof(int) + sizeof(IdentTask)) * nm, 2);
+    pipe_.add_io((long long)(sizeof(CutSelectIn) + sizeof(IdentTask)) * nm + (long long)sizeof(DirPoint) * npts,
+                 (long long)(sizeof(IdentResult) + sizeof(int) + sizeof(IdentTask)) * nm, 3);
 }
 
 namespace {
@@ -468,27 +476,37 @@ void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w
     }
     const auto t2 = clk::now();
 
-    // Identification: the outer points sorted by angle on the host, then cut
-    // selection and identification on the GPU, on the level-0 frame there.
+    // Identification: the outer points sorted by angle, subsampled, cut
+    // selection and identification on the GPU, on the level-0 frame there (a
+    // marker with more outer points than the sort kernel holds is sorted and
+    // subsampled here).
     float ms_ident = 0.f, ms_cut = 0.f;
     if (params_.doIdentification && !markers.empty()) {
         const int nm = int(markers.size());
         const auto tc0 = clk::now();
-        std::vector<std::vector<DirPoint>> outer(markers.size());
-        pool_->parallel_for(nm, [&](int i) {
-            outer[size_t(i)] = sorted_outer_points(markers[size_t(i)].rescaled, markers[size_t(i)].rescaled_points,
-                                                   size_t(params_.nSamplesOuterEllipse));
+        if (params_.nSamplesOuterEllipse < 0 || params_.nSamplesOuterEllipse > kMaxOuterPoints)
+            throw Error{CCTAGB_BAD_ARG, "nSamplesOuterEllipse above " + std::to_string(kMaxOuterPoints)};
+        std::vector<std::vector<DirPoint>> presorted(markers.size());
+        std::vector<int> big;
+        for (int i = 0; i < nm; ++i)
+            if (markers[size_t(i)].rescaled_points.size() > size_t(kCutSortCap)) big.push_back(i);
+        pool_->parallel_for(int(big.size()), [&](int k) {
+            const MarkerCand& m = markers[size_t(big[size_t(k)])];
+            presorted[size_t(big[size_t(k)])] =
+                sorted_outer_points(m.rescaled, m.rescaled_points, size_t(params_.nSamplesOuterEllipse));
         });
+        auto points_of = [&](int i) -> const std::vector<DirPoint>& {
+            const MarkerCand& m = markers[size_t(i)];
+            return m.rescaled_points.size() > size_t(kCutSortCap) ? presorted[size_t(i)] : m.rescaled_points;
+        };
         int npts = 0;
-        for (const auto& o : outer) npts += int(o.size());
+        for (int i = 0; i < nm; ++i) npts += int(points_of(i).size());
         ensure_cut_capacity(nm, npts);
         int first = 0;
         for (int i = 0; i < nm; ++i) {
             const MarkerCand& m = markers[size_t(i)];
             const geo::Ellipse& e = m.rescaled;
-            const auto& o = outer[size_t(i)];
-            if (o.size() > size_t(kMaxOuterPoints))
-                throw Error{CCTAGB_BAD_ARG, "nSamplesOuterEllipse above " + std::to_string(kMaxOuterPoints)};
+            const auto& o = points_of(i);
             CutSelectIn& ci = h_cutin_[i];
             ci.cx = e.cx;
             ci.cy = e.cy;
@@ -499,6 +517,7 @@ void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w
             ci.scale = m.scale;
             ci.first = first;
             ci.count = int(o.size());
+            ci.presorted = m.rescaled_points.size() > size_t(kCutSortCap) ? 1 : 0;
             std::copy(o.begin(), o.end(), h_cutpts_ + first);
             first += int(o.size());
             IdentTask& t = h_tasks_[i];
@@ -516,7 +535,6 @@ void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w
             t.roi[1] = 0;
             t.roi[2] = w;
             t.roi[3] = h;
-            h_st1_[i] = o.size() < 5 ? CCTAGB_TOO_FEW_OUTER_POINTS : CCTAGB_ID_RELIABLE;
         }
         ms_cut = std::chrono::duration<float, std::milli>(clk::now() - tc0).count();
         select_and_identify(nm, npts, w, h);

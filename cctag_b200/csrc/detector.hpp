@@ -82,6 +82,8 @@ private:
     DirPoint* d_cutpts_ = nullptr;               // sorted outer points of all markers
     DirPoint* h_cutpts_ = nullptr;
     int* d_st1_ = nullptr;                       // cut selection status per marker
+    int16_t* d_sel_ = nullptr;                   // per marker: its selected outer points (k_outer_select)
+    int* d_nsel_ = nullptr;
     int* h_st1_ = nullptr;
     int cut_cap_ = 0, pts_cap_ = 0;
     float* d_bank_inv_ = nullptr;                // kMaxBankIds x kMaxBankRatios

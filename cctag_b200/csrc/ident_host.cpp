@@ -12,7 +12,8 @@ std::vector<DirPoint> sorted_outer_points(const geo::Ellipse& e, const std::vect
 {
     std::vector<std::pair<float, size_t>> ang;
     ang.reserve(pts.size());
-    for (size_t i = 0; i < pts.size(); ++i) ang.emplace_back(std::atan2(pts[i].y - e.cy, pts[i].x - e.cx), i);
+    // the correctly rounded float atan2 (pmath), as the GPU's sort
+    for (size_t i = 0; i < pts.size(); ++i) ang.emplace_back(pm::atan2f_(pts[i].y - e.cy, pts[i].x - e.cx), i);
     std::sort(ang.begin(), ang.end());
     const size_t nOuter = std::min(requested, pts.size());
     // With one point the reference's step is a division by zero and the

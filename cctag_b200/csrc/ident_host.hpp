@@ -38,12 +38,16 @@ constexpr int kMaxOuterPoints = 256;    // outer points per marker (nSamplesOute
 constexpr int kMaxRefineSamples = 64;   // numSamplesOuterEdgePointsRefinement
 
 // Cut selection of one marker on the GPU (k_cut_select): its level-0 outer
-// ellipse and the outer points the host sorted by angle.
+// ellipse and its outer points, which the kernel sorts by angle and
+// subsamples (getSortedOuterPoints) unless the host already did
+// (`presorted`: more points than the kernel sorts in shared memory).
+constexpr int kCutSortCap = 4096;
 struct CutSelectIn {
     float cx, cy, a, b;     // the ellipse (cuts start at its center)
     float cosA, sinA;       // cos / sin of its angle, computed on the host
     float scale;            // the marker's pyramid scale (refinement length)
     int first, count;       // its outer points in the point array
+    int presorted;          // 1: the points are the sorted selection
 };
 
 struct CutSelectParams {
@@ -51,6 +55,7 @@ struct CutSelectParams {
     int nSamples;           // sampleCutLength
     int nRefine;            // numSamplesOuterEdgePointsRefinement
     int maxSelect;          // min(numCutsInIdentStep, kMaxCuts)
+    int nOuter;             // nSamplesOuterEllipse (<= kMaxOuterPoints)
 };
 
 // geometry/Ellipse.cpp:259-300: up to `requested` outer points, sorted by the
@@ -58,10 +63,16 @@ struct CutSelectParams {
 std::vector<DirPoint> sorted_outer_points(const geo::Ellipse& e, const std::vector<DirPoint>& pts, size_t requested);
 
 // Writes stop[] and ncuts of tasks[i] (the rest filled by the host) and
-// status[i] (CCTAGB_ID_RELIABLE, _NO_COLLECTED_CUTS or _NO_SELECTED_CUTS;
-// left alone for markers with fewer than 5 outer points).
+// status[i] (CCTAGB_ID_RELIABLE, _TOO_FEW_OUTER_POINTS, _NO_COLLECTED_CUTS or
+// _NO_SELECTED_CUTS).
 void launch_cut_select(const uint8_t* d_img, int W, int H, const CutSelectIn* d_ins, const DirPoint* d_pts,
-                       IdentTask* d_tasks, int* d_status, int n, const CutSelectParams& cp, cudaStream_t s);
+                       const int16_t* d_sel, const int* d_nsel, IdentTask* d_tasks, int* d_status, int n,
+                       const CutSelectParams& cp, cudaStream_t s);
+// The outer points of each marker sorted by angle and subsampled to at most
+// nOuterReq (k_outer_select): sel[i * kMaxOuterPoints + k] is the k-th
+// selected point of marker i (relative to its first), nsel[i] their number.
+void launch_outer_select(const CutSelectIn* d_ins, const DirPoint* d_pts, int nOuterReq, int16_t* d_sel, int* d_nsel,
+                         int n, cudaStream_t s);
 
 // Signal start along the cut as a fraction of the unit radius.
 float begin_signal(int nCrowns);

@@ -162,7 +162,7 @@ typedef struct cctagb_stats {
     long long d2h_bytes;       /* device->host bytes copied by the call */
     int kernel_launches;       /* kernels launched by the call         */
     float ms_download;         /* host wall time of the edge-point downloads */
-    float ms_cut_selection;    /* host wall time of the cut-selection set-up (outer points sorted by angle, tasks filled); the cut selection itself then runs on the GPU, just before identification */
+    float ms_cut_selection;    /* host wall time of the cut-selection set-up (outer points and tasks staged); the angular sort, subsampling and cut selection then run on the GPU, just before identification */
     int grown_gpu;             /* candidates whose ellipse growing ran on the GPU */
     int grown_host;            /* ... on the host (gpuEllipseGrowing 0, or too many outer points for the kernel) */
 } cctagb_stats;
