@@ -447,6 +447,7 @@ struct Candidate {
     std::vector<int> outer;
     Ellipse outerEllipse;
     std::vector<int> filtered;
+    std::vector<int> chains;  // per filtered point, its numCircles - 1 link hops (LoopTwoIn::chain)
     int score = 0;
     size_t nLabel = 0;
     float averageReceivedVote = 0.f;
@@ -531,10 +532,13 @@ bool in_ellipse(const Ellipse& e, float x, float y)
     return s1 * s2 > 0;
 }
 
-// EllipseGrowing.cpp:63-178 addCandidateFlowtoCCTag
-bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vector<int>& outer, const Ellipse& oe,
-                        std::vector<std::vector<DirPoint>>& pts, size_t numCircles)
+// EllipseGrowing.cpp:63-178 addCandidateFlowtoCCTag.  The links walked from
+// fc[k] are chains[k * (numCircles - 1) + j - 1].
+bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vector<int>& chains,
+                        const std::vector<int>& outer, const Ellipse& oe, std::vector<std::vector<DirPoint>>& pts,
+                        size_t numCircles)
 {
+    if (chains.size() != fc.size() * (numCircles - 1)) throw std::logic_error("link chains do not match the points");
     pts.resize(numCircles);
     for (int e : outer) pts.back().push_back({float(es.x(e)), float(es.y(e)), es.dx(e), es.dy(e)});
     // The reference marks visited points in a shared per-point flag and clears
@@ -559,14 +563,16 @@ bool add_candidate_flow(EdgeSet& es, const std::vector<int>& fc, const std::vect
     const float qc1 = Q.m[1][0] * oe.cx + Q.m[1][1] * oe.cy + Q.m[1][2];
     const float qc2 = Q.m[2][0] * oe.cx + Q.m[2][1] * oe.cy + Q.m[2][2];
     size_t nGradientOut = 0, nAdded = 0;
-    for (int p0 : fc) {
+    for (size_t k = 0; k < fc.size(); ++k) {
+        const int p0 = fc[k];
+        const int* chain = chains.data() + k * (numCircles - 1);
         int dir = -1;
         int p = p0;
         const float ox = float(es.x(p0)), oy = float(es.y(p0));
         const float a = ox - oe.cx, b = oy - oe.cy;
         const float line[3] = {a, b, -a * oe.cx - b * oe.cy};
         for (size_t j = 1; j < numCircles; ++j) {
-            p = dir == -1 ? es.before[p] : es.after[p];
+            p = chain[j - 1];  // dir == -1 ? before[p] : after[p]
             if (p < 0) {
                 throw std::out_of_range("EdgePointCollection: missing link");
             }
@@ -667,7 +673,7 @@ bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& ou
     for (int q : merged) d.push_back(geo::dist_point_ellipse(fitted.Q, float(es.x(q)), float(es.y(q))));
     const float SmFinal = geo::median_ref(d);
     if (!(SmFinal < thrMedian)) return false;
-    if (!add_candidate_flow(es, another.filtered, aout, fitted, pts, numCircles)) return false;
+    if (!add_candidate_flow(es, another.filtered, another.chains, aout, fitted, pts, numCircles)) return false;
     outer = merged;
     outerEllipse = fitted;
     return true;
@@ -715,7 +721,7 @@ void loop_two_iteration(EdgeSet& es, const std::vector<Candidate>& loop2, size_t
         float quality = quality_of(outer.size(), oe);
         if (p.searchForAnotherSegment && quality > 0.25 && quality < 0.7)
             flow_component_assembling(es, quality, ci, loop2, oe, outer, pts, p, rng);
-        if (!add_candidate_flow(es, c.filtered, c.outer, oe, pts, size_t(p.nCrowns) * 2)) return;
+        if (!add_candidate_flow(es, c.filtered, c.chains, c.outer, oe, pts, size_t(p.nCrowns) * 2)) return;
         const Ellipse rescale = Ellipse::from_params(oe.cx, oe.cy, oe.a * scale, oe.b * scale, oe.angle);
         const float realSize = quality * float(geo::rasterize_perimeter(rescale));
         if ((quality <= 0.35 && realSize >= 300.0f) ||
@@ -830,7 +836,20 @@ void phases_a_b(std::vector<LevelJob>& jobs, const cctagb_params& p, const Paral
     pf(int(tasks.size()), [&](int t) {
         const int l = tasks[t].first, i = tasks[t].second;
         geo::Pcg32 rng = candidate_rng(jobs[l].level, size_t(i), 0);
-        st[l].keep[i] = flow_component_filter(st[l].loop1[i], *jobs[l].es, p, rng) ? 1 : 0;
+        Candidate& c = st[l].loop1[i];
+        st[l].keep[i] = flow_component_filter(c, *jobs[l].es, p, rng) ? 1 : 0;
+        // the link chains of the filtered points, from the host's links
+        const int len = 2 * p.nCrowns - 1;
+        const EdgeSet& es = *jobs[l].es;
+        c.chains.clear();
+        if (st[l].keep[i])
+            for (int p0 : c.filtered) {
+                int q = p0;
+                for (int j = 0; j < len; ++j) {
+                    q = q < 0 ? -1 : (j & 1) ? es.after[q] : es.before[q];
+                    c.chains.push_back(q);
+                }
+            }
     });
 }
 
@@ -851,9 +870,13 @@ void link_and_filter(std::vector<LevelJob>& jobs, const cctagb_params& p, const 
             o.flow.push_back(c.flow);
             o.score.push_back(c.score);
             o.keep.push_back(st[l].keep[i]);
-            if (st[l].keep[i]) o.flt.insert(o.flt.end(), c.filtered.begin(), c.filtered.end());
+            if (st[l].keep[i]) {
+                o.flt.insert(o.flt.end(), c.filtered.begin(), c.filtered.end());
+                o.chain.insert(o.chain.end(), c.chains.begin(), c.chains.end());
+            }
             o.foff.push_back(int32_t(o.flt.size()));
         }
+        o.chainLen = 2 * p.nCrowns - 1;
     }
 }
 
@@ -878,6 +901,10 @@ void detect_from_edges(std::vector<LevelJob>& jobs, const cctagb_params& p, cons
                 c.flow = g.flow[i];
                 c.score = g.score[i];
                 c.filtered.assign(g.flt.begin() + g.foff[i], g.flt.begin() + g.foff[i + 1]);
+                if (g.chainLen != 2 * p.nCrowns - 1 || g.chain.size() != g.flt.size() * size_t(g.chainLen))
+                    throw std::runtime_error("loop-two inputs without their link chains");
+                c.chains.assign(g.chain.begin() + size_t(g.foff[i]) * g.chainLen,
+                                g.chain.begin() + size_t(g.foff[i + 1]) * g.chainLen);
             }
         }
     }

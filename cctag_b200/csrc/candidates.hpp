@@ -100,6 +100,11 @@ struct LoopTwoIn {
     std::vector<uint8_t> keep;
     std::vector<int32_t> foff;  // candidate i: flt[foff[i], foff[i + 1]) (empty unless kept)
     std::vector<int32_t> flt;
+    // flt[k]'s link chain: chain[k * chainLen + j], the point reached after
+    // j + 1 alternating before / after links (before first), -1 past a
+    // missing link; what addCandidateFlowtoCCTag walks (EllipseGrowing.cpp:63-178)
+    std::vector<int32_t> chain;
+    int chainLen = 0;
 };
 
 // Loop 1 and the outlier removal of loop 2 on the host, per level.

@@ -1011,6 +1011,30 @@ __global__ void __launch_bounds__(256) k_refit_pack(const int32_t* hullAll, int 
 }
 
 // Kept candidates' filtered children, in candidate order, into one array.
+// The link chains of the packed filtered children: point i of level l (the
+// levels' entries are contiguous, from first[l]) walks len alternating
+// before / after links, as addCandidateFlowtoCCTag does (EllipseGrowing.cpp:
+// 63-178).
+struct ChainLevels {
+    const int32_t* before[kMaxLevels];
+    const int32_t* after[kMaxLevels];
+    int first[kMaxLevels + 1];
+};
+
+__global__ void __launch_bounds__(256) k_chains(const int32_t* __restrict__ packed, int total, int len,
+                                                ChainLevels cl, int nl, int32_t* __restrict__ chain)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    int l = 0;
+    while (l < nl - 1 && i >= cl.first[l + 1]) ++l;
+    int q = packed[i];
+    for (int j = 0; j < len; ++j) {
+        q = q < 0 ? -1 : (j & 1) ? cl.after[l][q] : cl.before[l][q];
+        chain[size_t(i) * len + j] = q;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_pack(LoopOneArgs a, int32_t* packed)
 {
     const int b = blockIdx.x;
@@ -1122,6 +1146,8 @@ LoopOneGpu::~LoopOneGpu()
     if (h_meta_) cudaFreeHost(h_meta_);
     if (h_cflow_) cudaFreeHost(h_cflow_);
     if (h_flt_) cudaFreeHost(h_flt_);
+    if (d_chain_) cudaFree(d_chain_);
+    if (h_chain_) cudaFreeHost(h_chain_);
 }
 
 void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const std::vector<int32_t>*>& seeds,
@@ -1143,6 +1169,8 @@ void LoopOneGpu::launch(const Levels& lv, const int* E, const std::vector<const 
         L.voff = v.voff;
         L.vlist = v.vlist;
         L.bitidx = v.bitidx;
+        L.before = v.before;
+        L.after = v.after;
         L.flow = v.flow;
         L.level = l;
         L.slot0 = l * maxSlotsPerLevel_;
@@ -1206,6 +1234,7 @@ void LoopOneGpu::run_kernels(cudaStream_t s)
 
 void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
 {
+    chainLaunches_ = 0;
     waiter_.wait(s);
     const int32_t* made = h_meta_ + size_t(nl_) * n2max_ * 4;
     // a candidate with more voters than the room: more room, same kernels
@@ -1234,16 +1263,50 @@ void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
         CCTAGB_CUDA(cudaMallocHost(&h_flt_, sizeof(int32_t) * total));
         h_flt_cap_ = total;
     }
+    // the link chains of the filtered children (the host's flow assembling
+    // walks them; the links themselves stay on the device)
+    const int len = 2 * p_.nCrowns - 1;
+    ChainLevels cl{};
+    {
+        size_t off = 0;
+        for (int l = 0; l < nl_; ++l) {
+            cl.before[l] = args_.lv[l].before;
+            cl.after[l] = args_.lv[l].after;
+            cl.first[l] = int(off);
+            const int n2 = std::min(made[l], n2max_);
+            for (int r = 0; r < n2; ++r) {
+                const int32_t* m = h_meta_ + (size_t(l) * n2max_ + r) * 4;
+                if (m[2]) off += size_t(m[3]);
+            }
+        }
+        cl.first[nl_] = int(off);
+    }
+    if (total * len > chain_cap_) {
+        if (d_chain_) cudaFree(d_chain_);
+        if (h_chain_) cudaFreeHost(h_chain_);
+        d_chain_ = nullptr;
+        h_chain_ = nullptr;
+        chain_cap_ = 0;
+        const size_t cap = std::max(total * len, size_t(65536));
+        CCTAGB_CUDA(cudaMalloc(&d_chain_, sizeof(int32_t) * cap));
+        CCTAGB_CUDA(cudaMallocHost(&h_chain_, sizeof(int32_t) * cap));
+        chain_cap_ = cap;
+    }
     if (total) {
+        k_chains<<<int((total + 255) / 256), 256, 0, s>>>(d_packed_, int(total), len, cl, nl_, d_chain_);
+        CCTAGB_CUDA(cudaGetLastError());
+        ++chainLaunches_;
         CCTAGB_CUDA(cudaMemcpyAsync(h_flt_, d_packed_, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, s));
+        CCTAGB_CUDA(cudaMemcpyAsync(h_chain_, d_chain_, sizeof(int32_t) * total * len, cudaMemcpyDeviceToHost, s));
         waiter_.wait(s);
     }
-    d2h_ += 4LL * total;
+    d2h_ += 4LL * total * (1 + len);
     out.assign(size_t(nl_), {});
     size_t off = 0;
     for (int l = 0; l < nl_; ++l) {
         LoopTwoIn& o = out[size_t(l)];
         const int n2 = std::min(made[l], n2max_);
+        o.chainLen = len;
         o.foff.push_back(0);
         for (int r = 0; r < n2; ++r) {
             const int32_t* m = h_meta_ + (size_t(l) * n2max_ + r) * 4;
@@ -1253,6 +1316,7 @@ void LoopOneGpu::collect(cudaStream_t s, std::vector<LoopTwoIn>& out)
             o.keep.push_back(uint8_t(m[2]));
             if (m[2]) {
                 o.flt.insert(o.flt.end(), h_flt_ + off, h_flt_ + off + m[3]);
+                o.chain.insert(o.chain.end(), h_chain_ + off * len, h_chain_ + (off + m[3]) * len);
                 off += size_t(m[3]);
             }
             o.foff.push_back(int32_t(o.flt.size()));

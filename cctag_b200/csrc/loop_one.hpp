@@ -29,6 +29,8 @@ struct LoopOneLevel {
     const int32_t* voff;
     const int32_t* vlist;
     const uint2* bitidx;     // WW*H: (edge bitmap word, edge index of its first set bit)
+    const int32_t* before;  // E: the walks' links
+    const int32_t* after;
     const int32_t* order;   // seeds in processing order, nProc of them
     int nProc, slot0;       // seed slots [slot0, slot0 + nProc)
     int4* rec;              // E point records (3 int4 each): xy, angle, voters, seed slot; 8 neighbours
@@ -95,7 +97,7 @@ public:
     // (fewer than 5 when the marker keeps its coarse-level ellipse).
     void refit(const Levels& lv, const std::vector<RefitTask>& tasks, cudaStream_t s,
                std::vector<std::vector<int32_t>>& filtered);
-    int launches() const { return 6; }
+    int launches() const { return 6 + chainLaunches_; }
     int refit_launches() const { return 2; }
     long long h2d_bytes() const { return h2d_; }
     long long d2h_bytes() const { return d2h_; }
@@ -132,6 +134,10 @@ private:
     float* h_cflow_ = nullptr;     // pinned: seeds' flow lengths
     int32_t* h_flt_ = nullptr;     // pinned: filtered children, all candidates
     size_t h_flt_cap_ = 0;
+    int32_t* d_chain_ = nullptr;   // link chains of the filtered children (k_chains)
+    int32_t* h_chain_ = nullptr;   // pinned
+    size_t chain_cap_ = 0;
+    int chainLaunches_ = 0;        // k_chains launches of the last collect
     std::vector<void*> allocs_;
     long long h2d_ = 0, d2h_ = 0;
 };

@@ -532,8 +532,10 @@ void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
 {
     out.resize(lv_.n);
     // One compacting launch and two copies: the seeds of every level (index,
-    // key, votes) on the pipeline stream, then the edge points' positions,
-    // gradients and links on the copy stream.
+    // key, votes) on the pipeline stream, then the edge points' positions and
+    // gradients on the copy stream.  The links stay on the device: the host
+    // reads them only as the link chains of the loop-two candidates' points,
+    // which loop one computes and downloads (LoopOneGpu::collect).
     PackSegs ps{};
     long long off = 0;
     auto seg = [&](const int32_t* src, long long n) {
@@ -555,8 +557,6 @@ void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
         const long long E = h_cnt_[l].E;
         seg(v.exy, E);
         seg(v.grad, E);
-        seg(v.before, E);
-        seg(v.after, E);
     }
     ps.off[ps.n] = off;
     if (off > pack_words_) throw Error{CCTAGB_INTERNAL, "download staging too small"};
@@ -574,11 +574,11 @@ void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
         k.sidx = h_pack_ + ps.off[3 * l];
         k.skey = h_pack_ + ps.off[3 * l + 1];
         k.svotes = h_pack_ + ps.off[3 * l + 2];
-        const int p = 3 * lv_.n + 4 * l;
+        const int p = 3 * lv_.n + 2 * l;
         k.exy = h_pack_ + ps.off[p];
         k.grad = h_pack_ + ps.off[p + 1];
-        k.before = h_pack_ + ps.off[p + 2];
-        k.after = h_pack_ + ps.off[p + 3];
+        k.before = nullptr;
+        k.after = nullptr;
     }
     waiter_.wait(stream_);
     for (int l = 0; l < lv_.n; ++l) {
