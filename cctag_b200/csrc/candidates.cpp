@@ -23,21 +23,23 @@ using geo::Pt;
 
 void EdgeSet::index_points()
 {
-    const size_t nw = (size_t(W) * size_t(H) + 63) / 64;
-    ebits.assign(nw, 0);
-    erank.resize(nw);
+    WW = (W + 31) / 32;
+    const size_t nw = size_t(WW) * size_t(H);
+    own_bidx.assign(nw, Word{0u, 0});
     long long last = -1;
     for (int i = 0; i < E; ++i) {
-        const long long pos = (long long)(exy[i] >> 16) * W + (exy[i] & 0xffff);
-        if (pos <= last || pos >= (long long)W * H) throw std::runtime_error("edge points not in raster order");
+        const int x = exy[i] & 0xffff, y = exy[i] >> 16;
+        const long long pos = (long long)y * W + x;
+        if (pos <= last || x >= W || y >= H) throw std::runtime_error("edge points not in raster order");
         last = pos;
-        ebits[size_t(pos) >> 6] |= uint64_t(1) << (pos & 63);
+        own_bidx[size_t(y) * WW + size_t(x >> 5)].bits |= 1u << (x & 31);
     }
     int32_t r = 0;
     for (size_t k = 0; k < nw; ++k) {
-        erank[k] = r;
-        r += int32_t(__builtin_popcountll(ebits[k]));
+        own_bidx[k].first = r;
+        r += int32_t(__builtin_popcount(own_bidx[k].bits));
     }
+    bidx = own_bidx.data();
 }
 
 void EdgeSet::reset_state()

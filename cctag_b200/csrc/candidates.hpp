@@ -25,11 +25,18 @@ struct EdgeSet {
     const int32_t* vlist = nullptr;
     const float* flow = nullptr;
     // Point index of a pixel: the points are in raster order, so a pixel's
-    // index is its rank among the edge pixels.  ebits holds the edge pixels
-    // (bit x + y W), erank the number of points before each 64-bit word: 1/16
-    // of the bytes of a dense W x H index map, so lookups stay in cache.
-    std::vector<uint64_t> ebits;
-    std::vector<int32_t> erank;
+    // index is its rank among the edge pixels.  bidx holds, per 32-pixel word
+    // of each row (WW words per row), the word's edge pixels and the index of
+    // its first one (the GPU's word + first-index plane, downloaded with the
+    // points, or built by index_points): 1/16 of the bytes of a dense W x H
+    // index map, so lookups stay in cache.
+    struct Word {
+        uint32_t bits;
+        int32_t first;
+    };
+    const Word* bidx = nullptr;
+    int WW = 0;
+    std::vector<Word> own_bidx;  // index_points' copy
 
     std::vector<uint8_t> processed_in;  // loop 1 on the host
     std::vector<int32_t> n_segment_out;
@@ -48,11 +55,13 @@ struct EdgeSet {
     int voters(int i) const { return voff[i + 1] - voff[i]; }
     int at(int px, int py) const
     {
-        const size_t pos = size_t(py) * size_t(W) + size_t(px);
-        const uint64_t w = ebits[pos >> 6], bit = uint64_t(1) << (pos & 63);
-        return (w & bit) ? erank[pos >> 6] + __builtin_popcountll(w & (bit - 1)) : -1;
+        const Word w = bidx[size_t(py) * size_t(WW) + size_t(px >> 5)];
+        const uint32_t bit = 1u << (px & 31);
+        if (!(w.bits & bit)) return -1;
+        const int i = w.first + __builtin_popcount(w.bits & (bit - 1u));
+        return i < E ? i : -1;
     }
-    // Builds ebits / erank from exy[0, E); throws unless the points are in
+    // Builds bidx from exy[0, E) (own_bidx); throws unless the points are in
     // strict raster order.
     void index_points();
     void reset_state();

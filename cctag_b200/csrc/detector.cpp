@@ -392,7 +392,12 @@ void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w
         e.voff = L.voff;
         e.vlist = L.vlist;
         e.flow = L.flow;
-        e.index_points();
+        if (L.bidx) {  // the GPU's word + first-index plane, downloaded with the points
+            e.bidx = reinterpret_cast<const EdgeSet::Word*>(L.bidx);
+            e.WW = L.WW;
+        } else {
+            e.index_points();
+        }
         e.reset_state();
     };
     pool_->parallel_for(nl, fill_level);

@@ -157,9 +157,11 @@ void Pipeline::alloc(int max_w, int max_h)
         h /= 2;
         if (w < 1 || h < 1) throw Error{CCTAGB_BAD_ARG, "frame too small for the number of pyramid levels"};
     }
-    // Compact download staging: seeds and edge points of every level.
+    // Compact download staging: seeds, edge points and word index planes of
+    // every level.
     pack_words_ = 0;
-    for (int l = 0; l < nl; ++l) pack_words_ += 3LL * la_[l].seedcap + 4LL * la_[l].cap;
+    for (int l = 0, lw = max_w, lh = max_h; l < nl; ++l, lw /= 2, lh /= 2)
+        pack_words_ += 3LL * la_[l].seedcap + 2LL * la_[l].cap + 2LL * ((lw + 31) / 32) * lh;
     d_pack_ = dev_alloc<int32_t>(allocs_, size_t(pack_words_));
     CCTAGB_CUDA(cudaMallocHost(&h_pack_, size_t(pack_words_) * 4));
     host_allocs_.push_back(h_pack_);
@@ -557,6 +559,7 @@ void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
         const long long E = h_cnt_[l].E;
         seg(v.exy, E);
         seg(v.grad, E);
+        seg(reinterpret_cast<const int32_t*>(v.bitidx), 2LL * v.WW * v.H);
     }
     ps.off[ps.n] = off;
     if (off > pack_words_) throw Error{CCTAGB_INTERNAL, "download staging too small"};
@@ -574,9 +577,10 @@ void Pipeline::download_seeds_then_points(std::vector<HostLevel>& out)
         k.sidx = h_pack_ + ps.off[3 * l];
         k.skey = h_pack_ + ps.off[3 * l + 1];
         k.svotes = h_pack_ + ps.off[3 * l + 2];
-        const int p = 3 * lv_.n + 2 * l;
+        const int p = 3 * lv_.n + 3 * l;
         k.exy = h_pack_ + ps.off[p];
         k.grad = h_pack_ + ps.off[p + 1];
+        k.bidx = h_pack_ + ps.off[p + 2];
         k.before = nullptr;
         k.after = nullptr;
     }
@@ -597,6 +601,8 @@ void Pipeline::wait_points(std::vector<HostLevel>& out)
         out[l].grad = k.grad;
         out[l].before = k.before;
         out[l].after = k.after;
+        out[l].bidx = k.bidx;
+        out[l].WW = lv_.l[l].WW;
     }
 }
 

@@ -24,6 +24,8 @@ struct HostLevel {
     const int32_t* grad = nullptr;
     const int32_t* before = nullptr;
     const int32_t* after = nullptr;
+    const int32_t* bidx = nullptr;   // WW * H (word, first index) pairs, or null
+    int WW = 0;
     const int32_t* voff = nullptr;   // E + 1
     const int32_t* vlist = nullptr;  // V
     const float* flow = nullptr;
@@ -154,7 +156,7 @@ private:
     int32_t* h_pack_ = nullptr;  // pinned
     long long pack_words_ = 0;
     struct Packed {
-        const int32_t *sidx, *skey, *svotes, *exy, *grad, *before, *after;
+        const int32_t *sidx, *skey, *svotes, *exy, *grad, *before, *after, *bidx;
     } pk_[kMaxLevels] = {};
     cudaEvent_t ev_pack_ = nullptr;  // the pack launch, for the copy stream
     Levels lv_{};
