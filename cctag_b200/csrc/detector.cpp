@@ -400,7 +400,9 @@ void Detector::after_image_stage(std::chrono::steady_clock::time_point t0, int w
         }
         e.reset_state();
     };
-    pool_->parallel_for(nl, fill_level);
+    // on this thread: with the GPU's index planes the levels only take
+    // pointers (a pooled task could wait behind other frames' work)
+    for (int l = 0; l < nl; ++l) fill_level(l);
     loop1_->collect(pipe_.stream(), loop2in_);
     pipe_.add_io(loop1_->h2d_bytes(), loop1_->d2h_bytes(), loop1_->launches());
     std::vector<LevelJob> jobs(nl);
