@@ -662,6 +662,7 @@ def run_c3(args, flush, torch, peak, peak_src):
         fr[i].gray, fr[i].w, fr[i].h, fr[i].pitch, fr[i].is_device, fr[i].frame_id = t.data_ptr(), W, H, W, 1, i
         fr[i].out = C.cast(outs[i], C.POINTER(capi.Marker))
         fr[i].cap = cap
+    tune = autotune(det, fr, reps=3)
     for _ in range(args.warmup):
         det._check(det._lib.cctagb_detect_batch(det._h, fr, len(frames)), "detect_batch")
     steps = max(5, min(args.steps, 20))
@@ -706,7 +707,9 @@ def run_c3(args, flush, torch, peak, peak_src):
            "image_stage_ms": round(sum(stage_ms.values()), 4), "stages": stages,
            "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(ach / peak, 4), "peak_source": peak_src},
-           "note": "cctagb_detect_batch of 4 distinct frames per call, frames in device memory"}
+           "autotune": tune,
+           "note": "cctagb_detect_batch of 4 distinct frames per call, frames in device memory; stages of one "
+                   "frame's image stage (single-frame launch)"}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(frames[:2], budget_s=min(args.cpu_budget, 10.0), threads=1)
     return out
