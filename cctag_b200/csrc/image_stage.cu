@@ -731,11 +731,16 @@ __global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
 // two or three steps, a few run the full distance), so a warp does not run
 // one walk per lane to the end of its longest: each lane takes the next walk
 // of the warp's chunk as soon as its current one stops.  One iteration of the
-// loop below is one step of a lane's walk, with the probes the reference makes
-// after that step; the steps and probes of every walk are those of the
-// reference in the same order, so the results do not depend on the schedule.
+// loop below is kWalkAhead steps of a lane's walk, with the probes the
+// reference makes after each step, all loaded before the first is tested; the
+// steps and probes of every walk are those of the reference in the same order
+// (steps past the walk's end are computed and dropped), so the results do not
+// depend on the schedule.
 constexpr int kWalkWarps = 8;
 constexpr int kWalkChunk = 512;  // walks (two per point) a warp takes at once, at most
+// steps a lane takes per iteration (16-frame C2 launch: 1 step 0.71 ms, 2 steps
+// 0.63 ms, 4 steps 0.69 ms, 8 steps 0.92 ms: more lookahead costs occupancy)
+constexpr int kWalkAhead = 2;
 
 __device__ __forceinline__ int sgn_i(int v) { return (v > 0) - (v < 0); }
 
@@ -809,10 +814,23 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                 q += __popc(idle);
                 if (!__any_sync(kAll, act)) break;
                 if (!act) continue;
-                int res = -2;  // -2: the walk goes on
-                if (n >= 2 && n > nmax) {
-                    res = -1;
-                } else {
+                // The next kWalkAhead steps of the walk: its positions do not
+                // depend on what the probes find, so all their probes are
+                // issued before the first is looked at.  kind: 0 a step without
+                // a probe, 1 one probe, 2 a probe and the side probe, 3 the
+                // walk ends here (distSearch), 4 past the end.
+                int kind[kWalkAhead], px[kWalkAhead], py[kWalkAhead], sx[kWalkAhead], sy[kWalkAhead];
+                bool over = false;
+#pragma unroll
+                for (int j = 0; j < kWalkAhead; ++j) {
+                    kind[j] = 4;
+                    px[j] = py[j] = sx[j] = sy[j] = -1;
+                    if (over) continue;
+                    if (n >= 2 && n > nmax) {
+                        kind[j] = 3;
+                        over = true;
+                        continue;
+                    }
                     const float dmaj = ymaj ? dy : dx, dmin = ymaj ? dx : dy;
                     const int smaj = sgn_i(int(dmaj)), smin = sgn_i(int(dmin));
                     e = __fadd_rn(e, a);
@@ -831,19 +849,45 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                             dx = float(d * gdx);
                             dy = float(d * gdy);
                         }
+                        kind[j] = 0;
                     } else {
-                        // -1 outside the level, -2 no edge pixel, else its
-                        // index (-1 past a clamped edge count)
-                        auto probe = [&](int qx, int qy) -> int {
-                            if (qx < 0 || qx >= W || qy < 0 || qy >= H) return -1;
-                            const uint2 v = __ldg(&L.bitidx[size_t(qy) * WW + (qx >> 5)]);
-                            const uint32_t bit = 1u << (qx & 31);
-                            if (!(v.x & bit)) return -2;
-                            const int idx = int(v.y) + __popc(v.x & (bit - 1u));
-                            return idx < E ? idx : -1;
-                        };
-                        res = probe(x, y);
-                        if (res == -2 && n > 2) res = probe(ymaj ? x : x - stpX, ymaj ? y - stpY : y);
+                        kind[j] = n > 2 ? 2 : 1;
+                        px[j] = x;
+                        py[j] = y;
+                        sx[j] = ymaj ? x : x - stpX;
+                        sy[j] = ymaj ? y - stpY : y;
+                    }
+                }
+                uint2 w[kWalkAhead], ws[kWalkAhead];
+#pragma unroll
+                for (int j = 0; j < kWalkAhead; ++j) {
+                    w[j] = ws[j] = make_uint2(0u, 0u);
+                    if (kind[j] == 1 || kind[j] == 2) {
+                        if (px[j] >= 0 && px[j] < W && py[j] >= 0 && py[j] < H)
+                            w[j] = __ldg(&L.bitidx[size_t(py[j]) * WW + (px[j] >> 5)]);
+                        if (kind[j] == 2 && sx[j] >= 0 && sx[j] < W && sy[j] >= 0 && sy[j] < H)
+                            ws[j] = __ldg(&L.bitidx[size_t(sy[j]) * WW + (sx[j] >> 5)]);
+                    }
+                }
+                // the first step, in walk order, that ends the walk: -1
+                // outside the level or at distSearch, else the index of the
+                // edge pixel met (-1 past a clamped edge count)
+                auto found = [&](uint2 v, int qx, int qy) -> int {
+                    if (qx < 0 || qx >= W || qy < 0 || qy >= H) return -1;
+                    const uint32_t bit = 1u << (qx & 31);
+                    if (!(v.x & bit)) return -2;
+                    const int idx = int(v.y) + __popc(v.x & (bit - 1u));
+                    return idx < E ? idx : -1;
+                };
+                int res = -2;  // -2: the walk goes on
+#pragma unroll
+                for (int j = 0; j < kWalkAhead; ++j) {
+                    if (res != -2) continue;
+                    if (kind[j] == 3) {
+                        res = -1;
+                    } else if (kind[j] == 1 || kind[j] == 2) {
+                        res = found(w[j], px[j], py[j]);
+                        if (res == -2 && kind[j] == 2) res = found(ws[j], sx[j], sy[j]);
                     }
                 }
                 if (res != -2) {
@@ -1230,7 +1274,12 @@ void launch_image_stage(const Levels& lv, const VoteParamsDev& vp, cudaStream_t 
     mark(ev, kStPyramid + 1, s);
     launch_edges(lv, vp, s, 1, ev);
     const int G = 148 * 8;
-    k_walk<<<148 * 5, 32 * kWalkWarps, 0, s>>>(lv, vp);  // 5 resident per SM (48 registers, 40 KB)
+    static const int walkBlocks = [] {
+        int per = 0;
+        CCTAGB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_walk, 32 * kWalkWarps, 0));
+        return 148 * (per > 0 ? per : 1);
+    }();
+    k_walk<<<walkBlocks, 32 * kWalkWarps, 0, s>>>(lv, vp);  // the blocks resident at once
     mark(ev, kStWalk + 1, s);
     k_vote<<<G, 256, 0, s>>>(lv, vp);
     mark(ev, kStVote + 1, s);
