@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <deque>
 #include <limits>
 #include <stdexcept>
@@ -198,6 +199,24 @@ bool median_below(const float* v, size_t n, float bound)
     size_t below = 0;
     for (size_t i = 0; i < n; ++i) below += v[i] < bound;
     return below >= n / 2 + 1;
+}
+
+// For 0 <= s1 < sm: the smallest float b >= 0 with s1 + b >= sm (float sum).
+// The sum grows with b, so for any x >= 0, s1 + x < sm exactly when x < b.
+// Binary search over the bit patterns of the non-negative floats, which are
+// ordered as their values.
+float sum_threshold(float s1, float sm)
+{
+    uint32_t lo = 0, hi = 0x7f800000u;  // +0 (s1 + 0 < sm) .. +inf (s1 + inf >= sm)
+    while (hi - lo > 1) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        float x;
+        std::memcpy(&x, &mid, 4);
+        if (s1 + x >= sm) hi = mid; else lo = mid;
+    }
+    float b;
+    std::memcpy(&b, &hi, 4);
+    return b;
 }
 
 // Vote.cpp:414-576 outlierRemoval: LMedS ellipse from random 5-point subsets
@@ -618,7 +637,7 @@ bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& ou
     std::vector<Pt> P(outer.size()), AP(aout.size());
     for (size_t i = 0; i < outer.size(); ++i) P[i] = {float(es.x(outer[i])), float(es.y(outer[i]))};
     for (size_t i = 0; i < aout.size(); ++i) AP[i] = {float(es.x(aout[i])), float(es.y(aout[i]))};
-    std::vector<float> d;
+    std::vector<float> d, d2(AP.size());
     d.reserve(std::max(P.size(), AP.size()));
     for (const Pt& q : P) d.push_back(geo::dist_point_ellipse(outerEllipse.Q, q.x, q.y));
     const float SRef = geo::median_ref(d);
@@ -650,10 +669,20 @@ bool is_another_segment(EdgeSet& es, Ellipse& outerEllipse, std::vector<int>& ou
                 ++cnt;
                 continue;
             }
+            // distances are >= 0 or NaN, so S < Sm needs S2 < Sm, and holds
+            // exactly when S2 is below sum_threshold(S1, Sm): most draws are
+            // decided by counting
+            dist_to_ellipse(q.Q, AP.data(), AP.size(), d2.data());
+            if (!median_below(d2.data(), d2.size(), Sm)) {
+                ++cnt;
+                continue;
+            }
             const float S1 = geo::median_ref(d);
-            d.resize(AP.size());
-            dist_to_ellipse(q.Q, AP.data(), AP.size(), d.data());
-            const float S2 = geo::median_ref(d);
+            if (!median_below(d2.data(), d2.size(), sum_threshold(S1, Sm))) {
+                ++cnt;
+                continue;
+            }
+            const float S2 = geo::median_ref(d2);
             const float S = S1 + S2;
             if (S < Sm) {
                 cnt = 0;
