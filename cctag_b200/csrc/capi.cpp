@@ -273,7 +273,7 @@ void cctagb_params_default(cctagb_params* p, int nCrowns)
     p->doIdentification = 1;
     p->maxEdges = 20000;
     p->refineMode = CCTAGB_REFINE_GRID;
-    p->gnIterations = 10;
+    p->gnIterations = 12;
     p->gnCoarseRounds = 1;
     p->edgeCapacityDivisor = 4;
     p->gnCoarseGrid = 3;

@@ -116,7 +116,7 @@ typedef struct cctagb_params {
     uint32_t maxEdges;                          /* 20000 (unused by the reference path) */
     /* B200-specific */
     int refineMode;                             /* CCTAGB_REFINE_GRID */
-    int gnIterations;                           /* 10: cost evaluations at most in REFINE_GAUSS_NEWTON */
+    int gnIterations;                           /* 12: cost evaluations at most in REFINE_GAUSS_NEWTON */
     int gnCoarseRounds;                         /* 1: grid rounds before Gauss-Newton */
     int edgeCapacityDivisor;                    /* 4: edge capacity per level = W*H/divisor */
     int hostThreads;                            /* 0: host threads of the candidate stage; 0 = one per physical core, less one per detection slot beyond the first */
