@@ -785,9 +785,19 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                 s_a[wid][i] = fabsf(__fdiv_rn(ym ? gx : gy, ym ? gy : gx));
             }
             __syncwarp();
-            int q = t0, t = 0, x = 0, y = 0, stpX = 0, stpY = 0, n = 0, gdx = 0, gdy = 0;
+            int q = t0, t = 0, x = 0, y = 0, n = 0, gdx = 0, gdy = 0;
+            int mx = 0, my = 0, nx = 0, ny = 0;  // major and minor step (the side probe is one major step back)
             float e = 0.f, dx = 0.f, dy = 0.f, a = 0.f;
             bool act = false, ymaj = false;
+            // the steps of the direction (dx, dy) along the axis chosen at the
+            // walk's start (the reference's dmaj / dmin signs)
+            auto set_steps = [&]() {
+                const int smaj = sgn_i(int(ymaj ? dy : dx)), smin = sgn_i(int(ymaj ? dx : dy));
+                mx = ymaj ? 0 : smaj;
+                my = ymaj ? smaj : 0;
+                nx = ymaj ? smin : 0;
+                ny = ymaj ? 0 : smin;
+            };
             while (true) {
                 const unsigned idle = __ballot_sync(kAll, !act);
                 if (!act) {
@@ -808,7 +818,7 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                         a = s_a[wid][i];
                         e = 0.f;
                         n = 0;
-                        stpX = stpY = 0;
+                        set_steps();
                     }
                 }
                 q += __popc(idle);
@@ -831,12 +841,12 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                         over = true;
                         continue;
                     }
-                    const float dmaj = ymaj ? dy : dx, dmin = ymaj ? dx : dy;
-                    const int smaj = sgn_i(int(dmaj)), smin = sgn_i(int(dmin));
                     e = __fadd_rn(e, a);
-                    if (ymaj) { stpY = smaj; stpX = smin; y += smaj; } else { stpX = smaj; stpY = smin; x += smaj; }
+                    x += mx;
+                    y += my;
                     if (e >= 0.5f) {
-                        if (ymaj) x += smin; else y += smin;
+                        x += nx;
+                        y += ny;
                         e = __fadd_rn(e, -1.f);
                     }
                     ++n;
@@ -848,14 +858,15 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                             const int d = (v > 0.f) - (v < 0.f);
                             dx = float(d * gdx);
                             dy = float(d * gdy);
+                            set_steps();
                         }
                         kind[j] = 0;
                     } else {
                         kind[j] = n > 2 ? 2 : 1;
                         px[j] = x;
                         py[j] = y;
-                        sx[j] = ymaj ? x : x - stpX;
-                        sy[j] = ymaj ? y - stpY : y;
+                        sx[j] = x - mx;
+                        sy[j] = y - my;
                     }
                 }
                 uint2 w[kWalkAhead], ws[kWalkAhead];
@@ -863,9 +874,9 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                 for (int j = 0; j < kWalkAhead; ++j) {
                     w[j] = ws[j] = make_uint2(0u, 0u);
                     if (kind[j] == 1 || kind[j] == 2) {
-                        if (px[j] >= 0 && px[j] < W && py[j] >= 0 && py[j] < H)
+                        if (unsigned(px[j]) < unsigned(W) && unsigned(py[j]) < unsigned(H))
                             w[j] = __ldg(&L.bitidx[size_t(py[j]) * WW + (px[j] >> 5)]);
-                        if (kind[j] == 2 && sx[j] >= 0 && sx[j] < W && sy[j] >= 0 && sy[j] < H)
+                        if (kind[j] == 2 && unsigned(sx[j]) < unsigned(W) && unsigned(sy[j]) < unsigned(H))
                             ws[j] = __ldg(&L.bitidx[size_t(sy[j]) * WW + (sx[j] >> 5)]);
                     }
                 }
@@ -873,7 +884,7 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                 // outside the level or at distSearch, else the index of the
                 // edge pixel met (-1 past a clamped edge count)
                 auto found = [&](uint2 v, int qx, int qy) -> int {
-                    if (qx < 0 || qx >= W || qy < 0 || qy >= H) return -1;
+                    if (unsigned(qx) >= unsigned(W) || unsigned(qy) >= unsigned(H)) return -1;
                     const uint32_t bit = 1u << (qx & 31);
                     if (!(v.x & bit)) return -2;
                     const int idx = int(v.y) + __popc(v.x & (bit - 1u));
