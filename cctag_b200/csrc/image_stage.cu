@@ -755,7 +755,6 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
     const unsigned below = (1u << lane) - 1u;
     const int gw = blockIdx.x * kWalkWarps + wid, NW = gridDim.x * kWalkWarps;
     const int nmax = vp.distSearch;
-    const float thr = float(vp.thrGradient);
     // chunk size: the launch's walks spread over its warps (a multiple of 32,
     // 32 .. kWalkChunk), the same in every block
     long long walks = 0;
@@ -773,31 +772,26 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
         for (; c < nch; c += NW) {
             const int t0 = c * chunk, t1 = min(2 * E, t0 + chunk);
             const int p0 = t0 >> 1, np = (t1 - t0) >> 1;
-            // the chunk's points, and |dmin / dmaj| per point (the same for
-            // both directions and before and after the re-orientation: the
-            // signs of both components flip together)
+            // the chunk's points, |dmin / dmaj| per point (the same for both
+            // directions) and the major and minor steps of the +1 direction,
+            // (x, y) components packed as value + 1 in 2 bits each (the -1
+            // direction's are their negatives)
             for (int i = lane; i < np; i += 32) {
                 const int xy = L.exy[p0 + i], g = L.grad[p0 + i];
-                const float gx = float(int16_t(g & 0xffff)), gy = float(g >> 16);
+                const int gxi = int16_t(g & 0xffff), gyi = g >> 16;
+                const float gx = float(gxi), gy = float(gyi);
                 const bool ym = fabsf(gy) > fabsf(gx);
+                const int smaj = sgn_i(ym ? gyi : gxi), smin = sgn_i(ym ? gxi : gyi);
                 s_xy[wid][i] = xy;
-                s_g[wid][i] = g;
+                s_g[wid][i] = ((ym ? 0 : smaj) + 1) | ((ym ? smaj : 0) + 1) << 2 | ((ym ? smin : 0) + 1) << 4 |
+                              ((ym ? 0 : smin) + 1) << 6;
                 s_a[wid][i] = fabsf(__fdiv_rn(ym ? gx : gy, ym ? gy : gx));
             }
             __syncwarp();
-            int q = t0, t = 0, x = 0, y = 0, n = 0, gdx = 0, gdy = 0;
+            int q = t0, t = 0, x = 0, y = 0, n = 0;
             int mx = 0, my = 0, nx = 0, ny = 0;  // major and minor step (the side probe is one major step back)
-            float e = 0.f, dx = 0.f, dy = 0.f, a = 0.f;
-            bool act = false, ymaj = false;
-            // the steps of the direction (dx, dy) along the axis chosen at the
-            // walk's start (the reference's dmaj / dmin signs)
-            auto set_steps = [&]() {
-                const int smaj = sgn_i(int(ymaj ? dy : dx)), smin = sgn_i(int(ymaj ? dx : dy));
-                mx = ymaj ? 0 : smaj;
-                my = ymaj ? smaj : 0;
-                nx = ymaj ? smin : 0;
-                ny = ymaj ? 0 : smin;
-            };
+            float e = 0.f, a = 0.f;
+            bool act = false;
             while (true) {
                 const unsigned idle = __ballot_sync(kAll, !act);
                 if (!act) {
@@ -806,19 +800,17 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                         t = k;
                         act = true;
                         const int i = (k - t0) >> 1;
-                        const int xy = s_xy[wid][i], g = s_g[wid][i];
+                        const int xy = s_xy[wid][i], st = s_g[wid][i];
                         const int dir = (k & 1) ? 1 : -1;
                         x = xy & 0xffff;
                         y = xy >> 16;
-                        gdx = int16_t(g & 0xffff);
-                        gdy = g >> 16;
-                        dx = float(dir * gdx);
-                        dy = float(dir * gdy);
-                        ymaj = fabsf(dy) > fabsf(dx);
+                        mx = dir * ((st & 3) - 1);
+                        my = dir * ((st >> 2 & 3) - 1);
+                        nx = dir * ((st >> 4 & 3) - 1);
+                        ny = dir * ((st >> 6 & 3) - 1);
                         a = s_a[wid][i];
                         e = 0.f;
                         n = 0;
-                        set_steps();
                     }
                 }
                 q += __popc(idle);
@@ -850,16 +842,12 @@ __global__ void __launch_bounds__(32 * kWalkWarps) k_walk(Levels lv, VoteParamsD
                         e = __fadd_rn(e, -1.f);
                     }
                     ++n;
+                    // After the first step the reference re-orients the walk
+                    // along the gradient at its start point (Bresenham.cpp:
+                    // 74-81): the direction already is dir * g, its product
+                    // with g is dir * |g|^2, so the direction stays dir * g
+                    // (0 when g is 0) and the steps are unchanged.
                     if (n == 1) {
-                        // after the first step: re-orient along the gradient
-                        // when the direction is long enough
-                        if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) > thr) {
-                            const float v = __fadd_rn(__fmul_rn(float(gdx), dx), __fmul_rn(float(gdy), dy));
-                            const int d = (v > 0.f) - (v < 0.f);
-                            dx = float(d * gdx);
-                            dy = float(d * gdy);
-                            set_steps();
-                        }
                         kind[j] = 0;
                     } else {
                         kind[j] = n > 2 ? 2 : 1;
