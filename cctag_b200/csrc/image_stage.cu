@@ -81,6 +81,13 @@ __device__ __forceinline__ int16_t sat_round16(float s)
     return int16_t(r);
 }
 
+// Gradient magnitude, rintf(sqrtf(dx^2 + dy^2)) as cvRecode.cpp:200-211.
+__device__ __forceinline__ int magnitude(int16_t gx, int16_t gy)
+{
+    const float fx = float(gx), fy = float(gy);
+    return int(rintf(__fsqrt_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)))));
+}
+
 __device__ __forceinline__ bool edge_bit(const LevelView& L, int x, int y)
 {
     return (L.bitmap[size_t(y) * L.WW + (x >> 5)] >> (x & 31)) & 1u;
@@ -224,10 +231,15 @@ __global__ void __launch_bounds__(128) k_deriv_nms(Levels lv, VoteParamsDev vp, 
                 }
             }
         }
+        // derivatives and magnitude of this thread's 8 pixels
+        const int xx = x0 - 1 + c;
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
-            s_dx[r0 + r][c] = sat_round16(ax[r]);
-            s_dy[r0 + r][c] = sat_round16(ay[r]);
+            const int16_t gx = sat_round16(ax[r]), gy = sat_round16(ay[r]);
+            s_dx[r0 + r][c] = gx;
+            s_dy[r0 + r][c] = gy;
+            const int yy = y0 - 1 + r0 + r;
+            s_mag[r0 + r][c] = xx >= 0 && xx < W && yy >= 0 && yy < H ? magnitude(gx, gy) : 0;
         }
     } else {
         // Derivatives supplied by the caller: load them with the same halo.
@@ -241,27 +253,17 @@ __global__ void __launch_bounds__(128) k_deriv_nms(Levels lv, VoteParamsDev vp, 
             }
             s_dx[r][c] = gx;
             s_dy[r][c] = gy;
+            s_mag[r][c] = xx >= 0 && xx < W && yy >= 0 && yy < H ? magnitude(gx, gy) : 0;
         }
     }
     __syncthreads();
-    // Magnitude, rintf(sqrtf(dx^2 + dy^2)) as cvRecode.cpp:200-211; 0 outside the image.
-    for (int i = t; i < kNmsD * kNmsD; i += 128) {
-        const int r = i / kNmsD, c = i % kNmsD;
-        const int yy = y0 - 1 + r, xx = x0 - 1 + c;
-        int m = 0;
-        if (xx >= 0 && xx < W && yy >= 0 && yy < H) {
-            const float fx = float(s_dx[r][c]), fy = float(s_dy[r][c]);
-            m = int(rintf(__fsqrt_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)))));
-        }
-        s_mag[r][c] = m;
-    }
-    __syncthreads();
-    // NMS, cvRecode.cpp:258-323.
+    // NMS, cvRecode.cpp:258-323: lane ox of warp w takes column ox of rows
+    // w, w + 4, ...
     const int TG22 = int(0.4142135623730950488016887242097 * (1 << 15) + 0.5);
-    for (int i = t; i < kNmsT * kNmsT; i += 128) {
-        const int oy = i / kNmsT, ox = i % kNmsT;
+    const int ox = t & 31;
+    for (int oy = t >> 5; oy < kNmsT; oy += 4) {
         const int x = x0 + ox, y = y0 + oy;
-        if (x >= W || y >= H) continue;
+        if (ox >= kNmsT || x >= W || y >= H) continue;
         const int r = oy + 1, c = ox + 1;
         int gx = s_dx[r][c], gy = s_dy[r][c];
         const int s = gx ^ gy;
