@@ -355,12 +355,11 @@ bool ellipse_growing_init(const EdgeSet& es, const std::vector<int>& fc, Ellipse
 // it is marked, so no later pass can grow anything from it (marks only grow
 // until the growing loop resets them).
 bool connected_point(std::vector<int>& pts, RunMarks& mk, EdgeSet& es, const Ellipse& qIn, const Ellipse& qOut,
-                     int p)
+                     int p, std::vector<EdgeSet::DfsFrame>& st)
 {
     static const int xoff[8] = {1, 1, 0, -1, -1, -1, 0, 1};
     static const int yoff[8] = {0, -1, -1, -1, 0, 1, 1, 1};
     using Frame = EdgeSet::DfsFrame;
-    thread_local std::vector<Frame> st;  // reused across calls of this thread
     st.clear();
     mk.set(p);  // the reference marks the start point; a listed point already is
     st.push_back({es.x(p), es.y(p), 0});
@@ -397,14 +396,14 @@ bool connected_point(std::vector<int>& pts, RunMarks& mk, EdgeSet& es, const Ell
 // EllipseGrowing.cpp:443-457.  sat[i]: list point i is saturated (skipped:
 // it would add nothing and mark nothing).
 void ellipse_hull(EdgeSet& es, std::vector<int>& pts, const Ellipse& e, float delta, RunMarks& mk,
-                  std::vector<uint8_t>& sat)
+                  std::vector<uint8_t>& sat, std::vector<EdgeSet::DfsFrame>& st)
 {
     Ellipse qIn, qOut;
     geo::compute_hull(e, delta, qIn, qOut);
     const size_t init = pts.size();
     sat.resize(init, 0);
     for (size_t i = 0; i < init; ++i)
-        if (!sat[i] && connected_point(pts, mk, es, qIn, qOut, pts[i])) sat[i] = 1;
+        if (!sat[i] && connected_point(pts, mk, es, qIn, qOut, pts[i], st)) sat[i] = 1;
 }
 
 size_t count_in_hull(const EdgeSet& es, const std::vector<int>& pts, const Ellipse& e, float width)
@@ -423,6 +422,7 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
 {
     thread_local RunMarks mk;
     thread_local std::vector<uint8_t> sat;  // saturated list points (connected_point)
+    thread_local std::vector<EdgeSet::DfsFrame> st;  // connected_point's depth-first stack
     mk.begin(size_t(es.E));
     sat.clear();
     outer = fc;
@@ -435,7 +435,7 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
         ++nIter;
         while (newSize - lastSize > 0) {
             lastSize = int(count_in_hull(es, outer, ellipse, width));
-            ellipse_hull(es, outer, ellipse, width, mk, sat);
+            ellipse_hull(es, outer, ellipse, width, mk, sat, st);
             sets.push_back(outer);
             ells.push_back(ellipse);
             ellipse = fit_circle_points(es, outer);
@@ -457,7 +457,7 @@ void ellipse_growing2(EdgeSet& es, const std::vector<int>& fc, std::vector<int>&
     size_t lastSize = 0;
     while (outer.size() > lastSize) {
         lastSize = outer.size();
-        ellipse_hull(es, outer, ellipse, width, mk, sat);
+        ellipse_hull(es, outer, ellipse, width, mk, sat, st);
         ellipse = fit_points(es, outer);
     }
 }

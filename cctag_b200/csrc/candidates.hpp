@@ -42,10 +42,9 @@ struct EdgeSet {
     std::vector<int32_t> n_segment_out;
     std::vector<uint32_t> link_stamp;  // edge linking: point visited in call `link_token`
     uint32_t link_token = 0;
-    struct DfsFrame {
+    struct DfsFrame {  // one level of the ellipse-growing depth-first search
         int x, y, k;
     };
-    std::vector<DfsFrame> dfs_stack;  // ellipse-growing DFS scratch
 
     int x(int i) const { return exy[i] & 0xffff; }
     int y(int i) const { return exy[i] >> 16; }
