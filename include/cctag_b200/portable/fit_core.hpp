@@ -24,6 +24,9 @@
 #include <cfloat>
 #include <cmath>
 #include <cstddef>
+#if defined(__SSE2__) && !defined(__CUDA_ARCH__)
+#include <emmintrin.h>
+#endif
 
 #include "pmath.hpp"
 
@@ -54,25 +57,25 @@ CCTAGB_HD inline FitCplx cx_div(FitCplx a, FitCplx b)
     return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
 }
 
-// Real cube root (sign kept): Newton's iteration from an estimate of the right
-// binary magnitude, to convergence.
+// Real cube root (sign kept): Newton's iteration from 2^k, k = floor(log8 a)
+// (the power of two whose cube brings a into [1, 8)), until an iterate
+// repeats, at most 60 steps.  When the iterates settle into two alternating
+// values the 60th is known without running the rest.
 CCTAGB_HD inline double cbrt_d(double y)
 {
     if (y == 0.0 || !(y == y) || ::fabs(y) > DBL_MAX) return y;
     const double a = ::fabs(y);
-    // estimate: 2^(floor(log2 a) / 3) by halving / doubling
-    double x = 1.0, t = a;
-    while (t >= 8.0) {
-        t *= 0.125;
-        x *= 2.0;
-    }
-    while (t < 1.0) {
-        t *= 8.0;
-        x *= 0.5;
-    }
+    const int e = ::ilogb(a);  // floor(log2 a)
+    const int k = e >= 0 ? e / 3 : -((2 - e) / 3);
+    double x = ::ldexp(1.0, k), prev = 0.0;
     for (int it = 0; it < 60; ++it) {
         const double nx = x - (x * x * x - a) / (3.0 * x * x);
         if (nx == x) break;
+        if (it > 0 && nx == prev) {  // x_(it+1) == x_(it-1): x_60 is x_(it-1) or x_it
+            x = (61 - it) % 2 == 0 ? prev : x;
+            break;
+        }
+        prev = x;
         x = nx;
     }
     return y < 0.0 ? -x : x;
@@ -227,6 +230,50 @@ CCTAGB_HD inline int fit_ellipse_core(PointAt pt, size_t n, float& ocx, float& o
     double a00 = 0, a01 = 0, a02 = 0, a11 = 0, a12 = 0, a22 = 0;  // S1
     double b00 = 0, b01 = 0, b02 = 0, b10 = 0, b11 = 0, b12 = 0, b20 = 0, b21 = 0, b22 = 0;  // S2
     double c00 = 0, c01 = 0, c02 = 0, c11 = 0, c12 = 0, c22 = 0;  // S3
+#if defined(__SSE2__) && !defined(__CUDA_ARCH__)
+    // The same products and sums, two accumulators per SSE2 operation (IEEE
+    // double multiplies and adds; each accumulator is still summed in point
+    // order, so the results are the same bits).  S3's x x, x y, y y are the
+    // q0, q1, q2 products.
+    {
+        const __m128d z = _mm_setzero_pd(), vo = _mm_set_pd(oy, ox);
+        __m128d A0 = z, A1 = z, A2 = z;                // (a00 a01) (a02 a11) (a12 a22)
+        __m128d B0 = z, B1 = z, B2 = z, B3 = z, B4 = z;  // (b00 b01) (b10 b11) (b20 b21) (b02 b12) (b22 c00)
+        __m128d C0 = z, C1 = z;                        // (c01 c11) (c02 c12)
+        for (size_t i = 0; i < n; ++i) {
+            float xf, yf;
+            pt(i, xf, yf);
+            const __m128d xy = _mm_sub_pd(_mm_set_pd(double(yf), double(xf)), vo);  // (x, y)
+            const __m128d q01 = _mm_mul_pd(_mm_unpacklo_pd(xy, xy), xy);            // (q0, q1)
+            const __m128d yy = _mm_unpackhi_pd(xy, xy);
+            const __m128d q22 = _mm_mul_pd(yy, yy);                                 // (q2, q2)
+            const __m128d q00 = _mm_unpacklo_pd(q01, q01), q11 = _mm_unpackhi_pd(q01, q01);
+            const __m128d q12 = _mm_shuffle_pd(q01, q22, 1);                        // (q1, q2)
+            A0 = _mm_add_pd(A0, _mm_mul_pd(q00, q01));
+            A1 = _mm_add_pd(A1, _mm_mul_pd(q01, _mm_shuffle_pd(q22, q01, 2)));     // (q0 q2, q1 q1)
+            A2 = _mm_add_pd(A2, _mm_mul_pd(q12, q22));
+            B0 = _mm_add_pd(B0, _mm_mul_pd(q00, xy));
+            B1 = _mm_add_pd(B1, _mm_mul_pd(q11, xy));
+            B2 = _mm_add_pd(B2, _mm_mul_pd(q22, xy));
+            B3 = _mm_add_pd(B3, q01);
+            B4 = _mm_add_pd(B4, _mm_shuffle_pd(q22, q01, 0));                      // (q2, q0)
+            C0 = _mm_add_pd(C0, q12);
+            C1 = _mm_add_pd(C1, xy);
+            c22 += 1.0;
+        }
+        double v[2];
+        _mm_storeu_pd(v, A0), a00 = v[0], a01 = v[1];
+        _mm_storeu_pd(v, A1), a02 = v[0], a11 = v[1];
+        _mm_storeu_pd(v, A2), a12 = v[0], a22 = v[1];
+        _mm_storeu_pd(v, B0), b00 = v[0], b01 = v[1];
+        _mm_storeu_pd(v, B1), b10 = v[0], b11 = v[1];
+        _mm_storeu_pd(v, B2), b20 = v[0], b21 = v[1];
+        _mm_storeu_pd(v, B3), b02 = v[0], b12 = v[1];
+        _mm_storeu_pd(v, B4), b22 = v[0], c00 = v[1];
+        _mm_storeu_pd(v, C0), c01 = v[0], c11 = v[1];
+        _mm_storeu_pd(v, C1), c02 = v[0], c12 = v[1];
+    }
+#else
     for (size_t i = 0; i < n; ++i) {
         float xf, yf;
         pt(i, xf, yf);
@@ -254,6 +301,7 @@ CCTAGB_HD inline int fit_ellipse_core(PointAt pt, size_t n, float& ocx, float& o
         c12 += y;
         c22 += 1.0;
     }
+#endif
     const double S1[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
     const double S2[3][3] = {{b00, b01, b02}, {b10, b11, b12}, {b20, b21, b22}};
     const double S3[3][3] = {{c00, c01, c02}, {c01, c11, c12}, {c02, c12, c22}};
