@@ -740,8 +740,9 @@ __global__ void __launch_bounds__(128) k_emit(Levels lv, int rows_total)
 // depend on the schedule.
 constexpr int kWalkWarps = 8;
 constexpr int kWalkChunk = 512;  // walks (two per point) a warp takes at once, at most
-// steps a lane takes per iteration (16-frame C2 launch: 1 step 0.71 ms, 2 steps
-// 0.63 ms, 4 steps 0.69 ms, 8 steps 0.92 ms: more lookahead costs occupancy)
+// steps a lane takes per iteration (16-frame C2 launch: 2 steps 0.50 ms, 3 steps
+// 0.52 ms; with the steps re-derived per step, 1 step 0.71 ms, 4 steps 0.69 ms,
+// 8 steps 0.92 ms: more lookahead costs occupancy)
 constexpr int kWalkAhead = 2;
 
 __device__ __forceinline__ int sgn_i(int v) { return (v > 0) - (v < 0); }
