@@ -650,7 +650,8 @@ def _c3_frame(seed):
 
 def run_c3(args, flush, torch, peak, peak_src):
     """4K clutter (C3): 3840x2160 frames with 30 markers, 200 distractor
-    ellipses and 300 line segments (1-3 M Canny edge points).  Frames/s of a
+    ellipses, 300 line segments and a band-limited background texture (about
+    1.7 M Canny edge points, 1.2 M on level 0).  Frames/s of a
     4-frame batch per call, the edge points and votes, per-stage GB/s and the
     roofline of the dominant image-stage kernel group, and the CPU baseline."""
     import cctag_b200

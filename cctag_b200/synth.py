@@ -200,10 +200,16 @@ def _draw_distractors(rng, canvas, n_ellipses, n_lines):
 def render_frame(width, height, n_markers, radius_range, max_tilt_deg, *, seed, bg=128.0,
                  noise_sigma=4.0, blur_sigma=1.0, motion_len=0.0, motion_angle=0.0,
                  illum_grad=0.0, n_ellipses=0, n_lines=0, margin=1.3, ss=None,
-                 bank=THREE_CROWNS, white=235.0, black=20.0) -> Frame:
-    """Render one frame; markers do not overlap (rejection placement)."""
+                 bank=THREE_CROWNS, white=235.0, black=20.0, texture=(0.0, 0.0)) -> Frame:
+    """Render one frame; markers do not overlap (rejection placement).
+    texture = (amplitude, sigma): a band-limited background (white noise
+    blurred by sigma px, scaled to that standard deviation) under the
+    distractors and markers, for clutter with dense edges."""
     rng = np.random.default_rng(seed)
     canvas = np.full((height, width), bg, np.float32)
+    if texture[0] > 0:
+        t = _gauss_blur(rng.standard_normal((height, width)).astype(np.float32), texture[1])
+        canvas += np.float32(texture[0]) * t / max(float(t.std()), 1e-6)
     if n_ellipses or n_lines:
         _draw_distractors(rng, canvas, n_ellipses, n_lines)
     focal = 1.2 * max(width, height)
@@ -251,8 +257,10 @@ def config_frame(name: str, seed: int = 0) -> Frame:
                             motion_len=float(rng.uniform(0, 5)), motion_angle=float(rng.uniform(0, np.pi)),
                             illum_grad=40.0)
     if name == "c3_4k_clutter":
+        # a band-limited background texture brings the Canny points into the
+        # 1-3 M range of this workload (about 1.2 M on level 0)
         return render_frame(3840, 2160, 30, (15, 300), 60, seed=seed, noise_sigma=6.0, blur_sigma=1.0,
-                            n_ellipses=200, n_lines=300)
+                            n_ellipses=200, n_lines=300, texture=(6.0, 2.0))
     if name == "small":
         return render_frame(320, 240, 1, (40, 60), 30, seed=seed, noise_sigma=3.0, blur_sigma=1.0)
     raise ValueError(f"unknown configuration {name!r}")

@@ -86,8 +86,9 @@ def test_canny_from_opencv_derivatives(detector, orc, opencv_cases):
 
 
 def test_clutter_4k_vote_counts(detector, orc):
-    """Clutter stress: 4K with distractor ellipses and lines, integer vote
-    counts bit-exact at every level."""
+    """Clutter stress: 4K with distractor ellipses, lines and a textured
+    background (about 1.7 M edge points), integer vote counts bit-exact at
+    every level."""
     img = config_frame("c3_4k_clutter", seed=3).image
     detector.image_stage(img)
     for lvl, src in enumerate(orc.pyramid(img, 4)):
