@@ -27,3 +27,12 @@ def test_oracle_fp32_matches_fp64_refinement(orc):
     assert [m.id for m in a] == [m.id for m in b]
     for m, n in zip(a, b):
         assert np.hypot(m.x - n.x, m.y - n.y) < 0.05
+
+
+def test_clutter_frames_have_the_workload_edge_density(orc):
+    """The 4K clutter workload's frames carry 1-3 M Canny edge points over the
+    pyramid (its stated range), most of them on level 0."""
+    img = config_frame("c3_4k_clutter", seed=300).image
+    counts = [int((orc.level(lv)[2] != 0).sum()) for lv in orc.pyramid(img, 4)]
+    assert 1_000_000 <= sum(counts) <= 3_000_000, counts
+    assert counts[0] >= 1_000_000, counts
